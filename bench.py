@@ -1,0 +1,316 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 epsilon-div-div operator apply (TerraNeo hot path).
+
+Workload (one "step"): one FP64 EpsilonDivDivKerngen apply, Dirichlet on both
+radii, Replace mode with the additive inter-diamond halo, on the level-6 thick
+shell r in [0.55, 1] (10 diamonds x 64 x 64 x 64 cells, 2,746,250 stored nodes,
+7,987,590 velocity DoFs), viscosity k = exp(ln(1e4) (0.5 radial ramp + 0.5
+Gaussian-blob field)) clamped to contrast 1e4, src ~ N(0,1) made consistent on
+duplicated nodes.  GDoF/s = unique velocity DoFs / time per apply, the
+reference's definition (apps/benchmarks/performance/benchmark_operators.cpp:208).
+
+Inputs rotate over 4 (src, dst) buffer sets (4 x 132 MB > 126 MB L2) so no
+step reads data cached by the previous one.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+For N > 1 (torchrun) every rank runs the same apply on its own GPU (replicas:
+the ten diamonds of one shell fit one GPU), timed with CUDA
+events, max over ranks; value is the aggregate over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "L6 Stokes time-to-1e-8 (FP32-MG+FP64 refine vs FP64); apply GDoF/s, %HBM"
+LEVEL, RMIN, RMAX = 6, 0.55, 1.0
+BYTES_PER_NODE_F64 = 56  # 3 src + 1 k + 3 dst doubles per stored node
+BYTES_PER_NODE_F32 = 28
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def synthetic_inputs(coords, radii, omask_lat, seed=2024):
+    """Seeded k and src fields in the reference layout (numpy, host)."""
+    n1 = radii.shape[1]
+    rng = np.random.default_rng(seed)
+    rho = (radii - RMIN) / (RMAX - RMIN)
+    x = coords[:, :, :, None, :] * radii[:, None, None, :, None]
+    field = np.zeros((10, n1, n1, n1))
+    for _ in range(6):
+        c = rng.normal(size=3)
+        c = c / np.linalg.norm(c) * rng.uniform(RMIN, RMAX)
+        w = rng.uniform(0.1, 0.3)
+        field += np.exp(-np.sum((x - c) ** 2, axis=-1) / (2 * w * w))
+    field = (field - field.min()) / (field.max() - field.min())
+    k = np.clip(np.exp(np.log(1e4) * (0.5 * rho[:, None, None, :] + 0.5 * field)), 1.0, 1e4)
+    src = rng.normal(size=(3, 10, n1, n1, n1))
+    return k, src
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx, self.rows, self.proc = str(gpu_index), [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) >= 9:
+                for n, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(steps):
+    """The reference's own Kokkos-OpenMP apply (oracle/_ref), else the C oracle, on this host."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
+    cores = os.cpu_count() or 1
+    dofs = 3 * (10 * (1 << LEVEL) ** 2 + 2) * ((1 << LEVEL) + 1)
+    if os.path.exists(ref):
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="spread", OMP_PLACES="cores")
+        out = subprocess.run([ref, "time_kerngen", str(LEVEL), str(RMIN), str(RMAX), "1", "1", str(steps)],
+                             env=env, capture_output=True, text=True, timeout=1800)
+        line = [l for l in out.stdout.splitlines() if l.startswith("{")]
+        if out.returncode == 0 and line:
+            info = json.loads(line[-1])
+            sec = info["seconds_per_apply"]
+            return {"value": dofs / sec / 1e9, "unit": "GDoF/s", "cores": info["threads"], "kind": "reference",
+                    "sample": f"{steps} EpsilonDivDivKerngen<double> applies (Dirichlet/Dirichlet, level {LEVEL}) "
+                              f"after 1 warm-up, Kokkos-OpenMP, {info['threads']} threads",
+                    "seconds_per_apply": sec}
+    # C restatement (single thread) as fallback
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Mesh
+    m = Mesh(LEVEL, RMIN, RMAX)
+    k = np.ones(m.shape)
+    u = np.ones((3,) + m.shape)
+    t0 = time.perf_counter()
+    m.kerngen(k, u, 1, 1, False)
+    sec = time.perf_counter() - t0
+    return {"value": dofs / sec / 1e9, "unit": "GDoF/s", "cores": 1, "kind": "port",
+            "sample": f"1 oracle apply (Dirichlet/Dirichlet, level {LEVEL}), single thread", "seconds_per_apply": sec}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    steps = max(1, min(args.steps, 10))
+    cb = cpu_baseline(steps)
+    line = {"metric": METRIC, "impl": "reference", "value": cb["value"], "unit": "GDoF/s", "n_gpus": args.gpus,
+            "steps": steps, "warmup": 1, "ms_per_step": cb["seconds_per_apply"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"EpsilonDivDivKerngen apply, level {LEVEL} shell (7,987,590 velocity DoFs), "
+                                   "Dirichlet/Dirichlet, FP64"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    from terraneo_b200 import shell, _capi as C
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    assert args.warmup >= 3, "at least 3 warm-up steps"
+
+    mesh = shell.ShellMesh(LEVEL, RMIN, RMAX)
+    coords, radii = mesh.geometry()
+    _, omask = mesh.masks()
+    k_np, src_np = synthetic_inputs(coords, radii, omask)
+    k = shell.VectorQ1Scalar(mesh)
+    k.set_numpy(k_np)
+    nsets = 4
+    srcs, dsts = [], []
+    for i in range(nsets):
+        s = shell.VectorQ1Vec(mesh)
+        s.set_numpy(np.roll(src_np, i, axis=-1))
+        # consistent on duplicated nodes: keep owner values, then sum copies
+        s.data.mul_(torch.as_tensor(omask, device="cuda", dtype=torch.float64))
+        s.halo_sum()
+        srcs.append(s)
+        dsts.append(shell.VectorQ1Vec(mesh))
+    op = shell.EpsilonDivDivKerngen(mesh, k, C.BC_DIRICHLET, C.BC_DIRICHLET)
+    stream = torch.cuda.current_stream()
+
+    def step(i):
+        shell.apply(op, srcs[i % nsets], dsts[i % nsets])
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for i in range(args.steps):
+            step(i)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    dofs = 3 * mesh.unique_nodes
+    value = world * dofs / (ms * 1e-3) / 1e9
+
+    # dominant kernel alone: Neumann/Neumann without communication is exactly one
+    # launch of the tiled apply kernel (same per-cell work as the headline step)
+    op_k = shell.EpsilonDivDivKerngen(mesh, k, C.BC_NEUMANN, C.BC_NEUMANN, comm_mode=C.COMM_SKIP)
+    for i in range(3):
+        shell.apply(op_k, srcs[i % nsets], dsts[i % nsets])
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for i in range(args.steps):
+        shell.apply(op_k, srcs[i % nsets], dsts[i % nsets])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    kms = ev0.elapsed_time(ev1) / args.steps
+    alg_bytes = BYTES_PER_NODE_F64 * mesh.stored_nodes
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg_bytes / (kms * 1e-3) / 1e9
+
+    # FP32 apply (same workload, FP32 storage and arithmetic)
+    k32 = shell.VectorQ1Scalar(mesh, torch.float32)
+    k32.data.copy_(k.data)
+    s32 = [shell.VectorQ1Vec(mesh, torch.float32) for _ in range(nsets)]
+    d32 = [shell.VectorQ1Vec(mesh, torch.float32) for _ in range(nsets)]
+    for a, b in zip(s32, srcs):
+        a.data.copy_(b.data)
+    op32 = shell.EpsilonDivDivKerngen(mesh, k32, C.BC_DIRICHLET, C.BC_DIRICHLET)
+    for i in range(3):
+        shell.apply(op32, s32[i % nsets], d32[i % nsets])
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for i in range(args.steps):
+        shell.apply(op32, s32[i % nsets], d32[i % nsets])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms32 = ev0.elapsed_time(ev1) / args.steps
+
+    # end to end through the public API with host buffers: pinned H2D of src,
+    # apply, D2H of dst, every step
+    h_src = torch.empty((3,) + mesh.shape, dtype=torch.float64).pin_memory()
+    h_src.copy_(srcs[0].data.cpu())
+    h_dst = torch.empty_like(h_src).pin_memory()
+    e_src, e_dst = shell.VectorQ1Vec(mesh), shell.VectorQ1Vec(mesh)
+    e2e_steps = max(3, args.steps // 5)
+    for i in range(2):
+        e_src.data.copy_(h_src, non_blocking=True)
+        shell.apply(op, e_src, e_dst)
+        h_dst.copy_(e_dst.data, non_blocking=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for i in range(e2e_steps):
+        e_src.data.copy_(h_src, non_blocking=True)
+        shell.apply(op, e_src, e_dst)
+        h_dst.copy_(e_dst.data, non_blocking=True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    vec_bytes = 3 * mesh.stored_nodes * 8
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "EpsilonDivDivKerngen FP64 apply, level-6 shell (10x64x64x64 cells, "
+                                   "7,987,590 velocity DoFs), Dirichlet/Dirichlet, Replace + halo",
+                       "l2": "inputs rotate over 4 buffer sets (528 MB > 126 MB L2)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "kernel": "kerngen_tile_kernel<double>", "kernel_ms": round(kms, 5),
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
+            "fp32_apply": {"value": round(world * dofs / (ms32 * 1e-3) / 1e9, 3), "unit": "GDoF/s",
+                           "ms_per_step": round(ms32, 5)},
+            "e2e": {"value": round(world * dofs / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GDoF/s",
+                    "h2d_bytes_per_step": vec_bytes, "d2h_bytes_per_step": vec_bytes},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            cb = cpu_baseline(steps=3)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,143 @@
+/* terraneo_b200: C ABI of the B200 (sm_100a) matrix-free hot path of TerraNeo.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, returns
+ * an int status (0 = success, negative = error, see TN_ERR_*) and never throws.
+ * Device pointers are CUDA global-memory pointers of the current device;
+ * `stream` is a cudaStream_t (NULL = legacy default stream).  Apply and vector
+ * kernels are asynchronous on `stream`; functions that return a host scalar
+ * (dot products, norms) synchronise that stream before returning, which keeps
+ * the reference's synchronous semantics at every apply_impl / dot_impl.
+ *
+ * Data layout is the reference's own (src/terra/grid/grid_types.hpp:12-57):
+ * a scalar field is [10][N+1][N+1][N+1] (diamond, x, y, r), r fastest; a vector
+ * field is three such scalar fields passed as three pointers (the reference's
+ * Grid4DDataVec holds three separate scalar views).  N = 2^level, one
+ * subdomain per diamond, all ten diamonds on one GPU.
+ *
+ * Boundary-condition codes follow grid/shell/bit_masks.hpp:24:
+ * 0 = NEUMANN, 1 = DIRICHLET, 2 = FREESLIP. */
+#ifndef TERRANEO_B200_H
+#define TERRANEO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined( __GNUC__ )
+#define TN_API __attribute__( ( visibility( "default" ) ) )
+#else
+#define TN_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TN_OK 0
+#define TN_ERR_ARG -1      /* invalid argument (sizes, codes, null pointers) */
+#define TN_ERR_CUDA -2     /* a CUDA runtime call failed */
+#define TN_ERR_NOMEM -3    /* device or host allocation failed */
+#define TN_ERR_STATE -4    /* object not set up for this call */
+
+#define TN_BC_NEUMANN 0
+#define TN_BC_DIRICHLET 1
+#define TN_BC_FREESLIP 2
+
+/* OperatorApplyMode / OperatorCommunicationMode (linalg/operator.hpp:29-44) */
+#define TN_APPLY_REPLACE 0
+#define TN_APPLY_ADD 1
+#define TN_COMM_SKIP 0
+#define TN_COMM_ADDITIVE 1
+
+typedef struct tn_mesh tn_mesh;
+
+/* Last error message of the calling thread (never NULL). */
+TN_API const char* tn_last_error( void );
+
+/* ---------------------------------------------------------------------------
+ * Shell mesh: geometry, masks and the duplicated-node (halo) map.
+ * Replaces DistributedDomain::create_uniform_single_subdomain_per_diamond
+ * (grid/shell/spherical_shell.hpp:2520), subdomain_unit_sphere_single_shell_coords
+ * (:2724), subdomain_shell_radii (:2759), setup_node_ownership_mask_data
+ * (grid/bit_masks.hpp:29) and setup_boundary_mask_data (grid/shell/bit_masks.hpp:82).
+ * `level` refines laterally and radially alike (N = 2^level cells per side). */
+TN_API int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** out );
+TN_API int tn_mesh_destroy( tn_mesh* mesh );
+/* stored nodes = 10 (N+1)^3, unique nodes = (10 N^2 + 2)(N+1) */
+TN_API int tn_mesh_dims( const tn_mesh* mesh, int* level, size_t* stored_nodes, size_t* unique_nodes );
+/* host copies: coords [10][N+1][N+1][3], radii [10][N+1] (either may be NULL) */
+TN_API int tn_mesh_geometry( const tn_mesh* mesh, double* coords, double* radii );
+/* host copies of the boundary flags (1 INNER, 6 CMB, 10 SURFACE) and the
+ * ownership flags (1 OWNED), both [10][N+1][N+1][N+1] (either may be NULL) */
+TN_API int tn_mesh_masks( const tn_mesh* mesh, uint8_t* boundary_mask, uint8_t* ownership_mask );
+
+/* Additive inter-diamond halo: every copy of a duplicated node becomes the sum
+ * of all copies.  Replaces send_recv_with_plan / pack_send_and_recv +
+ * unpack_and_reduce_local_subdomain_boundaries (communication/shell/
+ * communication.hpp:242-747, communication_plan.hpp:48-68) for one GPU. */
+TN_API int tn_halo_sum_f64( const tn_mesh* mesh, double* const* fields, int nfields, void* stream );
+TN_API int tn_halo_sum_f32( const tn_mesh* mesh, float* const* fields, int nfields, void* stream );
+
+/* ---------------------------------------------------------------------------
+ * EpsilonDivDivKerngen::apply_impl (fe/wedge/operators/shell/epsilon_divdiv_kerngen.hpp:513)
+ * a(u,v) = int k (2 eps(u):eps(v) - 2/3 div u div v), one-point quadrature;
+ * Dirichlet / Neumann / free-slip at CMB and SURFACE; `diagonal` != 0 gives the
+ * diagonal-only action; with free-slip on both boundaries the rigid-rotation
+ * penalty dst += eps_p sum_i (m_i^T src) m_i is added (eps_p = penalty_eps,
+ * the reference default is 1, :138).  `k` is the nodal coefficient field. */
+typedef struct
+{
+    int    bc_cmb;
+    int    bc_surface;
+    int    diagonal;
+    int    apply_mode; /* TN_APPLY_* */
+    int    comm_mode;  /* TN_COMM_* */
+    double penalty_eps;
+} tn_epsdivdiv_params;
+
+TN_API int tn_epsdivdiv_apply_f64( const tn_mesh* mesh, const tn_epsdivdiv_params* p, const double* k,
+                            const double* const* src, double* const* dst, void* stream );
+TN_API int tn_epsdivdiv_apply_f32( const tn_mesh* mesh, const tn_epsdivdiv_params* p, const float* k,
+                            const float* const* src, float* const* dst, void* stream );
+
+/* ---------------------------------------------------------------------------
+ * Laplace::apply_impl (fe/wedge/operators/shell/laplace.hpp:68): int grad u . grad v,
+ * 3x2 Felippa quadrature; treat_boundary != 0 eliminates the CMB/SURFACE
+ * Dirichlet rows and columns keeping the diagonal; diagonal != 0 gives the
+ * diagonal-only action. */
+TN_API int tn_laplace_apply_f64( const tn_mesh* mesh, int treat_boundary, int diagonal, int apply_mode, int comm_mode,
+                          const double* src, double* dst, void* stream );
+TN_API int tn_laplace_apply_f32( const tn_mesh* mesh, int treat_boundary, int diagonal, int apply_mode, int comm_mode,
+                          const float* src, float* dst, void* stream );
+
+/* ---------------------------------------------------------------------------
+ * Krylov vector kernels (kernels/common/grid_operations.hpp).  A vector is
+ * `ncomp` scalar fields (1 or 3) of stored-node length.
+ *
+ * lincomb: y = c0 + sum_i c[i] x_i, nx = 0..3 (grid_operations.hpp:12,154;
+ *          VectorQ1Vec::lincomb_impl, linalg/vector_q1.hpp:52-87)
+ * dot:     owned-node dot product summed over components, compensated FP64
+ *          accumulation in both precisions (masked_dot_product, :644)
+ * others:  invert_inplace (:253), mult_elementwise_inplace (:273),
+ *          max_abs_entry (:337), has_nan_or_inf (:714), cast (:746). */
+TN_API int tn_vec_lincomb_f64( const tn_mesh* mesh, int ncomp, double* const* y, double c0, int nx, const double* c,
+                        const double* const* x, void* stream );
+TN_API int tn_vec_lincomb_f32( const tn_mesh* mesh, int ncomp, float* const* y, double c0, int nx, const double* c,
+                        const float* const* x, void* stream );
+TN_API int tn_vec_dot_f64( const tn_mesh* mesh, int ncomp, const double* const* a, const double* const* b, double* result,
+                    void* stream );
+TN_API int tn_vec_dot_f32( const tn_mesh* mesh, int ncomp, const float* const* a, const float* const* b, double* result,
+                    void* stream );
+TN_API int tn_vec_invert_f64( const tn_mesh* mesh, int ncomp, double* const* y, void* stream );
+TN_API int tn_vec_invert_f32( const tn_mesh* mesh, int ncomp, float* const* y, void* stream );
+TN_API int tn_vec_mult_f64( const tn_mesh* mesh, int ncomp, double* const* y, const double* const* x, void* stream );
+TN_API int tn_vec_mult_f32( const tn_mesh* mesh, int ncomp, float* const* y, const float* const* x, void* stream );
+TN_API int tn_vec_max_abs_f64( const tn_mesh* mesh, int ncomp, const double* const* x, double* result, void* stream );
+TN_API int tn_vec_has_nan_or_inf_f64( const tn_mesh* mesh, int ncomp, const double* const* x, int* result, void* stream );
+TN_API int tn_vec_has_nan_or_inf_f32( const tn_mesh* mesh, int ncomp, const float* const* x, int* result, void* stream );
+TN_API int tn_vec_cast_f64_to_f32( const tn_mesh* mesh, int ncomp, float* const* y, const double* const* x, void* stream );
+TN_API int tn_vec_cast_f32_to_f64( const tn_mesh* mesh, int ncomp, double* const* y, const float* const* x, void* stream );
+
+#ifdef __cplusplus
+}
+#endif
+#endif

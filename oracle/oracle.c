@@ -1,0 +1,649 @@
+/* CPU restatement of the reference's hot path (TEST INFRASTRUCTURE, not the
+ * product).  See oracle.h for layout conventions.  Plain scalar C; every
+ * function names the reference code it restates. */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define NDIAMOND 10
+
+static inline size_t lat_idx( int n1, int d, int x, int y ) { return ( (size_t) d * n1 + x ) * n1 + y; }
+static inline size_t node_idx( int n1, int d, int x, int y, int r )
+{
+    return ( ( (size_t) d * n1 + x ) * n1 + y ) * n1 + r;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Mesh: grid/shell/spherical_shell.hpp                                      */
+/* ------------------------------------------------------------------------ */
+
+static void normalize3( double v[3] )
+{
+    /* dense/vec.hpp:76-98: norm = sqrt(sum of squares), divide if > 1e-15 */
+    double s = 0.0;
+    for ( int i = 0; i < 3; ++i )
+        s += v[i] * v[i];
+    double m = sqrt( s );
+    if ( m > 1e-15 )
+        for ( int i = 0; i < 3; ++i )
+            v[i] /= m;
+}
+
+/* Icosahedral base points and diamond table: spherical_shell.hpp:420-559.
+ * Diamond corners p00 = pole, pN0 = "left", pNN = opposite, p0N = "right". */
+static void diamond_corners( int diamond, double p00[3], double pN0[3], double pNN[3], double p0N[3] )
+{
+    double node[12][3];
+    double fifthpi = 0.4 * asin( 1.0 );
+    double w       = 2.0 * acos( 1.0 / ( 2.0 * sin( fifthpi ) ) );
+    double cosw = cos( w ), sinw = sin( w );
+    node[0][0] = 0.0, node[0][1] = 0.0, node[0][2] = 1.0;
+    node[11][0] = 0.0, node[11][1] = 0.0, node[11][2] = -1.0;
+    for ( int k = 1; k <= 5; ++k )
+    {
+        double phi = 2.0 * ( (double) k - 0.5 ) * fifthpi;
+        node[k][0] = sinw * cos( phi ), node[k][1] = sinw * sin( phi ), node[k][2] = cosw;
+    }
+    for ( int k = 1; k <= 5; ++k )
+    {
+        double phi     = 2.0 * ( (double) k - 1 ) * fifthpi;
+        node[k + 5][0] = sinw * cos( phi ), node[k + 5][1] = sinw * sin( phi ), node[k + 5][2] = -cosw;
+    }
+    static const int dn[10][4] = { { 0, 5, 6, 1 },   { 0, 1, 7, 2 },  { 0, 2, 8, 3 },  { 0, 3, 9, 4 },
+                                   { 0, 4, 10, 5 },  { 11, 7, 1, 6 }, { 11, 8, 2, 7 }, { 11, 9, 3, 8 },
+                                   { 11, 10, 4, 9 }, { 11, 6, 5, 10 } };
+    int L = diamond < 5 ? 1 : 3, R = diamond < 5 ? 3 : 1;
+    for ( int i = 0; i < 3; ++i )
+    {
+        p00[i] = node[dn[diamond][0]][i];
+        pN0[i] = node[dn[diamond][L]][i];
+        pNN[i] = node[dn[diamond][2]][i];
+        p0N[i] = node[dn[diamond][R]][i];
+    }
+}
+
+/* compute_node_recursive (spherical_shell.hpp:231-346): each new point is
+ * normalize(p1 + p2) of its two parents on the next-coarser grid; rows
+ * (i%l==0, j%l==l/2), columns (i%l==l/2, j%l==0), diagonals (both l/2, parents
+ * (i-l/2, j+l/2) and (i+l/2, j-l/2)).  Restated level by level, coarse to fine. */
+void or_unit_sphere_coords( int L, double* coords )
+{
+    const int N = 1 << L, n1 = N + 1;
+    for ( int d = 0; d < NDIAMOND; ++d )
+    {
+        double* c = coords + (size_t) d * n1 * n1 * 3;
+#define P( i, j ) ( c + ( (size_t) ( i ) * n1 + ( j ) ) * 3 )
+        diamond_corners( d, P( 0, 0 ), P( N, 0 ), P( N, N ), P( 0, N ) );
+        for ( int l = N; l >= 2; l /= 2 )
+        {
+            const int h = l / 2;
+            for ( int i = 0; i <= N; i += h )
+                for ( int j = 0; j <= N; j += h )
+                {
+                    const int ri = i % l, rj = j % l;
+                    const double *a, *b;
+                    if ( ri == 0 && rj == h )
+                        a = P( i, j - h ), b = P( i, j + h );
+                    else if ( ri == h && rj == 0 )
+                        a = P( i - h, j ), b = P( i + h, j );
+                    else if ( ri == h && rj == h )
+                        a = P( i - h, j + h ), b = P( i + h, j - h );
+                    else
+                        continue;
+                    double* o = P( i, j );
+                    for ( int k = 0; k < 3; ++k )
+                        o[k] = a[k] + b[k];
+                    normalize3( o );
+                }
+        }
+#undef P
+    }
+}
+
+/* uniform_shell_radii (spherical_shell.hpp:28-50) + subdomain_shell_radii (:2759) */
+void or_shell_radii( int L, double rmin, double rmax, double* radii )
+{
+    const int    N    = 1 << L;
+    const double step = ( rmax - rmin ) / N;
+    for ( int d = 0; d < NDIAMOND; ++d )
+    {
+        for ( int i = 0; i <= N; ++i )
+            radii[d * ( N + 1 ) + i] = rmin + i * step;
+        radii[d * ( N + 1 ) + N] = rmax;
+    }
+}
+
+/* setup_boundary_mask_data (grid/shell/bit_masks.hpp:82-137):
+ * INNER = 1 everywhere, CMB = 6 at r = 0, SURFACE = 10 at r = N. */
+void or_boundary_mask( int L, uint8_t* bmask )
+{
+    const int n1 = ( 1 << L ) + 1;
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < n1; ++x )
+            for ( int y = 0; y < n1; ++y )
+                for ( int r = 0; r < n1; ++r )
+                    bmask[node_idx( n1, d, x, y, r )] = r == 0 ? 6 : ( r == n1 - 1 ? 10 : 1 );
+}
+
+/* Duplicated lateral positions: nodes of different diamonds that are the
+ * same point on the sphere (shared diamond edges and icosahedral vertices).
+ * They are found by exact comparison of the unit-sphere coordinates, which
+ * the bisection produces bit-identically on both sides of a shared edge. */
+typedef struct
+{
+    double c[3];
+    int    d, x, y;
+} LatNode;
+
+static int cmp_latnode( const void* pa, const void* pb )
+{
+    const LatNode* a = (const LatNode*) pa;
+    const LatNode* b = (const LatNode*) pb;
+    for ( int k = 0; k < 3; ++k )
+    {
+        if ( a->c[k] < b->c[k] )
+            return -1;
+        if ( a->c[k] > b->c[k] )
+            return 1;
+    }
+    return a->d - b->d;
+}
+
+/* Returns sorted lateral nodes; *ngroups groups given by start offsets. */
+static LatNode* build_groups( int L, const double* coords, int** gstart, int* ngroups )
+{
+    const int n1 = ( 1 << L ) + 1;
+    const int nl = NDIAMOND * n1 * n1;
+    LatNode*  v  = (LatNode*) malloc( sizeof( LatNode ) * nl );
+    int       t  = 0;
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < n1; ++x )
+            for ( int y = 0; y < n1; ++y, ++t )
+            {
+                memcpy( v[t].c, coords + lat_idx( n1, d, x, y ) * 3, sizeof( double ) * 3 );
+                v[t].d = d, v[t].x = x, v[t].y = y;
+            }
+    qsort( v, nl, sizeof( LatNode ), cmp_latnode );
+    int* gs = (int*) malloc( sizeof( int ) * ( nl + 1 ) );
+    int  g  = 0;
+    for ( int i = 0; i < nl; ++i )
+        if ( i == 0 || memcmp( v[i].c, v[i - 1].c, sizeof( double ) * 3 ) != 0 )
+            gs[g++] = i;
+    gs[g]    = nl;
+    *gstart  = gs;
+    *ngroups = g;
+    return v;
+}
+
+/* setup_node_ownership_mask_data (grid/bit_masks.hpp:29-80): a node is OWNED
+ * (1) on the copy whose global subdomain id is the minimum among all copies;
+ * with one subdomain per diamond that is the lowest diamond id. */
+void or_ownership_mask( int L, const double* coords, uint8_t* omask )
+{
+    const int n1 = ( 1 << L ) + 1;
+    int *     gs, ng;
+    LatNode*  v = build_groups( L, coords, &gs, &ng );
+    memset( omask, 0, (size_t) NDIAMOND * n1 * n1 * n1 );
+    for ( int g = 0; g < ng; ++g )
+    {
+        const LatNode* o = &v[gs[g]]; /* sorted by diamond inside a group */
+        for ( int r = 0; r < n1; ++r )
+            omask[node_idx( n1, o->d, o->x, o->y, r )] = 1;
+    }
+    free( gs );
+    free( v );
+}
+
+/* Additive halo exchange (communication/shell/communication.hpp:242-747 and
+ * communication_plan.hpp:48-68): every copy of a duplicated node receives the
+ * sum of all copies. */
+void or_halo_sum( int L, const double* coords, double* field, int ncomp )
+{
+    const int    n1 = ( 1 << L ) + 1;
+    const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1;
+    int *        gs, ng;
+    LatNode*     v = build_groups( L, coords, &gs, &ng );
+    for ( int c = 0; c < ncomp; ++c )
+    {
+        double* f = field + c * ns;
+        for ( int g = 0; g < ng; ++g )
+        {
+            if ( gs[g + 1] - gs[g] < 2 )
+                continue;
+            for ( int r = 0; r < n1; ++r )
+            {
+                double s = 0.0;
+                for ( int i = gs[g]; i < gs[g + 1]; ++i )
+                    s += f[node_idx( n1, v[i].d, v[i].x, v[i].y, r )];
+                for ( int i = gs[g]; i < gs[g + 1]; ++i )
+                    f[node_idx( n1, v[i].d, v[i].x, v[i].y, r )] = s;
+            }
+        }
+    }
+    free( gs );
+    free( v );
+}
+
+double or_masked_dot( size_t n, const double* a, const double* b, const uint8_t* omask )
+{
+    /* kernels/common/grid_operations.hpp:644 masked_dot_product */
+    double s = 0.0;
+    for ( size_t i = 0; i < n; ++i )
+        if ( omask[i] & 1 )
+            s += a[i] * b[i];
+    return s;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Wedge geometry: fe/wedge/integrands.hpp, kernel_helpers.hpp               */
+/* ------------------------------------------------------------------------ */
+
+/* wedge node -> (dx, dy, dr) inside the hex cell (kernel_helpers.hpp:26-60,
+ * epsilon_divdiv_kerngen.hpp:1160-1162) */
+static const int WNODE[2][6][3] = { { { 0, 0, 0 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 }, { 1, 0, 1 }, { 0, 1, 1 } },
+                                    { { 1, 1, 0 }, { 0, 1, 0 }, { 1, 0, 0 }, { 1, 1, 1 }, { 0, 1, 1 }, { 1, 0, 1 } } };
+
+/* Jacobian of x = r(zeta) ((1-xi-eta) p0 + xi p1 + eta p2) (integrands.hpp:634-681) */
+static void wedge_jac( const double* p[3], double r1, double r2, double xi, double eta, double zeta, double J[3][3] )
+{
+    const double r  = r1 + 0.5 * ( r2 - r1 ) * ( 1 + zeta );
+    const double dr = 0.5 * ( r2 - r1 );
+    for ( int a = 0; a < 3; ++a )
+    {
+        J[a][0] = ( p[1][a] - p[0][a] ) * r;
+        J[a][1] = ( p[2][a] - p[0][a] ) * r;
+        J[a][2] = ( ( 1 - xi - eta ) * p[0][a] + xi * p[1][a] + eta * p[2][a] ) * dr;
+    }
+}
+
+static double det3( double J[3][3] )
+{
+    return J[0][0] * ( J[1][1] * J[2][2] - J[1][2] * J[2][1] ) - J[0][1] * ( J[1][0] * J[2][2] - J[1][2] * J[2][0] ) +
+           J[0][2] * ( J[1][0] * J[2][1] - J[1][1] * J[2][0] );
+}
+
+/* inverse transposed: IT[a][b] = (J^{-1})[b][a] */
+static void inv_transposed3( double J[3][3], double det, double IT[3][3] )
+{
+    const double id = 1.0 / det;
+    IT[0][0]        = ( J[1][1] * J[2][2] - J[1][2] * J[2][1] ) * id;
+    IT[0][1]        = ( J[1][2] * J[2][0] - J[1][0] * J[2][2] ) * id;
+    IT[0][2]        = ( J[1][0] * J[2][1] - J[1][1] * J[2][0] ) * id;
+    IT[1][0]        = ( J[0][2] * J[2][1] - J[0][1] * J[2][2] ) * id;
+    IT[1][1]        = ( J[0][0] * J[2][2] - J[0][2] * J[2][0] ) * id;
+    IT[1][2]        = ( J[0][1] * J[2][0] - J[0][0] * J[2][1] ) * id;
+    IT[2][0]        = ( J[0][1] * J[1][2] - J[0][2] * J[1][1] ) * id;
+    IT[2][1]        = ( J[0][2] * J[1][0] - J[0][0] * J[1][2] ) * id;
+    IT[2][2]        = ( J[0][0] * J[1][1] - J[0][1] * J[1][0] ) * id;
+}
+
+/* reference-element gradient of wedge shape function n (integrands.hpp:160-227) */
+static void grad_shape_ref( int n, double xi, double eta, double zeta, double g[3] )
+{
+    static const double gxi[3] = { -1.0, 1.0, 0.0 }, geta[3] = { -1.0, 0.0, 1.0 };
+    const double        nrad   = n < 3 ? 0.5 * ( 1 - zeta ) : 0.5 * ( 1 + zeta );
+    const double        grad   = n < 3 ? -0.5 : 0.5;
+    const double        lat[3] = { 1.0 - xi - eta, xi, eta };
+    g[0]                       = gxi[n % 3] * nrad;
+    g[1]                       = geta[n % 3] * nrad;
+    g[2]                       = lat[n % 3] * grad;
+}
+
+static void wedge_lateral_points( int n1, const double* coords, int d, int x, int y, int w, const double* p[3] )
+{
+    for ( int i = 0; i < 3; ++i )
+        p[i] = coords + lat_idx( n1, d, x + WNODE[w][i][0], y + WNODE[w][i][1] ) * 3;
+}
+
+/* trafo_mat_cartesian_to_normal_tangential
+ * (linalg/trafo/local_basis_trafo_normal_tangential.hpp:36-73): rows n, t1, t2 */
+static void trafo_nt( const double nin[3], double R[3][3] )
+{
+    double n[3] = { nin[0], nin[1], nin[2] };
+    normalize3( n );
+    const double ax = fabs( n[0] ), ay = fabs( n[1] ), az = fabs( n[2] );
+    double       ref[3] = { 0, 0, 0 };
+    if ( ax <= ay && ax <= az )
+        ref[0] = 1;
+    else if ( ay <= ax && ay <= az )
+        ref[1] = 1;
+    else
+        ref[2] = 1;
+    double t1[3] = { ref[1] * n[2] - ref[2] * n[1], ref[2] * n[0] - ref[0] * n[2], ref[0] * n[1] - ref[1] * n[0] };
+    normalize3( t1 );
+    if ( sqrt( t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2] ) < 1e-15 )
+    {
+        t1[0] = n[1], t1[1] = -n[0], t1[2] = 0;
+        normalize3( t1 );
+    }
+    double t2[3] = { n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0] };
+    normalize3( t2 );
+    for ( int k = 0; k < 3; ++k )
+        R[0][k] = n[k], R[1][k] = t1[k], R[2][k] = t2[k];
+}
+
+/* ------------------------------------------------------------------------ */
+/* EpsilonDivDivKerngen (fe/wedge/operators/shell/epsilon_divdiv_kerngen.hpp) */
+/* ------------------------------------------------------------------------ */
+
+/* One-point (centroid) quadrature of the wedge: physical gradients g[6][3]
+ * and kwJ = mean nodal k * |det J| (kerngen :1189-1259). */
+static void kerngen_wedge_geometry( const double* p[3], double r0, double r1, const double kn[6], double g[6][3],
+                                    double* kwJ )
+{
+    double J[3][3], IT[3][3];
+    wedge_jac( p, r0, r1, 1.0 / 3.0, 1.0 / 3.0, 0.0, J );
+    const double det = det3( J );
+    inv_transposed3( J, det, IT );
+    double ks = 0.0;
+    for ( int n = 0; n < 6; ++n )
+        ks += kn[n];
+    *kwJ = ( ks / 6.0 ) * fabs( det );
+    for ( int n = 0; n < 6; ++n )
+    {
+        double gr[3];
+        grad_shape_ref( n, 1.0 / 3.0, 1.0 / 3.0, 0.0, gr );
+        for ( int a = 0; a < 3; ++a )
+            g[n][a] = IT[a][0] * gr[0] + IT[a][1] * gr[1] + IT[a][2] * gr[2];
+    }
+}
+
+static void fs_project( const double n[3], double v[3] )
+{
+    const double dt = n[0] * v[0] + n[1] * v[1] + n[2] * v[2];
+    for ( int k = 0; k < 3; ++k )
+        v[k] -= dt * n[k];
+}
+
+/* Penalty null modes for free-slip on both boundaries (kerngen :287-408):
+ * m_i = tangential part of (e_i x x) on boundary nodes, Gram-Schmidt
+ * orthonormalised with owned-masked dot products. modes: [3][3*ns]. */
+static void kerngen_null_modes( int L, const double* coords, const double* radii, const uint8_t* omask, double* modes )
+{
+    const int    n1 = ( 1 << L ) + 1;
+    const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1;
+    for ( int ax = 0; ax < 3; ++ax )
+    {
+        double* m = modes + (size_t) ax * 3 * ns;
+        for ( int d = 0; d < NDIAMOND; ++d )
+            for ( int x = 0; x < n1; ++x )
+                for ( int y = 0; y < n1; ++y )
+                    for ( int r = 0; r < n1; ++r )
+                    {
+                        const size_t  i  = node_idx( n1, d, x, y, r );
+                        const double* u  = coords + lat_idx( n1, d, x, y ) * 3;
+                        const double  rr = radii[d * n1 + r];
+                        double        c[3] = { u[0] * rr, u[1] * rr, u[2] * rr };
+                        double        v[3] = { 0, 0, 0 };
+                        const int     a1 = ( ax + 1 ) % 3, a2 = ( ax + 2 ) % 3;
+                        v[a1]              = c[a2];
+                        v[a2]              = -c[a1];
+                        if ( r == 0 || r == n1 - 1 )
+                        {
+                            double n[3] = { u[0], u[1], u[2] };
+                            normalize3( n );
+                            fs_project( n, v );
+                        }
+                        for ( int k = 0; k < 3; ++k )
+                            m[k * ns + i] = v[k];
+                    }
+    }
+    for ( int i = 0; i < 3; ++i )
+    {
+        double* mi = modes + (size_t) i * 3 * ns;
+        for ( int j = 0; j < i; ++j )
+        {
+            double* mj = modes + (size_t) j * 3 * ns;
+            double  dt = 0.0;
+            for ( int k = 0; k < 3; ++k )
+                dt += or_masked_dot( ns, mi + k * ns, mj + k * ns, omask );
+            for ( size_t t = 0; t < 3 * ns; ++t )
+                mi[t] -= dt * mj[t];
+        }
+        double nn = 0.0;
+        for ( int k = 0; k < 3; ++k )
+            nn += or_masked_dot( ns, mi + k * ns, mi + k * ns, omask );
+        const double inv = 1.0 / sqrt( nn );
+        for ( size_t t = 0; t < 3 * ns; ++t )
+            mi[t] *= inv;
+    }
+}
+
+/* Matrix-free apply of the production viscous operator
+ *   a(u, v) = int k (2 eps(u):eps(v) - 2/3 div u div v)
+ * with one-point quadrature, restating the fast Dirichlet/Neumann path
+ * (kerngen :1055-1389), the fast free-slip path (:1421-1940) and the fs/fs
+ * penalty (:585-606) followed by the additive halo (:611-616).  Replace mode. */
+void or_kerngen_apply( int L, const double* coords, const double* radii, const double* k, const double* src,
+                       double* dst, int bc_cmb, int bc_surf, int diag )
+{
+    const int    N = 1 << L, n1 = N + 1;
+    const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1;
+    memset( dst, 0, sizeof( double ) * 3 * ns );
+
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                {
+                    const int at_cmb = r == 0, at_surf = r == N - 1;
+                    const int cmb_dir = at_cmb && bc_cmb == 1, surf_dir = at_surf && bc_surf == 1;
+                    const int cmb_fs = at_cmb && bc_cmb == 2, surf_fs = at_surf && bc_surf == 2;
+                    /* node of cell-corner (dx,dy,dr) -> 8-slot accumulator */
+                    double acc[2][2][2][3];
+                    double ann[2][2][2];
+                    memset( acc, 0, sizeof( acc ) );
+                    memset( ann, 0, sizeof( ann ) );
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const double* p[3];
+                        wedge_lateral_points( n1, coords, d, x, y, w, p );
+                        double kn[6], s[6][3], sp[6][3], nrm[6][3];
+                        for ( int n = 0; n < 6; ++n )
+                        {
+                            const int    X = x + WNODE[w][n][0], Y = y + WNODE[w][n][1], Rr = r + WNODE[w][n][2];
+                            const size_t i = node_idx( n1, d, X, Y, Rr );
+                            kn[n]          = k[i];
+                            for ( int c = 0; c < 3; ++c )
+                                s[n][c] = sp[n][c] = src[c * ns + i];
+                            const double* u = coords + lat_idx( n1, d, X, Y ) * 3;
+                            nrm[n][0] = u[0], nrm[n][1] = u[1], nrm[n][2] = u[2];
+                            normalize3( nrm[n] );
+                            if ( ( cmb_fs && n < 3 ) || ( surf_fs && n >= 3 ) )
+                                fs_project( nrm[n], sp[n] );
+                        }
+                        double g[6][3], kwJ;
+                        kerngen_wedge_geometry( p, radii[d * n1 + r], radii[d * n1 + r + 1], kn, g, &kwJ );
+                        /* Dirichlet boundary nodes drop out of gather and scatter (matvec only) */
+                        int active[6];
+                        for ( int n = 0; n < 6; ++n )
+                            active[n] = diag ? 1 : !( ( cmb_dir && n < 3 ) || ( surf_dir && n >= 3 ) );
+                        if ( !diag )
+                        {
+                            double G[3][3] = { { 0 } }, div = 0.0;
+                            for ( int n = 0; n < 6; ++n )
+                                if ( active[n] )
+                                    for ( int a = 0; a < 3; ++a )
+                                        for ( int b = 0; b < 3; ++b )
+                                            G[a][b] += g[n][a] * sp[n][b]; /* G[a][b] = sum g_a u_b */
+                            div = G[0][0] + G[1][1] + G[2][2];
+                            double E[3][3];
+                            for ( int a = 0; a < 3; ++a )
+                                for ( int b = 0; b < 3; ++b )
+                                    E[a][b] = 0.5 * ( G[a][b] + G[b][a] );
+                            for ( int n = 0; n < 6; ++n )
+                            {
+                                if ( !active[n] )
+                                    continue;
+                                double* o = acc[WNODE[w][n][0]][WNODE[w][n][1]][WNODE[w][n][2]];
+                                for ( int c = 0; c < 3; ++c )
+                                    o[c] += kwJ * ( 2.0 * ( g[n][0] * E[0][c] + g[n][1] * E[1][c] + g[n][2] * E[2][c] ) -
+                                                    ( 2.0 / 3.0 ) * g[n][c] * div );
+                                if ( ( cmb_fs && n < 3 ) || ( surf_fs && n >= 3 ) )
+                                {
+                                    const double gg = g[n][0] * g[n][0] + g[n][1] * g[n][1] + g[n][2] * g[n][2];
+                                    const double ng = nrm[n][0] * g[n][0] + nrm[n][1] * g[n][1] + nrm[n][2] * g[n][2];
+                                    ann[WNODE[w][n][0]][WNODE[w][n][1]][WNODE[w][n][2]] += kwJ * ( gg + ng * ng / 3.0 );
+                                }
+                            }
+                        }
+                        /* diagonal blocks: all nodes in diagonal mode, Dirichlet nodes in matvec mode */
+                        for ( int n = 0; n < 6; ++n )
+                        {
+                            const int is_dir = ( cmb_dir && n < 3 ) || ( surf_dir && n >= 3 );
+                            const int is_fs  = ( cmb_fs && n < 3 ) || ( surf_fs && n >= 3 );
+                            if ( !( diag || is_dir ) )
+                                continue;
+                            double*      o  = acc[WNODE[w][n][0]][WNODE[w][n][1]][WNODE[w][n][2]];
+                            const double gg = g[n][0] * g[n][0] + g[n][1] * g[n][1] + g[n][2] * g[n][2];
+                            if ( diag && is_fs )
+                            {
+                                /* R^T diag(R A_nn R^T) R s, A_nn = kwJ (|g|^2 I + g g^T / 3) */
+                                double R[3][3], Rg[3], Rs[3], v[3];
+                                trafo_nt( nrm[n], R );
+                                for ( int a = 0; a < 3; ++a )
+                                {
+                                    Rg[a] = R[a][0] * g[n][0] + R[a][1] * g[n][1] + R[a][2] * g[n][2];
+                                    Rs[a] = R[a][0] * s[n][0] + R[a][1] * s[n][1] + R[a][2] * s[n][2];
+                                    v[a]  = kwJ * ( gg + Rg[a] * Rg[a] / 3.0 ) * Rs[a];
+                                }
+                                for ( int c = 0; c < 3; ++c )
+                                    o[c] += R[0][c] * v[0] + R[1][c] * v[1] + R[2][c] * v[2];
+                            }
+                            else
+                            {
+                                for ( int c = 0; c < 3; ++c )
+                                    o[c] += kwJ * s[n][c] * ( gg + g[n][c] * g[n][c] / 3.0 );
+                            }
+                        }
+                    }
+                    /* free-slip: test-side projection + normal-normal add back (:1880-1935) */
+                    if ( !diag && ( cmb_fs || surf_fs ) )
+                    {
+                        const int dr = cmb_fs ? 0 : 1;
+                        for ( int dx = 0; dx < 2; ++dx )
+                            for ( int dy = 0; dy < 2; ++dy )
+                            {
+                                const size_t  i   = node_idx( n1, d, x + dx, y + dy, r + dr );
+                                const double* u   = coords + lat_idx( n1, d, x + dx, y + dy ) * 3;
+                                double        n[3] = { u[0], u[1], u[2] };
+                                normalize3( n );
+                                double* o = acc[dx][dy][dr];
+                                fs_project( n, o );
+                                const double un = n[0] * src[i] + n[1] * src[ns + i] + n[2] * src[2 * ns + i];
+                                for ( int c = 0; c < 3; ++c )
+                                    o[c] += ann[dx][dy][dr] * un * n[c];
+                            }
+                    }
+                    for ( int dx = 0; dx < 2; ++dx )
+                        for ( int dy = 0; dy < 2; ++dy )
+                            for ( int dr = 0; dr < 2; ++dr )
+                            {
+                                const size_t i = node_idx( n1, d, x + dx, y + dy, r + dr );
+                                for ( int c = 0; c < 3; ++c )
+                                    dst[c * ns + i] += acc[dx][dy][dr][c];
+                            }
+                }
+
+    if ( !diag && bc_cmb == 2 && bc_surf == 2 )
+    {
+        /* dst += eps * sum_i (m_i^T src)_owned m_i on every stored node, eps = 1 */
+        uint8_t* om    = (uint8_t*) malloc( ns );
+        double*  modes = (double*) malloc( sizeof( double ) * 9 * ns );
+        or_ownership_mask( L, coords, om );
+        kerngen_null_modes( L, coords, radii, om, modes );
+        for ( int i = 0; i < 3; ++i )
+        {
+            const double* m  = modes + (size_t) i * 3 * ns;
+            double        al = 0.0;
+            for ( int c = 0; c < 3; ++c )
+                al += or_masked_dot( ns, m + c * ns, src + c * ns, om );
+            for ( size_t t = 0; t < 3 * ns; ++t )
+                dst[t] += al * m[t];
+        }
+        free( modes );
+        free( om );
+    }
+    or_halo_sum( L, coords, dst, 3 );
+}
+
+/* ------------------------------------------------------------------------ */
+/* Laplace (fe/wedge/operators/shell/laplace.hpp:106-330), 3x2 Felippa rule  */
+/* ------------------------------------------------------------------------ */
+
+static const double QP32[6][3] = { { 0.6666666666666666, 0.1666666666666667, -0.5773502691896257 },
+                                   { 0.1666666666666667, 0.6666666666666666, -0.5773502691896257 },
+                                   { 0.1666666666666667, 0.1666666666666667, -0.5773502691896257 },
+                                   { 0.6666666666666666, 0.1666666666666667, 0.5773502691896257 },
+                                   { 0.1666666666666667, 0.6666666666666666, 0.5773502691896257 },
+                                   { 0.1666666666666667, 0.1666666666666667, 0.5773502691896257 } };
+static const double QW32       = 0.1666666666666667;
+
+void or_laplace_apply( int L, const double* coords, const double* radii, const double* src, double* dst,
+                       int treat_boundary, int diag )
+{
+    const int    N = 1 << L, n1 = N + 1;
+    const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1;
+    memset( dst, 0, sizeof( double ) * ns );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                {
+                    /* bottom check wins when a cell touches both (laplace.hpp:140-168) */
+                    const int bot = treat_boundary && r == 0;
+                    const int top = treat_boundary && !bot && r == N - 1;
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const double* p[3];
+                        wedge_lateral_points( n1, coords, d, x, y, w, p );
+                        size_t idx[6];
+                        double s[6], out[6] = { 0 };
+                        for ( int n = 0; n < 6; ++n )
+                        {
+                            idx[n] = node_idx( n1, d, x + WNODE[w][n][0], y + WNODE[w][n][1], r + WNODE[w][n][2] );
+                            s[n]   = src[idx[n]];
+                        }
+                        for ( int q = 0; q < 6; ++q )
+                        {
+                            double J[3][3], IT[3][3], g[6][3];
+                            wedge_jac( p, radii[d * n1 + r], radii[d * n1 + r + 1], QP32[q][0], QP32[q][1], QP32[q][2], J );
+                            const double det = det3( J );
+                            inv_transposed3( J, det, IT );
+                            for ( int n = 0; n < 6; ++n )
+                            {
+                                double gr[3];
+                                grad_shape_ref( n, QP32[q][0], QP32[q][1], QP32[q][2], gr );
+                                for ( int a = 0; a < 3; ++a )
+                                    g[n][a] = IT[a][0] * gr[0] + IT[a][1] * gr[1] + IT[a][2] * gr[2];
+                            }
+                            const double wdet = QW32 * fabs( det );
+                            /* coupled node set: all, or the side away from the Dirichlet boundary */
+                            int lo = 0, hi = 6;
+                            if ( bot )
+                                lo = 3;
+                            if ( top )
+                                hi = 3;
+                            if ( diag )
+                                lo = 6, hi = 6;
+                            double gu[3] = { 0, 0, 0 };
+                            for ( int n = lo; n < hi; ++n )
+                                for ( int a = 0; a < 3; ++a )
+                                    gu[a] += s[n] * g[n][a];
+                            for ( int n = lo; n < hi; ++n )
+                                out[n] += wdet * ( g[n][0] * gu[0] + g[n][1] * gu[1] + g[n][2] * gu[2] );
+                            for ( int n = 0; n < 6; ++n )
+                            {
+                                const int dg = diag || ( bot && n < 3 ) || ( top && n >= 3 );
+                                if ( dg )
+                                    out[n] += wdet * s[n] * ( g[n][0] * g[n][0] + g[n][1] * g[n][1] + g[n][2] * g[n][2] );
+                            }
+                        }
+                        for ( int n = 0; n < 6; ++n )
+                            dst[idx[n]] += out[n];
+                    }
+                }
+    or_halo_sum( L, coords, dst, 1 );
+}

@@ -1,0 +1,49 @@
+/* CPU restatement of the reference's hot-path algorithms (TEST INFRASTRUCTURE).
+ *
+ * This library is the oracle: tests/, __graft_entry__.smoke() and the CPU
+ * baseline leg of bench.py use it to check the CUDA product.  The product
+ * never links, loads or calls it.  Each function cites the reference file
+ * (path inside the reference project) whose behaviour it restates.
+ *
+ * Parity pinning: tests/test_oracle_pinning.py compares these functions with
+ * the reference itself (compiled by oracle/ref_build into oracle/_ref) and
+ * with the committed fixtures in tests/golden/ generated from it.
+ *
+ * Layout conventions (identical to the reference, grid/grid_types.hpp:12-57):
+ *   lateral coords  [10][N+1][N+1][3]   unit-sphere points of each diamond
+ *   radii           [10][N+1]
+ *   scalar field    [10][N+1][N+1][N+1] (diamond, x, y, r), r fastest
+ *   vector field    3 scalar fields one after another (SoA)
+ * with N = 2^L cells per diamond side and one subdomain per diamond.
+ * Boundary-condition codes: 0 Neumann, 1 Dirichlet, 2 free-slip. */
+#ifndef TN_ORACLE_H
+#define TN_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* mesh + masks */
+void or_unit_sphere_coords( int L, double* coords );
+void or_shell_radii( int L, double rmin, double rmax, double* radii );
+void or_boundary_mask( int L, uint8_t* bmask );
+void or_ownership_mask( int L, const double* coords, uint8_t* omask );
+/* duplicated-node additive reduction (halo SUM) of ncomp scalar fields */
+void or_halo_sum( int L, const double* coords, double* field, int ncomp );
+
+/* operators (Replace mode, additive communication) */
+void or_kerngen_apply( int L, const double* coords, const double* radii, const double* k, const double* src,
+                       double* dst, int bc_cmb, int bc_surf, int diag );
+void or_laplace_apply( int L, const double* coords, const double* radii, const double* src, double* dst,
+                       int treat_boundary, int diag );
+
+/* Krylov vector kernels */
+double or_masked_dot( size_t n, const double* a, const double* b, const uint8_t* omask );
+
+#ifdef __cplusplus
+}
+#endif
+#endif

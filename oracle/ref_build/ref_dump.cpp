@@ -1,0 +1,216 @@
+// Reference dump/timing driver (test infrastructure, never shipped).
+//
+// Compiles the reference's own header-only implementation of the hot path on
+// Kokkos-OpenMP and exposes it as a command-line tool that reads seeded inputs
+// from raw little-endian files and writes the reference's outputs, so the C
+// restatement in oracle/ and the CUDA product can be compared with the
+// reference itself.  Inputs are always generated outside (never with the
+// reference's non-deterministic `randomize`).
+//
+// File layout of every field: the reference's own (subdomain, x, y, r) order,
+// r fastest; vector fields are three such scalar blocks one after another
+// (Grid4DDataVec is SoA, grid/grid_types.hpp:57).
+//
+// Commands (bc codes: 0 = Neumann, 1 = Dirichlet, 2 = free-slip):
+//   mesh    L rmin rmax OUT               coords/radii/boundary+ownership masks
+//   kerngen L rmin rmax bcc bcs diag DIR  EpsilonDivDivKerngen<double> apply
+//   laplace L rmin rmax treat diag DIR    Laplace<double> apply
+//   time_kerngen L rmin rmax bcc bcs reps prints seconds per apply (CPU baseline)
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "communication/shell/communication.hpp"
+#include "fe/wedge/operators/shell/epsilon_divdiv_kerngen.hpp"
+#include "fe/wedge/operators/shell/laplace.hpp"
+#include "grid/bit_masks.hpp"
+#include "grid/shell/bit_masks.hpp"
+#include "grid/shell/spherical_shell.hpp"
+#include "linalg/vector_q1.hpp"
+#include "util/init.hpp"
+
+using namespace terra;
+using grid::shell::BoundaryConditionFlag;
+using grid::shell::BoundaryConditions;
+using grid::shell::DistributedDomain;
+using grid::shell::ShellBoundaryFlag;
+
+namespace {
+
+template < typename T >
+std::vector< T > read_file( const std::string& path, size_t n )
+{
+    std::vector< T > v( n );
+    std::ifstream    f( path, std::ios::binary );
+    if ( !f )
+        throw std::runtime_error( "cannot open " + path );
+    f.read( reinterpret_cast< char* >( v.data() ), n * sizeof( T ) );
+    if ( size_t( f.gcount() ) != n * sizeof( T ) )
+        throw std::runtime_error( "short read " + path );
+    return v;
+}
+
+template < typename T >
+void write_file( const std::string& path, const T* p, size_t n )
+{
+    std::ofstream f( path, std::ios::binary );
+    f.write( reinterpret_cast< const char* >( p ), n * sizeof( T ) );
+}
+
+template < typename View >
+void view_from_host( View& v, const typename View::value_type* src )
+{
+    auto h = Kokkos::create_mirror_view( v );
+    std::copy( src, src + h.size(), h.data() );
+    Kokkos::deep_copy( v, h );
+}
+
+template < typename View >
+std::vector< typename View::non_const_value_type > view_to_host( const View& v )
+{
+    auto h = Kokkos::create_mirror_view( v );
+    Kokkos::deep_copy( h, v );
+    return std::vector< typename View::non_const_value_type >( h.data(), h.data() + h.size() );
+}
+
+BoundaryConditionFlag bc_of( int c )
+{
+    return c == 1 ? BoundaryConditionFlag::DIRICHLET : ( c == 2 ? BoundaryConditionFlag::FREESLIP :
+                                                                  BoundaryConditionFlag::NEUMANN );
+}
+
+struct Setup
+{
+    DistributedDomain                                        domain;
+    grid::Grid4DDataScalar< grid::NodeOwnershipFlag >        omask;
+    grid::Grid4DDataScalar< grid::shell::ShellBoundaryFlag > bmask;
+    grid::Grid3DDataVec< double, 3 >                         coords;
+    grid::Grid2DDataScalar< double >                         radii;
+    size_t                                                   nodes;
+
+    Setup( int L, double rmin, double rmax )
+    {
+        domain = DistributedDomain::create_uniform_single_subdomain_per_diamond( L, L, rmin, rmax );
+        omask  = grid::setup_node_ownership_mask_data( domain );
+        bmask  = grid::shell::setup_boundary_mask_data( domain );
+        coords = grid::shell::subdomain_unit_sphere_single_shell_coords< double >( domain );
+        radii  = grid::shell::subdomain_shell_radii< double >( domain );
+        nodes  = omask.size();
+    }
+};
+
+void load_vec( linalg::VectorQ1Vec< double >& v, const std::string& path, size_t n )
+{
+    auto h = read_file< double >( path, 3 * n );
+    for ( int d = 0; d < 3; ++d )
+        view_from_host( v.grid_data().comp_[d], h.data() + d * n );
+}
+
+void save_vec( const linalg::VectorQ1Vec< double >& v, const std::string& path, size_t n )
+{
+    std::vector< double > out( 3 * n );
+    for ( int d = 0; d < 3; ++d )
+    {
+        auto c = view_to_host( v.grid_data().comp_[d] );
+        std::copy( c.begin(), c.end(), out.begin() + d * n );
+    }
+    write_file( path, out.data(), out.size() );
+}
+
+int cmd_mesh( int L, double rmin, double rmax, const std::string& out )
+{
+    Setup s( L, rmin, rmax );
+    auto  c  = view_to_host( s.coords );
+    auto  r  = view_to_host( s.radii );
+    auto  bm = view_to_host( s.bmask );
+    auto  om = view_to_host( s.omask );
+    write_file( out + "/coords.bin", c.data(), c.size() );
+    write_file( out + "/radii.bin", r.data(), r.size() );
+    write_file( out + "/bmask.bin", reinterpret_cast< const uint8_t* >( bm.data() ), bm.size() );
+    write_file( out + "/omask.bin", reinterpret_cast< const uint8_t* >( om.data() ), om.size() );
+    return 0;
+}
+
+using Kerngen = fe::wedge::operators::shell::EpsilonDivDivKerngen< double >;
+
+Kerngen make_kerngen( Setup& s, linalg::VectorQ1Scalar< double >& k, int bcc, int bcs, bool diag )
+{
+    BoundaryConditions bcs_ = { { ShellBoundaryFlag::CMB, bc_of( bcc ) }, { ShellBoundaryFlag::SURFACE, bc_of( bcs ) } };
+    return Kerngen( s.domain, s.coords, s.radii, s.bmask, k.grid_data(), bcs_, diag );
+}
+
+int cmd_kerngen( int L, double rmin, double rmax, int bcc, int bcs, int diag, const std::string& dir )
+{
+    Setup                            s( L, rmin, rmax );
+    linalg::VectorQ1Scalar< double > k( "k", s.domain, s.omask );
+    view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", s.nodes ).data() );
+    linalg::VectorQ1Vec< double > src( "src", s.domain, s.omask ), dst( "dst", s.domain, s.omask );
+    load_vec( src, dir + "/src.bin", s.nodes );
+    auto op = make_kerngen( s, k, bcc, bcs, diag != 0 );
+    linalg::apply( op, src, dst );
+    save_vec( dst, dir + "/dst.bin", s.nodes );
+    return 0;
+}
+
+int cmd_time_kerngen( int L, double rmin, double rmax, int bcc, int bcs, int reps )
+{
+    Setup                            s( L, rmin, rmax );
+    linalg::VectorQ1Scalar< double > k( "k", s.domain, s.omask );
+    linalg::VectorQ1Vec< double >    src( "src", s.domain, s.omask ), dst( "dst", s.domain, s.omask );
+    linalg::assign( k, 1.0 );
+    linalg::assign( src, 1.0 );
+    auto op = make_kerngen( s, k, bcc, bcs, false );
+    linalg::apply( op, src, dst ); // warm-up, as measure_run_time does
+    Kokkos::fence();
+    auto t0 = std::chrono::steady_clock::now();
+    for ( int i = 0; i < reps; ++i )
+        linalg::apply( op, src, dst );
+    Kokkos::fence();
+    auto   t1 = std::chrono::steady_clock::now();
+    double dt = std::chrono::duration< double >( t1 - t0 ).count() / reps;
+    std::printf( "{\"seconds_per_apply\": %.9g, \"threads\": %d, \"stored_nodes\": %zu}\n",
+                 dt,
+                 Kokkos::DefaultExecutionSpace().concurrency(),
+                 s.nodes );
+    return 0;
+}
+
+int cmd_laplace( int L, double rmin, double rmax, int treat, int diag, const std::string& dir )
+{
+    Setup                            s( L, rmin, rmax );
+    linalg::VectorQ1Scalar< double > src( "src", s.domain, s.omask ), dst( "dst", s.domain, s.omask );
+    view_from_host( src.grid_data(), read_file< double >( dir + "/src.bin", s.nodes ).data() );
+    fe::wedge::operators::shell::Laplace< double > op( s.domain, s.coords, s.radii, s.bmask, treat != 0, diag != 0 );
+    linalg::apply( op, src, dst );
+    auto out = view_to_host( dst.grid_data() );
+    write_file( dir + "/dst.bin", out.data(), out.size() );
+    return 0;
+}
+
+} // namespace
+
+int main( int argc, char** argv )
+{
+    util::terra_initialize( &argc, &argv );
+    if ( argc < 2 )
+    {
+        std::fprintf( stderr, "usage: ref_dump <command> ...\n" );
+        return 2;
+    }
+    const std::string cmd = argv[1];
+    auto              I   = [&]( int i ) { return std::atoi( argv[i] ); };
+    auto              D   = [&]( int i ) { return std::atof( argv[i] ); };
+    if ( cmd == "mesh" && argc == 6 )
+        return cmd_mesh( I( 2 ), D( 3 ), D( 4 ), argv[5] );
+    if ( cmd == "kerngen" && argc == 9 )
+        return cmd_kerngen( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
+    if ( cmd == "time_kerngen" && argc == 8 )
+        return cmd_time_kerngen( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ) );
+    if ( cmd == "laplace" && argc == 8 )
+        return cmd_laplace( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
+    std::fprintf( stderr, "ref_dump: bad command line\n" );
+    return 2;
+}

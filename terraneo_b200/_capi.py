@@ -1,0 +1,90 @@
+"""ctypes binding of libterraneo_b200.so, the C ABI declared in include/terraneo_b200.h.
+
+The library is the product: every operator, vector kernel and solver call below
+runs CUDA code from it.  There is no CPU fallback; importing this module without
+the built library raises.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libterraneo_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "terraneo_b200.h")
+
+TN_OK = 0
+BC_NEUMANN, BC_DIRICHLET, BC_FREESLIP = 0, 1, 2
+APPLY_REPLACE, APPLY_ADD = 0, 1
+COMM_SKIP, COMM_ADDITIVE = 0, 1
+
+c_int, c_double, c_size_t, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_size_t, ctypes.c_void_p
+P = ctypes.POINTER
+
+
+class EpsDivDivParams(ctypes.Structure):
+    _fields_ = [("bc_cmb", c_int), ("bc_surface", c_int), ("diagonal", c_int), ("apply_mode", c_int),
+                ("comm_mode", c_int), ("penalty_eps", c_double)]
+
+
+class TNError(RuntimeError):
+    pass
+
+
+_lib = None
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "tn_last_error": (ctypes.c_char_p, []),
+    "tn_mesh_create": (c_int, [c_int, c_double, c_double, P(c_void_p)]),
+    "tn_mesh_destroy": (c_int, [c_void_p]),
+    "tn_mesh_dims": (c_int, [c_void_p, P(c_int), P(c_size_t), P(c_size_t)]),
+    "tn_mesh_geometry": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "tn_mesh_masks": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "tn_halo_sum_f64": (c_int, [c_void_p, P(c_void_p), c_int, c_void_p]),
+    "tn_halo_sum_f32": (c_int, [c_void_p, P(c_void_p), c_int, c_void_p]),
+    "tn_epsdivdiv_apply_f64": (c_int, [c_void_p, P(EpsDivDivParams), c_void_p, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_epsdivdiv_apply_f32": (c_int, [c_void_p, P(EpsDivDivParams), c_void_p, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_laplace_apply_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "tn_laplace_apply_f32": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "tn_vec_lincomb_f64": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p), c_void_p]),
+    "tn_vec_lincomb_f32": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p), c_void_p]),
+    "tn_vec_dot_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_double), c_void_p]),
+    "tn_vec_dot_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_double), c_void_p]),
+    "tn_vec_invert_f64": (c_int, [c_void_p, c_int, P(c_void_p), c_void_p]),
+    "tn_vec_invert_f32": (c_int, [c_void_p, c_int, P(c_void_p), c_void_p]),
+    "tn_vec_mult_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_vec_mult_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_vec_max_abs_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_double), c_void_p]),
+    "tn_vec_has_nan_or_inf_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), c_void_p]),
+    "tn_vec_has_nan_or_inf_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), c_void_p]),
+    "tn_vec_cast_f64_to_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_vec_cast_f32_to_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+}
+
+
+def lib():
+    """Load the CUDA library (raises when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"terraneo_b200: {LIB_PATH} is missing; build it with "
+                              "`make -C terraneo_b200/csrc` or __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def check(rc, what=""):
+    if rc != TN_OK:
+        msg = lib().tn_last_error().decode()
+        raise TNError(f"{what}: status {rc}: {msg}")
+
+
+def ptrs(*addrs):
+    """A C array of device pointers (void*[n])."""
+    arr = (c_void_p * max(3, len(addrs)))()
+    for i, a in enumerate(addrs):
+        arr[i] = a
+    return arr

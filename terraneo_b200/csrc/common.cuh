@@ -1,0 +1,99 @@
+// Shared definitions of the terraneo_b200 CUDA library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/terraneo_b200.h"
+
+namespace tn {
+
+constexpr int kDiamonds = 10;
+
+// Per-thread error text returned by tn_last_error().
+void set_error( const std::string& msg );
+
+#define TN_CUDA_TRY( expr )                                                                              \
+    do                                                                                                   \
+    {                                                                                                    \
+        cudaError_t err_ = ( expr );                                                                     \
+        if ( err_ != cudaSuccess )                                                                       \
+        {                                                                                                \
+            ::tn::set_error( std::string( #expr ) + ": " + cudaGetErrorString( err_ ) );                 \
+            return TN_ERR_CUDA;                                                                          \
+        }                                                                                                \
+    } while ( 0 )
+
+#define TN_CHECK_ARG( cond, msg )                                                                        \
+    do                                                                                                   \
+    {                                                                                                    \
+        if ( !( cond ) )                                                                                 \
+        {                                                                                                \
+            ::tn::set_error( msg );                                                                      \
+            return TN_ERR_ARG;                                                                           \
+        }                                                                                                \
+    } while ( 0 )
+
+// Launch-error check after a kernel launch.
+#define TN_LAUNCH_CHECK() TN_CUDA_TRY( cudaGetLastError() )
+
+inline cudaStream_t as_stream( void* s ) { return reinterpret_cast< cudaStream_t >( s ); }
+
+template < typename T >
+struct Ptr3
+{
+    T* p[3];
+};
+
+// Device-side view of the mesh handed to kernels by value.
+template < typename T >
+struct MeshView
+{
+    int      N;      // cells per side
+    int      n1;     // nodes per side (N + 1)
+    size_t   ns;     // stored nodes 10 (N+1)^3
+    const T* coords; // [10][n1][n1][3] lateral unit-sphere points
+    const T* radii;  // [10][n1]
+};
+
+}  // namespace tn
+
+// The mesh object behind the opaque tn_mesh handle.
+struct tn_mesh
+{
+    int    level = 0, N = 0, n1 = 0;
+    double r_min = 0, r_max = 0;
+    size_t ns = 0, nu = 0, nlat = 0;
+
+    std::vector< double > h_coords;    // [10][n1][n1][3]
+    std::vector< double > h_radii;     // [10][n1]
+    std::vector< uint8_t > h_lat_owned; // [10][n1][n1]
+
+    double*  d_coords   = nullptr;
+    double*  d_radii    = nullptr;
+    float*   d_coords32 = nullptr;
+    float*   d_radii32  = nullptr;
+    uint8_t* d_lat_owned = nullptr; // lateral ownership (same for every r)
+
+    // duplicated lateral positions, CSR: members of group g are
+    // halo_members[halo_offsets[g] .. halo_offsets[g+1]) as lateral indices
+    int  n_halo_groups    = 0;
+    int* d_halo_offsets   = nullptr;
+    int* d_halo_members   = nullptr;
+
+    // fs/fs penalty: the orthonormalised modes are m = C (e_j x x); G = C^T C
+    double penalty_gram_inv[9] = { 0 };
+
+    // device scratch: reduction partials + counters
+    double*       d_red_partials = nullptr; // kRedMaxBlocks * 8 doubles
+    double*       d_red_result   = nullptr; // 16 doubles
+    unsigned int* d_red_counter  = nullptr;
+    double*       h_red_result   = nullptr; // pinned, 16 doubles
+};
+
+namespace tn {
+constexpr int kRedMaxBlocks = 1184; // 148 SMs x 8
+}

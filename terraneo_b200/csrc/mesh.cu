@@ -1,0 +1,331 @@
+// Shell mesh: geometry generation (host), masks, duplicated-node map and the
+// additive halo kernel.
+//
+// Geometry follows grid/shell/spherical_shell.hpp: the 10 icosahedral diamonds
+// (:420-559) are refined by recursive chord bisection, every new lateral point
+// being normalize(p1 + p2) of its two parents (compute_node_recursive,
+// :231-346); radii are uniform in [r_min, r_max] with the last one set exactly
+// (uniform_shell_radii, :28).  Here the recursion is unrolled level by level,
+// which computes each point once from the same parents and hence the same bits.
+#include <math.h>
+
+#include <algorithm>
+#include <array>
+#include <cstring>
+#include <map>
+#include <mutex>
+
+#include "common.cuh"
+
+namespace tn {
+
+static thread_local std::string g_last_error = "no error";
+void set_error( const std::string& msg ) { g_last_error = msg; }
+
+namespace {
+
+struct V3
+{
+    double x, y, z;
+};
+
+V3 unit( V3 v )
+{
+    const double s = v.x * v.x + v.y * v.y + v.z * v.z;
+    const double m = sqrt( s );
+    if ( m > 1e-15 )
+        v = { v.x / m, v.y / m, v.z / m };
+    return v;
+}
+
+// The twelve icosahedron vertices: poles plus two staggered rings of five.
+std::array< V3, 12 > icosahedron()
+{
+    std::array< V3, 12 > v{};
+    const double         pi5 = 0.4 * asin( 1.0 );
+    const double         w   = 2.0 * acos( 1.0 / ( 2.0 * sin( pi5 ) ) );
+    const double         cw = cos( w ), sw = sin( w );
+    v[0]  = { 0.0, 0.0, 1.0 };
+    v[11] = { 0.0, 0.0, -1.0 };
+    for ( int k = 1; k <= 5; ++k )
+    {
+        const double up = 2.0 * ( double( k ) - 0.5 ) * pi5;
+        const double lo = 2.0 * ( double( k ) - 1 ) * pi5;
+        v[k]            = { sw * cos( up ), sw * sin( up ), cw };
+        v[k + 5]        = { sw * cos( lo ), sw * sin( lo ), -cw };
+    }
+    return v;
+}
+
+// Corner vertex ids of each diamond: pole, then counter-clockwise.
+constexpr int kDiamondVerts[10][4] = { { 0, 5, 6, 1 },   { 0, 1, 7, 2 },  { 0, 2, 8, 3 },  { 0, 3, 9, 4 },
+                                       { 0, 4, 10, 5 },  { 11, 7, 1, 6 }, { 11, 8, 2, 7 }, { 11, 9, 3, 8 },
+                                       { 11, 10, 4, 9 }, { 11, 6, 5, 10 } };
+
+void diamond_lateral_points( int diamond, int N, double* out /* [n1][n1][3] */ )
+{
+    const auto ico = icosahedron();
+    const int  n1  = N + 1;
+    auto       at  = [&]( int i, int j ) -> double* { return out + ( size_t( i ) * n1 + j ) * 3; };
+    auto       put = [&]( int i, int j, V3 v ) {
+        double* p = at( i, j );
+        p[0] = v.x, p[1] = v.y, p[2] = v.z;
+    };
+    // northern diamonds run "left" = ring vertex 1, southern ones mirror it
+    const int left = diamond < 5 ? 1 : 3, right = diamond < 5 ? 3 : 1;
+    put( 0, 0, ico[kDiamondVerts[diamond][0]] );
+    put( N, 0, ico[kDiamondVerts[diamond][left]] );
+    put( N, N, ico[kDiamondVerts[diamond][2]] );
+    put( 0, N, ico[kDiamondVerts[diamond][right]] );
+    for ( int stride = N; stride >= 2; stride /= 2 )
+    {
+        const int h = stride / 2;
+        for ( int i = 0; i <= N; i += h )
+            for ( int j = 0; j <= N; j += h )
+            {
+                const int   ri = i % stride, rj = j % stride;
+                const double *a = nullptr, *b = nullptr;
+                if ( ri == 0 && rj == h ) // along a row
+                    a = at( i, j - h ), b = at( i, j + h );
+                else if ( ri == h && rj == 0 ) // along a column
+                    a = at( i - h, j ), b = at( i + h, j );
+                else if ( ri == h && rj == h ) // on the anti-diagonal
+                    a = at( i - h, j + h ), b = at( i + h, j - h );
+                else
+                    continue;
+                put( i, j, unit( { a[0] + b[0], a[1] + b[1], a[2] + b[2] } ) );
+            }
+    }
+}
+
+template < typename T >
+int upload( const T* h, size_t n, T** d )
+{
+    TN_CUDA_TRY( cudaMalloc( d, n * sizeof( T ) ) );
+    TN_CUDA_TRY( cudaMemcpy( *d, h, n * sizeof( T ), cudaMemcpyHostToDevice ) );
+    return TN_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Halo kernel: one thread per (duplicate group, r, field); the copies are
+// summed in ascending diamond order and the sum written to every copy.
+// Coalesced along r (consecutive threads = consecutive r).
+template < typename T >
+__global__ void halo_sum_kernel( int n_groups, int n1, const int* __restrict__ offsets, const int* __restrict__ members,
+                                 Ptr3< T > fields, int nfields )
+{
+    const long long tid   = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    const long long total = (long long) n_groups * n1 * nfields;
+    if ( tid >= total )
+        return;
+    const int r = int( tid % n1 );
+    const int g = int( ( tid / n1 ) % n_groups );
+    const int f = int( tid / ( (long long) n1 * n_groups ) );
+    T*        v = fields.p[f];
+    const int b = offsets[g], e = offsets[g + 1];
+    T         s = 0;
+    for ( int m = b; m < e; ++m )
+        s += v[(size_t) members[m] * n1 + r];
+    for ( int m = b; m < e; ++m )
+        v[(size_t) members[m] * n1 + r] = s;
+}
+
+template < typename T >
+int halo_sum( const tn_mesh* m, T* const* fields, int nfields, cudaStream_t st )
+{
+    TN_CHECK_ARG( m && fields && nfields >= 1 && nfields <= 3, "halo_sum: bad arguments" );
+    Ptr3< T > f{};
+    for ( int i = 0; i < nfields; ++i )
+    {
+        TN_CHECK_ARG( fields[i], "halo_sum: null field" );
+        f.p[i] = fields[i];
+    }
+    const long long total = (long long) m->n_halo_groups * m->n1 * nfields;
+    if ( total == 0 )
+        return TN_OK;
+    const int threads = 256;
+    halo_sum_kernel< T ><<< unsigned( ( total + threads - 1 ) / threads ), threads, 0, st >>>(
+        m->n_halo_groups, m->n1, m->d_halo_offsets, m->d_halo_members, f, nfields );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+template int halo_sum< double >( const tn_mesh*, double* const*, int, cudaStream_t );
+template int halo_sum< float >( const tn_mesh*, float* const*, int, cudaStream_t );
+
+}  // namespace tn
+
+using namespace tn;
+
+extern "C" const char* tn_last_error( void ) { return tn::g_last_error.c_str(); }
+
+extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** out )
+{
+    TN_CHECK_ARG( out, "tn_mesh_create: out is NULL" );
+    *out = nullptr;
+    TN_CHECK_ARG( level >= 1 && level <= 9, "tn_mesh_create: level must be in [1, 9]" );
+    TN_CHECK_ARG( r_min < r_max, "tn_mesh_create: r_min must be strictly less than r_max" );
+    tn_mesh* m = new tn_mesh();
+    m->level = level, m->N = 1 << level, m->n1 = m->N + 1;
+    m->r_min = r_min, m->r_max = r_max;
+    const int n1 = m->n1, N = m->N;
+    m->nlat = size_t( kDiamonds ) * n1 * n1;
+    m->ns   = m->nlat * n1;
+    m->nu   = ( size_t( 10 ) * N * N + 2 ) * n1;
+
+    m->h_coords.resize( m->nlat * 3 );
+    for ( int d = 0; d < kDiamonds; ++d )
+        diamond_lateral_points( d, N, m->h_coords.data() + size_t( d ) * n1 * n1 * 3 );
+    m->h_radii.resize( size_t( kDiamonds ) * n1 );
+    const double step = ( r_max - r_min ) / N;
+    for ( int d = 0; d < kDiamonds; ++d )
+    {
+        for ( int i = 0; i <= N; ++i )
+            m->h_radii[d * n1 + i] = r_min + i * step;
+        m->h_radii[d * n1 + N] = r_max;
+    }
+
+    // Duplicates: identical lateral points in different diamonds (the bisection
+    // reproduces shared edges bit for bit).  Owner = lowest diamond id.
+    std::map< std::array< uint64_t, 3 >, std::vector< int > > by_point;
+    for ( size_t l = 0; l < m->nlat; ++l )
+    {
+        std::array< uint64_t, 3 > key;
+        std::memcpy( key.data(), &m->h_coords[l * 3], 24 );
+        by_point[key].push_back( int( l ) );
+    }
+    m->h_lat_owned.assign( m->nlat, 0 );
+    std::vector< int > offsets{ 0 }, members;
+    for ( auto& kv : by_point )
+    {
+        auto& v = kv.second; // lateral indices, ascending = ascending diamond id
+        m->h_lat_owned[v[0]] = 1;
+        if ( v.size() > 1 )
+        {
+            members.insert( members.end(), v.begin(), v.end() );
+            offsets.push_back( int( members.size() ) );
+        }
+    }
+    m->n_halo_groups = int( offsets.size() ) - 1;
+
+    // Gram matrix of the rigid rotations e_j x x over owned nodes, inverted:
+    // the orthonormalised penalty modes m = C (e_j x x) satisfy C^T C = Gram^{-1}.
+    double Gm[3][3] = { { 0 } };
+    for ( size_t l = 0; l < m->nlat; ++l )
+    {
+        if ( !m->h_lat_owned[l] )
+            continue;
+        const int d = int( l / ( size_t( n1 ) * n1 ) );
+        for ( int r = 0; r < n1; ++r )
+        {
+            const double rr = m->h_radii[d * n1 + r];
+            const double x[3] = { m->h_coords[l * 3] * rr, m->h_coords[l * 3 + 1] * rr, m->h_coords[l * 3 + 2] * rr };
+            const double x2   = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+            for ( int i = 0; i < 3; ++i )
+                for ( int j = 0; j < 3; ++j )
+                    Gm[i][j] += ( i == j ? x2 : 0.0 ) - x[i] * x[j];
+        }
+    }
+    {
+        const double a = Gm[0][0], b = Gm[0][1], c = Gm[0][2], d = Gm[1][1], e = Gm[1][2], f = Gm[2][2];
+        const double c00 = d * f - e * e, c01 = c * e - b * f, c02 = b * e - c * d;
+        const double c11 = a * f - c * c, c12 = b * c - a * e, c22 = a * d - b * b;
+        const double det = a * c00 + b * c01 + c * c02;
+        const double inv[9] = { c00 / det, c01 / det, c02 / det, c01 / det, c11 / det, c12 / det, c02 / det, c12 / det, c22 / det };
+        std::memcpy( m->penalty_gram_inv, inv, sizeof( inv ) );
+    }
+
+    int rc;
+    std::vector< float > c32( m->h_coords.begin(), m->h_coords.end() ), r32( m->h_radii.begin(), m->h_radii.end() );
+    if ( ( rc = upload( m->h_coords.data(), m->h_coords.size(), &m->d_coords ) ) ||
+         ( rc = upload( m->h_radii.data(), m->h_radii.size(), &m->d_radii ) ) ||
+         ( rc = upload( c32.data(), c32.size(), &m->d_coords32 ) ) ||
+         ( rc = upload( r32.data(), r32.size(), &m->d_radii32 ) ) ||
+         ( rc = upload( m->h_lat_owned.data(), m->h_lat_owned.size(), &m->d_lat_owned ) ) ||
+         ( rc = upload( offsets.data(), offsets.size(), &m->d_halo_offsets ) ) ||
+         ( rc = upload( members.data(), std::max< size_t >( members.size(), 1 ), &m->d_halo_members ) ) )
+    {
+        tn_mesh_destroy( m );
+        return rc;
+    }
+    if ( cudaMalloc( &m->d_red_partials, sizeof( double ) * kRedMaxBlocks * 8 ) != cudaSuccess ||
+         cudaMalloc( &m->d_red_result, sizeof( double ) * 16 ) != cudaSuccess ||
+         cudaMalloc( &m->d_red_counter, sizeof( unsigned int ) ) != cudaSuccess ||
+         cudaMallocHost( &m->h_red_result, sizeof( double ) * 16 ) != cudaSuccess ||
+         cudaMemset( m->d_red_counter, 0, sizeof( unsigned int ) ) != cudaSuccess )
+    {
+        set_error( "tn_mesh_create: device scratch allocation failed" );
+        tn_mesh_destroy( m );
+        return TN_ERR_NOMEM;
+    }
+    *out = m;
+    return TN_OK;
+}
+
+extern "C" int tn_mesh_destroy( tn_mesh* m )
+{
+    if ( !m )
+        return TN_OK;
+    cudaFree( m->d_coords );
+    cudaFree( m->d_radii );
+    cudaFree( m->d_coords32 );
+    cudaFree( m->d_radii32 );
+    cudaFree( m->d_lat_owned );
+    cudaFree( m->d_halo_offsets );
+    cudaFree( m->d_halo_members );
+    cudaFree( m->d_red_partials );
+    cudaFree( m->d_red_result );
+    cudaFree( m->d_red_counter );
+    if ( m->h_red_result )
+        cudaFreeHost( m->h_red_result );
+    delete m;
+    return TN_OK;
+}
+
+extern "C" int tn_mesh_dims( const tn_mesh* m, int* level, size_t* stored, size_t* unique )
+{
+    TN_CHECK_ARG( m, "tn_mesh_dims: mesh is NULL" );
+    if ( level )
+        *level = m->level;
+    if ( stored )
+        *stored = m->ns;
+    if ( unique )
+        *unique = m->nu;
+    return TN_OK;
+}
+
+extern "C" int tn_mesh_geometry( const tn_mesh* m, double* coords, double* radii )
+{
+    TN_CHECK_ARG( m, "tn_mesh_geometry: mesh is NULL" );
+    if ( coords )
+        std::memcpy( coords, m->h_coords.data(), m->h_coords.size() * sizeof( double ) );
+    if ( radii )
+        std::memcpy( radii, m->h_radii.data(), m->h_radii.size() * sizeof( double ) );
+    return TN_OK;
+}
+
+extern "C" int tn_mesh_masks( const tn_mesh* m, uint8_t* bmask, uint8_t* omask )
+{
+    TN_CHECK_ARG( m, "tn_mesh_masks: mesh is NULL" );
+    const int n1 = m->n1;
+    for ( size_t l = 0; l < m->nlat; ++l )
+        for ( int r = 0; r < n1; ++r )
+        {
+            if ( bmask )
+                bmask[l * n1 + r] = r == 0 ? 6 : ( r == n1 - 1 ? 10 : 1 );
+            if ( omask )
+                omask[l * n1 + r] = m->h_lat_owned[l];
+        }
+    return TN_OK;
+}
+
+extern "C" int tn_halo_sum_f64( const tn_mesh* m, double* const* f, int n, void* s )
+{
+    return halo_sum< double >( m, f, n, as_stream( s ) );
+}
+extern "C" int tn_halo_sum_f32( const tn_mesh* m, float* const* f, int n, void* s )
+{
+    return halo_sum< float >( m, f, n, as_stream( s ) );
+}

@@ -1,0 +1,326 @@
+// Krylov vector kernels (restating kernels/common/grid_operations.hpp).
+//
+// Elementwise kernels run over all components of a vector in one launch (the
+// reference launches one kernel per component and fences after each).  The
+// dot product accumulates in FP64 with Neumaier compensation, reduces with
+// warp shuffles inside a block and finishes deterministically in the last
+// block (fixed order over block partials), so results do not depend on timing.
+#include "common.cuh"
+#include "reduce.cuh"
+
+namespace tn {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+unsigned grid_for( size_t n, int per_thread = 4 )
+{
+    size_t b = ( n + size_t( kThreads ) * per_thread - 1 ) / ( size_t( kThreads ) * per_thread );
+    if ( b < 1 )
+        b = 1;
+    if ( b > 148 * 32 )
+        b = 148 * 32;
+    return unsigned( b );
+}
+
+template < typename T >
+__global__ void lincomb_kernel( size_t ns, int ncomp, Ptr3< T > y, T c0, int nx, T c1, Ptr3< const T > x1, T c2,
+                                Ptr3< const T > x2, T c3, Ptr3< const T > x3 )
+{
+    const size_t total = ns * ncomp;
+    for ( size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; t < total; t += size_t( gridDim.x ) * blockDim.x )
+    {
+        const int    c = int( t / ns );
+        const size_t i = t - size_t( c ) * ns;
+        T            v = c0;
+        if ( nx >= 1 )
+            v = v + c1 * x1.p[c][i];
+        if ( nx >= 2 )
+            v = v + c2 * x2.p[c][i];
+        if ( nx >= 3 )
+            v = v + c3 * x3.p[c][i];
+        y.p[c][i] = v;
+    }
+}
+
+template < typename T, int OP >
+__global__ void elementwise_kernel( size_t ns, int ncomp, Ptr3< T > y, Ptr3< const T > x )
+{
+    const size_t total = ns * ncomp;
+    for ( size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; t < total; t += size_t( gridDim.x ) * blockDim.x )
+    {
+        const int    c = int( t / ns );
+        const size_t i = t - size_t( c ) * ns;
+        if ( OP == 0 )
+            y.p[c][i] = T( 1 ) / y.p[c][i]; // invert_inplace (grid_operations.hpp:253)
+        else
+            y.p[c][i] = y.p[c][i] * x.p[c][i]; // mult_elementwise_inplace (:273)
+    }
+}
+
+template < typename TO, typename TI >
+__global__ void cast_kernel( size_t ns, int ncomp, Ptr3< TO > y, Ptr3< const TI > x )
+{
+    const size_t total = ns * ncomp;
+    for ( size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; t < total; t += size_t( gridDim.x ) * blockDim.x )
+    {
+        const int    c = int( t / ns );
+        const size_t i = t - size_t( c ) * ns;
+        y.p[c][i]      = TO( x.p[c][i] );
+    }
+}
+
+// Owned-node dot product: one lateral ownership flag per (diamond, x, y).
+template < typename T >
+__global__ void dot_kernel( size_t ns, int n1, int ncomp, Ptr3< const T > a, Ptr3< const T > b,
+                            const uint8_t* __restrict__ lat_owned, double* partials, unsigned int* counter,
+                            double* result )
+{
+    Neumaier acc;
+    const size_t total = ns * ncomp;
+    for ( size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; t < total; t += size_t( gridDim.x ) * blockDim.x )
+    {
+        const int    c = int( t / ns );
+        const size_t i = t - size_t( c ) * ns;
+        if ( lat_owned[i / n1] )
+            acc.add( double( a.p[c][i] ) * double( b.p[c][i] ) );
+    }
+    block_sum_finish< 1 >( &acc, partials, counter, result );
+}
+
+template < typename T >
+__global__ void max_abs_kernel( size_t ns, int ncomp, Ptr3< const T > x, double* partials, unsigned int* counter,
+                                double* result )
+{
+    double m = 0.0;
+    const size_t total = ns * ncomp;
+    for ( size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; t < total; t += size_t( gridDim.x ) * blockDim.x )
+    {
+        const int    c = int( t / ns );
+        const size_t i = t - size_t( c ) * ns;
+        const double v = fabs( double( x.p[c][i] ) );
+        // NaN propagates as in Kokkos::max reductions only through comparisons;
+        // keep the reference's max-of-abs semantics for finite input.
+        m = v > m ? v : m;
+    }
+    block_max_finish( m, partials, counter, result );
+}
+
+template < typename T >
+__global__ void nan_kernel( size_t ns, int ncomp, Ptr3< const T > x, double* partials, unsigned int* counter,
+                            double* result )
+{
+    double flag = 0.0;
+    const size_t total = ns * ncomp;
+    for ( size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; t < total; t += size_t( gridDim.x ) * blockDim.x )
+    {
+        const int    c = int( t / ns );
+        const size_t i = t - size_t( c ) * ns;
+        if ( !isfinite( double( x.p[c][i] ) ) )
+            flag = 1.0;
+    }
+    block_max_finish( flag, partials, counter, result );
+}
+
+template < typename T >
+int ptr3( int ncomp, T* const* in, Ptr3< T >& out, const char* what )
+{
+    TN_CHECK_ARG( ncomp >= 1 && ncomp <= 3, std::string( what ) + ": ncomp must be 1..3" );
+    TN_CHECK_ARG( in, std::string( what ) + ": null vector" );
+    out = {};
+    for ( int c = 0; c < ncomp; ++c )
+    {
+        TN_CHECK_ARG( in[c], std::string( what ) + ": null component" );
+        out.p[c] = in[c];
+    }
+    return TN_OK;
+}
+
+template < typename T >
+int ptr3c( int ncomp, const T* const* in, Ptr3< const T >& out, const char* what )
+{
+    TN_CHECK_ARG( ncomp >= 1 && ncomp <= 3, std::string( what ) + ": ncomp must be 1..3" );
+    TN_CHECK_ARG( in, std::string( what ) + ": null vector" );
+    out = {};
+    for ( int c = 0; c < ncomp; ++c )
+    {
+        TN_CHECK_ARG( in[c], std::string( what ) + ": null component" );
+        out.p[c] = in[c];
+    }
+    return TN_OK;
+}
+
+int fetch_result( const tn_mesh* m, int n, cudaStream_t st, double* out )
+{
+    TN_CUDA_TRY( cudaMemcpyAsync( m->h_red_result, m->d_red_result, sizeof( double ) * n, cudaMemcpyDeviceToHost, st ) );
+    TN_CUDA_TRY( cudaStreamSynchronize( st ) );
+    for ( int i = 0; i < n; ++i )
+        out[i] = m->h_red_result[i];
+    return TN_OK;
+}
+
+}  // namespace
+
+template < typename T >
+int vec_lincomb( const tn_mesh* m, int ncomp, T* const* y, double c0, int nx, const double* c, const T* const* x,
+                 cudaStream_t st )
+{
+    TN_CHECK_ARG( m, "lincomb: mesh is NULL" );
+    TN_CHECK_ARG( nx >= 0 && nx <= 3, "lincomb: only 0 to 3 input vectors are supported" );
+    TN_CHECK_ARG( nx == 0 || ( c && x ), "lincomb: coefficients/vectors missing" );
+    Ptr3< T >       py;
+    Ptr3< const T > px[3] = {};
+    int             rc;
+    if ( ( rc = ptr3( ncomp, y, py, "lincomb" ) ) )
+        return rc;
+    for ( int i = 0; i < nx; ++i )
+        if ( ( rc = ptr3c( ncomp, reinterpret_cast< const T* const* >( x + 3 * i ), px[i], "lincomb" ) ) )
+            return rc;
+    const T k1 = nx > 0 ? T( c[0] ) : T( 0 ), k2 = nx > 1 ? T( c[1] ) : T( 0 ), k3 = nx > 2 ? T( c[2] ) : T( 0 );
+    lincomb_kernel< T ><<< grid_for( m->ns * ncomp ), kThreads, 0, st >>>( m->ns, ncomp, py, T( c0 ), nx, k1, px[0], k2,
+                                                                          px[1], k3, px[2] );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+template < typename T >
+int vec_dot( const tn_mesh* m, int ncomp, const T* const* a, const T* const* b, double* result, cudaStream_t st )
+{
+    TN_CHECK_ARG( m && result, "dot: bad arguments" );
+    Ptr3< const T > pa, pb;
+    int             rc;
+    if ( ( rc = ptr3c( ncomp, a, pa, "dot" ) ) || ( rc = ptr3c( ncomp, b, pb, "dot" ) ) )
+        return rc;
+    const unsigned blocks = std::min< unsigned >( grid_for( m->ns * ncomp, 8 ), kRedMaxBlocks );
+    dot_kernel< T ><<< blocks, kThreads, 0, st >>>( m->ns, m->n1, ncomp, pa, pb, m->d_lat_owned, m->d_red_partials,
+                                                   m->d_red_counter, m->d_red_result );
+    TN_LAUNCH_CHECK();
+    return fetch_result( m, 1, st, result );
+}
+
+template < typename T, int OP >
+int vec_elementwise( const tn_mesh* m, int ncomp, T* const* y, const T* const* x, cudaStream_t st )
+{
+    TN_CHECK_ARG( m, "elementwise: mesh is NULL" );
+    Ptr3< T >       py;
+    Ptr3< const T > px{};
+    int             rc;
+    if ( ( rc = ptr3( ncomp, y, py, "elementwise" ) ) )
+        return rc;
+    if ( OP == 1 && ( rc = ptr3c( ncomp, x, px, "elementwise" ) ) )
+        return rc;
+    elementwise_kernel< T, OP ><<< grid_for( m->ns * ncomp ), kThreads, 0, st >>>( m->ns, ncomp, py, px );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+template < typename TO, typename TI >
+int vec_cast( const tn_mesh* m, int ncomp, TO* const* y, const TI* const* x, cudaStream_t st )
+{
+    TN_CHECK_ARG( m, "cast: mesh is NULL" );
+    Ptr3< TO >       py;
+    Ptr3< const TI > px;
+    int              rc;
+    if ( ( rc = ptr3( ncomp, y, py, "cast" ) ) || ( rc = ptr3c( ncomp, x, px, "cast" ) ) )
+        return rc;
+    cast_kernel< TO, TI ><<< grid_for( m->ns * ncomp ), kThreads, 0, st >>>( m->ns, ncomp, py, px );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+template int vec_lincomb< double >( const tn_mesh*, int, double* const*, double, int, const double*,
+                                    const double* const*, cudaStream_t );
+template int vec_lincomb< float >( const tn_mesh*, int, float* const*, double, int, const double*, const float* const*,
+                                   cudaStream_t );
+template int vec_dot< double >( const tn_mesh*, int, const double* const*, const double* const*, double*, cudaStream_t );
+template int vec_dot< float >( const tn_mesh*, int, const float* const*, const float* const*, double*, cudaStream_t );
+
+}  // namespace tn
+
+using namespace tn;
+
+// `x` holds nx vectors of 3 pointer slots each (only ncomp slots are read).
+extern "C" int tn_vec_lincomb_f64( const tn_mesh* m, int ncomp, double* const* y, double c0, int nx, const double* c,
+                                   const double* const* x, void* s )
+{
+    return vec_lincomb< double >( m, ncomp, y, c0, nx, c, x, as_stream( s ) );
+}
+extern "C" int tn_vec_lincomb_f32( const tn_mesh* m, int ncomp, float* const* y, double c0, int nx, const double* c,
+                                   const float* const* x, void* s )
+{
+    return vec_lincomb< float >( m, ncomp, y, c0, nx, c, x, as_stream( s ) );
+}
+extern "C" int tn_vec_dot_f64( const tn_mesh* m, int ncomp, const double* const* a, const double* const* b, double* r,
+                               void* s )
+{
+    return vec_dot< double >( m, ncomp, a, b, r, as_stream( s ) );
+}
+extern "C" int tn_vec_dot_f32( const tn_mesh* m, int ncomp, const float* const* a, const float* const* b, double* r,
+                               void* s )
+{
+    return vec_dot< float >( m, ncomp, a, b, r, as_stream( s ) );
+}
+extern "C" int tn_vec_invert_f64( const tn_mesh* m, int ncomp, double* const* y, void* s )
+{
+    return vec_elementwise< double, 0 >( m, ncomp, y, nullptr, as_stream( s ) );
+}
+extern "C" int tn_vec_invert_f32( const tn_mesh* m, int ncomp, float* const* y, void* s )
+{
+    return vec_elementwise< float, 0 >( m, ncomp, y, nullptr, as_stream( s ) );
+}
+extern "C" int tn_vec_mult_f64( const tn_mesh* m, int ncomp, double* const* y, const double* const* x, void* s )
+{
+    return vec_elementwise< double, 1 >( m, ncomp, y, x, as_stream( s ) );
+}
+extern "C" int tn_vec_mult_f32( const tn_mesh* m, int ncomp, float* const* y, const float* const* x, void* s )
+{
+    return vec_elementwise< float, 1 >( m, ncomp, y, x, as_stream( s ) );
+}
+extern "C" int tn_vec_max_abs_f64( const tn_mesh* m, int ncomp, const double* const* x, double* result, void* s )
+{
+    TN_CHECK_ARG( m && result, "max_abs: bad arguments" );
+    Ptr3< const double > px;
+    int                  rc;
+    if ( ( rc = ptr3c( ncomp, x, px, "max_abs" ) ) )
+        return rc;
+    const unsigned blocks = std::min< unsigned >( grid_for( m->ns * ncomp, 8 ), kRedMaxBlocks );
+    max_abs_kernel< double ><<< blocks, kThreads, 0, as_stream( s ) >>>( m->ns, ncomp, px, m->d_red_partials,
+                                                                        m->d_red_counter, m->d_red_result );
+    TN_LAUNCH_CHECK();
+    return fetch_result( m, 1, as_stream( s ), result );
+}
+template < typename T >
+static int has_nan( const tn_mesh* m, int ncomp, const T* const* x, int* result, void* s )
+{
+    TN_CHECK_ARG( m && result, "has_nan_or_inf: bad arguments" );
+    Ptr3< const T > px;
+    int             rc;
+    if ( ( rc = ptr3c( ncomp, x, px, "has_nan_or_inf" ) ) )
+        return rc;
+    const unsigned blocks = std::min< unsigned >( grid_for( m->ns * ncomp, 8 ), kRedMaxBlocks );
+    nan_kernel< T ><<< blocks, kThreads, 0, as_stream( s ) >>>( m->ns, ncomp, px, m->d_red_partials, m->d_red_counter,
+                                                               m->d_red_result );
+    TN_LAUNCH_CHECK();
+    double f = 0;
+    if ( ( rc = fetch_result( m, 1, as_stream( s ), &f ) ) )
+        return rc;
+    *result = f != 0.0;
+    return TN_OK;
+}
+extern "C" int tn_vec_has_nan_or_inf_f64( const tn_mesh* m, int ncomp, const double* const* x, int* r, void* s )
+{
+    return has_nan< double >( m, ncomp, x, r, s );
+}
+extern "C" int tn_vec_has_nan_or_inf_f32( const tn_mesh* m, int ncomp, const float* const* x, int* r, void* s )
+{
+    return has_nan< float >( m, ncomp, x, r, s );
+}
+extern "C" int tn_vec_cast_f64_to_f32( const tn_mesh* m, int ncomp, float* const* y, const double* const* x, void* s )
+{
+    return vec_cast< float, double >( m, ncomp, y, x, as_stream( s ) );
+}
+extern "C" int tn_vec_cast_f32_to_f64( const tn_mesh* m, int ncomp, double* const* y, const float* const* x, void* s )
+{
+    return vec_cast< double, float >( m, ncomp, y, x, as_stream( s ) );
+}

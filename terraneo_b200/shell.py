@@ -1,0 +1,189 @@
+"""Python mirror of the reference's shell/vector/operator interface over the C ABI.
+
+Names follow the reference (src/terra): a mesh replaces DistributedDomain with
+one subdomain per diamond (grid/shell/spherical_shell.hpp:2520), VectorQ1Scalar /
+VectorQ1Vec hold device fields in the reference layout (linalg/vector_q1.hpp),
+and operator classes expose apply_impl(src, dst) (linalg/operator.hpp:57-71).
+Device memory is allocated through torch (plumbing only); every computation is
+a call into libterraneo_b200.so.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _capi as C
+
+_DT = {torch.float64: "f64", torch.float32: "f32"}
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class ShellMesh:
+    """Thick spherical shell, 10 diamonds x N x N lateral x N radial cells, N = 2**level."""
+
+    def __init__(self, level, r_min=0.55, r_max=1.0):
+        h = ctypes.c_void_p()
+        C.check(C.lib().tn_mesh_create(level, r_min, r_max, ctypes.byref(h)), "tn_mesh_create")
+        self._h = h
+        self.level, self.N, self.n1 = level, 1 << level, (1 << level) + 1
+        ns, nu, lv = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_int()
+        C.check(C.lib().tn_mesh_dims(h, ctypes.byref(lv), ctypes.byref(ns), ctypes.byref(nu)), "tn_mesh_dims")
+        self.stored_nodes, self.unique_nodes = ns.value, nu.value
+        self.shape = (10, self.n1, self.n1, self.n1)
+        self.r_min, self.r_max = r_min, r_max
+
+    @property
+    def handle(self):
+        return self._h
+
+    def geometry(self):
+        coords = np.zeros((10, self.n1, self.n1, 3))
+        radii = np.zeros((10, self.n1))
+        C.check(C.lib().tn_mesh_geometry(self._h, coords.ctypes.data, radii.ctypes.data), "tn_mesh_geometry")
+        return coords, radii
+
+    def masks(self):
+        b = np.zeros(self.shape, np.uint8)
+        o = np.zeros(self.shape, np.uint8)
+        C.check(C.lib().tn_mesh_masks(self._h, b.ctypes.data, o.ctypes.data), "tn_mesh_masks")
+        return b, o
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and C._lib is not None:
+            C.lib().tn_mesh_destroy(h)
+            self._h = None
+
+
+class _VectorBase:
+    ncomp = 1
+
+    def __init__(self, mesh, dtype=torch.float64, data=None):
+        self.mesh = mesh
+        self.dtype = dtype
+        if data is None:
+            data = torch.zeros((self.ncomp,) + mesh.shape, dtype=dtype, device="cuda")
+        self.data = data  # shallow handle semantics: copies share this tensor
+
+    @property
+    def tag(self):
+        return _DT[self.dtype]
+
+    def comp_ptrs(self):
+        return C.ptrs(*[self.data[c].data_ptr() for c in range(self.ncomp)])
+
+    # VectorLike (linalg/vector.hpp:8-37)
+    def lincomb_impl(self, c, xs, c0=0.0):
+        if len(c) != len(xs):
+            raise RuntimeError("lincomb: c and x must have the same size")
+        if len(xs) > 3:
+            raise RuntimeError("lincomb: not implemented")
+        xarr = (ctypes.c_void_p * 9)()
+        for i, x in enumerate(xs):
+            for k in range(self.ncomp):
+                xarr[3 * i + k] = x.data[k].data_ptr()
+        carr = (ctypes.c_double * 3)(*([float(v) for v in c] + [0.0] * (3 - len(c))))
+        f = getattr(C.lib(), f"tn_vec_lincomb_{self.tag}")
+        C.check(f(self.mesh.handle, self.ncomp, self.comp_ptrs(), float(c0), len(xs), carr, xarr, _stream()), "lincomb")
+
+    def dot_impl(self, other):
+        r = ctypes.c_double()
+        f = getattr(C.lib(), f"tn_vec_dot_{self.tag}")
+        C.check(f(self.mesh.handle, self.ncomp, self.comp_ptrs(), other.comp_ptrs(), ctypes.byref(r), _stream()), "dot")
+        return r.value
+
+    def invert_entries_impl(self):
+        C.check(getattr(C.lib(), f"tn_vec_invert_{self.tag}")(self.mesh.handle, self.ncomp, self.comp_ptrs(),
+                                                              _stream()), "invert")
+
+    def scale_with_vector_impl(self, x):
+        C.check(getattr(C.lib(), f"tn_vec_mult_{self.tag}")(self.mesh.handle, self.ncomp, self.comp_ptrs(),
+                                                            x.comp_ptrs(), _stream()), "mult")
+
+    def has_nan_or_inf_impl(self):
+        r = ctypes.c_int()
+        C.check(getattr(C.lib(), f"tn_vec_has_nan_or_inf_{self.tag}")(self.mesh.handle, self.ncomp, self.comp_ptrs(),
+                                                                      ctypes.byref(r), _stream()), "has_nan")
+        return bool(r.value)
+
+    def max_abs_entry_impl(self):
+        if self.dtype != torch.float64:
+            raise NotImplementedError
+        r = ctypes.c_double()
+        C.check(C.lib().tn_vec_max_abs_f64(self.mesh.handle, self.ncomp, self.comp_ptrs(), ctypes.byref(r),
+                                           _stream()), "max_abs")
+        return r.value
+
+    def swap_impl(self, other):
+        self.data, other.data = other.data, self.data
+
+    def halo_sum(self):
+        f = getattr(C.lib(), f"tn_halo_sum_{self.tag}")
+        C.check(f(self.mesh.handle, self.comp_ptrs(), self.ncomp, _stream()), "halo_sum")
+
+    def numpy(self):
+        return self.data.detach().cpu().numpy()
+
+    def set_numpy(self, arr):
+        self.data.copy_(torch.as_tensor(np.asarray(arr).reshape(self.data.shape), dtype=self.dtype))
+
+
+class VectorQ1Scalar(_VectorBase):
+    ncomp = 1
+
+
+class VectorQ1Vec(_VectorBase):
+    ncomp = 3
+
+
+class EpsilonDivDivKerngen:
+    """EpsilonDivDivKerngen (fe/wedge/operators/shell/epsilon_divdiv_kerngen.hpp:62)."""
+
+    def __init__(self, mesh, k, bc_cmb, bc_surface, diagonal=False, apply_mode=C.APPLY_REPLACE,
+                 comm_mode=C.COMM_ADDITIVE, penalty_eps=1.0):
+        self.mesh, self.k = mesh, k
+        self.p = C.EpsDivDivParams(bc_cmb, bc_surface, int(diagonal), apply_mode, comm_mode, penalty_eps)
+
+    def set_diagonal(self, v):
+        self.p.diagonal = int(v)
+
+    def set_operator_apply_and_communication_modes(self, apply_mode, comm_mode):
+        self.p.apply_mode, self.p.comm_mode = apply_mode, comm_mode
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_epsdivdiv_apply_{src.tag}")
+        C.check(f(self.mesh.handle, ctypes.byref(self.p), ctypes.c_void_p(self.k.data.data_ptr()), src.comp_ptrs(),
+                  dst.comp_ptrs(), _stream()), "epsdivdiv_apply")
+
+
+class Laplace:
+    """Laplace (fe/wedge/operators/shell/laplace.hpp:18)."""
+
+    def __init__(self, mesh, treat_boundary, diagonal=False, apply_mode=C.APPLY_REPLACE, comm_mode=C.COMM_ADDITIVE):
+        self.mesh = mesh
+        self.treat, self.diag, self.am, self.cm = int(treat_boundary), int(diagonal), apply_mode, comm_mode
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_laplace_apply_{src.tag}")
+        C.check(f(self.mesh.handle, self.treat, self.diag, self.am, self.cm, ctypes.c_void_p(src.data.data_ptr()),
+                  ctypes.c_void_p(dst.data.data_ptr()), _stream()), "laplace_apply")
+
+
+def apply(op, src, dst):
+    """linalg::apply (linalg/operator.hpp:156)."""
+    op.apply_impl(src, dst)
+
+
+def lincomb(y, c, xs, c0=0.0):
+    y.lincomb_impl(c, xs, c0)
+
+
+def assign(y, c0):
+    y.lincomb_impl([], [], c0)
+
+
+def dot(a, b):
+    return a.dot_impl(b)

@@ -1,0 +1,112 @@
+"""ctypes binding of the C oracle (oracle/liboracle.so) -- test infrastructure.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module; the product never imports it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+REF_DUMP = os.path.join(ORACLE_DIR, "_ref", "ref_dump")
+
+_lib = None
+
+_D = ctypes.POINTER(ctypes.c_double)
+_U8 = ctypes.POINTER(ctypes.c_uint8)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(ORACLE_DIR, "liboracle.so")
+        if not os.path.exists(path):
+            subprocess.check_call(["make", "-s", "-C", ORACLE_DIR])
+        L = ctypes.CDLL(path)
+        L.or_unit_sphere_coords.argtypes = [ctypes.c_int, _D]
+        L.or_shell_radii.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, _D]
+        L.or_boundary_mask.argtypes = [ctypes.c_int, _U8]
+        L.or_ownership_mask.argtypes = [ctypes.c_int, _D, _U8]
+        L.or_halo_sum.argtypes = [ctypes.c_int, _D, _D, ctypes.c_int]
+        L.or_kerngen_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.or_laplace_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
+        L.or_masked_dot.restype = ctypes.c_double
+        L.or_masked_dot.argtypes = [ctypes.c_size_t, _D, _D, _U8]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    assert a.flags.c_contiguous
+    if a.dtype == np.float64:
+        return a.ctypes.data_as(_D)
+    if a.dtype == np.uint8:
+        return a.ctypes.data_as(_U8)
+    raise TypeError(a.dtype)
+
+
+class Mesh:
+    """Oracle mesh of the 10-diamond shell at level L (one subdomain per diamond)."""
+
+    def __init__(self, L, rmin=0.55, rmax=1.0):
+        self.L, self.N, self.n1 = L, 1 << L, (1 << L) + 1
+        n1 = self.n1
+        self.shape = (10, n1, n1, n1)
+        self.ns = 10 * n1 ** 3
+        self.coords = np.zeros((10, n1, n1, 3))
+        lib().or_unit_sphere_coords(L, _p(self.coords))
+        self.radii = np.zeros((10, n1))
+        lib().or_shell_radii(L, rmin, rmax, _p(self.radii))
+        self.bmask = np.zeros(self.shape, np.uint8)
+        lib().or_boundary_mask(L, _p(self.bmask))
+        self.omask = np.zeros(self.shape, np.uint8)
+        lib().or_ownership_mask(L, _p(self.coords), _p(self.omask))
+
+    def halo_sum(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64).copy()
+        ncomp = f.size // self.ns
+        lib().or_halo_sum(self.L, _p(self.coords), _p(f), ncomp)
+        return f
+
+    def make_consistent(self, f):
+        """Copy the owner's value to every duplicate of a node."""
+        f = np.ascontiguousarray(f, dtype=np.float64).copy()
+        ncomp = f.size // self.ns
+        om = np.tile(self.omask.reshape(-1), ncomp).reshape(f.shape)
+        return self.halo_sum(np.where(om == 1, f, 0.0))
+
+    def kerngen(self, k, src, bc_cmb, bc_surf, diag=False):
+        dst = np.zeros((3,) + self.shape)
+        k = np.ascontiguousarray(k, dtype=np.float64)
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        lib().or_kerngen_apply(self.L, _p(self.coords), _p(self.radii), _p(k), _p(src), _p(dst),
+                               bc_cmb, bc_surf, int(diag))
+        return dst
+
+    def laplace(self, src, treat_boundary=True, diag=False):
+        dst = np.zeros(self.shape)
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        lib().or_laplace_apply(self.L, _p(self.coords), _p(self.radii), _p(src), _p(dst),
+                               int(treat_boundary), int(diag))
+        return dst
+
+    def dot(self, a, b):
+        """Owned-masked dot product summed over components."""
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1, self.ns)
+        b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1, self.ns)
+        om = np.ascontiguousarray(self.omask.reshape(-1))
+        return sum(lib().or_masked_dot(self.ns, _p(np.ascontiguousarray(a[i])), _p(np.ascontiguousarray(b[i])), _p(om))
+                   for i in range(a.shape[0]))
+
+
+def ref_available():
+    return os.path.exists(REF_DUMP)
+
+
+def run_ref(args, workdir, threads=4):
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="false")
+    subprocess.run([REF_DUMP] + [str(a) for a in args], cwd=workdir, env=env, check=True,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
