@@ -21,6 +21,8 @@
 //    normal-normal add-back, rotated diagonal), accumulating with atomics.  It
 //    also provides the diagonal mode and levels too small for tiling.
 //  * penalty kernels for free-slip on both boundaries.
+#include <cuda_pipeline.h>
+
 #include <algorithm>
 
 #include "common.cuh"
@@ -34,32 +36,28 @@ int halo_sum( const tn_mesh* m, T* const* fields, int nfields, cudaStream_t st )
 
 namespace {
 
-constexpr int kTile    = 8;  // owned lateral node columns per tile side
-constexpr int kWarps   = 8;
-constexpr int kThreads = kWarps * 32;
-constexpr int kRC      = 32; // radial cells per chunk (one per lane)
-constexpr int kCols    = ( kTile + 1 ) * ( kTile + 1 );
-constexpr int kAccCol  = kRC + 1;
+constexpr int kTS      = 8;       // owned node columns per x tile
+constexpr int kW       = kTS + 1; // warps = cell strips per CTA
+constexpr int kThreads = kW * 32;
+constexpr int kRC      = 32;      // radial cells per chunk (one per lane)
+#ifndef TN_TILE_MINBLOCKS
+#define TN_TILE_MINBLOCKS 2 // resident CTAs per SM the tiled kernel is compiled for
+#endif
+constexpr int kSegMax  = 24;      // longest run of node rows a CTA finalises in one y march
 
 template < typename T >
 struct TileParams
 {
-    int           N, n1, tiles;
+    int           N, n1, xtiles, seg_max; // seg_max: longest run of node rows one segment finalises
     const double* coords;
     const T*      radii;
     const T*      k;
     Ptr3< const T > src;
     Ptr3< T >     dst;
     int           add_mode;
-    int           skip_cmb, skip_surface; // leave that boundary layer of cells to the cell kernel
+    int           skip_cmb, skip_surface; // leave that boundary layer of cells to the boundary kernel
     const double* beta;                   // fs/fs penalty vector (3) or nullptr
 };
-
-template < typename T >
-size_t tile_smem_bytes( int n1 )
-{
-    return sizeof( T ) * ( size_t( ( n1 + 1 ) & ~1 ) + size_t( kCols ) * 20 + size_t( 3 ) * kCols * kAccCol );
-}
 
 // Per-wedge flux vectors S1 = sigma q0, S2 = sigma q1, S3 = kappa sigma q2 with
 // sigma = omega (2 sym(G) - 2/3 tr(G) I), G = q0 (x) v1 + q1 (x) v2 + q2 (x) kappa v3.
@@ -94,212 +92,325 @@ __device__ __forceinline__ void wedge_flux( const T* __restrict__ g, const T v1[
     S3[2] = kappa * ( s02 * q2[0] + s12 * q2[1] + s22 * q2[2] );
 }
 
+// Tiled owner-computes apply.  CTA = kW warps; warp w handles the cell strip
+// X = sx0 + w of one y segment, lanes = 32 consecutive radial cells.  The
+// warp marches along y: at step s it computes cell (X, cy) and finalises node
+// row cy, carrying its contributions to row cy+1 in registers.  A node column
+// X gets its two halves from strips X (left side) and X-1 (right side); right
+// halves are exchanged through shared memory, one barrier per step.  Node rows
+// (the CTA's kW+1 columns x 3 src components + k x 33 levels) are streamed
+// into a 4-slot shared-memory ring with cp.async three rows ahead, so global
+// latency overlaps the arithmetic of the previous steps.  The radial chunk
+// boundary level r0 + 32 is carried to the next chunk in shared memory.
+constexpr int kLev   = kRC + 1; // node levels per chunk
+constexpr int kSlots = 4;       // row ring depth (prefetch distance 3)
+
 template < typename T >
-__global__ void __launch_bounds__( kThreads ) kerngen_tile_kernel( TileParams< T > P )
+size_t tile_smem_bytes( int n1, int SY )
+{
+    const size_t radii = size_t( 10 ) * ( ( n1 + 1 ) & ~1 );
+    const size_t geo   = size_t( kW ) * ( SY + 2 ) * 20;
+    const size_t rows  = size_t( kSlots ) * ( kW + 1 ) * 4 * kLev;
+    const size_t xbuf  = size_t( 2 ) * kW * 3 * kLev;
+    const size_t carry = size_t( kW + 1 ) * ( SY + 2 ) * 3;
+    const size_t top   = size_t( kW ) * 2 * 4 * 3;
+    return sizeof( T ) * ( radii + geo + rows + xbuf + carry + top );
+}
+
+// Stream node row Y (the CTA's kW+1 columns, 3 src components + k, levels
+// r0..r0+RC) into a ring slot: warp w copies the (column, field) pairs
+// w, w+kW, ...; lane l copies level l, lane 0 also level 32.
+template < typename T >
+__device__ __forceinline__ void issue_row( const T* f0, const T* f1, const T* f2, const T* f3, int N, int n1, T* slot,
+                                           int d, int sx0, int Y, int r0, int RC, int lane, int warp )
+{
+    if ( Y < 0 || Y > N )
+        return;
+    for ( int p = warp; p < ( kW + 1 ) * 4; p += kW )
+    {
+        const int col = p >> 2, f = p & 3;
+        const int X   = sx0 + col;
+        if ( X < 0 || X > N )
+            continue;
+        const T* src = ( f == 0 ? f0 : ( f == 1 ? f1 : ( f == 2 ? f2 : f3 ) ) ) +
+                       ( lat_index( n1, d, X, Y ) * n1 + r0 );
+        T* dst = slot + p * kLev;
+        if ( lane <= RC )
+            __pipeline_memcpy_async( dst + lane, src + lane, sizeof( T ) );
+        if ( lane == 0 && RC == kRC )
+            __pipeline_memcpy_async( dst + kRC, src + kRC, sizeof( T ) );
+    }
+}
+
+template < typename T >
+__global__ void __launch_bounds__( kThreads, TN_TILE_MINBLOCKS ) kerngen_tile_kernel( TileParams< T > P )
 {
     extern __shared__ __align__( 16 ) unsigned char smem_raw[];
-    const int N = P.N, n1 = P.n1;
-    int       b  = blockIdx.x;
-    const int tx = b % P.tiles;
-    b /= P.tiles;
-    const int ty = b % P.tiles;
-    const int d  = b / P.tiles;
-
-    // owned node columns [xlo, xhi] x [ylo, yhi]; cells touching them
-    const int xlo = tx == 0 ? 0 : tx * kTile + 1, xhi = tx * kTile + kTile;
-    const int ylo = ty == 0 ? 0 : ty * kTile + 1, yhi = ty * kTile + kTile;
-    const int nyo = yhi - ylo + 1;
-    const int nxo = xhi - xlo + 1;
-    const int cxlo = tx * kTile, cxhi = min( xhi, N - 1 );
-    const int cylo = ty * kTile, cyhi = min( yhi, N - 1 );
-    const int ncx = cxhi - cxlo + 1, ncy = cyhi - cylo + 1;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int          N = P.N, n1 = P.n1, SM = P.seg_max;
+    const T *          f0 = P.src.p[0], *f1 = P.src.p[1], *f2 = P.src.p[2], *f3 = P.k;
+    T *                o0 = P.dst.p[0], *o1 = P.dst.p[1], *o2 = P.dst.p[2];
+    const bool         add_mode = P.add_mode != 0;
+    const double*      beta     = P.beta;
 
     T* s_radii = reinterpret_cast< T* >( smem_raw );
-    T* s_geo   = s_radii + ( ( n1 + 1 ) & ~1 );
-    T* s_acc   = s_geo + kCols * 20;
-    constexpr int kAccComp = kCols * kAccCol;
+    T* s_geo   = s_radii + 10 * ( ( n1 + 1 ) & ~1 );
+    T* s_rows  = s_geo + kW * ( SM + 2 ) * 20;
+    T* s_xbuf  = s_rows + kSlots * ( kW + 1 ) * 4 * kLev;
+    T* s_carry = s_xbuf + 2 * kW * 3 * kLev;
+    T* s_top   = s_carry + ( kW + 1 ) * ( SM + 2 ) * 3; // [w][parity][corner][c]: top contributions of lane RC-1
+    auto slot  = [s_rows]( int y ) { return s_rows + ( ( y + kSlots ) % kSlots ) * ( ( kW + 1 ) * 4 * kLev ); };
 
-    for ( int i = threadIdx.x; i < n1; i += blockDim.x )
-        s_radii[i] = P.radii[d * n1 + i];
-    for ( int i = threadIdx.x; i < ncx * ncy * 2; i += blockDim.x )
+    for ( int i = threadIdx.x; i < 10 * n1; i += blockDim.x )
+        s_radii[( i / n1 ) * ( ( n1 + 1 ) & ~1 ) + i % n1] = P.radii[i];
+
+    const int  lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int  RC   = min( kRC, N );
+
+    // Even split of all (diamond, x tile, node row) items over the grid: this
+    // CTA finalises rows [g_begin, g_end) of the flattened list, in runs
+    // (segments) of at most seg_max consecutive rows of one x tile.
+    const long long rows_per_tile = N + 1;
+    const long long total         = (long long) kDiamonds * P.xtiles * rows_per_tile;
+    const long long g_begin       = total * blockIdx.x / gridDim.x;
+    const long long g_end         = total * ( blockIdx.x + 1 ) / gridDim.x;
+
+    for ( long long g = g_begin; g < g_end; )
     {
-        const int     w = i & 1, col = i >> 1;
-        const int     X = cxlo + col / ncy, Y = cylo + col % ncy;
-        const double* c00 = P.coords + lat_index( n1, d, X, Y ) * 3;
-        const double* c10 = P.coords + lat_index( n1, d, X + 1, Y ) * 3;
-        const double* c01 = P.coords + lat_index( n1, d, X, Y + 1 ) * 3;
-        const double* c11 = P.coords + lat_index( n1, d, X + 1, Y + 1 ) * 3;
-        double        q[9], adet;
-        if ( w == 0 )
-            lateral_geometry( c00, c10, c01, q, &adet );
-        else
-            lateral_geometry( c11, c01, c10, q, &adet );
-        T* g = s_geo + i * 10;
-        for ( int j = 0; j < 9; ++j )
-            g[j] = T( q[j] );
-        g[9] = T( adet );
-    }
-    for ( int i = threadIdx.x; i < 3 * kAccComp; i += blockDim.x )
-        s_acc[i] = T( 0 );
-    double beta[3] = { 0, 0, 0 };
-    if ( P.beta )
-        beta[0] = P.beta[0], beta[1] = P.beta[1], beta[2] = P.beta[2];
-    __syncthreads();
+        const long long tile   = g / rows_per_tile;
+        const int       row_lo = int( g - tile * rows_per_tile );
+        const int       row_hi = int( min( (long long) N, row_lo + min( (long long) SM, g_end - g ) - 1 ) );
+        g += row_hi - row_lo + 1;
+        const int  tx        = int( tile % P.xtiles );
+        const int  d         = int( tile / P.xtiles );
+        const int  sx0       = tx * kTS - 1; // strip of warp 0
+        const int  nsteps    = row_hi - row_lo + 2; // step s computes cell cy = row_lo - 1 + s
+        const int  X         = sx0 + w;
+        const bool strip_ok  = X >= 0 && X <= N - 1;
+        const bool col_owned = w >= 1;                              // node column X belongs to this tile
+        const bool owns_last = tx == P.xtiles - 1 && w == kW - 1;   // ... and node column N = X + 1
+        const int  s0        = row_lo == 0 ? 1 : 0;
+        const T*   radii     = s_radii + d * ( ( n1 + 1 ) & ~1 );
 
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int RC   = min( kRC, N );
-    constexpr unsigned FULL = 0xffffffffu;
-
-    for ( int r0 = 0; r0 < N; r0 += RC )
-    {
-        const bool last_chunk = ( r0 + RC == N );
-        const int  r          = r0 + lane;
-        const int  rl         = min( r, N - 1 );
-        bool       valid      = lane < RC;
-        if ( ( P.skip_cmb && r == 0 ) || ( P.skip_surface && r == N - 1 ) )
-            valid = false;
-        const T r_lo = s_radii[rl], r_hi = s_radii[rl + 1];
-        const T h     = T( 0.5 ) * ( r_hi - r_lo );
-        const T kappa = T( 0.5 ) * ( r_hi + r_lo ) / ( T( 3 ) * h );
-        const T wbase = h * T( 0.25 ) * T( 1.0 / 6.0 ); // omega = k_sum/6 * |det M| * h/4
-
-        for ( int phase = 0; phase < 4; ++phase )
+        __syncthreads(); // previous segment done with the geometry buffer
+        for ( int i = threadIdx.x; i < kW * nsteps * 2; i += blockDim.x )
         {
-            const int ox = ( phase & 1 ) ^ ( cxlo & 1 ), oy = ( ( phase >> 1 ) & 1 ) ^ ( cylo & 1 );
-            const int nxp = ncx > ox ? ( ncx - ox + 1 ) / 2 : 0, nyp = ncy > oy ? ( ncy - oy + 1 ) / 2 : 0;
-            for ( int task = warp; task < nxp * nyp; task += kWarps )
-            {
-                const int lx = ox + 2 * ( task / nyp ), ly = oy + 2 * ( task % nyp );
-                const int X = cxlo + lx, Y = cylo + ly;
+            const int wdg = i & 1, cs = i >> 1;
+            const int ww = cs / nsteps, s = cs % nsteps;
+            const int Xg = sx0 + ww, Y = row_lo - 1 + s;
+            if ( Xg < 0 || Xg > N - 1 || Y < 0 || Y > N - 1 )
+                continue;
+            const double* c00 = P.coords + lat_index( n1, d, Xg, Y ) * 3;
+            const double* c10 = P.coords + lat_index( n1, d, Xg + 1, Y ) * 3;
+            const double* c01 = P.coords + lat_index( n1, d, Xg, Y + 1 ) * 3;
+            const double* c11 = P.coords + lat_index( n1, d, Xg + 1, Y + 1 ) * 3;
+            double        q[9], adet;
+            if ( wdg == 0 )
+                lateral_geometry( c00, c10, c01, q, &adet );
+            else
+                lateral_geometry( c11, c01, c10, q, &adet );
+            T* gg = s_geo + ( ( ww * ( SM + 2 ) + s ) * 2 + wdg ) * 10;
+            for ( int j = 0; j < 9; ++j )
+                gg[j] = T( q[j] );
+            gg[9] = T( adet );
+        }
 
-                // corner order: 0 = (0,0), 1 = (1,0), 2 = (0,1), 3 = (1,1)
-                T      ub[4][3], ut[4][3], kb[4], kt[4];
-                size_t base[4];
-#pragma unroll
-                for ( int q = 0; q < 4; ++q )
+        for ( int r0 = 0; r0 < N; r0 += RC )
+        {
+            const bool last_chunk = r0 + RC == N;
+            const int  r          = r0 + lane;
+            const int  rl         = min( r, N - 1 );
+            bool       lane_ok    = lane < RC;
+            if ( ( P.skip_cmb && r == 0 ) || ( P.skip_surface && r == N - 1 ) )
+                lane_ok = false;
+
+            const int cyb = row_lo - 1 + s0;
+            for ( int j = 0; j < kSlots - 1; ++j )
+            {
+                issue_row( f0, f1, f2, f3, N, n1, slot( cyb + j ), d, sx0, cyb + j, r0, RC, lane, w );
+                __pipeline_commit();
+            }
+            __pipeline_wait_prior( kSlots - 3 );
+            __syncthreads();
+
+            const T   r_lo = radii[rl], r_hi = radii[rl + 1];
+            const T   h     = T( 0.5 ) * ( r_hi - r_lo );
+            const T   kappa = T( 0.5 ) * ( r_hi + r_lo ) / ( T( 3 ) * h );
+            const T   wbase = h * T( 0.25 / 6.0 ); // omega = (k_sum / 6) |det M| h / 4
+            const int lb    = min( lane, kRC - 1 );
+
+            T  cL[3] = { 0, 0, 0 }, cR[3] = { 0, 0, 0 };
+            T* tw    = s_top + w * 24;
+            if ( lane < 24 )
+                tw[lane] = T( 0 );
+            __syncwarp();
+            for ( int s = s0; s < nsteps; ++s )
+            {
+                const int  cy      = row_lo - 1 + s;
+                const bool cell_ok = strip_ok && cy <= N - 1;
+                T          L[3], R[3];
                 {
-                    base[q] = lat_index( n1, d, X + ( q & 1 ), Y + ( q >> 1 ) ) * n1;
-                    kb[q]   = __ldg( P.k + base[q] + rl );
-#pragma unroll
-                    for ( int c = 0; c < 3; ++c )
-                        ub[q][c] = __ldg( P.src.p[c] + base[q] + rl );
-                }
-#pragma unroll
-                for ( int q = 0; q < 4; ++q )
-                {
-                    kt[q] = __shfl_down_sync( FULL, kb[q], 1 );
-#pragma unroll
-                    for ( int c = 0; c < 3; ++c )
-                        ut[q][c] = __shfl_down_sync( FULL, ub[q][c], 1 );
-                }
-                if ( lane == RC - 1 )
-                {
+                    // corners: 0 = (X, cy), 1 = (X+1, cy), 2 = (X, cy+1), 3 = (X+1, cy+1)
+                    const T* rp = slot( cy ) + w * 4 * kLev;
+                    const T* rn = slot( cy + 1 ) + w * 4 * kLev;
+                    T        S[4][3], D[4][3], K[4];
 #pragma unroll
                     for ( int q = 0; q < 4; ++q )
                     {
-                        kt[q] = __ldg( P.k + base[q] + rl + 1 );
+                        const T* base = ( q < 2 ? rp : rn ) + ( q & 1 ) * 4 * kLev;
 #pragma unroll
                         for ( int c = 0; c < 3; ++c )
-                            ut[q][c] = __ldg( P.src.p[c] + base[q] + rl + 1 );
+                        {
+                            const T bv = base[c * kLev + lb], tv = base[c * kLev + lb + 1];
+                            S[q][c] = bv + tv, D[q][c] = tv - bv;
+                        }
+                        K[q] = base[3 * kLev + lb] + base[3 * kLev + lb + 1];
                     }
-                }
-
-                T bot[4][3], top[4][3];
-                {
-                    T S[4][3], D[4][3];
-#pragma unroll
-                    for ( int q = 0; q < 4; ++q )
-#pragma unroll
-                        for ( int c = 0; c < 3; ++c )
-                            S[q][c] = ub[q][c] + ut[q][c], D[q][c] = ut[q][c] - ub[q][c];
-                    const T* g0 = s_geo + ( ( lx * ncy + ly ) * 2 ) * 10;
+                    const T* g0 = s_geo + ( ( w * ( SM + 2 ) + s ) * 2 ) * 10;
                     const T* g1 = g0 + 10;
                     T        v1[3], v2[3], v3[3], A1[3], A2[3], A3[3], B1[3], B2[3], B3[3];
-                    // wedge 0: nodes (0,0),(1,0),(0,1)
 #pragma unroll
                     for ( int c = 0; c < 3; ++c )
                         v1[c] = S[1][c] - S[0][c], v2[c] = S[2][c] - S[0][c], v3[c] = D[0][c] + D[1][c] + D[2][c];
-                    const T k0 = ( kb[0] + kb[1] + kb[2] ) + ( kt[0] + kt[1] + kt[2] );
-                    wedge_flux( g0, v1, v2, v3, kappa, wbase * k0 * g0[9], A1, A2, A3 );
-                    // wedge 1: nodes (1,1),(0,1),(1,0)
+                    wedge_flux( g0, v1, v2, v3, kappa, wbase * ( K[0] + K[1] + K[2] ) * g0[9], A1, A2, A3 );
 #pragma unroll
                     for ( int c = 0; c < 3; ++c )
                         v1[c] = S[2][c] - S[3][c], v2[c] = S[1][c] - S[3][c], v3[c] = D[3][c] + D[2][c] + D[1][c];
-                    const T k1 = ( kb[3] + kb[2] + kb[1] ) + ( kt[3] + kt[2] + kt[1] );
-                    wedge_flux( g1, v1, v2, v3, kappa, wbase * k1 * g1[9], B1, B2, B3 );
+                    wedge_flux( g1, v1, v2, v3, kappa, wbase * ( K[3] + K[2] + K[1] ) * g1[9], B1, B2, B3 );
+                    const bool ok = cell_ok && lane_ok;
 #pragma unroll
                     for ( int c = 0; c < 3; ++c )
                     {
                         const T xa = A1[c] + A2[c], xb = B1[c] + B2[c];
                         const T s33 = A3[c] + B3[c];
                         const T e10 = A1[c] + B2[c], e01 = A2[c] + B1[c];
-                        bot[0][c] = -xa - A3[c], top[0][c] = -xa + A3[c];
-                        bot[1][c] = e10 - s33, top[1][c] = e10 + s33;
-                        bot[2][c] = e01 - s33, top[2][c] = e01 + s33;
-                        bot[3][c] = -xb - B3[c], top[3][c] = -xb + B3[c];
-                        if ( !valid )
-                            bot[0][c] = top[0][c] = bot[1][c] = top[1][c] = bot[2][c] = top[2][c] = bot[3][c] =
-                                top[3][c] = T( 0 );
+                        T       bo[4], tp[4], val[4];
+                        bo[0] = -xa - A3[c], tp[0] = -xa + A3[c];
+                        bo[1] = e10 - s33, tp[1] = e10 + s33;
+                        bo[2] = e01 - s33, tp[2] = e01 + s33;
+                        bo[3] = -xb - B3[c], tp[3] = -xb + B3[c];
+#pragma unroll
+                        for ( int q = 0; q < 4; ++q )
+                        {
+                            if ( !ok )
+                                bo[q] = tp[q] = T( 0 );
+                            const T below = __shfl_up_sync( FULL, tp[q], 1 );
+                            val[q]        = bo[q] + ( lane > 0 ? below : T( 0 ) );
+                        }
+                        L[c] = val[0] + cL[c];
+                        R[c] = val[1] + cR[c];
+                        cL[c] = val[2], cR[c] = val[3];
+                        if ( lane == RC - 1 ) // level r0 + RC: only the top cell of the chunk contributes
+                        {
+                            T* tcur = tw + ( s & 1 ) * 12;
+#pragma unroll
+                            for ( int q = 0; q < 4; ++q )
+                                tcur[q * 3 + c] = tp[q];
+                        }
                     }
                 }
 
-#pragma unroll
-                for ( int q = 0; q < 4; ++q )
+                T* xb = s_xbuf + ( ( s & 1 ) * kW + w ) * 3 * kLev;
+                if ( lane < RC )
                 {
-                    const int  Xn = X + ( q & 1 ), Yn = Y + ( q >> 1 );
-                    const bool owned = Xn >= xlo && Xn <= xhi && Yn >= ylo && Yn <= yhi; // warp uniform
-                    T*         acc   = s_acc + ( ( Xn - xlo ) * ( kTile + 1 ) + ( Yn - ylo ) ) * kAccCol;
+#pragma unroll
+                    for ( int c = 0; c < 3; ++c )
+                        xb[c * kLev + lane] = R[c];
+                }
+                if ( lane == RC - 1 )
+                {
+                    const T* tcur = tw + ( s & 1 ) * 12;
+                    const T* tprv = tw + ( ( s + 1 ) & 1 ) * 12;
+#pragma unroll
+                    for ( int c = 0; c < 3; ++c )
+                        xb[c * kLev + RC] = tcur[3 + c] + tprv[9 + c];
+                }
+                issue_row( f0, f1, f2, f3, N, n1, slot( cy + kSlots - 1 ), d, sx0, cy + kSlots - 1, r0, RC, lane, w );
+                __pipeline_commit();
+                __pipeline_wait_prior( kSlots - 3 );
+                __syncthreads();
+
+                if ( s == 0 )
+                    continue; // row row_lo - 1 belongs to another segment
+#pragma unroll
+                for ( int side = 0; side < 2; ++side )
+                {
+                    if ( side == 0 ? !col_owned : !owns_last )
+                        continue;
+                    const int Xn  = X + side;
+                    const int slt = side == 0 ? w : kW;
+                    T         F[3], F32[3];
+                    const T*  xl   = s_xbuf + ( ( s & 1 ) * kW + ( w - 1 ) ) * 3 * kLev;
+                    const T*  tcur = tw + ( s & 1 ) * 12;
+                    const T*  tprv = tw + ( ( s + 1 ) & 1 ) * 12;
 #pragma unroll
                     for ( int c = 0; c < 3; ++c )
                     {
-                        const T below = __shfl_up_sync( FULL, top[q][c], 1 );
-                        if ( owned )
+                        if ( side == 0 )
                         {
-                            if ( lane < RC )
-                                acc[c * kAccComp + lane] += bot[q][c] + ( lane > 0 ? below : T( 0 ) );
-                            if ( lane == RC - 1 )
-                                acc[c * kAccComp + RC] += top[q][c];
+                            F[c]   = L[c] + ( lane < RC ? xl[c * kLev + lane] : T( 0 ) );
+                            F32[c] = tcur[c] + tprv[6 + c] + xl[c * kLev + RC];
+                        }
+                        else
+                        {
+                            F[c]   = R[c];
+                            F32[c] = tcur[3 + c] + tprv[9 + c];
+                        }
+                    }
+                    T* carry = s_carry + ( slt * ( SM + 2 ) + s ) * 3;
+                    if ( r0 > 0 && lane == 0 )
+                    {
+#pragma unroll
+                        for ( int c = 0; c < 3; ++c )
+                            F[c] += carry[c];
+                    }
+                    __syncwarp();
+                    const size_t nb  = lat_index( n1, d, Xn, cy ) * n1;
+                    const int    lev = lane < RC ? r : N; // lanes < RC: level r; lane RC-1 also level N
+                    if ( beta )
+                    {
+                        const double* u   = P.coords + lat_index( n1, d, Xn, cy ) * 3;
+                        const double  rr  = double( radii[lane < RC ? r : 0] ), rN = double( radii[N] );
+                        const double  x0  = u[0] * rr, x1 = u[1] * rr, x2 = u[2] * rr;
+                        const double  y0  = u[0] * rN, y1 = u[1] * rN, y2 = u[2] * rN;
+                        F[0] += T( beta[1] * x2 - beta[2] * x1 );
+                        F[1] += T( beta[2] * x0 - beta[0] * x2 );
+                        F[2] += T( beta[0] * x1 - beta[1] * x0 );
+                        F32[0] += T( beta[1] * y2 - beta[2] * y1 );
+                        F32[1] += T( beta[2] * y0 - beta[0] * y2 );
+                        F32[2] += T( beta[0] * y1 - beta[1] * y0 );
+                    }
+                    (void) lev;
+                    if ( lane < RC )
+                    {
+                        T* p0 = o0 + nb + r;
+                        T* p1 = o1 + nb + r;
+                        T* p2 = o2 + nb + r;
+                        *p0   = add_mode ? *p0 + F[0] : F[0];
+                        *p1   = add_mode ? *p1 + F[1] : F[1];
+                        *p2   = add_mode ? *p2 + F[2] : F[2];
+                    }
+                    if ( lane == RC - 1 )
+                    {
+                        if ( last_chunk )
+                        {
+                            T* p0 = o0 + nb + N;
+                            T* p1 = o1 + nb + N;
+                            T* p2 = o2 + nb + N;
+                            *p0   = add_mode ? *p0 + F32[0] : F32[0];
+                            *p1   = add_mode ? *p1 + F32[1] : F32[1];
+                            *p2   = add_mode ? *p2 + F32[2] : F32[2];
+                        }
+                        else
+                        {
+                            carry[0] = F32[0], carry[1] = F32[1], carry[2] = F32[2];
                         }
                     }
                 }
             }
+            __pipeline_wait_prior( 0 );
             __syncthreads();
         }
-
-        // write out completed node levels of all owned columns
-        const int nlev = last_chunk ? RC + 1 : RC;
-        for ( int t = warp; t < nxo * nyo * 3; t += kWarps )
-        {
-            const int    c = t % 3, col = t / 3;
-            const int    lx = col / nyo, ly = col % nyo;
-            const int    X = xlo + lx, Y = ylo + ly;
-            const size_t lat = lat_index( n1, d, X, Y );
-            const T*     acc = s_acc + c * kAccComp + ( lx * ( kTile + 1 ) + ly ) * kAccCol;
-            T*           out = P.dst.p[c] + lat * n1 + r0;
-            for ( int l = lane; l < nlev; l += 32 )
-            {
-                T v = acc[l];
-                if ( P.beta )
-                {
-                    const double  rr = double( s_radii[r0 + l] );
-                    const double* u  = P.coords + lat * 3;
-                    const double  x[3] = { u[0] * rr, u[1] * rr, u[2] * rr };
-                    const double  bx   = c == 0 ? beta[1] * x[2] - beta[2] * x[1]
-                                                : ( c == 1 ? beta[2] * x[0] - beta[0] * x[2] : beta[0] * x[1] - beta[1] * x[0] );
-                    v += T( bx );
-                }
-                out[l] = P.add_mode ? out[l] + v : v;
-            }
-        }
-        __syncthreads();
-        for ( int i = threadIdx.x; i < 3 * kCols; i += blockDim.x )
-        {
-            T* a = s_acc + size_t( i ) * kAccCol;
-            a[0] = a[RC];
-            for ( int l = 1; l <= RC; ++l )
-                a[l] = T( 0 );
-        }
-        __syncthreads();
     }
 }
 
@@ -316,7 +427,6 @@ struct CellParams
     Ptr3< const T > src;
     Ptr3< T >     dst;
     int           bc_cmb, bc_surf, diag;
-    int           layers; // 0: all cells; 1: r = 0 only; 2: r = N-1 only; 3: both boundary layers
 };
 
 template < typename T >
@@ -326,26 +436,16 @@ __device__ __forceinline__ void project_out( const T n[3], T v[3] )
     v[0] -= dt * n[0], v[1] -= dt * n[1], v[2] -= dt * n[2];
 }
 
+// Full contribution of cell (d, x, y, r) to its 8 nodes, acc[dx][dy][dr][c].
 template < typename T >
-__global__ void __launch_bounds__( 128 ) kerngen_cell_kernel( CellParams< T > P )
+__device__ void cell_full( const CellParams< T >& P, int d, int x, int y, int r, T acc[2][2][2][3] )
 {
-    const int       N = P.N, n1 = P.n1;
-    const long long t = blockIdx.x * (long long) blockDim.x + threadIdx.x;
-    const int       nr = P.layers == 0 ? N : ( P.layers == 3 ? 2 : 1 );
-    if ( t >= (long long) kDiamonds * N * N * nr )
-        return;
-    const int ri = int( t % nr );
-    const int y  = int( ( t / nr ) % N );
-    const int x  = int( ( t / ( (long long) nr * N ) ) % N );
-    const int d  = int( t / ( (long long) nr * N * N ) );
-    const int r  = P.layers == 0 ? ri : ( P.layers == 1 ? 0 : ( P.layers == 2 ? N - 1 : ( ri == 0 ? 0 : N - 1 ) ) );
-
+    const int  N = P.N, n1 = P.n1;
     const bool at_cmb = r == 0, at_surf = r == N - 1;
     const bool cmb_dir = at_cmb && P.bc_cmb == TN_BC_DIRICHLET, surf_dir = at_surf && P.bc_surf == TN_BC_DIRICHLET;
     const bool cmb_fs = at_cmb && P.bc_cmb == TN_BC_FREESLIP, surf_fs = at_surf && P.bc_surf == TN_BC_FREESLIP;
     const bool diag = P.diag != 0;
 
-    T acc[2][2][2][3];
     T ann[2][2][2];
 #pragma unroll
     for ( int i = 0; i < 8; ++i )
@@ -475,6 +575,22 @@ __global__ void __launch_bounds__( 128 ) kerngen_cell_kernel( CellParams< T > P 
                     o[c] += ann[dx][dy][dr] * un * n[c];
             }
     }
+}
+
+// One thread per cell, atomics (diagonal mode and levels below the tile size).
+template < typename T >
+__global__ void __launch_bounds__( 128 ) kerngen_cell_kernel( CellParams< T > P )
+{
+    const int       N = P.N, n1 = P.n1;
+    const long long t = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if ( t >= (long long) kDiamonds * N * N * N )
+        return;
+    const int r = int( t % N );
+    const int y = int( ( t / N ) % N );
+    const int x = int( ( t / ( (long long) N * N ) ) % N );
+    const int d = int( t / ( (long long) N * N * N ) );
+    T         acc[2][2][2][3];
+    cell_full( P, d, x, y, r, acc );
     for ( int dx = 0; dx < 2; ++dx )
         for ( int dy = 0; dy < 2; ++dy )
             for ( int dr = 0; dr < 2; ++dr )
@@ -483,6 +599,177 @@ __global__ void __launch_bounds__( 128 ) kerngen_cell_kernel( CellParams< T > P 
                 for ( int c = 0; c < 3; ++c )
                     atomicAdd( P.dst.p[c] + i, acc[dx][dy][dr][c] );
             }
+}
+
+// Boundary layers of a non-Neumann boundary, node-centric: one thread per
+// lateral node (d, X, Y) and boundary side visits the six wedges of the
+// boundary cell layer around it and adds their contributions to its two node
+// levels (the boundary node and the one above / below it).  Each wedge is
+// recomputed by each of its three lateral corners instead of scattering with
+// atomics; the tiled kernel has already written every node without these cells.
+// Free-slip: the boundary node's sum is projected once onto the tangent plane
+// and the normal-normal diagonal sum(Ann) (n . u) n added back, which equals
+// the reference's per-cell projection (kerngen :1880-1935) by linearity.
+constexpr int kBndNodes = 32; // boundary nodes per block (6 wedge threads each)
+
+template < typename T >
+__global__ void __launch_bounds__( 6 * kBndNodes, 4 ) kerngen_boundary_kernel( CellParams< T > P, int sides )
+{
+    __shared__ T sh[6][7][kBndNodes]; // per wedge: boundary-level (3), interior-level (3), Ann
+    const int       N = P.N, n1 = P.n1;
+    const int       nside = sides == 3 ? 2 : 1;
+    const int       j     = threadIdx.x % kBndNodes; // node slot
+    const int       a     = threadIdx.x / kBndNodes; // wedge around the node
+    const long long t     = blockIdx.x * (long long) kBndNodes + j;
+    const bool      live  = t < (long long) kDiamonds * n1 * n1 * nside;
+    // side slowest, then diamond, x, y: a block's nodes are consecutive in y and
+    // share most of the columns they read
+    const long long per   = (long long) kDiamonds * n1 * n1;
+    const int       si    = live ? int( t / per ) : 0;
+    const int       Y     = int( t % n1 );
+    const int       X     = int( ( t / n1 ) % n1 );
+    const int       d     = int( ( t % per ) / ( (long long) n1 * n1 ) );
+    const int       side  = sides == 3 ? si : ( sides == 1 ? 0 : 1 );
+    const int       rc    = side == 0 ? 0 : N - 1; // boundary cell layer
+    const int       bc    = side == 0 ? P.bc_cmb : P.bc_surf;
+    const bool      fs    = bc == TN_BC_FREESLIP;
+    const T         third = T( 1.0 / 3.0 );
+
+    T sum_b[3] = { 0, 0, 0 }, sum_i[3] = { 0, 0, 0 }, ann = 0;
+    // wedge a around node (X, Y): cell offset, wedge index, local lateral index
+    const int ax  = ( a == 1 || a == 2 || a == 5 ) ? -1 : 0;
+    const int ay  = ( a >= 3 ) ? -1 : 0;
+    const int wdg = ( a == 2 || a == 4 || a == 5 ) ? 1 : 0;
+    const int loc = a == 0 ? 0 : ( a == 1 ? 1 : ( a == 2 ? 2 : ( a == 3 ? 2 : ( a == 4 ? 1 : 0 ) ) ) );
+    const int cx = X + ax, cy = Y + ay;
+    if ( live && cx >= 0 && cx <= N - 1 && cy >= 0 && cy <= N - 1 )
+    {
+        const T r_lo = P.radii[d * n1 + rc], r_hi = P.radii[d * n1 + rc + 1];
+        T       p[3][3], u[6][3], kn[6];
+        size_t  lat[3];
+#pragma unroll
+        for ( int n = 0; n < 3; ++n )
+        {
+            // wedge 0: (0,0),(1,0),(0,1); wedge 1: (1,1),(0,1),(1,0)
+            const int ox = wdg == 0 ? ( n == 1 ? 1 : 0 ) : ( n == 1 ? 0 : 1 );
+            const int oy = wdg == 0 ? ( n == 2 ? 1 : 0 ) : ( n == 2 ? 0 : 1 );
+            lat[n]          = lat_index( n1, d, cx + ox, cy + oy );
+            const double* c = P.coords + lat[n] * 3;
+            p[n][0] = T( c[0] ), p[n][1] = T( c[1] ), p[n][2] = T( c[2] );
+        }
+#pragma unroll
+        for ( int n = 0; n < 6; ++n )
+        {
+            const size_t i = lat[n % 3] * n1 + rc + ( n < 3 ? 0 : 1 );
+            kn[n]          = P.k[i];
+            u[n][0] = P.src.p[0][i], u[n][1] = P.src.p[1][i], u[n][2] = P.src.p[2][i];
+        }
+        T       IT[3][3];
+        const T det = wedge_jacobian_it( p[0], p[1], p[2], r_lo, r_hi, third, third, T( 0 ), IT );
+        const T kwJ = ( ( kn[0] + kn[1] + kn[2] + kn[3] + kn[4] + kn[5] ) / T( 6 ) ) * fabs( det );
+        T       g[6][3];
+#pragma unroll
+        for ( int n = 0; n < 6; ++n )
+        {
+            T gr[3];
+            grad_shape_ref( n, third, third, T( 0 ), gr );
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+                g[n][c] = IT[c][0] * gr[0] + IT[c][1] * gr[1] + IT[c][2] * gr[2];
+        }
+        const int nb0 = side == 0 ? 0 : 3; // first boundary-level node of the wedge
+        // trial side: Dirichlet drops the boundary nodes, free-slip projects them
+        T G[3][3] = { { 0 } };
+#pragma unroll
+        for ( int n = 0; n < 6; ++n )
+        {
+            const bool on_b = n >= nb0 && n < nb0 + 3;
+            if ( on_b && !fs )
+                continue;
+            T v[3] = { u[n][0], u[n][1], u[n][2] };
+            if ( on_b )
+            {
+                T       nn[3] = { p[n % 3][0], p[n % 3][1], p[n % 3][2] };
+                const T mm    = sqrt( nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2] );
+                nn[0] /= mm, nn[1] /= mm, nn[2] /= mm;
+                project_out( nn, v );
+            }
+#pragma unroll
+            for ( int i = 0; i < 3; ++i )
+#pragma unroll
+                for ( int k = 0; k < 3; ++k )
+                    G[i][k] += g[n][i] * v[k];
+        }
+        const T div = G[0][0] + G[1][1] + G[2][2];
+        // test side: kwJ (2 eps(u) g_n - 2/3 div g_n) for the node's two levels
+        const int nb = nb0 + loc, ni = side == 0 ? loc + 3 : loc;
+        T         gb[3], gi[3], ub[3], pl[3]; // register selects keep all indexing static
+#pragma unroll
+        for ( int n = 0; n < 6; ++n )
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+            {
+                if ( n == nb )
+                    gb[c] = g[n][c], ub[c] = u[n][c];
+                if ( n == ni )
+                    gi[c] = g[n][c];
+                if ( n == loc )
+                    pl[c] = p[n][c];
+            }
+#pragma unroll
+        for ( int c = 0; c < 3; ++c )
+            sum_i[c] = kwJ * ( gi[0] * ( G[0][c] + G[c][0] ) + gi[1] * ( G[1][c] + G[c][1] ) +
+                               gi[2] * ( G[2][c] + G[c][2] ) - T( 2.0 / 3.0 ) * gi[c] * div );
+        const T gg = gb[0] * gb[0] + gb[1] * gb[1] + gb[2] * gb[2];
+        if ( fs )
+        {
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+                sum_b[c] = kwJ * ( gb[0] * ( G[0][c] + G[c][0] ) + gb[1] * ( G[1][c] + G[c][1] ) +
+                                   gb[2] * ( G[2][c] + G[c][2] ) - T( 2.0 / 3.0 ) * gb[c] * div );
+            const T mm = sqrt( pl[0] * pl[0] + pl[1] * pl[1] + pl[2] * pl[2] );
+            const T ng = ( pl[0] * gb[0] + pl[1] * gb[1] + pl[2] * gb[2] ) / mm;
+            ann        = kwJ * ( gg + ng * ng * third );
+        }
+        else
+        {
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+                sum_b[c] = kwJ * ub[c] * ( gg + gb[c] * gb[c] * third );
+        }
+    }
+#pragma unroll
+    for ( int c = 0; c < 3; ++c )
+        sh[a][c][j] = sum_b[c], sh[a][3 + c][j] = sum_i[c];
+    sh[a][6][j] = ann;
+    __syncthreads();
+    if ( a != 0 || !live )
+        return;
+    T tb[3] = { 0, 0, 0 }, ti[3] = { 0, 0, 0 }, tann = 0;
+    for ( int w = 0; w < 6; ++w )
+    {
+#pragma unroll
+        for ( int c = 0; c < 3; ++c )
+            tb[c] += sh[w][c][j], ti[c] += sh[w][3 + c][j];
+        tann += sh[w][6][j];
+    }
+    const size_t base = lat_index( n1, d, X, Y ) * n1;
+    const int    lb = side == 0 ? 0 : N, li = side == 0 ? 1 : N - 1;
+    if ( fs )
+    {
+        // project the summed boundary-node contribution, add the normal-normal diagonal
+        const double* un     = P.coords + lat_index( n1, d, X, Y ) * 3;
+        T             nrm[3] = { T( un[0] ), T( un[1] ), T( un[2] ) };
+        const T       mm     = sqrt( nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2] );
+        nrm[0] /= mm, nrm[1] /= mm, nrm[2] /= mm;
+        project_out( nrm, tb );
+        const T un_ = nrm[0] * P.src.p[0][base + lb] + nrm[1] * P.src.p[1][base + lb] + nrm[2] * P.src.p[2][base + lb];
+#pragma unroll
+        for ( int c = 0; c < 3; ++c )
+            tb[c] += tann * un_ * nrm[c];
+    }
+    P.dst.p[0][base + lb] += tb[0], P.dst.p[1][base + lb] += tb[1], P.dst.p[2][base + lb] += tb[2];
+    P.dst.p[0][base + li] += ti[0], P.dst.p[1][base + li] += ti[1], P.dst.p[2][base + li] += ti[2];
 }
 
 // ---------------------------------------------------------------------------
@@ -498,24 +785,31 @@ struct Mat3
 };
 
 template < typename T >
-__global__ void penalty_dots_kernel( size_t ns, int n1, const double* __restrict__ coords, const T* __restrict__ radii,
-                                     Ptr3< const T > src, const uint8_t* __restrict__ lat_owned, double* partials, unsigned int* counter, double* result )
+__global__ void penalty_dots_kernel( size_t nlat, int n1, const double* __restrict__ coords, const T* __restrict__ radii,
+                                     Ptr3< const T > src, const uint8_t* __restrict__ lat_owned, double* partials,
+                                     unsigned int* counter, double* result )
 {
-    Neumaier acc[3];
-    for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
+    // one warp per lateral column (owned columns only), lanes along r
+    Neumaier     acc[3];
+    const int    lane = threadIdx.x & 31;
+    const size_t wid = ( blockIdx.x * size_t( blockDim.x ) + threadIdx.x ) >> 5;
+    const size_t nw  = ( size_t( gridDim.x ) * blockDim.x ) >> 5;
+    for ( size_t lat = wid; lat < nlat; lat += nw )
     {
-        const size_t lat = i / n1;
         if ( !lat_owned[lat] )
             continue;
-        const int     r  = int( i - lat * n1 );
-        const int     d  = int( lat / ( size_t( n1 ) * n1 ) );
-        const double  rr = double( radii[d * n1 + r] );
-        const double* u  = coords + lat * 3;
-        const double  x[3] = { u[0] * rr, u[1] * rr, u[2] * rr };
-        const double  v[3] = { double( src.p[0][i] ), double( src.p[1][i] ), double( src.p[2][i] ) };
-        acc[0].add( x[1] * v[2] - x[2] * v[1] );
-        acc[1].add( x[2] * v[0] - x[0] * v[2] );
-        acc[2].add( x[0] * v[1] - x[1] * v[0] );
+        const int     d = int( lat / ( size_t( n1 ) * n1 ) );
+        const double* u = coords + lat * 3;
+        for ( int r = lane; r < n1; r += 32 )
+        {
+            const size_t i  = lat * n1 + r;
+            const double rr = double( radii[d * n1 + r] );
+            const double x[3] = { u[0] * rr, u[1] * rr, u[2] * rr };
+            const double v[3] = { double( src.p[0][i] ), double( src.p[1][i] ), double( src.p[2][i] ) };
+            acc[0].add( x[1] * v[2] - x[2] * v[1] );
+            acc[1].add( x[2] * v[0] - x[0] * v[2] );
+            acc[2].add( x[0] * v[1] - x[1] * v[0] );
+        }
     }
     block_sum_finish< 3 >( acc, partials, counter, result );
 }
@@ -561,16 +855,11 @@ const float* mesh_radii< float >( const tn_mesh* m )
 }
 
 template < typename T >
-int launch_cells( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k, Ptr3< const T > src, Ptr3< T > dst,
-                  int layers, cudaStream_t st )
+CellParams< T > cell_params( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k, Ptr3< const T > src,
+                             Ptr3< T > dst )
 {
-    CellParams< T > C{ m->N, m->n1, m->d_coords, mesh_radii< T >( m ), k, src, dst, p->bc_cmb, p->bc_surface,
-                       p->diagonal, layers };
-    const int       nr    = layers == 0 ? m->N : ( layers == 3 ? 2 : 1 );
-    const long long cells = (long long) kDiamonds * m->N * m->N * nr;
-    kerngen_cell_kernel< T ><<< unsigned( ( cells + 127 ) / 128 ), 128, 0, st >>>( C );
-    TN_LAUNCH_CHECK();
-    return TN_OK;
+    return CellParams< T >{ m->N, m->n1, m->d_coords, mesh_radii< T >( m ), k, src, dst, p->bc_cmb, p->bc_surface,
+                            p->diagonal };
 }
 
 }  // namespace
@@ -596,8 +885,8 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
         Mat3 gi;
         for ( int i = 0; i < 9; ++i )
             gi.a[i] = m->penalty_gram_inv[i];
-        const unsigned blocks = unsigned( std::min< size_t >( ( m->ns + 1023 ) / 1024, kRedMaxBlocks ) );
-        penalty_dots_kernel< T ><<< blocks, 256, 0, st >>>( m->ns, m->n1, m->d_coords, mesh_radii< T >( m ), s,
+        const unsigned blocks = unsigned( std::min< size_t >( ( m->nlat + 7 ) / 8, kRedMaxBlocks ) );
+        penalty_dots_kernel< T ><<< blocks, 256, 0, st >>>( m->nlat, m->n1, m->d_coords, mesh_radii< T >( m ), s,
                                                            m->d_lat_owned, m->d_red_partials,
                                                            m->d_red_counter, m->d_red_result );
         TN_LAUNCH_CHECK();
@@ -605,14 +894,14 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
         TN_LAUNCH_CHECK();
     }
 
-    if ( p->diagonal || N < kTile )
+    if ( p->diagonal || N < kTS )
     {
         if ( p->apply_mode == TN_APPLY_REPLACE )
             for ( int c = 0; c < 3; ++c )
                 TN_CUDA_TRY( cudaMemsetAsync( dst[c], 0, m->ns * sizeof( T ), st ) );
-        int rc = launch_cells< T >( m, p, k, s, o, 0, st );
-        if ( rc )
-            return rc;
+        const long long cells = (long long) kDiamonds * N * N * N;
+        kerngen_cell_kernel< T ><<< unsigned( ( cells + 127 ) / 128 ), 128, 0, st >>>( cell_params( m, p, k, s, o ) );
+        TN_LAUNCH_CHECK();
         if ( fsfs )
         {
             penalty_axpy_kernel< T ><<< 148 * 8, 256, 0, st >>>( m->ns, m->n1, m->d_coords, mesh_radii< T >( m ),
@@ -623,9 +912,21 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
     else
     {
         const bool      skip_cmb = p->bc_cmb != TN_BC_NEUMANN, skip_surf = p->bc_surface != TN_BC_NEUMANN;
+        static int num_sms = 0;
+        if ( num_sms == 0 )
+        {
+            int dev = 0;
+            TN_CUDA_TRY( cudaGetDevice( &dev ) );
+            TN_CUDA_TRY( cudaDeviceGetAttribute( &num_sms, cudaDevAttrMultiProcessorCount, dev ) );
+        }
+        const int       xtiles = N / kTS;
+        const long long items  = (long long) kDiamonds * xtiles * ( N + 1 );
+        const int       grid   = int( std::min< long long >( (long long) num_sms * TN_TILE_MINBLOCKS, items ) );
+        const int       seg    = int( std::min< long long >( kSegMax, ( items + grid - 1 ) / grid ) );
         TileParams< T > P{ N,
                            m->n1,
-                           N / kTile,
+                           xtiles,
+                           seg,
                            m->d_coords,
                            mesh_radii< T >( m ),
                            k,
@@ -635,22 +936,18 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
                            skip_cmb,
                            skip_surf,
                            fsfs ? m->d_red_result + 3 : nullptr };
-        const size_t smem = tile_smem_bytes< T >( m->n1 );
-        static bool  attr_set[2] = { false, false };
-        if ( !attr_set[sizeof( T ) == 8] )
-        {
-            TN_CUDA_TRY( cudaFuncSetAttribute( kerngen_tile_kernel< T >, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               int( smem ) + 8192 ) );
-            attr_set[sizeof( T ) == 8] = true;
-        }
-        const unsigned blocks = unsigned( kDiamonds * ( N / kTile ) * ( N / kTile ) );
-        kerngen_tile_kernel< T ><<< blocks, kThreads, smem, st >>>( P );
+        const size_t smem = tile_smem_bytes< T >( m->n1, seg );
+        TN_CUDA_TRY( cudaFuncSetAttribute( kerngen_tile_kernel< T >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           int( smem ) ) );
+        kerngen_tile_kernel< T ><<< grid, kThreads, smem, st >>>( P );
         TN_LAUNCH_CHECK();
         if ( skip_cmb || skip_surf )
         {
-            int rc = launch_cells< T >( m, p, k, s, o, skip_cmb && skip_surf ? 3 : ( skip_cmb ? 1 : 2 ), st );
-            if ( rc )
-                return rc;
+            const int       sides   = skip_cmb && skip_surf ? 3 : ( skip_cmb ? 1 : 2 );
+            const long long nodes = (long long) kDiamonds * m->n1 * m->n1 * ( sides == 3 ? 2 : 1 );
+            kerngen_boundary_kernel< T ><<< unsigned( ( nodes + kBndNodes - 1 ) / kBndNodes ), 6 * kBndNodes, 0, st >>>(
+                cell_params( m, p, k, s, o ), sides );
+            TN_LAUNCH_CHECK();
         }
     }
     if ( p->comm_mode == TN_COMM_ADDITIVE )

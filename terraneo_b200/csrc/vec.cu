@@ -28,12 +28,10 @@ template < typename T >
 __global__ void lincomb_kernel( size_t ns, int ncomp, Ptr3< T > y, T c0, int nx, T c1, Ptr3< const T > x1, T c2,
                                 Ptr3< const T > x2, T c3, Ptr3< const T > x3 )
 {
-    const size_t total = ns * ncomp;
-    for ( size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; t < total; t += size_t( gridDim.x ) * blockDim.x )
+    const int c = blockIdx.y;
+    for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
     {
-        const int    c = int( t / ns );
-        const size_t i = t - size_t( c ) * ns;
-        T            v = c0;
+        T v = c0;
         if ( nx >= 1 )
             v = v + c1 * x1.p[c][i];
         if ( nx >= 2 )
@@ -47,11 +45,9 @@ __global__ void lincomb_kernel( size_t ns, int ncomp, Ptr3< T > y, T c0, int nx,
 template < typename T, int OP >
 __global__ void elementwise_kernel( size_t ns, int ncomp, Ptr3< T > y, Ptr3< const T > x )
 {
-    const size_t total = ns * ncomp;
-    for ( size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; t < total; t += size_t( gridDim.x ) * blockDim.x )
+    const int c = blockIdx.y;
+    for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
     {
-        const int    c = int( t / ns );
-        const size_t i = t - size_t( c ) * ns;
         if ( OP == 0 )
             y.p[c][i] = T( 1 ) / y.p[c][i]; // invert_inplace (grid_operations.hpp:253)
         else
@@ -62,29 +58,33 @@ __global__ void elementwise_kernel( size_t ns, int ncomp, Ptr3< T > y, Ptr3< con
 template < typename TO, typename TI >
 __global__ void cast_kernel( size_t ns, int ncomp, Ptr3< TO > y, Ptr3< const TI > x )
 {
-    const size_t total = ns * ncomp;
-    for ( size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; t < total; t += size_t( gridDim.x ) * blockDim.x )
-    {
-        const int    c = int( t / ns );
-        const size_t i = t - size_t( c ) * ns;
-        y.p[c][i]      = TO( x.p[c][i] );
-    }
+    const int c = blockIdx.y;
+    for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
+        y.p[c][i] = TO( x.p[c][i] );
 }
 
-// Owned-node dot product: one lateral ownership flag per (diamond, x, y).
+// Owned-node dot product: one lateral ownership flag per (diamond, x, y); a
+// warp handles one lateral column (lanes along r, coalesced) at a time.
 template < typename T >
-__global__ void dot_kernel( size_t ns, int n1, int ncomp, Ptr3< const T > a, Ptr3< const T > b,
+__global__ void dot_kernel( size_t nlat, int n1, int ncomp, Ptr3< const T > a, Ptr3< const T > b,
                             const uint8_t* __restrict__ lat_owned, double* partials, unsigned int* counter,
                             double* result )
 {
-    Neumaier acc;
-    const size_t total = ns * ncomp;
-    for ( size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; t < total; t += size_t( gridDim.x ) * blockDim.x )
+    Neumaier     acc;
+    const int    lane = threadIdx.x & 31;
+    const size_t wid  = ( blockIdx.x * size_t( blockDim.x ) + threadIdx.x ) >> 5;
+    const size_t nw   = ( size_t( gridDim.x ) * blockDim.x ) >> 5;
+    for ( size_t lat = wid; lat < nlat; lat += nw )
     {
-        const int    c = int( t / ns );
-        const size_t i = t - size_t( c ) * ns;
-        if ( lat_owned[i / n1] )
-            acc.add( double( a.p[c][i] ) * double( b.p[c][i] ) );
+        if ( !lat_owned[lat] )
+            continue;
+        for ( int c = 0; c < ncomp; ++c )
+        {
+            const T* pa = a.p[c] + lat * n1;
+            const T* pb = b.p[c] + lat * n1;
+            for ( int r = lane; r < n1; r += 32 )
+                acc.add( double( pa[r] ) * double( pb[r] ) );
+        }
     }
     block_sum_finish< 1 >( &acc, partials, counter, result );
 }
@@ -94,11 +94,9 @@ __global__ void max_abs_kernel( size_t ns, int ncomp, Ptr3< const T > x, double*
                                 double* result )
 {
     double m = 0.0;
-    const size_t total = ns * ncomp;
-    for ( size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; t < total; t += size_t( gridDim.x ) * blockDim.x )
+    for ( int c = 0; c < ncomp; ++c )
+    for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
     {
-        const int    c = int( t / ns );
-        const size_t i = t - size_t( c ) * ns;
         const double v = fabs( double( x.p[c][i] ) );
         // NaN propagates as in Kokkos::max reductions only through comparisons;
         // keep the reference's max-of-abs semantics for finite input.
@@ -112,11 +110,9 @@ __global__ void nan_kernel( size_t ns, int ncomp, Ptr3< const T > x, double* par
                             double* result )
 {
     double flag = 0.0;
-    const size_t total = ns * ncomp;
-    for ( size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; t < total; t += size_t( gridDim.x ) * blockDim.x )
+    for ( int c = 0; c < ncomp; ++c )
+    for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
     {
-        const int    c = int( t / ns );
-        const size_t i = t - size_t( c ) * ns;
         if ( !isfinite( double( x.p[c][i] ) ) )
             flag = 1.0;
     }
@@ -178,7 +174,7 @@ int vec_lincomb( const tn_mesh* m, int ncomp, T* const* y, double c0, int nx, co
         if ( ( rc = ptr3c( ncomp, reinterpret_cast< const T* const* >( x + 3 * i ), px[i], "lincomb" ) ) )
             return rc;
     const T k1 = nx > 0 ? T( c[0] ) : T( 0 ), k2 = nx > 1 ? T( c[1] ) : T( 0 ), k3 = nx > 2 ? T( c[2] ) : T( 0 );
-    lincomb_kernel< T ><<< grid_for( m->ns * ncomp ), kThreads, 0, st >>>( m->ns, ncomp, py, T( c0 ), nx, k1, px[0], k2,
+    lincomb_kernel< T ><<< dim3( grid_for( m->ns ), ncomp ), kThreads, 0, st >>>( m->ns, ncomp, py, T( c0 ), nx, k1, px[0], k2,
                                                                           px[1], k3, px[2] );
     TN_LAUNCH_CHECK();
     return TN_OK;
@@ -192,8 +188,8 @@ int vec_dot( const tn_mesh* m, int ncomp, const T* const* a, const T* const* b, 
     int             rc;
     if ( ( rc = ptr3c( ncomp, a, pa, "dot" ) ) || ( rc = ptr3c( ncomp, b, pb, "dot" ) ) )
         return rc;
-    const unsigned blocks = std::min< unsigned >( grid_for( m->ns * ncomp, 8 ), kRedMaxBlocks );
-    dot_kernel< T ><<< blocks, kThreads, 0, st >>>( m->ns, m->n1, ncomp, pa, pb, m->d_lat_owned, m->d_red_partials,
+    const unsigned blocks = unsigned( std::min< size_t >( ( m->nlat + 15 ) / 16, kRedMaxBlocks ) );
+    dot_kernel< T ><<< blocks, kThreads, 0, st >>>( m->nlat, m->n1, ncomp, pa, pb, m->d_lat_owned, m->d_red_partials,
                                                    m->d_red_counter, m->d_red_result );
     TN_LAUNCH_CHECK();
     return fetch_result( m, 1, st, result );
@@ -210,7 +206,7 @@ int vec_elementwise( const tn_mesh* m, int ncomp, T* const* y, const T* const* x
         return rc;
     if ( OP == 1 && ( rc = ptr3c( ncomp, x, px, "elementwise" ) ) )
         return rc;
-    elementwise_kernel< T, OP ><<< grid_for( m->ns * ncomp ), kThreads, 0, st >>>( m->ns, ncomp, py, px );
+    elementwise_kernel< T, OP ><<< dim3( grid_for( m->ns ), ncomp ), kThreads, 0, st >>>( m->ns, ncomp, py, px );
     TN_LAUNCH_CHECK();
     return TN_OK;
 }
@@ -224,7 +220,7 @@ int vec_cast( const tn_mesh* m, int ncomp, TO* const* y, const TI* const* x, cud
     int              rc;
     if ( ( rc = ptr3( ncomp, y, py, "cast" ) ) || ( rc = ptr3c( ncomp, x, px, "cast" ) ) )
         return rc;
-    cast_kernel< TO, TI ><<< grid_for( m->ns * ncomp ), kThreads, 0, st >>>( m->ns, ncomp, py, px );
+    cast_kernel< TO, TI ><<< dim3( grid_for( m->ns ), ncomp ), kThreads, 0, st >>>( m->ns, ncomp, py, px );
     TN_LAUNCH_CHECK();
     return TN_OK;
 }
