@@ -110,6 +110,46 @@ TN_API int tn_laplace_apply_f32( const tn_mesh* mesh, int treat_boundary, int di
                           const float* src, float* dst, void* stream );
 
 /* ---------------------------------------------------------------------------
+ * Stokes coupling blocks of the Q1-iso-Q2 / Q1 pair: `mesh` carries the P1
+ * velocity (level L), `mesh_p` the P1 pressure (level L-1, same radii range).
+ * Divergence::apply_impl (fe/wedge/operators/shell/divergence.hpp:90): p = B u;
+ * Gradient::apply_impl (gradient.hpp:87): u = B^T p.  3x2 Felippa quadrature;
+ * Dirichlet velocity nodes are eliminated, free-slip ones projected tangentially. */
+TN_API int tn_divergence_apply_f64( const tn_mesh* mesh, const tn_mesh* mesh_p, int bc_cmb, int bc_surface,
+                                    int apply_mode, int comm_mode, const double* const* u, double* p, void* stream );
+TN_API int tn_divergence_apply_f32( const tn_mesh* mesh, const tn_mesh* mesh_p, int bc_cmb, int bc_surface,
+                                    int apply_mode, int comm_mode, const float* const* u, float* p, void* stream );
+TN_API int tn_gradient_apply_f64( const tn_mesh* mesh, const tn_mesh* mesh_p, int bc_cmb, int bc_surface,
+                                  int apply_mode, int comm_mode, const double* p, double* const* u, void* stream );
+TN_API int tn_gradient_apply_f32( const tn_mesh* mesh, const tn_mesh* mesh_p, int bc_cmb, int bc_surface,
+                                  int apply_mode, int comm_mode, const float* p, float* const* u, void* stream );
+
+/* ---------------------------------------------------------------------------
+ * KMass::apply_impl (fe/wedge/operators/shell/kmass.hpp:66): int k u v, 3x2
+ * Felippa rule, k interpolated at the quadrature points (k == NULL means
+ * k = 1, i.e. Mass, mass.hpp).  mode 0 consistent, 1 diagonal, 2 lumped
+ * diagonal (set_lumped_diagonal, :64). */
+TN_API int tn_kmass_apply_f64( const tn_mesh* mesh, const double* k, int mode, int apply_mode, int comm_mode,
+                               const double* src, double* dst, void* stream );
+TN_API int tn_kmass_apply_f32( const tn_mesh* mesh, const float* k, int mode, int apply_mode, int comm_mode,
+                               const float* src, float* dst, void* stream );
+
+/* ---------------------------------------------------------------------------
+ * Constant grid transfer of `ncomp` fields between `coarse` (level L-1) and
+ * `fine` (level L): ProlongationVecConstant::apply_impl
+ * (fe/wedge/operators/shell/prolongation_constant.hpp:121) and
+ * RestrictionVecConstant::apply_impl (restriction_constant.hpp:161; owned fine
+ * nodes only, followed by the additive coarse halo, Replace mode). */
+TN_API int tn_prolongation_constant_f64( const tn_mesh* fine, const tn_mesh* coarse, int ncomp, int apply_mode,
+                                         const double* const* src, double* const* dst, void* stream );
+TN_API int tn_prolongation_constant_f32( const tn_mesh* fine, const tn_mesh* coarse, int ncomp, int apply_mode,
+                                         const float* const* src, float* const* dst, void* stream );
+TN_API int tn_restriction_constant_f64( const tn_mesh* fine, const tn_mesh* coarse, int ncomp,
+                                        const double* const* src, double* const* dst, void* stream );
+TN_API int tn_restriction_constant_f32( const tn_mesh* fine, const tn_mesh* coarse, int ncomp,
+                                        const float* const* src, float* const* dst, void* stream );
+
+/* ---------------------------------------------------------------------------
  * Krylov vector kernels (kernels/common/grid_operations.hpp).  A vector is
  * `ncomp` scalar fields (1 or 3) of stored-node length.
  *

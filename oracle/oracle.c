@@ -647,3 +647,308 @@ void or_laplace_apply( int L, const double* coords, const double* radii, const d
                 }
     or_halo_sum( L, coords, dst, 1 );
 }
+
+/* ------------------------------------------------------------------------ */
+/* Stokes coupling blocks: Divergence (divergence.hpp:118-322) and Gradient  */
+/* (gradient.hpp:115-325).  Fine (level L) P1 velocity against coarse        */
+/* (level L-1) P1 pressure shape functions evaluated on the fine wedges      */
+/* (shape_coarse, integrands.hpp:266-400), 3x2 Felippa rule.                 */
+/* ------------------------------------------------------------------------ */
+
+/* coarse lateral shape value: coefficient table [node%3][fine lateral idx] = (a, b_xi, c_eta) */
+static const double COARSE_LAT[3][4][3] = {
+    { { 1.0, -0.5, -0.5 }, { 0.5, -0.5, -0.5 }, { 0.5, -0.5, -0.5 }, { 0.0, 0.5, 0.5 } },
+    { { 0.0, 0.5, 0.0 }, { 0.5, 0.5, 0.0 }, { 0.0, 0.5, 0.0 }, { 0.5, -0.5, 0.0 } },
+    { { 0.0, 0.0, 0.5 }, { 0.0, 0.0, 0.5 }, { 0.5, 0.0, 0.5 }, { 0.5, 0.0, -0.5 } } };
+
+static double shape_coarse( int i, int frad, int flat, double xi, double eta, double zeta )
+{
+    const double* c   = COARSE_LAT[i % 3][flat];
+    const double  lat = c[0] + c[1] * xi + c[2] * eta;
+    double        rad;
+    if ( i / 3 == 0 )
+        rad = frad == 0 ? 0.25 * ( 3 - zeta ) : 0.25 * ( 1 - zeta );
+    else
+        rad = frad == 0 ? 0.25 * ( 1 + zeta ) : 0.25 * ( 3 + zeta );
+    return lat * rad;
+}
+
+/* fine_lateral_wedge_idx (kernel_helpers.hpp:601) */
+static int fine_lat_idx( int x, int y, int w )
+{
+    static const int idx[2][2][2] = { { { 0, 1 }, { 2, 3 } }, { { 3, 2 }, { 1, 0 } } };
+    return idx[w][y % 2][x % 2];
+}
+
+/* per fine wedge: B_w[i][d][j] = sum_q w_q (-(J^-T grad N_j)_d N^c_i |det J|) */
+static void stokes_wedge_matrix( const double* p[3], double r1, double r2, int x, int y, int r, int w,
+                                 double B[6][3][6] )
+{
+    memset( B, 0, sizeof( double ) * 6 * 3 * 6 );
+    const int frad = r % 2, flat = fine_lat_idx( x, y, w );
+    for ( int q = 0; q < 6; ++q )
+    {
+        double J[3][3], IT[3][3];
+        wedge_jac( p, r1, r2, QP32[q][0], QP32[q][1], QP32[q][2], J );
+        const double det = det3( J );
+        inv_transposed3( J, det, IT );
+        double g[6][3];
+        for ( int n = 0; n < 6; ++n )
+        {
+            double gr[3];
+            grad_shape_ref( n, QP32[q][0], QP32[q][1], QP32[q][2], gr );
+            for ( int a = 0; a < 3; ++a )
+                g[n][a] = IT[a][0] * gr[0] + IT[a][1] * gr[1] + IT[a][2] * gr[2];
+        }
+        for ( int i = 0; i < 6; ++i )
+        {
+            const double Ni = shape_coarse( i, frad, flat, QP32[q][0], QP32[q][1], QP32[q][2] );
+            for ( int d = 0; d < 3; ++d )
+                for ( int j = 0; j < 6; ++j )
+                    B[i][d][j] += QW32 * ( -g[j][d] * Ni * fabs( det ) );
+        }
+    }
+}
+
+/* velocity node of fine wedge w is on the Dirichlet / free-slip boundary of this cell */
+static int stokes_bc_node( int N, int r, int n, int bc_cmb, int bc_surf, int* kind )
+{
+    *kind = 0;
+    if ( r == 0 && n < 3 )
+        *kind = bc_cmb;
+    else if ( r == N - 1 && n >= 3 )
+        *kind = bc_surf;
+    return *kind;
+}
+
+void or_divergence_apply( int L, const double* coords, const double* radii, const double* coords_c, const double* src,
+                          double* dst, int bc_cmb, int bc_surf )
+{
+    const int    N = 1 << L, n1 = N + 1, nc1 = N / 2 + 1;
+    const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1, nsc = (size_t) NDIAMOND * nc1 * nc1 * nc1;
+    memset( dst, 0, sizeof( double ) * nsc );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const double* p[3];
+                        wedge_lateral_points( n1, coords, d, x, y, w, p );
+                        double B[6][3][6];
+                        stokes_wedge_matrix( p, radii[d * n1 + r], radii[d * n1 + r + 1], x, y, r, w, B );
+                        double u[6][3];
+                        for ( int n = 0; n < 6; ++n )
+                        {
+                            const int    X = x + WNODE[w][n][0], Y = y + WNODE[w][n][1];
+                            const size_t i = node_idx( n1, d, X, Y, r + WNODE[w][n][2] );
+                            for ( int c = 0; c < 3; ++c )
+                                u[n][c] = src[c * ns + i];
+                            int kind;
+                            if ( stokes_bc_node( N, r, n, bc_cmb, bc_surf, &kind ) == 1 )
+                                u[n][0] = u[n][1] = u[n][2] = 0.0;
+                            else if ( kind == 2 )
+                            {
+                                double nn[3];
+                                memcpy( nn, coords + lat_idx( n1, d, X, Y ) * 3, sizeof( nn ) );
+                                normalize3( nn );
+                                fs_project( nn, u[n] );
+                            }
+                        }
+                        for ( int i = 0; i < 6; ++i )
+                        {
+                            double v = 0.0;
+                            for ( int dd = 0; dd < 3; ++dd )
+                                for ( int j = 0; j < 6; ++j )
+                                    v += B[i][dd][j] * u[j][dd];
+                            /* scatter with the coarse wedge-w node map (kernel_helpers.hpp:407-435) */
+                            const int X = x / 2 + WNODE[w][i][0], Y = y / 2 + WNODE[w][i][1], R = r / 2 + WNODE[w][i][2];
+                            dst[node_idx( nc1, d, X, Y, R )] += v;
+                        }
+                    }
+    or_halo_sum( L - 1, coords_c, dst, 1 );
+}
+
+void or_gradient_apply( int L, const double* coords, const double* radii, const double* src, double* dst, int bc_cmb,
+                        int bc_surf )
+{
+    const int    N = 1 << L, n1 = N + 1, nc1 = N / 2 + 1;
+    const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1;
+    memset( dst, 0, sizeof( double ) * 3 * ns );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const double* p[3];
+                        wedge_lateral_points( n1, coords, d, x, y, w, p );
+                        double B[6][3][6];
+                        stokes_wedge_matrix( p, radii[d * n1 + r], radii[d * n1 + r + 1], x, y, r, w, B );
+                        double pc[6];
+                        for ( int i = 0; i < 6; ++i )
+                            pc[i] = src[node_idx( nc1, d, x / 2 + WNODE[w][i][0], y / 2 + WNODE[w][i][1],
+                                                  r / 2 + WNODE[w][i][2] )];
+                        for ( int j = 0; j < 6; ++j )
+                        {
+                            double v[3] = { 0, 0, 0 };
+                            for ( int dd = 0; dd < 3; ++dd )
+                                for ( int i = 0; i < 6; ++i )
+                                    v[dd] += B[i][dd][j] * pc[i];
+                            const int X = x + WNODE[w][j][0], Y = y + WNODE[w][j][1];
+                            int       kind;
+                            if ( stokes_bc_node( N, r, j, bc_cmb, bc_surf, &kind ) == 1 )
+                                continue;
+                            if ( kind == 2 )
+                            {
+                                double nn[3];
+                                memcpy( nn, coords + lat_idx( n1, d, X, Y ) * 3, sizeof( nn ) );
+                                normalize3( nn );
+                                fs_project( nn, v );
+                            }
+                            const size_t i = node_idx( n1, d, X, Y, r + WNODE[w][j][2] );
+                            for ( int c = 0; c < 3; ++c )
+                                dst[c * ns + i] += v[c];
+                        }
+                    }
+    or_halo_sum( L, coords, dst, 3 );
+}
+
+/* ------------------------------------------------------------------------ */
+/* Constant grid transfer (fe/wedge/shell/grid_transfer_constant.hpp:6-82,  */
+/* prolongation_constant.hpp:103-190, restriction_constant.hpp:134-248).    */
+/* ------------------------------------------------------------------------ */
+
+/* prolongation_constant_weight: 1 / 1/2 on the coarse shell, 1/2 / 1/4 one fine shell off */
+static double prolong_weight( int xf, int yf, int rf, int xc, int yc, int rc )
+{
+    const int dx = xf - 2 * xc, dy = yf - 2 * yc, dr = rf - 2 * rc;
+    double    lat = 0.0;
+    if ( dx == 0 && dy == 0 )
+        lat = 1.0;
+    else if ( ( dy == 0 && ( dx == 1 || dx == -1 ) ) || ( dx == 0 && ( dy == 1 || dy == -1 ) ) ||
+              ( dx == -1 && dy == 1 ) || ( dx == 1 && dy == -1 ) )
+        lat = 0.5;
+    if ( dr == 0 )
+        return lat;
+    if ( dr == 1 || dr == -1 )
+        return 0.5 * lat;
+    return 0.0;
+}
+
+static const int STENCIL7[7][2] = { { -1, 0 }, { -1, 1 }, { 0, 1 }, { 1, 0 }, { 1, -1 }, { 0, -1 }, { 0, 0 } };
+
+/* coarse level Lc -> fine level Lc+1, ncomp fields, Replace mode, no communication */
+void or_prolongation_constant( int Lc, int ncomp, const double* src, double* dst )
+{
+    const int    nc1 = ( 1 << Lc ) + 1, nf1 = ( 1 << ( Lc + 1 ) ) + 1;
+    const size_t nsc = (size_t) NDIAMOND * nc1 * nc1 * nc1, nsf = (size_t) NDIAMOND * nf1 * nf1 * nf1;
+    memset( dst, 0, sizeof( double ) * nsf * ncomp );
+    for ( int c = 0; c < ncomp; ++c )
+        for ( int d = 0; d < NDIAMOND; ++d )
+            for ( int x = 0; x < nc1; ++x )
+                for ( int y = 0; y < nc1; ++y )
+                    for ( int r = 0; r < nc1; ++r )
+                        for ( int dr = -1; dr <= 1; ++dr )
+                            for ( int s = 0; s < 7; ++s )
+                            {
+                                const int xf = 2 * x + STENCIL7[s][0], yf = 2 * y + STENCIL7[s][1], rf = 2 * r + dr;
+                                if ( xf < 0 || xf >= nf1 || yf < 0 || yf >= nf1 || rf < 0 || rf >= nf1 )
+                                    continue;
+                                dst[c * nsf + node_idx( nf1, d, xf, yf, rf )] +=
+                                    prolong_weight( xf, yf, rf, x, y, r ) * src[c * nsc + node_idx( nc1, d, x, y, r )];
+                            }
+}
+
+/* fine level Lf -> coarse Lf-1: sum of weighted OWNED fine values, then coarse halo */
+void or_restriction_constant( int Lf, int ncomp, const double* coords_c, const uint8_t* omask_f, const double* src,
+                              double* dst )
+{
+    const int    nf1 = ( 1 << Lf ) + 1, nc1 = ( 1 << ( Lf - 1 ) ) + 1;
+    const size_t nsc = (size_t) NDIAMOND * nc1 * nc1 * nc1, nsf = (size_t) NDIAMOND * nf1 * nf1 * nf1;
+    memset( dst, 0, sizeof( double ) * nsc * ncomp );
+    for ( int c = 0; c < ncomp; ++c )
+        for ( int d = 0; d < NDIAMOND; ++d )
+            for ( int x = 0; x < nc1; ++x )
+                for ( int y = 0; y < nc1; ++y )
+                    for ( int r = 0; r < nc1; ++r )
+                    {
+                        double v = 0.0;
+                        for ( int dr = -1; dr <= 1; ++dr )
+                            for ( int s = 0; s < 7; ++s )
+                            {
+                                const int xf = 2 * x + STENCIL7[s][0], yf = 2 * y + STENCIL7[s][1], rf = 2 * r + dr;
+                                if ( xf < 0 || xf >= nf1 || yf < 0 || yf >= nf1 || rf < 0 || rf >= nf1 )
+                                    continue;
+                                const size_t i = node_idx( nf1, d, xf, yf, rf );
+                                v += prolong_weight( xf, yf, rf, x, y, r ) * ( omask_f[i] ? 1.0 : 0.0 ) * src[c * nsf + i];
+                            }
+                        dst[c * nsc + node_idx( nc1, d, x, y, r )] = v;
+                    }
+    or_halo_sum( Lf - 1, coords_c, dst, ncomp );
+}
+
+/* ------------------------------------------------------------------------ */
+/* KMass (fe/wedge/operators/shell/kmass.hpp): int k u v, 3x2 rule, k        */
+/* interpolated at the quadrature points; mode 0 full, 1 diagonal, 2 lumped. */
+/* ------------------------------------------------------------------------ */
+void or_kmass_apply( int L, const double* coords, const double* radii, const double* k, const double* src, double* dst,
+                     int mode )
+{
+    const int    N = 1 << L, n1 = N + 1;
+    const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1;
+    memset( dst, 0, sizeof( double ) * ns );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const double* p[3];
+                        wedge_lateral_points( n1, coords, d, x, y, w, p );
+                        size_t idx[6];
+                        for ( int n = 0; n < 6; ++n )
+                            idx[n] = node_idx( n1, d, x + WNODE[w][n][0], y + WNODE[w][n][1], r + WNODE[w][n][2] );
+                        const double r1 = radii[d * n1 + r], r2 = radii[d * n1 + r + 1];
+                        double       A[6][6] = { { 0 } };
+                        for ( int q = 0; q < 6; ++q )
+                        {
+                            const double xi = QP32[q][0], eta = QP32[q][1], zeta = QP32[q][2];
+                            double       M[3][3];
+                            for ( int a = 0; a < 3; ++a )
+                            {
+                                M[a][0] = p[1][a] - p[0][a];
+                                M[a][1] = p[2][a] - p[0][a];
+                                M[a][2] = ( 1 - xi - eta ) * p[0][a] + xi * p[1][a] + eta * p[2][a];
+                            }
+                            const double rq = r1 + 0.5 * ( r2 - r1 ) * ( 1 + zeta ), gr = 0.5 * ( r2 - r1 );
+                            double       N6[6];
+                            const double lat[3] = { 1 - xi - eta, xi, eta };
+                            double       kq     = 0.0;
+                            for ( int n = 0; n < 6; ++n )
+                            {
+                                N6[n] = lat[n % 3] * ( n < 3 ? 0.5 * ( 1 - zeta ) : 0.5 * ( 1 + zeta ) );
+                                kq += N6[n] * k[idx[n]];
+                            }
+                            const double f = QW32 * kq * rq * rq * gr * fabs( det3( M ) );
+                            for ( int i = 0; i < 6; ++i )
+                                for ( int j = 0; j < 6; ++j )
+                                    A[i][j] += f * N6[i] * N6[j];
+                        }
+                        for ( int i = 0; i < 6; ++i )
+                        {
+                            double v = 0.0;
+                            for ( int j = 0; j < 6; ++j )
+                            {
+                                if ( mode == 0 )
+                                    v += A[i][j] * src[idx[j]];
+                                else if ( mode == 1 && i == j )
+                                    v += A[i][j] * src[idx[j]];
+                                else if ( mode == 2 )
+                                    v += A[i][j] * src[idx[i]];
+                            }
+                            dst[idx[i]] += v;
+                        }
+                    }
+    or_halo_sum( L, coords, dst, 1 );
+}

@@ -40,6 +40,21 @@ void or_kerngen_apply( int L, const double* coords, const double* radii, const d
 void or_laplace_apply( int L, const double* coords, const double* radii, const double* src, double* dst,
                        int treat_boundary, int diag );
 
+/* Stokes coupling blocks (fine velocity at level L, coarse pressure at L-1) */
+void or_divergence_apply( int L, const double* coords, const double* radii, const double* coords_coarse,
+                          const double* src_u, double* dst_p, int bc_cmb, int bc_surf );
+void or_gradient_apply( int L, const double* coords, const double* radii, const double* src_p, double* dst_u,
+                        int bc_cmb, int bc_surf );
+
+/* KMass: mode 0 consistent, 1 diagonal, 2 lumped diagonal */
+void or_kmass_apply( int L, const double* coords, const double* radii, const double* k, const double* src, double* dst,
+                     int mode );
+
+/* constant grid transfer of ncomp fields between levels Lc and Lc+1 */
+void or_prolongation_constant( int Lc, int ncomp, const double* src_coarse, double* dst_fine );
+void or_restriction_constant( int Lf, int ncomp, const double* coords_coarse, const uint8_t* omask_fine,
+                              const double* src_fine, double* dst_coarse );
+
 /* Krylov vector kernels */
 double or_masked_dot( size_t n, const double* a, const double* b, const uint8_t* omask );
 

@@ -15,6 +15,10 @@
 //   mesh    L rmin rmax OUT               coords/radii/boundary+ownership masks
 //   kerngen L rmin rmax bcc bcs diag DIR  EpsilonDivDivKerngen<double> apply
 //   laplace L rmin rmax treat diag DIR    Laplace<double> apply
+//   divergence L rmin rmax bcc bcs DIR    Divergence<double>: fine velocity -> coarse pressure
+//   gradient   L rmin rmax bcc bcs DIR    Gradient<double>: coarse pressure -> fine velocity
+//   prolong / restrict Lf rmin rmax DIR    constant vector transfer between Lf-1 and Lf
+//   kmass   L rmin rmax mode DIR          KMass<double> (0 full, 1 diagonal, 2 lumped)
 //   time_kerngen L rmin rmax bcc bcs reps prints seconds per apply (CPU baseline)
 #include <chrono>
 #include <cstdio>
@@ -25,7 +29,12 @@
 
 #include "communication/shell/communication.hpp"
 #include "fe/wedge/operators/shell/epsilon_divdiv_kerngen.hpp"
+#include "fe/wedge/operators/shell/divergence.hpp"
+#include "fe/wedge/operators/shell/gradient.hpp"
+#include "fe/wedge/operators/shell/kmass.hpp"
 #include "fe/wedge/operators/shell/laplace.hpp"
+#include "fe/wedge/operators/shell/prolongation_constant.hpp"
+#include "fe/wedge/operators/shell/restriction_constant.hpp"
 #include "grid/bit_masks.hpp"
 #include "grid/shell/bit_masks.hpp"
 #include "grid/shell/spherical_shell.hpp"
@@ -190,6 +199,66 @@ int cmd_laplace( int L, double rmin, double rmax, int treat, int diag, const std
     return 0;
 }
 
+int cmd_stokes_block( bool div, int L, double rmin, double rmax, int bcc, int bcs, const std::string& dir )
+{
+    Setup              f( L, rmin, rmax ), c( L - 1, rmin, rmax );
+    BoundaryConditions b = { { ShellBoundaryFlag::CMB, bc_of( bcc ) }, { ShellBoundaryFlag::SURFACE, bc_of( bcs ) } };
+    linalg::VectorQ1Vec< double >    u( "u", f.domain, f.omask );
+    linalg::VectorQ1Scalar< double > p( "p", c.domain, c.omask );
+    if ( div )
+    {
+        load_vec( u, dir + "/src.bin", f.nodes );
+        fe::wedge::operators::shell::Divergence< double > op( f.domain, c.domain, f.coords, f.radii, f.bmask, b );
+        linalg::apply( op, u, p );
+        auto out = view_to_host( p.grid_data() );
+        write_file( dir + "/dst.bin", out.data(), out.size() );
+    }
+    else
+    {
+        view_from_host( p.grid_data(), read_file< double >( dir + "/src.bin", c.nodes ).data() );
+        fe::wedge::operators::shell::Gradient< double > op( f.domain, c.domain, f.coords, f.radii, f.bmask, b );
+        linalg::apply( op, p, u );
+        save_vec( u, dir + "/dst.bin", f.nodes );
+    }
+    return 0;
+}
+
+int cmd_transfer( bool prolong, int Lf, double rmin, double rmax, const std::string& dir )
+{
+    Setup                         f( Lf, rmin, rmax ), c( Lf - 1, rmin, rmax );
+    linalg::VectorQ1Vec< double > uf( "uf", f.domain, f.omask ), uc( "uc", c.domain, c.omask );
+    if ( prolong )
+    {
+        load_vec( uc, dir + "/src.bin", c.nodes );
+        fe::wedge::operators::shell::ProlongationVecConstant< double > P;
+        linalg::apply( P, uc, uf );
+        save_vec( uf, dir + "/dst.bin", f.nodes );
+    }
+    else
+    {
+        load_vec( uf, dir + "/src.bin", f.nodes );
+        fe::wedge::operators::shell::RestrictionVecConstant< double > R( c.domain );
+        linalg::apply( R, uf, uc );
+        save_vec( uc, dir + "/dst.bin", c.nodes );
+    }
+    return 0;
+}
+
+int cmd_kmass( int L, double rmin, double rmax, int mode, const std::string& dir )
+{
+    Setup                            s( L, rmin, rmax );
+    linalg::VectorQ1Scalar< double > k( "k", s.domain, s.omask ), src( "src", s.domain, s.omask ),
+        dst( "dst", s.domain, s.omask );
+    view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", s.nodes ).data() );
+    view_from_host( src.grid_data(), read_file< double >( dir + "/src.bin", s.nodes ).data() );
+    fe::wedge::operators::shell::KMass< double > op( s.domain, s.coords, s.radii, k.grid_data(), mode == 1 );
+    op.set_lumped_diagonal( mode == 2 );
+    linalg::apply( op, src, dst );
+    auto out = view_to_host( dst.grid_data() );
+    write_file( dir + "/dst.bin", out.data(), out.size() );
+    return 0;
+}
+
 } // namespace
 
 int main( int argc, char** argv )
@@ -209,6 +278,12 @@ int main( int argc, char** argv )
         return cmd_kerngen( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( cmd == "time_kerngen" && argc == 8 )
         return cmd_time_kerngen( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ) );
+    if ( ( cmd == "divergence" || cmd == "gradient" ) && argc == 8 )
+        return cmd_stokes_block( cmd == "divergence", I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
+    if ( ( cmd == "prolong" || cmd == "restrict" ) && argc == 6 )
+        return cmd_transfer( cmd == "prolong", I( 2 ), D( 3 ), D( 4 ), argv[5] );
+    if ( cmd == "kmass" && argc == 7 )
+        return cmd_kmass( I( 2 ), D( 3 ), D( 4 ), I( 5 ), argv[6] );
     if ( cmd == "laplace" && argc == 8 )
         return cmd_laplace( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     std::fprintf( stderr, "ref_dump: bad command line\n" );

@@ -45,6 +45,16 @@ _SIGS = {
     "tn_epsdivdiv_apply_f32": (c_int, [c_void_p, P(EpsDivDivParams), c_void_p, P(c_void_p), P(c_void_p), c_void_p]),
     "tn_laplace_apply_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "tn_laplace_apply_f32": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "tn_divergence_apply_f64": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, P(c_void_p), c_void_p, c_void_p]),
+    "tn_divergence_apply_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, P(c_void_p), c_void_p, c_void_p]),
+    "tn_gradient_apply_f64": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p, P(c_void_p), c_void_p]),
+    "tn_gradient_apply_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p, P(c_void_p), c_void_p]),
+    "tn_prolongation_constant_f64": (c_int, [c_void_p, c_void_p, c_int, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_prolongation_constant_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_restriction_constant_f64": (c_int, [c_void_p, c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_restriction_constant_f32": (c_int, [c_void_p, c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_kmass_apply_f64": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "tn_kmass_apply_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "tn_vec_lincomb_f64": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p), c_void_p]),
     "tn_vec_lincomb_f32": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p), c_void_p]),
     "tn_vec_dot_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_double), c_void_p]),

@@ -613,7 +613,7 @@ __global__ void __launch_bounds__( 128 ) kerngen_cell_kernel( CellParams< T > P 
 constexpr int kBndNodes = 32; // boundary nodes per block (6 wedge threads each)
 
 template < typename T >
-__global__ void __launch_bounds__( 6 * kBndNodes, 4 ) kerngen_boundary_kernel( CellParams< T > P, int sides )
+__global__ void __launch_bounds__( 6 * kBndNodes ) kerngen_boundary_kernel( CellParams< T > P, int sides )
 {
     __shared__ T sh[6][7][kBndNodes]; // per wedge: boundary-level (3), interior-level (3), Ann
     const int       N = P.N, n1 = P.n1;

@@ -1,0 +1,178 @@
+// Constant grid transfer between levels L-1 (coarse) and L (fine)
+// (fe/wedge/shell/grid_transfer_constant.hpp, prolongation_constant.hpp,
+// restriction_constant.hpp).
+//
+// The reference scatters from each coarse node into its 21-point fine
+// stencil with atomics.  Here both directions are gathers without atomics:
+//  * prolongation: each fine node reads its (at most 2 x 2) coarse parents —
+//    1 / 1/2 laterally (edge and anti-diagonal midpoints), 1 / 1/2 radially;
+//  * restriction: each coarse node sums its 21-point stencil of OWNED fine
+//    values with the same weights, then the coarse halo adds duplicates.
+#include "common.cuh"
+
+namespace tn {
+
+template < typename T >
+int halo_sum( const tn_mesh* m, T* const* fields, int nfields, cudaStream_t st );
+
+namespace {
+
+template < typename T >
+__global__ void prolong_constant_kernel( int nf1, int nc1, Ptr3< const T > src, Ptr3< T > dst, int ncomp, int add )
+{
+    const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    const long long total = (long long) kDiamonds * nf1 * nf1 * nf1;
+    if ( t >= total )
+        return;
+    const int rf = int( t % nf1 ), yf = int( ( t / nf1 ) % nf1 ), xf = int( ( t / ( (long long) nf1 * nf1 ) ) % nf1 );
+    const int d  = int( t / ( (long long) nf1 * nf1 * nf1 ) );
+    // lateral parents
+    int lx[2], ly[2], nl;
+    if ( !( xf & 1 ) && !( yf & 1 ) )
+        lx[0] = xf / 2, ly[0] = yf / 2, nl = 1;
+    else if ( ( xf & 1 ) && !( yf & 1 ) )
+        lx[0] = ( xf - 1 ) / 2, ly[0] = yf / 2, lx[1] = ( xf + 1 ) / 2, ly[1] = yf / 2, nl = 2;
+    else if ( !( xf & 1 ) && ( yf & 1 ) )
+        lx[0] = xf / 2, ly[0] = ( yf - 1 ) / 2, lx[1] = xf / 2, ly[1] = ( yf + 1 ) / 2, nl = 2;
+    else
+        lx[0] = ( xf + 1 ) / 2, ly[0] = ( yf - 1 ) / 2, lx[1] = ( xf - 1 ) / 2, ly[1] = ( yf + 1 ) / 2, nl = 2;
+    const int r0 = rf / 2, r1 = ( rf + 1 ) / 2;
+    const T   wl = nl == 1 ? T( 1 ) : T( 0.5 );
+    const T   wr = r0 == r1 ? T( 1 ) : T( 0.5 );
+    for ( int c = 0; c < ncomp; ++c )
+    {
+        T v = 0;
+        for ( int a = 0; a < nl; ++a )
+        {
+            const T* col = src.p[c] + ( ( size_t( d ) * nc1 + lx[a] ) * nc1 + ly[a] ) * nc1;
+            v += wl * ( r0 == r1 ? wr * col[r0] : wr * col[r0] + wr * col[r1] );
+        }
+        T* o = dst.p[c] + t;
+        *o   = add ? *o + v : v;
+    }
+}
+
+template < typename T >
+__global__ void restrict_constant_kernel( int nf1, int nc1, const uint8_t* __restrict__ owned_f, Ptr3< const T > src,
+                                          Ptr3< T > dst, int ncomp, int add )
+{
+    const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    const long long total = (long long) kDiamonds * nc1 * nc1 * nc1;
+    if ( t >= total )
+        return;
+    const int rc = int( t % nc1 ), yc = int( ( t / nc1 ) % nc1 ), xc = int( ( t / ( (long long) nc1 * nc1 ) ) % nc1 );
+    const int d  = int( t / ( (long long) nc1 * nc1 * nc1 ) );
+    constexpr int off[7][2] = { { -1, 0 }, { -1, 1 }, { 0, 1 }, { 1, 0 }, { 1, -1 }, { 0, -1 }, { 0, 0 } };
+    T             v[3]      = { 0, 0, 0 };
+    for ( int s = 0; s < 7; ++s )
+    {
+        const int xf = 2 * xc + off[s][0], yf = 2 * yc + off[s][1];
+        if ( xf < 0 || xf >= nf1 || yf < 0 || yf >= nf1 )
+            continue;
+        const size_t lat = ( size_t( d ) * nf1 + xf ) * nf1 + yf;
+        if ( !owned_f[lat] )
+            continue;
+        const T wl = s == 6 ? T( 1 ) : T( 0.5 );
+        for ( int dr = -1; dr <= 1; ++dr )
+        {
+            const int rf = 2 * rc + dr;
+            if ( rf < 0 || rf >= nf1 )
+                continue;
+            const T w = dr == 0 ? wl : T( 0.5 ) * wl;
+            for ( int c = 0; c < ncomp; ++c )
+                v[c] += w * src.p[c][lat * nf1 + rf];
+        }
+    }
+    for ( int c = 0; c < ncomp; ++c )
+    {
+        T* o = dst.p[c] + t;
+        *o   = add ? *o + v[c] : v[c];
+    }
+}
+
+int check_levels( const tn_mesh* f, const tn_mesh* c, int ncomp )
+{
+    TN_CHECK_ARG( f && c, "transfer: null mesh" );
+    TN_CHECK_ARG( c->level == f->level - 1, "transfer: coarse mesh must be one level below the fine mesh" );
+    TN_CHECK_ARG( ncomp >= 1 && ncomp <= 3, "transfer: ncomp must be 1..3" );
+    return TN_OK;
+}
+
+}  // namespace
+
+template < typename T >
+int prolong_constant( const tn_mesh* f, const tn_mesh* c, int ncomp, int apply_mode, const T* const* src, T* const* dst,
+                      cudaStream_t st )
+{
+    int rc;
+    if ( ( rc = check_levels( f, c, ncomp ) ) )
+        return rc;
+    Ptr3< const T > s{};
+    Ptr3< T >       o{};
+    for ( int i = 0; i < ncomp; ++i )
+    {
+        TN_CHECK_ARG( src[i] && dst[i], "prolongation: null component" );
+        s.p[i] = src[i], o.p[i] = dst[i];
+    }
+    const long long n = (long long) f->ns;
+    prolong_constant_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( f->n1, c->n1, s, o, ncomp,
+                                                                                 apply_mode == TN_APPLY_ADD );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+template < typename T >
+int restrict_constant( const tn_mesh* f, const tn_mesh* c, int ncomp, int apply_mode, const T* const* src,
+                       T* const* dst, cudaStream_t st )
+{
+    int rc;
+    if ( ( rc = check_levels( f, c, ncomp ) ) )
+        return rc;
+    TN_CHECK_ARG( apply_mode == TN_APPLY_REPLACE, "restriction: only Replace mode (the halo sums the whole field)" );
+    Ptr3< const T > s{};
+    Ptr3< T >       o{};
+    for ( int i = 0; i < ncomp; ++i )
+    {
+        TN_CHECK_ARG( src[i] && dst[i], "restriction: null component" );
+        s.p[i] = src[i], o.p[i] = dst[i];
+    }
+    const long long n = (long long) c->ns;
+    restrict_constant_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( f->n1, c->n1, f->d_lat_owned, s, o,
+                                                                                  ncomp, 0 );
+    TN_LAUNCH_CHECK();
+    return halo_sum< T >( c, dst, ncomp, st );
+}
+
+template int prolong_constant< double >( const tn_mesh*, const tn_mesh*, int, int, const double* const*,
+                                         double* const*, cudaStream_t );
+template int prolong_constant< float >( const tn_mesh*, const tn_mesh*, int, int, const float* const*, float* const*,
+                                        cudaStream_t );
+template int restrict_constant< double >( const tn_mesh*, const tn_mesh*, int, int, const double* const*,
+                                          double* const*, cudaStream_t );
+template int restrict_constant< float >( const tn_mesh*, const tn_mesh*, int, int, const float* const*, float* const*,
+                                         cudaStream_t );
+
+}  // namespace tn
+
+using namespace tn;
+
+extern "C" int tn_prolongation_constant_f64( const tn_mesh* f, const tn_mesh* c, int ncomp, int am,
+                                             const double* const* src, double* const* dst, void* s )
+{
+    return prolong_constant< double >( f, c, ncomp, am, src, dst, as_stream( s ) );
+}
+extern "C" int tn_prolongation_constant_f32( const tn_mesh* f, const tn_mesh* c, int ncomp, int am,
+                                             const float* const* src, float* const* dst, void* s )
+{
+    return prolong_constant< float >( f, c, ncomp, am, src, dst, as_stream( s ) );
+}
+extern "C" int tn_restriction_constant_f64( const tn_mesh* f, const tn_mesh* c, int ncomp, const double* const* src,
+                                            double* const* dst, void* s )
+{
+    return restrict_constant< double >( f, c, ncomp, TN_APPLY_REPLACE, src, dst, as_stream( s ) );
+}
+extern "C" int tn_restriction_constant_f32( const tn_mesh* f, const tn_mesh* c, int ncomp, const float* const* src,
+                                            float* const* dst, void* s )
+{
+    return restrict_constant< float >( f, c, ncomp, TN_APPLY_REPLACE, src, dst, as_stream( s ) );
+}

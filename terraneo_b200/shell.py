@@ -172,6 +172,75 @@ class Laplace:
                   ctypes.c_void_p(dst.data.data_ptr()), _stream()), "laplace_apply")
 
 
+class KMass:
+    """KMass (fe/wedge/operators/shell/kmass.hpp:17); k=None gives Mass. mode: 0 full, 1 diagonal, 2 lumped."""
+
+    def __init__(self, mesh, k=None, mode=0, apply_mode=C.APPLY_REPLACE, comm_mode=C.COMM_ADDITIVE):
+        self.mesh, self.k, self.mode, self.am, self.cm = mesh, k, mode, apply_mode, comm_mode
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_kmass_apply_{src.tag}")
+        kp = ctypes.c_void_p(self.k.data.data_ptr()) if self.k is not None else ctypes.c_void_p(0)
+        C.check(f(self.mesh.handle, kp, self.mode, self.am, self.cm, ctypes.c_void_p(src.data.data_ptr()),
+                  ctypes.c_void_p(dst.data.data_ptr()), _stream()), "kmass_apply")
+
+
+class Divergence:
+    """Divergence (fe/wedge/operators/shell/divergence.hpp:30): fine velocity -> coarse pressure."""
+
+    def __init__(self, mesh_u, mesh_p, bc_cmb, bc_surface, apply_mode=C.APPLY_REPLACE, comm_mode=C.COMM_ADDITIVE):
+        self.mu, self.mp, self.bc = mesh_u, mesh_p, (bc_cmb, bc_surface)
+        self.am, self.cm = apply_mode, comm_mode
+
+    def set_operator_apply_and_communication_modes(self, apply_mode, comm_mode):
+        self.am, self.cm = apply_mode, comm_mode
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_divergence_apply_{src.tag}")
+        C.check(f(self.mu.handle, self.mp.handle, self.bc[0], self.bc[1], self.am, self.cm, src.comp_ptrs(),
+                  ctypes.c_void_p(dst.data.data_ptr()), _stream()), "divergence_apply")
+
+
+class Gradient:
+    """Gradient (fe/wedge/operators/shell/gradient.hpp:28): coarse pressure -> fine velocity."""
+
+    def __init__(self, mesh_u, mesh_p, bc_cmb, bc_surface, apply_mode=C.APPLY_REPLACE, comm_mode=C.COMM_ADDITIVE):
+        self.mu, self.mp, self.bc = mesh_u, mesh_p, (bc_cmb, bc_surface)
+        self.am, self.cm = apply_mode, comm_mode
+
+    def set_operator_apply_and_communication_modes(self, apply_mode, comm_mode):
+        self.am, self.cm = apply_mode, comm_mode
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_gradient_apply_{src.tag}")
+        C.check(f(self.mu.handle, self.mp.handle, self.bc[0], self.bc[1], self.am, self.cm,
+                  ctypes.c_void_p(src.data.data_ptr()), dst.comp_ptrs(), _stream()), "gradient_apply")
+
+
+class ProlongationVecConstant:
+    """ProlongationVecConstant (fe/wedge/operators/shell/prolongation_constant.hpp:103): coarse -> fine."""
+
+    def __init__(self, mesh_fine, mesh_coarse, apply_mode=C.APPLY_REPLACE):
+        self.mf, self.mc, self.am = mesh_fine, mesh_coarse, apply_mode
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_prolongation_constant_{src.tag}")
+        C.check(f(self.mf.handle, self.mc.handle, src.ncomp, self.am, src.comp_ptrs(), dst.comp_ptrs(), _stream()),
+                "prolongation")
+
+
+class RestrictionVecConstant:
+    """RestrictionVecConstant (fe/wedge/operators/shell/restriction_constant.hpp:134): fine -> coarse."""
+
+    def __init__(self, mesh_fine, mesh_coarse):
+        self.mf, self.mc = mesh_fine, mesh_coarse
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_restriction_constant_{src.tag}")
+        C.check(f(self.mf.handle, self.mc.handle, src.ncomp, src.comp_ptrs(), dst.comp_ptrs(), _stream()),
+                "restriction")
+
+
 def apply(op, src, dst):
     """linalg::apply (linalg/operator.hpp:156)."""
     op.apply_impl(src, dst)

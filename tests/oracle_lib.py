@@ -33,6 +33,11 @@ def lib():
         L.or_halo_sum.argtypes = [ctypes.c_int, _D, _D, ctypes.c_int]
         L.or_kerngen_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.or_laplace_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
+        L.or_divergence_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
+        L.or_gradient_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
+        L.or_prolongation_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D]
+        L.or_restriction_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _U8, _D, _D]
+        L.or_kmass_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int]
         L.or_masked_dot.restype = ctypes.c_double
         L.or_masked_dot.argtypes = [ctypes.c_size_t, _D, _D, _U8]
         _lib = L
@@ -91,6 +96,38 @@ class Mesh:
         src = np.ascontiguousarray(src, dtype=np.float64)
         lib().or_laplace_apply(self.L, _p(self.coords), _p(self.radii), _p(src), _p(dst),
                                int(treat_boundary), int(diag))
+        return dst
+
+    def divergence(self, coarse, u, bc_cmb, bc_surf):
+        dst = np.zeros(coarse.shape)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        lib().or_divergence_apply(self.L, _p(self.coords), _p(self.radii), _p(coarse.coords), _p(u), _p(dst),
+                                  bc_cmb, bc_surf)
+        return dst
+
+    def gradient(self, coarse, p, bc_cmb, bc_surf):
+        dst = np.zeros((3,) + self.shape)
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        lib().or_gradient_apply(self.L, _p(self.coords), _p(self.radii), _p(p), _p(dst), bc_cmb, bc_surf)
+        return dst
+
+    def prolong(self, coarse, src, ncomp=3):
+        """constant prolongation from `coarse` (level L-1) to this mesh"""
+        dst = np.zeros((ncomp,) + self.shape)
+        lib().or_prolongation_constant(coarse.L, ncomp, _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst))
+        return dst
+
+    def restrict(self, coarse, src, ncomp=3):
+        """constant restriction from this mesh to `coarse` (level L-1)"""
+        dst = np.zeros((ncomp,) + coarse.shape)
+        lib().or_restriction_constant(self.L, ncomp, _p(coarse.coords), _p(np.ascontiguousarray(self.omask)),
+                                      _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst))
+        return dst
+
+    def kmass(self, k, src, mode=0):
+        dst = np.zeros(self.shape)
+        lib().or_kmass_apply(self.L, _p(self.coords), _p(self.radii), _p(np.ascontiguousarray(k, dtype=np.float64)),
+                             _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst), mode)
         return dst
 
     def dot(self, a, b):
