@@ -149,6 +149,15 @@ TN_API int tn_restriction_constant_f64( const tn_mesh* fine, const tn_mesh* coar
 TN_API int tn_restriction_constant_f32( const tn_mesh* fine, const tn_mesh* coarse, int ncomp,
                                         const float* const* src, float* const* dst, void* stream );
 
+/* Injection coarse(X,Y,R) = fine(2X,2Y,2R) of `ncomp` fields (coefficient
+ * fields on coarser multigrid levels). */
+TN_API int tn_injection_f64( const tn_mesh* fine, const tn_mesh* coarse, int ncomp, const double* const* src,
+                             double* const* dst, void* stream );
+/* In-place tangential projection of a 3-vector field at the CMB (cmb != 0)
+ * and SURFACE (surface != 0) nodes: strong_algebraic_freeslip_enforcement_in_place
+ * (fe/strong_algebraic_freeslip_enforcement.hpp:23). */
+TN_API int tn_freeslip_project_f64( const tn_mesh* mesh, double* const* y, int cmb, int surface, void* stream );
+
 /* ---------------------------------------------------------------------------
  * Krylov vector kernels (kernels/common/grid_operations.hpp).  A vector is
  * `ncomp` scalar fields (1 or 3) of stored-node length.
@@ -174,8 +183,72 @@ TN_API int tn_vec_mult_f32( const tn_mesh* mesh, int ncomp, float* const* y, con
 TN_API int tn_vec_max_abs_f64( const tn_mesh* mesh, int ncomp, const double* const* x, double* result, void* stream );
 TN_API int tn_vec_has_nan_or_inf_f64( const tn_mesh* mesh, int ncomp, const double* const* x, int* result, void* stream );
 TN_API int tn_vec_has_nan_or_inf_f32( const tn_mesh* mesh, int ncomp, const float* const* x, int* result, void* stream );
+/* randomize (grid_operations.hpp:759) made deterministic: uniform [-1, 1)
+ * from a counter-based hash of (seed, component, index). */
+TN_API int tn_vec_randomize_f64( const tn_mesh* mesh, int ncomp, double* const* y, unsigned long long seed,
+                                 void* stream );
+TN_API int tn_vec_randomize_f32( const tn_mesh* mesh, int ncomp, float* const* y, unsigned long long seed, void* stream );
 TN_API int tn_vec_cast_f64_to_f32( const tn_mesh* mesh, int ncomp, float* const* y, const double* const* x, void* stream );
 TN_API int tn_vec_cast_f32_to_f64( const tn_mesh* mesh, int ncomp, double* const* y, const float* const* x, void* stream );
+
+/* ---------------------------------------------------------------------------
+ * Solver drivers.
+ *
+ * PCG (linalg/solvers/pcg.hpp:78) without preconditioner on the scalar
+ * Laplace with homogeneous Dirichlet elimination on both radii
+ * (tests/test_laplace_cg.cpp:115-200 composition): solves A x = b from the
+ * initial guess in x; stops at ||r|| / ||r0|| <= relative_tolerance or
+ * ||r|| < absolute_tolerance. */
+TN_API int tn_laplace_pcg_solve_f64( const tn_mesh* mesh, const double* b, double* x, int max_iterations,
+                                     double relative_tolerance, double absolute_tolerance, int* iterations,
+                                     double* relative_residual );
+
+/* Stokes solver composed as apps/mantlecirculation/mantlecirculation.cpp:486-735:
+ * FGMRES(restart) (fgmres.hpp:108) on EpsDivDivStokes [A B^T; B 0]
+ * (epsilon_divdiv_stokes.hpp:55), BlockTriangularPreconditioner2x2
+ * (block_preconditioner_2x2.hpp:205) with a multigrid V-cycle (multigrid.hpp:119,
+ * Chebyshev smoothing chebyshev.hpp:100, constant transfers, PCG coarse solve)
+ * on A and the inverse lumped KMass(1/eta) (kmass.hpp) on the Schur block.
+ * Velocity on `level`, pressure on level-1; the multigrid spans mg_levels
+ * levels ending at `level`, coarser viscous operators re-discretised with the
+ * viscosity injected from `level`.  mg_fp32 != 0 runs the V-cycle in FP32
+ * (FP32 operators, smoothers, transfers) inside the FP64 FGMRES; the outer
+ * residual, dots, Schur diagonal and coarsest PCG are FP64. */
+typedef struct
+{
+    int    level;
+    int    mg_levels;
+    int    bc_cmb;
+    int    bc_surface;
+    int    mg_fp32;
+    int    chebyshev_order;
+    int    smoothing_steps;
+    int    power_iterations;
+    int    vcycles;
+    int    coarse_max_iterations;
+    double coarse_relative_tolerance;
+    int    restart;
+    int    max_iterations;
+    double relative_tolerance;
+    double absolute_tolerance;
+} tn_stokes_params;
+
+typedef struct tn_stokes_solver tn_stokes_solver;
+
+/* `viscosity`: device FP64 field on `level` (copied) */
+TN_API int tn_stokes_solver_create( const tn_stokes_params* params, double r_min, double r_max,
+                                    const double* viscosity, tn_stokes_solver** out );
+/* f_u (3 fields, level) / f_p (level-1): right-hand side; x_u / x_p: initial
+ * guess on entry, solution on return (device pointers). */
+TN_API int tn_stokes_solve( tn_stokes_solver* solver, const double* const* f_u, const double* f_p,
+                            double* const* x_u, double* x_p, int* iterations, double* relative_residual );
+/* relative residual history of the last solve (FGMRES estimates, entry 0 = 1) */
+TN_API int tn_stokes_history( const tn_stokes_solver* solver, double* out, int capacity, int* count,
+                              int* preconditioner_skips );
+/* out = K in (the FP64 Stokes operator of the solver) */
+TN_API int tn_stokes_apply( tn_stokes_solver* solver, const double* const* u, const double* p, double* const* out_u,
+                            double* out_p );
+TN_API int tn_stokes_solver_destroy( tn_stokes_solver* solver );
 
 #ifdef __cplusplus
 }

@@ -25,6 +25,14 @@ class EpsDivDivParams(ctypes.Structure):
                 ("comm_mode", c_int), ("penalty_eps", c_double)]
 
 
+class StokesParams(ctypes.Structure):
+    _fields_ = [("level", c_int), ("mg_levels", c_int), ("bc_cmb", c_int), ("bc_surface", c_int), ("mg_fp32", c_int),
+                ("chebyshev_order", c_int), ("smoothing_steps", c_int), ("power_iterations", c_int),
+                ("vcycles", c_int), ("coarse_max_iterations", c_int), ("coarse_relative_tolerance", c_double),
+                ("restart", c_int), ("max_iterations", c_int), ("relative_tolerance", c_double),
+                ("absolute_tolerance", c_double)]
+
+
 class TNError(RuntimeError):
     pass
 
@@ -55,6 +63,15 @@ _SIGS = {
     "tn_restriction_constant_f32": (c_int, [c_void_p, c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
     "tn_kmass_apply_f64": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "tn_kmass_apply_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "tn_injection_f64": (c_int, [c_void_p, c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_freeslip_project_f64": (c_int, [c_void_p, P(c_void_p), c_int, c_int, c_void_p]),
+    "tn_laplace_pcg_solve_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, P(c_int),
+                                         P(c_double)]),
+    "tn_stokes_solver_create": (c_int, [P(StokesParams), c_double, c_double, c_void_p, P(c_void_p)]),
+    "tn_stokes_solve": (c_int, [c_void_p, P(c_void_p), c_void_p, P(c_void_p), c_void_p, P(c_int), P(c_double)]),
+    "tn_stokes_history": (c_int, [c_void_p, P(c_double), c_int, P(c_int), P(c_int)]),
+    "tn_stokes_apply": (c_int, [c_void_p, P(c_void_p), c_void_p, P(c_void_p), c_void_p]),
+    "tn_stokes_solver_destroy": (c_int, [c_void_p]),
     "tn_vec_lincomb_f64": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p), c_void_p]),
     "tn_vec_lincomb_f32": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p), c_void_p]),
     "tn_vec_dot_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_double), c_void_p]),
@@ -66,6 +83,8 @@ _SIGS = {
     "tn_vec_max_abs_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_double), c_void_p]),
     "tn_vec_has_nan_or_inf_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), c_void_p]),
     "tn_vec_has_nan_or_inf_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), c_void_p]),
+    "tn_vec_randomize_f64": (c_int, [c_void_p, c_int, P(c_void_p), ctypes.c_ulonglong, c_void_p]),
+    "tn_vec_randomize_f32": (c_int, [c_void_p, c_int, P(c_void_p), ctypes.c_ulonglong, c_void_p]),
     "tn_vec_cast_f64_to_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
     "tn_vec_cast_f32_to_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
 }

@@ -1,0 +1,397 @@
+// C++ restatement of the reference's solver drivers (linalg/solvers/*.hpp)
+// over the terraneo_b200 C ABI.  Same concepts (SolverLike: solve_impl(A, x,
+// b)), same recurrences and stopping rules; the per-iteration vector work runs
+// in the CUDA library.  Iteration histories replace util::Table rows.
+#pragma once
+
+#include <cmath>
+#include <cstdio>
+#include <limits>
+#include <vector>
+
+#include "operators.hpp"
+
+namespace tn {
+
+// IterativeSolverParameters (linalg/solvers/iterative_solver_info.hpp:6)
+struct IterativeSolverParameters
+{
+    int    max_iterations              = 100;
+    double relative_residual_tolerance = 1e-12;
+    double absolute_residual_tolerance = 1e-12;
+};
+
+struct SolverStatistics
+{
+    std::vector< double > relative_residuals;
+    int                   iterations = 0;
+};
+
+// IdentitySolver (identity_solver.hpp): x = b
+template < typename Op >
+class IdentitySolver
+{
+  public:
+    template < typename X, typename B >
+    void solve_impl( Op&, X& x, const B& b )
+    {
+        assign( x, b );
+    }
+};
+
+// DiagonalSolver (diagonal_solver.hpp:20): x = D^{-1} b, D inverted at construction
+template < typename Op, typename V >
+class DiagonalSolver
+{
+  public:
+    explicit DiagonalSolver( const V& diagonal ) : inv_( diagonal ) { invert_entries( inv_ ); }
+    template < typename A >
+    void solve_impl( A&, V& x, const V& b )
+    {
+        assign( x, b );
+        scale_in_place( x, inv_ );
+    }
+
+  private:
+    V inv_;
+};
+
+// PCG (pcg.hpp:78-160)
+template < typename Op, typename Prec = IdentitySolver< Op > >
+class PCG
+{
+  public:
+    using V = typename Op::SrcVectorType;
+    PCG( IterativeSolverParameters prm, std::vector< V > tmps, Prec prec = Prec() )
+    : prm_( prm ), tmps_( std::move( tmps ) ), prec_( prec )
+    {
+        if ( tmps_.size() < 4 )
+            throw std::runtime_error( "PCG: needs 4 temporary vectors" );
+    }
+    SolverStatistics stats;
+    void             solve_impl( Op& A, V& x, const V& b )
+    {
+        auto& r = tmps_[0];
+        auto& p = tmps_[1];
+        auto& ap = tmps_[2];
+        auto& z = tmps_[3];
+        stats   = {};
+        apply( A, x, r );
+        lincomb( r, { 1.0, -1.0 }, { b, r } );
+        solve( prec_, A, z, r );
+        assign( p, z );
+        const double r0 = std::sqrt( double( dot( r, r ) ) );
+        stats.relative_residuals.push_back( 1.0 );
+        if ( r0 < prm_.absolute_residual_tolerance )
+            return;
+        for ( int it = 1; it <= prm_.max_iterations; ++it )
+        {
+            const auto an = dot( z, r );
+            apply( A, p, ap );
+            const auto alpha = an / dot( ap, p );
+            lincomb( x, { 1.0, alpha }, { x, p } );
+            lincomb( r, { 1.0, -alpha }, { r, ap } );
+            const double ar = std::sqrt( double( dot( r, r ) ) );
+            stats.relative_residuals.push_back( ar / r0 );
+            stats.iterations = it;
+            if ( ar / r0 <= prm_.relative_residual_tolerance || ar < prm_.absolute_residual_tolerance )
+                return;
+            solve( prec_, A, z, r );
+            const auto beta = dot( z, r ) / an;
+            lincomb( p, { 1.0, beta }, { z, p } );
+        }
+    }
+
+  private:
+    IterativeSolverParameters prm_;
+    std::vector< V >          tmps_;
+    Prec                      prec_;
+};
+
+// power_iteration (power_iteration.hpp:13-48) from a deterministic random start
+template < typename Op, typename V >
+double power_iteration( Op& op, V& it, V& aux, int iterations )
+{
+    using S = typename V::ScalarType;
+    randomize( it );
+    auto n = norm_2( it );
+    lincomb( it, { S( 1.0 / n ) }, { it }, S( 0 ) );
+    apply( op, it, aux );
+    double radius = 0;
+    for ( int k = 0; k < iterations; ++k )
+    {
+        n = norm_2( aux );
+        lincomb( it, { S( 1.0 / n ) }, { aux }, S( 0 ) );
+        apply( op, it, aux );
+        radius = double( dot( it, aux ) );
+    }
+    return radius;
+}
+
+// Chebyshev smoother (chebyshev.hpp:50-175): lambda_max = 1.5 * power-iteration
+// estimate of D^{-1} A, lambda_min = 0.1 * estimate.
+template < typename Op >
+class Chebyshev
+{
+  public:
+    using V = typename Op::SrcVectorType;
+    Chebyshev( int order, const V& inverse_diagonal, std::vector< V > tmps, int iterations, int power_iterations )
+    : order_( order ), inv_diag_( inverse_diagonal ), tmps_( std::move( tmps ) ), iterations_( iterations ),
+      power_iterations_( power_iterations )
+    {}
+    void refresh_max_eigenvalue_estimate_in_next_solve() { need_ev_ = true; }
+    double max_eigenvalue_estimate() const { return ev_; }
+    void   solve_impl( Op& A, V& x, const V& b )
+    {
+        if ( need_ev_ )
+        {
+            DiagonallyScaledOperator< Op > dA( A, inv_diag_ );
+            ev_      = power_iteration( dA, tmps_[0], tmps_[1], power_iterations_ );
+            need_ev_ = false;
+        }
+        auto&        d     = tmps_[0];
+        auto&        z     = tmps_[1];
+        const double lmax  = 1.5 * ev_, lmin = 0.1 * ev_;
+        const double theta = 0.5 * ( lmax + lmin ), delta = 0.5 * ( lmax - lmin );
+        const double sigma = theta / delta;
+        using S            = typename V::ScalarType;
+        double rho         = 1.0 / sigma; // carried across sweeps as in the reference (chebyshev.hpp:119)
+        for ( int it = 0; it < iterations_; ++it )
+        {
+            apply( A, x, z );
+            lincomb( z, { S( 1 ), S( -1 ) }, { b, z } );
+            scale_in_place( z, inv_diag_ );
+            lincomb( d, { S( 1.0 / theta ) }, { z } );
+            lincomb( x, { S( 1 ), S( 1 ) }, { x, d } );
+            for ( int i = 2; i <= order_; ++i )
+            {
+                const double rho_new = 1.0 / ( 2.0 * sigma - rho );
+                const double beta = rho_new * rho, alpha = 2.0 * rho_new / delta;
+                apply( A, x, z );
+                lincomb( z, { S( 1 ), S( -1 ) }, { b, z } );
+                scale_in_place( z, inv_diag_ );
+                lincomb( d, { S( alpha ), S( beta ) }, { z, d } );
+                lincomb( x, { S( 1 ), S( 1 ) }, { x, d } );
+                rho = rho_new;
+            }
+        }
+    }
+
+  private:
+    int              order_;
+    V                inv_diag_;
+    std::vector< V > tmps_;
+    int              iterations_, power_iterations_;
+    bool             need_ev_ = true;
+    double           ev_      = 0;
+};
+
+// Multigrid V-cycle (multigrid.hpp:24-211).  Level 0 is the coarsest.
+template < typename Op, typename P, typename R, typename Smoother, typename Coarse >
+class Multigrid
+{
+  public:
+    using V = typename Op::SrcVectorType;
+    Multigrid( std::vector< P > prolong_additive, std::vector< R > restrict_, std::vector< Op > coarse_ops,
+               std::vector< V > tmp_r, std::vector< V > tmp_e, std::vector< V > tmp, std::vector< Smoother > smoothers,
+               Coarse coarse, int cycles )
+    : P_( std::move( prolong_additive ) ), R_( std::move( restrict_ ) ), A_c_( std::move( coarse_ops ) ),
+      tmp_r_( std::move( tmp_r ) ), tmp_e_( std::move( tmp_e ) ), tmp_( std::move( tmp ) ),
+      smoothers_( std::move( smoothers ) ), coarse_( std::move( coarse ) ), cycles_( cycles )
+    {
+        if ( P_.size() != A_c_.size() || R_.size() != A_c_.size() || tmp_r_.size() != A_c_.size() ||
+             tmp_e_.size() != A_c_.size() || tmp_.size() != A_c_.size() + 1 || smoothers_.size() != A_c_.size() + 1 )
+            throw std::runtime_error( "Multigrid: inconsistent level sizes" );
+    }
+    Coarse& coarse_solver() { return coarse_; }
+    void    solve_impl( Op& A, V& x, const V& b )
+    {
+        for ( int c = 0; c < cycles_; ++c )
+            recurse( A, x, b, int( P_.size() ) );
+    }
+
+  private:
+    void recurse( Op& A, V& x, const V& b, int level )
+    {
+        using S = typename V::ScalarType;
+        if ( level == 0 )
+        {
+            solve( coarse_, A, tmp_e_[0], tmp_r_[0] );
+            return;
+        }
+        solve( smoothers_[level], A, x, b );
+        apply( A, x, tmp_[level] );
+        lincomb( tmp_[level], { S( 1 ), S( -1 ) }, { b, tmp_[level] } );
+        apply( R_[level - 1], tmp_[level], tmp_r_[level - 1] );
+        assign( tmp_e_[level - 1], S( 0 ) );
+        recurse( A_c_[level - 1], tmp_e_[level - 1], tmp_r_[level - 1], level - 1 );
+        apply( P_[level - 1], tmp_e_[level - 1], x );
+        solve( smoothers_[level], A, x, b );
+    }
+
+    std::vector< P >        P_;
+    std::vector< R >        R_;
+    std::vector< Op >       A_c_;
+    std::vector< V >        tmp_r_, tmp_e_, tmp_;
+    std::vector< Smoother > smoothers_;
+    Coarse                  coarse_;
+    int                     cycles_;
+};
+
+// BlockTriangularPreconditioner2x2 (block_preconditioner_2x2.hpp:145-217)
+template < typename Block11, typename Block12, typename Prec11, typename Prec22, typename BV >
+class BlockTriangularPreconditioner2x2
+{
+  public:
+    BlockTriangularPreconditioner2x2( Block11& a11, Block12& a12, BV tmp, Prec11& p11, Prec22& p22 )
+    : a11_( a11 ), a12_( a12 ), tmp_( tmp ), p11_( p11 ), p22_( p22 )
+    {}
+    template < typename Op >
+    void solve_impl( Op&, BV& x, const BV& b )
+    {
+        using S = typename BV::ScalarType;
+        solve( p22_, a11_, x.block_2(), b.block_2() );
+        apply( a12_, x.block_2(), tmp_.block_1() );
+        lincomb( tmp_.block_1(), { S( 1 ), S( 1 ) }, { tmp_.block_1(), b.block_1() } );
+        lincomb( x.block_2(), { S( -1 ) }, { x.block_2() } );
+        solve( p11_, a11_, x.block_1(), tmp_.block_1() );
+    }
+
+  private:
+    Block11& a11_;
+    Block12& a12_;
+    BV       tmp_;
+    Prec11&  p11_;
+    Prec22&  p22_;
+};
+
+// FGMRES(m) with modified Gram-Schmidt Arnoldi and Givens rotations
+// (fgmres.hpp:108-330), including the reference's fall-back of skipping the
+// preconditioner when it returns NaN / Inf.
+template < typename Op, typename Prec >
+class FGMRES
+{
+  public:
+    using V = typename Op::SrcVectorType;
+    FGMRES( std::vector< V > tmps, int restart, IterativeSolverParameters prm, Prec& prec )
+    : tmp_( std::move( tmps ) ), m_( restart ), prm_( prm ), prec_( prec )
+    {
+        if ( int( tmp_.size() ) < 2 * m_ + 4 )
+            throw std::runtime_error( "FGMRES: needs 2 * restart + 4 temporary vectors" );
+    }
+    SolverStatistics stats;
+    int              preconditioner_skips = 0;
+
+    void solve_impl( Op& A, V& x, const V& b )
+    {
+        using S = typename V::ScalarType;
+        stats   = {};
+        auto& r = tmp_[0];
+        apply( A, x, r );
+        lincomb( r, { S( 1 ), S( -1 ) }, { b, r } );
+        double       beta0 = std::sqrt( double( dot( r, r ) ) );
+        const double r0    = beta0;
+        stats.relative_residuals.push_back( 1.0 );
+        if ( beta0 <= prm_.absolute_residual_tolerance )
+            return;
+        const int offV = 1, offZ = offV + m_ + 1, idxW = offZ + m_, idxAcc = idxW + 1;
+        std::vector< double > H( ( m_ + 1 ) * m_ ), g( m_ + 1 ), cs( m_ + 1 ), sn( m_ + 1 );
+        auto h = [&]( int i, int j ) -> double& { return H[i * m_ + j]; };
+        int  total = 0;
+        while ( total < prm_.max_iterations )
+        {
+            lincomb( tmp_[offV], { S( 1.0 / beta0 ) }, { r } );
+            std::fill( H.begin(), H.end(), 0.0 );
+            std::fill( g.begin(), g.end(), 0.0 );
+            std::fill( cs.begin(), cs.end(), 0.0 );
+            std::fill( sn.begin(), sn.end(), 0.0 );
+            g[0]      = beta0;
+            int inner = 0;
+            for ( int j = 0; j < m_ && total < prm_.max_iterations; ++j, ++total )
+            {
+                auto& vj = tmp_[offV + j];
+                auto& zj = tmp_[offZ + j];
+                assign( zj, S( 0 ) );
+                solve( prec_, A, zj, vj );
+                if ( has_nan_or_inf( zj ) )
+                {
+                    assign( zj, vj );
+                    ++preconditioner_skips;
+                }
+                auto& w = tmp_[idxW];
+                apply( A, zj, w );
+                for ( int i = 0; i <= j; ++i )
+                {
+                    const double hij = double( dot( w, tmp_[offV + i] ) );
+                    h( i, j )        = hij;
+                    lincomb( w, { S( 1 ), S( -hij ) }, { w, tmp_[offV + i] } );
+                }
+                const double hj1 = std::sqrt( double( dot( w, w ) ) );
+                if ( hj1 < std::numeric_limits< double >::epsilon() * r0 )
+                {
+                    h( j + 1, j ) = 0;
+                    inner         = j + 1;
+                    break;
+                }
+                h( j + 1, j ) = hj1;
+                lincomb( tmp_[offV + j + 1], { S( 1.0 / hj1 ) }, { w } );
+                for ( int i = 0; i < j; ++i )
+                {
+                    const double t = cs[i] * h( i, j ) + sn[i] * h( i + 1, j );
+                    h( i + 1, j )  = -sn[i] * h( i, j ) + cs[i] * h( i + 1, j );
+                    h( i, j )      = t;
+                }
+                const double a = h( j, j ), bb = h( j + 1, j ), rab = std::hypot( a, bb );
+                cs[j]          = rab == 0 ? 1.0 : a / rab;
+                sn[j]          = rab == 0 ? 0.0 : bb / rab;
+                h( j, j )      = rab;
+                h( j + 1, j )  = 0;
+                if ( std::abs( rab ) < std::numeric_limits< double >::epsilon() )
+                {
+                    inner = j;
+                    break;
+                }
+                const double gj = g[j], gj1 = g[j + 1];
+                g[j]     = cs[j] * gj + sn[j] * gj1;
+                g[j + 1] = -sn[j] * gj + cs[j] * gj1;
+                stats.relative_residuals.push_back( std::abs( g[j + 1] ) / r0 );
+                stats.iterations = total + 1;
+                inner            = j + 1;
+                if ( std::abs( g[j + 1] ) / r0 <= prm_.relative_residual_tolerance ||
+                     std::abs( g[j + 1] ) < prm_.absolute_residual_tolerance )
+                {
+                    ++total;
+                    break;
+                }
+            }
+            std::vector< double > y( inner, 0.0 );
+            for ( int row = inner - 1; row >= 0; --row )
+            {
+                double s = g[row];
+                for ( int col = row + 1; col < inner; ++col )
+                    s -= h( row, col ) * y[col];
+                y[row] = s / h( row, row );
+            }
+            auto& acc = tmp_[idxAcc];
+            assign( acc, S( 0 ) );
+            for ( int i = 0; i < inner; ++i )
+                lincomb( acc, { S( 1 ), S( y[i] ) }, { acc, tmp_[offZ + i] } );
+            lincomb( x, { S( 1 ), S( 1 ) }, { x, acc } );
+            apply( A, x, r );
+            lincomb( r, { S( 1 ), S( -1 ) }, { b, r } );
+            beta0 = std::sqrt( double( dot( r, r ) ) );
+            true_relative_residual = beta0 / r0;
+            if ( beta0 <= prm_.absolute_residual_tolerance || beta0 / r0 <= prm_.relative_residual_tolerance )
+                return;
+        }
+    }
+    double true_relative_residual = 1.0;
+
+  private:
+    std::vector< V >          tmp_;
+    int                       m_;
+    IterativeSolverParameters prm_;
+    Prec&                     prec_;
+};
+
+}  // namespace tn

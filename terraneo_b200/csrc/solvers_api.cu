@@ -1,0 +1,358 @@
+// C ABI of the solver drivers: PCG on the scalar Laplace (the CG benchmark
+// configuration) and the Stokes solver (FGMRES + block-triangular
+// preconditioner, geometric multigrid on the viscous block with Chebyshev
+// smoothing and a PCG coarse solve, lumped inverse KMass(1/eta) Schur
+// approximation), composed as in the reference's mantle-circulation app
+// (apps/mantlecirculation/mantlecirculation.cpp:486-735).
+//
+// The multigrid preconditioner runs in FP32 (operators, smoothers, transfers,
+// FP32 viscosity) inside the FP64 outer FGMRES when mg_fp32 != 0; the outer
+// residual, dot products (compensated), Schur diagonal and the coarsest-level
+// PCG stay FP64.  Coarser-level viscous operators are re-discretised with the
+// viscosity injected from the finest level.
+#include <functional>
+#include <memory>
+
+#include "../cpp/tn/solvers.hpp"
+#include "common.cuh"
+
+using namespace tn;
+
+namespace {
+
+using A64 = EpsilonDivDivKerngen< double >;
+using A32 = EpsilonDivDivKerngen< float >;
+
+// FP32 V-cycle's coarsest solve done in FP64: cast, PCG, cast back
+struct CoarseFp64
+{
+    std::shared_ptr< PCG< A64 > > pcg;
+    std::shared_ptr< A64 >        A;
+    VectorQ1Vec< double >         x, b;
+    void                          solve_impl( A32&, VectorQ1Vec< float >& xo, const VectorQ1Vec< float >& bi )
+    {
+        cast( b, bi );
+        assign( x, 0.0 );
+        solve( *pcg, *A, x, b );
+        cast( xo, x );
+    }
+};
+
+template < typename T, typename Coarse >
+using MG = Multigrid< EpsilonDivDivKerngen< T >, ProlongationVecConstant< T >, RestrictionVecConstant< T >,
+                      Chebyshev< EpsilonDivDivKerngen< T > >, Coarse >;
+
+// FP32 multigrid as a preconditioner of the FP64 viscous block
+template < typename Inner >
+struct Fp32Preconditioner
+{
+    std::shared_ptr< Inner > mg;
+    std::shared_ptr< A32 >   A;
+    VectorQ1Vec< float >     x, b;
+    void                     solve_impl( A64&, VectorQ1Vec< double >& xo, const VectorQ1Vec< double >& bi )
+    {
+        cast( b, bi );
+        assign( x, 0.0f );
+        solve( *mg, *A, x, b );
+        cast( xo, x );
+    }
+};
+
+template < typename Inner >
+struct Fp64Preconditioner
+{
+    std::shared_ptr< Inner > mg;
+    void solve_impl( A64& A, VectorQ1Vec< double >& x, const VectorQ1Vec< double >& b ) { solve( *mg, A, x, b ); }
+};
+
+}  // namespace
+
+struct tn_stokes_solver
+{
+    tn_stokes_params                                         prm{};
+    std::vector< Mesh >                                      mesh; // index = level
+    std::vector< VectorQ1Scalar< double > >                  k64;
+    std::vector< VectorQ1Scalar< float > >                   k32;
+    std::vector< std::shared_ptr< A64 > >                    A64s;
+    std::unique_ptr< EpsDivDivStokes< double > >             K;
+    std::unique_ptr< Gradient< double > >                    BT;
+    std::function< void( VectorQ1IsoQ2Q1< double >&, const VectorQ1IsoQ2Q1< double >& ) > run;
+    std::vector< double >                                    history;
+    int                                                      iterations = 0;
+    double                                                   relres     = 1.0;
+    int                                                      skips      = 0;
+};
+
+namespace {
+
+template < typename T >
+VectorQ1Vec< T > inverse_diagonal_vec( EpsilonDivDivKerngen< T >& A, const Mesh& m )
+{
+    VectorQ1Vec< T > ones( m ), d( m );
+    assign( ones, T( 1 ) );
+    A.set_diagonal( true );
+    apply( A, ones, d );
+    A.set_diagonal( false );
+    invert_entries( d );
+    return d;
+}
+
+// builds the multigrid hierarchy in precision T over levels [Lmin, L]
+template < typename T, typename Coarse >
+std::shared_ptr< MG< T, Coarse > > build_mg( tn_stokes_solver& s, std::vector< std::shared_ptr< EpsilonDivDivKerngen< T > > >& ops,
+                                             Coarse coarse )
+{
+    const auto&                                prm = s.prm;
+    const int                                  L = prm.level, Lmin = prm.level - prm.mg_levels + 1;
+    BoundaryConditions                         bcs{ prm.bc_cmb, prm.bc_surface };
+    std::vector< ProlongationVecConstant< T > > P;
+    std::vector< RestrictionVecConstant< T > >  R;
+    std::vector< EpsilonDivDivKerngen< T > >    Ac;
+    std::vector< VectorQ1Vec< T > >             tr, te, tmp;
+    std::vector< Chebyshev< EpsilonDivDivKerngen< T > > > sm;
+    for ( int l = Lmin; l <= L; ++l )
+    {
+        const Mesh& m = s.mesh[l];
+        if constexpr ( std::is_same_v< T, double > )
+            ops.push_back( std::make_shared< EpsilonDivDivKerngen< T > >( m, s.k64[l], bcs, false ) );
+        else
+            ops.push_back( std::make_shared< EpsilonDivDivKerngen< T > >( m, s.k32[l], bcs, false ) );
+        auto inv = inverse_diagonal_vec( *ops.back(), m );
+        sm.emplace_back( prm.chebyshev_order, inv, std::vector< VectorQ1Vec< T > >{ VectorQ1Vec< T >( m ), VectorQ1Vec< T >( m ) },
+                         prm.smoothing_steps, prm.power_iterations );
+        tmp.emplace_back( m );
+        if ( l < L )
+        {
+            Ac.push_back( *ops.back() );
+            tr.emplace_back( m );
+            te.emplace_back( m );
+            P.emplace_back( s.mesh[l + 1], m, OperatorApplyMode::Add );
+            R.emplace_back( s.mesh[l + 1], m );
+        }
+    }
+    return std::make_shared< MG< T, Coarse > >( P, R, Ac, tr, te, tmp, sm, coarse, prm.vcycles );
+}
+
+template < typename Prec11 >
+void finish( tn_stokes_solver& s, std::shared_ptr< Prec11 > p11 )
+{
+    const auto& prm = s.prm;
+    const int   L   = prm.level;
+    BoundaryConditions bcs{ prm.bc_cmb, prm.bc_surface };
+    s.K  = std::make_unique< EpsDivDivStokes< double > >( s.mesh[L], s.mesh[L - 1], s.k64[L], bcs );
+    s.BT = std::make_unique< Gradient< double > >( s.mesh[L], s.mesh[L - 1], bcs );
+    // Schur: lumped KMass with k = 1 / eta on the pressure level (mantlecirculation.cpp:684-699)
+    VectorQ1Scalar< double > kp( s.mesh[L - 1] ), ones( s.mesh[L - 1] ), dp( s.mesh[L - 1] );
+    assign( kp, s.k64[L - 1] );
+    invert_entries( kp );
+    assign( ones, 1.0 );
+    KMass< double > pm( s.mesh[L - 1], kp, 2 );
+    apply( pm, ones, dp );
+    auto p22 = std::make_shared< DiagonalSolver< KMass< double >, VectorQ1Scalar< double > > >( dp );
+    auto a11 = s.A64s.back();
+    using BT = BlockTriangularPreconditioner2x2< A64, Gradient< double >, Prec11,
+                                                 DiagonalSolver< KMass< double >, VectorQ1Scalar< double > >,
+                                                 VectorQ1IsoQ2Q1< double > >;
+    auto prec = std::make_shared< BT >( *a11, *s.BT, VectorQ1IsoQ2Q1< double >( s.mesh[L], s.mesh[L - 1] ), *p11, *p22 );
+    std::vector< VectorQ1IsoQ2Q1< double > > tmps;
+    for ( int i = 0; i < 2 * prm.restart + 4; ++i )
+        tmps.emplace_back( s.mesh[L], s.mesh[L - 1] );
+    IterativeSolverParameters ip{ prm.max_iterations, prm.relative_tolerance, prm.absolute_tolerance };
+    auto fg = std::make_shared< FGMRES< EpsDivDivStokes< double >, BT > >( tmps, prm.restart, ip, *prec );
+    tn_stokes_solver* sp = &s;
+    s.run = [sp, fg, prec, p11, p22, a11]( VectorQ1IsoQ2Q1< double >& x, const VectorQ1IsoQ2Q1< double >& b ) {
+        solve( *fg, *sp->K, x, b );
+        sp->history    = fg->stats.relative_residuals;
+        sp->iterations = fg->stats.iterations;
+        sp->relres     = fg->true_relative_residual;
+        sp->skips      = fg->preconditioner_skips;
+    };
+}
+
+}  // namespace
+
+extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min, double r_max, const double* k,
+                                        tn_stokes_solver** out )
+{
+    TN_CHECK_ARG( p && k && out, "tn_stokes_solver_create: null argument" );
+    *out = nullptr;
+    TN_CHECK_ARG( p->mg_levels >= 1 && p->level - p->mg_levels + 1 >= 2 && p->level <= 8,
+                  "tn_stokes_solver_create: need level - mg_levels + 1 >= 2 (tiled coarsest operator) and level <= 8" );
+    TN_CHECK_ARG( p->restart >= 1 && p->max_iterations >= 1, "tn_stokes_solver_create: bad Krylov parameters" );
+    try
+    {
+        auto s = std::make_unique< tn_stokes_solver >();
+        s->prm = *p;
+        const int L = p->level, Lmin = L - p->mg_levels + 1;
+        const int Llo = std::min( Lmin, L - 1 );
+        s->mesh.resize( L + 1 );
+        s->k64.resize( L + 1 );
+        s->k32.resize( L + 1 );
+        for ( int l = Llo; l <= L; ++l )
+        {
+            s->mesh[l] = Mesh( l, r_min, r_max );
+            s->k64[l]  = VectorQ1Scalar< double >( s->mesh[l] );
+            s->k32[l]  = VectorQ1Scalar< float >( s->mesh[l] );
+        }
+        check( cudaMemcpy( s->k64[L].data(), k, sizeof( double ) * s->mesh[L].stored_nodes(), cudaMemcpyDeviceToDevice ) ==
+                       cudaSuccess
+                   ? TN_OK
+                   : TN_ERR_CUDA,
+               "copy viscosity" );
+        for ( int l = L - 1; l >= Llo; --l )
+        {
+            const double* src[1] = { s->k64[l + 1].data() };
+            double*       dst[1] = { s->k64[l].data() };
+            check( tn_injection_f64( s->mesh[l + 1].get(), s->mesh[l].get(), 1, src, dst, nullptr ), "injection" );
+        }
+        for ( int l = Llo; l <= L; ++l )
+        {
+            const double* src[1] = { s->k64[l].data() };
+            float*        dst[1] = { s->k32[l].data() };
+            check( tn_vec_cast_f64_to_f32( s->mesh[l].get(), 1, dst, src, nullptr ), "cast viscosity" );
+        }
+        // FP64 coarsest solve (both precisions): PCG, 4 temporaries
+        BoundaryConditions bcs{ p->bc_cmb, p->bc_surface };
+        auto               Ac64 = std::make_shared< A64 >( s->mesh[Lmin], s->k64[Lmin], bcs, false );
+        std::vector< VectorQ1Vec< double > > ct;
+        for ( int i = 0; i < 4; ++i )
+            ct.emplace_back( s->mesh[Lmin] );
+        auto pcg = std::make_shared< PCG< A64 > >(
+            IterativeSolverParameters{ p->coarse_max_iterations, p->coarse_relative_tolerance, 1e-16 }, ct );
+        if ( p->mg_fp32 )
+        {
+            std::vector< std::shared_ptr< A32 > > ops32;
+            CoarseFp64 cs{ pcg, Ac64, VectorQ1Vec< double >( s->mesh[Lmin] ), VectorQ1Vec< double >( s->mesh[Lmin] ) };
+            auto       mg = build_mg< float, CoarseFp64 >( *s, ops32, cs );
+            for ( int l = Lmin; l <= L; ++l )
+                s->A64s.push_back( std::make_shared< A64 >( s->mesh[l], s->k64[l], bcs, false ) );
+            auto p11 = std::make_shared< Fp32Preconditioner< MG< float, CoarseFp64 > > >(
+                Fp32Preconditioner< MG< float, CoarseFp64 > >{ mg, ops32.back(), VectorQ1Vec< float >( s->mesh[L] ),
+                                                                VectorQ1Vec< float >( s->mesh[L] ) } );
+            finish( *s, p11 );
+        }
+        else
+        {
+            auto mg  = build_mg< double, PCG< A64 > >( *s, s->A64s, *pcg );
+            auto p11 = std::make_shared< Fp64Preconditioner< MG< double, PCG< A64 > > > >(
+                Fp64Preconditioner< MG< double, PCG< A64 > > >{ mg } );
+            finish( *s, p11 );
+        }
+        *out = s.release();
+        return TN_OK;
+    }
+    catch ( const std::exception& e )
+    {
+        set_error( std::string( "tn_stokes_solver_create: " ) + e.what() );
+        return TN_ERR_STATE;
+    }
+}
+
+extern "C" int tn_stokes_solve( tn_stokes_solver* s, const double* const* f_u, const double* f_p, double* const* x_u,
+                                double* x_p, int* iterations, double* relative_residual )
+{
+    TN_CHECK_ARG( s && f_u && f_p && x_u && x_p, "tn_stokes_solve: null argument" );
+    try
+    {
+        const int                 L = s->prm.level;
+        const size_t              nu = s->mesh[L].stored_nodes();
+        VectorQ1IsoQ2Q1< double > b( s->mesh[L], s->mesh[L - 1] ), x( s->mesh[L], s->mesh[L - 1] );
+        for ( int c = 0; c < 3; ++c )
+        {
+            TN_CUDA_TRY( cudaMemcpyAsync( b.block_1().comp( c ), f_u[c], sizeof( double ) * nu, cudaMemcpyDeviceToDevice ) );
+            TN_CUDA_TRY( cudaMemcpyAsync( x.block_1().comp( c ), x_u[c], sizeof( double ) * nu, cudaMemcpyDeviceToDevice ) );
+        }
+        const size_t np = s->mesh[L - 1].stored_nodes();
+        TN_CUDA_TRY( cudaMemcpyAsync( b.block_2().data(), f_p, sizeof( double ) * np, cudaMemcpyDeviceToDevice ) );
+        TN_CUDA_TRY( cudaMemcpyAsync( x.block_2().data(), x_p, sizeof( double ) * np, cudaMemcpyDeviceToDevice ) );
+        s->run( x, b );
+        for ( int c = 0; c < 3; ++c )
+            TN_CUDA_TRY( cudaMemcpyAsync( x_u[c], x.block_1().comp( c ), sizeof( double ) * nu, cudaMemcpyDeviceToDevice ) );
+        TN_CUDA_TRY( cudaMemcpyAsync( x_p, x.block_2().data(), sizeof( double ) * np, cudaMemcpyDeviceToDevice ) );
+        TN_CUDA_TRY( cudaDeviceSynchronize() );
+        if ( iterations )
+            *iterations = s->iterations;
+        if ( relative_residual )
+            *relative_residual = s->relres;
+        return TN_OK;
+    }
+    catch ( const std::exception& e )
+    {
+        set_error( std::string( "tn_stokes_solve: " ) + e.what() );
+        return TN_ERR_STATE;
+    }
+}
+
+extern "C" int tn_stokes_history( const tn_stokes_solver* s, double* out, int cap, int* n, int* preconditioner_skips )
+{
+    TN_CHECK_ARG( s, "tn_stokes_history: null solver" );
+    const int m = int( s->history.size() );
+    if ( n )
+        *n = m;
+    if ( out )
+        for ( int i = 0; i < m && i < cap; ++i )
+            out[i] = s->history[i];
+    if ( preconditioner_skips )
+        *preconditioner_skips = s->skips;
+    return TN_OK;
+}
+
+extern "C" int tn_stokes_apply( tn_stokes_solver* s, const double* const* u, const double* p, double* const* ou,
+                                double* op )
+{
+    TN_CHECK_ARG( s && u && p && ou && op, "tn_stokes_apply: null argument" );
+    try
+    {
+        const int                 L = s->prm.level;
+        VectorQ1IsoQ2Q1< double > src( s->mesh[L], s->mesh[L - 1] ), dst( s->mesh[L], s->mesh[L - 1] );
+        const size_t              nu = s->mesh[L].stored_nodes(), np = s->mesh[L - 1].stored_nodes();
+        for ( int c = 0; c < 3; ++c )
+            TN_CUDA_TRY( cudaMemcpyAsync( src.block_1().comp( c ), u[c], sizeof( double ) * nu, cudaMemcpyDeviceToDevice ) );
+        TN_CUDA_TRY( cudaMemcpyAsync( src.block_2().data(), p, sizeof( double ) * np, cudaMemcpyDeviceToDevice ) );
+        apply( *s->K, src, dst );
+        for ( int c = 0; c < 3; ++c )
+            TN_CUDA_TRY( cudaMemcpyAsync( ou[c], dst.block_1().comp( c ), sizeof( double ) * nu, cudaMemcpyDeviceToDevice ) );
+        TN_CUDA_TRY( cudaMemcpyAsync( op, dst.block_2().data(), sizeof( double ) * np, cudaMemcpyDeviceToDevice ) );
+        return TN_OK;
+    }
+    catch ( const std::exception& e )
+    {
+        set_error( std::string( "tn_stokes_apply: " ) + e.what() );
+        return TN_ERR_STATE;
+    }
+}
+
+extern "C" int tn_stokes_solver_destroy( tn_stokes_solver* s )
+{
+    delete s;
+    return TN_OK;
+}
+
+extern "C" int tn_laplace_pcg_solve_f64( const tn_mesh* mesh, const double* b, double* x, int max_iterations,
+                                         double relative_tolerance, double absolute_tolerance, int* iterations,
+                                         double* relative_residual )
+{
+    TN_CHECK_ARG( mesh && b && x, "tn_laplace_pcg_solve_f64: null argument" );
+    try
+    {
+        Mesh                     m = Mesh::wrap( mesh );
+        Laplace< double >        A( m, true, false );
+        VectorQ1Scalar< double > vb( m, const_cast< double* >( b ) ), vx( m, x );
+        std::vector< VectorQ1Scalar< double > > t;
+        for ( int i = 0; i < 4; ++i )
+            t.emplace_back( m );
+        PCG< Laplace< double > > pcg( IterativeSolverParameters{ max_iterations, relative_tolerance, absolute_tolerance }, t );
+        solve( pcg, A, vx, vb );
+        TN_CUDA_TRY( cudaDeviceSynchronize() );
+        if ( iterations )
+            *iterations = pcg.stats.iterations;
+        if ( relative_residual )
+            *relative_residual = pcg.stats.relative_residuals.back();
+        return TN_OK;
+    }
+    catch ( const std::exception& e )
+    {
+        set_error( std::string( "tn_laplace_pcg_solve_f64: " ) + e.what() );
+        return TN_ERR_STATE;
+    }
+}

@@ -90,6 +90,42 @@ __global__ void restrict_constant_kernel( int nf1, int nc1, const uint8_t* __res
     }
 }
 
+// coarse(X, Y, R) = fine(2X, 2Y, 2R): coefficient fields on coarser levels
+template < typename T >
+__global__ void inject_kernel( int nf1, int nc1, Ptr3< const T > src, Ptr3< T > dst, int ncomp )
+{
+    const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    const long long total = (long long) kDiamonds * nc1 * nc1 * nc1;
+    if ( t >= total )
+        return;
+    const int rc = int( t % nc1 ), yc = int( ( t / nc1 ) % nc1 ), xc = int( ( t / ( (long long) nc1 * nc1 ) ) % nc1 );
+    const int d  = int( t / ( (long long) nc1 * nc1 * nc1 ) );
+    for ( int c = 0; c < ncomp; ++c )
+        dst.p[c][t] = src.p[c][( ( size_t( d ) * nf1 + 2 * xc ) * nf1 + 2 * yc ) * nf1 + 2 * rc];
+}
+
+// tangential projection of 3-vectors at CMB / SURFACE nodes
+// (strong_algebraic_freeslip_enforcement_in_place, fe/strong_algebraic_freeslip_enforcement.hpp:23)
+template < typename T >
+__global__ void freeslip_project_kernel( int n1, const double* __restrict__ coords, Ptr3< T > y, int cmb, int surf )
+{
+    const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    const long long total = (long long) kDiamonds * n1 * n1 * 2;
+    if ( t >= total )
+        return;
+    const int    side = int( t & 1 );
+    const size_t lat  = size_t( t >> 1 );
+    if ( ( side == 0 && !cmb ) || ( side == 1 && !surf ) )
+        return;
+    const double* c = coords + lat * 3;
+    const double  m = sqrt( c[0] * c[0] + c[1] * c[1] + c[2] * c[2] );
+    const double  n[3] = { c[0] / m, c[1] / m, c[2] / m };
+    const size_t  i    = lat * n1 + ( side == 0 ? 0 : n1 - 1 );
+    const double  v[3] = { double( y.p[0][i] ), double( y.p[1][i] ), double( y.p[2][i] ) };
+    const double  dt   = n[0] * v[0] + n[1] * v[1] + n[2] * v[2];
+    y.p[0][i] = T( v[0] - dt * n[0] ), y.p[1][i] = T( v[1] - dt * n[1] ), y.p[2][i] = T( v[2] - dt * n[2] );
+}
+
 int check_levels( const tn_mesh* f, const tn_mesh* c, int ncomp )
 {
     TN_CHECK_ARG( f && c, "transfer: null mesh" );
@@ -143,6 +179,37 @@ int restrict_constant( const tn_mesh* f, const tn_mesh* c, int ncomp, int apply_
     return halo_sum< T >( c, dst, ncomp, st );
 }
 
+template < typename T >
+int inject( const tn_mesh* f, const tn_mesh* c, int ncomp, const T* const* src, T* const* dst, cudaStream_t st )
+{
+    int rc;
+    if ( ( rc = check_levels( f, c, ncomp ) ) )
+        return rc;
+    Ptr3< const T > s{};
+    Ptr3< T >       o{};
+    for ( int i = 0; i < ncomp; ++i )
+    {
+        TN_CHECK_ARG( src[i] && dst[i], "injection: null component" );
+        s.p[i] = src[i], o.p[i] = dst[i];
+    }
+    const long long n = (long long) c->ns;
+    inject_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( f->n1, c->n1, s, o, ncomp );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+template < typename T >
+int freeslip_project( const tn_mesh* m, T* const* y, int cmb, int surf, cudaStream_t st )
+{
+    TN_CHECK_ARG( m && y && y[0] && y[1] && y[2], "freeslip_project: null argument" );
+    const long long n = (long long) m->nlat * 2;
+    freeslip_project_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( m->n1, m->d_coords,
+                                                                                  Ptr3< T >{ { y[0], y[1], y[2] } },
+                                                                                  cmb, surf );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
 template int prolong_constant< double >( const tn_mesh*, const tn_mesh*, int, int, const double* const*,
                                          double* const*, cudaStream_t );
 template int prolong_constant< float >( const tn_mesh*, const tn_mesh*, int, int, const float* const*, float* const*,
@@ -165,6 +232,15 @@ extern "C" int tn_prolongation_constant_f32( const tn_mesh* f, const tn_mesh* c,
                                              const float* const* src, float* const* dst, void* s )
 {
     return prolong_constant< float >( f, c, ncomp, am, src, dst, as_stream( s ) );
+}
+extern "C" int tn_injection_f64( const tn_mesh* f, const tn_mesh* c, int ncomp, const double* const* src,
+                                 double* const* dst, void* s )
+{
+    return inject< double >( f, c, ncomp, src, dst, as_stream( s ) );
+}
+extern "C" int tn_freeslip_project_f64( const tn_mesh* m, double* const* y, int cmb, int surface, void* s )
+{
+    return freeslip_project< double >( m, y, cmb, surface, as_stream( s ) );
 }
 extern "C" int tn_restriction_constant_f64( const tn_mesh* f, const tn_mesh* c, int ncomp, const double* const* src,
                                             double* const* dst, void* s )

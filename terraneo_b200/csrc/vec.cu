@@ -55,6 +55,23 @@ __global__ void elementwise_kernel( size_t ns, int ncomp, Ptr3< T > y, Ptr3< con
     }
 }
 
+// Deterministic replacement of the reference's randomize (grid_operations.hpp:759),
+// whose XorShift pool assignment depends on thread scheduling: uniform values
+// in [-1, 1) from a splitmix64 hash of (seed, component, index).
+template < typename T >
+__global__ void randomize_kernel( size_t ns, Ptr3< T > y, unsigned long long seed )
+{
+    const int c = blockIdx.y;
+    for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
+    {
+        unsigned long long z = seed + 0x9E3779B97F4A7C15ull * ( ( unsigned long long ) c * ns + i + 1 );
+        z                    = ( z ^ ( z >> 30 ) ) * 0xBF58476D1CE4E5B9ull;
+        z                    = ( z ^ ( z >> 27 ) ) * 0x94D049BB133111EBull;
+        z                    = z ^ ( z >> 31 );
+        y.p[c][i]            = T( double( z >> 11 ) * ( 2.0 / 9007199254740992.0 ) - 1.0 );
+    }
+}
+
 template < typename TO, typename TI >
 __global__ void cast_kernel( size_t ns, int ncomp, Ptr3< TO > y, Ptr3< const TI > x )
 {
@@ -311,6 +328,26 @@ extern "C" int tn_vec_has_nan_or_inf_f64( const tn_mesh* m, int ncomp, const dou
 extern "C" int tn_vec_has_nan_or_inf_f32( const tn_mesh* m, int ncomp, const float* const* x, int* r, void* s )
 {
     return has_nan< float >( m, ncomp, x, r, s );
+}
+template < typename T >
+static int randomize( const tn_mesh* m, int ncomp, T* const* y, unsigned long long seed, void* s )
+{
+    TN_CHECK_ARG( m, "randomize: mesh is NULL" );
+    Ptr3< T > py;
+    int       rc;
+    if ( ( rc = ptr3( ncomp, y, py, "randomize" ) ) )
+        return rc;
+    randomize_kernel< T ><<< dim3( grid_for( m->ns ), ncomp ), kThreads, 0, as_stream( s ) >>>( m->ns, py, seed );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+extern "C" int tn_vec_randomize_f64( const tn_mesh* m, int ncomp, double* const* y, unsigned long long seed, void* s )
+{
+    return randomize< double >( m, ncomp, y, seed, s );
+}
+extern "C" int tn_vec_randomize_f32( const tn_mesh* m, int ncomp, float* const* y, unsigned long long seed, void* s )
+{
+    return randomize< float >( m, ncomp, y, seed, s );
 }
 extern "C" int tn_vec_cast_f64_to_f32( const tn_mesh* m, int ncomp, float* const* y, const double* const* x, void* s )
 {

@@ -241,6 +241,63 @@ class RestrictionVecConstant:
                 "restriction")
 
 
+def laplace_pcg(mesh, b, x, max_iterations=1000, relative_tolerance=1e-10, absolute_tolerance=1e-30):
+    """Unpreconditioned PCG (linalg/solvers/pcg.hpp:78) on Laplace(treat_boundary=True); x is updated in place.
+    Returns (iterations, relative residual)."""
+    it, rr = ctypes.c_int(), ctypes.c_double()
+    C.check(C.lib().tn_laplace_pcg_solve_f64(mesh.handle, ctypes.c_void_p(b.data.data_ptr()),
+                                             ctypes.c_void_p(x.data.data_ptr()), max_iterations, relative_tolerance,
+                                             absolute_tolerance, ctypes.byref(it), ctypes.byref(rr)), "laplace_pcg")
+    return it.value, rr.value
+
+
+class StokesSolver:
+    """FGMRES + block-triangular preconditioner + multigrid on the viscous block
+    (apps/mantlecirculation/mantlecirculation.cpp:486-735); mg_fp32 selects the FP32 V-cycle."""
+
+    def __init__(self, level, viscosity, mg_levels=4, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=True,
+                 chebyshev_order=3, smoothing_steps=2, power_iterations=10, vcycles=1, coarse_max_iterations=50,
+                 coarse_relative_tolerance=1e-6, restart=30, max_iterations=200, relative_tolerance=1e-8,
+                 absolute_tolerance=1e-30, r_min=0.55, r_max=1.0):
+        self.prm = C.StokesParams(level, mg_levels, bc_cmb, bc_surface, int(mg_fp32), chebyshev_order, smoothing_steps,
+                                  power_iterations, vcycles, coarse_max_iterations, coarse_relative_tolerance, restart,
+                                  max_iterations, relative_tolerance, absolute_tolerance)
+        h = ctypes.c_void_p()
+        C.check(C.lib().tn_stokes_solver_create(ctypes.byref(self.prm), r_min, r_max,
+                                                ctypes.c_void_p(viscosity.data.data_ptr()), ctypes.byref(h)),
+                "stokes_solver_create")
+        self._h = h
+
+    def solve(self, f_u, f_p, x_u, x_p):
+        it, rr = ctypes.c_int(), ctypes.c_double()
+        C.check(C.lib().tn_stokes_solve(self._h, f_u.comp_ptrs(), ctypes.c_void_p(f_p.data.data_ptr()),
+                                        x_u.comp_ptrs(), ctypes.c_void_p(x_p.data.data_ptr()), ctypes.byref(it),
+                                        ctypes.byref(rr)), "stokes_solve")
+        return it.value, rr.value
+
+    def history(self):
+        n, skips = ctypes.c_int(), ctypes.c_int()
+        C.check(C.lib().tn_stokes_history(self._h, None, 0, ctypes.byref(n), ctypes.byref(skips)), "history")
+        out = (ctypes.c_double * max(1, n.value))()
+        C.check(C.lib().tn_stokes_history(self._h, out, n.value, ctypes.byref(n), ctypes.byref(skips)), "history")
+        return list(out[:n.value]), skips.value
+
+    def apply(self, u, p, out_u, out_p):
+        C.check(C.lib().tn_stokes_apply(self._h, u.comp_ptrs(), ctypes.c_void_p(p.data.data_ptr()), out_u.comp_ptrs(),
+                                        ctypes.c_void_p(out_p.data.data_ptr())), "stokes_apply")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and C._lib is not None:
+            C.lib().tn_stokes_solver_destroy(h)
+            self._h = None
+
+
+def freeslip_project(u, cmb=True, surface=True):
+    C.check(C.lib().tn_freeslip_project_f64(u.mesh.handle, u.comp_ptrs(), int(cmb), int(surface), _stream()),
+            "freeslip_project")
+
+
 def apply(op, src, dst):
     """linalg::apply (linalg/operator.hpp:156)."""
     op.apply_impl(src, dst)
