@@ -199,6 +199,8 @@ class Multigrid
       tmp_r_( std::move( tmp_r ) ), tmp_e_( std::move( tmp_e ) ), tmp_( std::move( tmp ) ),
       smoothers_( std::move( smoothers ) ), coarse_( std::move( coarse ) ), cycles_( cycles )
     {
+        if ( A_c_.empty() )
+            throw std::runtime_error( "Multigrid: needs at least one coarse level" );
         if ( P_.size() != A_c_.size() || R_.size() != A_c_.size() || tmp_r_.size() != A_c_.size() ||
              tmp_e_.size() != A_c_.size() || tmp_.size() != A_c_.size() + 1 || smoothers_.size() != A_c_.size() + 1 )
             throw std::runtime_error( "Multigrid: inconsistent level sizes" );

@@ -176,8 +176,8 @@ extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min,
 {
     TN_CHECK_ARG( p && k && out, "tn_stokes_solver_create: null argument" );
     *out = nullptr;
-    TN_CHECK_ARG( p->mg_levels >= 1 && p->level - p->mg_levels + 1 >= 2 && p->level <= 8,
-                  "tn_stokes_solver_create: need level - mg_levels + 1 >= 2 (tiled coarsest operator) and level <= 8" );
+    TN_CHECK_ARG( p->mg_levels >= 2 && p->level - p->mg_levels + 1 >= 2 && p->level <= 8,
+                  "tn_stokes_solver_create: need mg_levels >= 2, level - mg_levels + 1 >= 2 and level <= 8" );
     TN_CHECK_ARG( p->restart >= 1 && p->max_iterations >= 1, "tn_stokes_solver_create: bad Krylov parameters" );
     try
     {

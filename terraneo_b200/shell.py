@@ -53,7 +53,7 @@ class ShellMesh:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value and C._lib is not None:
+        if h is not None and h.value and C is not None and C._lib is not None:
             C.lib().tn_mesh_destroy(h)
             self._h = None
 
@@ -288,7 +288,7 @@ class StokesSolver:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value and C._lib is not None:
+        if h is not None and h.value and C is not None and C._lib is not None:
             C.lib().tn_stokes_solver_destroy(h)
             self._h = None
 
