@@ -183,6 +183,14 @@ TN_API int tn_vec_mult_f32( const tn_mesh* mesh, int ncomp, float* const* y, con
 TN_API int tn_vec_max_abs_f64( const tn_mesh* mesh, int ncomp, const double* const* x, double* result, void* stream );
 TN_API int tn_vec_has_nan_or_inf_f64( const tn_mesh* mesh, int ncomp, const double* const* x, int* result, void* stream );
 TN_API int tn_vec_has_nan_or_inf_f32( const tn_mesh* mesh, int ncomp, const float* const* x, int* result, void* stream );
+/* One fused Chebyshev step (linalg/solvers/chebyshev.hpp:127-160):
+ * d = alpha D^{-1} (b - ax) + beta d;  x = x + d.  beta = 0 does not read d. */
+TN_API int tn_vec_chebyshev_step_f64( const tn_mesh* mesh, int ncomp, double* const* x, double* const* d,
+                                      const double* const* b, const double* const* ax, const double* const* inv_diag,
+                                      double alpha, double beta, void* stream );
+TN_API int tn_vec_chebyshev_step_f32( const tn_mesh* mesh, int ncomp, float* const* x, float* const* d,
+                                      const float* const* b, const float* const* ax, const float* const* inv_diag,
+                                      double alpha, double beta, void* stream );
 /* randomize (grid_operations.hpp:759) made deterministic: uniform [-1, 1)
  * from a counter-based hash of (seed, component, index). */
 TN_API int tn_vec_randomize_f64( const tn_mesh* mesh, int ncomp, double* const* y, unsigned long long seed,
@@ -190,6 +198,52 @@ TN_API int tn_vec_randomize_f64( const tn_mesh* mesh, int ncomp, double* const* 
 TN_API int tn_vec_randomize_f32( const tn_mesh* mesh, int ncomp, float* const* y, unsigned long long seed, void* stream );
 TN_API int tn_vec_cast_f64_to_f32( const tn_mesh* mesh, int ncomp, float* const* y, const double* const* x, void* stream );
 TN_API int tn_vec_cast_f32_to_f64( const tn_mesh* mesh, int ncomp, double* const* y, const float* const* x, void* stream );
+
+/* ---------------------------------------------------------------------------
+ * Device-resident Krylov steps (no host synchronisation).
+ *
+ * A Krylov vector is passed as `nseg` (1..4) scalar fields, field k living on
+ * mesh[k] (stored-node length, reduced over mesh[k]'s owned nodes): a
+ * velocity field is 3 segments, the Stokes block vector (velocity on the fine
+ * mesh, pressure on the coarse one; linalg/vector_q1isoq2_q1.hpp:19) is 4.
+ * Scalars (`coeff`, `gate`, `result`, `state`) are DEVICE pointers.  These
+ * restate the host loops of linalg/solvers/fgmres.hpp:197-229 and
+ * linalg/solvers/pcg.hpp:78-102 with their scalars kept on the device; the
+ * reference has no C entry point of this shape.
+ *
+ * axpy_dot: if gate != NULL and *gate != 0 does nothing; otherwise
+ *   w = w - coeff[0] * x  (skipped when x == NULL), then
+ *   result[0] = <w, v>    (v == NULL: <w, w>), compensated FP64.
+ * Chaining these gives one pass per modified Gram-Schmidt step. */
+TN_API int tn_krylov_axpy_dot_f64( int nseg, const tn_mesh* const* mesh, double* const* w, const double* const* x,
+                                   const double* coeff, const double* const* v, const double* gate, double* result,
+                                   void* stream );
+TN_API int tn_krylov_axpy_dot_f32( int nseg, const tn_mesh* const* mesh, float* const* w, const float* const* x,
+                                   const double* coeff, const float* const* v, const double* gate, double* result,
+                                   void* stream );
+
+/* Unpreconditioned PCG (pcg.hpp:78-102; z = r) with its state in device
+ * memory.  state is a device array of at least 8 + max_iterations + 1
+ * doubles: [0] <r,r>, [1] <Ap,p>, [2] |r0|, [3] beta, [4] done flag (0/1),
+ * [5] iterations, [6] last relative residual, [8 + k] relative residual after
+ * iteration k ([8] = 1).  One iteration k (1-based) is
+ *     ap = A p                (any operator apply; runs regardless of done)
+ *     tn_pcg_pap_f64          <ap, p>
+ *     tn_pcg_update_f64(k)    x += alpha p, r -= alpha ap, stopping rule, beta
+ *     tn_pcg_direction_f64    p = r + beta p
+ * after tn_pcg_begin_f64 on r = b - A x.  Once the stopping rule fires
+ * (relres <= rtol or |r| < atol; begin: |r0| < atol) every later step leaves
+ * x, r, p and state untouched, so a caller may read the flag only now and
+ * then, or issue all iterations. */
+TN_API int tn_pcg_begin_f64( int nseg, const tn_mesh* const* mesh, const double* const* r, double* const* p,
+                             double* state, double atol, void* stream );
+TN_API int tn_pcg_pap_f64( int nseg, const tn_mesh* const* mesh, const double* const* ap, const double* const* p,
+                           double* state, void* stream );
+TN_API int tn_pcg_update_f64( int nseg, const tn_mesh* const* mesh, double* const* x, double* const* r,
+                              const double* const* p, const double* const* ap, double* state, int iteration,
+                              double rtol, double atol, void* stream );
+TN_API int tn_pcg_direction_f64( int nseg, const tn_mesh* const* mesh, double* const* p, const double* const* r,
+                                 const double* state, void* stream );
 
 /* ---------------------------------------------------------------------------
  * Solver drivers.

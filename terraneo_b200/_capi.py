@@ -65,6 +65,15 @@ _SIGS = {
     "tn_kmass_apply_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "tn_injection_f64": (c_int, [c_void_p, c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
     "tn_freeslip_project_f64": (c_int, [c_void_p, P(c_void_p), c_int, c_int, c_void_p]),
+    "tn_krylov_axpy_dot_f64": (c_int, [c_int, P(c_void_p), P(c_void_p), P(c_void_p), c_void_p, P(c_void_p), c_void_p,
+                                       c_void_p, c_void_p]),
+    "tn_krylov_axpy_dot_f32": (c_int, [c_int, P(c_void_p), P(c_void_p), P(c_void_p), c_void_p, P(c_void_p), c_void_p,
+                                       c_void_p, c_void_p]),
+    "tn_pcg_begin_f64": (c_int, [c_int, P(c_void_p), P(c_void_p), P(c_void_p), c_void_p, c_double, c_void_p]),
+    "tn_pcg_pap_f64": (c_int, [c_int, P(c_void_p), P(c_void_p), P(c_void_p), c_void_p, c_void_p]),
+    "tn_pcg_update_f64": (c_int, [c_int, P(c_void_p), P(c_void_p), P(c_void_p), P(c_void_p), P(c_void_p), c_void_p,
+                                  c_int, c_double, c_double, c_void_p]),
+    "tn_pcg_direction_f64": (c_int, [c_int, P(c_void_p), P(c_void_p), P(c_void_p), c_void_p, c_void_p]),
     "tn_laplace_pcg_solve_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, P(c_int),
                                          P(c_double)]),
     "tn_stokes_solver_create": (c_int, [P(StokesParams), c_double, c_double, c_void_p, P(c_void_p)]),
@@ -83,6 +92,10 @@ _SIGS = {
     "tn_vec_max_abs_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_double), c_void_p]),
     "tn_vec_has_nan_or_inf_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), c_void_p]),
     "tn_vec_has_nan_or_inf_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), c_void_p]),
+    "tn_vec_chebyshev_step_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_void_p), P(c_void_p),
+                                          P(c_void_p), c_double, c_double, c_void_p]),
+    "tn_vec_chebyshev_step_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_void_p), P(c_void_p),
+                                          P(c_void_p), c_double, c_double, c_void_p]),
     "tn_vec_randomize_f64": (c_int, [c_void_p, c_int, P(c_void_p), ctypes.c_ulonglong, c_void_p]),
     "tn_vec_randomize_f32": (c_int, [c_void_p, c_int, P(c_void_p), ctypes.c_ulonglong, c_void_p]),
     "tn_vec_cast_f64_to_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),

@@ -7,9 +7,9 @@
 // (linalg/vector.hpp:8-37).  Free functions lincomb / dot / assign / apply /
 // solve mirror linalg/vector.hpp:72-250 and linalg/operator.hpp:156.
 //
-// Every call is asynchronous on the library's default stream except those
-// that return a host value (dot, max_abs_entry, has_nan_or_inf), which
-// synchronise, keeping the reference's synchronous semantics.
+// Every call is asynchronous on tn::stream() except those that return a host
+// value (dot, max_abs_entry, has_nan_or_inf), which synchronise, keeping the
+// reference's synchronous semantics.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -30,6 +30,16 @@ inline void check( int rc, const char* what )
     if ( rc != TN_OK )
         throw std::runtime_error( std::string( what ) + ": " + tn_last_error() );
 }
+
+// The stream every call of this layer is issued on (default: the legacy
+// default stream).  A solver may switch it for the duration of a solve, e.g.
+// to capture a preconditioner into a CUDA graph.
+inline cudaStream_t& stream_ref()
+{
+    static thread_local cudaStream_t s = nullptr;
+    return s;
+}
+inline cudaStream_t stream() { return stream_ref(); }
 
 // shared device allocation
 template < typename T >
@@ -89,6 +99,7 @@ struct abi< double >
     static constexpr auto mult     = tn_vec_mult_f64;
     static constexpr auto has_nan  = tn_vec_has_nan_or_inf_f64;
     static constexpr auto rand     = tn_vec_randomize_f64;
+    static constexpr auto cheb     = tn_vec_chebyshev_step_f64;
     static constexpr auto halo     = tn_halo_sum_f64;
 };
 template <>
@@ -100,6 +111,7 @@ struct abi< float >
     static constexpr auto mult     = tn_vec_mult_f32;
     static constexpr auto has_nan  = tn_vec_has_nan_or_inf_f32;
     static constexpr auto rand     = tn_vec_randomize_f32;
+    static constexpr auto cheb     = tn_vec_chebyshev_step_f32;
     static constexpr auto halo     = tn_halo_sum_f32;
 };
 inline unsigned long long& rand_counter()
@@ -157,7 +169,7 @@ class VectorQ1Base
             for ( int k = 0; k < NC; ++k )
                 xs[3 * i + k] = x[i].comp( k );
         }
-        check( detail::abi< T >::lincomb( mesh_.get(), NC, y, double( c0 ), int( x.size() ), cc, xs, nullptr ),
+        check( detail::abi< T >::lincomb( mesh_.get(), NC, y, double( c0 ), int( x.size() ), cc, xs, stream() ),
                "lincomb" );
     }
     T dot_impl( const VectorQ1Base& x ) const
@@ -165,33 +177,33 @@ class VectorQ1Base
         const T* a[3] = { comp( 0 ), NC > 1 ? comp( 1 ) : nullptr, NC > 2 ? comp( 2 ) : nullptr };
         const T* b[3] = { x.comp( 0 ), NC > 1 ? x.comp( 1 ) : nullptr, NC > 2 ? x.comp( 2 ) : nullptr };
         double   r    = 0;
-        check( detail::abi< T >::dot( mesh_.get(), NC, a, b, &r, nullptr ), "dot" );
+        check( detail::abi< T >::dot( mesh_.get(), NC, a, b, &r, stream() ), "dot" );
         return T( r );
     }
     void invert_entries_impl()
     {
         T* y[3];
         ptrs( y );
-        check( detail::abi< T >::invert( mesh_.get(), NC, y, nullptr ), "invert" );
+        check( detail::abi< T >::invert( mesh_.get(), NC, y, stream() ), "invert" );
     }
     void scale_with_vector_impl( const VectorQ1Base& x )
     {
         T*       y[3];
         const T* xs[3] = { x.comp( 0 ), NC > 1 ? x.comp( 1 ) : nullptr, NC > 2 ? x.comp( 2 ) : nullptr };
         ptrs( y );
-        check( detail::abi< T >::mult( mesh_.get(), NC, y, xs, nullptr ), "scale_with_vector" );
+        check( detail::abi< T >::mult( mesh_.get(), NC, y, xs, stream() ), "scale_with_vector" );
     }
     void randomize_impl()
     {
         T* y[3];
         ptrs( y );
-        check( detail::abi< T >::rand( mesh_.get(), NC, y, detail::rand_counter()++, nullptr ), "randomize" );
+        check( detail::abi< T >::rand( mesh_.get(), NC, y, detail::rand_counter()++, stream() ), "randomize" );
     }
     bool has_nan_or_inf_impl() const
     {
         const T* a[3] = { comp( 0 ), NC > 1 ? comp( 1 ) : nullptr, NC > 2 ? comp( 2 ) : nullptr };
         int      r    = 0;
-        check( detail::abi< T >::has_nan( mesh_.get(), NC, a, &r, nullptr ), "has_nan_or_inf" );
+        check( detail::abi< T >::has_nan( mesh_.get(), NC, a, &r, stream() ), "has_nan_or_inf" );
         return r != 0;
     }
     void swap_impl( VectorQ1Base& o ) { std::swap( buf_, o.buf_ ); }
@@ -199,11 +211,11 @@ class VectorQ1Base
     {
         T* y[3];
         ptrs( y );
-        check( detail::abi< T >::halo( mesh_.get(), y, NC, nullptr ), "halo_sum" );
+        check( detail::abi< T >::halo( mesh_.get(), y, NC, stream() ), "halo_sum" );
     }
     void copy_from( const VectorQ1Base& o )
     {
-        if ( cudaMemcpyAsync( data(), o.data(), sizeof( T ) * size(), cudaMemcpyDeviceToDevice, nullptr ) != cudaSuccess )
+        if ( cudaMemcpyAsync( data(), o.data(), sizeof( T ) * size(), cudaMemcpyDeviceToDevice, stream() ) != cudaSuccess )
             throw std::runtime_error( "copy_from: cudaMemcpyAsync failed" );
     }
 
@@ -269,6 +281,56 @@ class VectorQ1IsoQ2Q1
     Block2Type p_;
 };
 
+// A vector as a list of scalar-field segments (one per component and block)
+// for the device-resident Krylov steps tn_krylov_axpy_dot_* / tn_pcg_*.
+template < typename T >
+struct Segments
+{
+    int            n = 0;
+    const tn_mesh* mesh[4]{};
+    T*             f[4]{};
+};
+template < typename T, int NC >
+void add_segments( const VectorQ1Base< T, NC >& v, Segments< T >& s )
+{
+    for ( int c = 0; c < NC; ++c )
+    {
+        if ( s.n >= 4 )
+            throw std::runtime_error( "segments: more than 4 fields" );
+        s.mesh[s.n] = v.mesh().get();
+        s.f[s.n++]  = v.comp( c );
+    }
+}
+template < typename T >
+void add_segments( const VectorQ1IsoQ2Q1< T >& v, Segments< T >& s )
+{
+    add_segments( v.block_1(), s );
+    add_segments( v.block_2(), s );
+}
+template < typename V >
+Segments< typename V::ScalarType > segments( const V& v )
+{
+    Segments< typename V::ScalarType > s;
+    add_segments( v, s );
+    return s;
+}
+
+// w = w - coeff[0] x (x != NULL); result[0] = <w, v> (v == NULL: <w, w>).
+// coeff, gate and result are device pointers; no synchronisation.
+template < typename T >
+void axpy_dot( const Segments< T >& w, const Segments< T >* x, const double* coeff, const Segments< T >* v,
+               const double* gate, double* result )
+{
+    const T* const* px = x ? x->f : nullptr;
+    const T* const* pv = v ? v->f : nullptr;
+    if constexpr ( std::is_same_v< T, double > )
+        check( tn_krylov_axpy_dot_f64( w.n, w.mesh, w.f, const_cast< const T* const* >( px ), coeff, pv, gate, result,
+                                       stream() ),
+               "axpy_dot" );
+    else
+        check( tn_krylov_axpy_dot_f32( w.n, w.mesh, w.f, px, coeff, pv, gate, result, stream() ), "axpy_dot" );
+}
+
 // free functions (linalg/vector.hpp:72-250)
 template < typename V >
 void lincomb( V& y, const std::vector< typename V::ScalarType >& c, const std::vector< V >& x,
@@ -329,20 +391,39 @@ void solve( Solver& s, Op& A, X& x, const B& b )
     s.solve_impl( A, x, b );
 }
 
+// One fused Chebyshev step: d = alpha D^{-1} (b - ax) + beta d, x += d
+template < typename T, int NC >
+void chebyshev_step( VectorQ1Base< T, NC >& x, VectorQ1Base< T, NC >& d, const VectorQ1Base< T, NC >& b,
+                     const VectorQ1Base< T, NC >& ax, const VectorQ1Base< T, NC >& inv_diag, double alpha,
+                     double beta )
+{
+    T *      px[3], *pd[3];
+    const T *pb[3], *pa[3], *pi[3];
+    x.ptrs( px );
+    d.ptrs( pd );
+    for ( int c = 0; c < 3; ++c )
+    {
+        pb[c] = c < NC ? b.comp( c ) : nullptr;
+        pa[c] = c < NC ? ax.comp( c ) : nullptr;
+        pi[c] = c < NC ? inv_diag.comp( c ) : nullptr;
+    }
+    check( detail::abi< T >::cheb( x.mesh().get(), NC, px, pd, pb, pa, pi, alpha, beta, stream() ), "chebyshev_step" );
+}
+
 // FP64 <-> FP32 copies for the mixed-precision preconditioner
 inline void cast( VectorQ1Vec< float >& y, const VectorQ1Vec< double >& x )
 {
     float*        yp[3];
     const double* xp[3] = { x.comp( 0 ), x.comp( 1 ), x.comp( 2 ) };
     y.ptrs( yp );
-    check( tn_vec_cast_f64_to_f32( y.mesh().get(), 3, yp, xp, nullptr ), "cast" );
+    check( tn_vec_cast_f64_to_f32( y.mesh().get(), 3, yp, xp, stream() ), "cast" );
 }
 inline void cast( VectorQ1Vec< double >& y, const VectorQ1Vec< float >& x )
 {
     double*      yp[3];
     const float* xp[3] = { x.comp( 0 ), x.comp( 1 ), x.comp( 2 ) };
     y.ptrs( yp );
-    check( tn_vec_cast_f32_to_f64( y.mesh().get(), 3, yp, xp, nullptr ), "cast" );
+    check( tn_vec_cast_f32_to_f64( y.mesh().get(), 3, yp, xp, stream() ), "cast" );
 }
 
 }  // namespace tn

@@ -58,9 +58,9 @@ class EpsilonDivDivKerngen
         T*       d[3];
         dst.ptrs( d );
         if constexpr ( std::is_same_v< T, double > )
-            check( tn_epsdivdiv_apply_f64( mesh_.get(), &p_, k_.comp( 0 ), s, d, nullptr ), "epsdivdiv apply" );
+            check( tn_epsdivdiv_apply_f64( mesh_.get(), &p_, k_.comp( 0 ), s, d, stream() ), "epsdivdiv apply" );
         else
-            check( tn_epsdivdiv_apply_f32( mesh_.get(), &p_, k_.comp( 0 ), s, d, nullptr ), "epsdivdiv apply" );
+            check( tn_epsdivdiv_apply_f32( mesh_.get(), &p_, k_.comp( 0 ), s, d, stream() ), "epsdivdiv apply" );
     }
 
   private:
@@ -86,11 +86,11 @@ class Laplace
     {
         if constexpr ( std::is_same_v< T, double > )
             check( tn_laplace_apply_f64( mesh_.get(), treat_, diag_, int( am_ ), int( cm_ ), src.comp( 0 ), dst.comp( 0 ),
-                                         nullptr ),
+                                         stream() ),
                    "laplace apply" );
         else
             check( tn_laplace_apply_f32( mesh_.get(), treat_, diag_, int( am_ ), int( cm_ ), src.comp( 0 ), dst.comp( 0 ),
-                                         nullptr ),
+                                         stream() ),
                    "laplace apply" );
     }
 
@@ -121,11 +121,11 @@ class Gradient
         dst.ptrs( d );
         if constexpr ( std::is_same_v< T, double > )
             check( tn_gradient_apply_f64( mu_.get(), mp_.get(), bcs_.cmb, bcs_.surface, int( am_ ), int( cm_ ),
-                                          src.comp( 0 ), d, nullptr ),
+                                          src.comp( 0 ), d, stream() ),
                    "gradient apply" );
         else
             check( tn_gradient_apply_f32( mu_.get(), mp_.get(), bcs_.cmb, bcs_.surface, int( am_ ), int( cm_ ),
-                                          src.comp( 0 ), d, nullptr ),
+                                          src.comp( 0 ), d, stream() ),
                    "gradient apply" );
     }
 
@@ -155,11 +155,11 @@ class Divergence
         const T* s[3] = { src.comp( 0 ), src.comp( 1 ), src.comp( 2 ) };
         if constexpr ( std::is_same_v< T, double > )
             check( tn_divergence_apply_f64( mu_.get(), mp_.get(), bcs_.cmb, bcs_.surface, int( am_ ), int( cm_ ), s,
-                                            dst.comp( 0 ), nullptr ),
+                                            dst.comp( 0 ), stream() ),
                    "divergence apply" );
         else
             check( tn_divergence_apply_f32( mu_.get(), mp_.get(), bcs_.cmb, bcs_.surface, int( am_ ), int( cm_ ), s,
-                                            dst.comp( 0 ), nullptr ),
+                                            dst.comp( 0 ), stream() ),
                    "divergence apply" );
     }
 
@@ -230,9 +230,9 @@ class ProlongationVecConstant
         T*       d[3];
         dst.ptrs( d );
         if constexpr ( std::is_same_v< T, double > )
-            check( tn_prolongation_constant_f64( f_.get(), c_.get(), 3, int( am_ ), s, d, nullptr ), "prolongation" );
+            check( tn_prolongation_constant_f64( f_.get(), c_.get(), 3, int( am_ ), s, d, stream() ), "prolongation" );
         else
-            check( tn_prolongation_constant_f32( f_.get(), c_.get(), 3, int( am_ ), s, d, nullptr ), "prolongation" );
+            check( tn_prolongation_constant_f32( f_.get(), c_.get(), 3, int( am_ ), s, d, stream() ), "prolongation" );
     }
 
   private:
@@ -253,9 +253,9 @@ class RestrictionVecConstant
         T*       d[3];
         dst.ptrs( d );
         if constexpr ( std::is_same_v< T, double > )
-            check( tn_restriction_constant_f64( f_.get(), c_.get(), 3, s, d, nullptr ), "restriction" );
+            check( tn_restriction_constant_f64( f_.get(), c_.get(), 3, s, d, stream() ), "restriction" );
         else
-            check( tn_restriction_constant_f32( f_.get(), c_.get(), 3, s, d, nullptr ), "restriction" );
+            check( tn_restriction_constant_f32( f_.get(), c_.get(), 3, s, d, stream() ), "restriction" );
     }
 
   private:
@@ -276,11 +276,11 @@ class KMass
     {
         if constexpr ( std::is_same_v< T, double > )
             check( tn_kmass_apply_f64( mesh_.get(), k_.comp( 0 ), mode_, TN_APPLY_REPLACE, TN_COMM_ADDITIVE,
-                                       src.comp( 0 ), dst.comp( 0 ), nullptr ),
+                                       src.comp( 0 ), dst.comp( 0 ), stream() ),
                    "kmass apply" );
         else
             check( tn_kmass_apply_f32( mesh_.get(), k_.comp( 0 ), mode_, TN_APPLY_REPLACE, TN_COMM_ADDITIVE,
-                                       src.comp( 0 ), dst.comp( 0 ), nullptr ),
+                                       src.comp( 0 ), dst.comp( 0 ), stream() ),
                    "kmass apply" );
     }
 

@@ -108,6 +108,81 @@ class PCG
     Prec                      prec_;
 };
 
+// PCG with an identity preconditioner whose scalars live in device memory
+// (tn_pcg_* in the C ABI): the same iteration and stopping rule as PCG above
+// (pcg.hpp:78-102 with z = r), issued without a host round trip per
+// iteration.  The done flag is read every `check_every` iterations unless the
+// stream is being captured, in which case all max_iterations are issued and
+// the gated steps leave the converged iterate untouched.
+template < typename Op >
+class DevicePCG
+{
+  public:
+    using V = typename Op::SrcVectorType;
+    DevicePCG( IterativeSolverParameters prm, std::vector< V > tmps, int check_every = 8 )
+    : prm_( prm ), tmps_( std::move( tmps ) ), check_every_( check_every ),
+      state_( device_alloc< double >( 8 + size_t( std::max( prm.max_iterations, 0 ) ) + 1 ) )
+    {
+        if ( tmps_.size() < 3 )
+            throw std::runtime_error( "DevicePCG: needs 3 temporary vectors" );
+    }
+    void solve_impl( Op& A, V& x, const V& b )
+    {
+        auto& r  = tmps_[0];
+        auto& p  = tmps_[1];
+        auto& ap = tmps_[2];
+        apply( A, x, r );
+        lincomb( r, { 1.0, -1.0 }, { b, r } );
+        const auto sx = segments( x ), sr = segments( r ), sp = segments( p ), sap = segments( ap );
+        double*    st = state_.get();
+        check( tn_pcg_begin_f64( sr.n, sr.mesh, sr.f, sp.f, st, prm_.absolute_residual_tolerance, stream() ),
+               "pcg_begin" );
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing( stream(), &cs );
+        const bool capturing = cs != cudaStreamCaptureStatusNone;
+        for ( int it = 1; it <= prm_.max_iterations; ++it )
+        {
+            if ( !capturing && ( it == 1 || ( it - 1 ) % check_every_ == 0 ) && done() )
+                break;
+            apply( A, p, ap );
+            check( tn_pcg_pap_f64( sp.n, sp.mesh, sap.f, sp.f, st, stream() ), "pcg_pap" );
+            check( tn_pcg_update_f64( sx.n, sx.mesh, sx.f, sr.f, sp.f, sap.f, st, it, prm_.relative_residual_tolerance,
+                                      prm_.absolute_residual_tolerance, stream() ),
+                   "pcg_update" );
+            check( tn_pcg_direction_f64( sp.n, sp.mesh, sp.f, sr.f, st, stream() ), "pcg_direction" );
+        }
+    }
+    // statistics of the last solve (synchronises)
+    SolverStatistics statistics() const
+    {
+        const size_t          n = 8 + size_t( std::max( prm_.max_iterations, 0 ) ) + 1;
+        std::vector< double > h( n );
+        if ( cudaMemcpyAsync( h.data(), state_.get(), n * sizeof( double ), cudaMemcpyDeviceToHost, stream() ) !=
+                 cudaSuccess ||
+             cudaStreamSynchronize( stream() ) != cudaSuccess )
+            throw std::runtime_error( "DevicePCG: reading the state failed" );
+        SolverStatistics out;
+        out.iterations = int( h[5] );
+        out.relative_residuals.assign( h.begin() + 8, h.begin() + 8 + out.iterations + 1 );
+        return out;
+    }
+
+  private:
+    bool done() const
+    {
+        double f = 0;
+        if ( cudaMemcpyAsync( &f, state_.get() + 4, sizeof( double ), cudaMemcpyDeviceToHost, stream() ) !=
+                 cudaSuccess ||
+             cudaStreamSynchronize( stream() ) != cudaSuccess )
+            throw std::runtime_error( "DevicePCG: reading the done flag failed" );
+        return f != 0.0;
+    }
+    IterativeSolverParameters  prm_;
+    std::vector< V >           tmps_;
+    int                        check_every_;
+    std::shared_ptr< double >  state_;
+};
+
 // power_iteration (power_iteration.hpp:13-48) from a deterministic random start
 template < typename Op, typename V >
 double power_iteration( Op& op, V& it, V& aux, int iterations )
@@ -154,24 +229,19 @@ class Chebyshev
         const double lmax  = 1.5 * ev_, lmin = 0.1 * ev_;
         const double theta = 0.5 * ( lmax + lmin ), delta = 0.5 * ( lmax - lmin );
         const double sigma = theta / delta;
-        using S            = typename V::ScalarType;
         double rho         = 1.0 / sigma; // carried across sweeps as in the reference (chebyshev.hpp:119)
         for ( int it = 0; it < iterations_; ++it )
         {
+            // z = A x;  d = D^{-1}(b - z) / theta;  x += d   (one fused vector pass)
             apply( A, x, z );
-            lincomb( z, { S( 1 ), S( -1 ) }, { b, z } );
-            scale_in_place( z, inv_diag_ );
-            lincomb( d, { S( 1.0 / theta ) }, { z } );
-            lincomb( x, { S( 1 ), S( 1 ) }, { x, d } );
+            chebyshev_step( x, d, b, z, inv_diag_, 1.0 / theta, 0.0 );
             for ( int i = 2; i <= order_; ++i )
             {
                 const double rho_new = 1.0 / ( 2.0 * sigma - rho );
                 const double beta = rho_new * rho, alpha = 2.0 * rho_new / delta;
+                // z = A x;  d = alpha D^{-1}(b - z) + beta d;  x += d
                 apply( A, x, z );
-                lincomb( z, { S( 1 ), S( -1 ) }, { b, z } );
-                scale_in_place( z, inv_diag_ );
-                lincomb( d, { S( alpha ), S( beta ) }, { z, d } );
-                lincomb( x, { S( 1 ), S( 1 ) }, { x, d } );
+                chebyshev_step( x, d, b, z, inv_diag_, alpha, beta );
                 rho = rho_new;
             }
         }
@@ -280,6 +350,8 @@ class FGMRES
     {
         if ( int( tmp_.size() ) < 2 * m_ + 4 )
             throw std::runtime_error( "FGMRES: needs 2 * restart + 4 temporary vectors" );
+        hdev_ = device_alloc< double >( size_t( m_ ) + 2 );
+        hhost_.assign( size_t( m_ ) + 2, 0.0 );
     }
     SolverStatistics stats;
     int              preconditioner_skips = 0;
@@ -322,13 +394,26 @@ class FGMRES
                 }
                 auto& w = tmp_[idxW];
                 apply( A, zj, w );
-                for ( int i = 0; i <= j; ++i )
+                // modified Gram-Schmidt (fgmres.hpp:197-209): h_ij = <w, v_i>,
+                // w -= h_ij v_i for i = 0..j, then |w|; each pass fuses the
+                // update by v_{i-1} with the projection on v_i and the
+                // coefficients stay on the device until one read at the end.
+                const auto sw = segments( w );
+                double*    hd = hdev_.get();
+                for ( int i = 0; i <= j + 1; ++i )
                 {
-                    const double hij = double( dot( w, tmp_[offV + i] ) );
-                    h( i, j )        = hij;
-                    lincomb( w, { S( 1 ), S( -hij ) }, { w, tmp_[offV + i] } );
+                    const auto sv = segments( tmp_[offV + std::min( i, j )] );
+                    const auto su = segments( tmp_[offV + std::max( i - 1, 0 )] );
+                    axpy_dot( sw, i > 0 ? &su : nullptr, i > 0 ? hd + i - 1 : nullptr, i <= j ? &sv : nullptr,
+                              nullptr, hd + i );
                 }
-                const double hj1 = std::sqrt( double( dot( w, w ) ) );
+                if ( cudaMemcpyAsync( hhost_.data(), hd, sizeof( double ) * ( j + 2 ), cudaMemcpyDeviceToHost,
+                                      stream() ) != cudaSuccess ||
+                     cudaStreamSynchronize( stream() ) != cudaSuccess )
+                    throw std::runtime_error( "FGMRES: reading the Hessenberg column failed" );
+                for ( int i = 0; i <= j; ++i )
+                    h( i, j ) = hhost_[i];
+                const double hj1 = std::sqrt( hhost_[j + 1] );
                 if ( hj1 < std::numeric_limits< double >::epsilon() * r0 )
                 {
                     h( j + 1, j ) = 0;
@@ -390,6 +475,8 @@ class FGMRES
     double true_relative_residual = 1.0;
 
   private:
+    std::shared_ptr< double > hdev_;
+    std::vector< double >     hhost_;
     std::vector< V >          tmp_;
     int                       m_;
     IterativeSolverParameters prm_;

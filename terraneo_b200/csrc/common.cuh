@@ -77,6 +77,7 @@ struct tn_mesh
     float*   d_coords32 = nullptr;
     float*   d_radii32  = nullptr;
     uint8_t* d_lat_owned = nullptr; // lateral ownership (same for every r)
+    uint8_t* d_node_owned = nullptr; // per stored node, for flat reductions
 
     // duplicated lateral positions, CSR: members of group g are
     // halo_members[halo_offsets[g] .. halo_offsets[g+1]) as lateral indices

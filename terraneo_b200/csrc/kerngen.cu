@@ -937,8 +937,13 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
                            skip_surf,
                            fsfs ? m->d_red_result + 3 : nullptr };
         const size_t smem = tile_smem_bytes< T >( m->n1, seg );
-        TN_CUDA_TRY( cudaFuncSetAttribute( kerngen_tile_kernel< T >, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           int( smem ) ) );
+        static int smem_attr[2] = { 0, 0 }; // largest dynamic shared memory requested so far (per precision)
+        if ( int( smem ) > smem_attr[sizeof( T ) == 8] )
+        {
+            TN_CUDA_TRY( cudaFuncSetAttribute( kerngen_tile_kernel< T >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               int( smem ) ) );
+            smem_attr[sizeof( T ) == 8] = int( smem );
+        }
         kerngen_tile_kernel< T ><<< grid, kThreads, smem, st >>>( P );
         TN_LAUNCH_CHECK();
         if ( skip_cmb || skip_surf )

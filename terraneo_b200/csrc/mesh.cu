@@ -237,6 +237,9 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
         std::memcpy( m->penalty_gram_inv, inv, sizeof( inv ) );
     }
 
+    std::vector< uint8_t > node_owned( m->ns );
+    for ( size_t l = 0; l < m->nlat; ++l )
+        std::memset( node_owned.data() + l * m->n1, m->h_lat_owned[l], m->n1 );
     int rc;
     std::vector< float > c32( m->h_coords.begin(), m->h_coords.end() ), r32( m->h_radii.begin(), m->h_radii.end() );
     if ( ( rc = upload( m->h_coords.data(), m->h_coords.size(), &m->d_coords ) ) ||
@@ -244,6 +247,7 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
          ( rc = upload( c32.data(), c32.size(), &m->d_coords32 ) ) ||
          ( rc = upload( r32.data(), r32.size(), &m->d_radii32 ) ) ||
          ( rc = upload( m->h_lat_owned.data(), m->h_lat_owned.size(), &m->d_lat_owned ) ) ||
+         ( rc = upload( node_owned.data(), node_owned.size(), &m->d_node_owned ) ) ||
          ( rc = upload( offsets.data(), offsets.size(), &m->d_halo_offsets ) ) ||
          ( rc = upload( members.data(), std::max< size_t >( members.size(), 1 ), &m->d_halo_members ) ) )
     {
@@ -273,6 +277,7 @@ extern "C" int tn_mesh_destroy( tn_mesh* m )
     cudaFree( m->d_coords32 );
     cudaFree( m->d_radii32 );
     cudaFree( m->d_lat_owned );
+    cudaFree( m->d_node_owned );
     cudaFree( m->d_halo_offsets );
     cudaFree( m->d_halo_members );
     cudaFree( m->d_red_partials );

@@ -42,9 +42,10 @@ __device__ __forceinline__ Neumaier warp_reduce( Neumaier a )
 }
 
 // Reduces K compensated sums over the whole grid; result[k] = total k.
-// Requires blockDim.x to be a multiple of 32 and <= 1024.
+// Requires blockDim.x to be a multiple of 32 and <= 1024.  Returns true in
+// the last block (where thread 0 has just written `result`), false elsewhere.
 template < int K >
-__device__ void block_sum_finish( Neumaier* acc, double* partials, unsigned int* counter, double* result )
+__device__ bool block_sum_finish( Neumaier* acc, double* partials, unsigned int* counter, double* result )
 {
     __shared__ double   sh_s[32][K], sh_c[32][K];
     __shared__ bool     is_last;
@@ -73,7 +74,7 @@ __device__ void block_sum_finish( Neumaier* acc, double* partials, unsigned int*
     }
     __syncthreads();
     if ( !is_last )
-        return;
+        return false;
     __threadfence();
 #pragma unroll
     for ( int k = 0; k < K; ++k )
@@ -98,6 +99,7 @@ __device__ void block_sum_finish( Neumaier* acc, double* partials, unsigned int*
         }
         *counter = 0u;
     }
+    return true;
 }
 
 // Grid-wide maximum of non-negative values (same last-block scheme).

@@ -26,7 +26,7 @@ using A32 = EpsilonDivDivKerngen< float >;
 // FP32 V-cycle's coarsest solve done in FP64: cast, PCG, cast back
 struct CoarseFp64
 {
-    std::shared_ptr< PCG< A64 > > pcg;
+    std::shared_ptr< DevicePCG< A64 > > pcg;
     std::shared_ptr< A64 >        A;
     VectorQ1Vec< double >         x, b;
     void                          solve_impl( A32&, VectorQ1Vec< float >& xo, const VectorQ1Vec< float >& bi )
@@ -211,13 +211,13 @@ extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min,
             float*        dst[1] = { s->k32[l].data() };
             check( tn_vec_cast_f64_to_f32( s->mesh[l].get(), 1, dst, src, nullptr ), "cast viscosity" );
         }
-        // FP64 coarsest solve (both precisions): PCG, 4 temporaries
+        // FP64 coarsest solve (both precisions): device-resident PCG, 3 temporaries
         BoundaryConditions bcs{ p->bc_cmb, p->bc_surface };
         auto               Ac64 = std::make_shared< A64 >( s->mesh[Lmin], s->k64[Lmin], bcs, false );
         std::vector< VectorQ1Vec< double > > ct;
-        for ( int i = 0; i < 4; ++i )
+        for ( int i = 0; i < 3; ++i )
             ct.emplace_back( s->mesh[Lmin] );
-        auto pcg = std::make_shared< PCG< A64 > >(
+        auto pcg = std::make_shared< DevicePCG< A64 > >(
             IterativeSolverParameters{ p->coarse_max_iterations, p->coarse_relative_tolerance, 1e-16 }, ct );
         if ( p->mg_fp32 )
         {
@@ -233,9 +233,9 @@ extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min,
         }
         else
         {
-            auto mg  = build_mg< double, PCG< A64 > >( *s, s->A64s, *pcg );
-            auto p11 = std::make_shared< Fp64Preconditioner< MG< double, PCG< A64 > > > >(
-                Fp64Preconditioner< MG< double, PCG< A64 > > >{ mg } );
+            auto mg  = build_mg< double, DevicePCG< A64 > >( *s, s->A64s, *pcg );
+            auto p11 = std::make_shared< Fp64Preconditioner< MG< double, DevicePCG< A64 > > > >(
+                Fp64Preconditioner< MG< double, DevicePCG< A64 > > >{ mg } );
             finish( *s, p11 );
         }
         *out = s.release();
@@ -339,15 +339,17 @@ extern "C" int tn_laplace_pcg_solve_f64( const tn_mesh* mesh, const double* b, d
         Laplace< double >        A( m, true, false );
         VectorQ1Scalar< double > vb( m, const_cast< double* >( b ) ), vx( m, x );
         std::vector< VectorQ1Scalar< double > > t;
-        for ( int i = 0; i < 4; ++i )
+        for ( int i = 0; i < 3; ++i )
             t.emplace_back( m );
-        PCG< Laplace< double > > pcg( IterativeSolverParameters{ max_iterations, relative_tolerance, absolute_tolerance }, t );
+        DevicePCG< Laplace< double > > pcg(
+            IterativeSolverParameters{ max_iterations, relative_tolerance, absolute_tolerance }, t );
         solve( pcg, A, vx, vb );
+        const SolverStatistics st = pcg.statistics();
         TN_CUDA_TRY( cudaDeviceSynchronize() );
         if ( iterations )
-            *iterations = pcg.stats.iterations;
+            *iterations = st.iterations;
         if ( relative_residual )
-            *relative_residual = pcg.stats.relative_residuals.back();
+            *relative_residual = st.relative_residuals.back();
         return TN_OK;
     }
     catch ( const std::exception& e )

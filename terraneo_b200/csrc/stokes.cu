@@ -71,56 +71,6 @@ struct StokesParams
     int           bc_cmb, bc_surf;
 };
 
-// B_w[i][d][j] of fine wedge w of cell (d_, x, y, r)
-template < typename T >
-__device__ void wedge_B( const StokesParams< T >& P, int dm, int x, int y, int r, int w, T B[6][3][6] )
-{
-    const int n1 = P.n1;
-    T         p[3][3];
-#pragma unroll
-    for ( int n = 0; n < 3; ++n )
-    {
-        const double* c = P.coords + lat_index( n1, dm, x + kWedgeNode[w][n][0], y + kWedgeNode[w][n][1] ) * 3;
-        p[n][0] = T( c[0] ), p[n][1] = T( c[1] ), p[n][2] = T( c[2] );
-    }
-    const T   r1 = P.radii[dm * n1 + r], r2 = P.radii[dm * n1 + r + 1];
-    const int frad = r & 1, flat = fine_lateral_wedge( x, y, w );
-#pragma unroll
-    for ( int i = 0; i < 6; ++i )
-#pragma unroll
-        for ( int d = 0; d < 3; ++d )
-#pragma unroll
-            for ( int j = 0; j < 6; ++j )
-                B[i][d][j] = T( 0 );
-    for ( int q = 0; q < 6; ++q )
-    {
-        const T xi = T( kQP[q][0] ), eta = T( kQP[q][1] ), zeta = T( kQP[q][2] );
-        T       IT[3][3];
-        const T det = wedge_jacobian_it( p[0], p[1], p[2], r1, r2, xi, eta, zeta, IT );
-        const T wd  = T( kQW ) * fabs( det );
-        T       g[6][3];
-#pragma unroll
-        for ( int n = 0; n < 6; ++n )
-        {
-            T gr[3];
-            grad_shape_ref( n, xi, eta, zeta, gr );
-#pragma unroll
-            for ( int a = 0; a < 3; ++a )
-                g[n][a] = IT[a][0] * gr[0] + IT[a][1] * gr[1] + IT[a][2] * gr[2];
-        }
-#pragma unroll
-        for ( int i = 0; i < 6; ++i )
-        {
-            const T ni = -wd * shape_coarse( i, frad, flat, xi, eta, zeta );
-#pragma unroll
-            for ( int d = 0; d < 3; ++d )
-#pragma unroll
-                for ( int j = 0; j < 6; ++j )
-                    B[i][d][j] += g[j][d] * ni;
-        }
-    }
-}
-
 // 0: interior, 1: Dirichlet (drop), 2: free-slip (project)
 __device__ __forceinline__ int velocity_bc( int N, int r, int n, int bc_cmb, int bc_surf )
 {
@@ -138,6 +88,76 @@ __device__ __forceinline__ void unit_normal( const double* c, T n[3] )
     n[0] = T( c[0] / m ), n[1] = T( c[1] / m ), n[2] = T( c[2] / m );
 }
 
+// Quadrature data of one fine wedge: for lateral point ql and radial point
+// qz, J = M(ql) diag(r(qz), r(qz), dr/2) with M = [p1-p0, p2-p0, p(xi,eta)], so
+// J^{-T} = M^{-T} diag(1/r, 1/r, 2/dr) and |det J| = |det M| r^2 dr/2: one 3x3
+// inverse per lateral point serves both radial points.  Calls f(q, wdet, g, xi,
+// eta, zeta) with g the 6 physical shape gradients.
+template < typename T, typename F >
+__device__ __forceinline__ void for_each_qp( const T p[3][3], T r1, T r2, F&& f )
+{
+    const T dr = T( 0.5 ) * ( r2 - r1 );
+#pragma unroll 1
+    for ( int ql = 0; ql < 3; ++ql )
+    {
+        const T xi = T( kQP[ql][0] ), eta = T( kQP[ql][1] );
+        T       M[3][3];
+#pragma unroll
+        for ( int a = 0; a < 3; ++a )
+        {
+            M[a][0] = p[1][a] - p[0][a];
+            M[a][1] = p[2][a] - p[0][a];
+            M[a][2] = ( T( 1 ) - xi - eta ) * p[0][a] + xi * p[1][a] + eta * p[2][a];
+        }
+        const T c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1], c01 = M[1][2] * M[2][0] - M[1][0] * M[2][2],
+                c02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+        const T det = M[0][0] * c00 + M[0][1] * c01 + M[0][2] * c02;
+        const T id  = T( 1 ) / det;
+        // Q = M^{-T}
+        T Q[3][3];
+        Q[0][0] = c00 * id, Q[0][1] = c01 * id, Q[0][2] = c02 * id;
+        Q[1][0] = ( M[0][2] * M[2][1] - M[0][1] * M[2][2] ) * id;
+        Q[1][1] = ( M[0][0] * M[2][2] - M[0][2] * M[2][0] ) * id;
+        Q[1][2] = ( M[0][1] * M[2][0] - M[0][0] * M[2][1] ) * id;
+        Q[2][0] = ( M[0][1] * M[1][2] - M[0][2] * M[1][1] ) * id;
+        Q[2][1] = ( M[0][2] * M[1][0] - M[0][0] * M[1][2] ) * id;
+        Q[2][2] = ( M[0][0] * M[1][1] - M[0][1] * M[1][0] ) * id;
+#pragma unroll
+        for ( int qz = 0; qz < 2; ++qz )
+        {
+            const int q    = ql + 3 * qz;
+            const T   zeta = T( kQP[q][2] );
+            const T   rq   = r1 + dr * ( T( 1 ) + zeta );
+            const T   s0 = T( 1 ) / rq, s2 = T( 1 ) / dr;
+            const T   wdet = T( kQW ) * fabs( det ) * rq * rq * dr;
+            T         g[6][3];
+#pragma unroll
+            for ( int n = 0; n < 6; ++n )
+            {
+                T gr[3];
+                grad_shape_ref( n, xi, eta, zeta, gr );
+                gr[0] *= s0, gr[1] *= s0, gr[2] *= s2;
+#pragma unroll
+                for ( int a = 0; a < 3; ++a )
+                    g[n][a] = Q[a][0] * gr[0] + Q[a][1] * gr[1] + Q[a][2] * gr[2];
+            }
+            f( q, wdet, g, xi, eta, zeta );
+        }
+    }
+}
+
+template < typename T >
+__device__ __forceinline__ void wedge_points( const StokesParams< T >& P, int dm, int x, int y, int w, T p[3][3] )
+{
+#pragma unroll
+    for ( int n = 0; n < 3; ++n )
+    {
+        const double* c = P.coords + lat_index( P.n1, dm, x + kWedgeNode[w][n][0], y + kWedgeNode[w][n][1] ) * 3;
+        p[n][0] = T( c[0] ), p[n][1] = T( c[1] ), p[n][2] = T( c[2] );
+    }
+}
+
+// p_coarse += B u: per quadrature point -w |det J| N^c_i div u
 template < typename T >
 __global__ void __launch_bounds__( 128 ) divergence_kernel( StokesParams< T > P, Ptr3< const T > u, T* __restrict__ p )
 {
@@ -153,11 +173,15 @@ __global__ void __launch_bounds__( 128 ) divergence_kernel( StokesParams< T > P,
 #pragma unroll
     for ( int i = 0; i < 8; ++i )
         out[i >> 2][( i >> 1 ) & 1][i & 1] = T( 0 );
+    const T   r1 = P.radii[dm * n1 + r], r2 = P.radii[dm * n1 + r + 1];
+    const int frad = r & 1;
+#pragma unroll
     for ( int w = 0; w < 2; ++w )
     {
-        T B[6][3][6];
-        wedge_B( P, dm, x, y, r, w, B );
-        T uu[6][3];
+        T p3[3][3];
+        wedge_points( P, dm, x, y, w, p3 );
+        const int flat = fine_lateral_wedge( x, y, w );
+        T         uu[6][3];
 #pragma unroll
         for ( int n = 0; n < 6; ++n )
         {
@@ -175,19 +199,23 @@ __global__ void __launch_bounds__( 128 ) divergence_kernel( StokesParams< T > P,
                 uu[n][0] -= dt * nn[0], uu[n][1] -= dt * nn[1], uu[n][2] -= dt * nn[2];
             }
         }
+        T acc[6] = { 0, 0, 0, 0, 0, 0 };
+        for_each_qp( p3, r1, r2, [&]( int, T wdet, const T ( &g )[6][3], T xi, T eta, T zeta ) {
+            T div = 0;
+#pragma unroll
+            for ( int n = 0; n < 6; ++n )
+                div += g[n][0] * uu[n][0] + g[n][1] * uu[n][1] + g[n][2] * uu[n][2];
+            const T s = -wdet * div;
+#pragma unroll
+            for ( int i = 0; i < 6; ++i )
+                acc[i] += s * shape_coarse( i, frad, flat, xi, eta, zeta );
+        } );
 #pragma unroll
         for ( int i = 0; i < 6; ++i )
-        {
-            T v = 0;
-#pragma unroll
-            for ( int d = 0; d < 3; ++d )
-#pragma unroll
-                for ( int j = 0; j < 6; ++j )
-                    v += B[i][d][j] * uu[j][d];
-            out[kWedgeNode[w][i][0]][kWedgeNode[w][i][1]][kWedgeNode[w][i][2]] += v;
-        }
+            out[kWedgeNode[w][i][0]][kWedgeNode[w][i][1]][kWedgeNode[w][i][2]] += acc[i];
     }
     const int xc = x >> 1, yc = y >> 1, rc = r >> 1;
+#pragma unroll
     for ( int a = 0; a < 8; ++a )
     {
         const int dx = a >> 2, dy = ( a >> 1 ) & 1, dr = a & 1;
@@ -195,6 +223,7 @@ __global__ void __launch_bounds__( 128 ) divergence_kernel( StokesParams< T > P,
     }
 }
 
+// u_fine += B^T p: per quadrature point -w |det J| p^c(q) grad N_j
 template < typename T >
 __global__ void __launch_bounds__( 128 ) gradient_kernel( StokesParams< T > P, const T* __restrict__ p, Ptr3< T > u )
 {
@@ -213,32 +242,44 @@ __global__ void __launch_bounds__( 128 ) gradient_kernel( StokesParams< T > P, c
         for ( int c = 0; c < 3; ++c )
             out[i >> 2][( i >> 1 ) & 1][i & 1][c] = T( 0 );
     const int xc = x >> 1, yc = y >> 1, rc = r >> 1;
+    const T   r1 = P.radii[dm * n1 + r], r2 = P.radii[dm * n1 + r + 1];
+    const int frad = r & 1;
+#pragma unroll
     for ( int w = 0; w < 2; ++w )
     {
-        T B[6][3][6];
-        wedge_B( P, dm, x, y, r, w, B );
-        T pc[6];
+        T p3[3][3];
+        wedge_points( P, dm, x, y, w, p3 );
+        const int flat = fine_lateral_wedge( x, y, w );
+        T         pc[6];
 #pragma unroll
         for ( int i = 0; i < 6; ++i )
             pc[i] = p[lat_index( nc1, dm, xc + kWedgeNode[w][i][0], yc + kWedgeNode[w][i][1] ) * nc1 + rc +
                       kWedgeNode[w][i][2]];
+        T acc[6][3];
+#pragma unroll
+        for ( int n = 0; n < 6; ++n )
+            acc[n][0] = acc[n][1] = acc[n][2] = T( 0 );
+        for_each_qp( p3, r1, r2, [&]( int, T wdet, const T ( &g )[6][3], T xi, T eta, T zeta ) {
+            T pq = 0;
+#pragma unroll
+            for ( int i = 0; i < 6; ++i )
+                pq += shape_coarse( i, frad, flat, xi, eta, zeta ) * pc[i];
+            const T s = -wdet * pq;
+#pragma unroll
+            for ( int n = 0; n < 6; ++n )
+                acc[n][0] += s * g[n][0], acc[n][1] += s * g[n][1], acc[n][2] += s * g[n][2];
+        } );
 #pragma unroll
         for ( int j = 0; j < 6; ++j )
         {
-            T v[3] = { 0, 0, 0 };
-#pragma unroll
-            for ( int d = 0; d < 3; ++d )
-#pragma unroll
-                for ( int i = 0; i < 6; ++i )
-                    v[d] += B[i][d][j] * pc[i];
-            const int bc = velocity_bc( N, r, j, P.bc_cmb, P.bc_surf );
+            T         v[3] = { acc[j][0], acc[j][1], acc[j][2] };
+            const int bc   = velocity_bc( N, r, j, P.bc_cmb, P.bc_surf );
             if ( bc == TN_BC_DIRICHLET )
                 continue;
             if ( bc == TN_BC_FREESLIP )
             {
                 T nn[3];
-                unit_normal( P.coords + lat_index( n1, dm, x + kWedgeNode[w][j][0], y + kWedgeNode[w][j][1] ) * 3,
-                             nn );
+                unit_normal( P.coords + lat_index( n1, dm, x + kWedgeNode[w][j][0], y + kWedgeNode[w][j][1] ) * 3, nn );
                 const T dt = nn[0] * v[0] + nn[1] * v[1] + nn[2] * v[2];
                 v[0] -= dt * nn[0], v[1] -= dt * nn[1], v[2] -= dt * nn[2];
             }
@@ -246,6 +287,7 @@ __global__ void __launch_bounds__( 128 ) gradient_kernel( StokesParams< T > P, c
             o[0] += v[0], o[1] += v[1], o[2] += v[2];
         }
     }
+#pragma unroll
     for ( int a = 0; a < 8; ++a )
     {
         const int    dx = a >> 2, dy = ( a >> 1 ) & 1, dr = a & 1;

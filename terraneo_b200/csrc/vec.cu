@@ -80,30 +80,41 @@ __global__ void cast_kernel( size_t ns, int ncomp, Ptr3< TO > y, Ptr3< const TI 
         y.p[c][i] = TO( x.p[c][i] );
 }
 
-// Owned-node dot product: one lateral ownership flag per (diamond, x, y); a
-// warp handles one lateral column (lanes along r, coalesced) at a time.
+// Owned-node dot product over a flat per-stored-node ownership mask; each
+// thread keeps a Neumaier-compensated FP64 partial over a grid-stride range.
 template < typename T >
-__global__ void dot_kernel( size_t nlat, int n1, int ncomp, Ptr3< const T > a, Ptr3< const T > b,
-                            const uint8_t* __restrict__ lat_owned, double* partials, unsigned int* counter,
+__global__ void dot_kernel( size_t ns, int ncomp, Ptr3< const T > a, Ptr3< const T > b,
+                            const uint8_t* __restrict__ owned, double* partials, unsigned int* counter,
                             double* result )
 {
-    Neumaier     acc;
-    const int    lane = threadIdx.x & 31;
-    const size_t wid  = ( blockIdx.x * size_t( blockDim.x ) + threadIdx.x ) >> 5;
-    const size_t nw   = ( size_t( gridDim.x ) * blockDim.x ) >> 5;
-    for ( size_t lat = wid; lat < nlat; lat += nw )
+    Neumaier acc;
+    for ( int c = 0; c < ncomp; ++c )
     {
-        if ( !lat_owned[lat] )
-            continue;
-        for ( int c = 0; c < ncomp; ++c )
+        const T* __restrict__ pa = a.p[c];
+        const T* __restrict__ pb = b.p[c];
+        for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
         {
-            const T* pa = a.p[c] + lat * n1;
-            const T* pb = b.p[c] + lat * n1;
-            for ( int r = lane; r < n1; r += 32 )
-                acc.add( double( pa[r] ) * double( pb[r] ) );
+            const double v = double( pa[i] ) * double( pb[i] );
+            acc.add( owned[i] ? v : 0.0 );
         }
     }
     block_sum_finish< 1 >( &acc, partials, counter, result );
+}
+
+// One Chebyshev step (linalg/solvers/chebyshev.hpp:127-160) fused into a
+// single pass: z = D^{-1} (b - Ax), d = alpha z + beta d, x = x + d.
+template < typename T >
+__global__ void chebyshev_kernel( size_t ns, Ptr3< T > x, Ptr3< T > d, Ptr3< const T > b, Ptr3< const T > ax,
+                                  Ptr3< const T > inv_diag, T alpha, T beta )
+{
+    const int c = blockIdx.y;
+    for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
+    {
+        const T z  = inv_diag.p[c][i] * ( b.p[c][i] - ax.p[c][i] );
+        const T dn = beta == T( 0 ) ? alpha * z : alpha * z + beta * d.p[c][i];
+        d.p[c][i]  = dn;
+        x.p[c][i]  = x.p[c][i] + dn;
+    }
 }
 
 template < typename T >
@@ -205,8 +216,8 @@ int vec_dot( const tn_mesh* m, int ncomp, const T* const* a, const T* const* b, 
     int             rc;
     if ( ( rc = ptr3c( ncomp, a, pa, "dot" ) ) || ( rc = ptr3c( ncomp, b, pb, "dot" ) ) )
         return rc;
-    const unsigned blocks = unsigned( std::min< size_t >( ( m->nlat + 15 ) / 16, kRedMaxBlocks ) );
-    dot_kernel< T ><<< blocks, kThreads, 0, st >>>( m->nlat, m->n1, ncomp, pa, pb, m->d_lat_owned, m->d_red_partials,
+    const unsigned blocks = std::min< unsigned >( grid_for( m->ns, 8 ), kRedMaxBlocks );
+    dot_kernel< T ><<< blocks, kThreads, 0, st >>>( m->ns, ncomp, pa, pb, m->d_node_owned, m->d_red_partials,
                                                    m->d_red_counter, m->d_red_result );
     TN_LAUNCH_CHECK();
     return fetch_result( m, 1, st, result );
@@ -328,6 +339,35 @@ extern "C" int tn_vec_has_nan_or_inf_f64( const tn_mesh* m, int ncomp, const dou
 extern "C" int tn_vec_has_nan_or_inf_f32( const tn_mesh* m, int ncomp, const float* const* x, int* r, void* s )
 {
     return has_nan< float >( m, ncomp, x, r, s );
+}
+template < typename T >
+static int chebyshev_step( const tn_mesh* m, int ncomp, T* const* x, T* const* d, const T* const* b, const T* const* ax,
+                           const T* const* inv_diag, double alpha, double beta, void* s )
+{
+    TN_CHECK_ARG( m, "chebyshev_step: mesh is NULL" );
+    Ptr3< T >       px, pd;
+    Ptr3< const T > pb, pa, pi;
+    int             rc;
+    if ( ( rc = ptr3( ncomp, x, px, "chebyshev_step" ) ) || ( rc = ptr3( ncomp, d, pd, "chebyshev_step" ) ) ||
+         ( rc = ptr3c( ncomp, b, pb, "chebyshev_step" ) ) || ( rc = ptr3c( ncomp, ax, pa, "chebyshev_step" ) ) ||
+         ( rc = ptr3c( ncomp, inv_diag, pi, "chebyshev_step" ) ) )
+        return rc;
+    chebyshev_kernel< T ><<< dim3( grid_for( m->ns ), ncomp ), kThreads, 0, as_stream( s ) >>>(
+        m->ns, px, pd, pb, pa, pi, T( alpha ), T( beta ) );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+extern "C" int tn_vec_chebyshev_step_f64( const tn_mesh* m, int ncomp, double* const* x, double* const* d,
+                                          const double* const* b, const double* const* ax,
+                                          const double* const* inv_diag, double alpha, double beta, void* s )
+{
+    return chebyshev_step< double >( m, ncomp, x, d, b, ax, inv_diag, alpha, beta, s );
+}
+extern "C" int tn_vec_chebyshev_step_f32( const tn_mesh* m, int ncomp, float* const* x, float* const* d,
+                                          const float* const* b, const float* const* ax, const float* const* inv_diag,
+                                          double alpha, double beta, void* s )
+{
+    return chebyshev_step< float >( m, ncomp, x, d, b, ax, inv_diag, alpha, beta, s );
 }
 template < typename T >
 static int randomize( const tn_mesh* m, int ncomp, T* const* y, unsigned long long seed, void* s )
