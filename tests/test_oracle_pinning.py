@@ -1,0 +1,101 @@
+"""Pins the oracle (the C restatement under oracle/) to the reference.
+
+The golden fixture tests/golden/ref_L2.npz holds outputs of the reference's
+own operators (compiled from its sources by oracle/ref_build) on a seeded L2
+mesh; make_golden.py beside it regenerates it.  Every case is recomputed here
+by the oracle from the same seeded inputs.  When the compiled reference is
+present (oracle/_ref/ref_dump), a second test compares oracle and reference
+live on an L3 mesh.  CPU only.
+"""
+import os
+import sys
+import tempfile
+
+import numpy as np
+import pytest
+
+from helpers import rel
+from oracle_lib import Mesh, ref_available, run_ref
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+import make_golden as G  # noqa: E402
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "ref_L2.npz")
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def case():
+    g = np.load(GOLDEN)
+    fine, coarse = Mesh(int(g["level"])), Mesh(int(g["level"]) - 1)
+    x = G.inputs(fine, coarse)
+    return g, fine, coarse, x
+
+
+def test_inputs_regenerate(case):
+    g, _, _, x = case
+    for name, a in x.items():
+        assert np.allclose(G.checksum(a), g["checksum_" + name], rtol=1e-13, atol=0), name
+
+
+def test_mesh_matches_reference(case):
+    g, fine, _, _ = case
+    assert np.abs(fine.coords - g["coords"]).max() <= 1e-15
+    assert np.abs(fine.radii - g["radii"]).max() <= 1e-15
+    assert np.array_equal(fine.bmask, g["bmask"])
+    assert np.array_equal(fine.omask, g["omask"])
+
+
+@pytest.mark.parametrize("bcc,bcs,diag", G.KERNGEN_CASES)
+def test_kerngen_matches_reference(case, bcc, bcs, diag):
+    g, fine, _, x = case
+    assert rel(fine.kerngen(x["k"], x["u"], bcc, bcs, diag), g[f"kerngen_{bcc}{bcs}{diag}"]) <= TOL
+
+
+@pytest.mark.parametrize("treat,diag", G.LAPLACE_CASES)
+def test_laplace_matches_reference(case, treat, diag):
+    g, fine, _, x = case
+    assert rel(fine.laplace(x["s"], treat, diag), g[f"laplace_{treat}{diag}"]) <= TOL
+
+
+@pytest.mark.parametrize("bcc,bcs", G.STOKES_BCS)
+def test_stokes_blocks_match_reference(case, bcc, bcs):
+    g, fine, coarse, x = case
+    assert rel(fine.divergence(coarse, x["u"], bcc, bcs), g[f"divergence_{bcc}{bcs}"]) <= TOL
+    assert rel(fine.gradient(coarse, x["p"], bcc, bcs), g[f"gradient_{bcc}{bcs}"]) <= TOL
+
+
+def test_transfers_match_reference(case):
+    g, fine, coarse, x = case
+    assert rel(fine.prolong(coarse, x["uc"]), g["prolong"]) <= TOL
+    assert rel(fine.restrict(coarse, x["u"]), g["restrict"]) <= TOL
+
+
+@pytest.mark.parametrize("mode", G.KMASS_MODES)
+def test_kmass_matches_reference(case, mode):
+    g, fine, _, x = case
+    assert rel(fine.kmass(x["k"], x["s"], mode), g[f"kmass_{mode}"]) <= TOL
+
+
+def test_golden_fixture_is_not_trivial(case):
+    """A planted error in the oracle's input must break the comparison."""
+    g, fine, _, x = case
+    u = x["u"].copy()
+    u[0, 3, 1, 2, 2] += 1e-3
+    assert rel(fine.kerngen(x["k"], u, 1, 1, 0), g["kerngen_110"]) > 1e-8
+
+
+@pytest.mark.skipif(not ref_available(), reason="compiled reference (oracle/_ref/ref_dump) not built here")
+def test_oracle_matches_live_reference_L3():
+    L = 3
+    m = Mesh(L)
+    rs = np.random.RandomState(7)
+    k = m.make_consistent(np.exp(rs.normal(size=m.shape)))
+    u = m.make_consistent(rs.normal(size=(3,) + m.shape))
+    with tempfile.TemporaryDirectory() as d:
+        k.tofile(f"{d}/k.bin")
+        u.tofile(f"{d}/src.bin")
+        for bcc, bcs in [(2, 2), (1, 2)]:
+            run_ref(["kerngen", L, 0.55, 1.0, bcc, bcs, 0, d], d)
+            ref = np.fromfile(f"{d}/dst.bin").reshape((3,) + m.shape)
+            assert rel(m.kerngen(k, u, bcc, bcs, False), ref) <= TOL
