@@ -34,6 +34,9 @@ METRIC = "L6 Stokes time-to-1e-8 (FP32-MG+FP64 refine vs FP64); apply GDoF/s, %H
 LEVEL, RMIN, RMAX = 6, 0.55, 1.0
 BYTES_PER_NODE_F64 = 56  # 3 src + 1 k + 3 dst doubles per stored node
 BYTES_PER_NODE_F32 = 28
+# DRAM bytes (read + write) of one level-6 kerngen_tile_kernel<double> launch,
+# from an ncu capture (profiles/kerngen_tile_kernel_f64_L6_dirichlet.md)
+TILE_TRAFFIC_BYTES = 126152192 + 39593216
 
 
 def parse():
@@ -43,6 +46,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-stokes", action="store_true", help="skip the level-6 Stokes time-to-1e-8 leg")
     return ap.parse_args()
 
 
@@ -62,6 +66,74 @@ def synthetic_inputs(coords, radii, omask_lat, seed=2024):
     k = np.clip(np.exp(np.log(1e4) * (0.5 * rho[:, None, None, :] + 0.5 * field)), 1.0, 1e4)
     src = rng.normal(size=(3, 10, n1, n1, n1))
     return k, src
+
+
+def stokes_rhs(shell, mesh, coords, radii, seed=2025):
+    """Buoyancy RHS f = M (Ra T r_hat), Ra = 1e5, T = conductive profile
+    (1/r - 1/r_max) / (1/r_min - 1/r_max) + 0.05 s(x), s a seeded smooth field
+    of unit RMS (sum of Gaussian blobs); free-slip projected on both radii."""
+    rng = np.random.default_rng(seed)
+    r = radii[:, None, None, :]
+    tc = (1 / r - 1 / RMAX) / (1 / RMIN - 1 / RMAX)
+    x = coords[:, :, :, None, :] * radii[:, None, None, :, None]
+    pert = np.zeros(x.shape[:-1])
+    for _ in range(12):
+        c = rng.normal(size=3)
+        c = c / np.linalg.norm(c) * rng.uniform(RMIN, RMAX)
+        pert += rng.normal() * np.exp(-np.sum((x - c) ** 2, axis=-1) / (2 * 0.15 ** 2))
+    pert -= pert.mean()
+    temp = tc + 0.05 * pert / np.sqrt(np.mean(pert ** 2))
+    rhat = coords / np.linalg.norm(coords, axis=-1, keepdims=True)
+    g = 1e5 * temp[..., None] * rhat[:, :, :, None, :]
+    f = shell.VectorQ1Vec(mesh)
+    tmp, out = shell.VectorQ1Scalar(mesh), shell.VectorQ1Scalar(mesh)
+    mass = shell.KMass(mesh, None, 0)
+    for c in range(3):
+        tmp.set_numpy(g[..., c])
+        shell.apply(mass, tmp, out)
+        f.data[c].copy_(out.data[0])
+    shell.freeslip_project(f, True, True)
+    return f
+
+
+def stokes_leg(shell, C, torch, k_np):
+    """Level-6 free-slip Stokes solve to 1e-8: FP32-multigrid vs FP64-multigrid
+    preconditioner (FGMRES(50) outer in FP64, block-triangular preconditioner,
+    4-level V-cycle with Chebyshev order 3, coarse PCG in FP64)."""
+    pf, pc = shell.ShellMesh(LEVEL, RMIN, RMAX), shell.ShellMesh(LEVEL - 1, RMIN, RMAX)
+    coords, radii = pf.geometry()
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(k_np)
+    fu, fp = stokes_rhs(shell, pf, coords, radii), shell.VectorQ1Scalar(pc)
+    fnorm = np.sqrt(shell.dot(fu, fu))
+    out = {"workload": "Stokes solve, velocity level 6 / pressure level 5, free-slip both radii, 1e4 viscosity "
+                       "contrast, buoyancy RHS (Ra 1e5), FGMRES(50) + block-triangular preconditioner, V-cycle over "
+                       "levels 3-6 (Chebyshev order 3, 2 smoothing steps, coarse PCG FP64 50 its / 1e-6), "
+                       "stop at 1e-8 relative FP64 residual"}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for tag, mg32 in (("fp32_mg", True), ("fp64_mg", False)):
+        s = shell.StokesSolver(LEVEL, kv, mg_levels=4, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP,
+                               mg_fp32=mg32, chebyshev_order=3, relative_tolerance=1e-8, max_iterations=1000,
+                               restart=50, r_min=RMIN, r_max=RMAX)
+        xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+        s.solve(fu, fp, xu, xp)  # warm-up: eigenvalue estimates, first-touch
+        xu.data.zero_()
+        xp.data.zero_()
+        torch.cuda.synchronize()
+        ev0.record()
+        it, rr = s.solve(fu, fp, xu, xp)
+        ev1.record()
+        torch.cuda.synchronize()
+        sec = ev0.elapsed_time(ev1) / 1e3
+        ku, kp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+        s.apply(xu, xp, ku, kp)
+        shell.lincomb(ku, [1.0, -1.0], [fu, ku])
+        shell.lincomb(kp, [1.0, -1.0], [fp, kp])
+        true_rr = np.sqrt(shell.dot(ku, ku) + shell.dot(kp, kp)) / fnorm
+        out[tag] = {"seconds": round(sec, 4), "iterations": it, "true_relres": float(f"{true_rr:.3e}")}
+        del s
+    out["speedup_fp32_mg"] = round(out["fp64_mg"]["seconds"] / out["fp32_mg"]["seconds"], 3)
+    return out
 
 
 class ClockSampler:
@@ -291,7 +363,10 @@ def main():
                        "l2": "inputs rotate over 4 buffer sets (528 MB > 126 MB L2)",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "frac": round(achieved / peak, 4), "traffic": TILE_TRAFFIC_BYTES,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                           "kerngen_tile_kernel<double> launch at level 6 (Dirichlet apply; "
+                                           "profiles/kerngen_tile_kernel_f64_L6_dirichlet.md)",
                          "kernel": "kerngen_tile_kernel<double>", "kernel_ms": round(kms, 5),
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
@@ -302,6 +377,8 @@ def main():
             "gpu_launches": 3 * args.steps,
             "clocks": clk.summary(),
         }
+        if world == 1 and not args.no_stokes:
+            line["stokes"] = stokes_leg(shell, C, torch, k_np)
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_baseline(steps=3)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
