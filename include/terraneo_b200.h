@@ -176,6 +176,21 @@ TN_API int tn_vec_dot_f64( const tn_mesh* mesh, int ncomp, const double* const* 
                     void* stream );
 TN_API int tn_vec_dot_f32( const tn_mesh* mesh, int ncomp, const float* const* a, const float* const* b, double* result,
                     void* stream );
+/* Allocation-free variant of tn_vec_dot_f64 (no counterpart in the
+ * reference): for callers that cannot let a library allocate device memory.
+ * It needs no mesh handle and calls no cudaMalloc / cudaFree / allocating
+ * library routine: its reduction scratch is a static device array of
+ * 262,656 bytes inside the library.  result = sum over c < ncomp and
+ * i < n of a[c][i] b[c][i] where owned[i] != 0 (owned NULL: every entry),
+ * compensated FP64; returns after the value is on the host.  Limits:
+ * n <= 33,554,432 entries per component (a larger n is rejected with
+ * TN_ERR_ARG), ncomp 1..3.  The first call on each device does a one-time
+ * set-up (the scratch's address is looked up and cached), so make it outside
+ * any stream capture.  All calls on one device share the scratch: calls that
+ * can overlap (several streams or host threads) race and must be serialised
+ * by the caller. */
+TN_API int tn_vec_dot_noalloc_f64( size_t n, int ncomp, const double* const* a, const double* const* b,
+                                   const uint8_t* owned, double* result, void* stream );
 TN_API int tn_vec_invert_f64( const tn_mesh* mesh, int ncomp, double* const* y, void* stream );
 TN_API int tn_vec_invert_f32( const tn_mesh* mesh, int ncomp, float* const* y, void* stream );
 TN_API int tn_vec_mult_f64( const tn_mesh* mesh, int ncomp, double* const* y, const double* const* x, void* stream );

@@ -8,6 +8,9 @@
 #include "common.cuh"
 #include "reduce.cuh"
 
+#include <mutex>
+#include <string>
+
 namespace tn {
 
 namespace {
@@ -396,4 +399,116 @@ extern "C" int tn_vec_cast_f64_to_f32( const tn_mesh* m, int ncomp, float* const
 extern "C" int tn_vec_cast_f32_to_f64( const tn_mesh* m, int ncomp, double* const* y, const float* const* x, void* s )
 {
     return vec_cast< double, float >( m, ncomp, y, x, as_stream( s ) );
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free owned-node dot product (tn_vec_dot_noalloc_f64).
+//
+// For callers that cannot let a library allocate device memory: no mesh
+// handle, no cudaMalloc / cudaFree / allocating library call.  The reduction
+// scratch is one file-scope device array loaded with the module:
+//   [0, 262144)        2 doubles (sum, compensation) per block, 16384 blocks
+//   [262144, +8)       result
+//   [262400, +4)       block ticket (cleared by every call before its launch)
+// One block per 2048 entries, so at most 16384 x 2048 = 33,554,432 entries
+// per component; longer fields are rejected.  All calls on a device share the
+// array: calls that can overlap (several streams or host threads) race on it
+// and must be serialised by the caller.  The first call on each device looks
+// the array's address up (cudaGetSymbolAddress) and caches it.
+namespace tn {
+namespace {
+
+constexpr unsigned kNoAllocMaxBlocks     = 16384;
+constexpr unsigned kNoAllocPerThread     = 8;
+constexpr size_t   kNoAllocMaxEntries    = size_t( kNoAllocMaxBlocks ) * kThreads * kNoAllocPerThread;
+constexpr size_t   kNoAllocPartialsBytes = sizeof( double ) * 2 * kNoAllocMaxBlocks;
+constexpr size_t   kNoAllocResultOffset  = kNoAllocPartialsBytes;
+constexpr size_t   kNoAllocCounterOffset = kNoAllocPartialsBytes + 256;
+constexpr size_t   kNoAllocBytes         = kNoAllocPartialsBytes + 512;
+constexpr int      kNoAllocMaxDevices    = 64;
+
+static __device__ __align__( 256 ) unsigned char g_dot_scratch[kNoAllocBytes];
+
+std::mutex     g_dot_scratch_mutex;
+unsigned char* g_dot_scratch_addr[kNoAllocMaxDevices] = {};
+
+int dot_scratch_address( unsigned char** out )
+{
+    int dev = 0;
+    TN_CUDA_TRY( cudaGetDevice( &dev ) );
+    TN_CHECK_ARG( dev >= 0 && dev < kNoAllocMaxDevices, "tn_vec_dot_noalloc_f64: device index out of range" );
+    std::lock_guard< std::mutex > lock( g_dot_scratch_mutex );
+    if ( !g_dot_scratch_addr[dev] )
+    {
+        void* p = nullptr;
+        TN_CUDA_TRY( cudaGetSymbolAddress( &p, g_dot_scratch ) );
+        g_dot_scratch_addr[dev] = static_cast< unsigned char* >( p );
+    }
+    *out = g_dot_scratch_addr[dev];
+    return TN_OK;
+}
+
+// Neumaier-compensated FP64 sum of a[i] b[i] over entries with owned[i] != 0
+// (owned == NULL: all entries), grid-stride, deterministic last-block finish.
+__global__ void dot_noalloc_kernel( size_t n, int ncomp, Ptr3< const double > a, Ptr3< const double > b,
+                                    const uint8_t* __restrict__ owned, double* partials, unsigned int* counter,
+                                    double* result )
+{
+    Neumaier acc;
+    for ( int c = 0; c < ncomp; ++c )
+    {
+        const double* __restrict__ pa = a.p[c];
+        const double* __restrict__ pb = b.p[c];
+        for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < n; i += size_t( gridDim.x ) * blockDim.x )
+        {
+            const double v = pa[i] * pb[i];
+            acc.add( ( owned && !owned[i] ) ? 0.0 : v );
+        }
+    }
+    block_sum_finish< 1 >( &acc, partials, counter, result );
+}
+
+}  // namespace
+}  // namespace tn
+
+extern "C" int tn_vec_dot_noalloc_f64( size_t n, int ncomp, const double* const* a, const double* const* b,
+                                       const uint8_t* owned, double* result, void* s )
+{
+    using namespace tn;
+    TN_CHECK_ARG( a && b && result, "tn_vec_dot_noalloc_f64: NULL argument" );
+    TN_CHECK_ARG( ncomp >= 1 && ncomp <= 3, "tn_vec_dot_noalloc_f64: ncomp must be 1, 2 or 3" );
+    if ( n > kNoAllocMaxEntries )
+    {
+        set_error( "tn_vec_dot_noalloc_f64: " + std::to_string( n ) + " entries per component exceed the static scratch "
+                   "(at most " + std::to_string( kNoAllocMaxEntries ) + ")" );
+        return TN_ERR_ARG;
+    }
+    Ptr3< const double > pa{}, pb{};
+    for ( int c = 0; c < ncomp; ++c )
+    {
+        TN_CHECK_ARG( a[c] && b[c], "tn_vec_dot_noalloc_f64: NULL field pointer" );
+        pa.p[c] = a[c];
+        pb.p[c] = b[c];
+    }
+    if ( n == 0 )
+    {
+        *result = 0.0;
+        return TN_OK;
+    }
+    unsigned char* base = nullptr;
+    int            rc   = dot_scratch_address( &base );
+    if ( rc )
+        return rc;
+    double*       partials = reinterpret_cast< double* >( base );
+    double*       dres     = reinterpret_cast< double* >( base + kNoAllocResultOffset );
+    unsigned int* counter  = reinterpret_cast< unsigned int* >( base + kNoAllocCounterOffset );
+    const size_t  per_block = size_t( kThreads ) * kNoAllocPerThread;
+    const unsigned blocks   = unsigned( ( n + per_block - 1 ) / per_block );
+    cudaStream_t   st       = as_stream( s );
+    TN_CUDA_TRY( cudaMemsetAsync( counter, 0, sizeof( unsigned int ), st ) );
+    dot_noalloc_kernel<<< blocks, kThreads, 0, st >>>( n, ncomp, pa, pb, owned, partials, counter, dres );
+    TN_LAUNCH_CHECK();
+    TN_CUDA_TRY( cudaMemcpyAsync( result, dres, sizeof( double ), cudaMemcpyDeviceToHost, st ) );
+    TN_CUDA_TRY( cudaStreamSynchronize( st ) );
+    return TN_OK;
 }
