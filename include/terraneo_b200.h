@@ -109,6 +109,42 @@ TN_API int tn_laplace_apply_f64( const tn_mesh* mesh, int treat_boundary, int di
 TN_API int tn_laplace_apply_f32( const tn_mesh* mesh, int treat_boundary, int diagonal, int apply_mode, int comm_mode,
                           const float* src, float* dst, void* stream );
 
+/* DivKGrad::apply_impl (fe/wedge/operators/shell/div_k_grad.hpp:219-345):
+ * int k grad u . grad v with k (nodal field) interpolated by the wedge shape
+ * functions at each quadrature point; treat_boundary / diagonal as for the
+ * Laplace; single_quadpoint != 0 uses the 1-point rule (set_single_quadpoint). */
+TN_API int tn_divkgrad_apply_f64( const tn_mesh* mesh, const double* k, int treat_boundary, int diagonal,
+                                  int single_quadpoint, int apply_mode, int comm_mode, const double* src, double* dst,
+                                  void* stream );
+TN_API int tn_divkgrad_apply_f32( const tn_mesh* mesh, const float* k, int treat_boundary, int diagonal,
+                                  int single_quadpoint, int apply_mode, int comm_mode, const float* src, float* dst,
+                                  void* stream );
+
+/* VectorLaplace::apply_impl (fe/wedge/operators/shell/vector_laplace.hpp:131-255):
+ * the Laplace on each of three components, 3x2 rule.  Boundary handling as
+ * the reference selects it per cell from the flag of the cell's (x, y, r)
+ * node: layer 0 follows bc_cmb, every other layer bc_surface (Dirichlet
+ * decouples that side's nodes keeping their diagonal).  Only TN_BC_NEUMANN
+ * and TN_BC_DIRICHLET are accepted (the reference aborts otherwise). */
+TN_API int tn_vector_laplace_apply_f64( const tn_mesh* mesh, int bc_cmb, int bc_surface, int diagonal, int apply_mode,
+                                        int comm_mode, const double* const* src, double* const* dst, void* stream );
+TN_API int tn_vector_laplace_apply_f32( const tn_mesh* mesh, int bc_cmb, int bc_surface, int diagonal, int apply_mode,
+                                        int comm_mode, const float* const* src, float* const* dst, void* stream );
+
+/* Viscosity derivative of the epsilon-div-div form (backward kernel of the
+ * adjoint viscosity gradient; no reference counterpart).  The one-point
+ * operator A(k) of tn_epsdivdiv_apply_* is linear in k, so
+ *     grad_k[n] = d (lambda^T A(k) u) / d k_n
+ * does not depend on k: the sum over the wedges w holding n of
+ * lambda_w^T A_w(1) u_w / 6, with the same Dirichlet / free-slip treatment as
+ * the apply and without the k-independent fs/fs rotation penalty.
+ * comm_mode TN_COMM_SKIP: derivative with respect to each stored copy of k;
+ * TN_COMM_ADDITIVE: with respect to each unique node, on all its copies. */
+TN_API int tn_epsdivdiv_kgrad_f64( const tn_mesh* mesh, int bc_cmb, int bc_surface, int comm_mode,
+                                   const double* const* u, const double* const* lambda, double* grad_k, void* stream );
+TN_API int tn_epsdivdiv_kgrad_f32( const tn_mesh* mesh, int bc_cmb, int bc_surface, int comm_mode,
+                                   const float* const* u, const float* const* lambda, float* grad_k, void* stream );
+
 /* ---------------------------------------------------------------------------
  * Stokes coupling blocks of the Q1-iso-Q2 / Q1 pair: `mesh` carries the P1
  * velocity (level L), `mesh_p` the P1 pressure (level L-1, same radii range).
@@ -317,6 +353,20 @@ TN_API int tn_stokes_history( const tn_stokes_solver* solver, double* out, int c
 /* out = K in (the FP64 Stokes operator of the solver) */
 TN_API int tn_stokes_apply( tn_stokes_solver* solver, const double* const* u, const double* p, double* const* out_u,
                             double* out_p );
+/* Backward of the Stokes solve with respect to the log-viscosity (adjoint
+ * viscosity gradient; no reference counterpart).  u is the forward velocity
+ * solution of this solver, grad_u the derivative of an objective J with
+ * respect to the stored velocity entries (copy-wise: for J = 1/2 sum over
+ * owned nodes |u - u_obs|^2 it is (u - u_obs) on owned copies, 0 elsewhere).
+ * Sums grad_u over node copies, applies the velocity boundary treatment,
+ * solves the adjoint system K lambda = (grad_u, 0) with the solver's FGMRES
+ * (K is symmetric) and returns grad_log_k = dJ/d log k = -k * d(lambda^T K x)/dk
+ * (tn_epsdivdiv_kgrad_f64 with comm_mode: per stored copy, or per unique node
+ * on all copies).  lambda_u / lambda_p receive the adjoint solution when not
+ * NULL; iterations the adjoint FGMRES iterations.  Synchronises. */
+TN_API int tn_stokes_viscosity_backward( tn_stokes_solver* solver, const double* const* u, const double* const* grad_u,
+                                         int comm_mode, double* grad_log_k, double* const* lambda_u, double* lambda_p,
+                                         int* iterations );
 TN_API int tn_stokes_solver_destroy( tn_stokes_solver* solver );
 
 #ifdef __cplusplus

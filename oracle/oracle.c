@@ -649,6 +649,148 @@ void or_laplace_apply( int L, const double* coords, const double* radii, const d
 }
 
 /* ------------------------------------------------------------------------ */
+/* DivKGrad (div_k_grad.hpp:219-572) and VectorLaplace                       */
+/* (vector_laplace.hpp:131-420): the Laplace form, with k interpolated by    */
+/* the wedge shape functions at every quadrature point (DivKGrad) or applied */
+/* to each of three components (VectorLaplace).  Per cell one of four       */
+/* couplings: all nodes (NEU), boundary nodes of the CMB side (BOT) or of the */
+/* SURFACE side (TOP) decoupled keeping their diagonal, or diagonal only.    */
+/* ------------------------------------------------------------------------ */
+
+enum { GM_NEU = 0, GM_BOT = 1, GM_TOP = 2, GM_DIAG = 3 };
+
+static double shape_ref( int n, double xi, double eta, double zeta )
+{
+    /* integrands.hpp:86-159: lateral P1 times radial linear */
+    const double lat = n % 3 == 0 ? 1 - xi - eta : ( n % 3 == 1 ? xi : eta );
+    return lat * ( n < 3 ? 0.5 * ( 1 - zeta ) : 0.5 * ( 1 + zeta ) );
+}
+
+static void grad_family_apply( int L, const double* coords, const double* radii, const double* k, int ncomp,
+                               const double* src, double* dst, const int* cell_mode_of_r, int single )
+{
+    const int    N = 1 << L, n1 = N + 1;
+    const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1;
+    memset( dst, 0, sizeof( double ) * ns * ncomp );
+    const int nq = single ? 1 : 6;
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                {
+                    const int mode = cell_mode_of_r[r];
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const double* p[3];
+                        wedge_lateral_points( n1, coords, d, x, y, w, p );
+                        size_t idx[6];
+                        double s[3][6], kv[6], out[3][6];
+                        memset( out, 0, sizeof( out ) );
+                        for ( int n = 0; n < 6; ++n )
+                        {
+                            idx[n] = node_idx( n1, d, x + WNODE[w][n][0], y + WNODE[w][n][1], r + WNODE[w][n][2] );
+                            for ( int c = 0; c < ncomp; ++c )
+                                s[c][n] = src[c * ns + idx[n]];
+                            kv[n] = k ? k[idx[n]] : 1.0;
+                        }
+                        for ( int q = 0; q < nq; ++q )
+                        {
+                            /* quad_felippa_1x1: (1/3, 1/3, 0), weight 1 (quadrature.hpp:32-46) */
+                            const double xi   = single ? 1.0 / 3.0 : QP32[q][0];
+                            const double eta  = single ? 1.0 / 3.0 : QP32[q][1];
+                            const double zeta = single ? 0.0 : QP32[q][2];
+                            const double wq   = single ? 1.0 : QW32;
+                            double       J[3][3], IT[3][3], g[6][3];
+                            wedge_jac( p, radii[d * n1 + r], radii[d * n1 + r + 1], xi, eta, zeta, J );
+                            const double det = det3( J );
+                            inv_transposed3( J, det, IT );
+                            for ( int n = 0; n < 6; ++n )
+                            {
+                                double gr[3];
+                                grad_shape_ref( n, xi, eta, zeta, gr );
+                                for ( int a = 0; a < 3; ++a )
+                                    g[n][a] = IT[a][0] * gr[0] + IT[a][1] * gr[1] + IT[a][2] * gr[2];
+                            }
+                            double wdet = wq * fabs( det );
+                            if ( k )
+                            {
+                                double ke = 0.0;
+                                for ( int n = 0; n < 6; ++n )
+                                    ke += shape_ref( n, xi, eta, zeta ) * kv[n];
+                                wdet *= ke;
+                            }
+                            int lo = 0, hi = 6;
+                            if ( mode == GM_BOT )
+                                lo = 3;
+                            if ( mode == GM_TOP )
+                                hi = 3;
+                            if ( mode == GM_DIAG )
+                                lo = hi = 6;
+                            for ( int c = 0; c < ncomp; ++c )
+                            {
+                                double gu[3] = { 0, 0, 0 };
+                                for ( int n = lo; n < hi; ++n )
+                                    for ( int a = 0; a < 3; ++a )
+                                        gu[a] += s[c][n] * g[n][a];
+                                for ( int n = lo; n < hi; ++n )
+                                    out[c][n] += wdet * ( g[n][0] * gu[0] + g[n][1] * gu[1] + g[n][2] * gu[2] );
+                                for ( int n = 0; n < 6; ++n )
+                                {
+                                    const int dg = mode == GM_DIAG || ( mode == GM_BOT && n < 3 ) ||
+                                                   ( mode == GM_TOP && n >= 3 );
+                                    if ( dg )
+                                        out[c][n] += wdet * s[c][n] *
+                                                     ( g[n][0] * g[n][0] + g[n][1] * g[n][1] + g[n][2] * g[n][2] );
+                                }
+                            }
+                        }
+                        for ( int c = 0; c < ncomp; ++c )
+                            for ( int n = 0; n < 6; ++n )
+                                dst[c * ns + idx[n]] += out[c][n];
+                    }
+                }
+    or_halo_sum( L, coords, dst, ncomp );
+}
+
+void or_divkgrad_apply( int L, const double* coords, const double* radii, const double* k, const double* src,
+                        double* dst, int treat_boundary, int diag, int single_quadpoint )
+{
+    /* coupling per cell: div_k_grad.hpp:455-512 (the CMB check wins; diagonal
+     * mode couples nothing and keeps every node's diagonal) */
+    const int N = 1 << L;
+    int*      mode = (int*) malloc( sizeof( int ) * N );
+    for ( int r = 0; r < N; ++r )
+    {
+        const int bot = treat_boundary && r == 0;
+        const int top = treat_boundary && !bot && r == N - 1;
+        mode[r]       = diag ? GM_DIAG : ( bot ? GM_BOT : ( top ? GM_TOP : GM_NEU ) );
+    }
+    grad_family_apply( L, coords, radii, k, 1, src, dst, mode, single_quadpoint );
+    free( mode );
+}
+
+int or_vector_laplace_apply( int L, const double* coords, const double* radii, const double* src, double* dst,
+                             int bc_cmb, int bc_surf, int diag )
+{
+    /* vector_laplace.hpp:181-210: the branch follows the boundary flag of the
+     * cell's own (x, y, r) node: CMB for r = 0, otherwise SURFACE, so a
+     * Dirichlet surface selects the top-boundary coupling for every cell
+     * above the first layer.  Only Neumann and Dirichlet are accepted. */
+    const int N = 1 << L;
+    if ( ( bc_cmb != 0 && bc_cmb != 1 ) || ( bc_surf != 0 && bc_surf != 1 ) )
+        return -1;
+    int* mode = (int*) malloc( sizeof( int ) * N );
+    for ( int r = 0; r < N; ++r )
+    {
+        const int bc = r == 0 ? bc_cmb : bc_surf;
+        mode[r]      = diag ? GM_DIAG : ( bc == 1 ? ( r == 0 ? GM_BOT : GM_TOP ) : GM_NEU );
+    }
+    grad_family_apply( L, coords, radii, NULL, 3, src, dst, mode, 0 );
+    free( mode );
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Stokes coupling blocks: Divergence (divergence.hpp:118-322) and Gradient  */
 /* (gradient.hpp:115-325).  Fine (level L) P1 velocity against coarse        */
 /* (level L-1) P1 pressure shape functions evaluated on the fine wedges      */

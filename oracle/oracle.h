@@ -40,6 +40,15 @@ void or_kerngen_apply( int L, const double* coords, const double* radii, const d
 void or_laplace_apply( int L, const double* coords, const double* radii, const double* src, double* dst,
                        int treat_boundary, int diag );
 
+/* DivKGrad: int k grad u . grad v, k interpolated at the quadrature points;
+ * single_quadpoint selects the 1-point rule */
+void or_divkgrad_apply( int L, const double* coords, const double* radii, const double* k, const double* src,
+                        double* dst, int treat_boundary, int diag, int single_quadpoint );
+/* VectorLaplace on three components; bc codes 0 Neumann, 1 Dirichlet only
+ * (returns -1 otherwise) */
+int or_vector_laplace_apply( int L, const double* coords, const double* radii, const double* src, double* dst,
+                             int bc_cmb, int bc_surf, int diag );
+
 /* Stokes coupling blocks (fine velocity at level L, coarse pressure at L-1) */
 void or_divergence_apply( int L, const double* coords, const double* radii, const double* coords_coarse,
                           const double* src_u, double* dst_p, int bc_cmb, int bc_surf );

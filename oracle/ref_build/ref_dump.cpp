@@ -19,6 +19,8 @@
 //   gradient   L rmin rmax bcc bcs DIR    Gradient<double>: coarse pressure -> fine velocity
 //   prolong / restrict Lf rmin rmax DIR    constant vector transfer between Lf-1 and Lf
 //   kmass   L rmin rmax mode DIR          KMass<double> (0 full, 1 diagonal, 2 lumped)
+//   divkgrad L rmin rmax treat diag single DIR   DivKGrad<double> (k.bin, src.bin)
+//   vlaplace L rmin rmax bcc bcs diag DIR  VectorLaplace<double>
 //   time_kerngen L rmin rmax bcc bcs reps prints seconds per apply (CPU baseline)
 #include <chrono>
 #include <cstdio>
@@ -29,12 +31,14 @@
 
 #include "communication/shell/communication.hpp"
 #include "fe/wedge/operators/shell/epsilon_divdiv_kerngen.hpp"
+#include "fe/wedge/operators/shell/div_k_grad.hpp"
 #include "fe/wedge/operators/shell/divergence.hpp"
 #include "fe/wedge/operators/shell/gradient.hpp"
 #include "fe/wedge/operators/shell/kmass.hpp"
 #include "fe/wedge/operators/shell/laplace.hpp"
 #include "fe/wedge/operators/shell/prolongation_constant.hpp"
 #include "fe/wedge/operators/shell/restriction_constant.hpp"
+#include "fe/wedge/operators/shell/vector_laplace.hpp"
 #include "grid/bit_masks.hpp"
 #include "grid/shell/bit_masks.hpp"
 #include "grid/shell/spherical_shell.hpp"
@@ -259,6 +263,34 @@ int cmd_kmass( int L, double rmin, double rmax, int mode, const std::string& dir
     return 0;
 }
 
+int cmd_divkgrad( int L, double rmin, double rmax, int treat, int diag, int single, const std::string& dir )
+{
+    Setup                            s( L, rmin, rmax );
+    linalg::VectorQ1Scalar< double > k( "k", s.domain, s.omask ), src( "src", s.domain, s.omask ),
+        dst( "dst", s.domain, s.omask );
+    view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", s.nodes ).data() );
+    view_from_host( src.grid_data(), read_file< double >( dir + "/src.bin", s.nodes ).data() );
+    fe::wedge::operators::shell::DivKGrad< double > op( s.domain, s.coords, s.radii, s.bmask, k.grid_data(),
+                                                        treat != 0, diag != 0 );
+    op.set_single_quadpoint( single != 0 );
+    linalg::apply( op, src, dst );
+    auto out = view_to_host( dst.grid_data() );
+    write_file( dir + "/dst.bin", out.data(), out.size() );
+    return 0;
+}
+
+int cmd_vlaplace( int L, double rmin, double rmax, int bcc, int bcs, int diag, const std::string& dir )
+{
+    Setup              s( L, rmin, rmax );
+    BoundaryConditions b = { { ShellBoundaryFlag::CMB, bc_of( bcc ) }, { ShellBoundaryFlag::SURFACE, bc_of( bcs ) } };
+    linalg::VectorQ1Vec< double > src( "src", s.domain, s.omask ), dst( "dst", s.domain, s.omask );
+    load_vec( src, dir + "/src.bin", s.nodes );
+    fe::wedge::operators::shell::VectorLaplace< double > op( s.domain, s.coords, s.radii, s.bmask, b, diag != 0 );
+    linalg::apply( op, src, dst );
+    save_vec( dst, dir + "/dst.bin", s.nodes );
+    return 0;
+}
+
 } // namespace
 
 int main( int argc, char** argv )
@@ -284,6 +316,10 @@ int main( int argc, char** argv )
         return cmd_transfer( cmd == "prolong", I( 2 ), D( 3 ), D( 4 ), argv[5] );
     if ( cmd == "kmass" && argc == 7 )
         return cmd_kmass( I( 2 ), D( 3 ), D( 4 ), I( 5 ), argv[6] );
+    if ( cmd == "divkgrad" && argc == 9 )
+        return cmd_divkgrad( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
+    if ( cmd == "vlaplace" && argc == 9 )
+        return cmd_vlaplace( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( cmd == "laplace" && argc == 8 )
         return cmd_laplace( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     std::fprintf( stderr, "ref_dump: bad command line\n" );

@@ -74,6 +74,18 @@ _SIGS = {
     "tn_pcg_update_f64": (c_int, [c_int, P(c_void_p), P(c_void_p), P(c_void_p), P(c_void_p), P(c_void_p), c_void_p,
                                   c_int, c_double, c_double, c_void_p]),
     "tn_pcg_direction_f64": (c_int, [c_int, P(c_void_p), P(c_void_p), P(c_void_p), c_void_p, c_void_p]),
+    "tn_divkgrad_apply_f64": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
+                                      c_void_p]),
+    "tn_divkgrad_apply_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
+                                      c_void_p]),
+    "tn_vector_laplace_apply_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, P(c_void_p), P(c_void_p),
+                                            c_void_p]),
+    "tn_vector_laplace_apply_f32": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, P(c_void_p), P(c_void_p),
+                                            c_void_p]),
+    "tn_epsdivdiv_kgrad_f64": (c_int, [c_void_p, c_int, c_int, c_int, P(c_void_p), P(c_void_p), c_void_p, c_void_p]),
+    "tn_epsdivdiv_kgrad_f32": (c_int, [c_void_p, c_int, c_int, c_int, P(c_void_p), P(c_void_p), c_void_p, c_void_p]),
+    "tn_stokes_viscosity_backward": (c_int, [c_void_p, P(c_void_p), P(c_void_p), c_int, c_void_p, P(c_void_p),
+                                             c_void_p, P(c_int)]),
     "tn_laplace_pcg_solve_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, P(c_int),
                                          P(c_double)]),
     "tn_stokes_solver_create": (c_int, [P(StokesParams), c_double, c_double, c_void_p, P(c_void_p)]),

@@ -322,6 +322,70 @@ extern "C" int tn_stokes_apply( tn_stokes_solver* s, const double* const* u, con
     }
 }
 
+extern "C" int tn_stokes_viscosity_backward( tn_stokes_solver* s, const double* const* u, const double* const* grad_u,
+                                             int comm_mode, double* grad_log_k, double* const* lambda_u,
+                                             double* lambda_p, int* iterations )
+{
+    TN_CHECK_ARG( s && u && grad_u && grad_log_k, "tn_stokes_viscosity_backward: null argument" );
+    try
+    {
+        const int                 L  = s->prm.level;
+        const Mesh&               mu = s->mesh[L];
+        const tn_mesh*            m  = mu.get();
+        const size_t              nu = mu.stored_nodes(), np = s->mesh[L - 1].stored_nodes();
+        VectorQ1IsoQ2Q1< double > b( mu, s->mesh[L - 1] ), lam( mu, s->mesh[L - 1] );
+        // adjoint right-hand side: the copy-wise derivative summed over the
+        // copies of every node (the derivative with respect to the unique
+        // node), with the velocity boundary treatment of the forward RHS
+        for ( int c = 0; c < 3; ++c )
+            TN_CUDA_TRY( cudaMemcpyAsync( b.block_1().comp( c ), grad_u[c], sizeof( double ) * nu,
+                                          cudaMemcpyDeviceToDevice, stream() ) );
+        b.block_1().halo_sum();
+        const int bcc = s->prm.bc_cmb, bcs = s->prm.bc_surface;
+        for ( int c = 0; c < 3; ++c )
+        {
+            if ( bcc == TN_BC_DIRICHLET )
+                TN_CUDA_TRY( cudaMemset2DAsync( b.block_1().comp( c ), sizeof( double ) * m->n1, 0, sizeof( double ),
+                                                m->nlat, stream() ) );
+            if ( bcs == TN_BC_DIRICHLET )
+                TN_CUDA_TRY( cudaMemset2DAsync( b.block_1().comp( c ) + m->N, sizeof( double ) * m->n1, 0,
+                                                sizeof( double ), m->nlat, stream() ) );
+        }
+        if ( bcc == TN_BC_FREESLIP || bcs == TN_BC_FREESLIP )
+        {
+            double* f[3];
+            b.block_1().ptrs( f );
+            check( tn_freeslip_project_f64( m, f, bcc == TN_BC_FREESLIP, bcs == TN_BC_FREESLIP, stream() ),
+                   "freeslip_project" );
+        }
+        // adjoint solve (the Stokes operator is symmetric)
+        s->run( lam, b );
+        if ( iterations )
+            *iterations = s->iterations;
+        // dJ/dlog k = -k (d (lambda^T K(k) x) / dk)
+        const double* pu[3] = { u[0], u[1], u[2] };
+        const double* pl[3] = { lam.block_1().comp( 0 ), lam.block_1().comp( 1 ), lam.block_1().comp( 2 ) };
+        check( tn_epsdivdiv_kgrad_f64( m, bcc, bcs, comm_mode, pu, pl, grad_log_k, stream() ), "kgrad" );
+        VectorQ1Scalar< double > g( mu, grad_log_k );
+        scale_in_place( g, s->k64[L] );
+        lincomb( g, { -1.0 }, { g } );
+        if ( lambda_u )
+            for ( int c = 0; c < 3; ++c )
+                TN_CUDA_TRY( cudaMemcpyAsync( lambda_u[c], lam.block_1().comp( c ), sizeof( double ) * nu,
+                                              cudaMemcpyDeviceToDevice, stream() ) );
+        if ( lambda_p )
+            TN_CUDA_TRY( cudaMemcpyAsync( lambda_p, lam.block_2().data(), sizeof( double ) * np,
+                                          cudaMemcpyDeviceToDevice, stream() ) );
+        TN_CUDA_TRY( cudaStreamSynchronize( stream() ) );
+        return TN_OK;
+    }
+    catch ( const std::exception& e )
+    {
+        set_error( std::string( "tn_stokes_viscosity_backward: " ) + e.what() );
+        return TN_ERR_STATE;
+    }
+}
+
 extern "C" int tn_stokes_solver_destroy( tn_stokes_solver* s )
 {
     delete s;

@@ -172,6 +172,42 @@ class Laplace:
                   ctypes.c_void_p(dst.data.data_ptr()), _stream()), "laplace_apply")
 
 
+class DivKGrad:
+    """DivKGrad (fe/wedge/operators/shell/div_k_grad.hpp:18): int k grad u . grad v."""
+
+    def __init__(self, mesh, k, treat_boundary, diagonal=False, apply_mode=C.APPLY_REPLACE,
+                 comm_mode=C.COMM_ADDITIVE, single_quadpoint=False):
+        self.mesh, self.k = mesh, k
+        self.treat, self.diag, self.am, self.cm = int(treat_boundary), int(diagonal), apply_mode, comm_mode
+        self.single = int(single_quadpoint)
+
+    def set_diagonal(self, v):
+        self.diag = int(v)
+
+    def set_single_quadpoint(self, v):
+        self.single = int(v)
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_divkgrad_apply_{src.tag}")
+        C.check(f(self.mesh.handle, ctypes.c_void_p(self.k.data.data_ptr()), self.treat, self.diag, self.single,
+                  self.am, self.cm, ctypes.c_void_p(src.data.data_ptr()), ctypes.c_void_p(dst.data.data_ptr()),
+                  _stream()), "divkgrad_apply")
+
+
+class VectorLaplace:
+    """VectorLaplace (fe/wedge/operators/shell/vector_laplace.hpp:32); Neumann / Dirichlet only."""
+
+    def __init__(self, mesh, bc_cmb, bc_surface, diagonal=False, apply_mode=C.APPLY_REPLACE,
+                 comm_mode=C.COMM_ADDITIVE):
+        self.mesh, self.bc = mesh, (bc_cmb, bc_surface)
+        self.diag, self.am, self.cm = int(diagonal), apply_mode, comm_mode
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_vector_laplace_apply_{src.tag}")
+        C.check(f(self.mesh.handle, self.bc[0], self.bc[1], self.diag, self.am, self.cm, src.comp_ptrs(),
+                  dst.comp_ptrs(), _stream()), "vector_laplace_apply")
+
+
 class KMass:
     """KMass (fe/wedge/operators/shell/kmass.hpp:17); k=None gives Mass. mode: 0 full, 1 diagonal, 2 lumped."""
 
@@ -282,6 +318,16 @@ class StokesSolver:
         C.check(C.lib().tn_stokes_history(self._h, out, n.value, ctypes.byref(n), ctypes.byref(skips)), "history")
         return list(out[:n.value]), skips.value
 
+    def viscosity_backward(self, u, grad_u, grad_log_k, comm_mode=C.COMM_SKIP, lambda_u=None, lambda_p=None):
+        """dJ/dlog k from the copy-wise dJ/du (adjoint solve + backward kernel); returns adjoint iterations."""
+        it = ctypes.c_int()
+        C.check(C.lib().tn_stokes_viscosity_backward(
+            self._h, u.comp_ptrs(), grad_u.comp_ptrs(), comm_mode, ctypes.c_void_p(grad_log_k.data_ptr()),
+            lambda_u.comp_ptrs() if lambda_u is not None else None,
+            ctypes.c_void_p(lambda_p.data.data_ptr()) if lambda_p is not None else None, ctypes.byref(it)),
+            "viscosity_backward")
+        return it.value
+
     def apply(self, u, p, out_u, out_p):
         C.check(C.lib().tn_stokes_apply(self._h, u.comp_ptrs(), ctypes.c_void_p(p.data.data_ptr()), out_u.comp_ptrs(),
                                         ctypes.c_void_p(out_p.data.data_ptr())), "stokes_apply")
@@ -291,6 +337,13 @@ class StokesSolver:
         if h is not None and h.value and C is not None and C._lib is not None:
             C.lib().tn_stokes_solver_destroy(h)
             self._h = None
+
+
+def epsdivdiv_kgrad(mesh, bc_cmb, bc_surface, u, lam, out, comm_mode=C.COMM_ADDITIVE):
+    """out = d(lam^T A(k) u)/dk (tn_epsdivdiv_kgrad_*); out is a VectorQ1Scalar."""
+    f = getattr(C.lib(), f"tn_epsdivdiv_kgrad_{u.tag}")
+    C.check(f(mesh.handle, bc_cmb, bc_surface, comm_mode, u.comp_ptrs(), lam.comp_ptrs(),
+              ctypes.c_void_p(out.data.data_ptr()), _stream()), "epsdivdiv_kgrad")
 
 
 def freeslip_project(u, cmb=True, surface=True):

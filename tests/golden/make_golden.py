@@ -27,6 +27,8 @@ KERNGEN_CASES = [(1, 1, 0), (2, 2, 0), (2, 1, 0), (1, 2, 0), (0, 0, 0), (0, 1, 0
 LAPLACE_CASES = [(1, 0), (0, 0), (1, 1)]
 STOKES_BCS = [(1, 1), (2, 2), (0, 0)]
 KMASS_MODES = [0, 1, 2]
+DIVKGRAD_CASES = [(1, 0, 0), (0, 0, 0), (1, 1, 0), (1, 0, 1)]
+VLAPLACE_CASES = [(1, 1, 0), (0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 1)]
 
 
 def inputs(fine, coarse):
@@ -89,6 +91,13 @@ def main():
         for mode in KMASS_MODES:
             run_ref(["kmass", L, R_MIN, R_MAX, mode, d], d)
             out[f"kmass_{mode}"] = np.fromfile(f"{d}/dst.bin").reshape(fine.shape)
+        for treat, diag, single in DIVKGRAD_CASES:
+            run_ref(["divkgrad", L, R_MIN, R_MAX, treat, diag, single, d], d)
+            out[f"divkgrad_{treat}{diag}{single}"] = np.fromfile(f"{d}/dst.bin").reshape(fine.shape)
+        x["u"].tofile(f"{d}/src.bin")
+        for bcc, bcs, diag in VLAPLACE_CASES:
+            run_ref(["vlaplace", L, R_MIN, R_MAX, bcc, bcs, diag, d], d)
+            out[f"vlaplace_{bcc}{bcs}{diag}"] = np.fromfile(f"{d}/dst.bin").reshape((3,) + fine.shape)
     path = os.path.join(HERE, f"ref_L{L}.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")

@@ -35,6 +35,9 @@ def lib():
         L.or_laplace_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
         L.or_divergence_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
         L.or_gradient_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
+        L.or_divkgrad_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.or_vector_laplace_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.or_vector_laplace_apply.restype = ctypes.c_int
         L.or_prolongation_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D]
         L.or_restriction_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _U8, _D, _D]
         L.or_kmass_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int]
@@ -96,6 +99,22 @@ class Mesh:
         src = np.ascontiguousarray(src, dtype=np.float64)
         lib().or_laplace_apply(self.L, _p(self.coords), _p(self.radii), _p(src), _p(dst),
                                int(treat_boundary), int(diag))
+        return dst
+
+    def divkgrad(self, k, src, treat_boundary=True, diag=False, single=False):
+        dst = np.zeros(self.shape)
+        lib().or_divkgrad_apply(self.L, _p(self.coords), _p(self.radii), _p(np.ascontiguousarray(k, dtype=np.float64)),
+                                _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst), int(treat_boundary),
+                                int(diag), int(single))
+        return dst
+
+    def vector_laplace(self, src, bc_cmb, bc_surf, diag=False):
+        dst = np.zeros((3,) + self.shape)
+        rc = lib().or_vector_laplace_apply(self.L, _p(self.coords), _p(self.radii),
+                                           _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst), bc_cmb, bc_surf,
+                                           int(diag))
+        if rc != 0:
+            raise ValueError("VectorLaplace: Neumann or Dirichlet only")
         return dst
 
     def divergence(self, coarse, u, bc_cmb, bc_surf):

@@ -77,6 +77,18 @@ def test_kmass_matches_reference(case, mode):
     assert rel(fine.kmass(x["k"], x["s"], mode), g[f"kmass_{mode}"]) <= TOL
 
 
+@pytest.mark.parametrize("treat,diag,single", G.DIVKGRAD_CASES)
+def test_divkgrad_matches_reference(case, treat, diag, single):
+    g, fine, _, x = case
+    assert rel(fine.divkgrad(x["k"], x["s"], treat, diag, single), g[f"divkgrad_{treat}{diag}{single}"]) <= TOL
+
+
+@pytest.mark.parametrize("bcc,bcs,diag", G.VLAPLACE_CASES)
+def test_vector_laplace_matches_reference(case, bcc, bcs, diag):
+    g, fine, _, x = case
+    assert rel(fine.vector_laplace(x["u"], bcc, bcs, diag), g[f"vlaplace_{bcc}{bcs}{diag}"]) <= TOL
+
+
 def test_golden_fixture_is_not_trivial(case):
     """A planted error in the oracle's input must break the comparison."""
     g, fine, _, x = case
