@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-stokes", action="store_true", help="skip the level-6 Stokes time-to-1e-8 leg")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the level-5 adjoint viscosity gradient leg")
     return ap.parse_args()
 
 
@@ -134,6 +135,63 @@ def stokes_leg(shell, C, torch, k_np):
         del s
     out["speedup_fp32_mg"] = round(out["fp64_mg"]["seconds"] / out["fp32_mg"]["seconds"], 3)
     return out
+
+
+def smooth_field(coords, radii, seed, blobs=4, width=0.2):
+    """Seeded smooth nodal field (sum of Gaussian blobs), max |value| = 1."""
+    rng = np.random.default_rng(seed)
+    x = coords[:, :, :, None, :] * radii[:, None, None, :, None]
+    f = np.zeros(x.shape[:-1])
+    for _ in range(blobs):
+        c = rng.normal(size=3)
+        c = c / np.linalg.norm(c) * rng.uniform(RMIN + 0.05, RMAX - 0.05)
+        f += rng.normal() * np.exp(-np.sum((x - c) ** 2, axis=-1) / (2 * width ** 2))
+    return f / np.abs(f).max()
+
+
+def adjoint_leg(shell, C, torch, level=5, directions=2, h=1e-5):
+    """Adjoint viscosity gradient at level 5 (velocity L5 / pressure L4):
+    J = 1/2 sum over owned velocity nodes |u - u_obs|^2, u_obs from a solve with
+    a seeded perturbed viscosity; gradient = forward solve + adjoint solve +
+    backward kernel (timed), checked against central differences."""
+    from terraneo_b200.adjoint import stokes_velocity
+    pf, pc = shell.ShellMesh(level, RMIN, RMAX), shell.ShellMesh(level - 1, RMIN, RMAX)
+    coords, radii = pf.geometry()
+    _, omask = pf.masks()
+    k0, _ = synthetic_inputs(coords, radii, None)
+    m0 = torch.as_tensor(np.log(k0), device="cuda")
+    fu, fp = stokes_rhs(shell, pf, coords, radii), shell.VectorQ1Scalar(pc)
+    kw = dict(mg_levels=level - 2, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=False,
+              relative_tolerance=1e-12, max_iterations=2000, restart=100, r_min=RMIN, r_max=RMAX)
+    owned = torch.as_tensor(omask.astype(np.float64), device="cuda")
+    m_obs = m0 + 0.1 * torch.as_tensor(smooth_field(coords, radii, 31), device="cuda")
+    u_obs = stokes_velocity(m_obs, level, fu, fp, **kw).detach()
+
+    def J(m):
+        u = stokes_velocity(m, level, fu, fp, **kw)
+        return 0.5 * (owned * (u - u_obs) ** 2).sum()
+
+    m = m0.clone().requires_grad_(True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    j = J(m)
+    j.backward()
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    grad = m.grad.detach()
+    errs = []
+    for s in range(directions):
+        d = torch.as_tensor(smooth_field(coords, radii, 200 + s), device="cuda")
+        with torch.no_grad():
+            fd = (J(m0 + h * d) - J(m0 - h * d)).item() / (2 * h)
+        ad = float((grad * d).sum())
+        errs.append(abs(fd - ad) / abs(ad))
+    return {"workload": f"adjoint viscosity gradient, velocity level {level} / pressure level {level - 1}, free-slip "
+                        "both radii, J = 1/2 sum_owned |u - u_obs|^2, FP64 solves to 1e-12 (FGMRES(100), FP64 "
+                        f"multigrid over {level - 2} levels)",
+            "seconds_forward_adjoint_backward": round(sec, 4),
+            "J": float(j.item()), "fd_directions": directions, "fd_step": h,
+            "fd_max_rel_error": float(f"{max(errs):.3e}")}
 
 
 class ClockSampler:
@@ -379,6 +437,8 @@ def main():
         }
         if world == 1 and not args.no_stokes:
             line["stokes"] = stokes_leg(shell, C, torch, k_np)
+        if world == 1 and not args.no_adjoint:
+            line["adjoint"] = adjoint_leg(shell, C, torch)
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_baseline(steps=3)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}

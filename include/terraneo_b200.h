@@ -185,6 +185,24 @@ TN_API int tn_restriction_constant_f64( const tn_mesh* fine, const tn_mesh* coar
 TN_API int tn_restriction_constant_f32( const tn_mesh* fine, const tn_mesh* coarse, int ncomp,
                                         const float* const* src, float* const* dst, void* stream );
 
+/* ProlongationLinear / RestrictionLinear (fe/wedge/operators/shell/
+ * prolongation_linear.hpp:14-190, restriction_linear.hpp:14-223, weights
+ * fe/wedge/shell/grid_transfer_linear.hpp): a fine node on a coarse node
+ * copies it, one between radially aligned coarse nodes interpolates by
+ * radius, any other interpolates radially between the chord midpoints of two
+ * lateral coarse pairs (exact for affine functions).  Restriction is the
+ * transpose over OWNED fine nodes followed by the coarse halo sum (Replace).
+ * ncomp fields are transferred with the same weights (the reference's vector
+ * variants are unused; see the design notes). */
+TN_API int tn_prolongation_linear_f64( const tn_mesh* fine, const tn_mesh* coarse, int ncomp, int apply_mode,
+                                       const double* const* src, double* const* dst, void* stream );
+TN_API int tn_prolongation_linear_f32( const tn_mesh* fine, const tn_mesh* coarse, int ncomp, int apply_mode,
+                                       const float* const* src, float* const* dst, void* stream );
+TN_API int tn_restriction_linear_f64( const tn_mesh* fine, const tn_mesh* coarse, int ncomp, const double* const* src,
+                                      double* const* dst, void* stream );
+TN_API int tn_restriction_linear_f32( const tn_mesh* fine, const tn_mesh* coarse, int ncomp, const float* const* src,
+                                      float* const* dst, void* stream );
+
 /* Injection coarse(X,Y,R) = fine(2X,2Y,2R) of `ncomp` fields (coefficient
  * fields on coarser multigrid levels). */
 TN_API int tn_injection_f64( const tn_mesh* fine, const tn_mesh* coarse, int ncomp, const double* const* src,
@@ -307,6 +325,37 @@ TN_API int tn_pcg_direction_f64( int nseg, const tn_mesh* const* mesh, double* c
 TN_API int tn_laplace_pcg_solve_f64( const tn_mesh* mesh, const double* b, double* x, int max_iterations,
                                      double relative_tolerance, double absolute_tolerance, int* iterations,
                                      double* relative_residual );
+
+/* Multigrid-preconditioned CG on DivKGrad (k NULL: k = 1, the Laplace) with
+ * homogeneous Dirichlet elimination on both radii: one V-cycle per CG
+ * iteration over levels [level - mg_levels + 1, level], linear transfers
+ * (prolongation_linear.hpp / restriction_linear.hpp), Jacobi (smoother 1,
+ * jacobi.hpp: smoothing_steps sweeps with jacobi_omega) or Chebyshev
+ * (smoother 0, chebyshev.hpp: chebyshev_order, smoothing_steps sweeps,
+ * power_iterations), unpreconditioned PCG on the coarsest level; coarser
+ * levels use k injected from the finest (the composition of the reference's
+ * tests/test_div_k_grad_multigrid*.cpp).  b, x, k are device fields of the
+ * finest mesh; x holds the initial guess and receives the solution. */
+typedef struct
+{
+    int    level;
+    int    mg_levels;
+    int    smoother;        /* 0 Chebyshev, 1 Jacobi */
+    int    smoothing_steps; /* sweeps before and after the coarse correction */
+    int    chebyshev_order;
+    int    power_iterations;
+    double jacobi_omega;
+    int    vcycles;
+    int    coarse_max_iterations;
+    double coarse_relative_tolerance;
+    int    max_iterations;
+    double relative_tolerance;
+    double absolute_tolerance;
+} tn_scalar_mg_params;
+
+TN_API int tn_divkgrad_mg_pcg_solve_f64( const tn_scalar_mg_params* params, double r_min, double r_max,
+                                         const double* k, const double* b, double* x, int* iterations,
+                                         double* relative_residual );
 
 /* Stokes solver composed as apps/mantlecirculation/mantlecirculation.cpp:486-735:
  * FGMRES(restart) (fgmres.hpp:108) on EpsDivDivStokes [A B^T; B 0]

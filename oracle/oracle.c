@@ -1034,6 +1034,111 @@ void or_restriction_constant( int Lf, int ncomp, const double* coords_c, const u
 /* KMass (fe/wedge/operators/shell/kmass.hpp): int k u v, 3x2 rule, k        */
 /* interpolated at the quadrature points; mode 0 full, 1 diagonal, 2 lumped. */
 /* ------------------------------------------------------------------------ */
+/* ------------------------------------------------------------------------ */
+/* Linear grid transfer (prolongation_linear.hpp:104-189,                    */
+/* restriction_linear.hpp:106-222, weights grid_transfer_linear.hpp:14-158): */
+/* a fine node on a coarse node takes its value; one between two radially    */
+/* aligned coarse nodes interpolates by radius; any other lies on a wedge    */
+/* facet spanned by two lateral coarse pairs and interpolates radially       */
+/* between the chord midpoints of the pairs (weights halved per pair).       */
+/* ------------------------------------------------------------------------ */
+
+static double norm3v( const double v[3] ) { return sqrt( v[0] * v[0] + v[1] * v[1] + v[2] * v[2] ); }
+
+/* contributions (coarse x, y, r, weight) of the coarse nodes to fine node (x, y, r) */
+static int linear_stencil( int Nf, const double* coords_f, const double* radii_f, int d, int x, int y, int r,
+                           int cx[4], int cy[4], int cr[4], double w[4] )
+{
+    const int n1 = Nf + 1;
+    if ( x % 2 == 0 && y % 2 == 0 && r % 2 == 0 )
+    {
+        cx[0] = x / 2, cy[0] = y / 2, cr[0] = r / 2, w[0] = 1.0;
+        return 1;
+    }
+    const int rb = r < Nf ? r / 2 : r / 2 - 1, rt = rb + 1;
+    const double* c  = coords_f + lat_idx( n1, d, x, y ) * 3;
+    const double  Rf = radii_f[d * n1 + r], Rb = radii_f[d * n1 + 2 * rb], Rt = radii_f[d * n1 + 2 * rt];
+    double        fine[3];
+    for ( int a = 0; a < 3; ++a )
+        fine[a] = c[a] * Rf;
+    if ( x % 2 == 0 && y % 2 == 0 )
+    {
+        double pb[3], pt[3];
+        for ( int a = 0; a < 3; ++a )
+            pb[a] = c[a] * Rb, pt[a] = c[a] * Rt;
+        const double nu = ( norm3v( fine ) - norm3v( pb ) ) / ( norm3v( pt ) - norm3v( pb ) );
+        cx[0] = cx[1] = x / 2, cy[0] = cy[1] = y / 2, cr[0] = rb, cr[1] = rt;
+        w[0] = 1.0 - nu, w[1] = nu;
+        return 2;
+    }
+    int x0, x1, y0, y1;
+    if ( x % 2 == 0 )
+        x0 = x1 = x / 2, y0 = y / 2, y1 = y / 2 + 1; /* "vertical" edge */
+    else if ( y % 2 == 0 )
+        x0 = x / 2, x1 = x / 2 + 1, y0 = y1 = y / 2; /* "horizontal" edge */
+    else
+        x0 = x / 2 + 1, x1 = x / 2, y0 = y / 2, y1 = y / 2 + 1; /* "diagonal" edge */
+    const double* c0 = coords_f + lat_idx( n1, d, 2 * x0, 2 * y0 ) * 3;
+    const double* c1 = coords_f + lat_idx( n1, d, 2 * x1, 2 * y1 ) * 3;
+    double        bot[3], top[3];
+    for ( int a = 0; a < 3; ++a )
+    {
+        bot[a] = 0.5 * ( c0[a] * Rb + c1[a] * Rb );
+        top[a] = 0.5 * ( c0[a] * Rt + c1[a] * Rt );
+    }
+    const double nu = ( norm3v( fine ) - norm3v( bot ) ) / ( norm3v( top ) - norm3v( bot ) );
+    const double wb = 0.5 * ( 1.0 - nu ), wt = 0.5 * nu;
+    cx[0] = x0, cy[0] = y0, cr[0] = rb, w[0] = wb;
+    cx[1] = x1, cy[1] = y1, cr[1] = rb, w[1] = wb;
+    cx[2] = x0, cy[2] = y0, cr[2] = rt, w[2] = wt;
+    cx[3] = x1, cy[3] = y1, cr[3] = rt, w[3] = wt;
+    return 4;
+}
+
+void or_prolongation_linear( int Lc, int ncomp, const double* coords_f, const double* radii_f, const double* src,
+                             double* dst )
+{
+    const int    Nf = 2 << Lc, n1f = Nf + 1, n1c = ( 1 << Lc ) + 1;
+    const size_t nsf = (size_t) NDIAMOND * n1f * n1f * n1f, nsc = (size_t) NDIAMOND * n1c * n1c * n1c;
+    for ( int c = 0; c < ncomp; ++c )
+        for ( int d = 0; d < NDIAMOND; ++d )
+            for ( int x = 0; x <= Nf; ++x )
+                for ( int y = 0; y <= Nf; ++y )
+                    for ( int r = 0; r <= Nf; ++r )
+                    {
+                        int    cx[4], cy[4], cr[4];
+                        double w[4], v = 0.0;
+                        const int k = linear_stencil( Nf, coords_f, radii_f, d, x, y, r, cx, cy, cr, w );
+                        for ( int i = 0; i < k; ++i )
+                            v += w[i] * src[c * nsc + node_idx( n1c, d, cx[i], cy[i], cr[i] )];
+                        dst[c * nsf + node_idx( n1f, d, x, y, r )] = v;
+                    }
+}
+
+void or_restriction_linear( int Lf, int ncomp, const double* coords_f, const double* radii_f, const double* coords_c,
+                            const uint8_t* omask_f, const double* src, double* dst )
+{
+    const int    Nf = 1 << Lf, n1f = Nf + 1, n1c = Nf / 2 + 1;
+    const size_t nsf = (size_t) NDIAMOND * n1f * n1f * n1f, nsc = (size_t) NDIAMOND * n1c * n1c * n1c;
+    memset( dst, 0, sizeof( double ) * nsc * ncomp );
+    for ( int c = 0; c < ncomp; ++c )
+        for ( int d = 0; d < NDIAMOND; ++d )
+            for ( int x = 0; x <= Nf; ++x )
+                for ( int y = 0; y <= Nf; ++y )
+                    for ( int r = 0; r <= Nf; ++r )
+                    {
+                        const size_t f = node_idx( n1f, d, x, y, r );
+                        if ( !omask_f[f] )
+                            continue;
+                        int       cx[4], cy[4], cr[4];
+                        double    w[4];
+                        const int k = linear_stencil( Nf, coords_f, radii_f, d, x, y, r, cx, cy, cr, w );
+                        for ( int i = 0; i < k; ++i )
+                            dst[c * nsc + node_idx( n1c, d, cx[i], cy[i], cr[i] )] += w[i] * src[c * nsf + f];
+                    }
+    or_halo_sum( Lf - 1, coords_c, dst, ncomp );
+}
+
 void or_kmass_apply( int L, const double* coords, const double* radii, const double* k, const double* src, double* dst,
                      int mode )
 {

@@ -64,6 +64,13 @@ void or_prolongation_constant( int Lc, int ncomp, const double* src_coarse, doub
 void or_restriction_constant( int Lf, int ncomp, const double* coords_coarse, const uint8_t* omask_fine,
                               const double* src_fine, double* dst_coarse );
 
+/* linear grid transfer of ncomp fields (coords / radii of the FINE mesh) */
+void or_prolongation_linear( int Lc, int ncomp, const double* coords_fine, const double* radii_fine,
+                             const double* src_coarse, double* dst_fine );
+void or_restriction_linear( int Lf, int ncomp, const double* coords_fine, const double* radii_fine,
+                            const double* coords_coarse, const uint8_t* omask_fine, const double* src_fine,
+                            double* dst_coarse );
+
 /* Krylov vector kernels */
 double or_masked_dot( size_t n, const double* a, const double* b, const uint8_t* omask );
 

@@ -20,6 +20,7 @@
 //   prolong / restrict Lf rmin rmax DIR    constant vector transfer between Lf-1 and Lf
 //   kmass   L rmin rmax mode DIR          KMass<double> (0 full, 1 diagonal, 2 lumped)
 //   divkgrad L rmin rmax treat diag single DIR   DivKGrad<double> (k.bin, src.bin)
+//   prolong_linear / restrict_linear Lf rmin rmax DIR  scalar linear transfer between Lf-1 and Lf
 //   vlaplace L rmin rmax bcc bcs diag DIR  VectorLaplace<double>
 //   time_kerngen L rmin rmax bcc bcs reps prints seconds per apply (CPU baseline)
 #include <chrono>
@@ -37,7 +38,9 @@
 #include "fe/wedge/operators/shell/kmass.hpp"
 #include "fe/wedge/operators/shell/laplace.hpp"
 #include "fe/wedge/operators/shell/prolongation_constant.hpp"
+#include "fe/wedge/operators/shell/prolongation_linear.hpp"
 #include "fe/wedge/operators/shell/restriction_constant.hpp"
+#include "fe/wedge/operators/shell/restriction_linear.hpp"
 #include "fe/wedge/operators/shell/vector_laplace.hpp"
 #include "grid/bit_masks.hpp"
 #include "grid/shell/bit_masks.hpp"
@@ -263,6 +266,29 @@ int cmd_kmass( int L, double rmin, double rmax, int mode, const std::string& dir
     return 0;
 }
 
+int cmd_transfer_linear( bool prolong, int Lf, double rmin, double rmax, const std::string& dir )
+{
+    Setup                            f( Lf, rmin, rmax ), c( Lf - 1, rmin, rmax );
+    linalg::VectorQ1Scalar< double > uf( "uf", f.domain, f.omask ), uc( "uc", c.domain, c.omask );
+    if ( prolong )
+    {
+        view_from_host( uc.grid_data(), read_file< double >( dir + "/src.bin", c.nodes ).data() );
+        fe::wedge::operators::shell::ProlongationLinear< double > P( f.coords, f.radii );
+        linalg::apply( P, uc, uf );
+        auto out = view_to_host( uf.grid_data() );
+        write_file( dir + "/dst.bin", out.data(), out.size() );
+    }
+    else
+    {
+        view_from_host( uf.grid_data(), read_file< double >( dir + "/src.bin", f.nodes ).data() );
+        fe::wedge::operators::shell::RestrictionLinear< double > R( c.domain, f.coords, f.radii );
+        linalg::apply( R, uf, uc );
+        auto out = view_to_host( uc.grid_data() );
+        write_file( dir + "/dst.bin", out.data(), out.size() );
+    }
+    return 0;
+}
+
 int cmd_divkgrad( int L, double rmin, double rmax, int treat, int diag, int single, const std::string& dir )
 {
     Setup                            s( L, rmin, rmax );
@@ -316,6 +342,8 @@ int main( int argc, char** argv )
         return cmd_transfer( cmd == "prolong", I( 2 ), D( 3 ), D( 4 ), argv[5] );
     if ( cmd == "kmass" && argc == 7 )
         return cmd_kmass( I( 2 ), D( 3 ), D( 4 ), I( 5 ), argv[6] );
+    if ( ( cmd == "prolong_linear" || cmd == "restrict_linear" ) && argc == 6 )
+        return cmd_transfer_linear( cmd == "prolong_linear", I( 2 ), D( 3 ), D( 4 ), argv[5] );
     if ( cmd == "divkgrad" && argc == 9 )
         return cmd_divkgrad( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( cmd == "vlaplace" && argc == 9 )

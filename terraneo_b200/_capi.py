@@ -33,6 +33,13 @@ class StokesParams(ctypes.Structure):
                 ("absolute_tolerance", c_double)]
 
 
+class ScalarMGParams(ctypes.Structure):
+    _fields_ = [("level", c_int), ("mg_levels", c_int), ("smoother", c_int), ("smoothing_steps", c_int),
+                ("chebyshev_order", c_int), ("power_iterations", c_int), ("jacobi_omega", c_double),
+                ("vcycles", c_int), ("coarse_max_iterations", c_int), ("coarse_relative_tolerance", c_double),
+                ("max_iterations", c_int), ("relative_tolerance", c_double), ("absolute_tolerance", c_double)]
+
+
 class TNError(RuntimeError):
     pass
 
@@ -86,6 +93,12 @@ _SIGS = {
     "tn_epsdivdiv_kgrad_f32": (c_int, [c_void_p, c_int, c_int, c_int, P(c_void_p), P(c_void_p), c_void_p, c_void_p]),
     "tn_stokes_viscosity_backward": (c_int, [c_void_p, P(c_void_p), P(c_void_p), c_int, c_void_p, P(c_void_p),
                                              c_void_p, P(c_int)]),
+    "tn_prolongation_linear_f64": (c_int, [c_void_p, c_void_p, c_int, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_prolongation_linear_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_restriction_linear_f64": (c_int, [c_void_p, c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_restriction_linear_f32": (c_int, [c_void_p, c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_divkgrad_mg_pcg_solve_f64": (c_int, [P(ScalarMGParams), c_double, c_double, c_void_p, c_void_p, c_void_p,
+                                             P(c_int), P(c_double)]),
     "tn_laplace_pcg_solve_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, P(c_int),
                                          P(c_double)]),
     "tn_stokes_solver_create": (c_int, [P(StokesParams), c_double, c_double, c_void_p, P(c_void_p)]),

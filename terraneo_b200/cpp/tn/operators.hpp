@@ -101,6 +101,43 @@ class Laplace
     OperatorCommunicationMode cm_ = OperatorCommunicationMode::CommunicateAdditively;
 };
 
+// DivKGrad (div_k_grad.hpp:18): int k grad u . grad v
+template < typename T >
+class DivKGrad
+{
+  public:
+    using SrcVectorType = VectorQ1Scalar< T >;
+    using DstVectorType = VectorQ1Scalar< T >;
+    using ScalarType    = T;
+    DivKGrad( const Mesh& mesh, const VectorQ1Scalar< T >& k, bool treat_boundary, bool diagonal = false )
+    : mesh_( mesh ), k_( k ), treat_( treat_boundary ), diag_( diagonal )
+    {}
+    void set_diagonal( bool v ) { diag_ = v; }
+    void set_single_quadpoint( bool v ) { single_ = v; }
+    void set_operator_apply_and_communication_modes( OperatorApplyMode am, OperatorCommunicationMode cm )
+    {
+        am_ = am, cm_ = cm;
+    }
+    void apply_impl( const SrcVectorType& src, DstVectorType& dst )
+    {
+        if constexpr ( std::is_same_v< T, double > )
+            check( tn_divkgrad_apply_f64( mesh_.get(), k_.comp( 0 ), treat_, diag_, single_, int( am_ ), int( cm_ ),
+                                          src.comp( 0 ), dst.comp( 0 ), stream() ),
+                   "divkgrad apply" );
+        else
+            check( tn_divkgrad_apply_f32( mesh_.get(), k_.comp( 0 ), treat_, diag_, single_, int( am_ ), int( cm_ ),
+                                          src.comp( 0 ), dst.comp( 0 ), stream() ),
+                   "divkgrad apply" );
+    }
+
+  private:
+    Mesh                      mesh_;
+    VectorQ1Scalar< T >       k_;
+    bool                      treat_, diag_, single_ = false;
+    OperatorApplyMode         am_ = OperatorApplyMode::Replace;
+    OperatorCommunicationMode cm_ = OperatorCommunicationMode::CommunicateAdditively;
+};
+
 // Gradient (gradient.hpp:28): coarse pressure -> fine velocity
 template < typename T >
 class Gradient
@@ -238,6 +275,53 @@ class ProlongationVecConstant
   private:
     Mesh              f_, c_;
     OperatorApplyMode am_;
+};
+
+// ProlongationLinear / RestrictionLinear (prolongation_linear.hpp:15,
+// restriction_linear.hpp:15) on scalar fields
+template < typename T >
+class ProlongationLinear
+{
+  public:
+    using SrcVectorType = VectorQ1Scalar< T >;
+    using DstVectorType = VectorQ1Scalar< T >;
+    ProlongationLinear( const Mesh& fine, const Mesh& coarse, OperatorApplyMode am = OperatorApplyMode::Replace )
+    : f_( fine ), c_( coarse ), am_( am )
+    {}
+    void apply_impl( const SrcVectorType& src, DstVectorType& dst )
+    {
+        const T* s[1] = { src.comp( 0 ) };
+        T*       d[1] = { dst.comp( 0 ) };
+        if constexpr ( std::is_same_v< T, double > )
+            check( tn_prolongation_linear_f64( f_.get(), c_.get(), 1, int( am_ ), s, d, stream() ), "prolongation" );
+        else
+            check( tn_prolongation_linear_f32( f_.get(), c_.get(), 1, int( am_ ), s, d, stream() ), "prolongation" );
+    }
+
+  private:
+    Mesh              f_, c_;
+    OperatorApplyMode am_;
+};
+
+template < typename T >
+class RestrictionLinear
+{
+  public:
+    using SrcVectorType = VectorQ1Scalar< T >;
+    using DstVectorType = VectorQ1Scalar< T >;
+    RestrictionLinear( const Mesh& fine, const Mesh& coarse ) : f_( fine ), c_( coarse ) {}
+    void apply_impl( const SrcVectorType& src, DstVectorType& dst )
+    {
+        const T* s[1] = { src.comp( 0 ) };
+        T*       d[1] = { dst.comp( 0 ) };
+        if constexpr ( std::is_same_v< T, double > )
+            check( tn_restriction_linear_f64( f_.get(), c_.get(), 1, s, d, stream() ), "restriction" );
+        else
+            check( tn_restriction_linear_f32( f_.get(), c_.get(), 1, s, d, stream() ), "restriction" );
+    }
+
+  private:
+    Mesh f_, c_;
 };
 
 template < typename T >

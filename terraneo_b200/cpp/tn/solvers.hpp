@@ -256,6 +256,35 @@ class Chebyshev
     double           ev_      = 0;
 };
 
+// Jacobi (jacobi.hpp:14-62): x += omega D^{-1} (b - A x), `iterations`
+// times; the update is one fused pass (tn_vec_chebyshev_step with beta = 0).
+template < typename Op >
+class Jacobi
+{
+  public:
+    using V = typename Op::SrcVectorType;
+    Jacobi( const V& inverse_diagonal, int iterations, std::vector< V > tmps, double omega = 1.0 )
+    : inv_diag_( inverse_diagonal ), iterations_( iterations ), tmps_( std::move( tmps ) ), omega_( omega )
+    {
+        if ( tmps_.size() < 2 )
+            throw std::runtime_error( "Jacobi: needs 2 temporary vectors" );
+    }
+    void solve_impl( Op& A, V& x, const V& b )
+    {
+        for ( int it = 0; it < iterations_; ++it )
+        {
+            apply( A, x, tmps_[0] );
+            chebyshev_step( x, tmps_[1], b, tmps_[0], inv_diag_, omega_, 0.0 );
+        }
+    }
+
+  private:
+    V                inv_diag_;
+    int              iterations_;
+    std::vector< V > tmps_;
+    double           omega_;
+};
+
 // Multigrid V-cycle (multigrid.hpp:24-211).  Level 0 is the coarsest.
 template < typename Op, typename P, typename R, typename Smoother, typename Coarse >
 class Multigrid

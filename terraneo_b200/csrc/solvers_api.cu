@@ -392,6 +392,133 @@ extern "C" int tn_stokes_solver_destroy( tn_stokes_solver* s )
     return TN_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Multigrid-preconditioned CG on DivKGrad with homogeneous Dirichlet radii:
+// linear transfers, Jacobi or Chebyshev smoothing, coarse PCG, coarser
+// operators re-discretised with injected k (the composition of the
+// reference's tests/test_div_k_grad_multigrid*.cpp and
+// tests/test_laplace_multigrid*.cpp).
+namespace {
+
+using DKG = DivKGrad< double >;
+
+// runtime choice of the two smoothers of the reference
+struct ScalarSmoother
+{
+    std::shared_ptr< Jacobi< DKG > >    jacobi;
+    std::shared_ptr< Chebyshev< DKG > > cheb;
+    void solve_impl( DKG& A, VectorQ1Scalar< double >& x, const VectorQ1Scalar< double >& b )
+    {
+        if ( jacobi )
+            solve( *jacobi, A, x, b );
+        else
+            solve( *cheb, A, x, b );
+    }
+};
+
+using ScalarMG = Multigrid< DKG, ProlongationLinear< double >, RestrictionLinear< double >, ScalarSmoother,
+                            DevicePCG< DKG > >;
+
+struct MGPreconditioner
+{
+    std::shared_ptr< ScalarMG > mg;
+    void solve_impl( DKG& A, VectorQ1Scalar< double >& z, const VectorQ1Scalar< double >& r )
+    {
+        assign( z, 0.0 );
+        solve( *mg, A, z, r );
+    }
+};
+
+}  // namespace
+
+extern "C" int tn_divkgrad_mg_pcg_solve_f64( const tn_scalar_mg_params* p, double r_min, double r_max, const double* k,
+                                             const double* b, double* x, int* iterations, double* relative_residual )
+{
+    TN_CHECK_ARG( p && b && x, "tn_divkgrad_mg_pcg_solve_f64: null argument" );
+    TN_CHECK_ARG( p->mg_levels >= 2 && p->level - p->mg_levels + 1 >= 0, "tn_divkgrad_mg_pcg_solve_f64: bad levels" );
+    TN_CHECK_ARG( p->smoother == 0 || p->smoother == 1, "tn_divkgrad_mg_pcg_solve_f64: smoother must be 0 or 1" );
+    try
+    {
+        const int                                L = p->level, Lmin = L - p->mg_levels + 1;
+        std::vector< Mesh >                      mesh( L + 1 );
+        std::vector< VectorQ1Scalar< double > >  kl( L + 1 );
+        for ( int l = Lmin; l <= L; ++l )
+        {
+            mesh[l] = Mesh( l, r_min, r_max );
+            kl[l]   = VectorQ1Scalar< double >( mesh[l] );
+        }
+        if ( k )
+            TN_CUDA_TRY( cudaMemcpy( kl[L].data(), k, sizeof( double ) * mesh[L].stored_nodes(), cudaMemcpyDeviceToDevice ) );
+        else
+            assign( kl[L], 1.0 );
+        for ( int l = L - 1; l >= Lmin; --l )
+        {
+            const double* src[1] = { kl[l + 1].data() };
+            double*       dst[1] = { kl[l].data() };
+            check( tn_injection_f64( mesh[l + 1].get(), mesh[l].get(), 1, src, dst, stream() ), "injection" );
+        }
+        std::vector< ProlongationLinear< double > > P;
+        std::vector< RestrictionLinear< double > >  R;
+        std::vector< DKG >                          A;
+        std::vector< VectorQ1Scalar< double > >     tr, te, tmp;
+        std::vector< ScalarSmoother >               sm;
+        for ( int l = Lmin; l <= L; ++l )
+        {
+            DKG op( mesh[l], kl[l], true );
+            VectorQ1Scalar< double > ones( mesh[l] ), inv( mesh[l] );
+            assign( ones, 1.0 );
+            op.set_diagonal( true );
+            apply( op, ones, inv );
+            op.set_diagonal( false );
+            invert_entries( inv );
+            std::vector< VectorQ1Scalar< double > > t2{ VectorQ1Scalar< double >( mesh[l] ),
+                                                        VectorQ1Scalar< double >( mesh[l] ) };
+            ScalarSmoother s;
+            if ( p->smoother == 1 )
+                s.jacobi = std::make_shared< Jacobi< DKG > >( inv, p->smoothing_steps, t2, p->jacobi_omega );
+            else
+                s.cheb = std::make_shared< Chebyshev< DKG > >( p->chebyshev_order, inv, t2, p->smoothing_steps,
+                                                               p->power_iterations );
+            sm.push_back( s );
+            tmp.emplace_back( mesh[l] );
+            A.push_back( op );
+            if ( l < L )
+            {
+                tr.emplace_back( mesh[l] );
+                te.emplace_back( mesh[l] );
+                P.emplace_back( mesh[l + 1], mesh[l], OperatorApplyMode::Add );
+                R.emplace_back( mesh[l + 1], mesh[l] );
+            }
+        }
+        DKG                                     Afine = A.back();
+        std::vector< DKG >                      Ac( A.begin(), A.end() - 1 );
+        std::vector< VectorQ1Scalar< double > > ct{ VectorQ1Scalar< double >( mesh[Lmin] ),
+                                                    VectorQ1Scalar< double >( mesh[Lmin] ),
+                                                    VectorQ1Scalar< double >( mesh[Lmin] ) };
+        DevicePCG< DKG > coarse( IterativeSolverParameters{ p->coarse_max_iterations, p->coarse_relative_tolerance, 1e-30 },
+                                 ct );
+        MGPreconditioner prec{ std::make_shared< ScalarMG >( P, R, Ac, tr, te, tmp, sm, coarse, p->vcycles ) };
+        std::vector< VectorQ1Scalar< double > > t4;
+        for ( int i = 0; i < 4; ++i )
+            t4.emplace_back( mesh[L] );
+        PCG< DKG, MGPreconditioner > pcg(
+            IterativeSolverParameters{ p->max_iterations, p->relative_tolerance, p->absolute_tolerance }, t4, prec );
+        VectorQ1Scalar< double > vb( mesh[L], const_cast< double* >( b ) ), vx( mesh[L], x );
+        solve( pcg, Afine, vx, vb );
+        TN_CUDA_TRY( cudaDeviceSynchronize() );
+        if ( iterations )
+            *iterations = pcg.stats.iterations;
+        if ( relative_residual )
+            *relative_residual = pcg.stats.relative_residuals.back();
+        return TN_OK;
+    }
+    catch ( const std::exception& e )
+    {
+        set_error( std::string( "tn_divkgrad_mg_pcg_solve_f64: " ) + e.what() );
+        return TN_ERR_STATE;
+    }
+}
+
 extern "C" int tn_laplace_pcg_solve_f64( const tn_mesh* mesh, const double* b, double* x, int max_iterations,
                                          double relative_tolerance, double absolute_tolerance, int* iterations,
                                          double* relative_residual )

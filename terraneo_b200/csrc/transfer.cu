@@ -1,6 +1,7 @@
-// Constant grid transfer between levels L-1 (coarse) and L (fine)
+// Grid transfer between levels L-1 (coarse) and L (fine): constant
 // (fe/wedge/shell/grid_transfer_constant.hpp, prolongation_constant.hpp,
-// restriction_constant.hpp).
+// restriction_constant.hpp) and linear (grid_transfer_linear.hpp,
+// prolongation_linear.hpp, restriction_linear.hpp).
 //
 // The reference scatters from each coarse node into its 21-point fine
 // stencil with atomics.  Here both directions are gathers without atomics:
@@ -9,6 +10,7 @@
 //  * restriction: each coarse node sums its 21-point stencil of OWNED fine
 //    values with the same weights, then the coarse halo adds duplicates.
 #include "common.cuh"
+#include "wedge.cuh"
 
 namespace tn {
 
@@ -126,6 +128,105 @@ __global__ void freeslip_project_kernel( int n1, const double* __restrict__ coor
     y.p[0][i] = T( v[0] - dt * n[0] ), y.p[1][i] = T( v[1] - dt * n[1] ), y.p[2][i] = T( v[2] - dt * n[2] );
 }
 
+// Linear transfer stencil of fine node (d, x, y, r) on a fine mesh of Nf
+// cells (grid_transfer_linear.hpp:14-158, prolongation_linear.hpp:104-189):
+// on a coarse node: weight 1; between two radially aligned coarse nodes:
+// interpolation by radius; otherwise on the wedge facet of two lateral coarse
+// pairs: radial interpolation between the pairs' chord midpoints, each pair
+// member weighted half.  Returns the number of (coarse x, y, r, weight).
+__device__ int linear_stencil( int Nf, const double* __restrict__ coords, const double* __restrict__ radii, int d,
+                               int x, int y, int r, int cx[4], int cy[4], int cr[4], double w[4] )
+{
+    const int n1 = Nf + 1;
+    if ( !( x & 1 ) && !( y & 1 ) && !( r & 1 ) )
+    {
+        cx[0] = x / 2, cy[0] = y / 2, cr[0] = r / 2, w[0] = 1.0;
+        return 1;
+    }
+    const int     rb = r < Nf ? r / 2 : r / 2 - 1, rt = rb + 1;
+    const double* c  = coords + lat_index( n1, d, x, y ) * 3;
+    const double  Rf = radii[d * n1 + r], Rb = radii[d * n1 + 2 * rb], Rt = radii[d * n1 + 2 * rt];
+    const double  nf = sqrt( ( c[0] * Rf ) * ( c[0] * Rf ) + ( c[1] * Rf ) * ( c[1] * Rf ) + ( c[2] * Rf ) * ( c[2] * Rf ) );
+    if ( !( x & 1 ) && !( y & 1 ) )
+    {
+        const double nb = sqrt( ( c[0] * Rb ) * ( c[0] * Rb ) + ( c[1] * Rb ) * ( c[1] * Rb ) + ( c[2] * Rb ) * ( c[2] * Rb ) );
+        const double nt = sqrt( ( c[0] * Rt ) * ( c[0] * Rt ) + ( c[1] * Rt ) * ( c[1] * Rt ) + ( c[2] * Rt ) * ( c[2] * Rt ) );
+        const double nu = ( nf - nb ) / ( nt - nb );
+        cx[0] = cx[1] = x / 2, cy[0] = cy[1] = y / 2, cr[0] = rb, cr[1] = rt;
+        w[0] = 1.0 - nu, w[1] = nu;
+        return 2;
+    }
+    int x0, x1, y0, y1;
+    if ( !( x & 1 ) )
+        x0 = x1 = x / 2, y0 = y / 2, y1 = y / 2 + 1;
+    else if ( !( y & 1 ) )
+        x0 = x / 2, x1 = x / 2 + 1, y0 = y1 = y / 2;
+    else
+        x0 = x / 2 + 1, x1 = x / 2, y0 = y / 2, y1 = y / 2 + 1;
+    const double* c0 = coords + lat_index( n1, d, 2 * x0, 2 * y0 ) * 3;
+    const double* c1 = coords + lat_index( n1, d, 2 * x1, 2 * y1 ) * 3;
+    double        sb = 0.0, st = 0.0;
+    for ( int a = 0; a < 3; ++a )
+    {
+        const double b = 0.5 * ( c0[a] * Rb + c1[a] * Rb ), t = 0.5 * ( c0[a] * Rt + c1[a] * Rt );
+        sb += b * b, st += t * t;
+    }
+    const double nb = sqrt( sb ), nt = sqrt( st );
+    const double nu = ( nf - nb ) / ( nt - nb );
+    const double wb = 0.5 * ( 1.0 - nu ), wt = 0.5 * nu;
+    cx[0] = x0, cy[0] = y0, cr[0] = rb, w[0] = wb;
+    cx[1] = x1, cy[1] = y1, cr[1] = rb, w[1] = wb;
+    cx[2] = x0, cy[2] = y0, cr[2] = rt, w[2] = wt;
+    cx[3] = x1, cy[3] = y1, cr[3] = rt, w[3] = wt;
+    return 4;
+}
+
+// Prolongation: each fine node gathers its coarse parents (blockIdx.y = component).
+template < typename T >
+__global__ void prolong_linear_kernel( int Nf, int nc1, const double* __restrict__ coords,
+                                       const double* __restrict__ radii, Ptr3< const T > src, Ptr3< T > dst, int add )
+{
+    const int       nf1   = Nf + 1;
+    const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    const long long total = (long long) kDiamonds * nf1 * nf1 * nf1;
+    if ( t >= total )
+        return;
+    const int r = int( t % nf1 ), y = int( ( t / nf1 ) % nf1 ), x = int( ( t / ( (long long) nf1 * nf1 ) ) % nf1 );
+    const int d = int( t / ( (long long) nf1 * nf1 * nf1 ) );
+    int       cx[4], cy[4], cr[4];
+    double    w[4];
+    const int k = linear_stencil( Nf, coords, radii, d, x, y, r, cx, cy, cr, w );
+    const T*  s = src.p[blockIdx.y];
+    T         v = T( 0 );
+    for ( int i = 0; i < k; ++i )
+        v += T( w[i] ) * s[( ( size_t( d ) * nc1 + cx[i] ) * nc1 + cy[i] ) * nc1 + cr[i]];
+    T* o = dst.p[blockIdx.y] + t;
+    *o   = add ? *o + v : v;
+}
+
+// Restriction = transpose over owned fine nodes: each pushes its weighted
+// value to its coarse parents (restriction_linear.hpp:106-222); the coarse
+// halo then sums duplicated coarse nodes.
+template < typename T >
+__global__ void restrict_linear_kernel( int Nf, int nc1, const double* __restrict__ coords,
+                                        const double* __restrict__ radii, const uint8_t* __restrict__ owned,
+                                        Ptr3< const T > src, Ptr3< T > dst )
+{
+    const int       nf1   = Nf + 1;
+    const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    const long long total = (long long) kDiamonds * nf1 * nf1 * nf1;
+    if ( t >= total || !owned[t] )
+        return;
+    const int r = int( t % nf1 ), y = int( ( t / nf1 ) % nf1 ), x = int( ( t / ( (long long) nf1 * nf1 ) ) % nf1 );
+    const int d = int( t / ( (long long) nf1 * nf1 * nf1 ) );
+    int       cx[4], cy[4], cr[4];
+    double    w[4];
+    const int k = linear_stencil( Nf, coords, radii, d, x, y, r, cx, cy, cr, w );
+    const T   v = src.p[blockIdx.y][t];
+    for ( int i = 0; i < k; ++i )
+        atomicAdd( dst.p[blockIdx.y] + ( ( size_t( d ) * nc1 + cx[i] ) * nc1 + cy[i] ) * nc1 + cr[i], T( w[i] ) * v );
+}
+
 int check_levels( const tn_mesh* f, const tn_mesh* c, int ncomp )
 {
     TN_CHECK_ARG( f && c, "transfer: null mesh" );
@@ -175,6 +276,51 @@ int restrict_constant( const tn_mesh* f, const tn_mesh* c, int ncomp, int apply_
     const long long n = (long long) c->ns;
     restrict_constant_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( f->n1, c->n1, f->d_lat_owned, s, o,
                                                                                   ncomp, 0 );
+    TN_LAUNCH_CHECK();
+    return halo_sum< T >( c, dst, ncomp, st );
+}
+
+template < typename T >
+int prolong_linear( const tn_mesh* f, const tn_mesh* c, int ncomp, int apply_mode, const T* const* src, T* const* dst,
+                    cudaStream_t st )
+{
+    int rc;
+    if ( ( rc = check_levels( f, c, ncomp ) ) )
+        return rc;
+    TN_CHECK_ARG( src && dst, "prolongation: null argument" );
+    Ptr3< const T > s{};
+    Ptr3< T >       o{};
+    for ( int i = 0; i < ncomp; ++i )
+    {
+        TN_CHECK_ARG( src[i] && dst[i], "prolongation: null component" );
+        s.p[i] = src[i], o.p[i] = dst[i];
+    }
+    const long long n = (long long) f->ns;
+    prolong_linear_kernel< T ><<< dim3( unsigned( ( n + 255 ) / 256 ), ncomp ), 256, 0, st >>>(
+        f->N, c->n1, f->d_coords, f->d_radii, s, o, apply_mode == TN_APPLY_ADD );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+template < typename T >
+int restrict_linear( const tn_mesh* f, const tn_mesh* c, int ncomp, const T* const* src, T* const* dst,
+                     cudaStream_t st )
+{
+    int rc;
+    if ( ( rc = check_levels( f, c, ncomp ) ) )
+        return rc;
+    TN_CHECK_ARG( src && dst, "restriction: null argument" );
+    Ptr3< const T > s{};
+    Ptr3< T >       o{};
+    for ( int i = 0; i < ncomp; ++i )
+    {
+        TN_CHECK_ARG( src[i] && dst[i], "restriction: null component" );
+        s.p[i] = src[i], o.p[i] = dst[i];
+        TN_CUDA_TRY( cudaMemsetAsync( dst[i], 0, sizeof( T ) * c->ns, st ) );
+    }
+    const long long n = (long long) f->ns;
+    restrict_linear_kernel< T ><<< dim3( unsigned( ( n + 255 ) / 256 ), ncomp ), 256, 0, st >>>(
+        f->N, c->n1, f->d_coords, f->d_radii, f->d_node_owned, s, o );
     TN_LAUNCH_CHECK();
     return halo_sum< T >( c, dst, ncomp, st );
 }
@@ -232,6 +378,26 @@ extern "C" int tn_prolongation_constant_f32( const tn_mesh* f, const tn_mesh* c,
                                              const float* const* src, float* const* dst, void* s )
 {
     return prolong_constant< float >( f, c, ncomp, am, src, dst, as_stream( s ) );
+}
+extern "C" int tn_prolongation_linear_f64( const tn_mesh* f, const tn_mesh* c, int ncomp, int am,
+                                           const double* const* src, double* const* dst, void* s )
+{
+    return prolong_linear< double >( f, c, ncomp, am, src, dst, as_stream( s ) );
+}
+extern "C" int tn_prolongation_linear_f32( const tn_mesh* f, const tn_mesh* c, int ncomp, int am,
+                                           const float* const* src, float* const* dst, void* s )
+{
+    return prolong_linear< float >( f, c, ncomp, am, src, dst, as_stream( s ) );
+}
+extern "C" int tn_restriction_linear_f64( const tn_mesh* f, const tn_mesh* c, int ncomp, const double* const* src,
+                                          double* const* dst, void* s )
+{
+    return restrict_linear< double >( f, c, ncomp, src, dst, as_stream( s ) );
+}
+extern "C" int tn_restriction_linear_f32( const tn_mesh* f, const tn_mesh* c, int ncomp, const float* const* src,
+                                          float* const* dst, void* s )
+{
+    return restrict_linear< float >( f, c, ncomp, src, dst, as_stream( s ) );
 }
 extern "C" int tn_injection_f64( const tn_mesh* f, const tn_mesh* c, int ncomp, const double* const* src,
                                  double* const* dst, void* s )

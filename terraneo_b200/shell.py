@@ -277,6 +277,30 @@ class RestrictionVecConstant:
                 "restriction")
 
 
+class ProlongationLinear:
+    """ProlongationLinear (fe/wedge/operators/shell/prolongation_linear.hpp:15): coarse -> fine, per component."""
+
+    def __init__(self, mesh_fine, mesh_coarse, apply_mode=C.APPLY_REPLACE):
+        self.mf, self.mc, self.am = mesh_fine, mesh_coarse, apply_mode
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_prolongation_linear_{src.tag}")
+        C.check(f(self.mf.handle, self.mc.handle, src.ncomp, self.am, src.comp_ptrs(), dst.comp_ptrs(), _stream()),
+                "prolongation_linear")
+
+
+class RestrictionLinear:
+    """RestrictionLinear (fe/wedge/operators/shell/restriction_linear.hpp:15): fine -> coarse, per component."""
+
+    def __init__(self, mesh_fine, mesh_coarse):
+        self.mf, self.mc = mesh_fine, mesh_coarse
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_restriction_linear_{src.tag}")
+        C.check(f(self.mf.handle, self.mc.handle, src.ncomp, src.comp_ptrs(), dst.comp_ptrs(), _stream()),
+                "restriction_linear")
+
+
 def laplace_pcg(mesh, b, x, max_iterations=1000, relative_tolerance=1e-10, absolute_tolerance=1e-30):
     """Unpreconditioned PCG (linalg/solvers/pcg.hpp:78) on Laplace(treat_boundary=True); x is updated in place.
     Returns (iterations, relative residual)."""
@@ -284,6 +308,24 @@ def laplace_pcg(mesh, b, x, max_iterations=1000, relative_tolerance=1e-10, absol
     C.check(C.lib().tn_laplace_pcg_solve_f64(mesh.handle, ctypes.c_void_p(b.data.data_ptr()),
                                              ctypes.c_void_p(x.data.data_ptr()), max_iterations, relative_tolerance,
                                              absolute_tolerance, ctypes.byref(it), ctypes.byref(rr)), "laplace_pcg")
+    return it.value, rr.value
+
+
+def divkgrad_mg_pcg(level, b, x, k=None, mg_levels=3, smoother=1, smoothing_steps=2, chebyshev_order=2,
+                    power_iterations=10, jacobi_omega=0.6, vcycles=1, coarse_max_iterations=100,
+                    coarse_relative_tolerance=1e-8, max_iterations=200, relative_tolerance=1e-10,
+                    absolute_tolerance=1e-30, r_min=0.55, r_max=1.0):
+    """Multigrid-preconditioned CG on DivKGrad (k None: Laplace), Dirichlet radii; x updated in place.
+    smoother: 0 Chebyshev, 1 Jacobi.  Returns (iterations, relative residual)."""
+    prm = C.ScalarMGParams(level, mg_levels, smoother, smoothing_steps, chebyshev_order, power_iterations,
+                           jacobi_omega, vcycles, coarse_max_iterations, coarse_relative_tolerance, max_iterations,
+                           relative_tolerance, absolute_tolerance)
+    it, rr = ctypes.c_int(), ctypes.c_double()
+    kp = ctypes.c_void_p(k.data.data_ptr()) if k is not None else None
+    C.check(C.lib().tn_divkgrad_mg_pcg_solve_f64(ctypes.byref(prm), r_min, r_max, kp,
+                                                 ctypes.c_void_p(b.data.data_ptr()),
+                                                 ctypes.c_void_p(x.data.data_ptr()), ctypes.byref(it),
+                                                 ctypes.byref(rr)), "divkgrad_mg_pcg")
     return it.value, rr.value
 
 

@@ -39,7 +39,8 @@ def inputs(fine, coarse):
     s = fine.make_consistent(rs.normal(size=fine.shape))
     p = coarse.make_consistent(rs.normal(size=coarse.shape))
     uc = coarse.make_consistent(rs.normal(size=(3,) + coarse.shape))
-    return dict(k=k, u=u, s=s, p=p, uc=uc)
+    pc = coarse.make_consistent(rs.normal(size=coarse.shape))
+    return dict(k=k, u=u, s=s, p=p, uc=uc, pc=pc)
 
 
 def checksum(a):
@@ -85,6 +86,13 @@ def main():
         x["u"].tofile(f"{d}/src.bin")
         run_ref(["restrict", L, R_MIN, R_MAX, d], d)
         out["restrict"] = np.fromfile(f"{d}/dst.bin").reshape((3,) + coarse.shape)
+
+        x["pc"].tofile(f"{d}/src.bin")
+        run_ref(["prolong_linear", L, R_MIN, R_MAX, d], d)
+        out["prolong_linear"] = np.fromfile(f"{d}/dst.bin").reshape(fine.shape)
+        x["s"].tofile(f"{d}/src.bin")
+        run_ref(["restrict_linear", L, R_MIN, R_MAX, d], d)
+        out["restrict_linear"] = np.fromfile(f"{d}/dst.bin").reshape(coarse.shape)
 
         x["k"].tofile(f"{d}/k.bin")
         x["s"].tofile(f"{d}/src.bin")

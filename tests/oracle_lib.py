@@ -38,6 +38,8 @@ def lib():
         L.or_divkgrad_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.or_vector_laplace_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.or_vector_laplace_apply.restype = ctypes.c_int
+        L.or_prolongation_linear.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D]
+        L.or_restriction_linear.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _U8, _D, _D]
         L.or_prolongation_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D]
         L.or_restriction_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _U8, _D, _D]
         L.or_kmass_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int]
@@ -142,6 +144,21 @@ class Mesh:
         lib().or_restriction_constant(self.L, ncomp, _p(coarse.coords), _p(np.ascontiguousarray(self.omask)),
                                       _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst))
         return dst
+
+    def prolong_linear(self, coarse, src, ncomp=1):
+        """linear prolongation from `coarse` (level L-1) to this mesh"""
+        dst = np.zeros((ncomp,) + self.shape)
+        lib().or_prolongation_linear(coarse.L, ncomp, _p(self.coords), _p(self.radii),
+                                     _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst))
+        return dst[0] if ncomp == 1 else dst
+
+    def restrict_linear(self, coarse, src, ncomp=1):
+        """linear restriction from this mesh to `coarse` (level L-1)"""
+        dst = np.zeros((ncomp,) + coarse.shape)
+        lib().or_restriction_linear(self.L, ncomp, _p(self.coords), _p(self.radii), _p(coarse.coords),
+                                    _p(np.ascontiguousarray(self.omask)),
+                                    _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst))
+        return dst[0] if ncomp == 1 else dst
 
     def kmass(self, k, src, mode=0):
         dst = np.zeros(self.shape)

@@ -71,6 +71,12 @@ def test_transfers_match_reference(case):
     assert rel(fine.restrict(coarse, x["u"]), g["restrict"]) <= TOL
 
 
+def test_linear_transfers_match_reference(case):
+    g, fine, coarse, x = case
+    assert rel(fine.prolong_linear(coarse, x["pc"]), g["prolong_linear"]) <= TOL
+    assert rel(fine.restrict_linear(coarse, x["s"]), g["restrict_linear"]) <= TOL
+
+
 @pytest.mark.parametrize("mode", G.KMASS_MODES)
 def test_kmass_matches_reference(case, mode):
     g, fine, _, x = case

@@ -106,3 +106,27 @@ def test_stokes_fp32_mg_matches_fp64_mg(stokes_case):
         s.solve(fu, fp, xu, xp)
         sols.append(xu.numpy())
     assert rel(sols[1], sols[0]) <= 1e-8
+
+
+@pytest.mark.parametrize("smoother", [0, 1])
+@pytest.mark.parametrize("with_k", [False, True])
+def test_divkgrad_multigrid_pcg(smoother, with_k):
+    """V-cycle (linear transfers, Jacobi or Chebyshev, coarse PCG) preconditioned CG on DivKGrad."""
+    from terraneo_b200 import shell
+    L = 4
+    om, pm = Mesh(L), shell.ShellMesh(L)
+    k = viscosity_field(om, seed=3, contrast=1e2) if with_k else np.ones(om.shape)
+    b = random_vector(om, seed=12, ncomp=1)
+    b[om.bmask != 1] = 0.0
+    vb, vx = shell.VectorQ1Scalar(pm), shell.VectorQ1Scalar(pm)
+    vb.set_numpy(b)
+    vk = None
+    if with_k:
+        vk = shell.VectorQ1Scalar(pm)
+        vk.set_numpy(k)
+    it, rr = shell.divkgrad_mg_pcg(L, vb, vx, k=vk, mg_levels=3, smoother=smoother, relative_tolerance=1e-10)
+    assert rr <= 1e-10
+    assert it <= 60
+    x = vx.numpy()[0]
+    r = b - om.divkgrad(k, x, True)
+    assert np.sqrt(om.dot(r, r)) / np.sqrt(om.dot(b, b)) <= 1e-9
