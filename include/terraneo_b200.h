@@ -100,6 +100,39 @@ TN_API int tn_epsdivdiv_apply_f32( const tn_mesh* mesh, const tn_epsdivdiv_param
                             const float* const* src, float* const* dst, void* stream );
 
 /* ---------------------------------------------------------------------------
+ * Stored local matrices and GCA coarse operators of the epsilon-div-div
+ * operator (OperatorStoredMatrixMode::Full, linalg/operator.hpp:46; the
+ * kerngen slow path epsilon_divdiv_kerngen.hpp:823-1052; TwoGridGCA
+ * linalg/solvers/gca/gca.hpp:42-528; LocalMatrixStorage
+ * linalg/solvers/gca/local_matrix_storage.hpp:29-243).
+ *
+ * Storage: [cell][wedge][18 x 18], cells (diamond, x, y, r) with r fastest,
+ * entries in DIMENSIONWISE order (local node + 6 * dimension) and each matrix
+ * COLUMN-major (entry (I, J) at J * 18 + I).  tn_local_matrix_count gives the
+ * number of entries, 10 N^3 * 648 (FP64: 5,184 bytes per cell). */
+TN_API int tn_local_matrix_count( const tn_mesh* mesh, size_t* entries );
+/* kerngen assemble_local_matrix (:2051-2110) of every wedge: one-point rule,
+ * nodal coefficient k (NULL: k = 1), no boundary treatment. */
+TN_API int tn_kerngen_local_matrices_f64( const tn_mesh* mesh, const double* k, double* mats, void* stream );
+/* TwoGridGCA: mats_coarse = per coarse cell sum of P^T A_fine P over its
+ * 8 fine hexes x 2 wedges; A_fine from the kerngen matrices of k_fine (the
+ * finest level, Neumann operator) or from stored matrices mats_fine (exactly
+ * one of the two non-NULL); mode 0 constant (the reference default),
+ * 1 linear interpolation weights. */
+TN_API int tn_gca_coarsen_f64( const tn_mesh* fine, const tn_mesh* coarse, const double* k_fine,
+                               const double* mats_fine, int mode, double* mats_coarse, void* stream );
+/* Apply with stored matrices: the slow path's boundary treatment (Dirichlet
+ * masks, free-slip rotation with the normal component decoupled), diagonal
+ * mode, the fs/fs rotation penalty (p->penalty_eps) and apply / communication
+ * modes as tn_epsdivdiv_apply_*. */
+TN_API int tn_stored_epsdivdiv_apply_f64( const tn_mesh* mesh, const double* mats, const tn_epsdivdiv_params* p,
+                                          const double* const* src, double* const* dst, void* stream );
+TN_API int tn_stored_epsdivdiv_apply_f32( const tn_mesh* mesh, const float* mats, const tn_epsdivdiv_params* p,
+                                          const float* const* src, float* const* dst, void* stream );
+/* dst[i] = (float) src[i], i < n (FP32 copies of stored matrices) */
+TN_API int tn_array_cast_f64_to_f32( size_t n, const double* src, float* dst, void* stream );
+
+/* ---------------------------------------------------------------------------
  * Laplace::apply_impl (fe/wedge/operators/shell/laplace.hpp:68): int grad u . grad v,
  * 3x2 Felippa quadrature; treat_boundary != 0 eliminates the CMB/SURFACE
  * Dirichlet rows and columns keeping the diagonal; diagonal != 0 gives the
@@ -385,6 +418,8 @@ typedef struct
     int    max_iterations;
     double relative_tolerance;
     double absolute_tolerance;
+    int    gca; /* coarse viscous operators: 0 re-discretised with injected viscosity, 1 GCA with
+                   constant interpolation (TwoGridGCA default), 2 GCA with linear interpolation */
 } tn_stokes_params;
 
 typedef struct tn_stokes_solver tn_stokes_solver;

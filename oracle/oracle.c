@@ -570,6 +570,343 @@ void or_kerngen_apply( int L, const double* coords, const double* radii, const d
 }
 
 /* ------------------------------------------------------------------------ */
+/* Stored local matrices and GCA coarse operators                            */
+/* ------------------------------------------------------------------------ */
+
+static int    linear_stencil( int Nf, const double* coords_f, const double* radii_f, int d, int x, int y, int r,
+                              int cx[4], int cy[4], int cr[4], double w[4] );
+static double prolong_weight( int xf, int yf, int rf, int xc, int yc, int rc );
+
+/* kerngen assemble_local_matrix (epsilon_divdiv_kerngen.hpp:2051-2110): the
+ * wedge's 18x18 matrix in DIMENSIONWISE order (node + 6 dim), one-point rule,
+ * no boundary treatment:
+ * A[i+6a][j+6b] = kwJ (2 sym(g_j e_b):sym(g_i e_a) - 2/3 g_{j,b} g_{i,a}) */
+static void kerngen_local_matrix( const double* p[3], double r0, double r1, const double kn[6], double A[18][18] )
+{
+    double g[6][3], kwJ;
+    kerngen_wedge_geometry( p, r0, r1, kn, g, &kwJ );
+    for ( int a = 0; a < 3; ++a )
+        for ( int b = 0; b < 3; ++b )
+            for ( int i = 0; i < 6; ++i )
+                for ( int j = 0; j < 6; ++j )
+                {
+                    const double gg = a == b ? g[i][0] * g[j][0] + g[i][1] * g[j][1] + g[i][2] * g[j][2] : 0.0;
+                    A[i + 6 * a][j + 6 * b] = kwJ * ( gg + g[i][b] * g[j][a] - 2.0 / 3.0 * g[j][b] * g[i][a] );
+                }
+}
+
+void or_kerngen_local_matrices( int L, const double* coords, const double* radii, const double* k, double* mats )
+{
+    const int N = 1 << L, n1 = N + 1;
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const double* p[3];
+                        wedge_lateral_points( n1, coords, d, x, y, w, p );
+                        double kn[6];
+                        for ( int n = 0; n < 6; ++n )
+                            kn[n] = k[node_idx( n1, d, x + WNODE[w][n][0], y + WNODE[w][n][1], r + WNODE[w][n][2] )];
+                        double A[18][18];
+                        kerngen_local_matrix( p, radii[d * n1 + r], radii[d * n1 + r + 1], kn, A );
+                        const size_t cell = ( ( (size_t) d * N + x ) * N + y ) * N + r;
+                        memcpy( mats + ( cell * 2 + w ) * 324, A, sizeof( A ) );
+                    }
+}
+
+/* TwoGridGCA (linalg/solvers/gca/gca.hpp:154-528): per coarse cell, sum over
+ * its 8 fine hexes x 2 wedges of P^T A_fine P with the 6x6 local interpolation
+ * P (columns = local nodes of the coarse wedge the fine wedge lies in),
+ * constant (mode 0, the default) or linear (mode 1) weights. */
+static void gca_local_P( int Nf, const double* coords_f, const double* radii_f, int d, int xh, int yh, int rh, int w,
+                         int mode, double P[6][6] )
+{
+    const int n1 = Nf + 1;
+    memset( P, 0, sizeof( double ) * 36 );
+    for ( int i = 0; i < 6; ++i )
+    {
+        const int x = xh + WNODE[w][i][0], y = yh + WNODE[w][i][1], r = rh + WNODE[w][i][2];
+        if ( x % 2 == 0 && y % 2 == 0 && r % 2 == 0 )
+        {
+            P[i][i] = 1.0;
+            continue;
+        }
+        const int rb = r < n1 - 1 ? r / 2 : r / 2 - 1, rt = rb + 1;
+        int       cx[4], cy[4], cr[4];
+        double    wl[4];
+        if ( x % 2 == 0 && y % 2 == 0 )
+        {
+            double w0 = 0.5, w1 = 0.5;
+            if ( mode == 1 )
+            {
+                linear_stencil( Nf, coords_f, radii_f, d, x, y, r, cx, cy, cr, wl );
+                w0 = wl[0], w1 = wl[1];
+            }
+            const int col = i % 3;
+            P[i][col]     = w0;
+            P[i][col + 3] = w1;
+            continue;
+        }
+        int x0, x1, y0, y1, li[4];
+        if ( x % 2 == 0 )
+        {
+            x0 = x1 = x / 2, y0 = y / 2, y1 = y / 2 + 1;
+            li[0] = 0, li[1] = 2, li[2] = 3, li[3] = 5;
+        }
+        else if ( y % 2 == 0 )
+        {
+            x0 = x / 2, x1 = x / 2 + 1, y0 = y1 = y / 2;
+            li[0] = 0, li[1] = 1, li[2] = 3, li[3] = 4;
+        }
+        else
+        {
+            x0 = x / 2 + 1, x1 = x / 2, y0 = y / 2, y1 = y / 2 + 1;
+            li[0] = 1, li[1] = 2, li[2] = 4, li[3] = 5;
+        }
+        if ( mode == 1 )
+        {
+            linear_stencil( Nf, coords_f, radii_f, d, x, y, r, cx, cy, cr, wl );
+            P[i][li[0]] = wl[0], P[i][li[1]] = wl[0], P[i][li[2]] = wl[2], P[i][li[3]] = wl[2];
+        }
+        else
+        {
+            P[i][li[0]] = prolong_weight( x, y, r, x0, y0, rb );
+            P[i][li[1]] = prolong_weight( x, y, r, x1, y1, rb );
+            P[i][li[2]] = prolong_weight( x, y, r, x0, y0, rt );
+            P[i][li[3]] = prolong_weight( x, y, r, x1, y1, rt );
+        }
+    }
+}
+
+/* coarse wedge (0 or 1) holding fine wedge w of fine hex h (gca.hpp:434-452) */
+static int gca_coarse_wedge( int h, int w )
+{
+    if ( ( w == 0 && ( h == 0 || h == 1 || h == 2 || h == 4 || h == 5 || h == 6 ) ) || ( w == 1 && ( h == 0 || h == 4 ) ) )
+        return 0;
+    return 1;
+}
+
+void or_gca_coarsen( int Lf, const double* coords_f, const double* radii_f, const double* k_fine,
+                     const double* mats_fine, int mode, double* mats_coarse )
+{
+    const int Nf = 1 << Lf, Nc = Nf / 2, n1 = Nf + 1;
+    static const int HS[8][3] = { { 0, 0, 0 }, { 1, 0, 0 }, { 0, 1, 0 }, { 1, 1, 0 },
+                                  { 0, 0, 1 }, { 1, 0, 1 }, { 0, 1, 1 }, { 1, 1, 1 } };
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int xc = 0; xc < Nc; ++xc )
+            for ( int yc = 0; yc < Nc; ++yc )
+                for ( int rc = 0; rc < Nc; ++rc )
+                {
+                    double Ac[2][18][18];
+                    memset( Ac, 0, sizeof( Ac ) );
+                    for ( int h = 0; h < 8; ++h )
+                        for ( int w = 0; w < 2; ++w )
+                        {
+                            const int xh = 2 * xc + HS[h][0], yh = 2 * yc + HS[h][1], rh = 2 * rc + HS[h][2];
+                            double    P[6][6], A[18][18];
+                            gca_local_P( Nf, coords_f, radii_f, d, xh, yh, rh, w, mode, P );
+                            if ( mats_fine )
+                            {
+                                const size_t cell = ( ( (size_t) d * Nf + xh ) * Nf + yh ) * Nf + rh;
+                                memcpy( A, mats_fine + ( cell * 2 + w ) * 324, sizeof( A ) );
+                            }
+                            else
+                            {
+                                const double* p[3];
+                                wedge_lateral_points( n1, coords_f, d, xh, yh, w, p );
+                                double kn[6];
+                                for ( int n = 0; n < 6; ++n )
+                                    kn[n] = k_fine[node_idx( n1, d, xh + WNODE[w][n][0], yh + WNODE[w][n][1],
+                                                             rh + WNODE[w][n][2] )];
+                                kerngen_local_matrix( p, radii_f[d * n1 + rh], radii_f[d * n1 + rh + 1], kn, A );
+                            }
+                            const int cw = gca_coarse_wedge( h, w );
+                            /* P_vec = blockdiag(P, P, P) in DIMENSIONWISE order */
+                            for ( int a = 0; a < 3; ++a )
+                                for ( int b = 0; b < 3; ++b )
+                                    for ( int i = 0; i < 6; ++i )
+                                        for ( int j = 0; j < 6; ++j )
+                                        {
+                                            double v = 0.0;
+                                            for ( int m = 0; m < 6; ++m )
+                                                for ( int n = 0; n < 6; ++n )
+                                                    v += P[m][i] * A[m + 6 * a][n + 6 * b] * P[n][j];
+                                            Ac[cw][i + 6 * a][j + 6 * b] += v;
+                                        }
+                        }
+                    const size_t cell = ( ( (size_t) d * Nc + xc ) * Nc + yc ) * Nc + rc;
+                    memcpy( mats_coarse + cell * 2 * 324, Ac, sizeof( Ac ) );
+                }
+}
+
+/* kerngen slow path with stored matrices (epsilon_divdiv_kerngen.hpp:823-1052):
+ * Dirichlet cells mask the boundary nodes' couplings (keeping the node's own
+ * same-dimension diagonal); free-slip cells rotate the boundary nodes to the
+ * (n, t1, t2) basis, decouple the normal component keeping its diagonal and
+ * rotate back; diag keeps the diagonal of the treated matrix; fs/fs adds the
+ * rigid-rotation penalty; additive halo. */
+void or_stored_apply( int L, const double* coords, const double* radii, const double* mats, const double* src,
+                      double* dst, int bc_cmb, int bc_surf, int diag )
+{
+    const int    N = 1 << L, n1 = N + 1;
+    const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1;
+    memset( dst, 0, sizeof( double ) * 3 * ns );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                {
+                    const int at_cmb = r == 0, at_surf = r == N - 1;
+                    int       bcf = 0;
+                    if ( at_cmb || at_surf )
+                        bcf = at_cmb ? bc_cmb : bc_surf;
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const size_t cell = ( ( (size_t) d * N + x ) * N + y ) * N + r;
+                        double       A[18][18], M[18][18], s[18], out[18];
+                        memcpy( A, mats + ( cell * 2 + w ) * 324, sizeof( A ) );
+                        size_t idx[6];
+                        for ( int n = 0; n < 6; ++n )
+                        {
+                            idx[n] = node_idx( n1, d, x + WNODE[w][n][0], y + WNODE[w][n][1], r + WNODE[w][n][2] );
+                            for ( int a = 0; a < 3; ++a )
+                                s[n + 6 * a] = src[a * ns + idx[n]];
+                        }
+                        if ( bcf == 2 )
+                        {
+                            /* NODEWISE order (3 node + dim), rotate the 3 boundary nodes */
+                            double R[18][18], An[18][18], sn[18], T[18][18];
+                            memset( R, 0, sizeof( R ) );
+                            for ( int i = 0; i < 18; ++i )
+                                R[i][i] = 1.0;
+                            for ( int i = 0; i < 6; ++i )
+                                for ( int a = 0; a < 3; ++a )
+                                {
+                                    sn[3 * i + a] = s[i + 6 * a];
+                                    for ( int j = 0; j < 6; ++j )
+                                        for ( int b = 0; b < 3; ++b )
+                                            An[3 * i + a][3 * j + b] = A[i + 6 * a][j + 6 * b];
+                                }
+                            const int off = at_cmb ? 0 : 3;
+                            for ( int bn = 0; bn < 3; ++bn )
+                            {
+                                const int     node = off + bn;
+                                const double* c    = coords + lat_idx( n1, d, x + WNODE[w][node][0], y + WNODE[w][node][1] ) * 3;
+                                const double  rad  = radii[d * n1 + r + ( at_cmb ? 0 : 1 )];
+                                double        nv[3] = { c[0] * rad, c[1] * rad, c[2] * rad }, Ri[3][3];
+                                trafo_nt( nv, Ri );
+                                for ( int a = 0; a < 3; ++a )
+                                    for ( int b = 0; b < 3; ++b )
+                                        R[3 * node + a][3 * node + b] = Ri[a][b];
+                            }
+                            /* An <- R An R^T, sn <- R sn */
+                            for ( int i = 0; i < 18; ++i )
+                                for ( int j = 0; j < 18; ++j )
+                                {
+                                    double v = 0.0;
+                                    for ( int m = 0; m < 18; ++m )
+                                        v += An[i][m] * R[j][m];
+                                    T[i][j] = v;
+                                }
+                            for ( int i = 0; i < 18; ++i )
+                                for ( int j = 0; j < 18; ++j )
+                                {
+                                    double v = 0.0;
+                                    for ( int m = 0; m < 18; ++m )
+                                        v += R[i][m] * T[m][j];
+                                    An[i][j] = v;
+                                }
+                            double sr[18];
+                            for ( int i = 0; i < 18; ++i )
+                            {
+                                double v = 0.0;
+                                for ( int m = 0; m < 18; ++m )
+                                    v += R[i][m] * sn[m];
+                                sr[i] = v;
+                            }
+                            /* decouple the normal components (row/col 3 node), keep the diagonal */
+                            for ( int bn = 0; bn < 3; ++bn )
+                            {
+                                const int q = 3 * ( off + bn );
+                                for ( int k = 0; k < 18; ++k )
+                                    if ( k != q )
+                                        An[q][k] = An[k][q] = 0.0;
+                            }
+                            double yr[18];
+                            for ( int i = 0; i < 18; ++i )
+                            {
+                                double v = 0.0;
+                                if ( diag )
+                                    v = An[i][i] * sr[i];
+                                else
+                                    for ( int m = 0; m < 18; ++m )
+                                        v += An[i][m] * sr[m];
+                                yr[i] = v;
+                            }
+                            for ( int i = 0; i < 18; ++i )
+                            {
+                                double v = 0.0;
+                                for ( int m = 0; m < 18; ++m )
+                                    v += R[m][i] * yr[m];
+                                out[( i / 3 ) + 6 * ( i % 3 )] = v;
+                            }
+                        }
+                        else
+                        {
+                            for ( int a = 0; a < 3; ++a )
+                                for ( int b = 0; b < 3; ++b )
+                                    for ( int i = 0; i < 6; ++i )
+                                        for ( int j = 0; j < 6; ++j )
+                                        {
+                                            int keep = 1;
+                                            if ( bcf == 1 )
+                                            {
+                                                const int bi = at_cmb ? i < 3 : i >= 3, bj = at_cmb ? j < 3 : j >= 3;
+                                                if ( a == b ? ( i != j && ( bi || bj ) ) : ( bi || bj ) )
+                                                    keep = 0;
+                                            }
+                                            M[i + 6 * a][j + 6 * b] = keep ? A[i + 6 * a][j + 6 * b] : 0.0;
+                                        }
+                            for ( int i = 0; i < 18; ++i )
+                            {
+                                double v = 0.0;
+                                if ( diag )
+                                    v = M[i][i] * s[i];
+                                else
+                                    for ( int m = 0; m < 18; ++m )
+                                        v += M[i][m] * s[m];
+                                out[i] = v;
+                            }
+                        }
+                        for ( int n = 0; n < 6; ++n )
+                            for ( int a = 0; a < 3; ++a )
+                                dst[a * ns + idx[n]] += out[n + 6 * a];
+                    }
+                }
+    if ( !diag && bc_cmb == 2 && bc_surf == 2 )
+    {
+        uint8_t* om    = (uint8_t*) malloc( ns );
+        double*  modes = (double*) malloc( sizeof( double ) * 9 * ns );
+        or_ownership_mask( L, coords, om );
+        kerngen_null_modes( L, coords, radii, om, modes );
+        for ( int i = 0; i < 3; ++i )
+        {
+            const double* m  = modes + (size_t) i * 3 * ns;
+            double        al = 0.0;
+            for ( int c = 0; c < 3; ++c )
+                al += or_masked_dot( ns, m + c * ns, src + c * ns, om );
+            for ( size_t t = 0; t < 3 * ns; ++t )
+                dst[t] += al * m[t];
+        }
+        free( modes );
+        free( om );
+    }
+    or_halo_sum( L, coords, dst, 3 );
+}
+
+/* ------------------------------------------------------------------------ */
 /* Laplace (fe/wedge/operators/shell/laplace.hpp:106-330), 3x2 Felippa rule  */
 /* ------------------------------------------------------------------------ */
 

@@ -71,6 +71,18 @@ void or_restriction_linear( int Lf, int ncomp, const double* coords_fine, const 
                             const double* coords_coarse, const uint8_t* omask_fine, const double* src_fine,
                             double* dst_coarse );
 
+/* stored local matrices: [cell (d, x, y, r), r fastest][wedge][18][18],
+ * DIMENSIONWISE (node + 6 dim), row-major */
+void or_kerngen_local_matrices( int L, const double* coords, const double* radii, const double* k, double* mats );
+/* GCA coarsening Lf -> Lf-1 from fine stored matrices (mats_fine) or, when
+ * mats_fine is NULL, from the kerngen matrices of k_fine; mode 0 constant,
+ * 1 linear interpolation */
+void or_gca_coarsen( int Lf, const double* coords_f, const double* radii_f, const double* k_fine,
+                     const double* mats_fine, int mode, double* mats_coarse );
+/* apply with stored matrices and boundary treatment (+ fs/fs penalty) */
+void or_stored_apply( int L, const double* coords, const double* radii, const double* mats, const double* src,
+                      double* dst, int bc_cmb, int bc_surf, int diag );
+
 /* Krylov vector kernels */
 double or_masked_dot( size_t n, const double* a, const double* b, const uint8_t* omask );
 

@@ -21,6 +21,9 @@
 //   kmass   L rmin rmax mode DIR          KMass<double> (0 full, 1 diagonal, 2 lumped)
 //   divkgrad L rmin rmax treat diag single DIR   DivKGrad<double> (k.bin, src.bin)
 //   prolong_linear / restrict_linear Lf rmin rmax DIR  scalar linear transfer between Lf-1 and Lf
+//   gca L rmin rmax bcc bcs diag mode DIR  TwoGridGCA (mode 0 constant, 1 linear) of the Neumann kerngen
+//                                          operator at level L (k.bin) into level L-1 with bcs, then the
+//                                          stored-matrix apply of the coarse operator to src.bin
 //   vlaplace L rmin rmax bcc bcs diag DIR  VectorLaplace<double>
 //   time_kerngen L rmin rmax bcc bcs reps prints seconds per apply (CPU baseline)
 #include <chrono>
@@ -43,6 +46,7 @@
 #include "fe/wedge/operators/shell/restriction_linear.hpp"
 #include "fe/wedge/operators/shell/vector_laplace.hpp"
 #include "grid/bit_masks.hpp"
+#include "linalg/solvers/gca/gca.hpp"
 #include "grid/shell/bit_masks.hpp"
 #include "grid/shell/spherical_shell.hpp"
 #include "linalg/vector_q1.hpp"
@@ -289,6 +293,32 @@ int cmd_transfer_linear( bool prolong, int Lf, double rmin, double rmax, const s
     return 0;
 }
 
+int cmd_gca( int L, double rmin, double rmax, int bcc, int bcs, int diag, int mode, const std::string& dir )
+{
+    using Op = fe::wedge::operators::shell::EpsilonDivDivKerngen< double >;
+    Setup                            f( L, rmin, rmax ), c( L - 1, rmin, rmax );
+    linalg::VectorQ1Scalar< double > k( "k", f.domain, f.omask ), kc( "kc", c.domain, c.omask ),
+        gcae( "gcae", c.domain, c.omask );
+    view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", f.nodes ).data() );
+    linalg::assign( kc, 1.0 );
+    linalg::assign( gcae, 1.0 );
+    BoundaryConditions bn = { { ShellBoundaryFlag::CMB, BoundaryConditionFlag::NEUMANN },
+                              { ShellBoundaryFlag::SURFACE, BoundaryConditionFlag::NEUMANN } };
+    BoundaryConditions b  = { { ShellBoundaryFlag::CMB, bc_of( bcc ) }, { ShellBoundaryFlag::SURFACE, bc_of( bcs ) } };
+    Op Af( f.domain, f.coords, f.radii, f.bmask, k.grid_data(), bn, false );
+    Op Ac( c.domain, c.coords, c.radii, c.bmask, kc.grid_data(), b, false );
+    Ac.set_stored_matrix_mode( linalg::OperatorStoredMatrixMode::Full, 0, gcae.grid_data() );
+    linalg::solvers::TwoGridGCA< double, Op >( Af, Ac, 0, gcae.grid_data(), true,
+                                               mode == 1 ? linalg::solvers::InterpolationMode::Linear :
+                                                           linalg::solvers::InterpolationMode::Constant );
+    Ac.set_diagonal( diag != 0 );
+    linalg::VectorQ1Vec< double > src( "src", c.domain, c.omask ), dst( "dst", c.domain, c.omask );
+    load_vec( src, dir + "/src.bin", c.nodes );
+    linalg::apply( Ac, src, dst );
+    save_vec( dst, dir + "/dst.bin", c.nodes );
+    return 0;
+}
+
 int cmd_divkgrad( int L, double rmin, double rmax, int treat, int diag, int single, const std::string& dir )
 {
     Setup                            s( L, rmin, rmax );
@@ -344,6 +374,8 @@ int main( int argc, char** argv )
         return cmd_kmass( I( 2 ), D( 3 ), D( 4 ), I( 5 ), argv[6] );
     if ( ( cmd == "prolong_linear" || cmd == "restrict_linear" ) && argc == 6 )
         return cmd_transfer_linear( cmd == "prolong_linear", I( 2 ), D( 3 ), D( 4 ), argv[5] );
+    if ( cmd == "gca" && argc == 10 )
+        return cmd_gca( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), I( 8 ), argv[9] );
     if ( cmd == "divkgrad" && argc == 9 )
         return cmd_divkgrad( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( cmd == "vlaplace" && argc == 9 )

@@ -30,7 +30,7 @@ class StokesParams(ctypes.Structure):
                 ("chebyshev_order", c_int), ("smoothing_steps", c_int), ("power_iterations", c_int),
                 ("vcycles", c_int), ("coarse_max_iterations", c_int), ("coarse_relative_tolerance", c_double),
                 ("restart", c_int), ("max_iterations", c_int), ("relative_tolerance", c_double),
-                ("absolute_tolerance", c_double)]
+                ("absolute_tolerance", c_double), ("gca", c_int)]
 
 
 class ScalarMGParams(ctypes.Structure):
@@ -99,6 +99,14 @@ _SIGS = {
     "tn_restriction_linear_f32": (c_int, [c_void_p, c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
     "tn_divkgrad_mg_pcg_solve_f64": (c_int, [P(ScalarMGParams), c_double, c_double, c_void_p, c_void_p, c_void_p,
                                              P(c_int), P(c_double)]),
+    "tn_local_matrix_count": (c_int, [c_void_p, P(c_size_t)]),
+    "tn_kerngen_local_matrices_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "tn_gca_coarsen_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "tn_stored_epsdivdiv_apply_f64": (c_int, [c_void_p, c_void_p, P(EpsDivDivParams), P(c_void_p), P(c_void_p),
+                                              c_void_p]),
+    "tn_stored_epsdivdiv_apply_f32": (c_int, [c_void_p, c_void_p, P(EpsDivDivParams), P(c_void_p), P(c_void_p),
+                                              c_void_p]),
+    "tn_array_cast_f64_to_f32": (c_int, [c_size_t, c_void_p, c_void_p, c_void_p]),
     "tn_laplace_pcg_solve_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, P(c_int),
                                          P(c_double)]),
     "tn_stokes_solver_create": (c_int, [P(StokesParams), c_double, c_double, c_void_p, P(c_void_p)]),

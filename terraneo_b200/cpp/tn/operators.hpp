@@ -69,6 +69,75 @@ class EpsilonDivDivKerngen
     tn_epsdivdiv_params p_{};
 };
 
+// EpsilonDivDivKerngen with OperatorStoredMatrixMode::Full: stored 18x18
+// wedge matrices (tn_stored_epsdivdiv_apply_*), e.g. GCA coarse operators
+template < typename T >
+class StoredEpsilonDivDiv
+{
+  public:
+    using SrcVectorType = VectorQ1Vec< T >;
+    using DstVectorType = VectorQ1Vec< T >;
+    using ScalarType    = T;
+    StoredEpsilonDivDiv() = default;
+    StoredEpsilonDivDiv( const Mesh& mesh, std::shared_ptr< T > mats, BoundaryConditions bcs, bool diagonal = false )
+    : mesh_( mesh ), mats_( std::move( mats ) )
+    {
+        p_ = tn_epsdivdiv_params{ bcs.cmb, bcs.surface, diagonal ? 1 : 0, TN_APPLY_REPLACE, TN_COMM_ADDITIVE, 1.0 };
+    }
+    void set_operator_apply_and_communication_modes( OperatorApplyMode am, OperatorCommunicationMode cm )
+    {
+        p_.apply_mode = int( am ), p_.comm_mode = int( cm );
+    }
+    void set_diagonal( bool v ) { p_.diagonal = v ? 1 : 0; }
+    void apply_impl( const SrcVectorType& src, DstVectorType& dst )
+    {
+        const T* s[3] = { src.comp( 0 ), src.comp( 1 ), src.comp( 2 ) };
+        T*       d[3];
+        dst.ptrs( d );
+        if constexpr ( std::is_same_v< T, double > )
+            check( tn_stored_epsdivdiv_apply_f64( mesh_.get(), mats_.get(), &p_, s, d, stream() ), "stored apply" );
+        else
+            check( tn_stored_epsdivdiv_apply_f32( mesh_.get(), mats_.get(), &p_, s, d, stream() ), "stored apply" );
+    }
+
+  private:
+    Mesh                 mesh_;
+    std::shared_ptr< T > mats_;
+    tn_epsdivdiv_params  p_{};
+};
+
+// The viscous operator of one multigrid level: matrix-free kerngen or stored
+// matrices, chosen at run time (copies share the underlying operator)
+template < typename T >
+class ViscousOp
+{
+  public:
+    using SrcVectorType = VectorQ1Vec< T >;
+    using DstVectorType = VectorQ1Vec< T >;
+    using ScalarType    = T;
+    ViscousOp() = default;
+    explicit ViscousOp( std::shared_ptr< EpsilonDivDivKerngen< T > > k ) : k_( std::move( k ) ) {}
+    explicit ViscousOp( std::shared_ptr< StoredEpsilonDivDiv< T > > s ) : s_( std::move( s ) ) {}
+    void set_diagonal( bool v )
+    {
+        if ( k_ )
+            k_->set_diagonal( v );
+        else
+            s_->set_diagonal( v );
+    }
+    void apply_impl( const SrcVectorType& src, DstVectorType& dst )
+    {
+        if ( k_ )
+            k_->apply_impl( src, dst );
+        else
+            s_->apply_impl( src, dst );
+    }
+
+  private:
+    std::shared_ptr< EpsilonDivDivKerngen< T > > k_;
+    std::shared_ptr< StoredEpsilonDivDiv< T > >  s_;
+};
+
 // Laplace (laplace.hpp:18)
 template < typename T >
 class Laplace

@@ -960,6 +960,31 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
     return TN_OK;
 }
 
+// dst += eps sum_i (m_i^T src) m_i, the fs/fs rigid-rotation penalty on every
+// stored node (no halo); shared with the stored-matrix apply.
+template < typename T >
+int fsfs_penalty_add( const tn_mesh* m, double eps, const T* const* src, T* const* dst, cudaStream_t st )
+{
+    Ptr3< const T > s{ { src[0], src[1], src[2] } };
+    Ptr3< T >       o{ { dst[0], dst[1], dst[2] } };
+    Mat3            gi;
+    for ( int i = 0; i < 9; ++i )
+        gi.a[i] = m->penalty_gram_inv[i];
+    const unsigned blocks = unsigned( std::min< size_t >( ( m->nlat + 7 ) / 8, kRedMaxBlocks ) );
+    penalty_dots_kernel< T ><<< blocks, 256, 0, st >>>( m->nlat, m->n1, m->d_coords, mesh_radii< T >( m ), s,
+                                                       m->d_lat_owned, m->d_red_partials, m->d_red_counter,
+                                                       m->d_red_result );
+    TN_LAUNCH_CHECK();
+    penalty_beta_kernel<<< 1, 1, 0, st >>>( eps, gi, m->d_red_result );
+    TN_LAUNCH_CHECK();
+    penalty_axpy_kernel< T ><<< 148 * 8, 256, 0, st >>>( m->ns, m->n1, m->d_coords, mesh_radii< T >( m ),
+                                                        m->d_red_result + 3, o );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+template int fsfs_penalty_add< double >( const tn_mesh*, double, const double* const*, double* const*, cudaStream_t );
+template int fsfs_penalty_add< float >( const tn_mesh*, double, const float* const*, float* const*, cudaStream_t );
+
 }  // namespace tn
 
 using namespace tn;

@@ -22,14 +22,16 @@ namespace {
 
 using A64 = EpsilonDivDivKerngen< double >;
 using A32 = EpsilonDivDivKerngen< float >;
+using V64 = ViscousOp< double >;
+using V32 = ViscousOp< float >;
 
 // FP32 V-cycle's coarsest solve done in FP64: cast, PCG, cast back
 struct CoarseFp64
 {
-    std::shared_ptr< DevicePCG< A64 > > pcg;
-    std::shared_ptr< A64 >        A;
-    VectorQ1Vec< double >         x, b;
-    void                          solve_impl( A32&, VectorQ1Vec< float >& xo, const VectorQ1Vec< float >& bi )
+    std::shared_ptr< DevicePCG< V64 > > pcg;
+    std::shared_ptr< V64 >              A;
+    VectorQ1Vec< double >               x, b;
+    void                                solve_impl( V32&, VectorQ1Vec< float >& xo, const VectorQ1Vec< float >& bi )
     {
         cast( b, bi );
         assign( x, 0.0 );
@@ -39,15 +41,15 @@ struct CoarseFp64
 };
 
 template < typename T, typename Coarse >
-using MG = Multigrid< EpsilonDivDivKerngen< T >, ProlongationVecConstant< T >, RestrictionVecConstant< T >,
-                      Chebyshev< EpsilonDivDivKerngen< T > >, Coarse >;
+using MG = Multigrid< ViscousOp< T >, ProlongationVecConstant< T >, RestrictionVecConstant< T >,
+                      Chebyshev< ViscousOp< T > >, Coarse >;
 
 // FP32 multigrid as a preconditioner of the FP64 viscous block
 template < typename Inner >
 struct Fp32Preconditioner
 {
     std::shared_ptr< Inner > mg;
-    std::shared_ptr< A32 >   A;
+    std::shared_ptr< V32 >   A;
     VectorQ1Vec< float >     x, b;
     void                     solve_impl( A64&, VectorQ1Vec< double >& xo, const VectorQ1Vec< double >& bi )
     {
@@ -62,7 +64,8 @@ template < typename Inner >
 struct Fp64Preconditioner
 {
     std::shared_ptr< Inner > mg;
-    void solve_impl( A64& A, VectorQ1Vec< double >& x, const VectorQ1Vec< double >& b ) { solve( *mg, A, x, b ); }
+    std::shared_ptr< V64 >   A;
+    void solve_impl( A64&, VectorQ1Vec< double >& x, const VectorQ1Vec< double >& b ) { solve( *mg, *A, x, b ); }
 };
 
 }  // namespace
@@ -73,7 +76,9 @@ struct tn_stokes_solver
     std::vector< Mesh >                                      mesh; // index = level
     std::vector< VectorQ1Scalar< double > >                  k64;
     std::vector< VectorQ1Scalar< float > >                   k32;
-    std::vector< std::shared_ptr< A64 > >                    A64s;
+    std::vector< std::shared_ptr< double > >                 mats64; // GCA matrices per coarse level
+    std::vector< std::shared_ptr< float > >                  mats32;
+    std::shared_ptr< A64 >                                   A64fine;
     std::unique_ptr< EpsDivDivStokes< double > >             K;
     std::unique_ptr< Gradient< double > >                    BT;
     std::function< void( VectorQ1IsoQ2Q1< double >&, const VectorQ1IsoQ2Q1< double >& ) > run;
@@ -85,9 +90,10 @@ struct tn_stokes_solver
 
 namespace {
 
-template < typename T >
-VectorQ1Vec< T > inverse_diagonal_vec( EpsilonDivDivKerngen< T >& A, const Mesh& m )
+template < typename Op >
+VectorQ1Vec< typename Op::ScalarType > inverse_diagonal_vec( Op& A, const Mesh& m )
 {
+    using T = typename Op::ScalarType;
     VectorQ1Vec< T > ones( m ), d( m );
     assign( ones, T( 1 ) );
     A.set_diagonal( true );
@@ -97,26 +103,65 @@ VectorQ1Vec< T > inverse_diagonal_vec( EpsilonDivDivKerngen< T >& A, const Mesh&
     return d;
 }
 
+// viscous operator of level l: stored GCA matrices on coarse levels when
+// enabled, matrix-free kerngen otherwise
+template < typename T >
+ViscousOp< T > level_op( tn_stokes_solver& s, int l )
+{
+    BoundaryConditions bcs{ s.prm.bc_cmb, s.prm.bc_surface };
+    if ( s.prm.gca && l < s.prm.level )
+    {
+        if constexpr ( std::is_same_v< T, double > )
+            return ViscousOp< T >( std::make_shared< StoredEpsilonDivDiv< T > >( s.mesh[l], s.mats64[l], bcs ) );
+        else
+            return ViscousOp< T >( std::make_shared< StoredEpsilonDivDiv< T > >( s.mesh[l], s.mats32[l], bcs ) );
+    }
+    if constexpr ( std::is_same_v< T, double > )
+        return ViscousOp< T >( std::make_shared< EpsilonDivDivKerngen< T > >( s.mesh[l], s.k64[l], bcs, false ) );
+    else
+        return ViscousOp< T >( std::make_shared< EpsilonDivDivKerngen< T > >( s.mesh[l], s.k32[l], bcs, false ) );
+}
+
+// GCA matrices of levels [Lmin, L-1] (mantlecirculation.cpp:580-592): the
+// finest from the Neumann kerngen matrices of the finest viscosity, each
+// coarser one from the stored matrices above it
+void build_gca( tn_stokes_solver& s )
+{
+    const int L = s.prm.level, Lmin = L - s.prm.mg_levels + 1, mode = s.prm.gca == 2 ? 1 : 0;
+    s.mats64.assign( L + 1, nullptr );
+    s.mats32.assign( L + 1, nullptr );
+    for ( int l = L - 1; l >= Lmin; --l )
+    {
+        size_t n = 0;
+        check( tn_local_matrix_count( s.mesh[l].get(), &n ), "local_matrix_count" );
+        s.mats64[l] = device_alloc< double >( n );
+        check( tn_gca_coarsen_f64( s.mesh[l + 1].get(), s.mesh[l].get(), l == L - 1 ? s.k64[L].data() : nullptr,
+                                   l == L - 1 ? nullptr : s.mats64[l + 1].get(), mode, s.mats64[l].get(), stream() ),
+               "gca_coarsen" );
+        if ( s.prm.mg_fp32 )
+        {
+            s.mats32[l] = device_alloc< float >( n );
+            check( tn_array_cast_f64_to_f32( n, s.mats64[l].get(), s.mats32[l].get(), stream() ), "cast matrices" );
+        }
+    }
+}
+
 // builds the multigrid hierarchy in precision T over levels [Lmin, L]
 template < typename T, typename Coarse >
-std::shared_ptr< MG< T, Coarse > > build_mg( tn_stokes_solver& s, std::vector< std::shared_ptr< EpsilonDivDivKerngen< T > > >& ops,
+std::shared_ptr< MG< T, Coarse > > build_mg( tn_stokes_solver& s, std::vector< std::shared_ptr< ViscousOp< T > > >& ops,
                                              Coarse coarse )
 {
-    const auto&                                prm = s.prm;
-    const int                                  L = prm.level, Lmin = prm.level - prm.mg_levels + 1;
-    BoundaryConditions                         bcs{ prm.bc_cmb, prm.bc_surface };
+    const auto&                                 prm = s.prm;
+    const int                                   L = prm.level, Lmin = prm.level - prm.mg_levels + 1;
     std::vector< ProlongationVecConstant< T > > P;
     std::vector< RestrictionVecConstant< T > >  R;
-    std::vector< EpsilonDivDivKerngen< T > >    Ac;
+    std::vector< ViscousOp< T > >               Ac;
     std::vector< VectorQ1Vec< T > >             tr, te, tmp;
-    std::vector< Chebyshev< EpsilonDivDivKerngen< T > > > sm;
+    std::vector< Chebyshev< ViscousOp< T > > >  sm;
     for ( int l = Lmin; l <= L; ++l )
     {
         const Mesh& m = s.mesh[l];
-        if constexpr ( std::is_same_v< T, double > )
-            ops.push_back( std::make_shared< EpsilonDivDivKerngen< T > >( m, s.k64[l], bcs, false ) );
-        else
-            ops.push_back( std::make_shared< EpsilonDivDivKerngen< T > >( m, s.k32[l], bcs, false ) );
+        ops.push_back( std::make_shared< ViscousOp< T > >( level_op< T >( s, l ) ) );
         auto inv = inverse_diagonal_vec( *ops.back(), m );
         sm.emplace_back( prm.chebyshev_order, inv, std::vector< VectorQ1Vec< T > >{ VectorQ1Vec< T >( m ), VectorQ1Vec< T >( m ) },
                          prm.smoothing_steps, prm.power_iterations );
@@ -149,7 +194,7 @@ void finish( tn_stokes_solver& s, std::shared_ptr< Prec11 > p11 )
     KMass< double > pm( s.mesh[L - 1], kp, 2 );
     apply( pm, ones, dp );
     auto p22 = std::make_shared< DiagonalSolver< KMass< double >, VectorQ1Scalar< double > > >( dp );
-    auto a11 = s.A64s.back();
+    auto a11 = s.A64fine;
     using BT = BlockTriangularPreconditioner2x2< A64, Gradient< double >, Prec11,
                                                  DiagonalSolver< KMass< double >, VectorQ1Scalar< double > >,
                                                  VectorQ1IsoQ2Q1< double > >;
@@ -179,6 +224,7 @@ extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min,
     TN_CHECK_ARG( p->mg_levels >= 2 && p->level - p->mg_levels + 1 >= 2 && p->level <= 8,
                   "tn_stokes_solver_create: need mg_levels >= 2, level - mg_levels + 1 >= 2 and level <= 8" );
     TN_CHECK_ARG( p->restart >= 1 && p->max_iterations >= 1, "tn_stokes_solver_create: bad Krylov parameters" );
+    TN_CHECK_ARG( p->gca >= 0 && p->gca <= 2, "tn_stokes_solver_create: gca must be 0, 1 or 2" );
     try
     {
         auto s = std::make_unique< tn_stokes_solver >();
@@ -211,31 +257,34 @@ extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min,
             float*        dst[1] = { s->k32[l].data() };
             check( tn_vec_cast_f64_to_f32( s->mesh[l].get(), 1, dst, src, nullptr ), "cast viscosity" );
         }
-        // FP64 coarsest solve (both precisions): device-resident PCG, 3 temporaries
+        // GCA coarse operators (optional), the FP64 fine operator of the outer system
         BoundaryConditions bcs{ p->bc_cmb, p->bc_surface };
-        auto               Ac64 = std::make_shared< A64 >( s->mesh[Lmin], s->k64[Lmin], bcs, false );
+        if ( p->gca )
+            build_gca( *s );
+        s->A64fine = std::make_shared< A64 >( s->mesh[L], s->k64[L], bcs, false );
+        // FP64 coarsest solve (both precisions): device-resident PCG, 3 temporaries
+        auto Ac64 = std::make_shared< V64 >( level_op< double >( *s, Lmin ) );
         std::vector< VectorQ1Vec< double > > ct;
         for ( int i = 0; i < 3; ++i )
             ct.emplace_back( s->mesh[Lmin] );
-        auto pcg = std::make_shared< DevicePCG< A64 > >(
+        auto pcg = std::make_shared< DevicePCG< V64 > >(
             IterativeSolverParameters{ p->coarse_max_iterations, p->coarse_relative_tolerance, 1e-16 }, ct );
         if ( p->mg_fp32 )
         {
-            std::vector< std::shared_ptr< A32 > > ops32;
+            std::vector< std::shared_ptr< V32 > > ops32;
             CoarseFp64 cs{ pcg, Ac64, VectorQ1Vec< double >( s->mesh[Lmin] ), VectorQ1Vec< double >( s->mesh[Lmin] ) };
-            auto       mg = build_mg< float, CoarseFp64 >( *s, ops32, cs );
-            for ( int l = Lmin; l <= L; ++l )
-                s->A64s.push_back( std::make_shared< A64 >( s->mesh[l], s->k64[l], bcs, false ) );
-            auto p11 = std::make_shared< Fp32Preconditioner< MG< float, CoarseFp64 > > >(
+            auto       mg  = build_mg< float, CoarseFp64 >( *s, ops32, cs );
+            auto       p11 = std::make_shared< Fp32Preconditioner< MG< float, CoarseFp64 > > >(
                 Fp32Preconditioner< MG< float, CoarseFp64 > >{ mg, ops32.back(), VectorQ1Vec< float >( s->mesh[L] ),
                                                                 VectorQ1Vec< float >( s->mesh[L] ) } );
             finish( *s, p11 );
         }
         else
         {
-            auto mg  = build_mg< double, DevicePCG< A64 > >( *s, s->A64s, *pcg );
-            auto p11 = std::make_shared< Fp64Preconditioner< MG< double, DevicePCG< A64 > > > >(
-                Fp64Preconditioner< MG< double, DevicePCG< A64 > > >{ mg } );
+            std::vector< std::shared_ptr< V64 > > ops64;
+            auto mg  = build_mg< double, DevicePCG< V64 > >( *s, ops64, *pcg );
+            auto p11 = std::make_shared< Fp64Preconditioner< MG< double, DevicePCG< V64 > > > >(
+                Fp64Preconditioner< MG< double, DevicePCG< V64 > > >{ mg, ops64.back() } );
             finish( *s, p11 );
         }
         *out = s.release();

@@ -128,59 +128,6 @@ __global__ void freeslip_project_kernel( int n1, const double* __restrict__ coor
     y.p[0][i] = T( v[0] - dt * n[0] ), y.p[1][i] = T( v[1] - dt * n[1] ), y.p[2][i] = T( v[2] - dt * n[2] );
 }
 
-// Linear transfer stencil of fine node (d, x, y, r) on a fine mesh of Nf
-// cells (grid_transfer_linear.hpp:14-158, prolongation_linear.hpp:104-189):
-// on a coarse node: weight 1; between two radially aligned coarse nodes:
-// interpolation by radius; otherwise on the wedge facet of two lateral coarse
-// pairs: radial interpolation between the pairs' chord midpoints, each pair
-// member weighted half.  Returns the number of (coarse x, y, r, weight).
-__device__ int linear_stencil( int Nf, const double* __restrict__ coords, const double* __restrict__ radii, int d,
-                               int x, int y, int r, int cx[4], int cy[4], int cr[4], double w[4] )
-{
-    const int n1 = Nf + 1;
-    if ( !( x & 1 ) && !( y & 1 ) && !( r & 1 ) )
-    {
-        cx[0] = x / 2, cy[0] = y / 2, cr[0] = r / 2, w[0] = 1.0;
-        return 1;
-    }
-    const int     rb = r < Nf ? r / 2 : r / 2 - 1, rt = rb + 1;
-    const double* c  = coords + lat_index( n1, d, x, y ) * 3;
-    const double  Rf = radii[d * n1 + r], Rb = radii[d * n1 + 2 * rb], Rt = radii[d * n1 + 2 * rt];
-    const double  nf = sqrt( ( c[0] * Rf ) * ( c[0] * Rf ) + ( c[1] * Rf ) * ( c[1] * Rf ) + ( c[2] * Rf ) * ( c[2] * Rf ) );
-    if ( !( x & 1 ) && !( y & 1 ) )
-    {
-        const double nb = sqrt( ( c[0] * Rb ) * ( c[0] * Rb ) + ( c[1] * Rb ) * ( c[1] * Rb ) + ( c[2] * Rb ) * ( c[2] * Rb ) );
-        const double nt = sqrt( ( c[0] * Rt ) * ( c[0] * Rt ) + ( c[1] * Rt ) * ( c[1] * Rt ) + ( c[2] * Rt ) * ( c[2] * Rt ) );
-        const double nu = ( nf - nb ) / ( nt - nb );
-        cx[0] = cx[1] = x / 2, cy[0] = cy[1] = y / 2, cr[0] = rb, cr[1] = rt;
-        w[0] = 1.0 - nu, w[1] = nu;
-        return 2;
-    }
-    int x0, x1, y0, y1;
-    if ( !( x & 1 ) )
-        x0 = x1 = x / 2, y0 = y / 2, y1 = y / 2 + 1;
-    else if ( !( y & 1 ) )
-        x0 = x / 2, x1 = x / 2 + 1, y0 = y1 = y / 2;
-    else
-        x0 = x / 2 + 1, x1 = x / 2, y0 = y / 2, y1 = y / 2 + 1;
-    const double* c0 = coords + lat_index( n1, d, 2 * x0, 2 * y0 ) * 3;
-    const double* c1 = coords + lat_index( n1, d, 2 * x1, 2 * y1 ) * 3;
-    double        sb = 0.0, st = 0.0;
-    for ( int a = 0; a < 3; ++a )
-    {
-        const double b = 0.5 * ( c0[a] * Rb + c1[a] * Rb ), t = 0.5 * ( c0[a] * Rt + c1[a] * Rt );
-        sb += b * b, st += t * t;
-    }
-    const double nb = sqrt( sb ), nt = sqrt( st );
-    const double nu = ( nf - nb ) / ( nt - nb );
-    const double wb = 0.5 * ( 1.0 - nu ), wt = 0.5 * nu;
-    cx[0] = x0, cy[0] = y0, cr[0] = rb, w[0] = wb;
-    cx[1] = x1, cy[1] = y1, cr[1] = rb, w[1] = wb;
-    cx[2] = x0, cy[2] = y0, cr[2] = rt, w[2] = wt;
-    cx[3] = x1, cy[3] = y1, cr[3] = rt, w[3] = wt;
-    return 4;
-}
-
 // Prolongation: each fine node gathers its coarse parents (blockIdx.y = component).
 template < typename T >
 __global__ void prolong_linear_kernel( int Nf, int nc1, const double* __restrict__ coords,

@@ -159,6 +159,48 @@ class EpsilonDivDivKerngen:
                   dst.comp_ptrs(), _stream()), "epsdivdiv_apply")
 
 
+def local_matrix_count(mesh):
+    n = ctypes.c_size_t()
+    C.check(C.lib().tn_local_matrix_count(mesh.handle, ctypes.byref(n)), "local_matrix_count")
+    return n.value
+
+
+def kerngen_local_matrices(mesh, k=None):
+    """kerngen 18x18 wedge matrices (torch [cells, 2, 18, 18], column-major per matrix)."""
+    out = torch.empty(local_matrix_count(mesh), dtype=torch.float64, device="cuda")
+    kp = ctypes.c_void_p(k.data.data_ptr()) if k is not None else None
+    C.check(C.lib().tn_kerngen_local_matrices_f64(mesh.handle, kp, ctypes.c_void_p(out.data_ptr()), _stream()),
+            "kerngen_local_matrices")
+    return out.view(-1, 2, 18, 18)
+
+
+def gca_coarsen(fine, coarse, k_fine=None, mats_fine=None, mode=0):
+    """TwoGridGCA matrices of `coarse` from kerngen (k_fine) or stored (mats_fine) fine matrices."""
+    out = torch.empty(local_matrix_count(coarse), dtype=torch.float64, device="cuda")
+    kp = ctypes.c_void_p(k_fine.data.data_ptr()) if k_fine is not None else None
+    mp = ctypes.c_void_p(mats_fine.data_ptr()) if mats_fine is not None else None
+    C.check(C.lib().tn_gca_coarsen_f64(fine.handle, coarse.handle, kp, mp, mode, ctypes.c_void_p(out.data_ptr()),
+                                       _stream()), "gca_coarsen")
+    return out.view(-1, 2, 18, 18)
+
+
+class StoredEpsilonDivDiv:
+    """EpsilonDivDivKerngen with OperatorStoredMatrixMode::Full: stored wedge matrices + boundary treatment."""
+
+    def __init__(self, mesh, mats, bc_cmb, bc_surface, diagonal=False, apply_mode=C.APPLY_REPLACE,
+                 comm_mode=C.COMM_ADDITIVE, penalty_eps=1.0):
+        self.mesh, self.mats = mesh, mats
+        self.prm = C.EpsDivDivParams(bc_cmb, bc_surface, int(diagonal), apply_mode, comm_mode, penalty_eps)
+
+    def set_diagonal(self, v):
+        self.prm.diagonal = int(v)
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_stored_epsdivdiv_apply_{src.tag}")
+        C.check(f(self.mesh.handle, ctypes.c_void_p(self.mats.data_ptr()), ctypes.byref(self.prm), src.comp_ptrs(),
+                  dst.comp_ptrs(), _stream()), "stored_apply")
+
+
 class Laplace:
     """Laplace (fe/wedge/operators/shell/laplace.hpp:18)."""
 
@@ -336,10 +378,10 @@ class StokesSolver:
     def __init__(self, level, viscosity, mg_levels=4, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=True,
                  chebyshev_order=3, smoothing_steps=2, power_iterations=10, vcycles=1, coarse_max_iterations=50,
                  coarse_relative_tolerance=1e-6, restart=30, max_iterations=200, relative_tolerance=1e-8,
-                 absolute_tolerance=1e-30, r_min=0.55, r_max=1.0):
+                 absolute_tolerance=1e-30, r_min=0.55, r_max=1.0, gca=0):
         self.prm = C.StokesParams(level, mg_levels, bc_cmb, bc_surface, int(mg_fp32), chebyshev_order, smoothing_steps,
                                   power_iterations, vcycles, coarse_max_iterations, coarse_relative_tolerance, restart,
-                                  max_iterations, relative_tolerance, absolute_tolerance)
+                                  max_iterations, relative_tolerance, absolute_tolerance, int(gca))
         h = ctypes.c_void_p()
         C.check(C.lib().tn_stokes_solver_create(ctypes.byref(self.prm), r_min, r_max,
                                                 ctypes.c_void_p(viscosity.data.data_ptr()), ctypes.byref(h)),

@@ -40,6 +40,9 @@ def lib():
         L.or_vector_laplace_apply.restype = ctypes.c_int
         L.or_prolongation_linear.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D]
         L.or_restriction_linear.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _U8, _D, _D]
+        L.or_kerngen_local_matrices.argtypes = [ctypes.c_int, _D, _D, _D, _D]
+        L.or_gca_coarsen.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, _D]
+        L.or_stored_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.or_prolongation_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D]
         L.or_restriction_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _U8, _D, _D]
         L.or_kmass_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int]
@@ -159,6 +162,31 @@ class Mesh:
                                     _p(np.ascontiguousarray(self.omask)),
                                     _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst))
         return dst[0] if ncomp == 1 else dst
+
+    @property
+    def cells(self):
+        return 10 * self.N ** 3
+
+    def local_matrices(self, k):
+        """kerngen 18x18 wedge matrices [cells][2][18][18] (DIMENSIONWISE, row-major)"""
+        mats = np.zeros((self.cells, 2, 18, 18))
+        lib().or_kerngen_local_matrices(self.L, _p(self.coords), _p(self.radii),
+                                        _p(np.ascontiguousarray(k, dtype=np.float64)), _p(mats))
+        return mats
+
+    def gca_coarsen(self, coarse, mats_fine=None, k=None, mode=0):
+        """GCA matrices of `coarse` (level L-1) from this level's stored matrices or kerngen matrices of k"""
+        out = np.zeros((coarse.cells, 2, 18, 18))
+        mf = None if mats_fine is None else _p(np.ascontiguousarray(mats_fine))
+        kf = None if k is None else _p(np.ascontiguousarray(k, dtype=np.float64))
+        lib().or_gca_coarsen(self.L, _p(self.coords), _p(self.radii), kf, mf, mode, _p(out))
+        return out
+
+    def stored_apply(self, mats, src, bc_cmb, bc_surf, diag=False):
+        dst = np.zeros((3,) + self.shape)
+        lib().or_stored_apply(self.L, _p(self.coords), _p(self.radii), _p(np.ascontiguousarray(mats)),
+                              _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst), bc_cmb, bc_surf, int(diag))
+        return dst
 
     def kmass(self, k, src, mode=0):
         dst = np.zeros(self.shape)

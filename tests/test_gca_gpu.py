@@ -1,0 +1,100 @@
+"""Stored wedge matrices, GCA coarsening and the stored-matrix apply against the oracle
+(which is pinned to the reference's TwoGridGCA and slow path)."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import random_vector, rel, viscosity_field
+from oracle_lib import Mesh
+
+pytestmark = pytest.mark.gpu
+
+BCS = [(0, 0), (1, 1), (2, 2), (1, 2), (2, 1)]
+
+
+def _colmajor(m):
+    """oracle layout (row-major per matrix) -> the library's column-major layout"""
+    return np.ascontiguousarray(np.swapaxes(m, -1, -2))
+
+
+@pytest.fixture(scope="module")
+def level3():
+    from terraneo_b200 import shell
+    L = 3
+    of, oc = Mesh(L), Mesh(L - 1)
+    pf, pc = shell.ShellMesh(L), shell.ShellMesh(L - 1)
+    k = viscosity_field(of, seed=9, contrast=1e3)
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(k)
+    return of, oc, pf, pc, k, kv
+
+
+def test_local_matrices_match_oracle(level3):
+    from terraneo_b200 import shell
+    of, oc, pf, pc, k, kv = level3
+    m = shell.kerngen_local_matrices(pf, kv).cpu().numpy()
+    assert rel(m, _colmajor(of.local_matrices(k))) <= 1e-13
+
+
+@pytest.mark.parametrize("bc", BCS)
+@pytest.mark.parametrize("diag", [False, True])
+def test_stored_apply_with_kerngen_matrices_equals_kerngen_apply(level3, bc, diag):
+    from terraneo_b200 import shell
+    of, oc, pf, pc, k, kv = level3
+    m = shell.kerngen_local_matrices(pf, kv)
+    u = random_vector(of, seed=3)
+    src, d1, d2 = shell.VectorQ1Vec(pf), shell.VectorQ1Vec(pf), shell.VectorQ1Vec(pf)
+    src.set_numpy(u)
+    shell.apply(shell.StoredEpsilonDivDiv(pf, m, bc[0], bc[1], diag), src, d1)
+    shell.apply(shell.EpsilonDivDivKerngen(pf, kv, bc[0], bc[1], diagonal=diag), src, d2)
+    assert rel(d1.numpy(), d2.numpy()) <= 1e-12
+    assert rel(d1.numpy(), of.kerngen(k, u, bc[0], bc[1], diag)) <= 1e-12
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_gca_coarsening_matches_oracle(level3, mode):
+    from terraneo_b200 import shell
+    of, oc, pf, pc, k, kv = level3
+    mk = shell.gca_coarsen(pf, pc, k_fine=kv, mode=mode).cpu().numpy()
+    ref = _colmajor(of.gca_coarsen(oc, k=k, mode=mode))
+    assert rel(mk, ref) <= 1e-13
+    # from stored fine matrices gives the same
+    mf = shell.kerngen_local_matrices(pf, kv)
+    ms = shell.gca_coarsen(pf, pc, mats_fine=mf.reshape(-1), mode=mode).cpu().numpy()
+    assert rel(ms, mk) <= 1e-14
+
+
+@pytest.mark.parametrize("bc", BCS)
+@pytest.mark.parametrize("diag", [False, True])
+def test_gca_operator_apply_matches_oracle(level3, bc, diag):
+    from terraneo_b200 import shell
+    of, oc, pf, pc, k, kv = level3
+    mats = shell.gca_coarsen(pf, pc, k_fine=kv)
+    ref_m = of.gca_coarsen(oc, k=k)
+    u = random_vector(oc, seed=4)
+    src, dst = shell.VectorQ1Vec(pc), shell.VectorQ1Vec(pc)
+    src.set_numpy(u)
+    shell.apply(shell.StoredEpsilonDivDiv(pc, mats, bc[0], bc[1], diag), src, dst)
+    assert rel(dst.numpy(), oc.stored_apply(ref_m, u, bc[0], bc[1], diag)) <= 1e-12
+
+
+def test_gca_two_levels_and_fp32(level3):
+    """Level 4 -> 3 -> 2 (second step from stored matrices) and the FP32 apply."""
+    from terraneo_b200 import shell, _capi as C
+    L = 4
+    o4, o3, o2 = Mesh(L), Mesh(L - 1), Mesh(L - 2)
+    p4, p3, p2 = shell.ShellMesh(L), shell.ShellMesh(L - 1), shell.ShellMesh(L - 2)
+    k = viscosity_field(o4, seed=2, contrast=1e2)
+    kv = shell.VectorQ1Scalar(p4)
+    kv.set_numpy(k)
+    m3 = shell.gca_coarsen(p4, p3, k_fine=kv)
+    m2 = shell.gca_coarsen(p3, p2, mats_fine=m3.reshape(-1))
+    ref2 = o3.gca_coarsen(o2, mats_fine=o4.gca_coarsen(o3, k=k))
+    assert rel(m2.cpu().numpy(), _colmajor(ref2)) <= 1e-13
+    m2f = torch.empty(m2.numel(), dtype=torch.float32, device="cuda")
+    C.check(C.lib().tn_array_cast_f64_to_f32(m2.numel(), m2.data_ptr(), m2f.data_ptr(), None), "cast")
+    u = random_vector(o2, seed=5)
+    src, dst = shell.VectorQ1Vec(p2, torch.float32), shell.VectorQ1Vec(p2, torch.float32)
+    src.set_numpy(u)
+    shell.apply(shell.StoredEpsilonDivDiv(p2, m2f, 2, 2), src, dst)
+    assert rel(dst.numpy().astype(float), o2.stored_apply(ref2, u, 2, 2)) <= 1e-5

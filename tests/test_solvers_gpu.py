@@ -130,3 +130,26 @@ def test_divkgrad_multigrid_pcg(smoother, with_k):
     x = vx.numpy()[0]
     r = b - om.divkgrad(k, x, True)
     assert np.sqrt(om.dot(r, r)) / np.sqrt(om.dot(b, b)) <= 1e-9
+
+
+@pytest.mark.parametrize("bc", [(1, 1), (2, 2), (2, 1)])
+@pytest.mark.parametrize("gca,mg_fp32", [(1, False), (1, True), (2, False)])
+def test_stokes_solve_with_gca_coarse_operators(stokes_case, bc, gca, mg_fp32):
+    """GCA coarse operators (TwoGridGCA of the Neumann fine operator, stored-matrix applies)."""
+    from terraneo_b200 import shell
+    L, of, oc, k, f = stokes_case
+    pf, pc = shell.ShellMesh(L), shell.ShellMesh(L - 1)
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(k)
+    fu, fp = prepared_rhs(shell, pf, f, bc), shell.VectorQ1Scalar(pc)
+    tol = 1e-8
+    xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+    solver = shell.StokesSolver(L, kv, mg_levels=3, bc_cmb=bc[0], bc_surface=bc[1], mg_fp32=mg_fp32, gca=gca,
+                                relative_tolerance=tol, max_iterations=400, restart=50)
+    it, rr = solver.solve(fu, fp, xu, xp)
+    assert rr <= tol, (it, rr)
+    u, p, b = xu.numpy(), xp.numpy()[0], fu.numpy()
+    ru = of.kerngen(k, u, *bc) + of.gradient(oc, p, *bc) - b
+    rp = of.divergence(oc, u, *bc)
+    res = np.sqrt(of.dot(ru, ru) + oc.dot(rp, rp)) / np.sqrt(of.dot(b, b))
+    assert res <= 2 * tol, res
