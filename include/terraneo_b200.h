@@ -302,6 +302,47 @@ TN_API int tn_vec_cast_f64_to_f32( const tn_mesh* mesh, int ncomp, float* const*
 TN_API int tn_vec_cast_f32_to_f64( const tn_mesh* mesh, int ncomp, double* const* y, const float* const* x, void* stream );
 
 /* ---------------------------------------------------------------------------
+ * Finite-volume FCT advection-diffusion of a cell-centred scalar
+ * (fv/hex/operators/fct_advection_diffusion.hpp).  FV fields are
+ * [10][N+2][N+2][N+2] with one ghost layer, r fastest (linalg/vector_fv.hpp);
+ * cell (x, y, r), 1 <= x, y, r <= N, is FE cell (x-1, y-1, r-1) of `mesh`;
+ * vector FV fields (cell centres) are three such arrays.  `vel` is the Q1
+ * velocity on the mesh's stored nodes (3 fields). */
+typedef struct
+{
+    double T_cmb;
+    double T_surface;
+    int    apply_cmb;
+    int    apply_surface;
+} tn_fct_dirichlet; /* fv/hex/helpers.hpp DirichletBCs */
+
+/* entries of one FV field: 10 (N+2)^3 */
+TN_API int tn_fv_field_size( const tn_mesh* mesh, size_t* entries );
+/* doubles of the tn_fct_step_f64 workspace: 9 FV fields (T^L, 6 antidiffusive
+ * fluxes per cell, R+, R-) */
+TN_API int tn_fct_workspace_size( const tn_mesh* mesh, size_t* entries );
+/* update_fv_ghost_layers (communication/shell/fv_communication.hpp): lateral
+ * ghost cells := the real cells across each diamond face */
+TN_API int tn_fv_ghost_update_f64( const tn_mesh* mesh, double* field, void* stream );
+/* initialize_cell_centers (fv/hex/helpers.hpp:101-169): volume centroids of
+ * the cells, lateral ghosts filled, radial ghosts 0 */
+TN_API int tn_fv_cell_centers_f64( const tn_mesh* mesh, double* const* centers, void* stream );
+/* compute_dt_stable (fct_advection_diffusion.hpp:193-254): min over cells of
+ * volume / (inflow + two-point diffusion); synchronises */
+TN_API int tn_fct_dt_stable_f64( const tn_mesh* mesh, const double* const* vel, const double* const* centers,
+                                 double diffusivity, double* dt_stable, void* stream );
+/* apply_dirichlet_bcs (fv/hex/helpers.hpp:26-64): first / last real layer
+ * and its radial ghost */
+TN_API int tn_fct_apply_dirichlet_f64( const tn_mesh* mesh, double* T, const tn_fct_dirichlet* bcs, void* stream );
+/* fct_explicit_step (fct_advection_diffusion.hpp:720-750): T^{n+1} in place
+ * (T's lateral ghosts are refreshed first).  source (FV field) may be NULL;
+ * bcs NULL skips the Dirichlet treatment of T^L.  workspace holds
+ * tn_fct_workspace_size doubles; its first FV field is T^L on return. */
+TN_API int tn_fct_step_f64( const tn_mesh* mesh, double* T, const double* const* vel, const double* const* centers,
+                            double dt, double diffusivity, const double* source, int subtract_divergence,
+                            const tn_fct_dirichlet* bcs, double* workspace, void* stream );
+
+/* ---------------------------------------------------------------------------
  * Device-resident Krylov steps (no host synchronisation).
  *
  * A Krylov vector is passed as `nseg` (1..4) scalar fields, field k living on

@@ -1536,3 +1536,407 @@ void or_kmass_apply( int L, const double* coords, const double* radii, const dou
                     }
     or_halo_sum( L, coords, dst, 1 );
 }
+
+/* ------------------------------------------------------------------------ */
+/* Finite-volume FCT advection-diffusion on the hex cells of the shell       */
+/* (fv/hex/operators/fct_advection_diffusion.hpp, geometry_helper.hpp,       */
+/* fv/hex/helpers.hpp, communication/shell/fv_communication.hpp).            */
+/* FV fields: [10][N+2][N+2][N+2] with one ghost layer, r fastest; the cell  */
+/* (x, y, r), 1 <= x, y, r <= N, is the FE cell (x-1, y-1, r-1).             */
+/* ------------------------------------------------------------------------ */
+
+static inline size_t fv_idx( int n2, int d, int x, int y, int r ) { return ( ( (size_t) d * n2 + x ) * n2 + y ) * n2 + r; }
+
+static const int FV_OFF[6][3] = { { -1, 0, 0 }, { 1, 0, 0 }, { 0, -1, 0 }, { 0, 1, 0 }, { 0, 0, -1 }, { 0, 0, 1 } };
+
+/* wedge shape value (integrands.hpp:146) */
+static double shape_val( int n, double xi, double eta, double zeta )
+{
+    const double lat = n % 3 == 0 ? 1 - xi - eta : ( n % 3 == 1 ? xi : eta );
+    return lat * ( n < 3 ? 0.5 * ( 1 - zeta ) : 0.5 * ( 1 + zeta ) );
+}
+
+static void cross3( const double a[3], const double b[3], double c[3] )
+{
+    c[0] = a[1] * b[2] - a[2] * b[1], c[1] = a[2] * b[0] - a[0] * b[2], c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* lateral ghost map: for every ghost cell on the four lateral sides of a
+ * diamond, the real cell across the shared face in the neighbouring diamond
+ * (the two diamonds share the face's two edge nodes).  map[(d*4+side)*N + i]
+ * = (d', x', y') in FV indices; sides: x = 0, x = N+1, y = 0, y = N+1. */
+static void fv_ghost_map( int L, const double* coords, int* map )
+{
+    const int N = 1 << L, n1 = N + 1;
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int side = 0; side < 4; ++side )
+            for ( int i = 0; i < N; ++i )
+            {
+                int px, py, qx, qy; /* edge nodes (lateral FE indices) */
+                if ( side < 2 )
+                    px = qx = side == 0 ? 0 : N, py = i, qy = i + 1;
+                else
+                    py = qy = side == 2 ? 0 : N, px = i, qx = i + 1;
+                const double* P = coords + lat_idx( n1, d, px, py ) * 3;
+                const double* Q = coords + lat_idx( n1, d, qx, qy ) * 3;
+                int* out = map + ( (size_t) ( d * 4 + side ) * N + i ) * 3;
+                out[0] = out[1] = out[2] = -1;
+                for ( int e = 0; e < NDIAMOND && out[0] < 0; ++e )
+                {
+                    if ( e == d )
+                        continue;
+                    /* boundary lines of diamond e: (X fixed 0 / N) or (Y fixed 0 / N) */
+                    for ( int line = 0; line < 4 && out[0] < 0; ++line )
+                        for ( int j = 0; j < N; ++j )
+                        {
+                            int ax, ay, bx, by;
+                            if ( line < 2 )
+                                ax = bx = line == 0 ? 0 : N, ay = j, by = j + 1;
+                            else
+                                ay = by = line == 2 ? 0 : N, ax = j, bx = j + 1;
+                            const double* A = coords + lat_idx( n1, e, ax, ay ) * 3;
+                            const double* B = coords + lat_idx( n1, e, bx, by ) * 3;
+                            const int same = ( !memcmp( A, P, 24 ) && !memcmp( B, Q, 24 ) ) ||
+                                             ( !memcmp( A, Q, 24 ) && !memcmp( B, P, 24 ) );
+                            if ( !same )
+                                continue;
+                            out[0] = e;
+                            if ( line == 0 )
+                                out[1] = 1, out[2] = j + 1;
+                            else if ( line == 1 )
+                                out[1] = N, out[2] = j + 1;
+                            else if ( line == 2 )
+                                out[1] = j + 1, out[2] = 1;
+                            else
+                                out[1] = j + 1, out[2] = N;
+                            break;
+                        }
+                }
+            }
+}
+
+void or_fv_ghost_update( int L, const double* coords, double* field )
+{
+    const int N = 1 << L, n2 = N + 2;
+    int*      map = (int*) malloc( sizeof( int ) * 3 * NDIAMOND * 4 * N );
+    fv_ghost_map( L, coords, map );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int side = 0; side < 4; ++side )
+            for ( int i = 0; i < N; ++i )
+            {
+                const int* m  = map + ( (size_t) ( d * 4 + side ) * N + i ) * 3;
+                const int  gx = side == 0 ? 0 : ( side == 1 ? N + 1 : i + 1 );
+                const int  gy = side == 2 ? 0 : ( side == 3 ? N + 1 : i + 1 );
+                for ( int r = 1; r <= N; ++r )
+                    field[fv_idx( n2, d, gx, gy, r )] = field[fv_idx( n2, m[0], m[1], m[2], r )];
+            }
+    free( map );
+}
+
+/* compute_cell_centers (fv/hex/helpers.hpp:101-150): volume-weighted
+ * centroid over both wedges with the 3x2 rule, then the lateral ghosts */
+void or_fv_cell_centers( int L, const double* coords, const double* radii, double* centers )
+{
+    const int    N = 1 << L, n1 = N + 1, n2 = N + 2;
+    const size_t nf = (size_t) NDIAMOND * n2 * n2 * n2;
+    memset( centers, 0, sizeof( double ) * 3 * nf );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 1; x <= N; ++x )
+            for ( int y = 1; y <= N; ++y )
+                for ( int r = 1; r <= N; ++r )
+                {
+                    double vol = 0.0, c[3] = { 0, 0, 0 };
+                    const double r1 = radii[d * n1 + r - 1], r2 = radii[d * n1 + r];
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const double* p[3];
+                        wedge_lateral_points( n1, coords, d, x - 1, y - 1, w, p );
+                        for ( int q = 0; q < 6; ++q )
+                        {
+                            double J[3][3];
+                            wedge_jac( p, r1, r2, QP32[q][0], QP32[q][1], QP32[q][2], J );
+                            const double Jw = fabs( det3( J ) ) * QW32;
+                            const double rq = r1 + 0.5 * ( r2 - r1 ) * ( 1 + QP32[q][2] );
+                            vol += Jw;
+                            for ( int a = 0; a < 3; ++a )
+                                c[a] += ( ( 1 - QP32[q][0] - QP32[q][1] ) * p[0][a] + QP32[q][0] * p[1][a] +
+                                          QP32[q][1] * p[2][a] ) *
+                                        rq * Jw;
+                        }
+                    }
+                    for ( int a = 0; a < 3; ++a )
+                        centers[a * nf + fv_idx( n2, d, x, y, r )] = c[a] / vol;
+                }
+    for ( int a = 0; a < 3; ++a )
+        or_fv_ghost_update( L, coords, centers + a * nf );
+}
+
+/* GeometryHelper::compute_geometry (geometry_helper.hpp:180-363): face fluxes
+ * beta_n = int u . dS, face vectors S_n (oriented from the cell towards the
+ * neighbour's centre) and the cell volume M_ii */
+static void fv_geometry( int L, const double* coords, const double* radii, const double* centers, const double* vel,
+                         int d, int x, int y, int r, double beta[6], double* Mii, double S[6][3] )
+{
+    const int    N = 1 << L, n1 = N + 1, n2 = N + 2;
+    const size_t nf = (size_t) NDIAMOND * n2 * n2 * n2, ns = (size_t) NDIAMOND * n1 * n1 * n1;
+    const double r1 = radii[d * n1 + r - 1], r2 = radii[d * n1 + r];
+    static const double TQ[3][2] = { { 0.6666666666666666, 0.1666666666666667 },
+                                     { 0.1666666666666667, 0.6666666666666666 },
+                                     { 0.1666666666666667, 0.1666666666666667 } };
+    const double        g1      = -1.0 / sqrt( 3.0 ), g2 = 1.0 / sqrt( 3.0 );
+    const double        GL[2]   = { g1, g2 };
+    for ( int n = 0; n < 6; ++n )
+    {
+        beta[n] = 0.0;
+        S[n][0] = S[n][1] = S[n][2] = 0.0;
+    }
+    *Mii = 0.0;
+    const double* p[2][3];
+    double        u[2][6][3];
+    for ( int w = 0; w < 2; ++w )
+    {
+        wedge_lateral_points( n1, coords, d, x - 1, y - 1, w, p[w] );
+        for ( int i = 0; i < 6; ++i )
+        {
+            const size_t id = node_idx( n1, d, x - 1 + WNODE[w][i][0], y - 1 + WNODE[w][i][1], r - 1 + WNODE[w][i][2] );
+            for ( int a = 0; a < 3; ++a )
+                u[w][i][a] = vel[a * ns + id];
+        }
+    }
+    for ( int nb = 0; nb < 6; ++nb )
+    {
+        for ( int w = 0; w < 2; ++w )
+        {
+            /* contribution(): wedge 0 owns faces 0, 2 (quad), wedge 1 faces 1, 3; both the radial triangles */
+            int quad;
+            if ( nb >= 4 )
+                quad = 0;
+            else if ( ( w == 0 && ( nb == 0 || nb == 2 ) ) || ( w == 1 && ( nb == 1 || nb == 3 ) ) )
+                quad = 1;
+            else
+                continue;
+            const int nq = quad ? 4 : 3;
+            for ( int q = 0; q < nq; ++q )
+            {
+                double s, t, wq;
+                if ( quad )
+                    s = 0.5 * ( GL[q / 2] + 1.0 ), t = GL[q % 2], wq = 0.5;
+                else
+                    s = TQ[q][0], t = TQ[q][1], wq = 0.1666666666666667;
+                double xi, eta, zeta;
+                int    cpt; /* 0 xi-eta, 1 xi-zeta, 2 eta-zeta */
+                if ( nb == 0 || nb == 1 )
+                    xi = 0, eta = s, zeta = t, cpt = 2;
+                else if ( nb == 2 || nb == 3 )
+                    xi = s, eta = 0, zeta = t, cpt = 1;
+                else
+                    xi = s, eta = t, zeta = nb == 4 ? -1.0 : 1.0, cpt = 0;
+                double dxi[3] = { 0, 0, 0 }, deta[3] = { 0, 0, 0 }, dzeta[3] = { 0, 0, 0 }, uq[3] = { 0, 0, 0 };
+                for ( int i = 0; i < 6; ++i )
+                {
+                    double gr[3];
+                    grad_shape_ref( i, xi, eta, zeta, gr );
+                    const double sh = shape_val( i, xi, eta, zeta );
+                    const double rr = i < 3 ? r1 : r2;
+                    for ( int a = 0; a < 3; ++a )
+                    {
+                        const double xa = p[w][i % 3][a] * rr;
+                        dxi[a] += gr[0] * xa;
+                        deta[a] += gr[1] * xa;
+                        dzeta[a] += gr[2] * xa;
+                        uq[a] += sh * u[w][i][a];
+                    }
+                }
+                double nv[3];
+                if ( cpt == 0 )
+                    cross3( dxi, deta, nv );
+                else if ( cpt == 1 )
+                    cross3( dxi, dzeta, nv );
+                else
+                    cross3( deta, dzeta, nv );
+                beta[nb] += wq * ( uq[0] * nv[0] + uq[1] * nv[1] + uq[2] * nv[2] );
+                for ( int a = 0; a < 3; ++a )
+                    S[nb][a] += wq * nv[a];
+            }
+        }
+        double dc = 0.0;
+        for ( int a = 0; a < 3; ++a )
+            dc += S[nb][a] * ( centers[a * nf + fv_idx( n2, d, x + FV_OFF[nb][0], y + FV_OFF[nb][1], r + FV_OFF[nb][2] )] -
+                               centers[a * nf + fv_idx( n2, d, x, y, r )] );
+        if ( dc < 0 )
+        {
+            for ( int a = 0; a < 3; ++a )
+                S[nb][a] = -S[nb][a];
+            beta[nb] = -beta[nb];
+        }
+    }
+    for ( int w = 0; w < 2; ++w )
+        for ( int q = 0; q < 6; ++q )
+        {
+            double J[3][3];
+            wedge_jac( p[w], r1, r2, QP32[q][0], QP32[q][1], QP32[q][2], J );
+            *Mii += fabs( det3( J ) ) * QW32;
+        }
+}
+
+/* compute_dt_stable (fct_advection_diffusion.hpp:193-254) */
+double or_fct_dt_stable( int L, const double* coords, const double* radii, const double* centers, const double* vel,
+                         double diffusivity )
+{
+    const int    N = 1 << L, n2 = N + 2;
+    const size_t nf = (size_t) NDIAMOND * n2 * n2 * n2;
+    double       dtmin = 1e300;
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 1; x <= N; ++x )
+            for ( int y = 1; y <= N; ++y )
+                for ( int r = 1; r <= N; ++r )
+                {
+                    double beta[6], Mii, S[6][3], lambda = 0.0;
+                    fv_geometry( L, coords, radii, centers, vel, d, x, y, r, beta, &Mii, S );
+                    for ( int n = 0; n < 6; ++n )
+                    {
+                        if ( beta[n] < 0 )
+                            lambda -= beta[n];
+                        if ( diffusivity > 0 )
+                        {
+                            double dx[3], den = 0.0, ss = 0.0;
+                            for ( int a = 0; a < 3; ++a )
+                            {
+                                dx[a] = centers[a * nf + fv_idx( n2, d, x + FV_OFF[n][0], y + FV_OFF[n][1], r + FV_OFF[n][2] )] -
+                                        centers[a * nf + fv_idx( n2, d, x, y, r )];
+                                den += dx[a] * S[n][a];
+                                ss += S[n][a] * S[n][a];
+                            }
+                            if ( den > 0 )
+                                lambda += diffusivity * ss / den;
+                        }
+                    }
+                    const double dtc = lambda > 0 ? Mii / lambda : 1e30;
+                    if ( dtc < dtmin )
+                        dtmin = dtc;
+                }
+    return dtmin;
+}
+
+/* apply_dirichlet_bcs (fv/hex/helpers.hpp:26-64): first / last real layer and its ghost */
+void or_fct_dirichlet( int L, double* T, double T_cmb, double T_surf, int apply_cmb, int apply_surf )
+{
+    const int N = 1 << L, n2 = N + 2;
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 1; x <= N; ++x )
+            for ( int y = 1; y <= N; ++y )
+            {
+                if ( apply_cmb )
+                    T[fv_idx( n2, d, x, y, 1 )] = T[fv_idx( n2, d, x, y, 0 )] = T_cmb;
+                if ( apply_surf )
+                    T[fv_idx( n2, d, x, y, N )] = T[fv_idx( n2, d, x, y, N + 1 )] = T_surf;
+            }
+}
+
+/* fct_explicit_step (fct_advection_diffusion.hpp:720-750): predictor (low
+ * order upwind + two-point diffusion, pre-scaled antidiffusive fluxes),
+ * Dirichlet on T^L, limiter (Zalesak R+-), correction.  T is updated in
+ * place (its lateral ghosts are refreshed first); source may be NULL;
+ * bcs NULL skips the Dirichlet step; T_L_out (optional) receives T^L. */
+void or_fct_step( int L, const double* coords, const double* radii, const double* centers, const double* vel,
+                  double* T, double dt, double diffusivity, const double* source, int subtract_divergence,
+                  const double* bcs, double* T_L_out )
+{
+    const int    N = 1 << L, n2 = N + 2;
+    const size_t nf = (size_t) NDIAMOND * n2 * n2 * n2;
+    double*      TL = (double*) calloc( nf, sizeof( double ) );
+    double*      F  = (double*) calloc( nf * 6, sizeof( double ) );
+    double*      Rp = (double*) calloc( nf, sizeof( double ) );
+    double*      Rm = (double*) calloc( nf, sizeof( double ) );
+    or_fv_ghost_update( L, coords, T );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 1; x <= N; ++x )
+            for ( int y = 1; y <= N; ++y )
+                for ( int r = 1; r <= N; ++r )
+                {
+                    double       beta[6], Mii, S[6][3];
+                    const size_t i = fv_idx( n2, d, x, y, r );
+                    fv_geometry( L, coords, radii, centers, vel, d, x, y, r, beta, &Mii, S );
+                    const double Ti = T[i];
+                    double       lo_diag = 0.0, lo_update = 0.0, bsum = 0.0;
+                    for ( int n = 0; n < 6; ++n )
+                    {
+                        const size_t j  = fv_idx( n2, d, x + FV_OFF[n][0], y + FV_OFF[n][1], r + FV_OFF[n][2] );
+                        const double Tj = T[j];
+                        if ( beta[n] >= 0 )
+                            lo_diag += beta[n];
+                        else
+                            lo_update += beta[n] * Tj;
+                        bsum += beta[n];
+                        double den = 0.0, ss = 0.0;
+                        for ( int a = 0; a < 3; ++a )
+                        {
+                            den += ( centers[a * nf + j] - centers[a * nf + i] ) * S[n][a];
+                            ss += S[n][a] * S[n][a];
+                        }
+                        const double dc = diffusivity * ( ss / den );
+                        lo_diag += dc;
+                        lo_update -= dc * Tj;
+                        F[i * 6 + n] = ( dt / Mii ) * ( fabs( beta[n] ) / 2.0 ) * ( Ti - Tj );
+                    }
+                    if ( subtract_divergence )
+                        lo_diag -= bsum;
+                    double tl = Ti - ( dt / Mii ) * ( lo_diag * Ti + lo_update );
+                    if ( source )
+                        tl += dt * source[i];
+                    TL[i] = tl;
+                }
+    if ( bcs )
+        or_fct_dirichlet( L, TL, bcs[0], bcs[1], bcs[2] != 0, bcs[3] != 0 );
+    or_fv_ghost_update( L, coords, TL );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 1; x <= N; ++x )
+            for ( int y = 1; y <= N; ++y )
+                for ( int r = 1; r <= N; ++r )
+                {
+                    const size_t i = fv_idx( n2, d, x, y, r );
+                    double       Pp = 0.0, Pm = 0.0, tmax = TL[i], tmin = TL[i];
+                    for ( int n = 0; n < 6; ++n )
+                    {
+                        const double f = F[i * 6 + n];
+                        if ( f > 0 )
+                            Pp += f;
+                        else
+                            Pm += f;
+                        const double tj = TL[fv_idx( n2, d, x + FV_OFF[n][0], y + FV_OFF[n][1], r + FV_OFF[n][2] )];
+                        tmax = tj > tmax ? tj : tmax;
+                        tmin = tj < tmin ? tj : tmin;
+                    }
+                    const double Qp = tmax - TL[i], Qm = tmin - TL[i];
+                    Rp[i] = Pp > 0 ? ( Qp / Pp < 1.0 ? Qp / Pp : 1.0 ) : 1.0;
+                    Rm[i] = Pm < 0 ? ( Qm / Pm < 1.0 ? Qm / Pm : 1.0 ) : 1.0;
+                }
+    or_fv_ghost_update( L, coords, Rp );
+    or_fv_ghost_update( L, coords, Rm );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 1; x <= N; ++x )
+            for ( int y = 1; y <= N; ++y )
+                for ( int r = 1; r <= N; ++r )
+                {
+                    const size_t i = fv_idx( n2, d, x, y, r );
+                    double       corr = 0.0;
+                    for ( int n = 0; n < 6; ++n )
+                    {
+                        const size_t j = fv_idx( n2, d, x + FV_OFF[n][0], y + FV_OFF[n][1], r + FV_OFF[n][2] );
+                        const double f = F[i * 6 + n];
+                        double       al;
+                        if ( f > 0 )
+                            al = Rp[i] < Rm[j] ? Rp[i] : Rm[j];
+                        else
+                            al = Rm[i] < Rp[j] ? Rm[i] : Rp[j];
+                        corr += al * f;
+                    }
+                    T[i] = TL[i] + corr;
+                }
+    if ( T_L_out )
+        memcpy( T_L_out, TL, sizeof( double ) * nf );
+    free( TL );
+    free( F );
+    free( Rp );
+    free( Rm );
+}

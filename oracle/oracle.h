@@ -83,6 +83,17 @@ void or_gca_coarsen( int Lf, const double* coords_f, const double* radii_f, cons
 void or_stored_apply( int L, const double* coords, const double* radii, const double* mats, const double* src,
                       double* dst, int bc_cmb, int bc_surf, int diag );
 
+/* finite-volume FCT on the hex cells: fields [10][N+2][N+2][N+2] with ghosts */
+void   or_fv_ghost_update( int L, const double* coords, double* field );
+void   or_fv_cell_centers( int L, const double* coords, const double* radii, double* centers );
+double or_fct_dt_stable( int L, const double* coords, const double* radii, const double* centers, const double* vel,
+                         double diffusivity );
+void   or_fct_dirichlet( int L, double* T, double T_cmb, double T_surf, int apply_cmb, int apply_surf );
+/* bcs: NULL or {T_cmb, T_surface, apply_cmb, apply_surface} */
+void   or_fct_step( int L, const double* coords, const double* radii, const double* centers, const double* vel,
+                    double* T, double dt, double diffusivity, const double* source, int subtract_divergence,
+                    const double* bcs, double* T_L_out );
+
 /* Krylov vector kernels */
 double or_masked_dot( size_t n, const double* a, const double* b, const uint8_t* omask );
 

@@ -21,6 +21,9 @@
 //   kmass   L rmin rmax mode DIR          KMass<double> (0 full, 1 diagonal, 2 lumped)
 //   divkgrad L rmin rmax treat diag single DIR   DivKGrad<double> (k.bin, src.bin)
 //   prolong_linear / restrict_linear Lf rmin rmax DIR  scalar linear transfer between Lf-1 and Lf
+//   fct L rmin rmax dt kappa bc DIR  one fct_explicit_step on vel.bin (FE vector), T.bin and src.bin (FV
+//                                    fields with ghosts); bc 1: Dirichlet T_cmb = 1, T_surface = 0 on T before
+//                                    and in the step; writes centers.bin, dt.bin (dt_stable, dt), TL.bin, T.bin
 //   gca L rmin rmax bcc bcs diag mode DIR  TwoGridGCA (mode 0 constant, 1 linear) of the Neumann kerngen
 //                                          operator at level L (k.bin) into level L-1 with bcs, then the
 //                                          stored-matrix apply of the coarse operator to src.bin
@@ -45,10 +48,13 @@
 #include "fe/wedge/operators/shell/restriction_constant.hpp"
 #include "fe/wedge/operators/shell/restriction_linear.hpp"
 #include "fe/wedge/operators/shell/vector_laplace.hpp"
+#include "fv/hex/helpers.hpp"
+#include "fv/hex/operators/fct_advection_diffusion.hpp"
 #include "grid/bit_masks.hpp"
 #include "linalg/solvers/gca/gca.hpp"
 #include "grid/shell/bit_masks.hpp"
 #include "grid/shell/spherical_shell.hpp"
+#include "linalg/vector_fv.hpp"
 #include "linalg/vector_q1.hpp"
 #include "util/init.hpp"
 
@@ -293,6 +299,47 @@ int cmd_transfer_linear( bool prolong, int Lf, double rmin, double rmax, const s
     return 0;
 }
 
+int cmd_fct( int L, double rmin, double rmax, double dt, double kappa, int bc, const std::string& dir )
+{
+    Setup                               s( L, rmin, rmax );
+    linalg::VectorQ1Vec< double >       vel( "vel", s.domain, s.omask );
+    linalg::VectorFVScalar< double >    T( "T", s.domain ), src( "src", s.domain );
+    linalg::VectorFVVec< double, 3 >    centers( "centers", s.domain );
+    load_vec( vel, dir + "/vel.bin", s.nodes );
+    const size_t nf = T.grid_data().size();
+    view_from_host( T.grid_data(), read_file< double >( dir + "/T.bin", nf ).data() );
+    view_from_host( src.grid_data(), read_file< double >( dir + "/src.bin", nf ).data() );
+    fv::hex::initialize_cell_centers( centers, s.domain, s.coords, s.radii );
+    fv::hex::operators::FVFCTBuffers< double > bufs( s.domain );
+    const fv::hex::DirichletBCs< double > bcs{ .T_cmb = 1.0, .T_surface = 0.0, .apply_cmb = true, .apply_surface = true };
+    if ( bc )
+        fv::hex::apply_dirichlet_bcs( T, s.bmask, bcs, s.domain );
+    communication::shell::update_fv_ghost_layers( s.domain, T.grid_data() );
+    const double dt_stable =
+        fv::hex::operators::compute_dt_stable( s.domain, vel, centers.grid_data(), s.coords, s.radii, kappa );
+    const double step = dt > 0 ? dt : 0.5 * dt_stable;
+    if ( bc )
+        fv::hex::operators::fct_explicit_step( s.domain, T, vel, centers.grid_data(), s.coords, s.radii, step, bufs,
+                                               kappa, src.grid_data(), true, s.bmask, bcs );
+    else
+        fv::hex::operators::fct_explicit_step( s.domain, T, vel, centers.grid_data(), s.coords, s.radii, step, bufs,
+                                               kappa, src.grid_data(), true );
+    std::vector< double > c( 3 * nf );
+    for ( int a = 0; a < 3; ++a )
+    {
+        auto v = view_to_host( centers.grid_data().comp_[a] );
+        std::copy( v.begin(), v.end(), c.begin() + a * nf );
+    }
+    write_file( dir + "/centers.bin", c.data(), c.size() );
+    const double dts[2] = { dt_stable, step };
+    write_file( dir + "/dt.bin", dts, 2 );
+    auto tl = view_to_host( bufs.T_L );
+    write_file( dir + "/TL.bin", tl.data(), tl.size() );
+    auto tn = view_to_host( T.grid_data() );
+    write_file( dir + "/T.bin", tn.data(), tn.size() );
+    return 0;
+}
+
 int cmd_gca( int L, double rmin, double rmax, int bcc, int bcs, int diag, int mode, const std::string& dir )
 {
     using Op = fe::wedge::operators::shell::EpsilonDivDivKerngen< double >;
@@ -374,6 +421,8 @@ int main( int argc, char** argv )
         return cmd_kmass( I( 2 ), D( 3 ), D( 4 ), I( 5 ), argv[6] );
     if ( ( cmd == "prolong_linear" || cmd == "restrict_linear" ) && argc == 6 )
         return cmd_transfer_linear( cmd == "prolong_linear", I( 2 ), D( 3 ), D( 4 ), argv[5] );
+    if ( cmd == "fct" && argc == 9 )
+        return cmd_fct( I( 2 ), D( 3 ), D( 4 ), D( 5 ), D( 6 ), I( 7 ), argv[8] );
     if ( cmd == "gca" && argc == 10 )
         return cmd_gca( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), I( 8 ), argv[9] );
     if ( cmd == "divkgrad" && argc == 9 )

@@ -40,6 +40,10 @@ class ScalarMGParams(ctypes.Structure):
                 ("max_iterations", c_int), ("relative_tolerance", c_double), ("absolute_tolerance", c_double)]
 
 
+class FCTDirichlet(ctypes.Structure):
+    _fields_ = [("T_cmb", c_double), ("T_surface", c_double), ("apply_cmb", c_int), ("apply_surface", c_int)]
+
+
 class TNError(RuntimeError):
     pass
 
@@ -107,6 +111,14 @@ _SIGS = {
     "tn_stored_epsdivdiv_apply_f32": (c_int, [c_void_p, c_void_p, P(EpsDivDivParams), P(c_void_p), P(c_void_p),
                                               c_void_p]),
     "tn_array_cast_f64_to_f32": (c_int, [c_size_t, c_void_p, c_void_p, c_void_p]),
+    "tn_fv_field_size": (c_int, [c_void_p, P(c_size_t)]),
+    "tn_fct_workspace_size": (c_int, [c_void_p, P(c_size_t)]),
+    "tn_fv_ghost_update_f64": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "tn_fv_cell_centers_f64": (c_int, [c_void_p, P(c_void_p), c_void_p]),
+    "tn_fct_dt_stable_f64": (c_int, [c_void_p, P(c_void_p), P(c_void_p), c_double, P(c_double), c_void_p]),
+    "tn_fct_apply_dirichlet_f64": (c_int, [c_void_p, c_void_p, P(FCTDirichlet), c_void_p]),
+    "tn_fct_step_f64": (c_int, [c_void_p, c_void_p, P(c_void_p), P(c_void_p), c_double, c_double, c_void_p, c_int,
+                                P(FCTDirichlet), c_void_p, c_void_p]),
     "tn_laplace_pcg_solve_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, P(c_int),
                                          P(c_double)]),
     "tn_stokes_solver_create": (c_int, [P(StokesParams), c_double, c_double, c_void_p, P(c_void_p)]),

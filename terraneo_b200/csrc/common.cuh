@@ -85,6 +85,11 @@ struct tn_mesh
     int* d_halo_offsets   = nullptr;
     int* d_halo_members   = nullptr;
 
+    // finite-volume lateral ghost map: entry (d * 4 + side) * N + i gives the
+    // (diamond, x, y) FV cell across the face of ghost cell i on side
+    // (x = 0, x = N+1, y = 0, y = N+1) of diamond d
+    int* d_fv_ghost = nullptr;
+
     // fs/fs penalty: the orthonormalised modes are m = C (e_j x x); G = C^T C
     double penalty_gram_inv[9] = { 0 };
 

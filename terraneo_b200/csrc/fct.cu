@@ -1,0 +1,497 @@
+// Finite-volume FCT advection-diffusion on the hex cells of the shell
+// (fv/hex/operators/fct_advection_diffusion.hpp, geometry_helper.hpp,
+// fv/hex/helpers.hpp, communication/shell/fv_communication.hpp).
+//
+// FV fields are [10][N+2][N+2][N+2] with one ghost layer (r fastest); cell
+// (x, y, r), 1 <= x, y, r <= N, is the FE cell (x-1, y-1, r-1).  Lateral
+// ghosts are copies of the real cells across each diamond face (the mesh's
+// FV ghost map); radial ghosts hold what the boundary treatment writes.
+//
+// Every kernel runs one thread per interior cell, r fastest.  The cell
+// geometry (face fluxes beta, face vectors S, volume M) is recomputed from the
+// wedge map and the Q1 velocity in FP64 in the dt and predictor kernels, as
+// the reference does: 6 faces x (3 or 4) quadrature points per wedge face
+// plus the 3x2 volume rule, instead of storing ~150 values per cell.
+#include "common.cuh"
+#include "wedge.cuh"
+
+namespace tn {
+
+namespace {
+
+constexpr int kFvThreads = 128;
+
+__device__ __constant__ const int kFvOff[6][3] = { { -1, 0, 0 }, { 1, 0, 0 }, { 0, -1, 0 },
+                                                   { 0, 1, 0 },  { 0, 0, -1 }, { 0, 0, 1 } };
+
+__device__ __forceinline__ size_t fv_index( int n2, int d, int x, int y, int r )
+{
+    return ( ( size_t( d ) * n2 + x ) * n2 + y ) * n2 + r;
+}
+
+struct FvGeom
+{
+    int                  N;
+    const double*        coords;
+    const double*        radii;
+    Ptr3< const double > cen; // FV cell centres with ghosts
+    Ptr3< const double > vel; // Q1 velocity (stored nodes)
+};
+
+__device__ __forceinline__ void cross3( const double a[3], const double b[3], double c[3] )
+{
+    c[0] = a[1] * b[2] - a[2] * b[1], c[1] = a[2] * b[0] - a[0] * b[2], c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// GeometryHelper::compute_geometry (geometry_helper.hpp:180-363)
+__device__ void fv_geometry( const FvGeom& G, int d, int x, int y, int r, double beta[6], double& Mii, double S[6][3] )
+{
+    const int    N = G.N, n1 = N + 1, n2 = N + 2;
+    const double r1 = G.radii[d * n1 + r - 1], r2 = G.radii[d * n1 + r];
+    const double g1 = -0.5773502691896258, g2 = 0.5773502691896258; // -+ 1 / sqrt(3)
+    for ( int n = 0; n < 6; ++n )
+    {
+        beta[n] = 0.0;
+        S[n][0] = S[n][1] = S[n][2] = 0.0;
+    }
+    Mii = 0.0;
+    for ( int w = 0; w < 2; ++w )
+    {
+        double p[3][3], u[6][3];
+        for ( int i = 0; i < 6; ++i )
+        {
+            const size_t lat = lat_index( n1, d, x - 1 + kWedgeNode[w][i][0], y - 1 + kWedgeNode[w][i][1] );
+            if ( i < 3 )
+                for ( int a = 0; a < 3; ++a )
+                    p[i][a] = G.coords[lat * 3 + a];
+            const size_t id = lat * n1 + r - 1 + kWedgeNode[w][i][2];
+            for ( int a = 0; a < 3; ++a )
+                u[i][a] = G.vel.p[a][id];
+        }
+        // faces of this wedge: quads 0, 2 (wedge 0) or 1, 3 (wedge 1); radial triangles 4, 5
+        for ( int f = 0; f < 4; ++f )
+        {
+            const int  nb   = f < 2 ? ( w == 0 ? 2 * f : 2 * f + 1 ) : f + 2;
+            const bool quad = f < 2;
+            const int  nq   = quad ? 4 : 3;
+            for ( int q = 0; q < nq; ++q )
+            {
+                double s, t, wq;
+                if ( quad )
+                    s = 0.5 * ( ( q >> 1 ? g2 : g1 ) + 1.0 ), t = ( q & 1 ) ? g2 : g1, wq = 0.5;
+                else
+                {
+                    s  = q == 0 ? 0.6666666666666666 : 0.1666666666666667;
+                    t  = q == 1 ? 0.6666666666666666 : 0.1666666666666667;
+                    wq = 0.1666666666666667;
+                }
+                double xi, eta, zeta;
+                if ( nb < 2 )
+                    xi = 0.0, eta = s, zeta = t;
+                else if ( nb < 4 )
+                    xi = s, eta = 0.0, zeta = t;
+                else
+                    xi = s, eta = t, zeta = nb == 4 ? -1.0 : 1.0;
+                double dxi[3] = { 0, 0, 0 }, deta[3] = { 0, 0, 0 }, dzeta[3] = { 0, 0, 0 }, uq[3] = { 0, 0, 0 };
+                const double lat[3] = { 1.0 - xi - eta, xi, eta };
+                for ( int i = 0; i < 6; ++i )
+                {
+                    double gr[3];
+                    grad_shape_ref( i, xi, eta, zeta, gr );
+                    const double sh = lat[i % 3] * ( i < 3 ? 0.5 * ( 1.0 - zeta ) : 0.5 * ( 1.0 + zeta ) );
+                    const double rr = i < 3 ? r1 : r2;
+                    for ( int a = 0; a < 3; ++a )
+                    {
+                        const double xa = p[i % 3][a] * rr;
+                        dxi[a] += gr[0] * xa;
+                        deta[a] += gr[1] * xa;
+                        dzeta[a] += gr[2] * xa;
+                        uq[a] += sh * u[i][a];
+                    }
+                }
+                double nv[3];
+                if ( nb >= 4 )
+                    cross3( dxi, deta, nv );
+                else if ( nb >= 2 )
+                    cross3( dxi, dzeta, nv );
+                else
+                    cross3( deta, dzeta, nv );
+                beta[nb] += wq * ( uq[0] * nv[0] + uq[1] * nv[1] + uq[2] * nv[2] );
+                for ( int a = 0; a < 3; ++a )
+                    S[nb][a] += wq * nv[a];
+            }
+        }
+        for ( int q = 0; q < 6; ++q )
+        {
+            const double xi = q % 3 == 0 ? 0.6666666666666666 : 0.1666666666666667;
+            const double et = q % 3 == 1 ? 0.6666666666666666 : 0.1666666666666667;
+            const double ze = q < 3 ? -0.5773502691896257 : 0.5773502691896257;
+            double       IT[3][3];
+            const double det = wedge_jacobian_it( p[0], p[1], p[2], r1, r2, xi, et, ze, IT );
+            Mii += fabs( det ) * 0.1666666666666667;
+        }
+    }
+    // orient every face from this cell towards the neighbour's centre
+    const size_t ci = fv_index( n2, d, x, y, r );
+    for ( int nb = 0; nb < 6; ++nb )
+    {
+        const size_t cj = fv_index( n2, d, x + kFvOff[nb][0], y + kFvOff[nb][1], r + kFvOff[nb][2] );
+        double       dc = 0.0;
+        for ( int a = 0; a < 3; ++a )
+            dc += S[nb][a] * ( G.cen.p[a][cj] - G.cen.p[a][ci] );
+        if ( dc < 0 )
+        {
+            for ( int a = 0; a < 3; ++a )
+                S[nb][a] = -S[nb][a];
+            beta[nb] = -beta[nb];
+        }
+    }
+}
+
+__device__ __forceinline__ bool cell_of_thread( int N, int& d, int& x, int& y, int& r )
+{
+    const long long t = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if ( t >= (long long) kDiamonds * N * N * N )
+        return false;
+    r = int( t % N ) + 1;
+    y = int( ( t / N ) % N ) + 1;
+    x = int( ( t / ( (long long) N * N ) ) % N ) + 1;
+    d = int( t / ( (long long) N * N * N ) );
+    return true;
+}
+
+// compute_cell_centers (fv/hex/helpers.hpp:101-150)
+__global__ void __launch_bounds__( kFvThreads ) cell_centers_kernel( int N, const double* __restrict__ coords,
+                                                                     const double* __restrict__ radii, Ptr3< double > c )
+{
+    int d, x, y, r;
+    if ( !cell_of_thread( N, d, x, y, r ) )
+        return;
+    const int    n1 = N + 1, n2 = N + 2;
+    const double r1 = radii[d * n1 + r - 1], r2 = radii[d * n1 + r];
+    double       vol = 0.0, acc[3] = { 0, 0, 0 };
+    for ( int w = 0; w < 2; ++w )
+    {
+        double p[3][3];
+        for ( int i = 0; i < 3; ++i )
+        {
+            const size_t lat = lat_index( n1, d, x - 1 + kWedgeNode[w][i][0], y - 1 + kWedgeNode[w][i][1] );
+            for ( int a = 0; a < 3; ++a )
+                p[i][a] = coords[lat * 3 + a];
+        }
+        for ( int q = 0; q < 6; ++q )
+        {
+            const double xi = q % 3 == 0 ? 0.6666666666666666 : 0.1666666666666667;
+            const double et = q % 3 == 1 ? 0.6666666666666666 : 0.1666666666666667;
+            const double ze = q < 3 ? -0.5773502691896257 : 0.5773502691896257;
+            double       IT[3][3];
+            const double Jw = fabs( wedge_jacobian_it( p[0], p[1], p[2], r1, r2, xi, et, ze, IT ) ) * 0.1666666666666667;
+            const double rq = r1 + 0.5 * ( r2 - r1 ) * ( 1.0 + ze );
+            vol += Jw;
+            for ( int a = 0; a < 3; ++a )
+                acc[a] += ( ( 1.0 - xi - et ) * p[0][a] + xi * p[1][a] + et * p[2][a] ) * rq * Jw;
+        }
+    }
+    const size_t i = fv_index( n2, d, x, y, r );
+    for ( int a = 0; a < 3; ++a )
+        c.p[a][i] = acc[a] / vol;
+}
+
+// lateral ghost layer: thread per (ghost cell, r)
+__global__ void fv_ghost_kernel( int N, const int* __restrict__ map, double* __restrict__ f )
+{
+    const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    const long long total = (long long) kDiamonds * 4 * N * N;
+    if ( t >= total )
+        return;
+    const int  r     = int( t % N ) + 1;
+    const long long e = t / N; // (d * 4 + side) * N + i
+    const int  i     = int( e % N );
+    const int  side  = int( ( e / N ) % 4 );
+    const int  d     = int( e / ( 4LL * N ) );
+    const int* m     = map + e * 3;
+    const int  n2    = N + 2;
+    const int  gx    = side == 0 ? 0 : ( side == 1 ? N + 1 : i + 1 );
+    const int  gy    = side == 2 ? 0 : ( side == 3 ? N + 1 : i + 1 );
+    f[fv_index( n2, d, gx, gy, r )] = f[fv_index( n2, m[0], m[1], m[2], r )];
+}
+
+// compute_dt_stable (fct_advection_diffusion.hpp:193-254): min over cells of
+// M / (inflow + diffusion); positive doubles order like their bit patterns
+__global__ void __launch_bounds__( kFvThreads ) dt_kernel( FvGeom G, double kappa, unsigned long long* out )
+{
+    int    d, x, y, r;
+    double dtc = 1e300;
+    if ( cell_of_thread( G.N, d, x, y, r ) )
+    {
+        const int n2 = G.N + 2;
+        double    beta[6], Mii, S[6][3], lambda = 0.0;
+        fv_geometry( G, d, x, y, r, beta, Mii, S );
+        const size_t ci = fv_index( n2, d, x, y, r );
+        for ( int n = 0; n < 6; ++n )
+        {
+            if ( beta[n] < 0 )
+                lambda -= beta[n];
+            if ( kappa > 0 )
+            {
+                const size_t cj  = fv_index( n2, d, x + kFvOff[n][0], y + kFvOff[n][1], r + kFvOff[n][2] );
+                double       den = 0.0, ss = 0.0;
+                for ( int a = 0; a < 3; ++a )
+                {
+                    den += ( G.cen.p[a][cj] - G.cen.p[a][ci] ) * S[n][a];
+                    ss += S[n][a] * S[n][a];
+                }
+                if ( den > 0 )
+                    lambda += kappa * ss / den;
+            }
+        }
+        dtc = lambda > 0 ? Mii / lambda : 1e30;
+    }
+    for ( int off = 16; off > 0; off >>= 1 )
+        dtc = fmin( dtc, __shfl_down_sync( 0xffffffffu, dtc, off ) );
+    if ( ( threadIdx.x & 31 ) == 0 )
+        atomicMin( out, (unsigned long long) __double_as_longlong( dtc ) );
+}
+
+// FCTPredictorKernel (fct_advection_diffusion.hpp:262-376)
+__global__ void __launch_bounds__( kFvThreads )
+    predictor_kernel( FvGeom G, const double* __restrict__ T, double* __restrict__ TL, double* __restrict__ F, double dt,
+                      double kappa, const double* __restrict__ src, int subtract_divergence )
+{
+    int d, x, y, r;
+    if ( !cell_of_thread( G.N, d, x, y, r ) )
+        return;
+    const int n2 = G.N + 2;
+    double    beta[6], Mii, S[6][3];
+    fv_geometry( G, d, x, y, r, beta, Mii, S );
+    const size_t i  = fv_index( n2, d, x, y, r );
+    const double Ti = T[i];
+    double       lo_diag = 0.0, lo_update = 0.0, bsum = 0.0;
+    for ( int n = 0; n < 6; ++n )
+    {
+        const size_t j  = fv_index( n2, d, x + kFvOff[n][0], y + kFvOff[n][1], r + kFvOff[n][2] );
+        const double Tj = T[j];
+        if ( beta[n] >= 0 )
+            lo_diag += beta[n];
+        else
+            lo_update += beta[n] * Tj;
+        bsum += beta[n];
+        double den = 0.0, ss = 0.0;
+        for ( int a = 0; a < 3; ++a )
+        {
+            den += ( G.cen.p[a][j] - G.cen.p[a][i] ) * S[n][a];
+            ss += S[n][a] * S[n][a];
+        }
+        const double dc = kappa * ( ss / den );
+        lo_diag += dc;
+        lo_update -= dc * Tj;
+        F[i * 6 + n] = ( dt / Mii ) * ( fabs( beta[n] ) / 2.0 ) * ( Ti - Tj );
+    }
+    if ( subtract_divergence )
+        lo_diag -= bsum;
+    double tl = Ti - ( dt / Mii ) * ( lo_diag * Ti + lo_update );
+    if ( src )
+        tl += dt * src[i];
+    TL[i] = tl;
+}
+
+// apply_dirichlet_bcs (fv/hex/helpers.hpp:26-64): thread per lateral column
+__global__ void dirichlet_kernel( int N, double* __restrict__ T, double t_cmb, double t_surf, int cmb, int surf )
+{
+    const long long t = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if ( t >= (long long) kDiamonds * N * N )
+        return;
+    const int y = int( t % N ) + 1, x = int( ( t / N ) % N ) + 1, d = int( t / ( (long long) N * N ) );
+    const int n2 = N + 2;
+    if ( cmb )
+        T[fv_index( n2, d, x, y, 1 )] = T[fv_index( n2, d, x, y, 0 )] = t_cmb;
+    if ( surf )
+        T[fv_index( n2, d, x, y, N )] = T[fv_index( n2, d, x, y, N + 1 )] = t_surf;
+}
+
+// FCTLimiterKernel (fct_advection_diffusion.hpp:486-531)
+__global__ void __launch_bounds__( kFvThreads ) limiter_kernel( int N, const double* __restrict__ TL,
+                                                                const double* __restrict__ F, double* __restrict__ Rp,
+                                                                double* __restrict__ Rm )
+{
+    int d, x, y, r;
+    if ( !cell_of_thread( N, d, x, y, r ) )
+        return;
+    const int    n2 = N + 2;
+    const size_t i  = fv_index( n2, d, x, y, r );
+    const double ti = TL[i];
+    double       Pp = 0.0, Pm = 0.0, tmax = ti, tmin = ti;
+    for ( int n = 0; n < 6; ++n )
+    {
+        const double f = F[i * 6 + n];
+        if ( f > 0 )
+            Pp += f;
+        else
+            Pm += f;
+        const double tj = TL[fv_index( n2, d, x + kFvOff[n][0], y + kFvOff[n][1], r + kFvOff[n][2] )];
+        tmax            = fmax( tmax, tj );
+        tmin            = fmin( tmin, tj );
+    }
+    Rp[i] = Pp > 0 ? fmin( 1.0, ( tmax - ti ) / Pp ) : 1.0;
+    Rm[i] = Pm < 0 ? fmin( 1.0, ( tmin - ti ) / Pm ) : 1.0;
+}
+
+// FCTCorrectionKernel (fct_advection_diffusion.hpp:605-650)
+__global__ void __launch_bounds__( kFvThreads )
+    correction_kernel( int N, const double* __restrict__ TL, const double* __restrict__ F,
+                       const double* __restrict__ Rp, const double* __restrict__ Rm, double* __restrict__ T )
+{
+    int d, x, y, r;
+    if ( !cell_of_thread( N, d, x, y, r ) )
+        return;
+    const int    n2 = N + 2;
+    const size_t i  = fv_index( n2, d, x, y, r );
+    double       corr = 0.0;
+    for ( int n = 0; n < 6; ++n )
+    {
+        const size_t j  = fv_index( n2, d, x + kFvOff[n][0], y + kFvOff[n][1], r + kFvOff[n][2] );
+        const double f  = F[i * 6 + n];
+        const double al = f > 0 ? fmin( Rp[i], Rm[j] ) : fmin( Rm[i], Rp[j] );
+        corr += al * f;
+    }
+    T[i] = TL[i] + corr;
+}
+
+size_t fv_size( const tn_mesh* m )
+{
+    const size_t n2 = size_t( m->N ) + 2;
+    return size_t( kDiamonds ) * n2 * n2 * n2;
+}
+
+unsigned cell_blocks( const tn_mesh* m )
+{
+    return unsigned( ( (long long) kDiamonds * m->N * m->N * m->N + kFvThreads - 1 ) / kFvThreads );
+}
+
+int ghost_update( const tn_mesh* m, double* f, cudaStream_t st )
+{
+    const long long n = (long long) kDiamonds * 4 * m->N * m->N;
+    fv_ghost_kernel<<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( m->N, m->d_fv_ghost, f );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+int make_geom( const tn_mesh* m, const double* const* vel, const double* const* cen, FvGeom& G )
+{
+    TN_CHECK_ARG( vel && cen, "fct: null field list" );
+    for ( int a = 0; a < 3; ++a )
+    {
+        TN_CHECK_ARG( vel[a] && cen[a], "fct: null field pointer" );
+        G.vel.p[a] = vel[a];
+        G.cen.p[a] = cen[a];
+    }
+    G.N = m->N, G.coords = m->d_coords, G.radii = m->d_radii;
+    return TN_OK;
+}
+
+}  // namespace
+
+}  // namespace tn
+
+using namespace tn;
+
+extern "C" int tn_fv_field_size( const tn_mesh* m, size_t* n )
+{
+    TN_CHECK_ARG( m && n, "tn_fv_field_size: null argument" );
+    *n = fv_size( m );
+    return TN_OK;
+}
+
+extern "C" int tn_fct_workspace_size( const tn_mesh* m, size_t* n )
+{
+    TN_CHECK_ARG( m && n, "tn_fct_workspace_size: null argument" );
+    *n = 9 * fv_size( m );
+    return TN_OK;
+}
+
+extern "C" int tn_fv_ghost_update_f64( const tn_mesh* m, double* field, void* s )
+{
+    TN_CHECK_ARG( m && field, "tn_fv_ghost_update_f64: null argument" );
+    return ghost_update( m, field, as_stream( s ) );
+}
+
+extern "C" int tn_fv_cell_centers_f64( const tn_mesh* m, double* const* centers, void* s )
+{
+    TN_CHECK_ARG( m && centers && centers[0] && centers[1] && centers[2], "tn_fv_cell_centers_f64: null argument" );
+    cudaStream_t st = as_stream( s );
+    Ptr3< double > c{ { centers[0], centers[1], centers[2] } };
+    for ( int a = 0; a < 3; ++a )
+        TN_CUDA_TRY( cudaMemsetAsync( centers[a], 0, sizeof( double ) * fv_size( m ), st ) );
+    cell_centers_kernel<<< cell_blocks( m ), kFvThreads, 0, st >>>( m->N, m->d_coords, m->d_radii, c );
+    TN_LAUNCH_CHECK();
+    for ( int a = 0; a < 3; ++a )
+    {
+        int rc = ghost_update( m, centers[a], st );
+        if ( rc )
+            return rc;
+    }
+    return TN_OK;
+}
+
+extern "C" int tn_fct_dt_stable_f64( const tn_mesh* m, const double* const* vel, const double* const* centers,
+                                     double diffusivity, double* dt_stable, void* s )
+{
+    TN_CHECK_ARG( m && dt_stable, "tn_fct_dt_stable_f64: null argument" );
+    FvGeom G{};
+    int    rc;
+    if ( ( rc = make_geom( m, vel, centers, G ) ) )
+        return rc;
+    cudaStream_t        st   = as_stream( s );
+    unsigned long long* slot = reinterpret_cast< unsigned long long* >( m->d_red_result + 12 );
+    const double        init = 1e300;
+    TN_CUDA_TRY( cudaMemcpyAsync( slot, &init, sizeof( double ), cudaMemcpyHostToDevice, st ) );
+    dt_kernel<<< cell_blocks( m ), kFvThreads, 0, st >>>( G, diffusivity, slot );
+    TN_LAUNCH_CHECK();
+    TN_CUDA_TRY( cudaMemcpyAsync( dt_stable, slot, sizeof( double ), cudaMemcpyDeviceToHost, st ) );
+    TN_CUDA_TRY( cudaStreamSynchronize( st ) );
+    return TN_OK;
+}
+
+extern "C" int tn_fct_apply_dirichlet_f64( const tn_mesh* m, double* T, const tn_fct_dirichlet* bcs, void* s )
+{
+    TN_CHECK_ARG( m && T && bcs, "tn_fct_apply_dirichlet_f64: null argument" );
+    const long long n = (long long) kDiamonds * m->N * m->N;
+    dirichlet_kernel<<< unsigned( ( n + 255 ) / 256 ), 256, 0, as_stream( s ) >>>(
+        m->N, T, bcs->T_cmb, bcs->T_surface, bcs->apply_cmb, bcs->apply_surface );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+extern "C" int tn_fct_step_f64( const tn_mesh* m, double* T, const double* const* vel, const double* const* centers,
+                                double dt, double diffusivity, const double* source, int subtract_divergence,
+                                const tn_fct_dirichlet* bcs, double* workspace, void* s )
+{
+    TN_CHECK_ARG( m && T && workspace, "tn_fct_step_f64: null argument" );
+    FvGeom G{};
+    int    rc;
+    if ( ( rc = make_geom( m, vel, centers, G ) ) )
+        return rc;
+    cudaStream_t st = as_stream( s );
+    const size_t nf = fv_size( m );
+    double *     TL = workspace, *F = workspace + nf, *Rp = workspace + 7 * nf, *Rm = workspace + 8 * nf;
+    TN_CUDA_TRY( cudaMemsetAsync( TL, 0, sizeof( double ) * nf, st ) );
+    TN_CUDA_TRY( cudaMemsetAsync( Rp, 0, sizeof( double ) * 2 * nf, st ) );
+    // predictor (fct_advection_diffusion.hpp:384-433) on T with fresh lateral ghosts
+    if ( ( rc = ghost_update( m, T, st ) ) )
+        return rc;
+    predictor_kernel<<< cell_blocks( m ), kFvThreads, 0, st >>>( G, T, TL, F, dt, diffusivity, source,
+                                                                 subtract_divergence );
+    TN_LAUNCH_CHECK();
+    if ( bcs && ( rc = tn_fct_apply_dirichlet_f64( m, TL, bcs, s ) ) )
+        return rc;
+    // limiter (:539-566) and correction (:658-680)
+    if ( ( rc = ghost_update( m, TL, st ) ) )
+        return rc;
+    limiter_kernel<<< cell_blocks( m ), kFvThreads, 0, st >>>( m->N, TL, F, Rp, Rm );
+    TN_LAUNCH_CHECK();
+    if ( ( rc = ghost_update( m, Rp, st ) ) || ( rc = ghost_update( m, Rm, st ) ) )
+        return rc;
+    correction_kernel<<< cell_blocks( m ), kFvThreads, 0, st >>>( m->N, TL, F, Rp, Rm, T );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}

@@ -210,6 +210,62 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
     }
     m->n_halo_groups = int( offsets.size() ) - 1;
 
+    // FV ghost map: every lateral boundary face of a diamond is shared with
+    // exactly one other diamond; both sides hold its two edge nodes bit for bit
+    std::vector< int > fv_ghost( size_t( kDiamonds ) * 4 * N * 3, -1 );
+    {
+        using Key = std::array< uint64_t, 6 >;
+        std::map< Key, std::vector< std::array< int, 3 > > > edges; // (diamond, side, i)
+        auto edge_nodes = [&]( int side, int i, int& ax, int& ay, int& bx, int& by ) {
+            if ( side < 2 )
+                ax = bx = side == 0 ? 0 : N, ay = i, by = i + 1;
+            else
+                ay = by = side == 2 ? 0 : N, ax = i, bx = i + 1;
+        };
+        auto key_of = [&]( int d, int ax, int ay, int bx, int by ) {
+            std::array< uint64_t, 3 > ka, kb;
+            std::memcpy( ka.data(), &m->h_coords[( ( size_t( d ) * n1 + ax ) * n1 + ay ) * 3], 24 );
+            std::memcpy( kb.data(), &m->h_coords[( ( size_t( d ) * n1 + bx ) * n1 + by ) * 3], 24 );
+            if ( kb < ka )
+                std::swap( ka, kb );
+            return Key{ ka[0], ka[1], ka[2], kb[0], kb[1], kb[2] };
+        };
+        for ( int d = 0; d < kDiamonds; ++d )
+            for ( int side = 0; side < 4; ++side )
+                for ( int i = 0; i < N; ++i )
+                {
+                    int ax, ay, bx, by;
+                    edge_nodes( side, i, ax, ay, bx, by );
+                    edges[key_of( d, ax, ay, bx, by )].push_back( { d, side, i } );
+                }
+        for ( auto& kv : edges )
+        {
+            if ( kv.second.size() != 2 )
+            {
+                set_error( "tn_mesh_create: a diamond boundary edge is not shared by exactly two diamonds" );
+                tn_mesh_destroy( m );
+                return TN_ERR_STATE;
+            }
+            for ( int k = 0; k < 2; ++k )
+            {
+                const auto& me = kv.second[k];
+                const auto& ot = kv.second[1 - k];
+                // the real cell of the other diamond adjacent to its boundary edge
+                int x, y;
+                if ( ot[1] == 0 )
+                    x = 1, y = ot[2] + 1;
+                else if ( ot[1] == 1 )
+                    x = N, y = ot[2] + 1;
+                else if ( ot[1] == 2 )
+                    x = ot[2] + 1, y = 1;
+                else
+                    x = ot[2] + 1, y = N;
+                int* e = &fv_ghost[( size_t( me[0] * 4 + me[1] ) * N + me[2] ) * 3];
+                e[0] = ot[0], e[1] = x, e[2] = y;
+            }
+        }
+    }
+
     // Gram matrix of the rigid rotations e_j x x over owned nodes, inverted:
     // the orthonormalised penalty modes m = C (e_j x x) satisfy C^T C = Gram^{-1}.
     double Gm[3][3] = { { 0 } };
@@ -249,6 +305,7 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
          ( rc = upload( m->h_lat_owned.data(), m->h_lat_owned.size(), &m->d_lat_owned ) ) ||
          ( rc = upload( node_owned.data(), node_owned.size(), &m->d_node_owned ) ) ||
          ( rc = upload( offsets.data(), offsets.size(), &m->d_halo_offsets ) ) ||
+         ( rc = upload( fv_ghost.data(), fv_ghost.size(), &m->d_fv_ghost ) ) ||
          ( rc = upload( members.data(), std::max< size_t >( members.size(), 1 ), &m->d_halo_members ) ) )
     {
         tn_mesh_destroy( m );
@@ -280,6 +337,7 @@ extern "C" int tn_mesh_destroy( tn_mesh* m )
     cudaFree( m->d_node_owned );
     cudaFree( m->d_halo_offsets );
     cudaFree( m->d_halo_members );
+    cudaFree( m->d_fv_ghost );
     cudaFree( m->d_red_partials );
     cudaFree( m->d_red_result );
     cudaFree( m->d_red_counter );

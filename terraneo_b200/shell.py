@@ -430,6 +430,57 @@ def epsdivdiv_kgrad(mesh, bc_cmb, bc_surface, u, lam, out, comm_mode=C.COMM_ADDI
               ctypes.c_void_p(out.data.data_ptr()), _stream()), "epsdivdiv_kgrad")
 
 
+class FCTAdvectionDiffusion:
+    """FV FCT advection-diffusion (fv/hex/operators/fct_advection_diffusion.hpp) on the cells of `mesh`:
+    cell centres computed once, workspace kept; fields are torch [10, N+2, N+2, N+2] FP64 tensors."""
+
+    def __init__(self, mesh):
+        self.mesh = mesh
+        n2 = mesh.N + 2
+        self.fv_shape = (10, n2, n2, n2)
+        self.centers = torch.zeros((3,) + self.fv_shape, dtype=torch.float64, device="cuda")
+        C.check(C.lib().tn_fv_cell_centers_f64(mesh.handle, C.ptrs(*[self.centers[a].data_ptr() for a in range(3)]),
+                                               _stream()), "fv_cell_centers")
+        n = ctypes.c_size_t()
+        C.check(C.lib().tn_fct_workspace_size(mesh.handle, ctypes.byref(n)), "fct_workspace_size")
+        self.work = torch.zeros(n.value, dtype=torch.float64, device="cuda")
+
+    def field(self):
+        return torch.zeros(self.fv_shape, dtype=torch.float64, device="cuda")
+
+    def _c(self):
+        return C.ptrs(*[self.centers[a].data_ptr() for a in range(3)])
+
+    def dt_stable(self, vel, diffusivity=0.0):
+        dt = ctypes.c_double()
+        C.check(C.lib().tn_fct_dt_stable_f64(self.mesh.handle, vel.comp_ptrs(), self._c(), diffusivity,
+                                             ctypes.byref(dt), _stream()), "fct_dt_stable")
+        return dt.value
+
+    @staticmethod
+    def dirichlet(T_cmb, T_surface, cmb=True, surface=True):
+        return C.FCTDirichlet(T_cmb, T_surface, int(cmb), int(surface))
+
+    def apply_dirichlet(self, T, bcs):
+        C.check(C.lib().tn_fct_apply_dirichlet_f64(self.mesh.handle, ctypes.c_void_p(T.data_ptr()), ctypes.byref(bcs),
+                                                   _stream()), "fct_apply_dirichlet")
+
+    def ghost_update(self, f):
+        C.check(C.lib().tn_fv_ghost_update_f64(self.mesh.handle, ctypes.c_void_p(f.data_ptr()), _stream()),
+                "fv_ghost_update")
+
+    def step(self, T, vel, dt, diffusivity=0.0, source=None, subtract_divergence=True, bcs=None):
+        sp = ctypes.c_void_p(source.data_ptr()) if source is not None else None
+        bp = ctypes.byref(bcs) if bcs is not None else None
+        C.check(C.lib().tn_fct_step_f64(self.mesh.handle, ctypes.c_void_p(T.data_ptr()), vel.comp_ptrs(), self._c(),
+                                        dt, diffusivity, sp, int(subtract_divergence), bp,
+                                        ctypes.c_void_p(self.work.data_ptr()), _stream()), "fct_step")
+
+    @property
+    def T_L(self):
+        return self.work[:self.centers[0].numel()].view(self.fv_shape)
+
+
 def freeslip_project(u, cmb=True, surface=True):
     C.check(C.lib().tn_freeslip_project_f64(u.mesh.handle, u.comp_ptrs(), int(cmb), int(surface), _stream()),
             "freeslip_project")

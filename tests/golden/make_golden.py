@@ -43,6 +43,28 @@ def inputs(fine, coarse):
     return dict(k=k, u=u, s=s, p=p, uc=uc, pc=pc)
 
 
+FCT_CASES = [(0.0, 0), (0.01, 1)]
+
+
+def fct_inputs(fine):
+    """rigid rotation plus a smooth perturbation; temperature from the oracle's cell centres (seeded)"""
+    rs = np.random.RandomState(77)
+    x = fine.coords[:, :, :, None, :] * fine.radii[:, None, None, :, None]
+    w = rs.normal(size=3)
+    vel = np.cross(np.broadcast_to(w, x.shape), x)
+    vel += 0.2 * np.stack([np.sin(3 * x[..., 1]), np.cos(2 * x[..., 2]), np.sin(4 * x[..., 0])], axis=-1)
+    vel = fine.make_consistent(np.ascontiguousarray(np.moveaxis(vel, -1, 0)))
+    c = fine.fv_cell_centers()
+    N = fine.N
+    inner = (slice(None), slice(1, N + 1), slice(1, N + 1), slice(1, N + 1))
+    T = np.zeros(fine.fv_shape)
+    cc = c[(slice(None),) + inner]
+    T[inner] = 0.5 + 0.3 * np.sin(4 * cc[0]) * np.cos(3 * cc[1]) + 0.2 * (cc[2] > 0)
+    src = np.zeros(fine.fv_shape)
+    src[inner] = 0.1 * np.cos(cc[0])
+    return vel, T, src
+
+
 def checksum(a):
     a = np.asarray(a, dtype=np.float64)
     return np.array([a.sum(), (a * a).sum(), np.abs(a).max()])
@@ -106,6 +128,18 @@ def main():
         for bcc, bcs, diag in VLAPLACE_CASES:
             run_ref(["vlaplace", L, R_MIN, R_MAX, bcc, bcs, diag, d], d)
             out[f"vlaplace_{bcc}{bcs}{diag}"] = np.fromfile(f"{d}/dst.bin").reshape((3,) + fine.shape)
+        # FCT: one fct_explicit_step on a rotation-dominated velocity
+        vel, T, src = fct_inputs(fine)
+        vel.tofile(f"{d}/vel.bin")
+        for kappa, bc in FCT_CASES:
+            T.tofile(f"{d}/T.bin")
+            src.tofile(f"{d}/src.bin")
+            run_ref(["fct", L, R_MIN, R_MAX, -1, kappa, bc, d], d)
+            tag = f"fct_{kappa:g}_{bc}"
+            out[tag + "_dt"] = np.fromfile(f"{d}/dt.bin")
+            out[tag + "_T"] = np.fromfile(f"{d}/T.bin").reshape(fine.fv_shape)
+            out[tag + "_TL"] = np.fromfile(f"{d}/TL.bin").reshape(fine.fv_shape)
+        out["fct_centers"] = np.fromfile(f"{d}/centers.bin").reshape((3,) + fine.fv_shape)
     path = os.path.join(HERE, f"ref_L{L}.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")

@@ -43,6 +43,13 @@ def lib():
         L.or_kerngen_local_matrices.argtypes = [ctypes.c_int, _D, _D, _D, _D]
         L.or_gca_coarsen.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, _D]
         L.or_stored_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.or_fv_ghost_update.argtypes = [ctypes.c_int, _D, _D]
+        L.or_fv_cell_centers.argtypes = [ctypes.c_int, _D, _D, _D]
+        L.or_fct_dt_stable.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_double]
+        L.or_fct_dt_stable.restype = ctypes.c_double
+        L.or_fct_dirichlet.argtypes = [ctypes.c_int, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        L.or_fct_step.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, _D,
+                                  ctypes.c_int, _D, _D]
         L.or_prolongation_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D]
         L.or_restriction_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _U8, _D, _D]
         L.or_kmass_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int]
@@ -187,6 +194,40 @@ class Mesh:
         lib().or_stored_apply(self.L, _p(self.coords), _p(self.radii), _p(np.ascontiguousarray(mats)),
                               _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst), bc_cmb, bc_surf, int(diag))
         return dst
+
+    @property
+    def fv_shape(self):
+        return (10, self.N + 2, self.N + 2, self.N + 2)
+
+    def fv_cell_centers(self):
+        c = np.zeros((3,) + self.fv_shape)
+        lib().or_fv_cell_centers(self.L, _p(self.coords), _p(self.radii), _p(c))
+        return c
+
+    def fv_ghost_update(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64).copy()
+        lib().or_fv_ghost_update(self.L, _p(self.coords), _p(f))
+        return f
+
+    def fct_dt_stable(self, centers, vel, diffusivity=0.0):
+        return lib().or_fct_dt_stable(self.L, _p(self.coords), _p(self.radii), _p(np.ascontiguousarray(centers)),
+                                      _p(np.ascontiguousarray(vel, dtype=np.float64)), diffusivity)
+
+    def fct_dirichlet(self, T, T_cmb=1.0, T_surf=0.0, cmb=True, surf=True):
+        T = np.ascontiguousarray(T, dtype=np.float64).copy()
+        lib().or_fct_dirichlet(self.L, _p(T), T_cmb, T_surf, int(cmb), int(surf))
+        return T
+
+    def fct_step(self, centers, vel, T, dt, diffusivity=0.0, source=None, subtract_divergence=True, bcs=None):
+        """one FCT step; returns (T_new, T_L); bcs = (T_cmb, T_surface, apply_cmb, apply_surface) or None"""
+        T = np.ascontiguousarray(T, dtype=np.float64).copy()
+        TL = np.zeros(self.fv_shape)
+        b = None if bcs is None else _p(np.array(bcs, dtype=np.float64))
+        sp = None if source is None else _p(np.ascontiguousarray(source, dtype=np.float64))
+        lib().or_fct_step(self.L, _p(self.coords), _p(self.radii), _p(np.ascontiguousarray(centers)),
+                          _p(np.ascontiguousarray(vel, dtype=np.float64)), _p(T), dt, diffusivity, sp,
+                          int(subtract_divergence), b, _p(TL))
+        return T, TL
 
     def kmass(self, k, src, mode=0):
         dst = np.zeros(self.shape)

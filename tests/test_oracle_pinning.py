@@ -95,6 +95,24 @@ def test_vector_laplace_matches_reference(case, bcc, bcs, diag):
     assert rel(fine.vector_laplace(x["u"], bcc, bcs, diag), g[f"vlaplace_{bcc}{bcs}{diag}"]) <= TOL
 
 
+@pytest.mark.parametrize("kappa,bc", G.FCT_CASES)
+def test_fct_matches_reference(case, kappa, bc):
+    g, fine, _, _ = case
+    vel, T, src = G.fct_inputs(fine)
+    c = fine.fv_cell_centers()
+    assert np.abs(c - g["fct_centers"]).max() <= 1e-15
+    tag = f"fct_{kappa:g}_{bc}"
+    dt_stable, dt = g[tag + "_dt"]
+    assert fine.fct_dt_stable(c, vel, kappa) == pytest.approx(dt_stable, rel=1e-13)
+    T0 = fine.fct_dirichlet(T) if bc else T.copy()
+    Tn, TL = fine.fct_step(c, vel, fine.fv_ghost_update(T0), dt, kappa, src, True, (1.0, 0.0, 1, 1) if bc else None)
+    N = fine.N
+    inner = (slice(None), slice(1, N + 1), slice(1, N + 1), slice(1, N + 1))
+    assert rel(Tn[inner], g[tag + "_T"][inner]) <= TOL
+    assert rel(TL[inner], g[tag + "_TL"][inner]) <= TOL
+    assert rel(Tn, g[tag + "_T"]) <= TOL  # ghost layers included
+
+
 def test_golden_fixture_is_not_trivial(case):
     """A planted error in the oracle's input must break the comparison."""
     g, fine, _, x = case
