@@ -400,7 +400,8 @@ TN_API int tn_laplace_pcg_solve_f64( const tn_mesh* mesh, const double* b, doubl
                                      double relative_tolerance, double absolute_tolerance, int* iterations,
                                      double* relative_residual );
 
-/* Multigrid-preconditioned CG on DivKGrad (k NULL: k = 1, the Laplace) with
+/* Multigrid-preconditioned Krylov solve (CG, BiCGStab(2) or MINRES) on
+ * DivKGrad (k NULL: k = 1, the Laplace) with
  * homogeneous Dirichlet elimination on both radii: one V-cycle per CG
  * iteration over levels [level - mg_levels + 1, level], linear transfers
  * (prolongation_linear.hpp / restriction_linear.hpp), Jacobi (smoother 1,
@@ -425,6 +426,7 @@ typedef struct
     int    max_iterations;
     double relative_tolerance;
     double absolute_tolerance;
+    int    krylov; /* outer solver: 0 PCG (pcg.hpp), 1 PBiCGStab(2) (pbicgstab.hpp), 2 PMINRES (pminres.hpp) */
 } tn_scalar_mg_params;
 
 TN_API int tn_divkgrad_mg_pcg_solve_f64( const tn_scalar_mg_params* params, double r_min, double r_max,
@@ -461,6 +463,8 @@ typedef struct
     double absolute_tolerance;
     int    gca; /* coarse viscous operators: 0 re-discretised with injected viscosity, 1 GCA with
                    constant interpolation (TwoGridGCA default), 2 GCA with linear interpolation */
+    int    outer; /* 0 FGMRES(restart) + block-triangular preconditioner, 1 PMINRES + block-diagonal
+                     preconditioner (pminres.hpp, block_preconditioner_2x2.hpp:38-100) */
 } tn_stokes_params;
 
 typedef struct tn_stokes_solver tn_stokes_solver;

@@ -366,6 +366,252 @@ class BlockTriangularPreconditioner2x2
     Prec22&  p22_;
 };
 
+// BlockDiagonalPreconditioner2x2 (block_preconditioner_2x2.hpp:38-100):
+// x_1 = P11(b_1), x_2 = P22(b_2)
+template < typename Block11, typename Prec11, typename Prec22, typename BV >
+class BlockDiagonalPreconditioner2x2
+{
+  public:
+    BlockDiagonalPreconditioner2x2( Block11& a11, Prec11& p11, Prec22& p22 ) : a11_( a11 ), p11_( p11 ), p22_( p22 ) {}
+    template < typename Op >
+    void solve_impl( Op&, BV& x, const BV& b )
+    {
+        solve( p11_, a11_, x.block_1(), b.block_1() );
+        solve( p22_, a11_, x.block_2(), b.block_2() );
+    }
+
+  private:
+    Block11& a11_;
+    Prec11&  p11_;
+    Prec22&  p22_;
+};
+
+// swap of two vector handles (the VectorLike swap_impl)
+template < typename V >
+void swap_vectors( V& a, V& b )
+{
+    a.swap_impl( b );
+}
+
+// Preconditioned MINRES (pminres.hpp:30-175): Lanczos with the
+// preconditioner's inner product, Givens QR, short recurrences; stops on the
+// preconditioned residual estimate |eta|.
+template < typename Op, typename Prec = IdentitySolver< Op > >
+class PMINRES
+{
+  public:
+    using V = typename Op::SrcVectorType;
+    PMINRES( IterativeSolverParameters prm, std::vector< V > tmps, Prec prec = Prec() )
+    : prm_( prm ), tmp_( std::move( tmps ) ), prec_( prec )
+    {
+        if ( tmp_.size() < 7 )
+            throw std::runtime_error( "PMINRES: needs 7 temporary vectors" );
+    }
+    SolverStatistics stats;
+    void             solve_impl( Op& A, V& x, const V& b )
+    {
+        using S     = typename V::ScalarType;
+        auto& az    = tmp_[0];
+        auto& vjm1  = tmp_[1];
+        auto& vj    = tmp_[2];
+        auto& wjm1  = tmp_[3];
+        auto& wj    = tmp_[4];
+        auto& zjp1  = tmp_[5];
+        auto& z     = tmp_[6];
+        stats       = {};
+        assign( vjm1, S( 0 ) );
+        assign( wj, S( 0 ) );
+        assign( wjm1, S( 0 ) );
+        apply( A, x, vj );
+        lincomb( vj, { S( 1 ), S( -1 ) }, { b, vj } );
+        assign( z, S( 0 ) );
+        solve( prec_, A, z, vj );
+        double gjm1 = 1.0, gj = std::sqrt( double( dot( z, vj ) ) ), eta = gj;
+        double sjm1 = 0.0, sj = 0.0, cjm1 = 1.0, cj = 1.0;
+        const double r0 = gj;
+        stats.relative_residuals.push_back( 1.0 );
+        if ( r0 < prm_.absolute_residual_tolerance )
+            return;
+        for ( int it = 1; it <= prm_.max_iterations; ++it )
+        {
+            lincomb( z, { S( 1.0 / gj ) }, { z } );
+            apply( A, z, az );
+            const double delta = double( dot( az, z ) );
+            lincomb( vjm1, { S( 1 ), S( -delta / gj ), S( -gj / gjm1 ) }, { az, vj, vjm1 } );
+            swap_vectors( vjm1, vj );
+            assign( zjp1, S( 0 ) );
+            solve( prec_, A, zjp1, vj );
+            const double gjp1 = std::sqrt( double( dot( zjp1, vj ) ) );
+            const double a0 = cj * delta - cjm1 * sj * gj;
+            const double a1 = std::sqrt( a0 * a0 + gjp1 * gjp1 );
+            const double a2 = sj * delta + cjm1 * cj * gj;
+            const double a3 = sjm1 * gj;
+            const double cjp1 = a0 / a1, sjp1 = gjp1 / a1;
+            lincomb( wjm1, { S( 1.0 / a1 ), S( -a3 / a1 ), S( -a2 / a1 ) }, { z, wjm1, wj } );
+            swap_vectors( wjm1, wj );
+            lincomb( x, { S( 1 ), S( cjp1 * eta ) }, { x, wj } );
+            eta = -sjp1 * eta;
+            const double ar = std::abs( eta ), rr = ar / r0;
+            stats.relative_residuals.push_back( rr );
+            stats.iterations = it;
+            if ( rr <= prm_.relative_residual_tolerance || ar < prm_.absolute_residual_tolerance )
+                return;
+            swap_vectors( z, zjp1 );
+            gjm1 = gj, gj = gjp1;
+            cjm1 = cj, cj = cjp1;
+            sjm1 = sj, sj = sjp1;
+        }
+    }
+
+  private:
+    IterativeSolverParameters prm_;
+    std::vector< V >          tmp_;
+    Prec                      prec_;
+};
+
+// small dense solve with full pivoting (the reference uses Eigen's
+// fullPivLu for BiCGStab(l)'s l x l minimal-residual system)
+inline std::vector< double > dense_solve_full_pivot( std::vector< double > M, std::vector< double > rhs, int n )
+{
+    std::vector< int > colp( n );
+    for ( int i = 0; i < n; ++i )
+        colp[i] = i;
+    for ( int k = 0; k < n; ++k )
+    {
+        int    pi = k, pj = k;
+        double best = -1.0;
+        for ( int i = k; i < n; ++i )
+            for ( int j = k; j < n; ++j )
+                if ( std::abs( M[i * n + j] ) > best )
+                    best = std::abs( M[i * n + j] ), pi = i, pj = j;
+        if ( pi != k )
+        {
+            for ( int j = 0; j < n; ++j )
+                std::swap( M[k * n + j], M[pi * n + j] );
+            std::swap( rhs[k], rhs[pi] );
+        }
+        if ( pj != k )
+        {
+            for ( int i = 0; i < n; ++i )
+                std::swap( M[i * n + k], M[i * n + pj] );
+            std::swap( colp[k], colp[pj] );
+        }
+        if ( M[k * n + k] == 0.0 )
+            continue;
+        for ( int i = k + 1; i < n; ++i )
+        {
+            const double f = M[i * n + k] / M[k * n + k];
+            for ( int j = k; j < n; ++j )
+                M[i * n + j] -= f * M[k * n + j];
+            rhs[i] -= f * rhs[k];
+        }
+    }
+    std::vector< double > y( n, 0.0 ), out( n, 0.0 );
+    for ( int i = n - 1; i >= 0; --i )
+    {
+        double v = rhs[i];
+        for ( int j = i + 1; j < n; ++j )
+            v -= M[i * n + j] * y[j];
+        y[i] = M[i * n + i] != 0.0 ? v / M[i * n + i] : 0.0;
+    }
+    for ( int i = 0; i < n; ++i )
+        out[colp[i]] = y[i];
+    return out;
+}
+
+// Preconditioned BiCGStab(l) (pbicgstab.hpp:29-290): l BiCG steps and an
+// l-dimensional minimal-residual update per iteration, left preconditioning;
+// the shadow residual is the deterministic randomize of this library.
+template < typename Op, typename Prec = IdentitySolver< Op > >
+class PBiCGStab
+{
+  public:
+    using V = typename Op::SrcVectorType;
+    PBiCGStab( int l, IterativeSolverParameters prm, std::vector< V > tmps, Prec prec = Prec() )
+    : l_( l ), prm_( prm ), tmp_( std::move( tmps ) ), prec_( prec )
+    {
+        if ( int( tmp_.size() ) < 2 * ( l + 1 ) + 2 )
+            throw std::runtime_error( "PBiCGStab: needs 2 (l + 1) + 2 temporary vectors" );
+    }
+    SolverStatistics stats;
+    void             solve_impl( Op& A, V& x, const V& b )
+    {
+        using S = typename V::ScalarType;
+        stats   = {};
+        randomize( rshadow() );
+        for ( int j = 0; j < l_ + 1; ++j )
+            assign( us( j ), S( 0 ) );
+        apply( A, x, rs( 0 ) );
+        lincomb( rs( 0 ), { S( 1 ), S( -1 ) }, { b, rs( 0 ) } );
+        precondition( A, rs( 0 ) );
+        const double r0 = std::sqrt( double( dot( rs( 0 ), rs( 0 ) ) ) );
+        double       ar = r0;
+        stats.relative_residuals.push_back( 1.0 );
+        if ( r0 < prm_.absolute_residual_tolerance )
+            return;
+        double omega = 1.0, sigma = 1.0;
+        int    it    = 1;
+        for ( ; it < prm_.max_iterations; ++it )
+        {
+            sigma = -omega * sigma;
+            for ( int j = 0; j < l_; ++j )
+            {
+                const double rho  = double( dot( rshadow(), rs( j ) ) );
+                const double beta = rho / sigma;
+                for ( int i = 0; i <= j; ++i )
+                    lincomb( us( i ), { S( 1 ), S( -beta ) }, { rs( i ), us( i ) } );
+                apply( A, us( j ), us( j + 1 ) );
+                precondition( A, us( j + 1 ) );
+                sigma             = double( dot( rshadow(), us( j + 1 ) ) );
+                const double alpha = rho / sigma;
+                for ( int i = 0; i <= j; ++i )
+                    lincomb( rs( i ), { S( 1 ), S( -alpha ) }, { rs( i ), us( i + 1 ) } );
+                apply( A, rs( j ), rs( j + 1 ) );
+                precondition( A, rs( j + 1 ) );
+                lincomb( x, { S( 1 ), S( alpha ) }, { x, us( 0 ) } );
+            }
+            std::vector< double > M( l_ * l_ ), m0( l_ );
+            for ( int j = 1; j <= l_; ++j )
+                m0[j - 1] = double( dot( rs( 0 ), rs( j ) ) );
+            for ( int i = 0; i < l_; ++i )
+                for ( int j = 0; j < l_; ++j )
+                    M[i * l_ + j] = double( dot( rs( i + 1 ), rs( j + 1 ) ) );
+            const auto g = dense_solve_full_pivot( M, m0, l_ );
+            for ( int j = 1; j <= l_; ++j )
+                lincomb( us( 0 ), { S( 1 ), S( -g[j - 1] ) }, { us( 0 ), us( j ) } );
+            for ( int j = 0; j < l_; ++j )
+                lincomb( x, { S( 1 ), S( g[j] ) }, { x, rs( j ) } );
+            for ( int j = 1; j <= l_; ++j )
+                lincomb( rs( 0 ), { S( 1 ), S( -g[j - 1] ) }, { rs( 0 ), rs( j ) } );
+            omega            = g[l_ - 1];
+            ar               = std::sqrt( double( dot( rs( 0 ), rs( 0 ) ) ) );
+            stats.iterations = it;
+            stats.relative_residuals.push_back( ar / r0 );
+            if ( ar / r0 <= prm_.relative_residual_tolerance || ar < prm_.absolute_residual_tolerance )
+                return;
+        }
+    }
+
+  private:
+    V&   rshadow() { return tmp_[0]; }
+    V&   rs( int i ) { return tmp_[1 + i]; }
+    V&   us( int i ) { return tmp_[1 + l_ + 1 + i]; }
+    V&   tmp_prec() { return tmp_[1 + 2 * ( l_ + 1 )]; }
+    void precondition( Op& A, V& v )
+    {
+        if constexpr ( !std::is_same_v< Prec, IdentitySolver< Op > > )
+        {
+            assign( tmp_prec(), v );
+            solve( prec_, A, tmp_prec(), v );
+            assign( v, tmp_prec() );
+        }
+    }
+    int                       l_;
+    IterativeSolverParameters prm_;
+    std::vector< V >          tmp_;
+    Prec                      prec_;
+};
+
 // FGMRES(m) with modified Gram-Schmidt Arnoldi and Givens rotations
 // (fgmres.hpp:108-330), including the reference's fall-back of skipping the
 // preconditioner when it returns NaN / Inf.

@@ -195,6 +195,27 @@ void finish( tn_stokes_solver& s, std::shared_ptr< Prec11 > p11 )
     apply( pm, ones, dp );
     auto p22 = std::make_shared< DiagonalSolver< KMass< double >, VectorQ1Scalar< double > > >( dp );
     auto a11 = s.A64fine;
+    IterativeSolverParameters ip{ prm.max_iterations, prm.relative_tolerance, prm.absolute_tolerance };
+    tn_stokes_solver*         sp = &s;
+    if ( prm.outer == 1 )
+    {
+        // PMINRES with the block-diagonal preconditioner (pminres.hpp, block_preconditioner_2x2.hpp:38-100)
+        using BD  = BlockDiagonalPreconditioner2x2< A64, Prec11, DiagonalSolver< KMass< double >, VectorQ1Scalar< double > >,
+                                                    VectorQ1IsoQ2Q1< double > >;
+        auto prec = std::make_shared< BD >( *a11, *p11, *p22 );
+        std::vector< VectorQ1IsoQ2Q1< double > > tmps;
+        for ( int i = 0; i < 7; ++i )
+            tmps.emplace_back( s.mesh[L], s.mesh[L - 1] );
+        auto mr = std::make_shared< PMINRES< EpsDivDivStokes< double >, BD > >( ip, tmps, *prec );
+        s.run = [sp, mr, prec, p11, p22, a11]( VectorQ1IsoQ2Q1< double >& x, const VectorQ1IsoQ2Q1< double >& b ) {
+            solve( *mr, *sp->K, x, b );
+            sp->history    = mr->stats.relative_residuals;
+            sp->iterations = mr->stats.iterations;
+            sp->relres     = mr->stats.relative_residuals.back();
+            sp->skips      = 0;
+        };
+        return;
+    }
     using BT = BlockTriangularPreconditioner2x2< A64, Gradient< double >, Prec11,
                                                  DiagonalSolver< KMass< double >, VectorQ1Scalar< double > >,
                                                  VectorQ1IsoQ2Q1< double > >;
@@ -202,9 +223,7 @@ void finish( tn_stokes_solver& s, std::shared_ptr< Prec11 > p11 )
     std::vector< VectorQ1IsoQ2Q1< double > > tmps;
     for ( int i = 0; i < 2 * prm.restart + 4; ++i )
         tmps.emplace_back( s.mesh[L], s.mesh[L - 1] );
-    IterativeSolverParameters ip{ prm.max_iterations, prm.relative_tolerance, prm.absolute_tolerance };
     auto fg = std::make_shared< FGMRES< EpsDivDivStokes< double >, BT > >( tmps, prm.restart, ip, *prec );
-    tn_stokes_solver* sp = &s;
     s.run = [sp, fg, prec, p11, p22, a11]( VectorQ1IsoQ2Q1< double >& x, const VectorQ1IsoQ2Q1< double >& b ) {
         solve( *fg, *sp->K, x, b );
         sp->history    = fg->stats.relative_residuals;
@@ -225,6 +244,7 @@ extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min,
                   "tn_stokes_solver_create: need mg_levels >= 2, level - mg_levels + 1 >= 2 and level <= 8" );
     TN_CHECK_ARG( p->restart >= 1 && p->max_iterations >= 1, "tn_stokes_solver_create: bad Krylov parameters" );
     TN_CHECK_ARG( p->gca >= 0 && p->gca <= 2, "tn_stokes_solver_create: gca must be 0, 1 or 2" );
+    TN_CHECK_ARG( p->outer == 0 || p->outer == 1, "tn_stokes_solver_create: outer must be 0 or 1" );
     try
     {
         auto s = std::make_unique< tn_stokes_solver >();
@@ -486,6 +506,7 @@ extern "C" int tn_divkgrad_mg_pcg_solve_f64( const tn_scalar_mg_params* p, doubl
     TN_CHECK_ARG( p && b && x, "tn_divkgrad_mg_pcg_solve_f64: null argument" );
     TN_CHECK_ARG( p->mg_levels >= 2 && p->level - p->mg_levels + 1 >= 0, "tn_divkgrad_mg_pcg_solve_f64: bad levels" );
     TN_CHECK_ARG( p->smoother == 0 || p->smoother == 1, "tn_divkgrad_mg_pcg_solve_f64: smoother must be 0 or 1" );
+    TN_CHECK_ARG( p->krylov >= 0 && p->krylov <= 2, "tn_divkgrad_mg_pcg_solve_f64: krylov must be 0, 1 or 2" );
     try
     {
         const int                                L = p->level, Lmin = L - p->mg_levels + 1;
@@ -550,15 +571,39 @@ extern "C" int tn_divkgrad_mg_pcg_solve_f64( const tn_scalar_mg_params* p, doubl
         std::vector< VectorQ1Scalar< double > > t4;
         for ( int i = 0; i < 4; ++i )
             t4.emplace_back( mesh[L] );
-        PCG< DKG, MGPreconditioner > pcg(
-            IterativeSolverParameters{ p->max_iterations, p->relative_tolerance, p->absolute_tolerance }, t4, prec );
-        VectorQ1Scalar< double > vb( mesh[L], const_cast< double* >( b ) ), vx( mesh[L], x );
-        solve( pcg, Afine, vx, vb );
+        const IterativeSolverParameters ip{ p->max_iterations, p->relative_tolerance, p->absolute_tolerance };
+        VectorQ1Scalar< double >        vb( mesh[L], const_cast< double* >( b ) ), vx( mesh[L], x );
+        SolverStatistics                st;
+        if ( p->krylov == 1 )
+        {
+            // PBiCGStab(2), left-preconditioned (tests/test_laplace_pbicgstab_multigrid.cpp composition)
+            std::vector< VectorQ1Scalar< double > > t8;
+            for ( int i = 0; i < 2 * 3 + 2; ++i )
+                t8.emplace_back( mesh[L] );
+            PBiCGStab< DKG, MGPreconditioner > bicg( 2, ip, t8, prec );
+            solve( bicg, Afine, vx, vb );
+            st = bicg.stats;
+        }
+        else if ( p->krylov == 2 )
+        {
+            std::vector< VectorQ1Scalar< double > > t7;
+            for ( int i = 0; i < 7; ++i )
+                t7.emplace_back( mesh[L] );
+            PMINRES< DKG, MGPreconditioner > mr( ip, t7, prec );
+            solve( mr, Afine, vx, vb );
+            st = mr.stats;
+        }
+        else
+        {
+            PCG< DKG, MGPreconditioner > pcg( ip, t4, prec );
+            solve( pcg, Afine, vx, vb );
+            st = pcg.stats;
+        }
         TN_CUDA_TRY( cudaDeviceSynchronize() );
         if ( iterations )
-            *iterations = pcg.stats.iterations;
+            *iterations = st.iterations;
         if ( relative_residual )
-            *relative_residual = pcg.stats.relative_residuals.back();
+            *relative_residual = st.relative_residuals.back();
         return TN_OK;
     }
     catch ( const std::exception& e )

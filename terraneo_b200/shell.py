@@ -356,12 +356,12 @@ def laplace_pcg(mesh, b, x, max_iterations=1000, relative_tolerance=1e-10, absol
 def divkgrad_mg_pcg(level, b, x, k=None, mg_levels=3, smoother=1, smoothing_steps=2, chebyshev_order=2,
                     power_iterations=10, jacobi_omega=0.6, vcycles=1, coarse_max_iterations=100,
                     coarse_relative_tolerance=1e-8, max_iterations=200, relative_tolerance=1e-10,
-                    absolute_tolerance=1e-30, r_min=0.55, r_max=1.0):
-    """Multigrid-preconditioned CG on DivKGrad (k None: Laplace), Dirichlet radii; x updated in place.
-    smoother: 0 Chebyshev, 1 Jacobi.  Returns (iterations, relative residual)."""
+                    absolute_tolerance=1e-30, r_min=0.55, r_max=1.0, krylov=0):
+    """Multigrid-preconditioned Krylov solve on DivKGrad (k None: Laplace), Dirichlet radii; x updated in place.
+    smoother: 0 Chebyshev, 1 Jacobi; krylov: 0 PCG, 1 PBiCGStab(2), 2 PMINRES.  Returns (iterations, relres)."""
     prm = C.ScalarMGParams(level, mg_levels, smoother, smoothing_steps, chebyshev_order, power_iterations,
                            jacobi_omega, vcycles, coarse_max_iterations, coarse_relative_tolerance, max_iterations,
-                           relative_tolerance, absolute_tolerance)
+                           relative_tolerance, absolute_tolerance, krylov)
     it, rr = ctypes.c_int(), ctypes.c_double()
     kp = ctypes.c_void_p(k.data.data_ptr()) if k is not None else None
     C.check(C.lib().tn_divkgrad_mg_pcg_solve_f64(ctypes.byref(prm), r_min, r_max, kp,
@@ -378,10 +378,10 @@ class StokesSolver:
     def __init__(self, level, viscosity, mg_levels=4, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=True,
                  chebyshev_order=3, smoothing_steps=2, power_iterations=10, vcycles=1, coarse_max_iterations=50,
                  coarse_relative_tolerance=1e-6, restart=30, max_iterations=200, relative_tolerance=1e-8,
-                 absolute_tolerance=1e-30, r_min=0.55, r_max=1.0, gca=0):
+                 absolute_tolerance=1e-30, r_min=0.55, r_max=1.0, gca=0, outer=0):
         self.prm = C.StokesParams(level, mg_levels, bc_cmb, bc_surface, int(mg_fp32), chebyshev_order, smoothing_steps,
                                   power_iterations, vcycles, coarse_max_iterations, coarse_relative_tolerance, restart,
-                                  max_iterations, relative_tolerance, absolute_tolerance, int(gca))
+                                  max_iterations, relative_tolerance, absolute_tolerance, int(gca), int(outer))
         h = ctypes.c_void_p()
         C.check(C.lib().tn_stokes_solver_create(ctypes.byref(self.prm), r_min, r_max,
                                                 ctypes.c_void_p(viscosity.data.data_ptr()), ctypes.byref(h)),
