@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-stokes", action="store_true", help="skip the level-6 Stokes time-to-1e-8 leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the level-5 adjoint viscosity gradient leg")
+    ap.add_argument("--no-timestep", action="store_true", help="skip the level-7 mantle-circulation time-step leg")
     return ap.parse_args()
 
 
@@ -162,7 +163,11 @@ def adjoint_leg(shell, C, torch, level=5, directions=2, h=1e-5):
     k0, _ = synthetic_inputs(coords, radii, None)
     m0 = torch.as_tensor(np.log(k0), device="cuda")
     fu, fp = stokes_rhs(shell, pf, coords, radii), shell.VectorQ1Scalar(pc)
-    kw = dict(mg_levels=level - 2, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=False,
+    fu.data[:, :, :, :, 0] = 0.0  # Dirichlet rows of the right-hand side
+    fu.data[:, :, :, :, -1] = 0.0
+    # Dirichlet radii: the FP64 solves reach 1e-12 (free-slip ones plateau above it, which would turn
+    # the central differences into noise)
+    kw = dict(mg_levels=level - 2, bc_cmb=C.BC_DIRICHLET, bc_surface=C.BC_DIRICHLET, mg_fp32=False,
               relative_tolerance=1e-12, max_iterations=2000, restart=100, r_min=RMIN, r_max=RMAX)
     owned = torch.as_tensor(omask.astype(np.float64), device="cuda")
     m_obs = m0 + 0.1 * torch.as_tensor(smooth_field(coords, radii, 31), device="cuda")
@@ -187,12 +192,70 @@ def adjoint_leg(shell, C, torch, level=5, directions=2, h=1e-5):
             fd = (J(m0 + h * d) - J(m0 - h * d)).item() / (2 * h)
         ad = float((grad * d).sum())
         errs.append(abs(fd - ad) / abs(ad))
-    return {"workload": f"adjoint viscosity gradient, velocity level {level} / pressure level {level - 1}, free-slip "
+    return {"workload": f"adjoint viscosity gradient, velocity level {level} / pressure level {level - 1}, Dirichlet "
                         "both radii, J = 1/2 sum_owned |u - u_obs|^2, FP64 solves to 1e-12 (FGMRES(100), FP64 "
                         f"multigrid over {level - 2} levels)",
             "seconds_forward_adjoint_backward": round(sec, 4),
             "J": float(j.item()), "fd_directions": directions, "fd_step": h,
             "fd_max_rel_error": float(f"{max(errs):.3e}")}
+
+
+def timestep_leg(shell, C, torch, level=7):
+    """One mantle-circulation time step at level 7 (velocity 63,406,854 DoFs, pressure level 6,
+    20,971,520 FV cells): mixed-precision Stokes solve with the reference app's time-step Krylov
+    settings (FGMRES(10), at most 10 iterations, 1e-6; mantlecirculation parameters.hpp:59-62),
+    then one FP64 FCT advection-diffusion step at 0.5 x the stable dt (CFL 0.5)."""
+    free0, total = torch.cuda.mem_get_info()
+    pf, pc = shell.ShellMesh(level, RMIN, RMAX), shell.ShellMesh(level - 1, RMIN, RMAX)
+    coords, radii = pf.geometry()
+    k_np, _ = synthetic_inputs(coords, radii, None)
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(k_np)
+    fu, fp = stokes_rhs(shell, pf, coords, radii), shell.VectorQ1Scalar(pc)
+    del k_np
+    t0 = time.perf_counter()
+    s = shell.StokesSolver(level, kv, mg_levels=4, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=True,
+                           chebyshev_order=3, relative_tolerance=1e-6, max_iterations=10, restart=10, r_min=RMIN,
+                           r_max=RMAX, gca=1)
+    fct = shell.FCTAdvectionDiffusion(pf)
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t0
+    # temperature: conductive profile + smooth perturbation at the cell centres, Dirichlet 1 / 0
+    c = fct.centers
+    rr = torch.sqrt(c[0] ** 2 + c[1] ** 2 + c[2] ** 2).clamp_min(1e-30)
+    T = ((1 / rr - 1 / RMAX) / (1 / RMIN - 1 / RMAX)).clamp(0, 1) + 0.05 * torch.sin(4 * c[0]) * torch.cos(3 * c[1])
+    bcs = fct.dirichlet(1.0, 0.0)
+    fct.apply_dirichlet(T, bcs)
+    xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+    s.solve(fu, fp, xu, xp)  # warm-up step: eigenvalue estimates
+    xu.data.zero_()
+    xp.data.zero_()
+    T0 = T.clone()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    it, rr_s = s.solve(fu, fp, xu, xp)
+    ev[1].record()
+    dt = 0.5 * fct.dt_stable(xu, 0.0)
+    fct.step(T, xu, dt, 0.0, None, True, bcs)
+    fct.apply_dirichlet(T, bcs)
+    ev[2].record()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    stokes_s, fct_s = ev[0].elapsed_time(ev[1]) / 1e3, ev[1].elapsed_time(ev[2]) / 1e3
+    n = pf.N
+    Ti = T[:, 1:n + 1, 1:n + 1, 1:n + 1]
+    out = {"workload": f"time step at level {level}: Stokes (velocity level {level}, 63,406,854 DoFs; pressure level "
+                       f"{level - 1}; free-slip; FGMRES(10) <= 10 iterations to 1e-6 with the FP32 GCA V-cycle) + "
+                       "one FP64 FCT step of 20,971,520 FV cells at 0.5 dt_stable (advection, Dirichlet T)",
+           "seconds_per_step": round(stokes_s + fct_s, 4), "stokes_seconds": round(stokes_s, 4),
+           "stokes_iterations": it, "stokes_relres": float(f"{rr_s:.3e}"), "fct_seconds": round(fct_s, 5),
+           "dt": dt, "setup_seconds": round(setup, 2),
+           "device_memory_gb": round((total - free1) / 1e9, 2),
+           "T_range": [float(Ti.min()), float(Ti.max())]}
+    del s, fct, T, T0, xu, xp, fu, fp, kv
+    torch.cuda.empty_cache()
+    return out
 
 
 class ClockSampler:
@@ -440,6 +503,8 @@ def main():
             line["stokes"] = stokes_leg(shell, C, torch, k_np)
         if world == 1 and not args.no_adjoint:
             line["adjoint"] = adjoint_leg(shell, C, torch)
+        if world == 1 and not args.no_timestep:
+            line["timestep"] = timestep_leg(shell, C, torch)
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_baseline(steps=3)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}

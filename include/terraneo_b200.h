@@ -106,10 +106,15 @@ TN_API int tn_epsdivdiv_apply_f32( const tn_mesh* mesh, const tn_epsdivdiv_param
  * linalg/solvers/gca/gca.hpp:42-528; LocalMatrixStorage
  * linalg/solvers/gca/local_matrix_storage.hpp:29-243).
  *
- * Storage: [cell][wedge][18 x 18], cells (diamond, x, y, r) with r fastest,
- * entries in DIMENSIONWISE order (local node + 6 * dimension) and each matrix
- * COLUMN-major (entry (I, J) at J * 18 + I).  tn_local_matrix_count gives the
- * number of entries, 10 N^3 * 648 (FP64: 5,184 bytes per cell). */
+ * Storage: DIMENSIONWISE local order (local node + 6 * dimension).  The
+ * matrices are symmetric and only the upper triangle is stored, row by row:
+ * entry (I, J), I <= J, is entry e = 18 I - I (I - 1) / 2 + J - I of 171.
+ * Wedges are numbered w = 2 cell + wedge with cells (diamond, x, y, r), r
+ * fastest, and 32 consecutive wedges are interleaved entry by entry: entry e
+ * of wedge w lives at ((w / 32) * 171 + e) * 32 + w % 32.
+ * tn_local_matrix_count gives the number of entries (2 * 10 N^3 wedges padded
+ * to a multiple of 32, times 171; FP64 about 2,736 bytes per cell, the
+ * reference stores the full 5,184). */
 TN_API int tn_local_matrix_count( const tn_mesh* mesh, size_t* entries );
 /* kerngen assemble_local_matrix (:2051-2110) of every wedge: one-point rule,
  * nodal coefficient k (NULL: k = 1), no boundary treatment. */

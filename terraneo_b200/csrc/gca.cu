@@ -11,15 +11,19 @@
 //    slow path (epsilon_divdiv_kerngen.hpp:823-1052), the fs/fs penalty and
 //    the additive halo.
 //
-// Storage: [cell][wedge][18 x 18] with cells (d, x, y, r), r fastest, and each
-// matrix COLUMN-major (entry (I, J) at J * 18 + I) so that lane I of a warp
-// reading column J touches consecutive addresses.  FP64 5,184 B per cell.
+// Storage: the wedge matrices are symmetric (the kerngen form and every
+// P^T A P of it) and only the upper triangle is kept, row by row (entry
+// (I, J), I <= J, is entry e = 18 I - I (I - 1) / 2 + J - I of 171).  Wedges
+// are numbered w = 2 cell + wedge (cells (d, x, y, r), r fastest) and 32
+// consecutive wedges are interleaved: entry e of wedge w at
+// ((w / 32) 171 + e) 32 + w % 32.  FP64 2,736 B per cell.
 //
 // Coarsening: one 324-thread block per coarse cell, thread t owning entry
 // (t / 18, t % 18) of both coarse wedges; the interpolation matrices (and, at
 // the finest level, the fine wedges' geometry) of all 16 fine wedges are staged
 // in shared memory once, then per fine wedge T = A_f P and C += P^T T are two
-// 6-term passes.  Apply: one warp per wedge, lanes 0..17 own the rows.
+// 6-term passes.  Apply: one thread per wedge streams its 171 values (each
+// warp load is 32 consecutive values) and uses the symmetry.
 #include "common.cuh"
 #include "wedge.cuh"
 
@@ -33,6 +37,22 @@ int fsfs_penalty_add( const tn_mesh* m, double eps, const T* const* src, T* cons
 namespace {
 
 constexpr int kM          = 324; // entries of an 18 x 18 matrix
+constexpr int kP          = 171; // stored entries of a symmetric 18 x 18 matrix
+
+// Position of entry e of wedge w (w = 2 cell + wedge) in a stored array:
+// 32 consecutive wedges are interleaved entry by entry, so a warp with one
+// thread per wedge reads 32 consecutive values per entry.
+__device__ __forceinline__ size_t stored_pos( long long w, int e )
+{
+    return ( size_t( w >> 5 ) * 171 + e ) * 32 + size_t( w & 31 );
+}
+
+// position of entry (I, J) in the packed upper triangle
+__device__ __forceinline__ int packed( int I, int J )
+{
+    const int i = I < J ? I : J, j = I < J ? J : I;
+    return 18 * i - ( i * ( i - 1 ) ) / 2 + ( j - i );
+}
 constexpr int kGcaThreads = 352; // 11 warps, threads >= 324 only stage data
 
 // one-point kerngen geometry of wedge w of cell (d, x, y, r): physical
@@ -162,8 +182,9 @@ __global__ void __launch_bounds__( 64 ) local_matrices_kernel( int N, const doub
     __syncthreads();
     for ( int e = threadIdx.x; e < 2 * kM; e += blockDim.x )
     {
-        const int w = e / kM, J = ( e % kM ) / 18, I = ( e % kM ) % 18;
-        mats[cell * 2 * kM + e] = kerngen_entry( sg[w], skw[w], I, J );
+        const int w = e / kM, I = ( e % kM ) / 18, J = ( e % kM ) % 18;
+        if ( I <= J )
+            mats[stored_pos( cell * 2 + w, packed( I, J ) )] = kerngen_entry( sg[w], skw[w], I, J );
     }
 }
 
@@ -212,7 +233,7 @@ __global__ void __launch_bounds__( kGcaThreads ) gca_coarsen_kernel( int Nf, con
             const int       xh = 2 * xc + ( h & 1 ), yh = 2 * yc + ( ( h >> 1 ) & 1 ), rh = 2 * rc + ( h >> 2 );
             const long long cf = ( ( (long long) d * Nf + xh ) * Nf + yh ) * Nf + rh;
             if ( live )
-                sA[t] = mats_f[( cf * 2 + w ) * kM + t]; // column-major: sA[J * 18 + I] = A(I, J)
+                sA[I * 18 + J] = mats_f[stored_pos( cf * 2 + w, packed( I, J ) )];
             __syncthreads();
         }
         // T(I, J) = sum_n A(I, n + 6b) P(n, j)
@@ -221,7 +242,7 @@ __global__ void __launch_bounds__( kGcaThreads ) gca_coarsen_kernel( int Nf, con
             double v = 0.0;
             for ( int n = 0; n < 6; ++n )
             {
-                const double A = FROM_K ? kerngen_entry( sG[fw], sK[fw], I, n + 6 * b ) : sA[( n + 6 * b ) * 18 + I];
+                const double A = FROM_K ? kerngen_entry( sG[fw], sK[fw], I, n + 6 * b ) : sA[I * 18 + n + 6 * b];
                 v += A * sP[fw][n][j];
             }
             sT[I * 18 + J] = v;
@@ -240,10 +261,10 @@ __global__ void __launch_bounds__( kGcaThreads ) gca_coarsen_kernel( int Nf, con
         }
         __syncthreads();
     }
-    if ( live )
+    if ( live && I <= J )
     {
-        mats_c[( cell * 2 + 0 ) * kM + J * 18 + I] = acc0;
-        mats_c[( cell * 2 + 1 ) * kM + J * 18 + I] = acc1;
+        mats_c[stored_pos( cell * 2 + 0, packed( I, J ) )] = acc0;
+        mats_c[stored_pos( cell * 2 + 1, packed( I, J ) )] = acc1;
     }
 }
 
@@ -258,18 +279,16 @@ struct StoredParams
     int             bc_cmb, bc_surf, diag;
 };
 
-// One warp per wedge, lanes 0..17 own the rows (node = lane % 6, dim = lane / 6).
-template < typename T >
+// One thread per wedge (w = 2 cell + wedge).  The 171 stored values stream
+// in with compile-time offsets (fully unrolled), each contributing to rows I
+// and J by symmetry; the boundary treatment follows the slow path.
+template < typename T, bool DIAG >
 __global__ void __launch_bounds__( 128 ) stored_apply_kernel( StoredParams< T > P )
 {
-    __shared__ T    s_src[4][18], s_sp[4][18], s_y[4][18];
-    __shared__ T    s_n[4][3][3];
-    const int       lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-    const long long gw   = ( blockIdx.x * (long long) blockDim.x + threadIdx.x ) >> 5;
+    const long long gw = blockIdx.x * (long long) blockDim.x + threadIdx.x;
     const int       N = P.N, n1 = P.n1;
-    const long long cells = (long long) kDiamonds * N * N * N;
-    if ( gw >= 2 * cells )
-        return; // whole warp
+    if ( gw >= 2LL * kDiamonds * N * N * N )
+        return;
     const long long cell = gw >> 1;
     const int       w    = int( gw & 1 );
     const int r = int( cell % N ), y = int( ( cell / N ) % N ), x = int( ( cell / ( (long long) N * N ) ) % N );
@@ -277,103 +296,175 @@ __global__ void __launch_bounds__( 128 ) stored_apply_kernel( StoredParams< T > 
     const bool at_cmb = r == 0, at_surf = r == N - 1;
     const int  bcf    = at_cmb ? P.bc_cmb : ( at_surf ? P.bc_surf : TN_BC_NEUMANN );
     const int  boff   = at_cmb ? 0 : 3; // boundary-side local nodes boff..boff+2
-    const T*   M      = P.mats + ( cell * 2 + w ) * kM;
+    const bool dir = bcf == TN_BC_DIRICHLET, fs = bcf == TN_BC_FREESLIP;
 
-    const int    node = lane % 6, a = lane / 6;
-    const bool   row  = lane < 18;
-    const bool   bnd_node = bcf != TN_BC_NEUMANN && node >= boff && node < boff + 3;
-    size_t       idx  = 0;
-    if ( row )
+    size_t idx[6];
+    T      s[18], nrm[3][3], sn[3] = { 0, 0, 0 };
+    bool   bn[6];
+#pragma unroll
+    for ( int n = 0; n < 6; ++n )
     {
-        idx              = lat_index( n1, d, x + kWedgeNode[w][node][0], y + kWedgeNode[w][node][1] ) * n1 + r +
-              kWedgeNode[w][node][2];
-        s_src[wl][lane] = P.src.p[a][idx];
+        const size_t lat = lat_index( n1, d, x + kWedgeNode[w][n][0], y + kWedgeNode[w][n][1] );
+        idx[n]           = lat * n1 + r + kWedgeNode[w][n][2];
+        bn[n]            = bcf != TN_BC_NEUMANN && n >= boff && n < boff + 3;
+#pragma unroll
+        for ( int a = 0; a < 3; ++a )
+            s[n + 6 * a] = P.src.p[a][idx[n]];
     }
-    if ( bcf == TN_BC_FREESLIP && lane < 3 )
+    if ( fs )
     {
-        const int     bn = boff + lane;
-        const double* c  = P.coords + lat_index( n1, d, x + kWedgeNode[w][bn][0], y + kWedgeNode[w][bn][1] ) * 3;
-        const double  mm = sqrt( c[0] * c[0] + c[1] * c[1] + c[2] * c[2] );
+#pragma unroll
         for ( int q = 0; q < 3; ++q )
-            s_n[wl][lane][q] = T( c[q] / mm );
-    }
-    __syncwarp();
-    // free-slip: boundary nodes enter with their tangential part
-    if ( row )
-    {
-        T v = s_src[wl][lane];
-        if ( bcf == TN_BC_FREESLIP && bnd_node )
         {
-            const T* n  = s_n[wl][node - boff];
-            const T  dt = n[0] * s_src[wl][node] + n[1] * s_src[wl][node + 6] + n[2] * s_src[wl][node + 12];
-            v -= dt * n[a];
+            const int     n  = boff + q;
+            const double* c  = P.coords + lat_index( n1, d, x + kWedgeNode[w][n][0], y + kWedgeNode[w][n][1] ) * 3;
+            const double  mm = sqrt( c[0] * c[0] + c[1] * c[1] + c[2] * c[2] );
+            for ( int a = 0; a < 3; ++a )
+                nrm[q][a] = T( c[a] / mm );
+            sn[q] = nrm[q][0] * s[n] + nrm[q][1] * s[n + 6] + nrm[q][2] * s[n + 12];
         }
-        s_sp[wl][lane] = v;
     }
-    __syncwarp();
-    T yv = T( 0 );
-    if ( row )
+    const T* gm = P.mats + ( size_t( gw >> 5 ) * kP ) * 32 + size_t( gw & 31 );
+    T        yv[18];
+#pragma unroll
+    for ( int I = 0; I < 18; ++I )
+        yv[I] = T( 0 );
+
+    if ( !DIAG )
     {
-        if ( P.diag )
+        // free-slip: boundary nodes enter with their tangential part
+        T sv[18];
+#pragma unroll
+        for ( int I = 0; I < 18; ++I )
+            sv[I] = s[I];
+        if ( fs )
         {
-            if ( bcf == TN_BC_FREESLIP && bnd_node )
+#pragma unroll
+            for ( int q = 0; q < 3; ++q )
+#pragma unroll
+                for ( int a = 0; a < 3; ++a )
+                {
+                    // boff is 0 or 3: select the node without dynamic indexing
+                    const T t0 = sv[q + 6 * a] - sn[q] * nrm[q][a], t3 = sv[q + 3 + 6 * a] - sn[q] * nrm[q][a];
+                    if ( boff == 0 )
+                        sv[q + 6 * a] = t0;
+                    else
+                        sv[q + 3 + 6 * a] = t3;
+                }
+        }
+        T ann[3] = { 0, 0, 0 };
+#pragma unroll
+        for ( int I = 0; I < 18; ++I )
+#pragma unroll
+            for ( int J = I; J < 18; ++J )
             {
-                // diagonal of R A R^T in the (n, t1, t2) basis, rotated back
+                const T   v  = gm[size_t( 18 * I - ( I * ( I - 1 ) ) / 2 + J - I ) * 32];
+                const int ni = I % 6, nj = J % 6, a = I / 6, b = J / 6;
+                bool      keep = true;
+                if ( dir )
+                    keep = ( a == b ) ? !( ni != nj && ( bn[ni] || bn[nj] ) ) : !( bn[ni] || bn[nj] );
+                if ( keep )
+                {
+                    yv[I] += v * sv[J];
+                    if ( I != J )
+                        yv[J] += v * sv[I];
+                }
+                if ( fs && ni == nj && bn[ni] )
+                {
+                    // (n^T A_nn n) of boundary node ni, both triangles
+                    const int q   = ni - boff;
+                    const T   f   = ( I == J ? T( 1 ) : T( 2 ) ) * v;
+                    const T   nab = q == 0 ? nrm[0][a] * nrm[0][b] : ( q == 1 ? nrm[1][a] * nrm[1][b] : nrm[2][a] * nrm[2][b] );
+                    if ( q == 0 )
+                        ann[0] += f * nab;
+                    else if ( q == 1 )
+                        ann[1] += f * nab;
+                    else
+                        ann[2] += f * nab;
+                }
+            }
+        if ( fs )
+        {
+#pragma unroll
+            for ( int q = 0; q < 3; ++q )
+            {
+                const int n0 = q, n3 = q + 3; // candidates for boff = 0 / 3
+                T         y3[3];
+                for ( int a = 0; a < 3; ++a )
+                    y3[a] = boff == 0 ? yv[n0 + 6 * a] : yv[n3 + 6 * a];
+                const T yn = nrm[q][0] * y3[0] + nrm[q][1] * y3[1] + nrm[q][2] * y3[2];
+                for ( int a = 0; a < 3; ++a )
+                {
+                    const T v = y3[a] - yn * nrm[q][a] + ann[q] * sn[q] * nrm[q][a];
+                    if ( boff == 0 )
+                        yv[n0 + 6 * a] = v;
+                    else
+                        yv[n3 + 6 * a] = v;
+                }
+            }
+        }
+    }
+    else
+    {
+        // diagonal; free-slip boundary nodes: diagonal of R A R^T rotated back
+        T blk[3][3][3];
+#pragma unroll
+        for ( int I = 0; I < 18; ++I )
+#pragma unroll
+            for ( int J = I; J < 18; ++J )
+            {
+                const int ni = I % 6, nj = J % 6;
+                if ( ni != nj )
+                    continue;
+                const T   v = gm[size_t( 18 * I - ( I * ( I - 1 ) ) / 2 + J - I ) * 32];
+                const int a = I / 6, b = J / 6;
+                if ( I == J )
+                    yv[I] = v * s[I];
+                if ( fs )
+                {
+                    const int q = ni < 3 ? ni : ni - 3;
+                    if ( ( ni < 3 ) == ( boff == 0 ) )
+                    {
+                        blk[q][a][b] = v;
+                        blk[q][b][a] = v;
+                    }
+                }
+            }
+        if ( fs )
+        {
+#pragma unroll
+            for ( int q = 0; q < 3; ++q )
+            {
                 T R[3][3];
-                trafo_normal_tangential( s_n[wl][node - boff], R );
-                T s3[3] = { s_src[wl][node], s_src[wl][node + 6], s_src[wl][node + 12] };
-                for ( int q = 0; q < 3; ++q )
+                trafo_normal_tangential( nrm[q], R );
+                T s3[3], o3[3] = { 0, 0, 0 };
+                for ( int a = 0; a < 3; ++a )
+                    s3[a] = boff == 0 ? s[q + 6 * a] : s[q + 3 + 6 * a];
+                for ( int k = 0; k < 3; ++k )
                 {
                     T rar = T( 0 );
                     for ( int b = 0; b < 3; ++b )
                         for ( int c = 0; c < 3; ++c )
-                            rar += R[q][b] * M[( node + 6 * c ) * 18 + node + 6 * b] * R[q][c];
-                    const T rs = R[q][0] * s3[0] + R[q][1] * s3[1] + R[q][2] * s3[2];
-                    yv += R[q][a] * rar * rs;
+                            rar += R[k][b] * blk[q][b][c] * R[k][c];
+                    const T rs = R[k][0] * s3[0] + R[k][1] * s3[1] + R[k][2] * s3[2];
+                    for ( int a = 0; a < 3; ++a )
+                        o3[a] += R[k][a] * rar * rs;
+                }
+                for ( int a = 0; a < 3; ++a )
+                {
+                    if ( boff == 0 )
+                        yv[q + 6 * a] = o3[a];
+                    else
+                        yv[q + 3 + 6 * a] = o3[a];
                 }
             }
-            else
-                yv = M[lane * 18 + lane] * s_src[wl][lane];
-        }
-        else if ( bcf == TN_BC_DIRICHLET )
-        {
-            const bool bi = node >= boff && node < boff + 3;
-            for ( int J = 0; J < 18; ++J )
-            {
-                const int  nj = J % 6, b = J / 6;
-                const bool bj = nj >= boff && nj < boff + 3;
-                const bool masked = ( a == b ) ? ( node != nj && ( bi || bj ) ) : ( bi || bj );
-                if ( !masked )
-                    yv += M[J * 18 + lane] * s_src[wl][J];
-            }
-        }
-        else
-        {
-            const T* sv = bcf == TN_BC_FREESLIP ? s_sp[wl] : s_src[wl];
-            for ( int J = 0; J < 18; ++J )
-                yv += M[J * 18 + lane] * sv[J];
         }
     }
-    if ( bcf == TN_BC_FREESLIP && !P.diag )
-    {
-        // boundary rows: tangential part of (A P s) plus (n^T A_nn n)(n . s) n
-        if ( row )
-            s_y[wl][lane] = yv;
-        __syncwarp();
-        if ( row && bnd_node )
-        {
-            const T* n   = s_n[wl][node - boff];
-            const T  yn  = n[0] * s_y[wl][node] + n[1] * s_y[wl][node + 6] + n[2] * s_y[wl][node + 12];
-            const T  sn  = n[0] * s_src[wl][node] + n[1] * s_src[wl][node + 6] + n[2] * s_src[wl][node + 12];
-            T        ann = T( 0 );
-            for ( int b = 0; b < 3; ++b )
-                for ( int c = 0; c < 3; ++c )
-                    ann += n[b] * M[( node + 6 * c ) * 18 + node + 6 * b] * n[c];
-            yv = yv - yn * n[a] + ann * sn * n[a];
-        }
-    }
-    if ( row )
-        atomicAdd( P.dst.p[a] + idx, yv );
+#pragma unroll
+    for ( int n = 0; n < 6; ++n )
+#pragma unroll
+        for ( int a = 0; a < 3; ++a )
+            atomicAdd( P.dst.p[a] + idx[n], yv[n + 6 * a] );
 }
 
 __global__ void cast_array_kernel( size_t n, const double* __restrict__ src, float* __restrict__ dst )
@@ -403,8 +494,11 @@ int stored_apply( const tn_mesh* m, const T* mats, const tn_epsdivdiv_params* p,
     }
     P.N = m->N, P.n1 = m->n1, P.coords = m->d_coords, P.mats = mats;
     P.bc_cmb = p->bc_cmb, P.bc_surf = p->bc_surface, P.diag = p->diagonal != 0;
-    const long long warps = 2LL * kDiamonds * m->N * m->N * m->N;
-    stored_apply_kernel< T ><<< unsigned( ( warps * 32 + 127 ) / 128 ), 128, 0, st >>>( P );
+    const long long wedges = 2LL * kDiamonds * m->N * m->N * m->N;
+    if ( p->diagonal )
+        stored_apply_kernel< T, true ><<< unsigned( ( wedges + 127 ) / 128 ), 128, 0, st >>>( P );
+    else
+        stored_apply_kernel< T, false ><<< unsigned( ( wedges + 127 ) / 128 ), 128, 0, st >>>( P );
     TN_LAUNCH_CHECK();
     if ( !p->diagonal && p->bc_cmb == TN_BC_FREESLIP && p->bc_surface == TN_BC_FREESLIP )
     {
@@ -424,7 +518,8 @@ using namespace tn;
 extern "C" int tn_local_matrix_count( const tn_mesh* m, size_t* entries )
 {
     TN_CHECK_ARG( m && entries, "tn_local_matrix_count: null argument" );
-    *entries = size_t( kDiamonds ) * m->N * m->N * m->N * 2 * kM;
+    const size_t wedges = size_t( kDiamonds ) * m->N * m->N * m->N * 2;
+    *entries            = ( ( wedges + 31 ) / 32 ) * 32 * kP; // padded to whole groups of 32 wedges
     return TN_OK;
 }
 

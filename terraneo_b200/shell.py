@@ -166,12 +166,13 @@ def local_matrix_count(mesh):
 
 
 def kerngen_local_matrices(mesh, k=None):
-    """kerngen 18x18 wedge matrices (torch [cells, 2, 18, 18], column-major per matrix)."""
+    """kerngen 18x18 wedge matrices in the library's stored layout (packed upper triangles, 32 wedges
+    interleaved; torch FP64 vector of tn_local_matrix_count entries)."""
     out = torch.empty(local_matrix_count(mesh), dtype=torch.float64, device="cuda")
     kp = ctypes.c_void_p(k.data.data_ptr()) if k is not None else None
     C.check(C.lib().tn_kerngen_local_matrices_f64(mesh.handle, kp, ctypes.c_void_p(out.data_ptr()), _stream()),
             "kerngen_local_matrices")
-    return out.view(-1, 2, 18, 18)
+    return out
 
 
 def gca_coarsen(fine, coarse, k_fine=None, mats_fine=None, mode=0):
@@ -181,7 +182,7 @@ def gca_coarsen(fine, coarse, k_fine=None, mats_fine=None, mode=0):
     mp = ctypes.c_void_p(mats_fine.data_ptr()) if mats_fine is not None else None
     C.check(C.lib().tn_gca_coarsen_f64(fine.handle, coarse.handle, kp, mp, mode, ctypes.c_void_p(out.data_ptr()),
                                        _stream()), "gca_coarsen")
-    return out.view(-1, 2, 18, 18)
+    return out
 
 
 class StoredEpsilonDivDiv:

@@ -12,9 +12,17 @@ pytestmark = pytest.mark.gpu
 BCS = [(0, 0), (1, 1), (2, 2), (1, 2), (2, 1)]
 
 
+_IU = np.triu_indices(18)
+
+
 def _colmajor(m):
-    """oracle layout (row-major per matrix) -> the library's column-major layout"""
-    return np.ascontiguousarray(np.swapaxes(m, -1, -2))
+    """oracle layout [cells][2][18][18] -> the library's layout: packed upper triangles (171 per
+    wedge, wedge w = 2 cell + wedge) with 32 consecutive wedges interleaved entry by entry"""
+    p = m[..., _IU[0], _IU[1]].reshape(-1, 171)
+    nw = p.shape[0]
+    pad = (-nw) % 32
+    p = np.concatenate([p, np.zeros((pad, 171))])
+    return np.ascontiguousarray(p.reshape(-1, 32, 171).transpose(0, 2, 1)).reshape(-1)
 
 
 @pytest.fixture(scope="module")
@@ -32,7 +40,7 @@ def level3():
 def test_local_matrices_match_oracle(level3):
     from terraneo_b200 import shell
     of, oc, pf, pc, k, kv = level3
-    m = shell.kerngen_local_matrices(pf, kv).cpu().numpy()
+    m = shell.kerngen_local_matrices(pf, kv).cpu().numpy().reshape(-1)
     assert rel(m, _colmajor(of.local_matrices(k))) <= 1e-13
 
 
@@ -55,12 +63,12 @@ def test_stored_apply_with_kerngen_matrices_equals_kerngen_apply(level3, bc, dia
 def test_gca_coarsening_matches_oracle(level3, mode):
     from terraneo_b200 import shell
     of, oc, pf, pc, k, kv = level3
-    mk = shell.gca_coarsen(pf, pc, k_fine=kv, mode=mode).cpu().numpy()
+    mk = shell.gca_coarsen(pf, pc, k_fine=kv, mode=mode).cpu().numpy().reshape(-1)
     ref = _colmajor(of.gca_coarsen(oc, k=k, mode=mode))
     assert rel(mk, ref) <= 1e-13
     # from stored fine matrices gives the same
     mf = shell.kerngen_local_matrices(pf, kv)
-    ms = shell.gca_coarsen(pf, pc, mats_fine=mf.reshape(-1), mode=mode).cpu().numpy()
+    ms = shell.gca_coarsen(pf, pc, mats_fine=mf.reshape(-1), mode=mode).cpu().numpy().reshape(-1)
     assert rel(ms, mk) <= 1e-14
 
 
@@ -90,7 +98,7 @@ def test_gca_two_levels_and_fp32(level3):
     m3 = shell.gca_coarsen(p4, p3, k_fine=kv)
     m2 = shell.gca_coarsen(p3, p2, mats_fine=m3.reshape(-1))
     ref2 = o3.gca_coarsen(o2, mats_fine=o4.gca_coarsen(o3, k=k))
-    assert rel(m2.cpu().numpy(), _colmajor(ref2)) <= 1e-13
+    assert rel(m2.cpu().numpy().reshape(-1), _colmajor(ref2)) <= 1e-13
     m2f = torch.empty(m2.numel(), dtype=torch.float32, device="cuda")
     C.check(C.lib().tn_array_cast_f64_to_f32(m2.numel(), m2.data_ptr(), m2f.data_ptr(), None), "cast")
     u = random_vector(o2, seed=5)
