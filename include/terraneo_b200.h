@@ -137,6 +137,18 @@ TN_API int tn_stored_epsdivdiv_apply_f32( const tn_mesh* mesh, const float* mats
 /* dst[i] = (float) src[i], i < n (FP32 copies of stored matrices) */
 TN_API int tn_array_cast_f64_to_f32( size_t n, const double* src, float* dst, void* stream );
 
+/* EpsilonDivDiv::apply_impl (fe/wedge/operators/shell/epsilon_divdiv.hpp:218-600):
+ * the same form as the kerngen operator with the 3x2 Felippa rule and k
+ * interpolated by the shape functions at each quadrature point;
+ * treat_boundary eliminates the CMB nodes of layer 0 (else the SURFACE nodes
+ * of layer N-1) keeping their diagonal; diagonal != 0 keeps the diagonal only. */
+TN_API int tn_epsdivdiv3x2_apply_f64( const tn_mesh* mesh, const double* k, int treat_boundary, int diagonal,
+                                      int apply_mode, int comm_mode, const double* const* src, double* const* dst,
+                                      void* stream );
+TN_API int tn_epsdivdiv3x2_apply_f32( const tn_mesh* mesh, const float* k, int treat_boundary, int diagonal,
+                                      int apply_mode, int comm_mode, const float* const* src, float* const* dst,
+                                      void* stream );
+
 /* ---------------------------------------------------------------------------
  * Laplace::apply_impl (fe/wedge/operators/shell/laplace.hpp:68): int grad u . grad v,
  * 3x2 Felippa quadrature; treat_boundary != 0 eliminates the CMB/SURFACE
@@ -290,6 +302,16 @@ TN_API int tn_vec_mult_f32( const tn_mesh* mesh, int ncomp, float* const* y, con
 TN_API int tn_vec_max_abs_f64( const tn_mesh* mesh, int ncomp, const double* const* x, double* result, void* stream );
 TN_API int tn_vec_has_nan_or_inf_f64( const tn_mesh* mesh, int ncomp, const double* const* x, int* result, void* stream );
 TN_API int tn_vec_has_nan_or_inf_f32( const tn_mesh* mesh, int ncomp, const float* const* x, int* result, void* stream );
+/* assign_masked_else_keep_old (kernels/common/grid_operations.hpp) with the
+ * CMB / SURFACE boundary flags: on the radial boundary layers selected by cmb
+ * (r = 0) and surface (r = N), y = x, or the constant c when x is NULL; other
+ * nodes keep their values.  The strong Dirichlet enforcement of
+ * fe/strong_algebraic_dirichlet_enforcement.hpp is b -= A_neumann g followed by
+ * this assign with x = diag(A_neumann) g (or c = 0, homogeneous). */
+TN_API int tn_vec_assign_boundary_f64( const tn_mesh* mesh, int ncomp, double* const* y, const double* const* x,
+                                       double c, int cmb, int surface, void* stream );
+TN_API int tn_vec_assign_boundary_f32( const tn_mesh* mesh, int ncomp, float* const* y, const float* const* x,
+                                       double c, int cmb, int surface, void* stream );
 /* One fused Chebyshev step (linalg/solvers/chebyshev.hpp:127-160):
  * d = alpha D^{-1} (b - ax) + beta d;  x = x + d.  beta = 0 does not read d. */
 TN_API int tn_vec_chebyshev_step_f64( const tn_mesh* mesh, int ncomp, double* const* x, double* const* d,

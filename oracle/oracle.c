@@ -1940,3 +1940,93 @@ void or_fct_step( int L, const double* coords, const double* radii, const double
     free( Rp );
     free( Rm );
 }
+
+/* ------------------------------------------------------------------------ */
+/* EpsilonDivDiv with the 3x2 Felippa rule (epsilon_divdiv.hpp:218-600):     */
+/* int k (2 eps(u):eps(v) - 2/3 div u div v), k interpolated by the wedge    */
+/* shape functions at every quadrature point; treat_boundary eliminates the  */
+/* CMB nodes of layer 0 (else the SURFACE nodes of layer N-1) keeping their  */
+/* diagonal; diagonal mode keeps only the diagonal.                          */
+/* ------------------------------------------------------------------------ */
+
+void or_epsdivdiv3x2_apply( int L, const double* coords, const double* radii, const double* k, const double* src,
+                            double* dst, int treat_boundary, int diag )
+{
+    const int    N = 1 << L, n1 = N + 1;
+    const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1;
+    memset( dst, 0, sizeof( double ) * 3 * ns );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                {
+                    const int bot = treat_boundary && r == 0;
+                    const int top = treat_boundary && !bot && r == N - 1;
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const double* p[3];
+                        wedge_lateral_points( n1, coords, d, x, y, w, p );
+                        size_t idx[6];
+                        double s[6][3], kv[6], out[6][3];
+                        memset( out, 0, sizeof( out ) );
+                        for ( int n = 0; n < 6; ++n )
+                        {
+                            idx[n] = node_idx( n1, d, x + WNODE[w][n][0], y + WNODE[w][n][1], r + WNODE[w][n][2] );
+                            kv[n]  = k[idx[n]];
+                            for ( int c = 0; c < 3; ++c )
+                                s[n][c] = src[c * ns + idx[n]];
+                        }
+                        int coupled[6];
+                        for ( int n = 0; n < 6; ++n )
+                            coupled[n] = !diag && !( bot && n < 3 ) && !( top && n >= 3 );
+                        for ( int q = 0; q < 6; ++q )
+                        {
+                            double J[3][3], IT[3][3], g[6][3];
+                            wedge_jac( p, radii[d * n1 + r], radii[d * n1 + r + 1], QP32[q][0], QP32[q][1], QP32[q][2], J );
+                            const double det = det3( J );
+                            inv_transposed3( J, det, IT );
+                            double ke = 0.0;
+                            for ( int n = 0; n < 6; ++n )
+                            {
+                                double gr[3];
+                                grad_shape_ref( n, QP32[q][0], QP32[q][1], QP32[q][2], gr );
+                                for ( int a = 0; a < 3; ++a )
+                                    g[n][a] = IT[a][0] * gr[0] + IT[a][1] * gr[1] + IT[a][2] * gr[2];
+                                ke += shape_ref( n, QP32[q][0], QP32[q][1], QP32[q][2] ) * kv[n];
+                            }
+                            const double wk = QW32 * ke * fabs( det );
+                            /* coupled part: grad u over coupled nodes, tested by coupled nodes */
+                            double G[3][3] = { { 0 } };
+                            for ( int n = 0; n < 6; ++n )
+                                if ( coupled[n] )
+                                    for ( int a = 0; a < 3; ++a )
+                                        for ( int b = 0; b < 3; ++b )
+                                            G[a][b] += g[n][a] * s[n][b];
+                            const double div = G[0][0] + G[1][1] + G[2][2];
+                            for ( int n = 0; n < 6; ++n )
+                            {
+                                if ( coupled[n] )
+                                    for ( int c = 0; c < 3; ++c )
+                                    {
+                                        double e = 0.0;
+                                        for ( int a = 0; a < 3; ++a )
+                                            e += g[n][a] * ( G[a][c] + G[c][a] );
+                                        out[n][c] += wk * ( e - 2.0 / 3.0 * g[n][c] * div );
+                                    }
+                                else
+                                {
+                                    /* uncoupled (boundary or diagonal mode): the node's own diagonal */
+                                    const double gg = g[n][0] * g[n][0] + g[n][1] * g[n][1] + g[n][2] * g[n][2];
+                                    for ( int c = 0; c < 3; ++c )
+                                        out[n][c] += wk * s[n][c] * ( gg + g[n][c] * g[n][c] / 3.0 );
+                                }
+                            }
+                        }
+                        for ( int n = 0; n < 6; ++n )
+                            for ( int c = 0; c < 3; ++c )
+                                dst[c * ns + idx[n]] += out[n][c];
+                    }
+                }
+    or_halo_sum( L, coords, dst, 3 );
+}
+

@@ -40,6 +40,9 @@ void or_kerngen_apply( int L, const double* coords, const double* radii, const d
 void or_laplace_apply( int L, const double* coords, const double* radii, const double* src, double* dst,
                        int treat_boundary, int diag );
 
+/* EpsilonDivDiv, 3x2 rule, k interpolated; Dirichlet elimination on both radii */
+void or_epsdivdiv3x2_apply( int L, const double* coords, const double* radii, const double* k, const double* src,
+                            double* dst, int treat_boundary, int diag );
 /* DivKGrad: int k grad u . grad v, k interpolated at the quadrature points;
  * single_quadpoint selects the 1-point rule */
 void or_divkgrad_apply( int L, const double* coords, const double* radii, const double* k, const double* src,

@@ -20,6 +20,7 @@
 //   prolong / restrict Lf rmin rmax DIR    constant vector transfer between Lf-1 and Lf
 //   kmass   L rmin rmax mode DIR          KMass<double> (0 full, 1 diagonal, 2 lumped)
 //   divkgrad L rmin rmax treat diag single DIR   DivKGrad<double> (k.bin, src.bin)
+//   epsdivdiv L rmin rmax treat diag DIR   EpsilonDivDiv<double> (3x2 rule; k.bin, src.bin)
 //   prolong_linear / restrict_linear Lf rmin rmax DIR  scalar linear transfer between Lf-1 and Lf
 //   fct L rmin rmax dt kappa bc DIR  one fct_explicit_step on vel.bin (FE vector), T.bin and src.bin (FV
 //                                    fields with ghosts); bc 1: Dirichlet T_cmb = 1, T_surface = 0 on T before
@@ -37,6 +38,7 @@
 #include <vector>
 
 #include "communication/shell/communication.hpp"
+#include "fe/wedge/operators/shell/epsilon_divdiv.hpp"
 #include "fe/wedge/operators/shell/epsilon_divdiv_kerngen.hpp"
 #include "fe/wedge/operators/shell/div_k_grad.hpp"
 #include "fe/wedge/operators/shell/divergence.hpp"
@@ -366,6 +368,20 @@ int cmd_gca( int L, double rmin, double rmax, int bcc, int bcs, int diag, int mo
     return 0;
 }
 
+int cmd_epsdivdiv( int L, double rmin, double rmax, int treat, int diag, const std::string& dir )
+{
+    Setup                            s( L, rmin, rmax );
+    linalg::VectorQ1Scalar< double > k( "k", s.domain, s.omask );
+    view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", s.nodes ).data() );
+    linalg::VectorQ1Vec< double > src( "src", s.domain, s.omask ), dst( "dst", s.domain, s.omask );
+    load_vec( src, dir + "/src.bin", s.nodes );
+    fe::wedge::operators::shell::EpsilonDivDiv< double > op( s.domain, s.coords, s.radii, s.bmask, k.grid_data(),
+                                                             treat != 0, diag != 0 );
+    linalg::apply( op, src, dst );
+    save_vec( dst, dir + "/dst.bin", s.nodes );
+    return 0;
+}
+
 int cmd_divkgrad( int L, double rmin, double rmax, int treat, int diag, int single, const std::string& dir )
 {
     Setup                            s( L, rmin, rmax );
@@ -425,6 +441,8 @@ int main( int argc, char** argv )
         return cmd_fct( I( 2 ), D( 3 ), D( 4 ), D( 5 ), D( 6 ), I( 7 ), argv[8] );
     if ( cmd == "gca" && argc == 10 )
         return cmd_gca( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), I( 8 ), argv[9] );
+    if ( cmd == "epsdivdiv" && argc == 8 )
+        return cmd_epsdivdiv( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     if ( cmd == "divkgrad" && argc == 9 )
         return cmd_divkgrad( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( cmd == "vlaplace" && argc == 9 )

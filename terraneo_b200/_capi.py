@@ -120,6 +120,10 @@ _SIGS = {
     "tn_fct_apply_dirichlet_f64": (c_int, [c_void_p, c_void_p, P(FCTDirichlet), c_void_p]),
     "tn_fct_step_f64": (c_int, [c_void_p, c_void_p, P(c_void_p), P(c_void_p), c_double, c_double, c_void_p, c_int,
                                 P(FCTDirichlet), c_void_p, c_void_p]),
+    "tn_epsdivdiv3x2_apply_f64": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, P(c_void_p), P(c_void_p),
+                                          c_void_p]),
+    "tn_epsdivdiv3x2_apply_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, P(c_void_p), P(c_void_p),
+                                          c_void_p]),
     "tn_laplace_pcg_solve_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, P(c_int),
                                          P(c_double)]),
     "tn_stokes_solver_create": (c_int, [P(StokesParams), c_double, c_double, c_void_p, P(c_void_p)]),
@@ -139,6 +143,10 @@ _SIGS = {
     "tn_vec_has_nan_or_inf_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), c_void_p]),
     "tn_vec_has_nan_or_inf_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), c_void_p]),
     "tn_vec_dot_noalloc_f64": (c_int, [c_size_t, c_int, P(c_void_p), P(c_void_p), c_void_p, P(c_double), c_void_p]),
+    "tn_vec_assign_boundary_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_double, c_int, c_int,
+                                           c_void_p]),
+    "tn_vec_assign_boundary_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_double, c_int, c_int,
+                                           c_void_p]),
     "tn_vec_chebyshev_step_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_void_p), P(c_void_p),
                                           P(c_void_p), c_double, c_double, c_void_p]),
     "tn_vec_chebyshev_step_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_void_p), P(c_void_p),

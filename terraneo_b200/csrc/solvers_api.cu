@@ -13,6 +13,7 @@
 #include <functional>
 #include <memory>
 
+#include "../cpp/tn/enforcement.hpp"
 #include "../cpp/tn/solvers.hpp"
 #include "common.cuh"
 

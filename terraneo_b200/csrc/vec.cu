@@ -343,6 +343,53 @@ extern "C" int tn_vec_has_nan_or_inf_f32( const tn_mesh* m, int ncomp, const flo
 {
     return has_nan< float >( m, ncomp, x, r, s );
 }
+// assign_masked_else_keep_old (grid_operations.hpp) on the radial boundary
+// layers: y = x (or the constant c when x is NULL) at r = 0 (cmb) and r = N
+// (surface), unchanged elsewhere; thread per (lateral node, side), blockIdx.y
+// = component.
+template < typename T >
+__global__ void assign_boundary_kernel( size_t nlat, int n1, Ptr3< T > y, Ptr3< const T > x, T c, int cmb, int surf )
+{
+    const size_t t = blockIdx.x * size_t( blockDim.x ) + threadIdx.x;
+    if ( t >= 2 * nlat )
+        return;
+    const int side = int( t / nlat );
+    if ( ( side == 0 && !cmb ) || ( side == 1 && !surf ) )
+        return;
+    const size_t i = ( t % nlat ) * n1 + ( side == 0 ? 0 : n1 - 1 );
+    const int    k = blockIdx.y;
+    y.p[k][i]      = x.p[k] ? x.p[k][i] : c;
+}
+
+template < typename T >
+static int assign_boundary( const tn_mesh* m, int ncomp, T* const* y, const T* const* x, double c, int cmb, int surf,
+                            void* s )
+{
+    TN_CHECK_ARG( m, "assign_boundary: mesh is NULL" );
+    Ptr3< T >       py;
+    Ptr3< const T > px{};
+    int             rc;
+    if ( ( rc = ptr3( ncomp, y, py, "assign_boundary" ) ) )
+        return rc;
+    if ( x && ( rc = ptr3c( ncomp, x, px, "assign_boundary" ) ) )
+        return rc;
+    const size_t n = 2 * m->nlat;
+    assign_boundary_kernel< T ><<< dim3( unsigned( ( n + 255 ) / 256 ), ncomp ), 256, 0, as_stream( s ) >>>(
+        m->nlat, m->n1, py, px, T( c ), cmb, surf );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+extern "C" int tn_vec_assign_boundary_f64( const tn_mesh* m, int ncomp, double* const* y, const double* const* x,
+                                           double c, int cmb, int surface, void* s )
+{
+    return assign_boundary< double >( m, ncomp, y, x, c, cmb, surface, s );
+}
+extern "C" int tn_vec_assign_boundary_f32( const tn_mesh* m, int ncomp, float* const* y, const float* const* x,
+                                           double c, int cmb, int surface, void* s )
+{
+    return assign_boundary< float >( m, ncomp, y, x, c, cmb, surface, s );
+}
+
 template < typename T >
 static int chebyshev_step( const tn_mesh* m, int ncomp, T* const* x, T* const* d, const T* const* b, const T* const* ax,
                            const T* const* inv_diag, double alpha, double beta, void* s )

@@ -215,6 +215,22 @@ class Laplace:
                   ctypes.c_void_p(dst.data.data_ptr()), _stream()), "laplace_apply")
 
 
+class EpsilonDivDiv:
+    """EpsilonDivDiv (fe/wedge/operators/shell/epsilon_divdiv.hpp:18): 3x2 rule, k interpolated, Dirichlet radii."""
+
+    def __init__(self, mesh, k, treat_boundary, diagonal=False, apply_mode=C.APPLY_REPLACE, comm_mode=C.COMM_ADDITIVE):
+        self.mesh, self.k = mesh, k
+        self.treat, self.diag, self.am, self.cm = int(treat_boundary), int(diagonal), apply_mode, comm_mode
+
+    def set_diagonal(self, v):
+        self.diag = int(v)
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_epsdivdiv3x2_apply_{src.tag}")
+        C.check(f(self.mesh.handle, ctypes.c_void_p(self.k.data.data_ptr()), self.treat, self.diag, self.am, self.cm,
+                  src.comp_ptrs(), dst.comp_ptrs(), _stream()), "epsdivdiv3x2_apply")
+
+
 class DivKGrad:
     """DivKGrad (fe/wedge/operators/shell/div_k_grad.hpp:18): int k grad u . grad v."""
 
@@ -480,6 +496,22 @@ class FCTAdvectionDiffusion:
     @property
     def T_L(self):
         return self.work[:self.centers[0].numel()].view(self.fv_shape)
+
+
+def assign_boundary(y, x=None, c=0.0, cmb=True, surface=True):
+    """y = x (or c) on the CMB / SURFACE layers (assign_masked_else_keep_old with the boundary flags)."""
+    f = getattr(C.lib(), f"tn_vec_assign_boundary_{y.tag}")
+    C.check(f(y.mesh.handle, y.ncomp, y.comp_ptrs(), x.comp_ptrs() if x is not None else None, float(c), int(cmb),
+              int(surface), _stream()), "assign_boundary")
+
+
+def strong_algebraic_dirichlet_enforcement(A_neumann, A_neumann_diag, g, tmp, b, cmb=True, surface=True):
+    """b <- b - A_N g; b <- diag(A_N) g on the Dirichlet layers
+    (fe/strong_algebraic_dirichlet_enforcement.hpp:10-45)."""
+    apply(A_neumann, g, tmp)
+    lincomb(b, [1.0, -1.0], [b, tmp])
+    apply(A_neumann_diag, g, tmp)
+    assign_boundary(b, tmp, 0.0, cmb, surface)
 
 
 def freeslip_project(u, cmb=True, surface=True):

@@ -28,6 +28,7 @@ LAPLACE_CASES = [(1, 0), (0, 0), (1, 1)]
 STOKES_BCS = [(1, 1), (2, 2), (0, 0)]
 KMASS_MODES = [0, 1, 2]
 DIVKGRAD_CASES = [(1, 0, 0), (0, 0, 0), (1, 1, 0), (1, 0, 1)]
+EPSDIVDIV_CASES = [(1, 0), (0, 0), (1, 1)]
 VLAPLACE_CASES = [(1, 1, 0), (0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 1)]
 
 
@@ -121,6 +122,11 @@ def main():
         for mode in KMASS_MODES:
             run_ref(["kmass", L, R_MIN, R_MAX, mode, d], d)
             out[f"kmass_{mode}"] = np.fromfile(f"{d}/dst.bin").reshape(fine.shape)
+        x["u"].tofile(f"{d}/src.bin")
+        for treat, diag in EPSDIVDIV_CASES:
+            run_ref(["epsdivdiv", L, R_MIN, R_MAX, treat, diag, d], d)
+            out[f"epsdivdiv_{treat}{diag}"] = np.fromfile(f"{d}/dst.bin").reshape((3,) + fine.shape)
+        x["s"].tofile(f"{d}/src.bin")
         for treat, diag, single in DIVKGRAD_CASES:
             run_ref(["divkgrad", L, R_MIN, R_MAX, treat, diag, single, d], d)
             out[f"divkgrad_{treat}{diag}{single}"] = np.fromfile(f"{d}/dst.bin").reshape(fine.shape)

@@ -35,6 +35,7 @@ def lib():
         L.or_laplace_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
         L.or_divergence_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
         L.or_gradient_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
+        L.or_epsdivdiv3x2_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
         L.or_divkgrad_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.or_vector_laplace_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.or_vector_laplace_apply.restype = ctypes.c_int
@@ -111,6 +112,13 @@ class Mesh:
         src = np.ascontiguousarray(src, dtype=np.float64)
         lib().or_laplace_apply(self.L, _p(self.coords), _p(self.radii), _p(src), _p(dst),
                                int(treat_boundary), int(diag))
+        return dst
+
+    def epsdivdiv3x2(self, k, src, treat_boundary=True, diag=False):
+        dst = np.zeros((3,) + self.shape)
+        lib().or_epsdivdiv3x2_apply(self.L, _p(self.coords), _p(self.radii), _p(np.ascontiguousarray(k, dtype=np.float64)),
+                                    _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst), int(treat_boundary),
+                                    int(diag))
         return dst
 
     def divkgrad(self, k, src, treat_boundary=True, diag=False, single=False):

@@ -84,3 +84,34 @@ def test_epsdivdiv_add_mode_and_skip_comm(setup):
     # (base + A_local u) summed over copies = halo(base) + A u
     ref = om.halo_sum(base) + om.kerngen(k, u, 1, 1, False)
     assert rel(dst.numpy(), ref) <= 1e-12
+
+
+@pytest.mark.parametrize("L", [2, 3, 4])
+@pytest.mark.parametrize("treat,diag", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_epsdivdiv3x2_f64(L, treat, diag):
+    """EpsilonDivDiv with the 3x2 rule against the oracle (pinned to the reference)."""
+    from terraneo_b200 import shell
+    from helpers import random_vector, rel, viscosity_field
+    om, pm = Mesh(L), shell.ShellMesh(L)
+    k = viscosity_field(om, seed=L, contrast=1e3)
+    u = random_vector(om, seed=60 + L)
+    kv, src, dst = shell.VectorQ1Scalar(pm), shell.VectorQ1Vec(pm), shell.VectorQ1Vec(pm)
+    kv.set_numpy(k)
+    src.set_numpy(u)
+    shell.apply(shell.EpsilonDivDiv(pm, kv, treat, diag), src, dst)
+    assert rel(dst.numpy(), om.epsdivdiv3x2(k, u, treat, diag)) <= 1e-12
+
+
+def test_epsdivdiv3x2_f32():
+    from terraneo_b200 import shell
+    from helpers import random_vector, rel, viscosity_field
+    L = 3
+    om, pm = Mesh(L), shell.ShellMesh(L)
+    k = viscosity_field(om, seed=1, contrast=1e3)
+    u = random_vector(om, seed=61)
+    kv, src, dst = (shell.VectorQ1Scalar(pm, torch.float32), shell.VectorQ1Vec(pm, torch.float32),
+                    shell.VectorQ1Vec(pm, torch.float32))
+    kv.set_numpy(k)
+    src.set_numpy(u)
+    shell.apply(shell.EpsilonDivDiv(pm, kv, 1), src, dst)
+    assert rel(dst.numpy().astype(float), om.epsdivdiv3x2(k, u, 1, 0)) <= 1e-5

@@ -85,3 +85,26 @@ def test_vector_laplace_f32_and_rejects_freeslip():
     assert rel(dst.numpy().astype(float), om.vector_laplace(u, 1, 1)) <= 1e-5
     with pytest.raises(RuntimeError):
         shell.apply(shell.VectorLaplace(pm, C.BC_FREESLIP, 1), src, dst)
+
+
+def test_strong_dirichlet_enforcement_matches_oracle_composition():
+    """b - A_N g with diag(A_N) g on the boundary layers (Laplace, inhomogeneous g)."""
+    from terraneo_b200 import shell
+    L = 3
+    om, pm = Mesh(L), shell.ShellMesh(L)
+    b = random_vector(om, seed=70, ncomp=1)
+    g = random_vector(om, seed=71, ncomp=1)
+    vb, vg, tmp = shell.VectorQ1Scalar(pm), shell.VectorQ1Scalar(pm), shell.VectorQ1Scalar(pm)
+    vb.set_numpy(b)
+    vg.set_numpy(g)
+    shell.strong_algebraic_dirichlet_enforcement(shell.Laplace(pm, False), shell.Laplace(pm, False, True), vg, tmp, vb)
+    ref = b - om.laplace(g, 0, 0)
+    dg = om.laplace(g, 0, 1)
+    ref[om.bmask != 1] = dg[om.bmask != 1]
+    assert rel(vb.numpy()[0], ref) <= 1e-13
+    # homogeneous, surface only
+    vb.set_numpy(b)
+    shell.assign_boundary(vb, None, 0.0, cmb=False, surface=True)
+    ref = b.copy()
+    ref[:, :, :, -1] = 0.0
+    assert np.array_equal(vb.numpy()[0], ref)

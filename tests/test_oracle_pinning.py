@@ -83,6 +83,12 @@ def test_kmass_matches_reference(case, mode):
     assert rel(fine.kmass(x["k"], x["s"], mode), g[f"kmass_{mode}"]) <= TOL
 
 
+@pytest.mark.parametrize("treat,diag", G.EPSDIVDIV_CASES)
+def test_epsdivdiv3x2_matches_reference(case, treat, diag):
+    g, fine, _, x = case
+    assert rel(fine.epsdivdiv3x2(x["k"], x["u"], treat, diag), g[f"epsdivdiv_{treat}{diag}"]) <= TOL
+
+
 @pytest.mark.parametrize("treat,diag,single", G.DIVKGRAD_CASES)
 def test_divkgrad_matches_reference(case, treat, diag, single):
     g, fine, _, x = case
