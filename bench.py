@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-laplace-cg", action="store_true", help="skip the level-5 Laplace CG leg")
     ap.add_argument("--no-stokes", action="store_true", help="skip the level-6 Stokes time-to-1e-8 leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the level-5 adjoint viscosity gradient leg")
     ap.add_argument("--no-timestep", action="store_true", help="skip the level-7 mantle-circulation time-step leg")
@@ -96,6 +97,77 @@ def stokes_rhs(shell, mesh, coords, radii, seed=2025):
         f.data[c].copy_(out.data[0])
     shell.freeslip_project(f, True, True)
     return f
+
+
+def sh_rhs(coords, radii, seed, lmax=8):
+    """f(x) = sum_{l<=lmax, |m|<=l} a_lm Y_lm(x/|x|) (r - r_min)(r_max - r), a_lm ~ N(0,1) seeded,
+    Y_lm the orthonormal real spherical harmonics."""
+    from scipy.special import sph_harm_y
+    rng = np.random.default_rng(seed)
+    u = coords / np.linalg.norm(coords, axis=-1, keepdims=True)
+    theta, phi = np.arccos(np.clip(u[..., 2], -1, 1)), np.arctan2(u[..., 1], u[..., 0])
+    ang = np.zeros(coords.shape[:-1])
+    for l in range(lmax + 1):
+        for m in range(-l, l + 1):
+            y = sph_harm_y(l, abs(m), theta, phi)
+            if m > 0:
+                y = np.sqrt(2) * (-1) ** m * y.real
+            elif m < 0:
+                y = np.sqrt(2) * (-1) ** m * y.imag
+            else:
+                y = y.real
+            ang += rng.normal() * y
+    return ang[:, :, :, None] * ((radii - RMIN) * (RMAX - radii))[:, None, None, :]
+
+
+def laplace_cg_leg(shell, torch, level=5, seed=2026, reference=True):
+    """Plain FP64 CG on the scalar Laplace at level 5 (10 x 32^3 cells, 359,370 stored nodes),
+    homogeneous Dirichlet on both radii, b = M f with f the seeded degree-8 spherical-harmonic
+    field, from x = 0 to 1e-10 relative residual.  The reference's own Kokkos-OpenMP solver
+    (compiled from its sources) solves the same system on the host cores beside it."""
+    pm = shell.ShellMesh(level, RMIN, RMAX)
+    coords, radii = pm.geometry()
+    f = sh_rhs(coords, radii, seed)
+    vf, vb, vx = shell.VectorQ1Scalar(pm), shell.VectorQ1Scalar(pm), shell.VectorQ1Scalar(pm)
+    vf.set_numpy(f)
+    shell.apply(shell.KMass(pm, None, 0), vf, vb)
+    shell.assign_boundary(vb, None, 0.0, True, True)
+    shell.laplace_pcg(pm, vb, vx, 5000, 1e-10)  # warm-up
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    secs = []
+    for _ in range(3):
+        vx.data.zero_()
+        torch.cuda.synchronize()
+        ev0.record()
+        it, rr = shell.laplace_pcg(pm, vb, vx, 5000, 1e-10)
+        ev1.record()
+        torch.cuda.synchronize()
+        secs.append(ev0.elapsed_time(ev1) / 1e3)
+    sec = min(secs)
+    out = {"workload": f"FP64 CG, Laplace level {level} ({pm.unique_nodes:,} unique nodes), homogeneous Dirichlet "
+                       "both radii, b = M f (degree-8 spherical harmonics x (r-0.55)(1-r)), x0 = 0, to 1e-10",
+           "seconds": round(sec, 5), "iterations": it, "relres": float(f"{rr:.3e}"),
+           "apply_gdofs": round(pm.unique_nodes * it / sec / 1e9, 3)}
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
+    if reference and os.path.exists(ref):
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            vb.numpy()[0].tofile(os.path.join(d, "b.bin"))
+            env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 1), OMP_PROC_BIND="spread",
+                       OMP_PLACES="cores")
+            res = subprocess.run([ref, "laplace_cg", str(level), str(RMIN), str(RMAX), "5000", "1e-10", d], env=env,
+                                 capture_output=True, text=True, timeout=900)
+            line = [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
+            if res.returncode == 0 and line:
+                info = json.loads(line[-1])
+                xr = np.fromfile(os.path.join(d, "x.bin"))
+                xg = vx.numpy()[0].reshape(-1)
+                out["cpu_baseline"] = {"value": info["seconds"], "unit": "s", "cores": info["threads"],
+                                       "kind": "reference", "iterations": info["iterations"],
+                                       "sample": "the same solve with the reference's PCG<Laplace> (Kokkos-OpenMP)",
+                                       "solution_rel_diff": float(f"{np.linalg.norm(xg - xr) / np.linalg.norm(xr):.3e}")}
+                out["speedup_vs_cpu_reference"] = round(info["seconds"] / sec, 1)
+    return out
 
 
 def stokes_leg(shell, C, torch, k_np):
@@ -499,6 +571,8 @@ def main():
             "gpu_launches": 3 * args.steps,
             "clocks": clk.summary(),
         }
+        if world == 1 and not args.no_laplace_cg:
+            line["laplace_cg"] = laplace_cg_leg(shell, torch, reference=not args.no_cpu_baseline)
         if world == 1 and not args.no_stokes:
             line["stokes"] = stokes_leg(shell, C, torch, k_np)
         if world == 1 and not args.no_adjoint:

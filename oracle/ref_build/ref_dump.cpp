@@ -54,6 +54,8 @@
 #include "fv/hex/operators/fct_advection_diffusion.hpp"
 #include "grid/bit_masks.hpp"
 #include "linalg/solvers/gca/gca.hpp"
+#include "linalg/solvers/pcg.hpp"
+#include "util/table.hpp"
 #include "grid/shell/bit_masks.hpp"
 #include "grid/shell/spherical_shell.hpp"
 #include "linalg/vector_fv.hpp"
@@ -215,6 +217,42 @@ int cmd_laplace( int L, double rmin, double rmax, int treat, int diag, const std
     linalg::apply( op, src, dst );
     auto out = view_to_host( dst.grid_data() );
     write_file( dir + "/dst.bin", out.data(), out.size() );
+    return 0;
+}
+
+// Unpreconditioned PCG (linalg/solvers/pcg.hpp) on Laplace(treat_boundary =
+// true) from x = 0 for the right-hand side in b.bin; writes x.bin and prints
+// iterations, final relative residual ||b - A x|| / ||b||, solve seconds and
+// threads as one JSON line.
+int cmd_laplace_cg( int L, double rmin, double rmax, int maxit, double reltol, const std::string& dir )
+{
+    using V = linalg::VectorQ1Scalar< double >;
+    Setup s( L, rmin, rmax );
+    V     b( "b", s.domain, s.omask ), x( "x", s.domain, s.omask ), r( "r", s.domain, s.omask );
+    std::vector< V > tmps;
+    for ( int i = 0; i < 4; ++i )
+        tmps.emplace_back( "tmp" + std::to_string( i ), s.domain, s.omask );
+    view_from_host( b.grid_data(), read_file< double >( dir + "/b.bin", s.nodes ).data() );
+    linalg::assign( x, 0.0 );
+    using Lap = fe::wedge::operators::shell::Laplace< double >;
+    Lap  A( s.domain, s.coords, s.radii, s.bmask, true, false );
+    auto table = std::make_shared< util::Table >();
+    linalg::solvers::PCG< Lap > pcg( linalg::solvers::IterativeSolverParameters{ maxit, reltol, 1e-30 }, table, tmps );
+    Kokkos::fence();
+    auto t0 = std::chrono::steady_clock::now();
+    linalg::solvers::solve( pcg, A, x, b );
+    Kokkos::fence();
+    const double sec = std::chrono::duration< double >( std::chrono::steady_clock::now() - t0 ).count();
+    linalg::apply( A, x, r );
+    linalg::lincomb( r, { 1.0, -1.0 }, { b, r } );
+    const double rel = std::sqrt( linalg::dot( r, r ) / linalg::dot( b, b ) );
+    auto         out = view_to_host( x.grid_data() );
+    write_file( dir + "/x.bin", out.data(), out.size() );
+    std::printf( "{\"iterations\": %zu, \"relres\": %.6e, \"seconds\": %.9g, \"threads\": %d}\n",
+                 table->rows().size() - 1,
+                 rel,
+                 sec,
+                 Kokkos::DefaultExecutionSpace().concurrency() );
     return 0;
 }
 
@@ -447,6 +485,8 @@ int main( int argc, char** argv )
         return cmd_divkgrad( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( cmd == "vlaplace" && argc == 9 )
         return cmd_vlaplace( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
+    if ( cmd == "laplace_cg" && argc == 8 )
+        return cmd_laplace_cg( I( 2 ), D( 3 ), D( 4 ), I( 5 ), D( 6 ), argv[7] );
     if ( cmd == "laplace" && argc == 8 )
         return cmd_laplace( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     std::fprintf( stderr, "ref_dump: bad command line\n" );

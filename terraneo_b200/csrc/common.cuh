@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -89,6 +90,11 @@ struct tn_mesh
     // (diamond, x, y) FV cell across the face of ghost cell i on side
     // (x = 0, x = N+1, y = 0, y = N+1) of diamond d
     int* d_fv_ghost = nullptr;
+
+    // lateral quadrature tables of the gradient-form operators (Laplace,
+    // DivKGrad, VectorLaplace), built on first use: [10][N][N][2 wedges][105]
+    std::mutex      geom_mutex;
+    double*         d_grad_geom = nullptr;
 
     // fs/fs penalty: the orthonormalised modes are m = C (e_j x x); G = C^T C
     double penalty_gram_inv[9] = { 0 };

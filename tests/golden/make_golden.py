@@ -66,6 +66,17 @@ def fct_inputs(fine):
     return vel, T, src
 
 
+CG_MAXIT, CG_TOL = 500, 1e-13
+
+
+def cg_rhs(s):
+    """the seeded scalar field with its radial boundary layers zeroed (homogeneous Dirichlet rows)"""
+    b = s.copy()
+    b[..., 0] = 0.0
+    b[..., -1] = 0.0
+    return b
+
+
 def checksum(a):
     a = np.asarray(a, dtype=np.float64)
     return np.array([a.sum(), (a * a).sum(), np.abs(a).max()])
@@ -134,6 +145,11 @@ def main():
         for bcc, bcs, diag in VLAPLACE_CASES:
             run_ref(["vlaplace", L, R_MIN, R_MAX, bcc, bcs, diag, d], d)
             out[f"vlaplace_{bcc}{bcs}{diag}"] = np.fromfile(f"{d}/dst.bin").reshape((3,) + fine.shape)
+        # unpreconditioned PCG on the Laplace, homogeneous Dirichlet right-hand side
+        cg_rhs(x["s"]).tofile(f"{d}/b.bin")
+        info = run_ref(["laplace_cg", L, R_MIN, R_MAX, CG_MAXIT, CG_TOL, d], d, json_out=True)
+        out["laplace_cg_x"] = np.fromfile(f"{d}/x.bin").reshape(fine.shape)
+        out["laplace_cg_iterations"] = np.array(info["iterations"])
         # FCT: one fct_explicit_step on a rotation-dominated velocity
         vel, T, src = fct_inputs(fine)
         vel.tofile(f"{d}/vel.bin")

@@ -4,6 +4,7 @@ Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 module; the product never imports it.
 """
 import ctypes
+import json
 import os
 import subprocess
 
@@ -243,6 +244,27 @@ class Mesh:
                              _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst), mode)
         return dst
 
+    def laplace_pcg(self, b, max_iterations=1000, relative_tolerance=1e-10, absolute_tolerance=1e-30):
+        """Unpreconditioned PCG from x = 0 (linalg/solvers/pcg.hpp:78-160, z = r) on
+        Laplace(treat_boundary=True).  Returns (x, iterations)."""
+        x = np.zeros(self.shape)
+        r = np.array(b, dtype=np.float64)
+        p = r.copy()
+        r0 = np.sqrt(self.dot(r, r))
+        if r0 < absolute_tolerance:
+            return x, 0
+        for it in range(1, max_iterations + 1):
+            rz = self.dot(r, r)
+            ap = self.laplace(p, True, False)
+            alpha = rz / self.dot(ap, p)
+            x += alpha * p
+            r -= alpha * ap
+            res = np.sqrt(self.dot(r, r))
+            if res / r0 <= relative_tolerance or res < absolute_tolerance:
+                return x, it
+            p = r + (self.dot(r, r) / rz) * p
+        return x, max_iterations
+
     def dot(self, a, b):
         """Owned-masked dot product summed over components."""
         a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1, self.ns)
@@ -256,7 +278,11 @@ def ref_available():
     return os.path.exists(REF_DUMP)
 
 
-def run_ref(args, workdir, threads=4):
+def run_ref(args, workdir, threads=4, json_out=False):
+    """Run the compiled reference (ref_dump); with json_out, parse its last JSON output line."""
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="false")
-    subprocess.run([REF_DUMP] + [str(a) for a in args], cwd=workdir, env=env, check=True,
-                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    out = subprocess.run([REF_DUMP] + [str(a) for a in args], cwd=workdir, env=env, check=True,
+                         stdout=subprocess.PIPE if json_out else subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                         text=True)
+    if json_out:
+        return json.loads([ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1])

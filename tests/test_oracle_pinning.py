@@ -127,6 +127,14 @@ def test_golden_fixture_is_not_trivial(case):
     assert rel(fine.kerngen(x["k"], u, 1, 1, 0), g["kerngen_110"]) > 1e-8
 
 
+def test_laplace_pcg_matches_reference(case):
+    """The PCG restatement reaches the reference solver's solution in the same number of iterations."""
+    g, fine, _, x = case
+    sol, its = fine.laplace_pcg(G.cg_rhs(x["s"]), G.CG_MAXIT, G.CG_TOL)
+    assert its == int(g["laplace_cg_iterations"])
+    assert rel(sol, g["laplace_cg_x"]) <= 1e-11
+
+
 @pytest.mark.skipif(not ref_available(), reason="compiled reference (oracle/_ref/ref_dump) not built here")
 def test_oracle_matches_live_reference_L3():
     L = 3

@@ -10,38 +10,37 @@ from oracle_lib import Mesh
 pytestmark = pytest.mark.gpu
 
 
-def oracle_pcg(om, b, tol, maxit=2000):
-    """Unpreconditioned CG with the oracle Laplace (pcg.hpp:78-160)."""
-    x = np.zeros_like(b)
-    r = b - om.laplace(x)
-    p = r.copy()
-    r0 = np.sqrt(om.dot(r, r))
-    for it in range(1, maxit + 1):
-        an = om.dot(r, r)
-        ap = om.laplace(p)
-        alpha = an / om.dot(ap, p)
-        x += alpha * p
-        r -= alpha * ap
-        rr = np.sqrt(om.dot(r, r)) / r0
-        if rr <= tol:
-            return x, it, rr
-        p = r + (om.dot(r, r) / an) * p
-    return x, maxit, rr
-
-
 def test_laplace_pcg_matches_oracle_cg():
     from terraneo_b200 import shell
     L = 3
     om, pm = Mesh(L), shell.ShellMesh(L)
     b = random_vector(om, seed=11, ncomp=1)
     b[om.bmask != 1] = 0.0  # homogeneous Dirichlet rows
-    xo, ito, rro = oracle_pcg(om, b, 1e-10)
+    xo, ito = om.laplace_pcg(b, 2000, 1e-10)
     vb, vx = shell.VectorQ1Scalar(pm), shell.VectorQ1Scalar(pm)
     vb.set_numpy(b)
     it, rr = shell.laplace_pcg(pm, vb, vx, relative_tolerance=1e-10)
     assert rr <= 1e-10
     assert abs(it - ito) <= 2
     assert rel(vx.numpy()[0], xo) <= 1e-7
+
+
+def test_laplace_pcg_matches_reference_golden():
+    """PCG on the golden level-2 right-hand side: the reference solver's solution and iteration count."""
+    import os
+    import sys
+    from terraneo_b200 import shell
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden as G
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_L2.npz"))
+    fine, coarse = Mesh(G.L), Mesh(G.L - 1)
+    b = G.cg_rhs(G.inputs(fine, coarse)["s"])
+    pm = shell.ShellMesh(G.L)
+    vb, vx = shell.VectorQ1Scalar(pm), shell.VectorQ1Scalar(pm)
+    vb.set_numpy(b)
+    it, rr = shell.laplace_pcg(pm, vb, vx, G.CG_MAXIT, G.CG_TOL)
+    assert abs(it - int(g["laplace_cg_iterations"])) <= 1
+    assert rel(vx.numpy()[0], g["laplace_cg_x"]) <= 1e-11
 
 
 @pytest.fixture(scope="module")
