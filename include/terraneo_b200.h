@@ -492,6 +492,8 @@ typedef struct
                    constant interpolation (TwoGridGCA default), 2 GCA with linear interpolation */
     int    outer; /* 0 FGMRES(restart) + block-triangular preconditioner, 1 PMINRES + block-diagonal
                      preconditioner (pminres.hpp, block_preconditioner_2x2.hpp:38-100) */
+    int    eager; /* 0: after its first application the preconditioner is captured once per vector pair as a
+                     CUDA graph and replayed; 1: always launched kernel by kernel */
 } tn_stokes_params;
 
 typedef struct tn_stokes_solver tn_stokes_solver;

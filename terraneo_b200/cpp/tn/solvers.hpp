@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <limits>
+#include <map>
 #include <vector>
 
 #include "operators.hpp"
@@ -339,6 +340,94 @@ class Multigrid
     int                     cycles_;
 };
 
+// Replays one captured CUDA graph of a solver's launch sequence per (x, b)
+// storage.  The first solve runs eagerly (one-off host work such as the
+// Chebyshev eigenvalue estimates and lazily built tables happens there);
+// every later solve with storage not seen before is captured on a private
+// stream and instantiated, then launched on tn::stream().  The inner solver
+// must issue a fixed, data-independent launch sequence after its first solve
+// (the device-gated PCG coarse solver does so while capturing) and must not
+// change the values baked into its launches (e.g. smoother coefficients)
+// afterwards.
+template < typename Inner >
+class GraphReplay
+{
+  public:
+    GraphReplay( Inner& inner, bool enabled = true ) : inner_( inner ), enabled_( enabled ) {}
+    GraphReplay( const GraphReplay& )            = delete;
+    GraphReplay& operator=( const GraphReplay& ) = delete;
+    ~GraphReplay()
+    {
+        for ( auto& e : execs_ )
+            cudaGraphExecDestroy( e.second );
+        if ( cap_ )
+            cudaStreamDestroy( cap_ );
+    }
+    template < typename Op, typename V >
+    void solve_impl( Op& A, V& x, const V& b )
+    {
+        if ( !warm_ || !enabled_ )
+        {
+            solve( inner_, A, x, b );
+            warm_ = true;
+            return;
+        }
+        const auto         sx = segments( x ), sb = segments( b );
+        std::vector< const void* > key;
+        for ( int i = 0; i < sx.n; ++i )
+            key.push_back( sx.f[i] );
+        for ( int i = 0; i < sb.n; ++i )
+            key.push_back( sb.f[i] );
+        auto it = execs_.find( key );
+        if ( it == execs_.end() )
+        {
+            if ( !cap_ && cudaStreamCreateWithFlags( &cap_, cudaStreamNonBlocking ) != cudaSuccess )
+                throw std::runtime_error( "GraphReplay: creating the capture stream failed" );
+            cudaStream_t saved = stream_ref();
+            stream_ref()       = cap_;
+            cudaGraph_t g      = nullptr;
+            if ( cudaStreamBeginCapture( cap_, cudaStreamCaptureModeThreadLocal ) != cudaSuccess )
+            {
+                stream_ref() = saved;
+                throw std::runtime_error( "GraphReplay: cudaStreamBeginCapture failed" );
+            }
+            try
+            {
+                solve( inner_, A, x, b );
+            }
+            catch ( ... )
+            {
+                cudaStreamEndCapture( cap_, &g );
+                if ( g )
+                    cudaGraphDestroy( g );
+                stream_ref() = saved;
+                throw;
+            }
+            const cudaError_t ec = cudaStreamEndCapture( cap_, &g );
+            stream_ref()         = saved;
+            cudaGraphExec_t e    = nullptr;
+            if ( ec != cudaSuccess || cudaGraphInstantiate( &e, g, 0 ) != cudaSuccess )
+            {
+                if ( g )
+                    cudaGraphDestroy( g );
+                throw std::runtime_error( "GraphReplay: capturing the solver failed" );
+            }
+            cudaGraphDestroy( g );
+            it = execs_.emplace( std::move( key ), e ).first;
+        }
+        if ( cudaGraphLaunch( it->second, stream() ) != cudaSuccess )
+            throw std::runtime_error( "GraphReplay: cudaGraphLaunch failed" );
+    }
+    size_t graphs() const { return execs_.size(); }
+
+  private:
+    Inner&                                                     inner_;
+    bool                                                       enabled_;
+    bool                                                       warm_ = false;
+    cudaStream_t                                               cap_  = nullptr;
+    std::map< std::vector< const void* >, cudaGraphExec_t > execs_;
+};
+
 // BlockTriangularPreconditioner2x2 (block_preconditioner_2x2.hpp:145-217)
 template < typename Block11, typename Block12, typename Prec11, typename Prec22, typename BV >
 class BlockTriangularPreconditioner2x2
@@ -662,30 +751,41 @@ class FGMRES
                 auto& zj = tmp_[offZ + j];
                 assign( zj, S( 0 ) );
                 solve( prec_, A, zj, vj );
-                if ( has_nan_or_inf( zj ) )
+                auto&   w  = tmp_[idxW];
+                double* hd = hdev_.get();
+                // w = A z, then modified Gram-Schmidt (fgmres.hpp:197-209):
+                // h_ij = <w, v_i>, w -= h_ij v_i for i = 0..j, then |w|; each
+                // pass fuses the update by v_{i-1} with the projection on v_i
+                // and the coefficients stay on the device until one read at
+                // the end.  A NaN / Inf in z (the reference replaces z by v,
+                // fgmres.hpp:180-186) reaches every h_ij through A z, so the
+                // column read doubles as the check and the step is redone
+                // with z = v.
+                auto arnoldi = [&]() {
+                    apply( A, zj, w );
+                    const auto sw = segments( w );
+                    for ( int i = 0; i <= j + 1; ++i )
+                    {
+                        const auto sv = segments( tmp_[offV + std::min( i, j )] );
+                        const auto su = segments( tmp_[offV + std::max( i - 1, 0 )] );
+                        axpy_dot( sw, i > 0 ? &su : nullptr, i > 0 ? hd + i - 1 : nullptr, i <= j ? &sv : nullptr,
+                                  nullptr, hd + i );
+                    }
+                    if ( cudaMemcpyAsync( hhost_.data(), hd, sizeof( double ) * ( j + 2 ), cudaMemcpyDeviceToHost,
+                                          stream() ) != cudaSuccess ||
+                         cudaStreamSynchronize( stream() ) != cudaSuccess )
+                        throw std::runtime_error( "FGMRES: reading the Hessenberg column failed" );
+                    for ( int i = 0; i <= j + 1; ++i )
+                        if ( !std::isfinite( hhost_[i] ) )
+                            return false;
+                    return true;
+                };
+                if ( !arnoldi() )
                 {
                     assign( zj, vj );
                     ++preconditioner_skips;
+                    arnoldi();
                 }
-                auto& w = tmp_[idxW];
-                apply( A, zj, w );
-                // modified Gram-Schmidt (fgmres.hpp:197-209): h_ij = <w, v_i>,
-                // w -= h_ij v_i for i = 0..j, then |w|; each pass fuses the
-                // update by v_{i-1} with the projection on v_i and the
-                // coefficients stay on the device until one read at the end.
-                const auto sw = segments( w );
-                double*    hd = hdev_.get();
-                for ( int i = 0; i <= j + 1; ++i )
-                {
-                    const auto sv = segments( tmp_[offV + std::min( i, j )] );
-                    const auto su = segments( tmp_[offV + std::max( i - 1, 0 )] );
-                    axpy_dot( sw, i > 0 ? &su : nullptr, i > 0 ? hd + i - 1 : nullptr, i <= j ? &sv : nullptr,
-                              nullptr, hd + i );
-                }
-                if ( cudaMemcpyAsync( hhost_.data(), hd, sizeof( double ) * ( j + 2 ), cudaMemcpyDeviceToHost,
-                                      stream() ) != cudaSuccess ||
-                     cudaStreamSynchronize( stream() ) != cudaSuccess )
-                    throw std::runtime_error( "FGMRES: reading the Hessenberg column failed" );
                 for ( int i = 0; i <= j; ++i )
                     h( i, j ) = hhost_[i];
                 const double hj1 = std::sqrt( hhost_[j + 1] );

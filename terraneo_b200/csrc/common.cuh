@@ -95,6 +95,7 @@ struct tn_mesh
     // DivKGrad, VectorLaplace), built on first use: [10][N][N][2 wedges][105]
     std::mutex      geom_mutex;
     double*         d_grad_geom = nullptr;
+    double*         d_stokes_geom = nullptr; // Divergence / Gradient, this mesh as the velocity mesh
 
     // fs/fs penalty: the orthonormalised modes are m = C (e_j x x); G = C^T C
     double penalty_gram_inv[9] = { 0 };

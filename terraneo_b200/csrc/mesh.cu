@@ -339,6 +339,7 @@ extern "C" int tn_mesh_destroy( tn_mesh* m )
     cudaFree( m->d_halo_members );
     cudaFree( m->d_fv_ghost );
     cudaFree( m->d_grad_geom );
+    cudaFree( m->d_stokes_geom );
     cudaFree( m->d_red_partials );
     cudaFree( m->d_red_result );
     cudaFree( m->d_red_counter );

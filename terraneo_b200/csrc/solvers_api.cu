@@ -203,12 +203,14 @@ void finish( tn_stokes_solver& s, std::shared_ptr< Prec11 > p11 )
         // PMINRES with the block-diagonal preconditioner (pminres.hpp, block_preconditioner_2x2.hpp:38-100)
         using BD  = BlockDiagonalPreconditioner2x2< A64, Prec11, DiagonalSolver< KMass< double >, VectorQ1Scalar< double > >,
                                                     VectorQ1IsoQ2Q1< double > >;
-        auto prec = std::make_shared< BD >( *a11, *p11, *p22 );
+        auto prec  = std::make_shared< BD >( *a11, *p11, *p22 );
+        auto graph = std::make_shared< GraphReplay< BD > >( *prec, prm.eager == 0 );
         std::vector< VectorQ1IsoQ2Q1< double > > tmps;
         for ( int i = 0; i < 7; ++i )
             tmps.emplace_back( s.mesh[L], s.mesh[L - 1] );
-        auto mr = std::make_shared< PMINRES< EpsDivDivStokes< double >, BD > >( ip, tmps, *prec );
-        s.run = [sp, mr, prec, p11, p22, a11]( VectorQ1IsoQ2Q1< double >& x, const VectorQ1IsoQ2Q1< double >& b ) {
+        auto mr = std::make_shared< PMINRES< EpsDivDivStokes< double >, GraphReplay< BD >& > >( ip, tmps, *graph );
+        s.run = [sp, mr, prec, graph, p11, p22, a11]( VectorQ1IsoQ2Q1< double >& x,
+                                                      const VectorQ1IsoQ2Q1< double >& b ) {
             solve( *mr, *sp->K, x, b );
             sp->history    = mr->stats.relative_residuals;
             sp->iterations = mr->stats.iterations;
@@ -220,12 +222,13 @@ void finish( tn_stokes_solver& s, std::shared_ptr< Prec11 > p11 )
     using BT = BlockTriangularPreconditioner2x2< A64, Gradient< double >, Prec11,
                                                  DiagonalSolver< KMass< double >, VectorQ1Scalar< double > >,
                                                  VectorQ1IsoQ2Q1< double > >;
-    auto prec = std::make_shared< BT >( *a11, *s.BT, VectorQ1IsoQ2Q1< double >( s.mesh[L], s.mesh[L - 1] ), *p11, *p22 );
+    auto prec  = std::make_shared< BT >( *a11, *s.BT, VectorQ1IsoQ2Q1< double >( s.mesh[L], s.mesh[L - 1] ), *p11, *p22 );
+    auto graph = std::make_shared< GraphReplay< BT > >( *prec, prm.eager == 0 );
     std::vector< VectorQ1IsoQ2Q1< double > > tmps;
     for ( int i = 0; i < 2 * prm.restart + 4; ++i )
         tmps.emplace_back( s.mesh[L], s.mesh[L - 1] );
-    auto fg = std::make_shared< FGMRES< EpsDivDivStokes< double >, BT > >( tmps, prm.restart, ip, *prec );
-    s.run = [sp, fg, prec, p11, p22, a11]( VectorQ1IsoQ2Q1< double >& x, const VectorQ1IsoQ2Q1< double >& b ) {
+    auto fg = std::make_shared< FGMRES< EpsDivDivStokes< double >, GraphReplay< BT > > >( tmps, prm.restart, ip, *graph );
+    s.run = [sp, fg, prec, graph, p11, p22, a11]( VectorQ1IsoQ2Q1< double >& x, const VectorQ1IsoQ2Q1< double >& b ) {
         solve( *fg, *sp->K, x, b );
         sp->history    = fg->stats.relative_residuals;
         sp->iterations = fg->stats.iterations;

@@ -16,8 +16,24 @@
 // free-slip nodes are projected onto the tangent plane (the reference's
 // rotate / eliminate-normal / rotate-back sequence, :226-290).
 //
+// Factored form.  With the fine wedge's a = p1 - p0, b = p2 - p0, v = a x b,
+// D = v . p0, c = p0 + xi a + eta b, u_1 = b x c, u_2 = c x a,
+// u_0 = -(u_1 + u_2) and h = (r2 - r1) / 2, every quadrature point has
+//     |det J| grad N_n = sign(D) ( r h nr_n(zeta) u_m + r^2 s_n lat_m v )
+// (m the lateral vertex of node n, s_n = -+1/2, nr_n = (1 -+ zeta)/2), and the
+// coarse shape function is a lateral factor times a radial one.  On the
+// tensor-product 3x2 rule the block therefore separates into
+//     B_{i,(n,:)} = Ra[i/3][n/3] Uc[i%3][n%3] + s_n Rb[i/3] Lc[i%3][n%3] vt
+// with per-triangle lateral tables (Uc = -w sign(D) sum_q latc_i(q) u_m(q),
+// vt = -w sign(D) v, Lc = sum_q latc_i(q) lat_m(q)) built once per mesh and
+// the radial sums Ra = sum_zeta radc_i r h nr_n, Rb = sum_zeta radc_i r^2
+// formed per cell: the same integrals as the per-point Jacobian of
+// fe/wedge/integrands.hpp at a fraction of the arithmetic.
+//
 // One thread per fine cell (r fastest), both wedges, contributions summed per
 // node in registers and added with atomics.
+#include <cmath>
+
 #include "common.cuh"
 #include "wedge.cuh"
 
@@ -28,45 +44,35 @@ int halo_sum( const tn_mesh* m, T* const* fields, int nfields, cudaStream_t st )
 
 namespace {
 
-__device__ __constant__ const double kQP[6][3] = { { 0.6666666666666666, 0.1666666666666667, -0.5773502691896257 },
-                                                   { 0.1666666666666667, 0.6666666666666666, -0.5773502691896257 },
-                                                   { 0.1666666666666667, 0.1666666666666667, -0.5773502691896257 },
-                                                   { 0.6666666666666666, 0.1666666666666667, 0.5773502691896257 },
-                                                   { 0.1666666666666667, 0.6666666666666666, 0.5773502691896257 },
-                                                   { 0.1666666666666667, 0.1666666666666667, 0.5773502691896257 } };
-constexpr double kQW = 0.1666666666666667;
+constexpr double kQPHost[3][2] = { { 0.6666666666666666, 0.1666666666666667 },
+                                   { 0.1666666666666667, 0.6666666666666666 },
+                                   { 0.1666666666666667, 0.1666666666666667 } };
+constexpr double kZeta = 0.5773502691896257;
+constexpr double kQW   = 0.1666666666666667;
 
 // coarse lateral shape coefficients (a, b xi, c eta) per [node % 3][fine lateral wedge index]
-__device__ __constant__ const double kCoarseLat[3][4][3] = {
+// (shape_coarse, integrands.hpp:266-400)
+constexpr double kCoarseLat[3][4][3] = {
     { { 1.0, -0.5, -0.5 }, { 0.5, -0.5, -0.5 }, { 0.5, -0.5, -0.5 }, { 0.0, 0.5, 0.5 } },
     { { 0.0, 0.5, 0.0 }, { 0.5, 0.5, 0.0 }, { 0.0, 0.5, 0.0 }, { 0.5, -0.5, 0.0 } },
     { { 0.0, 0.0, 0.5 }, { 0.0, 0.0, 0.5 }, { 0.5, 0.0, 0.5 }, { 0.5, 0.0, -0.5 } } };
 
-template < typename T >
-__device__ __forceinline__ T shape_coarse( int i, int frad, int flat, T xi, T eta, T zeta )
-{
-    const T lat = T( kCoarseLat[i % 3][flat][0] ) + T( kCoarseLat[i % 3][flat][1] ) * xi +
-                  T( kCoarseLat[i % 3][flat][2] ) * eta;
-    T rad;
-    if ( i < 3 )
-        rad = frad == 0 ? T( 0.25 ) * ( T( 3 ) - zeta ) : T( 0.25 ) * ( T( 1 ) - zeta );
-    else
-        rad = frad == 0 ? T( 0.25 ) * ( T( 1 ) + zeta ) : T( 0.25 ) * ( T( 3 ) + zeta );
-    return lat * rad;
-}
-
-__device__ __forceinline__ int fine_lateral_wedge( int x, int y, int w )
+__host__ __device__ __forceinline__ int fine_lateral_wedge( int x, int y, int w )
 {
     // fine_lateral_wedge_idx (kernel_helpers.hpp:601)
     const int xm = x & 1, ym = y & 1;
     return w == 0 ? ( ym * 2 + xm ) : ( 3 - ( ym * 2 + xm ) );
 }
 
+// per fine wedge: Uc[3][3][3] (27), vt (3), Lc[3][3] (9)
+constexpr int kStokesStride = 39;
+
 template < typename T >
 struct StokesParams
 {
     int           N, n1, nc1;
     const double* coords; // fine lateral coords
+    const double* geom;   // kStokesStride doubles per fine wedge
     const T*      radii;  // fine radii
     int           bc_cmb, bc_surf;
 };
@@ -88,76 +94,37 @@ __device__ __forceinline__ void unit_normal( const double* c, T n[3] )
     n[0] = T( c[0] / m ), n[1] = T( c[1] / m ), n[2] = T( c[2] / m );
 }
 
-// Quadrature data of one fine wedge: for lateral point ql and radial point
-// qz, J = M(ql) diag(r(qz), r(qz), dr/2) with M = [p1-p0, p2-p0, p(xi,eta)], so
-// J^{-T} = M^{-T} diag(1/r, 1/r, 2/dr) and |det J| = |det M| r^2 dr/2: one 3x3
-// inverse per lateral point serves both radial points.  Calls f(q, wdet, g, xi,
-// eta, zeta) with g the 6 physical shape gradients.
-template < typename T, typename F >
-__device__ __forceinline__ void for_each_qp( const T p[3][3], T r1, T r2, F&& f )
-{
-    const T dr = T( 0.5 ) * ( r2 - r1 );
-#pragma unroll 1
-    for ( int ql = 0; ql < 3; ++ql )
-    {
-        const T xi = T( kQP[ql][0] ), eta = T( kQP[ql][1] );
-        T       M[3][3];
-#pragma unroll
-        for ( int a = 0; a < 3; ++a )
-        {
-            M[a][0] = p[1][a] - p[0][a];
-            M[a][1] = p[2][a] - p[0][a];
-            M[a][2] = ( T( 1 ) - xi - eta ) * p[0][a] + xi * p[1][a] + eta * p[2][a];
-        }
-        const T c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1], c01 = M[1][2] * M[2][0] - M[1][0] * M[2][2],
-                c02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
-        const T det = M[0][0] * c00 + M[0][1] * c01 + M[0][2] * c02;
-        const T id  = T( 1 ) / det;
-        // Q = M^{-T}
-        T Q[3][3];
-        Q[0][0] = c00 * id, Q[0][1] = c01 * id, Q[0][2] = c02 * id;
-        Q[1][0] = ( M[0][2] * M[2][1] - M[0][1] * M[2][2] ) * id;
-        Q[1][1] = ( M[0][0] * M[2][2] - M[0][2] * M[2][0] ) * id;
-        Q[1][2] = ( M[0][1] * M[2][0] - M[0][0] * M[2][1] ) * id;
-        Q[2][0] = ( M[0][1] * M[1][2] - M[0][2] * M[1][1] ) * id;
-        Q[2][1] = ( M[0][2] * M[1][0] - M[0][0] * M[1][2] ) * id;
-        Q[2][2] = ( M[0][0] * M[1][1] - M[0][1] * M[1][0] ) * id;
-#pragma unroll
-        for ( int qz = 0; qz < 2; ++qz )
-        {
-            const int q    = ql + 3 * qz;
-            const T   zeta = T( kQP[q][2] );
-            const T   rq   = r1 + dr * ( T( 1 ) + zeta );
-            const T   s0 = T( 1 ) / rq, s2 = T( 1 ) / dr;
-            const T   wdet = T( kQW ) * fabs( det ) * rq * rq * dr;
-            T         g[6][3];
-#pragma unroll
-            for ( int n = 0; n < 6; ++n )
-            {
-                T gr[3];
-                grad_shape_ref( n, xi, eta, zeta, gr );
-                gr[0] *= s0, gr[1] *= s0, gr[2] *= s2;
-#pragma unroll
-                for ( int a = 0; a < 3; ++a )
-                    g[n][a] = Q[a][0] * gr[0] + Q[a][1] * gr[1] + Q[a][2] * gr[2];
-            }
-            f( q, wdet, g, xi, eta, zeta );
-        }
-    }
-}
-
+// radial sums of one fine cell: Ra[ib][nb] = h sum_zeta radc_ib r nr_nb, Rb[ib] = sum_zeta radc_ib r^2
 template < typename T >
-__device__ __forceinline__ void wedge_points( const StokesParams< T >& P, int dm, int x, int y, int w, T p[3][3] )
+__device__ __forceinline__ void radial_sums( T r1, T r2, int frad, T Ra[2][2], T Rb[2] )
 {
+    const T h = T( 0.5 ) * ( r2 - r1 );
+    Ra[0][0] = Ra[0][1] = Ra[1][0] = Ra[1][1] = Rb[0] = Rb[1] = T( 0 );
 #pragma unroll
-    for ( int n = 0; n < 3; ++n )
+    for ( int zq = 0; zq < 2; ++zq )
     {
-        const double* c = P.coords + lat_index( P.n1, dm, x + kWedgeNode[w][n][0], y + kWedgeNode[w][n][1] ) * 3;
-        p[n][0] = T( c[0] ), p[n][1] = T( c[1] ), p[n][2] = T( c[2] );
+        const T zeta = zq ? T( kZeta ) : T( -kZeta );
+        const T rr   = r1 + h * ( T( 1 ) + zeta );
+        const T nr[2] = { T( 0.5 ) * ( T( 1 ) - zeta ), T( 0.5 ) * ( T( 1 ) + zeta ) };
+        const T rc[2] = { frad == 0 ? T( 0.25 ) * ( T( 3 ) - zeta ) : T( 0.25 ) * ( T( 1 ) - zeta ),
+                          frad == 0 ? T( 0.25 ) * ( T( 1 ) + zeta ) : T( 0.25 ) * ( T( 3 ) + zeta ) };
+#pragma unroll
+        for ( int ib = 0; ib < 2; ++ib )
+        {
+            Rb[ib] += rc[ib] * rr * rr;
+#pragma unroll
+            for ( int nb = 0; nb < 2; ++nb )
+                Ra[ib][nb] += rc[ib] * rr * h * nr[nb];
+        }
     }
 }
 
-// p_coarse += B u: per quadrature point -w |det J| N^c_i div u
+__device__ __forceinline__ size_t stokes_tri( int N, int dm, int x, int y, int w )
+{
+    return ( ( size_t( dm ) * N + x ) * N + y ) * 2 + w;
+}
+
+// p_coarse += B u
 template < typename T >
 __global__ void __launch_bounds__( 128 ) divergence_kernel( StokesParams< T > P, Ptr3< const T > u, T* __restrict__ p )
 {
@@ -173,15 +140,13 @@ __global__ void __launch_bounds__( 128 ) divergence_kernel( StokesParams< T > P,
 #pragma unroll
     for ( int i = 0; i < 8; ++i )
         out[i >> 2][( i >> 1 ) & 1][i & 1] = T( 0 );
-    const T   r1 = P.radii[dm * n1 + r], r2 = P.radii[dm * n1 + r + 1];
-    const int frad = r & 1;
+    T Ra[2][2], Rb[2];
+    radial_sums( P.radii[dm * n1 + r], P.radii[dm * n1 + r + 1], r & 1, Ra, Rb );
 #pragma unroll
     for ( int w = 0; w < 2; ++w )
     {
-        T p3[3][3];
-        wedge_points( P, dm, x, y, w, p3 );
-        const int flat = fine_lateral_wedge( x, y, w );
-        T         uu[6][3];
+        const double* G = P.geom + stokes_tri( N, dm, x, y, w ) * kStokesStride;
+        T             uu[6][3];
 #pragma unroll
         for ( int n = 0; n < 6; ++n )
         {
@@ -199,17 +164,30 @@ __global__ void __launch_bounds__( 128 ) divergence_kernel( StokesParams< T > P,
                 uu[n][0] -= dt * nn[0], uu[n][1] -= dt * nn[1], uu[n][2] -= dt * nn[2];
             }
         }
+        const T vt[3] = { T( G[27] ), T( G[28] ), T( G[29] ) };
+        T       vu[6];
+#pragma unroll
+        for ( int n = 0; n < 6; ++n )
+            vu[n] = ( n < 3 ? T( -0.5 ) : T( 0.5 ) ) * ( vt[0] * uu[n][0] + vt[1] * uu[n][1] + vt[2] * uu[n][2] );
         T acc[6] = { 0, 0, 0, 0, 0, 0 };
-        for_each_qp( p3, r1, r2, [&]( int, T wdet, const T ( &g )[6][3], T xi, T eta, T zeta ) {
-            T div = 0;
 #pragma unroll
-            for ( int n = 0; n < 6; ++n )
-                div += g[n][0] * uu[n][0] + g[n][1] * uu[n][1] + g[n][2] * uu[n][2];
-            const T s = -wdet * div;
+        for ( int ic = 0; ic < 3; ++ic )
 #pragma unroll
-            for ( int i = 0; i < 6; ++i )
-                acc[i] += s * shape_coarse( i, frad, flat, xi, eta, zeta );
-        } );
+            for ( int m = 0; m < 3; ++m )
+            {
+                const double* U  = G + ( ic * 3 + m ) * 3;
+                const T       U0 = T( U[0] ), U1 = T( U[1] ), U2 = T( U[2] ), lc = T( G[30 + ic * 3 + m] );
+#pragma unroll
+                for ( int nb = 0; nb < 2; ++nb )
+                {
+                    const int n  = nb * 3 + m;
+                    const T   cu = U0 * uu[n][0] + U1 * uu[n][1] + U2 * uu[n][2];
+                    const T   lv = lc * vu[n];
+#pragma unroll
+                    for ( int ib = 0; ib < 2; ++ib )
+                        acc[ib * 3 + ic] += Ra[ib][nb] * cu + Rb[ib] * lv;
+                }
+            }
 #pragma unroll
         for ( int i = 0; i < 6; ++i )
             out[kWedgeNode[w][i][0]][kWedgeNode[w][i][1]][kWedgeNode[w][i][2]] += acc[i];
@@ -223,7 +201,7 @@ __global__ void __launch_bounds__( 128 ) divergence_kernel( StokesParams< T > P,
     }
 }
 
-// u_fine += B^T p: per quadrature point -w |det J| p^c(q) grad N_j
+// u_fine += B^T p
 template < typename T >
 __global__ void __launch_bounds__( 128 ) gradient_kernel( StokesParams< T > P, const T* __restrict__ p, Ptr3< T > u )
 {
@@ -242,49 +220,61 @@ __global__ void __launch_bounds__( 128 ) gradient_kernel( StokesParams< T > P, c
         for ( int c = 0; c < 3; ++c )
             out[i >> 2][( i >> 1 ) & 1][i & 1][c] = T( 0 );
     const int xc = x >> 1, yc = y >> 1, rc = r >> 1;
-    const T   r1 = P.radii[dm * n1 + r], r2 = P.radii[dm * n1 + r + 1];
-    const int frad = r & 1;
+    T         Ra[2][2], Rb[2];
+    radial_sums( P.radii[dm * n1 + r], P.radii[dm * n1 + r + 1], r & 1, Ra, Rb );
 #pragma unroll
     for ( int w = 0; w < 2; ++w )
     {
-        T p3[3][3];
-        wedge_points( P, dm, x, y, w, p3 );
-        const int flat = fine_lateral_wedge( x, y, w );
-        T         pc[6];
+        const double* G = P.geom + stokes_tri( N, dm, x, y, w ) * kStokesStride;
+        T             pc[6];
 #pragma unroll
         for ( int i = 0; i < 6; ++i )
             pc[i] = p[lat_index( nc1, dm, xc + kWedgeNode[w][i][0], yc + kWedgeNode[w][i][1] ) * nc1 + rc +
                       kWedgeNode[w][i][2]];
-        T acc[6][3];
+        const T vt[3] = { T( G[27] ), T( G[28] ), T( G[29] ) };
+        // pr[nb][ic] = sum_ib Ra[ib][nb] pc[ib][ic]; pl[ic] = sum_ib Rb[ib] pc[ib][ic]
+        T pr[2][3], pl[3];
 #pragma unroll
-        for ( int n = 0; n < 6; ++n )
-            acc[n][0] = acc[n][1] = acc[n][2] = T( 0 );
-        for_each_qp( p3, r1, r2, [&]( int, T wdet, const T ( &g )[6][3], T xi, T eta, T zeta ) {
-            T pq = 0;
-#pragma unroll
-            for ( int i = 0; i < 6; ++i )
-                pq += shape_coarse( i, frad, flat, xi, eta, zeta ) * pc[i];
-            const T s = -wdet * pq;
-#pragma unroll
-            for ( int n = 0; n < 6; ++n )
-                acc[n][0] += s * g[n][0], acc[n][1] += s * g[n][1], acc[n][2] += s * g[n][2];
-        } );
-#pragma unroll
-        for ( int j = 0; j < 6; ++j )
+        for ( int ic = 0; ic < 3; ++ic )
         {
-            T         v[3] = { acc[j][0], acc[j][1], acc[j][2] };
-            const int bc   = velocity_bc( N, r, j, P.bc_cmb, P.bc_surf );
-            if ( bc == TN_BC_DIRICHLET )
-                continue;
-            if ( bc == TN_BC_FREESLIP )
+            pl[ic] = Rb[0] * pc[ic] + Rb[1] * pc[3 + ic];
+#pragma unroll
+            for ( int nb = 0; nb < 2; ++nb )
+                pr[nb][ic] = Ra[0][nb] * pc[ic] + Ra[1][nb] * pc[3 + ic];
+        }
+#pragma unroll
+        for ( int m = 0; m < 3; ++m )
+        {
+            T sv = T( 0 );
+#pragma unroll
+            for ( int ic = 0; ic < 3; ++ic )
+                sv += T( G[30 + ic * 3 + m] ) * pl[ic];
+#pragma unroll
+            for ( int nb = 0; nb < 2; ++nb )
             {
-                T nn[3];
-                unit_normal( P.coords + lat_index( n1, dm, x + kWedgeNode[w][j][0], y + kWedgeNode[w][j][1] ) * 3, nn );
-                const T dt = nn[0] * v[0] + nn[1] * v[1] + nn[2] * v[2];
-                v[0] -= dt * nn[0], v[1] -= dt * nn[1], v[2] -= dt * nn[2];
+                const int j = nb * 3 + m;
+                const T   s = ( nb ? T( 0.5 ) : T( -0.5 ) ) * sv;
+                T         v[3] = { s * vt[0], s * vt[1], s * vt[2] };
+#pragma unroll
+                for ( int ic = 0; ic < 3; ++ic )
+                {
+                    const double* U = G + ( ic * 3 + m ) * 3;
+                    v[0] += pr[nb][ic] * T( U[0] ), v[1] += pr[nb][ic] * T( U[1] ), v[2] += pr[nb][ic] * T( U[2] );
+                }
+                const int bc = velocity_bc( N, r, j, P.bc_cmb, P.bc_surf );
+                if ( bc == TN_BC_DIRICHLET )
+                    continue;
+                if ( bc == TN_BC_FREESLIP )
+                {
+                    T nn[3];
+                    unit_normal( P.coords + lat_index( n1, dm, x + kWedgeNode[w][j][0], y + kWedgeNode[w][j][1] ) * 3,
+                                 nn );
+                    const T dt = nn[0] * v[0] + nn[1] * v[1] + nn[2] * v[2];
+                    v[0] -= dt * nn[0], v[1] -= dt * nn[1], v[2] -= dt * nn[2];
+                }
+                T* o = out[kWedgeNode[w][j][0]][kWedgeNode[w][j][1]][kWedgeNode[w][j][2]];
+                o[0] += v[0], o[1] += v[1], o[2] += v[2];
             }
-            T* o = out[kWedgeNode[w][j][0]][kWedgeNode[w][j][1]][kWedgeNode[w][j][2]];
-            o[0] += v[0], o[1] += v[1], o[2] += v[2];
         }
     }
 #pragma unroll
@@ -296,6 +286,82 @@ __global__ void __launch_bounds__( 128 ) gradient_kernel( StokesParams< T > P, c
         atomicAdd( u.p[1] + i, out[dx][dy][dr][1] );
         atomicAdd( u.p[2] + i, out[dx][dy][dr][2] );
     }
+}
+
+// Host tabulation of the lateral factors of every fine wedge (double).
+void build_stokes_geometry( const tn_mesh* m, std::vector< double >& G )
+{
+    const int N = m->N, n1 = m->n1;
+    const int wn[2][3][2] = { { { 0, 0 }, { 1, 0 }, { 0, 1 } }, { { 1, 1 }, { 0, 1 }, { 1, 0 } } };
+    auto      cross = []( const double* a, const double* b, double* o ) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    G.assign( size_t( kDiamonds ) * N * N * 2 * kStokesStride, 0.0 );
+    for ( int d = 0; d < kDiamonds; ++d )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int w = 0; w < 2; ++w )
+                {
+                    double*       g = G.data() + ( ( ( size_t( d ) * N + x ) * N + y ) * 2 + w ) * kStokesStride;
+                    const int     flat = fine_lateral_wedge( x, y, w );
+                    const double* p[3];
+                    for ( int k = 0; k < 3; ++k )
+                        p[k] = m->h_coords.data() + lat_index( n1, d, x + wn[w][k][0], y + wn[w][k][1] ) * 3;
+                    double a[3], b[3], v[3];
+                    for ( int k = 0; k < 3; ++k )
+                        a[k] = p[1][k] - p[0][k], b[k] = p[2][k] - p[0][k];
+                    cross( a, b, v );
+                    const double D   = v[0] * p[0][0] + v[1] * p[0][1] + v[2] * p[0][2];
+                    const double sig = -kQW * ( D < 0 ? -1.0 : 1.0 );
+                    for ( int q = 0; q < 3; ++q )
+                    {
+                        const double xi = kQPHost[q][0], eta = kQPHost[q][1];
+                        const double lat[3] = { 1.0 - xi - eta, xi, eta };
+                        double       c[3], u[3][3];
+                        for ( int k = 0; k < 3; ++k )
+                            c[k] = p[0][k] + xi * a[k] + eta * b[k];
+                        cross( b, c, u[1] );
+                        cross( c, a, u[2] );
+                        for ( int k = 0; k < 3; ++k )
+                            u[0][k] = -( u[1][k] + u[2][k] );
+                        for ( int ic = 0; ic < 3; ++ic )
+                        {
+                            const double lc = kCoarseLat[ic][flat][0] + kCoarseLat[ic][flat][1] * xi +
+                                              kCoarseLat[ic][flat][2] * eta;
+                            for ( int mm = 0; mm < 3; ++mm )
+                            {
+                                for ( int k = 0; k < 3; ++k )
+                                    g[( ic * 3 + mm ) * 3 + k] += sig * lc * u[mm][k];
+                                g[30 + ic * 3 + mm] += lc * lat[mm];
+                            }
+                        }
+                    }
+                    for ( int k = 0; k < 3; ++k )
+                        g[27 + k] = sig * v[k];
+                }
+}
+
+const double* stokes_geometry( const tn_mesh* m )
+{
+    tn_mesh*                      mm = const_cast< tn_mesh* >( m );
+    std::lock_guard< std::mutex > lock( mm->geom_mutex );
+    if ( !mm->d_stokes_geom )
+    {
+        std::vector< double > G;
+        build_stokes_geometry( m, G );
+        double* ptr = nullptr;
+        if ( cudaMalloc( &ptr, G.size() * sizeof( double ) ) != cudaSuccess )
+            return nullptr;
+        if ( cudaMemcpy( ptr, G.data(), G.size() * sizeof( double ), cudaMemcpyHostToDevice ) != cudaSuccess )
+        {
+            cudaFree( ptr );
+            return nullptr;
+        }
+        mm->d_stokes_geom = ptr;
+    }
+    return mm->d_stokes_geom;
 }
 
 template < typename T >
@@ -324,7 +390,12 @@ int divergence_apply( const tn_mesh* f, const tn_mesh* c, int bc_cmb, int bc_sur
     TN_CHECK_ARG( u && u[0] && u[1] && u[2] && p, "divergence: null vector" );
     if ( apply_mode == TN_APPLY_REPLACE )
         TN_CUDA_TRY( cudaMemsetAsync( p, 0, c->ns * sizeof( T ), st ) );
-    StokesParams< T > P{ f->N, f->n1, c->n1, f->d_coords, radii_of< T >( f ), bc_cmb, bc_surf };
+    StokesParams< T > P{ f->N, f->n1, c->n1, f->d_coords, stokes_geometry( f ), radii_of< T >( f ), bc_cmb, bc_surf };
+    if ( !P.geom )
+    {
+        set_error( "stokes block: allocating the lateral quadrature table failed" );
+        return TN_ERR_NOMEM;
+    }
     const long long   cells = (long long) kDiamonds * f->N * f->N * f->N;
     divergence_kernel< T ><<< unsigned( ( cells + 127 ) / 128 ), 128, 0, st >>>( P, Ptr3< const T >{ { u[0], u[1], u[2] } },
                                                                                 p );
@@ -348,7 +419,12 @@ int gradient_apply( const tn_mesh* f, const tn_mesh* c, int bc_cmb, int bc_surf,
     if ( apply_mode == TN_APPLY_REPLACE )
         for ( int i = 0; i < 3; ++i )
             TN_CUDA_TRY( cudaMemsetAsync( u[i], 0, f->ns * sizeof( T ), st ) );
-    StokesParams< T > P{ f->N, f->n1, c->n1, f->d_coords, radii_of< T >( f ), bc_cmb, bc_surf };
+    StokesParams< T > P{ f->N, f->n1, c->n1, f->d_coords, stokes_geometry( f ), radii_of< T >( f ), bc_cmb, bc_surf };
+    if ( !P.geom )
+    {
+        set_error( "stokes block: allocating the lateral quadrature table failed" );
+        return TN_ERR_NOMEM;
+    }
     const long long   cells = (long long) kDiamonds * f->N * f->N * f->N;
     gradient_kernel< T ><<< unsigned( ( cells + 127 ) / 128 ), 128, 0, st >>>( P, p, Ptr3< T >{ { u[0], u[1], u[2] } } );
     TN_LAUNCH_CHECK();

@@ -395,10 +395,11 @@ class StokesSolver:
     def __init__(self, level, viscosity, mg_levels=4, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=True,
                  chebyshev_order=3, smoothing_steps=2, power_iterations=10, vcycles=1, coarse_max_iterations=50,
                  coarse_relative_tolerance=1e-6, restart=30, max_iterations=200, relative_tolerance=1e-8,
-                 absolute_tolerance=1e-30, r_min=0.55, r_max=1.0, gca=0, outer=0):
+                 absolute_tolerance=1e-30, r_min=0.55, r_max=1.0, gca=0, outer=0, eager=False):
         self.prm = C.StokesParams(level, mg_levels, bc_cmb, bc_surface, int(mg_fp32), chebyshev_order, smoothing_steps,
                                   power_iterations, vcycles, coarse_max_iterations, coarse_relative_tolerance, restart,
-                                  max_iterations, relative_tolerance, absolute_tolerance, int(gca), int(outer))
+                                  max_iterations, relative_tolerance, absolute_tolerance, int(gca), int(outer),
+                                  int(eager))
         h = ctypes.c_void_p()
         C.check(C.lib().tn_stokes_solver_create(ctypes.byref(self.prm), r_min, r_max,
                                                 ctypes.c_void_p(viscosity.data.data_ptr()), ctypes.byref(h)),

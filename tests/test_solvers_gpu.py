@@ -107,6 +107,33 @@ def test_stokes_fp32_mg_matches_fp64_mg(stokes_case):
     assert rel(sols[1], sols[0]) <= 1e-8
 
 
+@pytest.mark.parametrize("outer", [0, 1])
+def test_stokes_graph_replay_matches_eager(stokes_case, outer):
+    """The preconditioner replayed from captured CUDA graphs solves like the kernel-by-kernel one, over
+    several restarts and a second solve that reuses the graphs.  The cell kernels accumulate with atomics,
+    so two solves agree to rounding, not bit for bit."""
+    from terraneo_b200 import shell
+    L, of, oc, k, f = stokes_case
+    pf, pc = shell.ShellMesh(L), shell.ShellMesh(L - 1)
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(k)
+    fu, fp = prepared_rhs(shell, pf, f, (1, 1)), shell.VectorQ1Scalar(pc)
+    out = []
+    for eager in (True, False):
+        s = shell.StokesSolver(L, kv, mg_levels=3, bc_cmb=1, bc_surface=1, mg_fp32=True, gca=1,
+                               relative_tolerance=1e-9, max_iterations=400, restart=8, outer=outer, eager=eager)
+        res = []
+        for _ in range(2):
+            xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+            it, rr = s.solve(fu, fp, xu, xp)
+            res.append((it, rr, xu.numpy(), xp.numpy()))
+        out.append(res)
+    for (ie, re, ue, pe), (ig, rg, ug, pg) in zip(*out):
+        assert re <= 1e-9 and rg <= 1e-9
+        assert abs(ie - ig) <= max(3, ie // 50)
+        assert rel(ug, ue) <= 1e-7 and rel(pg, pe) <= 1e-6
+
+
 @pytest.mark.parametrize("smoother", [0, 1])
 @pytest.mark.parametrize("with_k", [False, True])
 def test_divkgrad_multigrid_pcg(smoother, with_k):
