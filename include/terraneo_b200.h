@@ -108,12 +108,13 @@ TN_API int tn_epsdivdiv_apply_f32( const tn_mesh* mesh, const tn_epsdivdiv_param
  *
  * Storage: DIMENSIONWISE local order (local node + 6 * dimension).  The
  * matrices are symmetric and only the upper triangle is stored, row by row:
- * entry (I, J), I <= J, is entry e = 18 I - I (I - 1) / 2 + J - I of 171.
- * Wedges are numbered w = 2 cell + wedge with cells (diamond, x, y, r), r
- * fastest, and 32 consecutive wedges are interleaved entry by entry: entry e
- * of wedge w lives at ((w / 32) * 171 + e) * 32 + w % 32.
+ * entry (I, J), I <= J, is entry e = 18 I - I (I - 1) / 2 + J - I of 171,
+ * followed by one zero padding entry (172 per wedge).  Wedges are numbered
+ * w = 2 cell + wedge with cells (diamond, x, y, r), r fastest, and 32
+ * consecutive wedges are interleaved in chunks of 4 entries: entry e of
+ * wedge w lives at (((w / 32) * 43 + e / 4) * 32 + w % 32) * 4 + e % 4.
  * tn_local_matrix_count gives the number of entries (2 * 10 N^3 wedges padded
- * to a multiple of 32, times 171; FP64 about 2,736 bytes per cell, the
+ * to a multiple of 32, times 172; FP64 about 2,752 bytes per cell, the
  * reference stores the full 5,184). */
 TN_API int tn_local_matrix_count( const tn_mesh* mesh, size_t* entries );
 /* kerngen assemble_local_matrix (:2051-2110) of every wedge: one-point rule,

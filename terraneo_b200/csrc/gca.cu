@@ -13,17 +13,19 @@
 //
 // Storage: the wedge matrices are symmetric (the kerngen form and every
 // P^T A P of it) and only the upper triangle is kept, row by row (entry
-// (I, J), I <= J, is entry e = 18 I - I (I - 1) / 2 + J - I of 171).  Wedges
-// are numbered w = 2 cell + wedge (cells (d, x, y, r), r fastest) and 32
-// consecutive wedges are interleaved: entry e of wedge w at
-// ((w / 32) 171 + e) 32 + w % 32.  FP64 2,736 B per cell.
+// (I, J), I <= J, is entry e = 18 I - I (I - 1) / 2 + J - I of 171, plus
+// one zero padding entry).  Wedges are numbered w = 2 cell + wedge (cells
+// (d, x, y, r), r fastest) and 32 consecutive wedges are interleaved in
+// chunks of 4 entries: entry e of wedge w at
+// (((w / 32) 43 + e / 4) 32 + w % 32) 4 + e % 4.  FP64 2,752 B per cell.
 //
 // Coarsening: one 324-thread block per coarse cell, thread t owning entry
 // (t / 18, t % 18) of both coarse wedges; the interpolation matrices (and, at
 // the finest level, the fine wedges' geometry) of all 16 fine wedges are staged
 // in shared memory once, then per fine wedge T = A_f P and C += P^T T are two
-// 6-term passes.  Apply: one thread per wedge streams its 171 values (each
-// warp load is 32 consecutive values) and uses the symmetry.
+// 6-term passes.  Apply: one thread per wedge streams its 43 chunks with
+// vector loads (each warp load is 32 x 4 consecutive values) and uses the
+// symmetry.
 #include "common.cuh"
 #include "wedge.cuh"
 
@@ -39,12 +41,15 @@ namespace {
 constexpr int kM          = 324; // entries of an 18 x 18 matrix
 constexpr int kP          = 171; // stored entries of a symmetric 18 x 18 matrix
 
-// Position of entry e of wedge w (w = 2 cell + wedge) in a stored array:
-// 32 consecutive wedges are interleaved entry by entry, so a warp with one
-// thread per wedge reads 32 consecutive values per entry.
-__device__ __forceinline__ size_t stored_pos( long long w, int e )
+constexpr int kChunks     = 43;  // 4-entry chunks of a wedge (172 entries, the last one padding)
+
+// Position of entry e of wedge w (w = 2 cell + wedge) in a stored array: 32
+// consecutive wedges are interleaved in chunks of 4 entries, so a warp with
+// one thread per wedge reads one 4-entry chunk per thread and 32 x 4
+// consecutive values per vector load.
+__host__ __device__ __forceinline__ size_t stored_pos( long long w, int e )
 {
-    return ( size_t( w >> 5 ) * 171 + e ) * 32 + size_t( w & 31 );
+    return ( ( size_t( w >> 5 ) * kChunks + size_t( e >> 2 ) ) * 32 + size_t( w & 31 ) ) * 4 + size_t( e & 3 );
 }
 
 // position of entry (I, J) in the packed upper triangle
@@ -185,6 +190,8 @@ __global__ void __launch_bounds__( 64 ) local_matrices_kernel( int N, const doub
         const int w = e / kM, I = ( e % kM ) / 18, J = ( e % kM ) % 18;
         if ( I <= J )
             mats[stored_pos( cell * 2 + w, packed( I, J ) )] = kerngen_entry( sg[w], skw[w], I, J );
+        if ( I == 17 && J == 17 )
+            mats[stored_pos( cell * 2 + w, kP )] = 0.0; // padding entry
     }
 }
 
@@ -265,7 +272,39 @@ __global__ void __launch_bounds__( kGcaThreads ) gca_coarsen_kernel( int Nf, con
     {
         mats_c[stored_pos( cell * 2 + 0, packed( I, J ) )] = acc0;
         mats_c[stored_pos( cell * 2 + 1, packed( I, J ) )] = acc1;
+        if ( I == 17 && J == 17 )
+            mats_c[stored_pos( cell * 2 + 0, kP )] = mats_c[stored_pos( cell * 2 + 1, kP )] = 0.0;
     }
+}
+
+__device__ __forceinline__ void load4( const float* p, float v[4] )
+{
+    const float4 q = __ldg( reinterpret_cast< const float4* >( p ) );
+    v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+}
+__device__ __forceinline__ void load4( const double* p, double v[4] )
+{
+    const double2 a = __ldg( reinterpret_cast< const double2* >( p ) );
+    const double2 b = __ldg( reinterpret_cast< const double2* >( p ) + 1 );
+    v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+}
+
+// outward unit normal at a lateral node (x / |x|, in the precision of the
+// apply; one reciprocal square root instead of a root and three divisions)
+__device__ __forceinline__ void unit_normal_of( const double* __restrict__ coords, int n1, int d, int X, int Y,
+                                                double n[3] )
+{
+    const double* c  = coords + lat_index( n1, d, X, Y ) * 3;
+    const double  im = rsqrt( c[0] * c[0] + c[1] * c[1] + c[2] * c[2] );
+    n[0] = c[0] * im, n[1] = c[1] * im, n[2] = c[2] * im;
+}
+__device__ __forceinline__ void unit_normal_of( const double* __restrict__ coords, int n1, int d, int X, int Y,
+                                                float n[3] )
+{
+    const double* c  = coords + lat_index( n1, d, X, Y ) * 3;
+    const float   c0 = float( c[0] ), c1 = float( c[1] ), c2 = float( c[2] );
+    const float   im = rsqrtf( c0 * c0 + c1 * c1 + c2 * c2 );
+    n[0] = c0 * im, n[1] = c1 * im, n[2] = c2 * im;
 }
 
 template < typename T >
@@ -283,12 +322,9 @@ struct StoredParams
 // in with compile-time offsets (fully unrolled), each contributing to rows I
 // and J by symmetry; the boundary treatment follows the slow path.
 template < typename T, bool DIAG >
-__global__ void __launch_bounds__( 128 ) stored_apply_kernel( StoredParams< T > P )
+__device__ __forceinline__ void stored_wedge( const StoredParams< T >& P, long long gw )
 {
-    const long long gw = blockIdx.x * (long long) blockDim.x + threadIdx.x;
     const int       N = P.N, n1 = P.n1;
-    if ( gw >= 2LL * kDiamonds * N * N * N )
-        return;
     const long long cell = gw >> 1;
     const int       w    = int( gw & 1 );
     const int r = int( cell % N ), y = int( ( cell / N ) % N ), x = int( ( cell / ( (long long) N * N ) ) % N );
@@ -324,7 +360,7 @@ __global__ void __launch_bounds__( 128 ) stored_apply_kernel( StoredParams< T > 
             sn[q] = nrm[q][0] * s[n] + nrm[q][1] * s[n + 6] + nrm[q][2] * s[n + 12];
         }
     }
-    const T* gm = P.mats + ( size_t( gw >> 5 ) * kP ) * 32 + size_t( gw & 31 );
+    const T* gm = P.mats + stored_pos( gw, 0 ); // chunk c at gm + 128 c
     T        yv[18];
 #pragma unroll
     for ( int I = 0; I < 18; ++I )
@@ -353,12 +389,20 @@ __global__ void __launch_bounds__( 128 ) stored_apply_kernel( StoredParams< T > 
                 }
         }
         T ann[3] = { 0, 0, 0 };
+        constexpr int kRing = 8; // vector-register ring, each chunk loaded kRing chunks ahead
+        T             ring[kRing][4];
+#pragma unroll
+        for ( int c = 0; c < kRing; ++c )
+            load4( gm + 128 * c, ring[c] );
 #pragma unroll
         for ( int I = 0; I < 18; ++I )
 #pragma unroll
             for ( int J = I; J < 18; ++J )
             {
-                const T   v  = gm[size_t( 18 * I - ( I * ( I - 1 ) ) / 2 + J - I ) * 32];
+                const int e = 18 * I - ( I * ( I - 1 ) ) / 2 + J - I;
+                const T   v = ring[( e >> 2 ) % kRing][e & 3];
+                if ( ( e & 3 ) == 3 && ( e >> 2 ) + kRing < kChunks )
+                    load4( gm + 128 * ( ( e >> 2 ) + kRing ), ring[( e >> 2 ) % kRing] );
                 const int ni = I % 6, nj = J % 6, a = I / 6, b = J / 6;
                 bool      keep = true;
                 if ( dir )
@@ -416,7 +460,8 @@ __global__ void __launch_bounds__( 128 ) stored_apply_kernel( StoredParams< T > 
                 const int ni = I % 6, nj = J % 6;
                 if ( ni != nj )
                     continue;
-                const T   v = gm[size_t( 18 * I - ( I * ( I - 1 ) ) / 2 + J - I ) * 32];
+                const int e = 18 * I - ( I * ( I - 1 ) ) / 2 + J - I;
+                const T   v = gm[128 * ( e >> 2 ) + ( e & 3 )];
                 const int a = I / 6, b = J / 6;
                 if ( I == J )
                     yv[I] = v * s[I];
@@ -467,6 +512,164 @@ __global__ void __launch_bounds__( 128 ) stored_apply_kernel( StoredParams< T > 
             atomicAdd( P.dst.p[a] + idx[n], yv[n + 6 * a] );
 }
 
+// Diagonal mode, every wedge.
+template < typename T >
+__global__ void __launch_bounds__( 128 ) stored_diag_kernel( StoredParams< T > P )
+{
+    const long long gw = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if ( gw < 2LL * kDiamonds * P.N * P.N * P.N )
+        stored_wedge< T, true >( P, gw );
+}
+
+// Non-diagonal apply, one thread per wedge.  The 43 chunks stream through a
+// ring of kRing vector registers, each loaded kRing chunks ahead of its use,
+// so every warp keeps kRing x 512 (FP32) or 1024 (FP64) bytes in flight.
+// The boundary treatment of the slow path is expressed around the plain
+// symmetric product, so every lane runs the same instruction stream:
+//  * Dirichlet: the boundary-node inputs are zeroed, so interior rows see
+//    only interior couplings, and afterwards the boundary rows are replaced
+//    by their diagonal entry times the input;
+//  * free-slip: the boundary-node inputs enter with their tangential part,
+//    the boundary rows are projected on the tangent plane afterwards and
+//    get n (n^T A_nn n)(n . s) back, A_nn the node's 3x3 block.
+// The diagonal blocks of the three boundary-side nodes are picked up from
+// the stream as it passes (compile-time positions, runtime side select).
+template < typename T >
+__global__ void __launch_bounds__( 128, sizeof( T ) == 4 ? 5 : 2 ) stored_apply_kernel( StoredParams< T > P )
+{
+    const long long gw = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    const int       N = P.N, n1 = P.n1;
+    if ( gw >= 2LL * kDiamonds * N * N * N )
+        return;
+    const long long cell = gw >> 1;
+    const int       w    = int( gw & 1 );
+    const int r = int( cell % N ), y = int( ( cell / N ) % N ), x = int( ( cell / ( (long long) N * N ) ) % N );
+    const int d = int( cell / ( (long long) N * N * N ) );
+    const int bcf = r == 0 ? P.bc_cmb : ( r == N - 1 ? P.bc_surf : TN_BC_NEUMANN );
+    const bool top = r != 0; // boundary-side nodes 3..5 (SURFACE) rather than 0..2 (CMB)
+    const bool dir = bcf == TN_BC_DIRICHLET, fs = bcf == TN_BC_FREESLIP;
+
+    T sv[18], yv[18], sn[3] = { 0, 0, 0 };
+#pragma unroll
+    for ( int n = 0; n < 6; ++n )
+    {
+        const size_t i = lat_index( n1, d, x + kWedgeNode[w][n][0], y + kWedgeNode[w][n][1] ) * n1 + r +
+                         kWedgeNode[w][n][2];
+#pragma unroll
+        for ( int a = 0; a < 3; ++a )
+            sv[n + 6 * a] = P.src.p[a][i];
+    }
+    // boundary-side node q of the wedge is node q + 3 top (nodes q and q + 3
+    // share the lateral position); selects keep every index compile-time
+    if ( dir || fs )
+    {
+#pragma unroll
+        for ( int q = 0; q < 3; ++q )
+        {
+            T nn[3] = { 0, 0, 0 };
+            if ( fs )
+                unit_normal_of( P.coords, n1, d, x + kWedgeNode[w][q][0], y + kWedgeNode[w][q][1], nn );
+            T b3[3];
+#pragma unroll
+            for ( int a = 0; a < 3; ++a )
+                b3[a] = top ? sv[q + 3 + 6 * a] : sv[q + 6 * a];
+            sn[q] = nn[0] * b3[0] + nn[1] * b3[1] + nn[2] * b3[2];
+#pragma unroll
+            for ( int a = 0; a < 3; ++a )
+            {
+                const T t = dir ? T( 0 ) : b3[a] - sn[q] * nn[a];
+                if ( top )
+                    sv[q + 3 + 6 * a] = t;
+                else
+                    sv[q + 6 * a] = t;
+            }
+        }
+    }
+#pragma unroll
+    for ( int I = 0; I < 18; ++I )
+        yv[I] = T( 0 );
+    T blk[3][6]; // boundary-side node q: (a, b) = 00 01 02 11 12 22
+#pragma unroll
+    for ( int q = 0; q < 3; ++q )
+#pragma unroll
+        for ( int i = 0; i < 6; ++i )
+            blk[q][i] = T( 0 );
+    const T*      gm    = P.mats + stored_pos( gw, 0 ); // chunk c at gm + 128 c
+    constexpr int kRing = 8;
+    T             ring[kRing][4];
+#pragma unroll
+    for ( int c = 0; c < kRing; ++c )
+        load4( gm + 128 * c, ring[c] );
+#pragma unroll
+    for ( int I = 0; I < 18; ++I )
+#pragma unroll
+        for ( int J = I; J < 18; ++J )
+        {
+            const int e = 18 * I - ( I * ( I - 1 ) ) / 2 + J - I;
+            const T   v = ring[( e >> 2 ) % kRing][e & 3];
+            if ( ( e & 3 ) == 3 && ( e >> 2 ) + kRing < kChunks )
+                load4( gm + 128 * ( ( e >> 2 ) + kRing ), ring[( e >> 2 ) % kRing] );
+            yv[I] += v * sv[J];
+            if ( I != J )
+                yv[J] += v * sv[I];
+            if ( I % 6 == J % 6 )
+            {
+                const int n = I % 6, a = I / 6, b = J / 6;
+                const int ab = a == 0 ? b : ( a == 1 ? 2 + b : 5 );
+                if ( ( n >= 3 ) == top )
+                    blk[n % 3][ab] = v;
+            }
+        }
+    if ( dir || fs )
+    {
+#pragma unroll
+        for ( int q = 0; q < 3; ++q )
+        {
+            const T* B = blk[q];
+            T        y3[3];
+#pragma unroll
+            for ( int a = 0; a < 3; ++a )
+                y3[a] = top ? yv[q + 3 + 6 * a] : yv[q + 6 * a];
+            if ( dir )
+            {
+                const int    X = x + kWedgeNode[w][q][0], Y = y + kWedgeNode[w][q][1];
+                const size_t i = lat_index( n1, d, X, Y ) * n1 + r + ( top ? 1 : 0 );
+                y3[0]          = B[0] * P.src.p[0][i];
+                y3[1]          = B[3] * P.src.p[1][i];
+                y3[2]          = B[5] * P.src.p[2][i];
+            }
+            else
+            {
+                T nn[3];
+                unit_normal_of( P.coords, n1, d, x + kWedgeNode[w][q][0], y + kWedgeNode[w][q][1], nn );
+                const T ann = nn[0] * nn[0] * B[0] + nn[1] * nn[1] * B[3] + nn[2] * nn[2] * B[5] +
+                              T( 2 ) * ( nn[0] * nn[1] * B[1] + nn[0] * nn[2] * B[2] + nn[1] * nn[2] * B[4] );
+                const T yn = nn[0] * y3[0] + nn[1] * y3[1] + nn[2] * y3[2];
+#pragma unroll
+                for ( int a = 0; a < 3; ++a )
+                    y3[a] += ( ann * sn[q] - yn ) * nn[a];
+            }
+#pragma unroll
+            for ( int a = 0; a < 3; ++a )
+            {
+                if ( top )
+                    yv[q + 3 + 6 * a] = y3[a];
+                else
+                    yv[q + 6 * a] = y3[a];
+            }
+        }
+    }
+#pragma unroll
+    for ( int n = 0; n < 6; ++n )
+    {
+        const size_t i = lat_index( n1, d, x + kWedgeNode[w][n][0], y + kWedgeNode[w][n][1] ) * n1 + r +
+                         kWedgeNode[w][n][2];
+#pragma unroll
+        for ( int a = 0; a < 3; ++a )
+            atomicAdd( P.dst.p[a] + i, yv[n + 6 * a] );
+    }
+}
+
 __global__ void cast_array_kernel( size_t n, const double* __restrict__ src, float* __restrict__ dst )
 {
     for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < n; i += size_t( gridDim.x ) * blockDim.x )
@@ -496,9 +699,11 @@ int stored_apply( const tn_mesh* m, const T* mats, const tn_epsdivdiv_params* p,
     P.bc_cmb = p->bc_cmb, P.bc_surf = p->bc_surface, P.diag = p->diagonal != 0;
     const long long wedges = 2LL * kDiamonds * m->N * m->N * m->N;
     if ( p->diagonal )
-        stored_apply_kernel< T, true ><<< unsigned( ( wedges + 127 ) / 128 ), 128, 0, st >>>( P );
+        stored_diag_kernel< T ><<< unsigned( ( wedges + 127 ) / 128 ), 128, 0, st >>>( P );
     else
-        stored_apply_kernel< T, false ><<< unsigned( ( wedges + 127 ) / 128 ), 128, 0, st >>>( P );
+    {
+        stored_apply_kernel< T ><<< unsigned( ( wedges + 127 ) / 128 ), 128, 0, st >>>( P );
+    }
     TN_LAUNCH_CHECK();
     if ( !p->diagonal && p->bc_cmb == TN_BC_FREESLIP && p->bc_surface == TN_BC_FREESLIP )
     {
@@ -519,7 +724,7 @@ extern "C" int tn_local_matrix_count( const tn_mesh* m, size_t* entries )
 {
     TN_CHECK_ARG( m && entries, "tn_local_matrix_count: null argument" );
     const size_t wedges = size_t( kDiamonds ) * m->N * m->N * m->N * 2;
-    *entries            = ( ( wedges + 31 ) / 32 ) * 32 * kP; // padded to whole groups of 32 wedges
+    *entries            = ( ( wedges + 31 ) / 32 ) * 32 * kChunks * 4; // whole groups of 32 wedges, 172 entries each
     return TN_OK;
 }
 

@@ -17,12 +17,14 @@ _IU = np.triu_indices(18)
 
 def _colmajor(m):
     """oracle layout [cells][2][18][18] -> the library's layout: packed upper triangles (171 per
-    wedge, wedge w = 2 cell + wedge) with 32 consecutive wedges interleaved entry by entry"""
+    wedge plus one zero, wedge w = 2 cell + wedge) with 32 consecutive wedges interleaved in chunks
+    of 4 entries"""
     p = m[..., _IU[0], _IU[1]].reshape(-1, 171)
+    p = np.concatenate([p, np.zeros((p.shape[0], 1))], axis=1)
     nw = p.shape[0]
     pad = (-nw) % 32
-    p = np.concatenate([p, np.zeros((pad, 171))])
-    return np.ascontiguousarray(p.reshape(-1, 32, 171).transpose(0, 2, 1)).reshape(-1)
+    p = np.concatenate([p, np.zeros((pad, 172))])
+    return np.ascontiguousarray(p.reshape(-1, 32, 43, 4).transpose(0, 2, 1, 3)).reshape(-1)
 
 
 @pytest.fixture(scope="module")
