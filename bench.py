@@ -172,7 +172,7 @@ def laplace_cg_leg(shell, torch, level=5, seed=2026, reference=True):
 
 def stokes_leg(shell, C, torch, k_np):
     """Level-6 free-slip Stokes solve to 1e-8: FP32-multigrid vs FP64-multigrid
-    preconditioner (FGMRES(50) outer in FP64, block-triangular preconditioner,
+    preconditioner (FGMRES(100) outer in FP64, block-triangular preconditioner,
     4-level V-cycle with Chebyshev order 3, coarse PCG in FP64)."""
     pf, pc = shell.ShellMesh(LEVEL, RMIN, RMAX), shell.ShellMesh(LEVEL - 1, RMIN, RMAX)
     coords, radii = pf.geometry()
@@ -181,7 +181,7 @@ def stokes_leg(shell, C, torch, k_np):
     fu, fp = stokes_rhs(shell, pf, coords, radii), shell.VectorQ1Scalar(pc)
     fnorm = np.sqrt(shell.dot(fu, fu))
     out = {"workload": "Stokes solve, velocity level 6 / pressure level 5, free-slip both radii, 1e4 viscosity "
-                       "contrast, buoyancy RHS (Ra 1e5), FGMRES(50) + block-triangular preconditioner, V-cycle over "
+                       "contrast, buoyancy RHS (Ra 1e5), FGMRES(100) + block-triangular preconditioner, V-cycle over "
                        "levels 3-6 (Chebyshev order 3, 2 smoothing steps, GCA coarse operators with constant "
                        "interpolation, coarse PCG FP64 50 its / 1e-6), "
                        "stop at 1e-8 relative FP64 residual"}
@@ -189,7 +189,7 @@ def stokes_leg(shell, C, torch, k_np):
     for tag, mg32 in (("fp32_mg", True), ("fp64_mg", False)):
         s = shell.StokesSolver(LEVEL, kv, mg_levels=4, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP,
                                mg_fp32=mg32, chebyshev_order=3, relative_tolerance=1e-8, max_iterations=1000,
-                               restart=50, r_min=RMIN, r_max=RMAX, gca=1)
+                               restart=100, r_min=RMIN, r_max=RMAX, gca=1)
         xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
         s.solve(fu, fp, xu, xp)  # warm-up: eigenvalue estimates, first-touch
         xu.data.zero_()

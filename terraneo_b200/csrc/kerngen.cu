@@ -784,33 +784,54 @@ struct Mat3
     double a[9];
 };
 
+// <m_j, u> over owned nodes for the three rotation modes m_j = e_j x x.
+// Flat grid-stride loop over stored nodes (coalesced src loads, several
+// independent nodes in flight per thread); lateral data (ownership, unit
+// coordinates) and radii come from L1.
 template < typename T >
-__global__ void penalty_dots_kernel( size_t nlat, int n1, const double* __restrict__ coords, const T* __restrict__ radii,
-                                     Ptr3< const T > src, const uint8_t* __restrict__ lat_owned, double* partials,
-                                     unsigned int* counter, double* result )
+__global__ void __launch_bounds__( 256 ) penalty_dots_kernel( size_t ns, int n1, const double* __restrict__ coords,
+                                                              const T* __restrict__ radii, Ptr3< const T > src,
+                                                              const uint8_t* __restrict__ lat_owned, double* partials,
+                                                              unsigned int* counter, double* result )
 {
-    // one warp per lateral column (owned columns only), lanes along r
-    Neumaier     acc[3];
-    const int    lane = threadIdx.x & 31;
-    const size_t wid = ( blockIdx.x * size_t( blockDim.x ) + threadIdx.x ) >> 5;
-    const size_t nw  = ( size_t( gridDim.x ) * blockDim.x ) >> 5;
-    for ( size_t lat = wid; lat < nlat; lat += nw )
+    // plain double sums per thread (a few nodes each), compensated sums
+    // across threads and blocks
+    double       sum[3] = { 0.0, 0.0, 0.0 };
+    const size_t stride = size_t( gridDim.x ) * blockDim.x;
+    constexpr int kU    = 4;
+    for ( size_t i0 = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i0 < ns; i0 += kU * stride )
     {
-        if ( !lat_owned[lat] )
-            continue;
-        const int     d = int( lat / ( size_t( n1 ) * n1 ) );
-        const double* u = coords + lat * 3;
-        for ( int r = lane; r < n1; r += 32 )
+        T        v[kU][3];
+        unsigned lat[kU];
+        int      rr[kU];
+#pragma unroll
+        for ( int u = 0; u < kU; ++u )
         {
-            const size_t i  = lat * n1 + r;
-            const double rr = double( radii[d * n1 + r] );
-            const double x[3] = { u[0] * rr, u[1] * rr, u[2] * rr };
-            const double v[3] = { double( src.p[0][i] ), double( src.p[1][i] ), double( src.p[2][i] ) };
-            acc[0].add( x[1] * v[2] - x[2] * v[1] );
-            acc[1].add( x[2] * v[0] - x[0] * v[2] );
-            acc[2].add( x[0] * v[1] - x[1] * v[0] );
+            const size_t i = i0 + u * stride;
+            lat[u]         = i < ns ? unsigned( i ) / unsigned( n1 ) : 0u; // ns < 2^32 at every level tn_mesh_create accepts (<= 9)
+            rr[u]          = i < ns ? int( unsigned( i ) - lat[u] * unsigned( n1 ) ) : 0;
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+                v[u][c] = i < ns ? src.p[c][i] : T( 0 );
+        }
+#pragma unroll
+        for ( int u = 0; u < kU; ++u )
+        {
+            if ( i0 + u * stride >= ns || !lat_owned[lat[u]] )
+                continue;
+            const int     d   = int( lat[u] / unsigned( n1 * n1 ) );
+            const double* cu  = coords + size_t( lat[u] ) * 3;
+            const double  rad = double( radii[d * n1 + rr[u]] );
+            const double  x0 = cu[0] * rad, x1 = cu[1] * rad, x2 = cu[2] * rad;
+            const double  w0 = double( v[u][0] ), w1 = double( v[u][1] ), w2 = double( v[u][2] );
+            sum[0] += x1 * w2 - x2 * w1;
+            sum[1] += x2 * w0 - x0 * w2;
+            sum[2] += x0 * w1 - x1 * w0;
         }
     }
+    Neumaier acc[3];
+    for ( int k = 0; k < 3; ++k )
+        acc[k].add( sum[k] );
     block_sum_finish< 3 >( acc, partials, counter, result );
 }
 
@@ -829,11 +850,11 @@ __global__ void penalty_axpy_kernel( size_t ns, int n1, const double* __restrict
     const double b[3] = { beta[0], beta[1], beta[2] };
     for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
     {
-        const size_t  lat = i / n1;
-        const int     r   = int( i - lat * n1 );
-        const int     d   = int( lat / ( size_t( n1 ) * n1 ) );
+        const unsigned lat = unsigned( i ) / unsigned( n1 ); // ns < 2^32 at every level tn_mesh_create accepts (<= 9)
+        const int      r   = int( unsigned( i ) - lat * unsigned( n1 ) );
+        const int      d   = int( lat / unsigned( n1 * n1 ) );
         const double  rr  = double( radii[d * n1 + r] );
-        const double* u   = coords + lat * 3;
+        const double* u   = coords + size_t( lat ) * 3;
         const double  x[3] = { u[0] * rr, u[1] * rr, u[2] * rr };
         dst.p[0][i] += T( b[1] * x[2] - b[2] * x[1] );
         dst.p[1][i] += T( b[2] * x[0] - b[0] * x[2] );
@@ -885,8 +906,8 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
         Mat3 gi;
         for ( int i = 0; i < 9; ++i )
             gi.a[i] = m->penalty_gram_inv[i];
-        const unsigned blocks = unsigned( std::min< size_t >( ( m->nlat + 7 ) / 8, kRedMaxBlocks ) );
-        penalty_dots_kernel< T ><<< blocks, 256, 0, st >>>( m->nlat, m->n1, m->d_coords, mesh_radii< T >( m ), s,
+        const unsigned blocks = unsigned( std::min< size_t >( ( m->ns + 1023 ) / 1024, kRedMaxBlocks ) );
+        penalty_dots_kernel< T ><<< blocks, 256, 0, st >>>( m->ns, m->n1, m->d_coords, mesh_radii< T >( m ), s,
                                                            m->d_lat_owned, m->d_red_partials,
                                                            m->d_red_counter, m->d_red_result );
         TN_LAUNCH_CHECK();
@@ -970,8 +991,8 @@ int fsfs_penalty_add( const tn_mesh* m, double eps, const T* const* src, T* cons
     Mat3            gi;
     for ( int i = 0; i < 9; ++i )
         gi.a[i] = m->penalty_gram_inv[i];
-    const unsigned blocks = unsigned( std::min< size_t >( ( m->nlat + 7 ) / 8, kRedMaxBlocks ) );
-    penalty_dots_kernel< T ><<< blocks, 256, 0, st >>>( m->nlat, m->n1, m->d_coords, mesh_radii< T >( m ), s,
+    const unsigned blocks = unsigned( std::min< size_t >( ( m->ns + 1023 ) / 1024, kRedMaxBlocks ) );
+    penalty_dots_kernel< T ><<< blocks, 256, 0, st >>>( m->ns, m->n1, m->d_coords, mesh_radii< T >( m ), s,
                                                        m->d_lat_owned, m->d_red_partials, m->d_red_counter,
                                                        m->d_red_result );
     TN_LAUNCH_CHECK();
