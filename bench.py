@@ -39,6 +39,127 @@ BYTES_PER_NODE_F32 = 28
 TILE_TRAFFIC_BYTES = 126152192 + 39593216
 
 
+def _case_laplace6(shell, C, torch):
+    m = shell.ShellMesh(6, RMIN, RMAX)
+    s, d = shell.VectorQ1Scalar(m), shell.VectorQ1Scalar(m)
+    s.data.uniform_(-1, 1)
+    op = shell.Laplace(m, True)
+    return {"Laplace apply, level 6, Dirichlet elimination": lambda: shell.apply(op, s, d)}
+
+
+def _case_vlaplace6(shell, C, torch):
+    m = shell.ShellMesh(6, RMIN, RMAX)
+    u, v = shell.VectorQ1Vec(m), shell.VectorQ1Vec(m)
+    u.data.uniform_(-1, 1)
+    op = shell.VectorLaplace(m, C.BC_DIRICHLET, C.BC_DIRICHLET)
+    return {"VectorLaplace apply, level 6, Dirichlet": lambda: shell.apply(op, u, v)}
+
+
+def _case_divkgrad6(shell, C, torch):
+    m = shell.ShellMesh(6, RMIN, RMAX)
+    s, d, k = shell.VectorQ1Scalar(m), shell.VectorQ1Scalar(m), shell.VectorQ1Scalar(m)
+    s.data.uniform_(-1, 1)
+    k.data.uniform_(1, 10)
+    op = shell.DivKGrad(m, k, True)
+    return {"DivKGrad apply (3x2 rule), level 6, Dirichlet elimination": lambda: shell.apply(op, s, d)}
+
+
+def _case_stokes_b6(shell, C, torch):
+    mf, mc = shell.ShellMesh(6, RMIN, RMAX), shell.ShellMesh(5, RMIN, RMAX)
+    u, v = shell.VectorQ1Vec(mf), shell.VectorQ1Vec(mf)
+    p, q = shell.VectorQ1Scalar(mc), shell.VectorQ1Scalar(mc)
+    u.data.uniform_(-1, 1)
+    p.data.uniform_(-1, 1)
+    B = shell.Divergence(mf, mc, C.BC_FREESLIP, C.BC_FREESLIP)
+    BT = shell.Gradient(mf, mc, C.BC_FREESLIP, C.BC_FREESLIP)
+    return {"Divergence (B), velocity level 6 -> pressure level 5, free-slip": lambda: shell.apply(B, u, q),
+            "Gradient (B^T), pressure level 5 -> velocity level 6, free-slip": lambda: shell.apply(BT, p, v)}
+
+
+def _case_stored5(shell, C, torch):
+    m = shell.ShellMesh(5, RMIN, RMAX)
+    coords, radii = m.geometry()
+    k_np, _ = synthetic_inputs(coords, radii, None)
+    k = shell.VectorQ1Scalar(m)
+    k.set_numpy(k_np)
+    m64 = shell.kerngen_local_matrices(m, k)
+    m32 = m64.float()
+    out = {}
+    for tag, mats, dt in (("FP32", m32, torch.float32), ("FP64", m64, torch.float64)):
+        u, v = shell.VectorQ1Vec(m, dt), shell.VectorQ1Vec(m, dt)
+        u.data.uniform_(-1, 1)
+        op = shell.StoredEpsilonDivDiv(m, mats, C.BC_FREESLIP, C.BC_FREESLIP)
+        out[f"stored-matrix apply {tag}, level 5 (451 / 902 MB of matrices), free-slip"] = \
+            (lambda op=op, u=u, v=v: shell.apply(op, u, v))
+    return out
+
+
+def _case_kerngen6_fs(shell, C, torch):
+    m = shell.ShellMesh(6, RMIN, RMAX)
+    coords, radii = m.geometry()
+    k_np, _ = synthetic_inputs(coords, radii, None)
+    out = {}
+    for tag, dt in (("FP32", torch.float32), ("FP64", torch.float64)):
+        k = shell.VectorQ1Scalar(m, dt)
+        k.data.copy_(torch.as_tensor(k_np))
+        u, v = shell.VectorQ1Vec(m, dt), shell.VectorQ1Vec(m, dt)
+        u.data.uniform_(-1, 1)
+        op = shell.EpsilonDivDivKerngen(m, k, C.BC_FREESLIP, C.BC_FREESLIP)
+        out[f"EpsilonDivDivKerngen apply {tag}, level 6, free-slip both radii"] = \
+            (lambda op=op, u=u, v=v: shell.apply(op, u, v))
+    return out
+
+
+def _case_stokes6(shell, C, torch):
+    """30 FGMRES iterations of the level-6 free-slip Stokes solve (FP32 multigrid): the launch list
+    of the C3 solve at a fixed iteration count"""
+    pf, pc = shell.ShellMesh(6, RMIN, RMAX), shell.ShellMesh(5, RMIN, RMAX)
+    coords, radii = pf.geometry()
+    k_np, _ = synthetic_inputs(coords, radii, None)
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(k_np)
+    fu, fp = stokes_rhs(shell, pf, coords, radii), shell.VectorQ1Scalar(pc)
+    s = shell.StokesSolver(6, kv, mg_levels=4, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=True,
+                           chebyshev_order=3, relative_tolerance=1e-30, max_iterations=30, restart=100,
+                           r_min=RMIN, r_max=RMAX, gca=1)
+    xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+
+    def run():
+        xu.data.zero_()
+        xp.data.zero_()
+        s.solve(fu, fp, xu, xp)
+    return {"Stokes solve, level 6 free-slip, FP32 multigrid, 30 FGMRES(100) iterations": run}
+
+
+# name -> builder returning {description: one launch sequence}
+CASES = {"laplace6": _case_laplace6, "vlaplace6": _case_vlaplace6, "divkgrad6": _case_divkgrad6,
+         "stokes_b6": _case_stokes_b6, "stored5": _case_stored5, "kerngen6_fs": _case_kerngen6_fs,
+         "stokes6": _case_stokes6}
+
+
+def run_case(args):
+    """Times each workload of one case with CUDA events (after args.warmup calls) and prints one JSON line."""
+    import torch
+    sys.path.insert(0, ROOT)
+    from terraneo_b200 import shell, _capi as C
+    torch.cuda.set_device(0)
+    work = CASES[args.case](shell, C, torch)
+    res = {}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for name, fn in work.items():
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(args.steps):
+            fn()
+        ev1.record()
+        torch.cuda.synchronize()
+        res[name] = {"ms_per_call": round(ev0.elapsed_time(ev1) / args.steps, 5)}
+    print(json.dumps({"case": args.case, "steps": args.steps, "warmup": args.warmup, "results": res}), flush=True)
+    return 0
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -50,6 +171,7 @@ def parse():
     ap.add_argument("--no-stokes", action="store_true", help="skip the level-6 Stokes time-to-1e-8 leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the level-5 adjoint viscosity gradient leg")
     ap.add_argument("--no-timestep", action="store_true", help="skip the level-7 mantle-circulation time-step leg")
+    ap.add_argument("--case", choices=sorted(CASES), help="time one operator workload (see CASES) instead of the bench")
     return ap.parse_args()
 
 
@@ -428,6 +550,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.case:
+        return run_case(args)
 
     import torch
     import torch.distributed as dist
