@@ -117,6 +117,24 @@ TN_API int tn_epsdivdiv_apply_f32( const tn_mesh* mesh, const tn_epsdivdiv_param
  * to a multiple of 32, times 172; FP64 about 2,752 bytes per cell, the
  * reference stores the full 5,184). */
 TN_API int tn_local_matrix_count( const tn_mesh* mesh, size_t* entries );
+/* Unpreconditioned PCG (linalg/solvers/pcg.hpp:78-102, z = r) on the
+ * stored-matrix operator of tn_stored_epsdivdiv_apply_f64 (non-diagonal,
+ * Replace, additive halo; the Dirichlet / free-slip treatment and the fs/fs
+ * penalty as there) with the operator's steps fused into the PCG steps: four
+ * launches per iteration (direction + clearing + penalty dots, wedge
+ * products, halo sum + penalty + <p, Ap>, tn_pcg_update_f64).  The same
+ * recurrences, owned-node dot products, stopping rule (|r| / |r0| <=
+ * relative_tolerance or |r| < absolute_tolerance, at most max_iterations)
+ * and state layout as the tn_pcg_* steps; every launch after the first
+ * three is gated by the stopping flag.  x: initial guess in, solution out.
+ * work: 12 fields (r, p, two operator results; 3 components each).  state:
+ * >= 9 + max_iterations doubles.  check_every > 0: outside stream capture the
+ * host reads the stopping flag every check_every iterations and stops
+ * launching (synchronises); 0: never (fully asynchronous). */
+TN_API int tn_stored_pcg_f64( const tn_mesh* mesh, const double* mats, const tn_epsdivdiv_params* p,
+                              const double* const* b, double* const* x, double* const* work, double* state,
+                              int max_iterations, double relative_tolerance, double absolute_tolerance,
+                              int check_every, void* stream );
 /* kerngen assemble_local_matrix (:2051-2110) of every wedge: one-point rule,
  * nodal coefficient k (NULL: k = 1), no boundary treatment. */
 TN_API int tn_kerngen_local_matrices_f64( const tn_mesh* mesh, const double* k, double* mats, void* stream );

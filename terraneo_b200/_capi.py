@@ -143,6 +143,8 @@ _SIGS = {
     "tn_vec_has_nan_or_inf_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), c_void_p]),
     "tn_vec_has_nan_or_inf_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), c_void_p]),
     "tn_vec_dot_noalloc_f64": (c_int, [c_size_t, c_int, P(c_void_p), P(c_void_p), c_void_p, P(c_double), c_void_p]),
+    "tn_stored_pcg_f64": (c_int, [c_void_p, c_void_p, c_void_p, P(c_void_p), P(c_void_p), P(c_void_p), c_void_p,
+                                  c_int, c_double, c_double, c_int, c_void_p]),
     "tn_vec_assign_boundary_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_double, c_int, c_int,
                                            c_void_p]),
     "tn_vec_assign_boundary_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_double, c_int, c_int,

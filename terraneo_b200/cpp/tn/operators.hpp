@@ -89,6 +89,9 @@ class StoredEpsilonDivDiv
         p_.apply_mode = int( am ), p_.comm_mode = int( cm );
     }
     void set_diagonal( bool v ) { p_.diagonal = v ? 1 : 0; }
+    const Mesh&                mesh() const { return mesh_; }
+    const T*                   matrices() const { return mats_.get(); }
+    const tn_epsdivdiv_params& params() const { return p_; }
     void apply_impl( const SrcVectorType& src, DstVectorType& dst )
     {
         const T* s[3] = { src.comp( 0 ), src.comp( 1 ), src.comp( 2 ) };
@@ -132,6 +135,8 @@ class ViscousOp
         else
             s_->apply_impl( src, dst );
     }
+    // the stored-matrix operator, or nullptr for the matrix-free one
+    const StoredEpsilonDivDiv< T >* stored() const { return s_.get(); }
 
   private:
     std::shared_ptr< EpsilonDivDivKerngen< T > > k_;

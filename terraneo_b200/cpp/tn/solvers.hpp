@@ -127,8 +127,30 @@ class DevicePCG
         if ( tmps_.size() < 3 )
             throw std::runtime_error( "DevicePCG: needs 3 temporary vectors" );
     }
+    // with the stored-matrix FP64 viscous operator and a 4th temporary the
+    // operator's steps are fused into the PCG steps (tn_stored_pcg_f64)
+    bool fused = true;
     void solve_impl( Op& A, V& x, const V& b )
     {
+        if constexpr ( std::is_same_v< Op, ViscousOp< double > > )
+        {
+            const StoredEpsilonDivDiv< double >* so = A.stored();
+            if ( fused && so && tmps_.size() >= 4 && !so->params().diagonal &&
+                 so->params().apply_mode == TN_APPLY_REPLACE && so->params().comm_mode == TN_COMM_ADDITIVE )
+            {
+                const double* bb[3] = { b.comp( 0 ), b.comp( 1 ), b.comp( 2 ) };
+                double*       xx[3];
+                x.ptrs( xx );
+                double* w[12];
+                for ( int k = 0; k < 4; ++k )
+                    tmps_[k].ptrs( w + 3 * k );
+                check( tn_stored_pcg_f64( so->mesh().get(), so->matrices(), &so->params(), bb, xx, w, state_.get(),
+                                          prm_.max_iterations, prm_.relative_residual_tolerance,
+                                          prm_.absolute_residual_tolerance, check_every_, stream() ),
+                       "stored_pcg" );
+                return;
+            }
+        }
         auto& r  = tmps_[0];
         auto& p  = tmps_[1];
         auto& ap = tmps_[2];

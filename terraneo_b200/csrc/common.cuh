@@ -85,6 +85,7 @@ struct tn_mesh
     int  n_halo_groups    = 0;
     int* d_halo_offsets   = nullptr;
     int* d_halo_members   = nullptr;
+    int* d_lat_group      = nullptr; // halo group of each lateral position, -1 if not duplicated
 
     // finite-volume lateral ghost map: entry (d * 4 + side) * N + i gives the
     // (diamond, x, y) FV cell across the face of ghost cell i on side

@@ -26,7 +26,10 @@
 // 6-term passes.  Apply: one thread per wedge streams its 43 chunks with
 // vector loads (each warp load is 32 x 4 consecutive values) and uses the
 // symmetry.
+#include <algorithm>
+
 #include "common.cuh"
+#include "reduce.cuh"
 #include "wedge.cuh"
 
 namespace tn {
@@ -316,6 +319,7 @@ struct StoredParams
     Ptr3< const T > src;
     Ptr3< T >       dst;
     int             bc_cmb, bc_surf, diag;
+    const double*   gate; // skip the launch when *gate != 0 (the PCG stopping flag), or NULL
 };
 
 // One thread per wedge (w = 2 cell + wedge).  The 171 stored values stream
@@ -539,7 +543,7 @@ __global__ void __launch_bounds__( 128, sizeof( T ) == 4 ? 5 : 2 ) stored_apply_
 {
     const long long gw = blockIdx.x * (long long) blockDim.x + threadIdx.x;
     const int       N = P.N, n1 = P.n1;
-    if ( gw >= 2LL * kDiamonds * N * N * N )
+    if ( gw >= 2LL * kDiamonds * N * N * N || ( P.gate && *P.gate != 0.0 ) )
         return;
     const long long cell = gw >> 1;
     const int       w    = int( gw & 1 );
@@ -676,6 +680,175 @@ __global__ void cast_array_kernel( size_t n, const double* __restrict__ src, flo
         dst[i] = float( src[i] );
 }
 
+// ---------------------------------------------------------------------------
+// PCG on the stored-matrix operator with the operator's pieces fused into the
+// PCG steps (pcg.hpp:78-102, z = r; the state layout and the x / r update of
+// the tn_pcg_* kernels).  Per iteration four launches instead of the ~11 of
+// the generic composition (memsets, apply, penalty dots / vector / axpy,
+// halo sum, <p, Ap>, update, direction):
+//   prepare: p = r + beta p (from the second iteration), ap = 0 and the fs/fs
+//            penalty dots sum_owned x_node x p, whose last block turns them
+//            into the penalty vector g = eps G^-1 d;
+//   stored_apply_kernel: ap += wedge products of p (atomics);
+//   gather:  aq = sum over the node's copies of (ap + g x x_node) -- the
+//            penalty added on every copy before the halo sum, in the order
+//            the operator uses -- and <p, aq> over owned nodes;
+//   tn_pcg_update_f64: x += alpha p, r -= alpha aq, <r, r>, stopping rule.
+// Every launch is gated by the stopping flag, so a fixed sequence (CUDA
+// graph capture) gives the iterate the host-checked loop stops at.
+enum : int
+{
+    kSpAn = 0, // tn_pcg_* state layout
+    kSpPap,
+    kSpR0,
+    kSpBeta,
+    kSpDone,
+    kSpIts,
+    kSpRelres,
+    kSpHist = 8
+};
+
+struct SpcgParams
+{
+    size_t         ns;
+    int            n1, fsfs;
+    double         eps, ginv[9];
+    const double * coords, *radii;
+    const int *    lat_group, *offsets, *members;
+    const uint8_t* owned;
+    double*        state;
+    double*        scratch; // [0..2] penalty dots, [3..5] penalty vector g
+    double*        partials;
+    unsigned*      counter;
+};
+
+__device__ __forceinline__ void spcg_position( const SpcgParams& S, unsigned i, double xp[3] )
+{
+    const unsigned n1  = unsigned( S.n1 );
+    const unsigned lat = i / n1; // ns < 2^32 at every level tn_mesh_create accepts (<= 9)
+    const unsigned r   = i - lat * n1;
+    const unsigned d   = lat / ( n1 * n1 );
+    const double   rr  = S.radii[d * n1 + r];
+    const double*  c   = S.coords + size_t( lat ) * 3;
+    xp[0] = c[0] * rr, xp[1] = c[1] * rr, xp[2] = c[2] * rr;
+}
+
+// v = p (after p = r + beta p when update_p) or the given field; ap = 0;
+// penalty dots of v and, in the last block, g = eps G^-1 d
+__global__ void __launch_bounds__( 256 ) spcg_prepare_kernel( SpcgParams S, Ptr3< double > p, Ptr3< const double > r,
+                                                               Ptr3< const double > v, Ptr3< double > ap, int update_p,
+                                                               int gated )
+{
+    if ( gated && S.state[kSpDone] != 0.0 )
+        return;
+    const double beta   = update_p ? S.state[kSpBeta] : 0.0;
+    const size_t stride = size_t( gridDim.x ) * blockDim.x;
+    double       sum[3] = { 0.0, 0.0, 0.0 };
+    for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < S.ns; i += stride )
+    {
+        double w[3];
+#pragma unroll
+        for ( int c = 0; c < 3; ++c )
+        {
+            if ( update_p )
+            {
+                w[c]      = r.p[c][i] + beta * p.p[c][i];
+                p.p[c][i] = w[c];
+            }
+            else
+                w[c] = v.p[c][i];
+            ap.p[c][i] = 0.0;
+        }
+        if ( S.fsfs && S.owned[i] )
+        {
+            double xp[3];
+            spcg_position( S, unsigned( i ), xp );
+            sum[0] += xp[1] * w[2] - xp[2] * w[1];
+            sum[1] += xp[2] * w[0] - xp[0] * w[2];
+            sum[2] += xp[0] * w[1] - xp[1] * w[0];
+        }
+    }
+    if ( !S.fsfs )
+        return;
+    Neumaier acc[3];
+    for ( int k = 0; k < 3; ++k )
+        acc[k].add( sum[k] );
+    if ( block_sum_finish< 3 >( acc, S.partials, S.counter, S.scratch ) && threadIdx.x == 0 )
+    {
+        const double d0 = S.scratch[0], d1 = S.scratch[1], d2 = S.scratch[2];
+        for ( int k = 0; k < 3; ++k )
+            S.scratch[3 + k] = S.eps * ( S.ginv[3 * k] * d0 + S.ginv[3 * k + 1] * d1 + S.ginv[3 * k + 2] * d2 );
+    }
+}
+
+// a = halo sum over the node's copies of (ap + g x x).  mode 0 (initial
+// residual): r = b - a, p = r, state from <r, r> (pcg.hpp:79-86); mode 1:
+// aq = a, state[kSpPap] = <p, aq>
+__global__ void __launch_bounds__( 256 ) spcg_gather_kernel( SpcgParams S, Ptr3< const double > ap, int mode,
+                                                              Ptr3< const double > b, Ptr3< double > r,
+                                                              Ptr3< double > p, Ptr3< double > aq, double atol )
+{
+    if ( mode == 1 && S.state[kSpDone] != 0.0 )
+        return;
+    const double g[3]   = { S.fsfs ? S.scratch[3] : 0.0, S.fsfs ? S.scratch[4] : 0.0, S.fsfs ? S.scratch[5] : 0.0 };
+    const size_t stride = size_t( gridDim.x ) * blockDim.x;
+    const unsigned n1   = unsigned( S.n1 );
+    Neumaier      acc;
+    for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < S.ns; i += stride )
+    {
+        double pen[3] = { 0.0, 0.0, 0.0 };
+        if ( S.fsfs )
+        {
+            double xp[3];
+            spcg_position( S, unsigned( i ), xp );
+            pen[0] = g[1] * xp[2] - g[2] * xp[1];
+            pen[1] = g[2] * xp[0] - g[0] * xp[2];
+            pen[2] = g[0] * xp[1] - g[1] * xp[0];
+        }
+        const unsigned lat = unsigned( i ) / n1, rr = unsigned( i ) - lat * n1;
+        const int      grp = S.lat_group[lat];
+        double         dot = 0.0;
+#pragma unroll
+        for ( int c = 0; c < 3; ++c )
+        {
+            double a;
+            if ( grp < 0 )
+                a = ap.p[c][i] + pen[c];
+            else
+            {
+                a = 0.0;
+                for ( int k = S.offsets[grp]; k < S.offsets[grp + 1]; ++k )
+                    a += ap.p[c][size_t( S.members[k] ) * n1 + rr] + pen[c];
+            }
+            if ( mode == 0 )
+            {
+                const double ri = b.p[c][i] - a;
+                r.p[c][i]       = ri;
+                p.p[c][i]       = ri;
+                dot += ri * ri;
+            }
+            else
+            {
+                aq.p[c][i] = a;
+                dot += p.p[c][i] * a;
+            }
+        }
+        acc.add( S.owned[i] ? dot : 0.0 );
+    }
+    double* st = S.state;
+    if ( block_sum_finish< 1 >( &acc, S.partials, S.counter, mode == 0 ? st + kSpAn : st + kSpPap ) &&
+         threadIdx.x == 0 && mode == 0 )
+    {
+        const double r0 = sqrt( st[kSpAn] );
+        st[kSpR0]       = r0;
+        st[kSpBeta]     = 0.0;
+        st[kSpDone]     = r0 < atol ? 1.0 : 0.0;
+        st[kSpIts]      = 0.0;
+        st[kSpRelres]   = 1.0;
+        st[kSpHist]     = 1.0;
+    }
+}
+
 }  // namespace
 
 template < typename T >
@@ -713,6 +886,89 @@ int stored_apply( const tn_mesh* m, const T* mats, const tn_epsdivdiv_params* p,
     }
     if ( p->comm_mode == TN_COMM_ADDITIVE )
         return halo_sum< T >( m, dst, 3, st );
+    return TN_OK;
+}
+
+// Host driver of the fused stored-matrix PCG (see spcg_prepare_kernel).
+static int stored_pcg( const tn_mesh* m, const double* mats, const tn_epsdivdiv_params* p, const double* const* b,
+                       double* const* x, double* const* work, double* state, int max_it, double rtol, double atol,
+                       int check_every, cudaStream_t st )
+{
+    TN_CHECK_ARG( m && mats && p && b && x && work && state, "stored_pcg: null argument" );
+    TN_CHECK_ARG( !p->diagonal && p->apply_mode == TN_APPLY_REPLACE && p->comm_mode == TN_COMM_ADDITIVE,
+                  "stored_pcg: needs the non-diagonal operator in Replace mode with the additive halo" );
+    TN_CHECK_ARG( p->bc_cmb >= 0 && p->bc_cmb <= 2 && p->bc_surface >= 0 && p->bc_surface <= 2,
+                  "stored_pcg: boundary condition codes must be 0, 1 or 2" );
+    TN_CHECK_ARG( max_it >= 0, "stored_pcg: max_iterations must be >= 0" );
+    Ptr3< const double > pb{}, cx{};
+    Ptr3< double >       px{}, pr{}, pp{}, pap{}, paq{};
+    for ( int c = 0; c < 3; ++c )
+    {
+        TN_CHECK_ARG( b[c] && x[c], "stored_pcg: null vector component" );
+        for ( int k = 0; k < 4; ++k )
+            TN_CHECK_ARG( work[3 * k + c], "stored_pcg: null work field" );
+        pb.p[c] = b[c], px.p[c] = x[c], cx.p[c] = x[c];
+        pr.p[c] = work[c], pp.p[c] = work[3 + c], pap.p[c] = work[6 + c], paq.p[c] = work[9 + c];
+    }
+    SpcgParams S{};
+    S.ns = m->ns, S.n1 = m->n1, S.fsfs = p->bc_cmb == TN_BC_FREESLIP && p->bc_surface == TN_BC_FREESLIP;
+    S.eps = p->penalty_eps;
+    for ( int i = 0; i < 9; ++i )
+        S.ginv[i] = m->penalty_gram_inv[i];
+    S.coords = m->d_coords, S.radii = m->d_radii;
+    S.lat_group = m->d_lat_group, S.offsets = m->d_halo_offsets, S.members = m->d_halo_members;
+    S.owned = m->d_node_owned, S.state = state, S.scratch = m->d_red_result;
+    S.partials = m->d_red_partials, S.counter = m->d_red_counter;
+
+    StoredParams< double > A{};
+    A.N = m->N, A.n1 = m->n1, A.coords = m->d_coords, A.mats = mats;
+    A.bc_cmb = p->bc_cmb, A.bc_surf = p->bc_surface, A.diag = 0;
+    for ( int c = 0; c < 3; ++c )
+        A.dst.p[c] = pap.p[c];
+    const long long wedges   = 2LL * kDiamonds * m->N * m->N * m->N;
+    const unsigned  ablocks  = unsigned( ( wedges + 127 ) / 128 );
+    // one node per thread: at coarse levels the dependent loads of a node, not bandwidth, set the time
+    const unsigned  nblocks  = unsigned( std::max< size_t >( 1, std::min< size_t >( ( m->ns + 255 ) / 256, kRedMaxBlocks ) ) );
+    const tn_mesh*  seg[3]   = { m, m, m };
+    double*         xs[3]    = { x[0], x[1], x[2] };
+    double*         rs[3]    = { work[0], work[1], work[2] };
+    const double*   ps[3]    = { work[3], work[4], work[5] };
+    const double*   aqs[3]   = { work[9], work[10], work[11] };
+    Ptr3< const double > cap{ { pap.p[0], pap.p[1], pap.p[2] } }, cr{ { pr.p[0], pr.p[1], pr.p[2] } };
+
+    // r = b - A x, p = r
+    spcg_prepare_kernel<<< nblocks, 256, 0, st >>>( S, pp, cr, cx, pap, 0, 0 );
+    TN_LAUNCH_CHECK();
+    A.src = cx, A.gate = nullptr;
+    stored_apply_kernel< double ><<< ablocks, 128, 0, st >>>( A );
+    TN_LAUNCH_CHECK();
+    spcg_gather_kernel<<< nblocks, 256, 0, st >>>( S, cap, 0, pb, pr, pp, paq, atol );
+    TN_LAUNCH_CHECK();
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    TN_CUDA_TRY( cudaStreamIsCapturing( st, &cs ) );
+    const bool capturing = cs != cudaStreamCaptureStatusNone;
+    A.src  = Ptr3< const double >{ { pp.p[0], pp.p[1], pp.p[2] } };
+    A.gate = state + kSpDone;
+    for ( int it = 1; it <= max_it; ++it )
+    {
+        if ( !capturing && check_every > 0 && ( it == 1 || ( it - 1 ) % check_every == 0 ) )
+        {
+            double done = 0.0;
+            TN_CUDA_TRY( cudaMemcpyAsync( &done, state + kSpDone, sizeof( double ), cudaMemcpyDeviceToHost, st ) );
+            TN_CUDA_TRY( cudaStreamSynchronize( st ) );
+            if ( done != 0.0 )
+                break;
+        }
+        spcg_prepare_kernel<<< nblocks, 256, 0, st >>>( S, pp, cr, A.src, pap, it > 1, 1 );
+        TN_LAUNCH_CHECK();
+        stored_apply_kernel< double ><<< ablocks, 128, 0, st >>>( A );
+        TN_LAUNCH_CHECK();
+        spcg_gather_kernel<<< nblocks, 256, 0, st >>>( S, cap, 1, pb, pr, pp, paq, atol );
+        TN_LAUNCH_CHECK();
+        int rc = tn_pcg_update_f64( 3, seg, xs, rs, ps, aqs, state, it, rtol, atol, st );
+        if ( rc )
+            return rc;
+    }
     return TN_OK;
 }
 
@@ -776,4 +1032,13 @@ extern "C" int tn_array_cast_f64_to_f32( size_t n, const double* src, float* dst
     cast_array_kernel<<< blocks, 256, 0, as_stream( s ) >>>( n, src, dst );
     TN_LAUNCH_CHECK();
     return TN_OK;
+}
+
+extern "C" int tn_stored_pcg_f64( const tn_mesh* m, const double* mats, const tn_epsdivdiv_params* p,
+                                  const double* const* b, double* const* x, double* const* work, double* state,
+                                  int max_iterations, double relative_tolerance, double absolute_tolerance,
+                                  int check_every, void* s )
+{
+    return stored_pcg( m, mats, p, b, x, work, state, max_iterations, relative_tolerance, absolute_tolerance,
+                       check_every, as_stream( s ) );
 }

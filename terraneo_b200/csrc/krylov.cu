@@ -93,7 +93,11 @@ unsigned red_blocks( const Segs& s )
     size_t n = 0;
     for ( int k = 0; k < s.n; ++k )
         n += s.len[k];
+    // 8 entries per thread on large fields; small (coarse-level) fields get one
+    // entry per thread up to two blocks per SM, since there the latency of a
+    // thread's dependent loads, not bandwidth, sets the time
     size_t b = ( n + size_t( kThreads ) * 8 - 1 ) / ( size_t( kThreads ) * 8 );
+    b        = std::max( b, std::min< size_t >( ( n + kThreads - 1 ) / kThreads, 296 ) );
     return unsigned( std::max< size_t >( 1, std::min< size_t >( b, kRedMaxBlocks ) ) );
 }
 

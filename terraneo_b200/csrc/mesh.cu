@@ -293,6 +293,11 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
         std::memcpy( m->penalty_gram_inv, inv, sizeof( inv ) );
     }
 
+    std::vector< int > lat_group( m->nlat, -1 );
+    for ( int g = 0; g + 1 < int( offsets.size() ); ++g )
+        for ( int k = offsets[g]; k < offsets[g + 1]; ++k )
+            lat_group[members[k]] = g;
+
     std::vector< uint8_t > node_owned( m->ns );
     for ( size_t l = 0; l < m->nlat; ++l )
         std::memset( node_owned.data() + l * m->n1, m->h_lat_owned[l], m->n1 );
@@ -306,7 +311,8 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
          ( rc = upload( node_owned.data(), node_owned.size(), &m->d_node_owned ) ) ||
          ( rc = upload( offsets.data(), offsets.size(), &m->d_halo_offsets ) ) ||
          ( rc = upload( fv_ghost.data(), fv_ghost.size(), &m->d_fv_ghost ) ) ||
-         ( rc = upload( members.data(), std::max< size_t >( members.size(), 1 ), &m->d_halo_members ) ) )
+         ( rc = upload( members.data(), std::max< size_t >( members.size(), 1 ), &m->d_halo_members ) ) ||
+         ( rc = upload( lat_group.data(), lat_group.size(), &m->d_lat_group ) ) )
     {
         tn_mesh_destroy( m );
         return rc;
@@ -337,6 +343,7 @@ extern "C" int tn_mesh_destroy( tn_mesh* m )
     cudaFree( m->d_node_owned );
     cudaFree( m->d_halo_offsets );
     cudaFree( m->d_halo_members );
+    cudaFree( m->d_lat_group );
     cudaFree( m->d_fv_ghost );
     cudaFree( m->d_grad_geom );
     cudaFree( m->d_stokes_geom );

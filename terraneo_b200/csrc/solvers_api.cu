@@ -286,10 +286,11 @@ extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min,
         if ( p->gca )
             build_gca( *s );
         s->A64fine = std::make_shared< A64 >( s->mesh[L], s->k64[L], bcs, false );
-        // FP64 coarsest solve (both precisions): device-resident PCG, 3 temporaries
+        // FP64 coarsest solve (both precisions): device-resident PCG; the 4th
+        // temporary lets the stored-matrix (GCA) operator use the fused steps
         auto Ac64 = std::make_shared< V64 >( level_op< double >( *s, Lmin ) );
         std::vector< VectorQ1Vec< double > > ct;
-        for ( int i = 0; i < 3; ++i )
+        for ( int i = 0; i < 4; ++i )
             ct.emplace_back( s->mesh[Lmin] );
         auto pcg = std::make_shared< DevicePCG< V64 > >(
             IterativeSolverParameters{ p->coarse_max_iterations, p->coarse_relative_tolerance, 1e-16 }, ct );

@@ -185,6 +185,23 @@ def gca_coarsen(fine, coarse, k_fine=None, mats_fine=None, mode=0):
     return out
 
 
+def stored_pcg(op, b, x, max_iterations=50, relative_tolerance=1e-6, absolute_tolerance=1e-30, check_every=8):
+    """Unpreconditioned PCG (linalg/solvers/pcg.hpp:78) on a StoredEpsilonDivDiv (FP64) with the operator's steps
+    fused into the PCG steps (tn_stored_pcg_f64); x is updated in place.
+    Returns (iterations, relative residual history)."""
+    m = op.mesh
+    work = [VectorQ1Vec(m) for _ in range(4)]
+    ptrs = (ctypes.c_void_p * 12)(*[w.data[c].data_ptr() for w in work for c in range(3)])
+    state = torch.zeros(9 + max_iterations, dtype=torch.float64, device="cuda")
+    C.check(C.lib().tn_stored_pcg_f64(m.handle, ctypes.c_void_p(op.mats.data_ptr()), ctypes.byref(op.prm),
+                                      b.comp_ptrs(), x.comp_ptrs(), ptrs, ctypes.c_void_p(state.data_ptr()),
+                                      max_iterations, relative_tolerance, absolute_tolerance, check_every,
+                                      _stream()), "stored_pcg")
+    st = state.cpu().numpy()
+    its = int(st[5])
+    return its, list(st[8:9 + its])
+
+
 class StoredEpsilonDivDiv:
     """EpsilonDivDivKerngen with OperatorStoredMatrixMode::Full: stored wedge matrices + boundary treatment."""
 

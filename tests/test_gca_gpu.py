@@ -108,3 +108,66 @@ def test_gca_two_levels_and_fp32(level3):
     src.set_numpy(u)
     shell.apply(shell.StoredEpsilonDivDiv(p2, m2f, 2, 2), src, dst)
     assert rel(dst.numpy().astype(float), o2.stored_apply(ref2, u, 2, 2)) <= 1e-5
+
+
+def _oracle_pcg(apply, dot, b, maxit, rtol):
+    """pcg.hpp:78-102 with z = r, from x = 0; returns (x, relative residual history)"""
+    x = np.zeros_like(b)
+    r = b - apply(x)
+    p = r.copy()
+    an = dot(r, r)
+    r0 = np.sqrt(an)
+    hist = [1.0]
+    for it in range(1, maxit + 1):
+        ap = apply(p)
+        alpha = an / dot(ap, p)
+        x += alpha * p
+        r -= alpha * ap
+        rr = dot(r, r)
+        hist.append(np.sqrt(rr) / r0)
+        if hist[-1] <= rtol:
+            break
+        p = r + (rr / an) * p
+        an = rr
+    return x, hist
+
+
+@pytest.mark.parametrize("bc", [(1, 1), (2, 2), (2, 1)])
+@pytest.mark.parametrize("contrast", [1.0, 1e3])
+@pytest.mark.parametrize("check_every", [8, 0])
+def test_fused_stored_pcg_matches_oracle_cg(level3, bc, contrast, check_every):
+    """The fused stored-matrix PCG (operator steps folded into the PCG steps) follows the oracle CG on the
+    oracle operator step by step.  Unpreconditioned CG amplifies rounding (the atomics order on the GPU),
+    so with the 1e3 viscosity contrast only the first iterations are compared tightly."""
+    from terraneo_b200 import shell
+    of, oc, pf, pc, _, _ = level3
+    k = viscosity_field(of, seed=9, contrast=contrast) if contrast > 1 else np.ones(of.shape)
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(k)
+    m = shell.kerngen_local_matrices(pf, kv)
+    f = random_vector(of, seed=17)
+    if bc[0] == 1:
+        f[:, :, :, :, 0] = 0.0
+    if bc[1] == 1:
+        f[:, :, :, :, -1] = 0.0
+    fb = shell.VectorQ1Vec(pf)
+    fb.set_numpy(f)
+    if 2 in bc:
+        shell.freeslip_project(fb, bc[0] == 2, bc[1] == 2)
+    b = fb.numpy()
+    op = shell.StoredEpsilonDivDiv(pf, m, bc[0], bc[1])
+    n = 60 if contrast == 1.0 else 15
+    x = shell.VectorQ1Vec(pf)
+    its, hist = shell.stored_pcg(op, fb, x, max_iterations=n, relative_tolerance=1e-30, check_every=check_every)
+    assert its == n
+    xo, ho = _oracle_pcg(lambda v: of.kerngen(k, v, bc[0], bc[1]), of.dot, b, n, 1e-30)
+    np.testing.assert_allclose(hist, ho, rtol=1e-6)
+    assert rel(x.numpy(), xo) <= 1e-7
+    # the stopping rule (gated launches after convergence), and an initial guess (continue from x)
+    x2 = shell.VectorQ1Vec(pf)
+    tol = ho[n // 2] * (1 + 1e-6)
+    its2, _ = shell.stored_pcg(op, fb, x2, max_iterations=n, relative_tolerance=tol, check_every=check_every)
+    assert abs(its2 - next(i for i in range(1, n + 1) if ho[i] <= tol)) <= 1
+    its3, hist3 = shell.stored_pcg(op, fb, x2, max_iterations=n - its2, relative_tolerance=1e-30,
+                                   check_every=check_every)
+    assert its3 == n - its2 and hist3[0] == 1.0
