@@ -113,26 +113,50 @@ __global__ void axpy_dot_kernel( Segs s, SegPtr< T > w, SegPtr< const T > x, con
         return;
     const bool upd = x.p[0] != nullptr;
     const T    a   = upd ? T( -coeff[0] ) : T( 0 );
-    Neumaier   acc;
+    // kU entries per thread and step, all loads issued before the arithmetic;
+    // plain FP64 sums per thread (two chains), compensated across threads
+    constexpr int kU     = 4;
+    double        sum[2] = { 0.0, 0.0 };
+    const size_t  stride = size_t( gridDim.x ) * blockDim.x;
     for ( int k = 0; k < s.n; ++k )
     {
         T* __restrict__ pw             = w.p[k];
         const T* __restrict__ px       = x.p[k];
-        const T* __restrict__ pv       = v.p[k] ? v.p[k] : w.p[k];
+        const T* __restrict__ pv       = v.p[k];
         const uint8_t* __restrict__ ow = s.owned[k];
-        for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < s.len[k];
-              i += size_t( gridDim.x ) * blockDim.x )
+        const size_t n                 = s.len[k];
+        for ( size_t i0 = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i0 < n; i0 += kU * stride )
         {
-            T wi = pw[i];
-            if ( upd )
+            T       wi[kU], xi[kU], vi[kU];
+            uint8_t oi[kU];
+#pragma unroll
+            for ( int u = 0; u < kU; ++u )
             {
-                wi    = wi + a * px[i];
-                pw[i] = wi;
+                const size_t i = i0 + u * stride;
+                const bool   in = i < n;
+                wi[u]           = in ? pw[i] : T( 0 );
+                xi[u]           = in && upd ? px[i] : T( 0 );
+                vi[u]           = in && pv ? pv[i] : T( 0 );
+                oi[u]           = in ? ow[i] : uint8_t( 0 );
             }
-            const double prod = double( wi ) * double( v.p[k] ? pv[i] : wi );
-            acc.add( ow[i] ? prod : 0.0 );
+#pragma unroll
+            for ( int u = 0; u < kU; ++u )
+            {
+                const size_t i = i0 + u * stride;
+                if ( upd )
+                {
+                    wi[u] = wi[u] + a * xi[u];
+                    if ( i < n )
+                        pw[i] = wi[u];
+                }
+                const double prod = double( wi[u] ) * double( pv ? vi[u] : wi[u] );
+                sum[u & 1] += oi[u] ? prod : 0.0;
+            }
         }
     }
+    Neumaier acc;
+    acc.add( sum[0] );
+    acc.add( sum[1] );
     block_sum_finish< 1 >( &acc, partials, counter, result );
 }
 
