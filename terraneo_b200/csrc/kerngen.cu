@@ -471,11 +471,12 @@ __device__ void cell_full( const CellParams< T >& P, int d, int x, int y, int r,
                     p[n][a] = T( u[a] );
             idx[n] = lat * n1 + R;
             kn[n]  = P.k[idx[n]];
+            // outward unit normals, needed by free-slip layers only (one reciprocal square root)
             T nn[3] = { T( u[0] ), T( u[1] ), T( u[2] ) };
-            const T mm = sqrt( nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2] );
+            const T im = ( cmb_fs || surf_fs ) ? rsqrt( nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2] ) : T( 0 );
             for ( int c = 0; c < 3; ++c )
             {
-                nrm[n][c] = nn[c] / mm;
+                nrm[n][c] = nn[c] * im;
                 s[n][c] = sp[n][c] = P.src.p[c][idx[n]];
             }
             if ( ( cmb_fs && n < 3 ) || ( surf_fs && n >= 3 ) )
@@ -565,8 +566,8 @@ __device__ void cell_full( const CellParams< T >& P, int d, int x, int y, int r,
                 const size_t  lat = lat_index( n1, d, x + dx, y + dy );
                 const double* u   = P.coords + lat * 3;
                 T             n[3] = { T( u[0] ), T( u[1] ), T( u[2] ) };
-                const T       mm   = sqrt( n[0] * n[0] + n[1] * n[1] + n[2] * n[2] );
-                n[0] /= mm, n[1] /= mm, n[2] /= mm;
+                const T       im   = rsqrt( n[0] * n[0] + n[1] * n[1] + n[2] * n[2] );
+                n[0] *= im, n[1] *= im, n[2] *= im;
                 T* o = acc[dx][dy][dr];
                 project_out( n, o );
                 const size_t i  = lat * n1 + r + dr;
@@ -589,6 +590,36 @@ __global__ void __launch_bounds__( 128 ) kerngen_cell_kernel( CellParams< T > P 
     const int y = int( ( t / N ) % N );
     const int x = int( ( t / ( (long long) N * N ) ) % N );
     const int d = int( t / ( (long long) N * N * N ) );
+    T         acc[2][2][2][3];
+    cell_full( P, d, x, y, r, acc );
+    for ( int dx = 0; dx < 2; ++dx )
+        for ( int dy = 0; dy < 2; ++dy )
+            for ( int dr = 0; dr < 2; ++dr )
+            {
+                const size_t i = lat_index( n1, d, x + dx, y + dy ) * n1 + r + dr;
+                for ( int c = 0; c < 3; ++c )
+                    atomicAdd( P.dst.p[c] + i, acc[dx][dy][dr][c] );
+            }
+}
+
+// Boundary cell layers, cell-centric: one thread per cell of the CMB layer
+// (r = 0) and / or the SURFACE layer (r = N - 1), both wedges with the full
+// boundary treatment of cell_full, atomics onto the values the tile kernel
+// wrote (it leaves these cells out).  Neighbouring threads are neighbouring
+// cells in y of one layer.
+template < typename T >
+__global__ void __launch_bounds__( 128 ) kerngen_bcell_kernel( CellParams< T > P, int sides )
+{
+    const int       N = P.N, n1 = P.n1;
+    const long long per = (long long) kDiamonds * N * N;
+    const long long t   = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if ( t >= per * ( sides == 3 ? 2 : 1 ) )
+        return;
+    const int side = sides == 3 ? int( t / per ) : ( sides == 1 ? 0 : 1 );
+    const int r    = side == 0 ? 0 : N - 1;
+    const int y    = int( t % N );
+    const int x    = int( ( t / N ) % N );
+    const int d    = int( ( t % per ) / ( (long long) N * N ) );
     T         acc[2][2][2][3];
     cell_full( P, d, x, y, r, acc );
     for ( int dx = 0; dx < 2; ++dx )
@@ -784,63 +815,74 @@ struct Mat3
     double a[9];
 };
 
-// <m_j, u> over owned nodes for the three rotation modes m_j = e_j x x.
-// Flat grid-stride loop over stored nodes (coalesced src loads, several
-// independent nodes in flight per thread); lateral data (ownership, unit
-// coordinates) and radii come from L1.
+// <m_j, u> over owned nodes for the three rotation modes m_j = e_j x x:
+// sum over owned lateral columns of c_lat x (sum_r rad_r u(lat, r)), c the
+// unit lateral position.  One warp per column (lanes along r, coalesced),
+// FP64 sums per lane, the column's radial sum reduced with shuffles and
+// crossed with c once; compensated sums across warps and blocks.
 template < typename T >
-__global__ void __launch_bounds__( 256 ) penalty_dots_kernel( size_t ns, int n1, const double* __restrict__ coords,
+__global__ void __launch_bounds__( 256 ) penalty_dots_kernel( size_t nlat, int n1, const double* __restrict__ coords,
                                                               const T* __restrict__ radii, Ptr3< const T > src,
                                                               const uint8_t* __restrict__ lat_owned, double* partials,
-                                                              unsigned int* counter, double* result )
+                                                              unsigned int* counter, double* result, double eps,
+                                                              Mat3 ginv )
 {
-    // plain double sums per thread (a few nodes each), compensated sums
-    // across threads and blocks
+    const int    lane  = threadIdx.x & 31;
+    const size_t warp  = ( blockIdx.x * size_t( blockDim.x ) + threadIdx.x ) >> 5;
+    const size_t warps = ( size_t( gridDim.x ) * blockDim.x ) >> 5;
     double       sum[3] = { 0.0, 0.0, 0.0 };
-    const size_t stride = size_t( gridDim.x ) * blockDim.x;
-    constexpr int kU    = 4;
-    for ( size_t i0 = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i0 < ns; i0 += kU * stride )
+    for ( size_t lat = warp; lat < nlat; lat += warps )
     {
-        T        v[kU][3];
-        unsigned lat[kU];
-        int      rr[kU];
-#pragma unroll
-        for ( int u = 0; u < kU; ++u )
+        if ( !lat_owned[lat] )
+            continue;
+        const int  d  = int( lat / ( size_t( n1 ) * n1 ) );
+        const T*   rd = radii + size_t( d ) * n1;
+        double     v0 = 0.0, v1 = 0.0, v2 = 0.0;
+        for ( int r = lane; r < n1; r += 32 )
         {
-            const size_t i = i0 + u * stride;
-            lat[u]         = i < ns ? unsigned( i ) / unsigned( n1 ) : 0u; // ns < 2^32 at every level tn_mesh_create accepts (<= 9)
-            rr[u]          = i < ns ? int( unsigned( i ) - lat[u] * unsigned( n1 ) ) : 0;
-#pragma unroll
-            for ( int c = 0; c < 3; ++c )
-                v[u][c] = i < ns ? src.p[c][i] : T( 0 );
+            const size_t i   = lat * n1 + r;
+            const double rad = double( rd[r] );
+            v0 += rad * double( src.p[0][i] );
+            v1 += rad * double( src.p[1][i] );
+            v2 += rad * double( src.p[2][i] );
         }
 #pragma unroll
-        for ( int u = 0; u < kU; ++u )
+        for ( int off = 16; off > 0; off >>= 1 )
         {
-            if ( i0 + u * stride >= ns || !lat_owned[lat[u]] )
-                continue;
-            const int     d   = int( lat[u] / unsigned( n1 * n1 ) );
-            const double* cu  = coords + size_t( lat[u] ) * 3;
-            const double  rad = double( radii[d * n1 + rr[u]] );
-            const double  x0 = cu[0] * rad, x1 = cu[1] * rad, x2 = cu[2] * rad;
-            const double  w0 = double( v[u][0] ), w1 = double( v[u][1] ), w2 = double( v[u][2] );
-            sum[0] += x1 * w2 - x2 * w1;
-            sum[1] += x2 * w0 - x0 * w2;
-            sum[2] += x0 * w1 - x1 * w0;
+            v0 += __shfl_xor_sync( 0xffffffffu, v0, off );
+            v1 += __shfl_xor_sync( 0xffffffffu, v1, off );
+            v2 += __shfl_xor_sync( 0xffffffffu, v2, off );
+        }
+        if ( lane == 0 )
+        {
+            const double* c = coords + lat * 3;
+            sum[0] += c[1] * v2 - c[2] * v1;
+            sum[1] += c[2] * v0 - c[0] * v2;
+            sum[2] += c[0] * v1 - c[1] * v0;
         }
     }
     Neumaier acc[3];
     for ( int k = 0; k < 3; ++k )
         acc[k].add( sum[k] );
-    block_sum_finish< 3 >( acc, partials, counter, result );
+    // the last block also forms the penalty vector beta = eps G^-1 d in result[3..5]
+    if ( block_sum_finish< 3 >( acc, partials, counter, result ) && threadIdx.x == 0 )
+    {
+        const double b0 = result[0], b1 = result[1], b2 = result[2];
+        result[3]       = eps * ( ginv.a[0] * b0 + ginv.a[1] * b1 + ginv.a[2] * b2 );
+        result[4]       = eps * ( ginv.a[3] * b0 + ginv.a[4] * b1 + ginv.a[5] * b2 );
+        result[5]       = eps * ( ginv.a[6] * b0 + ginv.a[7] * b1 + ginv.a[8] * b2 );
+    }
 }
 
-__global__ void penalty_beta_kernel( double eps, Mat3 ginv, double* result )
+
+// blocks of the penalty-dot reduction (8 warps, one lateral column per warp
+// and step): about 4 columns per warp on large meshes, one column per warp
+// up to two blocks per SM on coarse ones (latency-bound there)
+inline unsigned penalty_blocks( size_t nlat )
 {
-    const double b0 = result[0], b1 = result[1], b2 = result[2];
-    result[3]       = eps * ( ginv.a[0] * b0 + ginv.a[1] * b1 + ginv.a[2] * b2 );
-    result[4]       = eps * ( ginv.a[3] * b0 + ginv.a[4] * b1 + ginv.a[5] * b2 );
-    result[5]       = eps * ( ginv.a[6] * b0 + ginv.a[7] * b1 + ginv.a[8] * b2 );
+    size_t b = ( nlat + 31 ) / 32;
+    b        = std::max( b, std::min< size_t >( ( nlat + 7 ) / 8, 296 ) );
+    return unsigned( std::min< size_t >( b, kRedMaxBlocks ) );
 }
 
 template < typename T >
@@ -906,12 +948,9 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
         Mat3 gi;
         for ( int i = 0; i < 9; ++i )
             gi.a[i] = m->penalty_gram_inv[i];
-        const unsigned blocks = unsigned( std::min< size_t >( ( m->ns + 1023 ) / 1024, kRedMaxBlocks ) );
-        penalty_dots_kernel< T ><<< blocks, 256, 0, st >>>( m->ns, m->n1, m->d_coords, mesh_radii< T >( m ), s,
-                                                           m->d_lat_owned, m->d_red_partials,
-                                                           m->d_red_counter, m->d_red_result );
-        TN_LAUNCH_CHECK();
-        penalty_beta_kernel<<< 1, 1, 0, st >>>( p->penalty_eps, gi, m->d_red_result );
+        penalty_dots_kernel< T ><<< penalty_blocks( m->nlat ), 256, 0, st >>>(
+            m->nlat, m->n1, m->d_coords, mesh_radii< T >( m ), s, m->d_lat_owned, m->d_red_partials, m->d_red_counter,
+            m->d_red_result, p->penalty_eps, gi );
         TN_LAUNCH_CHECK();
     }
 
@@ -970,9 +1009,9 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
         if ( skip_cmb || skip_surf )
         {
             const int       sides   = skip_cmb && skip_surf ? 3 : ( skip_cmb ? 1 : 2 );
-            const long long nodes = (long long) kDiamonds * m->n1 * m->n1 * ( sides == 3 ? 2 : 1 );
-            kerngen_boundary_kernel< T ><<< unsigned( ( nodes + kBndNodes - 1 ) / kBndNodes ), 6 * kBndNodes, 0, st >>>(
-                cell_params( m, p, k, s, o ), sides );
+            const long long cells = (long long) kDiamonds * N * N * ( sides == 3 ? 2 : 1 );
+            kerngen_bcell_kernel< T ><<< unsigned( ( cells + 127 ) / 128 ), 128, 0, st >>>( cell_params( m, p, k, s, o ),
+                                                                                            sides );
             TN_LAUNCH_CHECK();
         }
     }
@@ -991,12 +1030,10 @@ int fsfs_penalty_add( const tn_mesh* m, double eps, const T* const* src, T* cons
     Mat3            gi;
     for ( int i = 0; i < 9; ++i )
         gi.a[i] = m->penalty_gram_inv[i];
-    const unsigned blocks = unsigned( std::min< size_t >( ( m->ns + 1023 ) / 1024, kRedMaxBlocks ) );
-    penalty_dots_kernel< T ><<< blocks, 256, 0, st >>>( m->ns, m->n1, m->d_coords, mesh_radii< T >( m ), s,
-                                                       m->d_lat_owned, m->d_red_partials, m->d_red_counter,
-                                                       m->d_red_result );
-    TN_LAUNCH_CHECK();
-    penalty_beta_kernel<<< 1, 1, 0, st >>>( eps, gi, m->d_red_result );
+    penalty_dots_kernel< T ><<< penalty_blocks( m->nlat ), 256, 0, st >>>( m->nlat, m->n1, m->d_coords,
+                                                                         mesh_radii< T >( m ), s, m->d_lat_owned,
+                                                                         m->d_red_partials, m->d_red_counter,
+                                                                         m->d_red_result, eps, gi );
     TN_LAUNCH_CHECK();
     penalty_axpy_kernel< T ><<< 148 * 8, 256, 0, st >>>( m->ns, m->n1, m->d_coords, mesh_radii< T >( m ),
                                                         m->d_red_result + 3, o );
