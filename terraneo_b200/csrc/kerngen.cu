@@ -16,10 +16,12 @@
 //    factorised as J = M diag(r_mid, r_mid, dr/2) with M the lateral triangle
 //    matrix, so M^{-T} is computed once per tile and each cell only rescales.
 //    Boundary-layer cells of a non-Neumann boundary are left out and added by
-//  * kerngen_cell_kernel: one thread per cell with the full boundary logic
-//    (Dirichlet elimination with kept diagonal, free-slip projection with the
-//    normal-normal add-back, rotated diagonal), accumulating with atomics.  It
-//    also provides the diagonal mode and levels too small for tiling.
+//  * kerngen_bcell_kernel: one thread per boundary-layer cell with the full
+//    boundary logic of cell_full (Dirichlet elimination with kept diagonal,
+//    free-slip projection with the normal-normal add-back), atomics onto the
+//    tile kernel's output;
+//  * kerngen_cell_kernel: the same per-cell logic for every cell (and the
+//    rotated diagonal), for the diagonal mode and levels too small for tiling.
 //  * penalty kernels for free-slip on both boundaries.
 #include <cuda_pipeline.h>
 
@@ -632,176 +634,6 @@ __global__ void __launch_bounds__( 128 ) kerngen_bcell_kernel( CellParams< T > P
             }
 }
 
-// Boundary layers of a non-Neumann boundary, node-centric: one thread per
-// lateral node (d, X, Y) and boundary side visits the six wedges of the
-// boundary cell layer around it and adds their contributions to its two node
-// levels (the boundary node and the one above / below it).  Each wedge is
-// recomputed by each of its three lateral corners instead of scattering with
-// atomics; the tiled kernel has already written every node without these cells.
-// Free-slip: the boundary node's sum is projected once onto the tangent plane
-// and the normal-normal diagonal sum(Ann) (n . u) n added back, which equals
-// the reference's per-cell projection (kerngen :1880-1935) by linearity.
-constexpr int kBndNodes = 32; // boundary nodes per block (6 wedge threads each)
-
-template < typename T >
-__global__ void __launch_bounds__( 6 * kBndNodes ) kerngen_boundary_kernel( CellParams< T > P, int sides )
-{
-    __shared__ T sh[6][7][kBndNodes]; // per wedge: boundary-level (3), interior-level (3), Ann
-    const int       N = P.N, n1 = P.n1;
-    const int       nside = sides == 3 ? 2 : 1;
-    const int       j     = threadIdx.x % kBndNodes; // node slot
-    const int       a     = threadIdx.x / kBndNodes; // wedge around the node
-    const long long t     = blockIdx.x * (long long) kBndNodes + j;
-    const bool      live  = t < (long long) kDiamonds * n1 * n1 * nside;
-    // side slowest, then diamond, x, y: a block's nodes are consecutive in y and
-    // share most of the columns they read
-    const long long per   = (long long) kDiamonds * n1 * n1;
-    const int       si    = live ? int( t / per ) : 0;
-    const int       Y     = int( t % n1 );
-    const int       X     = int( ( t / n1 ) % n1 );
-    const int       d     = int( ( t % per ) / ( (long long) n1 * n1 ) );
-    const int       side  = sides == 3 ? si : ( sides == 1 ? 0 : 1 );
-    const int       rc    = side == 0 ? 0 : N - 1; // boundary cell layer
-    const int       bc    = side == 0 ? P.bc_cmb : P.bc_surf;
-    const bool      fs    = bc == TN_BC_FREESLIP;
-    const T         third = T( 1.0 / 3.0 );
-
-    T sum_b[3] = { 0, 0, 0 }, sum_i[3] = { 0, 0, 0 }, ann = 0;
-    // wedge a around node (X, Y): cell offset, wedge index, local lateral index
-    const int ax  = ( a == 1 || a == 2 || a == 5 ) ? -1 : 0;
-    const int ay  = ( a >= 3 ) ? -1 : 0;
-    const int wdg = ( a == 2 || a == 4 || a == 5 ) ? 1 : 0;
-    const int loc = a == 0 ? 0 : ( a == 1 ? 1 : ( a == 2 ? 2 : ( a == 3 ? 2 : ( a == 4 ? 1 : 0 ) ) ) );
-    const int cx = X + ax, cy = Y + ay;
-    if ( live && cx >= 0 && cx <= N - 1 && cy >= 0 && cy <= N - 1 )
-    {
-        const T r_lo = P.radii[d * n1 + rc], r_hi = P.radii[d * n1 + rc + 1];
-        T       p[3][3], u[6][3], kn[6];
-        size_t  lat[3];
-#pragma unroll
-        for ( int n = 0; n < 3; ++n )
-        {
-            // wedge 0: (0,0),(1,0),(0,1); wedge 1: (1,1),(0,1),(1,0)
-            const int ox = wdg == 0 ? ( n == 1 ? 1 : 0 ) : ( n == 1 ? 0 : 1 );
-            const int oy = wdg == 0 ? ( n == 2 ? 1 : 0 ) : ( n == 2 ? 0 : 1 );
-            lat[n]          = lat_index( n1, d, cx + ox, cy + oy );
-            const double* c = P.coords + lat[n] * 3;
-            p[n][0] = T( c[0] ), p[n][1] = T( c[1] ), p[n][2] = T( c[2] );
-        }
-#pragma unroll
-        for ( int n = 0; n < 6; ++n )
-        {
-            const size_t i = lat[n % 3] * n1 + rc + ( n < 3 ? 0 : 1 );
-            kn[n]          = P.k[i];
-            u[n][0] = P.src.p[0][i], u[n][1] = P.src.p[1][i], u[n][2] = P.src.p[2][i];
-        }
-        T       IT[3][3];
-        const T det = wedge_jacobian_it( p[0], p[1], p[2], r_lo, r_hi, third, third, T( 0 ), IT );
-        const T kwJ = ( ( kn[0] + kn[1] + kn[2] + kn[3] + kn[4] + kn[5] ) / T( 6 ) ) * fabs( det );
-        T       g[6][3];
-#pragma unroll
-        for ( int n = 0; n < 6; ++n )
-        {
-            T gr[3];
-            grad_shape_ref( n, third, third, T( 0 ), gr );
-#pragma unroll
-            for ( int c = 0; c < 3; ++c )
-                g[n][c] = IT[c][0] * gr[0] + IT[c][1] * gr[1] + IT[c][2] * gr[2];
-        }
-        const int nb0 = side == 0 ? 0 : 3; // first boundary-level node of the wedge
-        // trial side: Dirichlet drops the boundary nodes, free-slip projects them
-        T G[3][3] = { { 0 } };
-#pragma unroll
-        for ( int n = 0; n < 6; ++n )
-        {
-            const bool on_b = n >= nb0 && n < nb0 + 3;
-            if ( on_b && !fs )
-                continue;
-            T v[3] = { u[n][0], u[n][1], u[n][2] };
-            if ( on_b )
-            {
-                T       nn[3] = { p[n % 3][0], p[n % 3][1], p[n % 3][2] };
-                const T mm    = sqrt( nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2] );
-                nn[0] /= mm, nn[1] /= mm, nn[2] /= mm;
-                project_out( nn, v );
-            }
-#pragma unroll
-            for ( int i = 0; i < 3; ++i )
-#pragma unroll
-                for ( int k = 0; k < 3; ++k )
-                    G[i][k] += g[n][i] * v[k];
-        }
-        const T div = G[0][0] + G[1][1] + G[2][2];
-        // test side: kwJ (2 eps(u) g_n - 2/3 div g_n) for the node's two levels
-        const int nb = nb0 + loc, ni = side == 0 ? loc + 3 : loc;
-        T         gb[3], gi[3], ub[3], pl[3]; // register selects keep all indexing static
-#pragma unroll
-        for ( int n = 0; n < 6; ++n )
-#pragma unroll
-            for ( int c = 0; c < 3; ++c )
-            {
-                if ( n == nb )
-                    gb[c] = g[n][c], ub[c] = u[n][c];
-                if ( n == ni )
-                    gi[c] = g[n][c];
-                if ( n == loc )
-                    pl[c] = p[n][c];
-            }
-#pragma unroll
-        for ( int c = 0; c < 3; ++c )
-            sum_i[c] = kwJ * ( gi[0] * ( G[0][c] + G[c][0] ) + gi[1] * ( G[1][c] + G[c][1] ) +
-                               gi[2] * ( G[2][c] + G[c][2] ) - T( 2.0 / 3.0 ) * gi[c] * div );
-        const T gg = gb[0] * gb[0] + gb[1] * gb[1] + gb[2] * gb[2];
-        if ( fs )
-        {
-#pragma unroll
-            for ( int c = 0; c < 3; ++c )
-                sum_b[c] = kwJ * ( gb[0] * ( G[0][c] + G[c][0] ) + gb[1] * ( G[1][c] + G[c][1] ) +
-                                   gb[2] * ( G[2][c] + G[c][2] ) - T( 2.0 / 3.0 ) * gb[c] * div );
-            const T mm = sqrt( pl[0] * pl[0] + pl[1] * pl[1] + pl[2] * pl[2] );
-            const T ng = ( pl[0] * gb[0] + pl[1] * gb[1] + pl[2] * gb[2] ) / mm;
-            ann        = kwJ * ( gg + ng * ng * third );
-        }
-        else
-        {
-#pragma unroll
-            for ( int c = 0; c < 3; ++c )
-                sum_b[c] = kwJ * ub[c] * ( gg + gb[c] * gb[c] * third );
-        }
-    }
-#pragma unroll
-    for ( int c = 0; c < 3; ++c )
-        sh[a][c][j] = sum_b[c], sh[a][3 + c][j] = sum_i[c];
-    sh[a][6][j] = ann;
-    __syncthreads();
-    if ( a != 0 || !live )
-        return;
-    T tb[3] = { 0, 0, 0 }, ti[3] = { 0, 0, 0 }, tann = 0;
-    for ( int w = 0; w < 6; ++w )
-    {
-#pragma unroll
-        for ( int c = 0; c < 3; ++c )
-            tb[c] += sh[w][c][j], ti[c] += sh[w][3 + c][j];
-        tann += sh[w][6][j];
-    }
-    const size_t base = lat_index( n1, d, X, Y ) * n1;
-    const int    lb = side == 0 ? 0 : N, li = side == 0 ? 1 : N - 1;
-    if ( fs )
-    {
-        // project the summed boundary-node contribution, add the normal-normal diagonal
-        const double* un     = P.coords + lat_index( n1, d, X, Y ) * 3;
-        T             nrm[3] = { T( un[0] ), T( un[1] ), T( un[2] ) };
-        const T       mm     = sqrt( nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2] );
-        nrm[0] /= mm, nrm[1] /= mm, nrm[2] /= mm;
-        project_out( nrm, tb );
-        const T un_ = nrm[0] * P.src.p[0][base + lb] + nrm[1] * P.src.p[1][base + lb] + nrm[2] * P.src.p[2][base + lb];
-#pragma unroll
-        for ( int c = 0; c < 3; ++c )
-            tb[c] += tann * un_ * nrm[c];
-    }
-    P.dst.p[0][base + lb] += tb[0], P.dst.p[1][base + lb] += tb[1], P.dst.p[2][base + lb] += tb[2];
-    P.dst.p[0][base + li] += ti[0], P.dst.p[1][base + li] += ti[1], P.dst.p[2][base + li] += ti[2];
-}
 
 // ---------------------------------------------------------------------------
 // fs/fs rigid-rotation penalty (kerngen :287-408, :585-606).  The reference
