@@ -439,27 +439,8 @@ __device__ __forceinline__ void project_out( const T n[3], T v[3] )
 }
 
 // Full contribution of cell (d, x, y, r) to its 8 nodes, acc[dx][dy][dr][c].
-// node data of cell_full straight from global memory
 template < typename T >
-struct GlobalCellLoad
-{
-    const CellParams< T >& P;
-    __device__ __forceinline__ const double* coord( int d, int X, int Y ) const
-    {
-        return P.coords + lat_index( P.n1, d, X, Y ) * 3;
-    }
-    __device__ __forceinline__ T k( int d, int X, int Y, int R ) const
-    {
-        return P.k[lat_index( P.n1, d, X, Y ) * P.n1 + R];
-    }
-    __device__ __forceinline__ T src( int c, int d, int X, int Y, int R ) const
-    {
-        return P.src.p[c][lat_index( P.n1, d, X, Y ) * P.n1 + R];
-    }
-};
-
-template < typename T, typename Load = GlobalCellLoad< T > >
-__device__ void cell_full( const CellParams< T >& P, int d, int x, int y, int r, T acc[2][2][2][3], Load ld )
+__device__ void cell_full( const CellParams< T >& P, int d, int x, int y, int r, T acc[2][2][2][3] )
 {
     const int  N = P.N, n1 = P.n1;
     const bool at_cmb = r == 0, at_surf = r == N - 1;
@@ -481,21 +462,24 @@ __device__ void cell_full( const CellParams< T >& P, int d, int x, int y, int r,
     {
         T      p[3][3];
         T      kn[6], s[6][3], sp[6][3], nrm[6][3];
+        size_t idx[6];
         for ( int n = 0; n < 6; ++n )
         {
             const int X = x + kWedgeNode[w][n][0], Y = y + kWedgeNode[w][n][1], R = r + kWedgeNode[w][n][2];
-            const double* u = ld.coord( d, X, Y );
+            const size_t  lat = lat_index( n1, d, X, Y );
+            const double* u   = P.coords + lat * 3;
             if ( n < 3 )
                 for ( int a = 0; a < 3; ++a )
                     p[n][a] = T( u[a] );
-            kn[n] = ld.k( d, X, Y, R );
+            idx[n] = lat * n1 + R;
+            kn[n]  = P.k[idx[n]];
             // outward unit normals, needed by free-slip layers only (one reciprocal square root)
             T nn[3] = { T( u[0] ), T( u[1] ), T( u[2] ) };
             const T im = ( cmb_fs || surf_fs ) ? rsqrt( nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2] ) : T( 0 );
             for ( int c = 0; c < 3; ++c )
             {
                 nrm[n][c] = nn[c] * im;
-                s[n][c] = sp[n][c] = ld.src( c, d, X, Y, R );
+                s[n][c] = sp[n][c] = P.src.p[c][idx[n]];
             }
             if ( ( cmb_fs && n < 3 ) || ( surf_fs && n >= 3 ) )
                 project_out( nrm[n], sp[n] );
@@ -581,15 +565,15 @@ __device__ void cell_full( const CellParams< T >& P, int d, int x, int y, int r,
         for ( int dx = 0; dx < 2; ++dx )
             for ( int dy = 0; dy < 2; ++dy )
             {
-                const double* u    = ld.coord( d, x + dx, y + dy );
+                const size_t  lat = lat_index( n1, d, x + dx, y + dy );
+                const double* u   = P.coords + lat * 3;
                 T             n[3] = { T( u[0] ), T( u[1] ), T( u[2] ) };
                 const T       im   = rsqrt( n[0] * n[0] + n[1] * n[1] + n[2] * n[2] );
                 n[0] *= im, n[1] *= im, n[2] *= im;
                 T* o = acc[dx][dy][dr];
                 project_out( n, o );
-                const int R  = r + dr;
-                const T   un = n[0] * ld.src( 0, d, x + dx, y + dy, R ) + n[1] * ld.src( 1, d, x + dx, y + dy, R ) +
-                             n[2] * ld.src( 2, d, x + dx, y + dy, R );
+                const size_t i  = lat * n1 + r + dr;
+                const T      un = n[0] * P.src.p[0][i] + n[1] * P.src.p[1][i] + n[2] * P.src.p[2][i];
                 for ( int c = 0; c < 3; ++c )
                     o[c] += ann[dx][dy][dr] * un * n[c];
             }
@@ -609,81 +593,7 @@ __global__ void __launch_bounds__( 128 ) kerngen_cell_kernel( CellParams< T > P 
     const int x = int( ( t / ( (long long) N * N ) ) % N );
     const int d = int( t / ( (long long) N * N * N ) );
     T         acc[2][2][2][3];
-    cell_full( P, d, x, y, r, acc, GlobalCellLoad< T >{ P } );
-    for ( int dx = 0; dx < 2; ++dx )
-        for ( int dy = 0; dy < 2; ++dy )
-            for ( int dr = 0; dr < 2; ++dr )
-            {
-                const size_t i = lat_index( n1, d, x + dx, y + dy ) * n1 + r + dr;
-                for ( int c = 0; c < 3; ++c )
-                    atomicAdd( P.dst.p[c] + i, acc[dx][dy][dr][c] );
-            }
-}
-
-// node data of cell_full from a block's shared-memory slab of one boundary
-// layer: columns (x0..x0+TX) x (y0..y0+TY), levels r0 and r0 + 1
-template < typename T >
-struct SlabCellLoad
-{
-    const T*      sk;
-    const T*      ss;
-    const double* sc;
-    int           x0, y0, r0, typ;
-    __device__ __forceinline__ int col( int X, int Y ) const { return ( X - x0 ) * typ + ( Y - y0 ); }
-    __device__ __forceinline__ const double* coord( int, int X, int Y ) const { return sc + col( X, Y ) * 3; }
-    __device__ __forceinline__ T k( int, int X, int Y, int R ) const { return sk[col( X, Y ) * 2 + ( R - r0 )]; }
-    __device__ __forceinline__ T src( int c, int, int X, int Y, int R ) const
-    {
-        return ss[( col( X, Y ) * 2 + ( R - r0 ) ) * 3 + c];
-    }
-};
-
-// Boundary cell layers, tiled: a block owns TX x TY cells of one layer of
-// one diamond and first stages the node data they need -- (TX+1) x (TY+1)
-// lateral columns x 2 levels of k and the three src components, and the
-// columns' unit coordinates -- in shared memory, each value loaded once by
-// the block (the layers cut across the r-fastest layout, so each column's
-// pair of levels is a separate sector; unstaged, every value is fetched by
-// the four cells around it).  Then one thread per cell runs cell_full on the
-// staged data and adds its node contributions with atomics onto the values
-// the tile kernel wrote.
-template < typename T >
-__global__ void __launch_bounds__( 128 ) kerngen_bcell_tile_kernel( CellParams< T > P, int sides, int TX, int TY )
-{
-    extern __shared__ __align__( 16 ) unsigned char smem_raw[];
-    const int N = P.N, n1 = P.n1;
-    const int xt = N / TX, yt = N / TY, tiles = kDiamonds * xt * yt;
-    int       b    = blockIdx.x;
-    const int side = sides == 3 ? b / tiles : ( sides == 1 ? 0 : 1 );
-    b %= tiles;
-    const int d = b / ( xt * yt ), x0 = ( ( b / yt ) % xt ) * TX, y0 = ( b % yt ) * TY;
-    const int r = side == 0 ? 0 : N - 1;
-    const int typ = TY + 1, ncol = ( TX + 1 ) * typ;
-    double*   sc  = reinterpret_cast< double* >( smem_raw ); // ncol x 3
-    T*        sk  = reinterpret_cast< T* >( sc + ncol * 3 );  // ncol x 2 levels
-    T*        ss  = sk + ncol * 2;                            // ncol x 2 levels x 3
-    // eight consecutive threads take one column's k and src at both levels
-    for ( int i = threadIdx.x; i < ncol * 8; i += blockDim.x )
-    {
-        const int    c = i >> 3, f = ( i & 7 ) >> 1, lev = i & 1;
-        const int    X = x0 + c / typ, Y = y0 + c % typ;
-        const size_t g = lat_index( n1, d, X, Y ) * n1 + r + lev;
-        if ( f == 0 )
-            sk[c * 2 + lev] = P.k[g];
-        else
-            ss[( c * 2 + lev ) * 3 + f - 1] = P.src.p[f - 1][g];
-    }
-    for ( int i = threadIdx.x; i < ncol * 3; i += blockDim.x )
-    {
-        const int c = i / 3, a = i % 3;
-        sc[i]       = P.coords[lat_index( n1, d, x0 + c / typ, y0 + c % typ ) * 3 + a];
-    }
-    __syncthreads();
-    if ( int( threadIdx.x ) >= TX * TY )
-        return;
-    const int x = x0 + int( threadIdx.x ) / TY, y = y0 + int( threadIdx.x ) % TY;
-    T         acc[2][2][2][3];
-    cell_full( P, d, x, y, r, acc, SlabCellLoad< T >{ sk, ss, sc, x0, y0, r, typ } );
+    cell_full( P, d, x, y, r, acc );
     for ( int dx = 0; dx < 2; ++dx )
         for ( int dy = 0; dy < 2; ++dy )
             for ( int dr = 0; dr < 2; ++dr )
@@ -713,7 +623,7 @@ __global__ void __launch_bounds__( 128 ) kerngen_bcell_kernel( CellParams< T > P
     const int x    = int( ( t / N ) % N );
     const int d    = int( ( t % per ) / ( (long long) N * N ) );
     T         acc[2][2][2][3];
-    cell_full( P, d, x, y, r, acc, GlobalCellLoad< T >{ P } );
+    cell_full( P, d, x, y, r, acc );
     for ( int dx = 0; dx < 2; ++dx )
         for ( int dy = 0; dy < 2; ++dy )
             for ( int dr = 0; dr < 2; ++dr )
@@ -931,13 +841,9 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
         if ( skip_cmb || skip_surf )
         {
             const int       sides   = skip_cmb && skip_surf ? 3 : ( skip_cmb ? 1 : 2 );
-            // tiles of TX x TY cells (N >= 8 here: a power of two)
-            const int    TY     = std::min( 32, N ), TX = std::min( 128 / TY, N );
-            const int    ncol   = ( TX + 1 ) * ( TY + 1 );
-            const size_t bsmem  = size_t( ncol ) * ( 3 * sizeof( double ) + 8 * sizeof( T ) );
-            const int    blocks = kDiamonds * ( N / TX ) * ( N / TY ) * ( sides == 3 ? 2 : 1 );
-            kerngen_bcell_tile_kernel< T ><<< blocks, TX * TY, bsmem, st >>>( cell_params( m, p, k, s, o ), sides, TX,
-                                                                               TY );
+            const long long cells = (long long) kDiamonds * N * N * ( sides == 3 ? 2 : 1 );
+            kerngen_bcell_kernel< T ><<< unsigned( ( cells + 127 ) / 128 ), 128, 0, st >>>( cell_params( m, p, k, s, o ),
+                                                                                            sides );
             TN_LAUNCH_CHECK();
         }
     }
