@@ -30,8 +30,8 @@
 // formed per cell: the same integrals as the per-point Jacobian of
 // fe/wedge/integrands.hpp at a fraction of the arithmetic.
 //
-// One thread per fine cell (r fastest), both wedges, contributions summed per
-// node in registers and added with atomics.
+// One thread per fine wedge (the wedge uniform within a warp), contributions
+// added with atomics.
 #include <cmath>
 
 #include "common.cuh"
@@ -87,11 +87,12 @@ __device__ __forceinline__ int velocity_bc( int N, int r, int n, int bc_cmb, int
     return 0;
 }
 
+// outward unit normal x / |x| (one reciprocal square root)
 template < typename T >
 __device__ __forceinline__ void unit_normal( const double* c, T n[3] )
 {
-    double m = sqrt( c[0] * c[0] + c[1] * c[1] + c[2] * c[2] );
-    n[0] = T( c[0] / m ), n[1] = T( c[1] / m ), n[2] = T( c[2] / m );
+    const double im = rsqrt( c[0] * c[0] + c[1] * c[1] + c[2] * c[2] );
+    n[0] = T( c[0] * im ), n[1] = T( c[1] * im ), n[2] = T( c[2] * im );
 }
 
 // radial sums of one fine cell: Ra[ib][nb] = h sum_zeta radc_ib r nr_nb, Rb[ib] = sum_zeta radc_ib r^2
@@ -124,168 +125,170 @@ __device__ __forceinline__ size_t stokes_tri( int N, int dm, int x, int y, int w
     return ( ( size_t( dm ) * N + x ) * N + y ) * 2 + w;
 }
 
-// p_coarse += B u
-template < typename T >
-__global__ void __launch_bounds__( 128 ) divergence_kernel( StokesParams< T > P, Ptr3< const T > u, T* __restrict__ p )
+// One thread per fine wedge: the first half of the grid takes wedge 0 of
+// every fine cell, the second half wedge 1, so the wedge is uniform within a
+// warp and a compile-time constant in the body; each wedge adds its six node
+// contributions with atomics (half the registers of a two-wedge thread, twice
+// the threads).
+__device__ __forceinline__ void fine_cell( int N, long long c, int& dm, int& x, int& y, int& r )
 {
-    const int       N = P.N, n1 = P.n1, nc1 = P.nc1;
-    const long long t = blockIdx.x * (long long) blockDim.x + threadIdx.x;
-    if ( t >= (long long) kDiamonds * N * N * N )
-        return;
-    const int r  = int( t % N );
-    const int y  = int( ( t / N ) % N );
-    const int x  = int( ( t / ( (long long) N * N ) ) % N );
-    const int dm = int( t / ( (long long) N * N * N ) );
-    T         out[2][2][2];
-#pragma unroll
-    for ( int i = 0; i < 8; ++i )
-        out[i >> 2][( i >> 1 ) & 1][i & 1] = T( 0 );
-    T Ra[2][2], Rb[2];
-    radial_sums( P.radii[dm * n1 + r], P.radii[dm * n1 + r + 1], r & 1, Ra, Rb );
-#pragma unroll
-    for ( int w = 0; w < 2; ++w )
-    {
-        const double* G = P.geom + stokes_tri( N, dm, x, y, w ) * kStokesStride;
-        T             uu[6][3];
-#pragma unroll
-        for ( int n = 0; n < 6; ++n )
-        {
-            const int    X = x + kWedgeNode[w][n][0], Y = y + kWedgeNode[w][n][1];
-            const size_t i = lat_index( n1, dm, X, Y ) * n1 + r + kWedgeNode[w][n][2];
-            uu[n][0] = u.p[0][i], uu[n][1] = u.p[1][i], uu[n][2] = u.p[2][i];
-            const int bc = velocity_bc( N, r, n, P.bc_cmb, P.bc_surf );
-            if ( bc == TN_BC_DIRICHLET )
-                uu[n][0] = uu[n][1] = uu[n][2] = T( 0 );
-            else if ( bc == TN_BC_FREESLIP )
-            {
-                T nn[3];
-                unit_normal( P.coords + lat_index( n1, dm, X, Y ) * 3, nn );
-                const T dt = nn[0] * uu[n][0] + nn[1] * uu[n][1] + nn[2] * uu[n][2];
-                uu[n][0] -= dt * nn[0], uu[n][1] -= dt * nn[1], uu[n][2] -= dt * nn[2];
-            }
-        }
-        const T vt[3] = { T( G[27] ), T( G[28] ), T( G[29] ) };
-        T       vu[6];
-#pragma unroll
-        for ( int n = 0; n < 6; ++n )
-            vu[n] = ( n < 3 ? T( -0.5 ) : T( 0.5 ) ) * ( vt[0] * uu[n][0] + vt[1] * uu[n][1] + vt[2] * uu[n][2] );
-        T acc[6] = { 0, 0, 0, 0, 0, 0 };
-#pragma unroll
-        for ( int ic = 0; ic < 3; ++ic )
-#pragma unroll
-            for ( int m = 0; m < 3; ++m )
-            {
-                const double* U  = G + ( ic * 3 + m ) * 3;
-                const T       U0 = T( U[0] ), U1 = T( U[1] ), U2 = T( U[2] ), lc = T( G[30 + ic * 3 + m] );
-#pragma unroll
-                for ( int nb = 0; nb < 2; ++nb )
-                {
-                    const int n  = nb * 3 + m;
-                    const T   cu = U0 * uu[n][0] + U1 * uu[n][1] + U2 * uu[n][2];
-                    const T   lv = lc * vu[n];
-#pragma unroll
-                    for ( int ib = 0; ib < 2; ++ib )
-                        acc[ib * 3 + ic] += Ra[ib][nb] * cu + Rb[ib] * lv;
-                }
-            }
-#pragma unroll
-        for ( int i = 0; i < 6; ++i )
-            out[kWedgeNode[w][i][0]][kWedgeNode[w][i][1]][kWedgeNode[w][i][2]] += acc[i];
-    }
-    const int xc = x >> 1, yc = y >> 1, rc = r >> 1;
-#pragma unroll
-    for ( int a = 0; a < 8; ++a )
-    {
-        const int dx = a >> 2, dy = ( a >> 1 ) & 1, dr = a & 1;
-        atomicAdd( p + lat_index( nc1, dm, xc + dx, yc + dy ) * nc1 + rc + dr, out[dx][dy][dr] );
-    }
+    r  = int( c % N );
+    y  = int( ( c / N ) % N );
+    x  = int( ( c / ( (long long) N * N ) ) % N );
+    dm = int( c / ( (long long) N * N * N ) );
 }
 
-// u_fine += B^T p
-template < typename T >
-__global__ void __launch_bounds__( 128 ) gradient_kernel( StokesParams< T > P, const T* __restrict__ p, Ptr3< T > u )
+// p_coarse += B u, wedge W of fine cell (dm, x, y, r)
+template < typename T, int W >
+__device__ __forceinline__ void divergence_wedge( const StokesParams< T >& P, const Ptr3< const T >& u, T* p, int dm,
+                                                  int x, int y, int r )
 {
-    const int       N = P.N, n1 = P.n1, nc1 = P.nc1;
-    const long long t = blockIdx.x * (long long) blockDim.x + threadIdx.x;
-    if ( t >= (long long) kDiamonds * N * N * N )
-        return;
-    const int r  = int( t % N );
-    const int y  = int( ( t / N ) % N );
-    const int x  = int( ( t / ( (long long) N * N ) ) % N );
-    const int dm = int( t / ( (long long) N * N * N ) );
-    T         out[2][2][2][3];
-#pragma unroll
-    for ( int i = 0; i < 8; ++i )
-#pragma unroll
-        for ( int c = 0; c < 3; ++c )
-            out[i >> 2][( i >> 1 ) & 1][i & 1][c] = T( 0 );
-    const int xc = x >> 1, yc = y >> 1, rc = r >> 1;
+    const int N = P.N, n1 = P.n1, nc1 = P.nc1;
     T         Ra[2][2], Rb[2];
     radial_sums( P.radii[dm * n1 + r], P.radii[dm * n1 + r + 1], r & 1, Ra, Rb );
+    const double* G = P.geom + stokes_tri( N, dm, x, y, W ) * kStokesStride;
+    T             uu[6][3];
 #pragma unroll
-    for ( int w = 0; w < 2; ++w )
+    for ( int n = 0; n < 6; ++n )
     {
-        const double* G = P.geom + stokes_tri( N, dm, x, y, w ) * kStokesStride;
-        T             pc[6];
-#pragma unroll
-        for ( int i = 0; i < 6; ++i )
-            pc[i] = p[lat_index( nc1, dm, xc + kWedgeNode[w][i][0], yc + kWedgeNode[w][i][1] ) * nc1 + rc +
-                      kWedgeNode[w][i][2]];
-        const T vt[3] = { T( G[27] ), T( G[28] ), T( G[29] ) };
-        // pr[nb][ic] = sum_ib Ra[ib][nb] pc[ib][ic]; pl[ic] = sum_ib Rb[ib] pc[ib][ic]
-        T pr[2][3], pl[3];
-#pragma unroll
-        for ( int ic = 0; ic < 3; ++ic )
+        const int    X = x + kWedgeNode[W][n][0], Y = y + kWedgeNode[W][n][1];
+        const size_t i = lat_index( n1, dm, X, Y ) * n1 + r + kWedgeNode[W][n][2];
+        uu[n][0] = u.p[0][i], uu[n][1] = u.p[1][i], uu[n][2] = u.p[2][i];
+        const int bc = velocity_bc( N, r, n, P.bc_cmb, P.bc_surf );
+        if ( bc == TN_BC_DIRICHLET )
+            uu[n][0] = uu[n][1] = uu[n][2] = T( 0 );
+        else if ( bc == TN_BC_FREESLIP )
         {
-            pl[ic] = Rb[0] * pc[ic] + Rb[1] * pc[3 + ic];
-#pragma unroll
-            for ( int nb = 0; nb < 2; ++nb )
-                pr[nb][ic] = Ra[0][nb] * pc[ic] + Ra[1][nb] * pc[3 + ic];
+            T nn[3];
+            unit_normal( P.coords + lat_index( n1, dm, X, Y ) * 3, nn );
+            const T dt = nn[0] * uu[n][0] + nn[1] * uu[n][1] + nn[2] * uu[n][2];
+            uu[n][0] -= dt * nn[0], uu[n][1] -= dt * nn[1], uu[n][2] -= dt * nn[2];
         }
+    }
+    const T vt[3] = { T( G[27] ), T( G[28] ), T( G[29] ) };
+    T       vu[6];
+#pragma unroll
+    for ( int n = 0; n < 6; ++n )
+        vu[n] = ( n < 3 ? T( -0.5 ) : T( 0.5 ) ) * ( vt[0] * uu[n][0] + vt[1] * uu[n][1] + vt[2] * uu[n][2] );
+    T acc[6] = { 0, 0, 0, 0, 0, 0 };
+#pragma unroll
+    for ( int ic = 0; ic < 3; ++ic )
 #pragma unroll
         for ( int m = 0; m < 3; ++m )
         {
-            T sv = T( 0 );
-#pragma unroll
-            for ( int ic = 0; ic < 3; ++ic )
-                sv += T( G[30 + ic * 3 + m] ) * pl[ic];
+            const double* U  = G + ( ic * 3 + m ) * 3;
+            const T       U0 = T( U[0] ), U1 = T( U[1] ), U2 = T( U[2] ), lc = T( G[30 + ic * 3 + m] );
 #pragma unroll
             for ( int nb = 0; nb < 2; ++nb )
             {
-                const int j = nb * 3 + m;
-                const T   s = ( nb ? T( 0.5 ) : T( -0.5 ) ) * sv;
-                T         v[3] = { s * vt[0], s * vt[1], s * vt[2] };
+                const int n  = nb * 3 + m;
+                const T   cu = U0 * uu[n][0] + U1 * uu[n][1] + U2 * uu[n][2];
+                const T   lv = lc * vu[n];
 #pragma unroll
-                for ( int ic = 0; ic < 3; ++ic )
-                {
-                    const double* U = G + ( ic * 3 + m ) * 3;
-                    v[0] += pr[nb][ic] * T( U[0] ), v[1] += pr[nb][ic] * T( U[1] ), v[2] += pr[nb][ic] * T( U[2] );
-                }
-                const int bc = velocity_bc( N, r, j, P.bc_cmb, P.bc_surf );
-                if ( bc == TN_BC_DIRICHLET )
-                    continue;
-                if ( bc == TN_BC_FREESLIP )
-                {
-                    T nn[3];
-                    unit_normal( P.coords + lat_index( n1, dm, x + kWedgeNode[w][j][0], y + kWedgeNode[w][j][1] ) * 3,
-                                 nn );
-                    const T dt = nn[0] * v[0] + nn[1] * v[1] + nn[2] * v[2];
-                    v[0] -= dt * nn[0], v[1] -= dt * nn[1], v[2] -= dt * nn[2];
-                }
-                T* o = out[kWedgeNode[w][j][0]][kWedgeNode[w][j][1]][kWedgeNode[w][j][2]];
-                o[0] += v[0], o[1] += v[1], o[2] += v[2];
+                for ( int ib = 0; ib < 2; ++ib )
+                    acc[ib * 3 + ic] += Ra[ib][nb] * cu + Rb[ib] * lv;
             }
         }
+    const int xc = x >> 1, yc = y >> 1, rc = r >> 1;
+#pragma unroll
+    for ( int i = 0; i < 6; ++i )
+        atomicAdd( p + lat_index( nc1, dm, xc + kWedgeNode[W][i][0], yc + kWedgeNode[W][i][1] ) * nc1 + rc +
+                       kWedgeNode[W][i][2],
+                   acc[i] );
+}
+
+template < typename T >
+__global__ void __launch_bounds__( 128 ) divergence_kernel( StokesParams< T > P, Ptr3< const T > u, T* __restrict__ p )
+{
+    const long long cells = (long long) kDiamonds * P.N * P.N * P.N;
+    const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if ( t >= 2 * cells )
+        return;
+    int dm, x, y, r;
+    fine_cell( P.N, t < cells ? t : t - cells, dm, x, y, r );
+    if ( t < cells )
+        divergence_wedge< T, 0 >( P, u, p, dm, x, y, r );
+    else
+        divergence_wedge< T, 1 >( P, u, p, dm, x, y, r );
+}
+
+// u_fine += B^T p, wedge W of fine cell (dm, x, y, r)
+template < typename T, int W >
+__device__ __forceinline__ void gradient_wedge( const StokesParams< T >& P, const T* p, const Ptr3< T >& u, int dm,
+                                                int x, int y, int r )
+{
+    const int N = P.N, n1 = P.n1, nc1 = P.nc1;
+    const int xc = x >> 1, yc = y >> 1, rc = r >> 1;
+    T         Ra[2][2], Rb[2];
+    radial_sums( P.radii[dm * n1 + r], P.radii[dm * n1 + r + 1], r & 1, Ra, Rb );
+    const double* G = P.geom + stokes_tri( N, dm, x, y, W ) * kStokesStride;
+    T             pc[6];
+#pragma unroll
+    for ( int i = 0; i < 6; ++i )
+        pc[i] = p[lat_index( nc1, dm, xc + kWedgeNode[W][i][0], yc + kWedgeNode[W][i][1] ) * nc1 + rc +
+                  kWedgeNode[W][i][2]];
+    const T vt[3] = { T( G[27] ), T( G[28] ), T( G[29] ) };
+    // pr[nb][ic] = sum_ib Ra[ib][nb] pc[ib][ic]; pl[ic] = sum_ib Rb[ib] pc[ib][ic]
+    T pr[2][3], pl[3];
+#pragma unroll
+    for ( int ic = 0; ic < 3; ++ic )
+    {
+        pl[ic] = Rb[0] * pc[ic] + Rb[1] * pc[3 + ic];
+#pragma unroll
+        for ( int nb = 0; nb < 2; ++nb )
+            pr[nb][ic] = Ra[0][nb] * pc[ic] + Ra[1][nb] * pc[3 + ic];
     }
 #pragma unroll
-    for ( int a = 0; a < 8; ++a )
+    for ( int m = 0; m < 3; ++m )
     {
-        const int    dx = a >> 2, dy = ( a >> 1 ) & 1, dr = a & 1;
-        const size_t i  = lat_index( n1, dm, x + dx, y + dy ) * n1 + r + dr;
-        atomicAdd( u.p[0] + i, out[dx][dy][dr][0] );
-        atomicAdd( u.p[1] + i, out[dx][dy][dr][1] );
-        atomicAdd( u.p[2] + i, out[dx][dy][dr][2] );
+        T sv = T( 0 );
+#pragma unroll
+        for ( int ic = 0; ic < 3; ++ic )
+            sv += T( G[30 + ic * 3 + m] ) * pl[ic];
+#pragma unroll
+        for ( int nb = 0; nb < 2; ++nb )
+        {
+            const int j = nb * 3 + m;
+            const T   s = ( nb ? T( 0.5 ) : T( -0.5 ) ) * sv;
+            T         v[3] = { s * vt[0], s * vt[1], s * vt[2] };
+#pragma unroll
+            for ( int ic = 0; ic < 3; ++ic )
+            {
+                const double* U = G + ( ic * 3 + m ) * 3;
+                v[0] += pr[nb][ic] * T( U[0] ), v[1] += pr[nb][ic] * T( U[1] ), v[2] += pr[nb][ic] * T( U[2] );
+            }
+            const int bc = velocity_bc( N, r, j, P.bc_cmb, P.bc_surf );
+            if ( bc == TN_BC_DIRICHLET )
+                continue;
+            const int X = x + kWedgeNode[W][j][0], Y = y + kWedgeNode[W][j][1];
+            if ( bc == TN_BC_FREESLIP )
+            {
+                T nn[3];
+                unit_normal( P.coords + lat_index( n1, dm, X, Y ) * 3, nn );
+                const T dt = nn[0] * v[0] + nn[1] * v[1] + nn[2] * v[2];
+                v[0] -= dt * nn[0], v[1] -= dt * nn[1], v[2] -= dt * nn[2];
+            }
+            const size_t i = lat_index( n1, dm, X, Y ) * n1 + r + kWedgeNode[W][j][2];
+            atomicAdd( u.p[0] + i, v[0] );
+            atomicAdd( u.p[1] + i, v[1] );
+            atomicAdd( u.p[2] + i, v[2] );
+        }
     }
+}
+
+template < typename T >
+__global__ void __launch_bounds__( 128 ) gradient_kernel( StokesParams< T > P, const T* __restrict__ p, Ptr3< T > u )
+{
+    const long long cells = (long long) kDiamonds * P.N * P.N * P.N;
+    const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if ( t >= 2 * cells )
+        return;
+    int dm, x, y, r;
+    fine_cell( P.N, t < cells ? t : t - cells, dm, x, y, r );
+    if ( t < cells )
+        gradient_wedge< T, 0 >( P, p, u, dm, x, y, r );
+    else
+        gradient_wedge< T, 1 >( P, p, u, dm, x, y, r );
 }
 
 // Host tabulation of the lateral factors of every fine wedge (double).
@@ -397,7 +400,7 @@ int divergence_apply( const tn_mesh* f, const tn_mesh* c, int bc_cmb, int bc_sur
         return TN_ERR_NOMEM;
     }
     const long long   cells = (long long) kDiamonds * f->N * f->N * f->N;
-    divergence_kernel< T ><<< unsigned( ( cells + 127 ) / 128 ), 128, 0, st >>>( P, Ptr3< const T >{ { u[0], u[1], u[2] } },
+    divergence_kernel< T ><<< unsigned( ( 2 * cells + 127 ) / 128 ), 128, 0, st >>>( P, Ptr3< const T >{ { u[0], u[1], u[2] } },
                                                                                 p );
     TN_LAUNCH_CHECK();
     if ( comm_mode == TN_COMM_ADDITIVE )
@@ -426,7 +429,7 @@ int gradient_apply( const tn_mesh* f, const tn_mesh* c, int bc_cmb, int bc_surf,
         return TN_ERR_NOMEM;
     }
     const long long   cells = (long long) kDiamonds * f->N * f->N * f->N;
-    gradient_kernel< T ><<< unsigned( ( cells + 127 ) / 128 ), 128, 0, st >>>( P, p, Ptr3< T >{ { u[0], u[1], u[2] } } );
+    gradient_kernel< T ><<< unsigned( ( 2 * cells + 127 ) / 128 ), 128, 0, st >>>( P, p, Ptr3< T >{ { u[0], u[1], u[2] } } );
     TN_LAUNCH_CHECK();
     if ( comm_mode == TN_COMM_ADDITIVE )
         return halo_sum< T >( f, u, 3, st );
