@@ -44,6 +44,8 @@
 #include "fe/wedge/operators/shell/divergence.hpp"
 #include "fe/wedge/operators/shell/gradient.hpp"
 #include "fe/wedge/operators/shell/kmass.hpp"
+#include "fe/wedge/operators/shell/mass.hpp"
+#include "fe/wedge/operators/shell/vector_mass.hpp"
 #include "fe/wedge/operators/shell/laplace.hpp"
 #include "fe/wedge/operators/shell/prolongation_constant.hpp"
 #include "fe/wedge/operators/shell/prolongation_linear.hpp"
@@ -316,6 +318,30 @@ int cmd_kmass( int L, double rmin, double rmax, int mode, const std::string& dir
     return 0;
 }
 
+// Mass (mass.hpp) on the scalar src (mode 0 full, 1 diagonal, 2 lumped) and
+// VectorMass< double, 3 > (vector_mass.hpp) on the vector src (mode 0 full,
+// 1 diagonal)
+int cmd_mass( bool vec, int L, double rmin, double rmax, int mode, const std::string& dir )
+{
+    Setup s( L, rmin, rmax );
+    if ( !vec )
+    {
+        linalg::VectorQ1Scalar< double > src( "src", s.domain, s.omask ), dst( "dst", s.domain, s.omask );
+        view_from_host( src.grid_data(), read_file< double >( dir + "/src.bin", s.nodes ).data() );
+        fe::wedge::operators::shell::Mass< double > op( s.domain, s.coords, s.radii, mode == 1, mode == 2 );
+        linalg::apply( op, src, dst );
+        auto out = view_to_host( dst.grid_data() );
+        write_file( dir + "/dst.bin", out.data(), out.size() );
+        return 0;
+    }
+    linalg::VectorQ1Vec< double > src( "src", s.domain, s.omask ), dst( "dst", s.domain, s.omask );
+    load_vec( src, dir + "/src.bin", s.nodes );
+    fe::wedge::operators::shell::VectorMass< double, 3 > op( s.domain, s.coords, s.radii, mode == 1 );
+    linalg::apply( op, src, dst );
+    save_vec( dst, dir + "/dst.bin", s.nodes );
+    return 0;
+}
+
 int cmd_transfer_linear( bool prolong, int Lf, double rmin, double rmax, const std::string& dir )
 {
     Setup                            f( Lf, rmin, rmax ), c( Lf - 1, rmin, rmax );
@@ -485,6 +511,8 @@ int main( int argc, char** argv )
         return cmd_divkgrad( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( cmd == "vlaplace" && argc == 9 )
         return cmd_vlaplace( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
+    if ( ( cmd == "mass" || cmd == "vmass" ) && argc == 7 )
+        return cmd_mass( cmd == "vmass", I( 2 ), D( 3 ), D( 4 ), I( 5 ), argv[6] );
     if ( cmd == "laplace_cg" && argc == 8 )
         return cmd_laplace_cg( I( 2 ), D( 3 ), D( 4 ), I( 5 ), D( 6 ), argv[7] );
     if ( cmd == "laplace" && argc == 8 )

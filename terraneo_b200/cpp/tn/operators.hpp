@@ -448,6 +448,43 @@ class KMass
     int                 mode_ = 0;
 };
 
+// VectorMass (vector_mass.hpp:17): the mass matrix (k = 1; full or diagonal)
+// applied to each of the NC components (the reference's ViscousMass)
+template < typename T, int NC = 3 >
+class VectorMass
+{
+  public:
+    using SrcVectorType = VectorQ1Base< T, NC >;
+    using DstVectorType = VectorQ1Base< T, NC >;
+    using ScalarType    = T;
+    VectorMass() = default;
+    VectorMass( const Mesh& mesh, bool diagonal ) : mesh_( mesh ), mode_( diagonal ? 1 : 0 ) {}
+    void set_operator_apply_and_communication_modes( OperatorApplyMode am, OperatorCommunicationMode cm )
+    {
+        am_ = am, cm_ = cm;
+    }
+    void apply_impl( const SrcVectorType& src, DstVectorType& dst )
+    {
+        for ( int c = 0; c < NC; ++c )
+        {
+            if constexpr ( std::is_same_v< T, double > )
+                check( tn_kmass_apply_f64( mesh_.get(), nullptr, mode_, int( am_ ), int( cm_ ), src.comp( c ),
+                                           dst.comp( c ), stream() ),
+                       "vector mass apply" );
+            else
+                check( tn_kmass_apply_f32( mesh_.get(), nullptr, mode_, int( am_ ), int( cm_ ), src.comp( c ),
+                                           dst.comp( c ), stream() ),
+                       "vector mass apply" );
+        }
+    }
+
+  private:
+    Mesh                      mesh_;
+    int                       mode_ = 0;
+    OperatorApplyMode         am_   = OperatorApplyMode::Replace;
+    OperatorCommunicationMode cm_   = OperatorCommunicationMode::CommunicateAdditively;
+};
+
 // DiagonallyScaledOperator (linalg/diagonally_scaled_operator.hpp:15): D^{-1} A
 template < typename Op >
 class DiagonallyScaledOperator

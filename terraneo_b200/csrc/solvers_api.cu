@@ -648,3 +648,7 @@ extern "C" int tn_laplace_pcg_solve_f64( const tn_mesh* mesh, const double* b, d
         return TN_ERR_STATE;
     }
 }
+
+// compile the header-only operators that no driver above instantiates
+template class tn::VectorMass< double, 3 >;
+template class tn::VectorMass< float, 3 >;

@@ -297,6 +297,20 @@ class KMass:
                   ctypes.c_void_p(dst.data.data_ptr()), _stream()), "kmass_apply")
 
 
+class VectorMass:
+    """VectorMass (fe/wedge/operators/shell/vector_mass.hpp:17): Mass (k = 1) on each component; full or diagonal."""
+
+    def __init__(self, mesh, diagonal=False, apply_mode=C.APPLY_REPLACE, comm_mode=C.COMM_ADDITIVE):
+        self.mesh, self.mode, self.am, self.cm = mesh, int(bool(diagonal)), apply_mode, comm_mode
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_kmass_apply_{src.tag}")
+        for c in range(src.ncomp):
+            C.check(f(self.mesh.handle, ctypes.c_void_p(0), self.mode, self.am, self.cm,
+                      ctypes.c_void_p(src.data[c].data_ptr()), ctypes.c_void_p(dst.data[c].data_ptr()), _stream()),
+                    "vector_mass_apply")
+
+
 class Divergence:
     """Divergence (fe/wedge/operators/shell/divergence.hpp:30): fine velocity -> coarse pressure."""
 

@@ -27,6 +27,8 @@ KERNGEN_CASES = [(1, 1, 0), (2, 2, 0), (2, 1, 0), (1, 2, 0), (0, 0, 0), (0, 1, 0
 LAPLACE_CASES = [(1, 0), (0, 0), (1, 1)]
 STOKES_BCS = [(1, 1), (2, 2), (0, 0)]
 KMASS_MODES = [0, 1, 2]
+MASS_MODES = [0, 1, 2]
+VMASS_MODES = [0, 1]
 DIVKGRAD_CASES = [(1, 0, 0), (0, 0, 0), (1, 1, 0), (1, 0, 1)]
 EPSDIVDIV_CASES = [(1, 0), (0, 0), (1, 1)]
 VLAPLACE_CASES = [(1, 1, 0), (0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 1)]
@@ -133,6 +135,13 @@ def main():
         for mode in KMASS_MODES:
             run_ref(["kmass", L, R_MIN, R_MAX, mode, d], d)
             out[f"kmass_{mode}"] = np.fromfile(f"{d}/dst.bin").reshape(fine.shape)
+        for mode in MASS_MODES:
+            run_ref(["mass", L, R_MIN, R_MAX, mode, d], d)
+            out[f"mass_{mode}"] = np.fromfile(f"{d}/dst.bin").reshape(fine.shape)
+        x["u"].tofile(f"{d}/src.bin")
+        for mode in VMASS_MODES:
+            run_ref(["vmass", L, R_MIN, R_MAX, mode, d], d)
+            out[f"vmass_{mode}"] = np.fromfile(f"{d}/dst.bin").reshape((3,) + fine.shape)
         x["u"].tofile(f"{d}/src.bin")
         for treat, diag in EPSDIVDIV_CASES:
             run_ref(["epsdivdiv", L, R_MIN, R_MAX, treat, diag, d], d)

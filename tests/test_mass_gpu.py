@@ -26,3 +26,21 @@ def test_kmass(L, mode):
     shell.apply(shell.KMass(pm, None, mode), src, dst2)
     torch.cuda.synchronize()
     assert rel(dst2.numpy()[0], om.kmass(np.ones(om.shape), u, mode)) <= 1e-13
+
+
+@pytest.mark.parametrize("diag", [False, True])
+def test_vector_mass_matches_reference_golden(diag):
+    """VectorMass against the reference's own VectorMass outputs (golden level-2 fixture)."""
+    import os
+    import sys
+    from terraneo_b200 import shell
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden as G
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_L2.npz"))
+    fine, coarse = Mesh(G.L), Mesh(G.L - 1)
+    u = G.inputs(fine, coarse)["u"]
+    pm = shell.ShellMesh(G.L)
+    src, dst = shell.VectorQ1Vec(pm), shell.VectorQ1Vec(pm)
+    src.set_numpy(u)
+    shell.apply(shell.VectorMass(pm, diag), src, dst)
+    assert rel(dst.numpy(), g[f"vmass_{int(diag)}"]) <= 1e-13

@@ -77,6 +77,21 @@ def test_linear_transfers_match_reference(case):
     assert rel(fine.restrict_linear(coarse, x["s"]), g["restrict_linear"]) <= TOL
 
 
+@pytest.mark.parametrize("mode", G.MASS_MODES)
+def test_mass_is_kmass_with_unit_k(case, mode):
+    """Mass (mass.hpp) equals KMass with k = 1: the oracle's kmass with unit k reproduces it."""
+    g, fine, _, x = case
+    assert rel(fine.kmass(np.ones(fine.shape), x["s"], mode), g[f"mass_{mode}"]) <= TOL
+
+
+@pytest.mark.parametrize("mode", G.VMASS_MODES)
+def test_vector_mass_is_componentwise_mass(case, mode):
+    """VectorMass (vector_mass.hpp) applies Mass to each component."""
+    g, fine, _, x = case
+    ref = np.stack([fine.kmass(np.ones(fine.shape), x["u"][c], mode) for c in range(3)])
+    assert rel(ref, g[f"vmass_{mode}"]) <= TOL
+
+
 @pytest.mark.parametrize("mode", G.KMASS_MODES)
 def test_kmass_matches_reference(case, mode):
     g, fine, _, x = case
