@@ -1,0 +1,145 @@
+"""Size-independent properties at the benchmark sizes (level 6 velocity / level 5 pressure and stored
+matrices), where the oracle is too slow for a direct comparison: symmetry and linearity of the
+operators, B and B^T as exact transposes, restriction as the transpose of prolongation, the stored
+apply equal to the matrix-free one, FP32 against FP64, and the true residual of the level-6 Stokes
+solve."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import rel, viscosity_field
+from oracle_lib import Mesh
+
+pytestmark = pytest.mark.gpu
+
+L = 6
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def meshes():
+    from terraneo_b200 import shell
+    pf, pc = shell.ShellMesh(L), shell.ShellMesh(L - 1)
+    k = shell.VectorQ1Scalar(pf)
+    k.set_numpy(viscosity_field(Mesh(L), seed=6, contrast=1e4))
+    return pf, pc, k
+
+
+def consistent(shell, mesh, ncomp, seed, dtype=torch.float64):
+    """seeded N(0,1) field with equal values on duplicated nodes (owner's value, then the halo sum)"""
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    v = shell.VectorQ1Vec(mesh, dtype) if ncomp == 3 else shell.VectorQ1Scalar(mesh, dtype)
+    v.data.copy_(torch.randn(v.data.shape, generator=g, device="cuda", dtype=dtype))
+    _, omask = mesh.masks()
+    v.data.mul_(torch.as_tensor(omask, device="cuda", dtype=dtype))
+    v.halo_sum()
+    return v
+
+
+def applied(shell, op, src, cls, mesh=None):
+    out = cls(mesh if mesh is not None else src.mesh)
+    shell.apply(op, src, out)
+    return out
+
+
+@pytest.mark.parametrize("bc", [(1, 1), (2, 1)])
+def test_epsdivdiv_symmetric_and_linear_at_level6(meshes, bc):
+    from terraneo_b200 import shell
+    pf, pc, k = meshes
+    op = shell.EpsilonDivDivKerngen(pf, k, *bc)
+    u, v = consistent(shell, pf, 3, 1), consistent(shell, pf, 3, 2)
+    au, av = applied(shell, op, u, shell.VectorQ1Vec), applied(shell, op, v, shell.VectorQ1Vec)
+    vau, uav = shell.dot(v, au), shell.dot(u, av)
+    assert abs(vau - uav) <= TOL * max(abs(vau), np.sqrt(shell.dot(au, au) * shell.dot(v, v)))
+    w = shell.VectorQ1Vec(pf)
+    shell.lincomb(w, [2.0, -3.0], [u, v])
+    aw = applied(shell, op, w, shell.VectorQ1Vec)
+    ref = shell.VectorQ1Vec(pf)
+    shell.lincomb(ref, [2.0, -3.0], [au, av])
+    assert rel(aw.numpy(), ref.numpy()) <= TOL
+
+
+def test_epsdivdiv_fp32_matches_fp64_at_level6(meshes):
+    from terraneo_b200 import shell
+    pf, pc, k = meshes
+    u = consistent(shell, pf, 3, 3)
+    y64 = applied(shell, shell.EpsilonDivDivKerngen(pf, k, 2, 2), u, shell.VectorQ1Vec)
+    k32, u32 = shell.VectorQ1Scalar(pf, torch.float32), shell.VectorQ1Vec(pf, torch.float32)
+    k32.data.copy_(k.data)
+    u32.data.copy_(u.data)
+    y32 = shell.VectorQ1Vec(pf, torch.float32)
+    shell.apply(shell.EpsilonDivDivKerngen(pf, k32, 2, 2), u32, y32)
+    assert rel(y32.numpy().astype(np.float64), y64.numpy()) <= 1e-5
+
+
+@pytest.mark.parametrize("bc", [(1, 1), (2, 2)])
+def test_stokes_blocks_are_transposes_at_level6(meshes, bc):
+    from terraneo_b200 import shell
+    pf, pc, k = meshes
+    u, q = consistent(shell, pf, 3, 4), consistent(shell, pc, 1, 5)
+    bu = applied(shell, shell.Divergence(pf, pc, *bc), u, shell.VectorQ1Scalar, pc)
+    btq = applied(shell, shell.Gradient(pf, pc, *bc), q, shell.VectorQ1Vec, pf)
+    a, b = shell.dot(q, bu), shell.dot(u, btq)
+    assert abs(a - b) <= TOL * np.sqrt(shell.dot(bu, bu) * shell.dot(q, q))
+
+
+def test_restriction_is_the_transpose_of_prolongation_at_level6(meshes):
+    from terraneo_b200 import shell
+    pf, pc, k = meshes
+    uf, vc = consistent(shell, pf, 3, 6), consistent(shell, pc, 3, 7)
+    ru = applied(shell, shell.RestrictionVecConstant(pf, pc), uf, shell.VectorQ1Vec, pc)
+    pv = applied(shell, shell.ProlongationVecConstant(pf, pc), vc, shell.VectorQ1Vec, pf)
+    a, b = shell.dot(ru, vc), shell.dot(uf, pv)
+    assert abs(a - b) <= TOL * np.sqrt(shell.dot(ru, ru) * shell.dot(vc, vc))
+
+
+@pytest.mark.parametrize("bc", [(1, 1), (2, 2)])
+def test_stored_apply_equals_matrix_free_at_level5(bc):
+    from terraneo_b200 import shell
+    pc = shell.ShellMesh(L - 1)
+    k = shell.VectorQ1Scalar(pc)
+    k.set_numpy(viscosity_field(Mesh(L - 1), seed=8, contrast=1e4))
+    u = consistent(shell, pc, 3, 9)
+    mats = shell.kerngen_local_matrices(pc, k)
+    a = applied(shell, shell.StoredEpsilonDivDiv(pc, mats, *bc), u, shell.VectorQ1Vec)
+    b = applied(shell, shell.EpsilonDivDivKerngen(pc, k, *bc), u, shell.VectorQ1Vec)
+    assert rel(a.numpy(), b.numpy()) <= TOL
+
+
+def test_laplace_symmetric_and_neumann_kernel_at_level6(meshes):
+    from terraneo_b200 import shell
+    pf, pc, k = meshes
+    u, v = consistent(shell, pf, 1, 10), consistent(shell, pf, 1, 11)
+    op = shell.Laplace(pf, True)
+    au, av = applied(shell, op, u, shell.VectorQ1Scalar), applied(shell, op, v, shell.VectorQ1Scalar)
+    vau, uav = shell.dot(v, au), shell.dot(u, av)
+    assert abs(vau - uav) <= TOL * np.sqrt(shell.dot(au, au) * shell.dot(v, v))
+    one = shell.VectorQ1Scalar(pf)
+    one.data.fill_(1.0)
+    a1 = applied(shell, shell.Laplace(pf, False), one, shell.VectorQ1Scalar)
+    assert float(a1.data.abs().max()) <= 1e-12 * float(au.data.abs().max())
+
+
+def test_stokes_solve_true_residual_at_level6(meshes):
+    """The level-6 free-slip solve (FP32 multigrid, GCA coarse operators) reaches 1e-8 in the FP64 residual of the
+    full operator, for a buoyancy right-hand side M (1e5 T r_hat)."""
+    from terraneo_b200 import shell
+    pf, pc, k = meshes
+    coords, radii = pf.geometry()
+    t = np.log(viscosity_field(Mesh(L), seed=13, contrast=10.0))
+    fu, fp, tmp, out = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc), shell.VectorQ1Scalar(pf), shell.VectorQ1Scalar(pf)
+    for c in range(3):
+        tmp.set_numpy(1e5 * t * coords[:, :, :, None, c])
+        shell.apply(shell.KMass(pf, None, 0), tmp, out)
+        fu.data[c].copy_(out.data[0])
+    shell.freeslip_project(fu, True, True)
+    s = shell.StokesSolver(L, k, mg_levels=4, bc_cmb=2, bc_surface=2, mg_fp32=True, chebyshev_order=3,
+                           relative_tolerance=1e-8, max_iterations=1500, restart=100, gca=1)
+    xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+    it, rr = s.solve(fu, fp, xu, xp)
+    ku, kp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+    s.apply(xu, xp, ku, kp)
+    shell.lincomb(ku, [1.0, -1.0], [fu, ku])
+    shell.lincomb(kp, [1.0, -1.0], [fp, kp])
+    true_rr = np.sqrt(shell.dot(ku, ku) + shell.dot(kp, kp)) / np.sqrt(shell.dot(fu, fu))
+    assert rr <= 1e-8 and true_rr <= 2e-8, (it, rr, true_rr)
