@@ -28,6 +28,8 @@
 // symmetry.
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "reduce.cuh"
 #include "wedge.cuh"
@@ -849,6 +851,315 @@ __global__ void __launch_bounds__( 256 ) spcg_gather_kernel( SpcgParams S, Ptr3<
     }
 }
 
+// ---------------------------------------------------------------------------
+// The vector steps of one coarse-grid PCG iteration in one launch of one
+// thread-block cluster.
+//
+// On the coarsest level (level 3: 7,290 stored nodes) the vector steps of the
+// multi-launch form are latency-bound: each launch costs its ramp and a
+// last-block reduction through global memory.  Here the steps between two
+// wedge-product launches (stored_apply_kernel over the whole GPU) run in one
+// cluster of 16 CTAs (8 where the GPU cannot schedule 16): halo gather +
+// <p, Ap>, the x / r update + <r, r> + stopping test, and the next direction
+// p = r + beta p with ap cleared and the penalty dots of p, separated by the
+// hardware cluster barrier (release / acquire at cluster scope).  Each
+// reduction is combined through distributed shared memory: every CTA writes
+// its compensated partial to its own shared memory and, after the barrier,
+// reads all partials in rank order, so all CTAs hold bit-identical sums and
+// take the same stopping decision.  Vectors are read with ld.global.cg (L2).
+// The arithmetic per node is that of the multi-launch form (pcg.hpp:79-110).
+//
+// Every thread runs the same sequence of cluster barriers: the stopping flag
+// is read by every thread before the first barrier (nothing writes it before
+// then), so an early return is uniform over the cluster.
+namespace cg = cooperative_groups;
+
+constexpr int kCpThreads      = 512; // 16 x 512 threads: one level-3 node per thread
+constexpr int kClusterMax     = 16;
+constexpr int kClusterPcgMaxN = 8; // levels <= 3
+
+struct ClusterPcgParams
+{
+    SpcgParams           S;
+    Ptr3< const double > b;
+    Ptr3< double >       x, r, p, ap, aq;
+    int                  it; // 0: initial residual (r = b - a, p = r); >= 1: PCG iteration it
+    double               rtol, atol;
+};
+
+// sum over the cluster of K compensated per-thread partials; the result is
+// the same in every thread of every CTA.  part: this CTA's partials in the
+// given slot (each slot is used once per launch).
+template < int K >
+__device__ void cluster_sum( cg::cluster_group& cl, Neumaier* acc, double ( *part )[K][2], int slot, double* out )
+{
+    __shared__ double sh[32][K][2];
+    __shared__ double res[K];
+    const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for ( int k = 0; k < K; ++k )
+    {
+        const Neumaier w = warp_reduce( acc[k] );
+        if ( lane == 0 )
+            sh[warp][k][0] = w.s, sh[warp][k][1] = w.c;
+    }
+    __syncthreads();
+    if ( threadIdx.x == 0 )
+        for ( int k = 0; k < K; ++k )
+        {
+            Neumaier b;
+            for ( int w = 0; w < int( blockDim.x >> 5 ); ++w )
+                b.merge( Neumaier{ sh[w][k][0], sh[w][k][1] } );
+            part[slot][k][0] = b.s, part[slot][k][1] = b.c;
+        }
+    cl.sync();
+    if ( warp == 0 )
+    {
+        // lane j fetches rank j's partials (one round of remote loads), then
+        // every lane merges them in rank order from shuffles
+        const unsigned nb = cl.num_blocks();
+        double         qs[K], qc[K];
+#pragma unroll
+        for ( int k = 0; k < K; ++k )
+            qs[k] = qc[k] = 0.0;
+        if ( unsigned( lane ) < nb )
+        {
+            const double* q = cl.map_shared_rank( &part[slot][0][0], unsigned( lane ) );
+#pragma unroll
+            for ( int k = 0; k < K; ++k )
+                qs[k] = q[2 * k], qc[k] = q[2 * k + 1];
+        }
+#pragma unroll
+        for ( int k = 0; k < K; ++k )
+        {
+            Neumaier t;
+            for ( unsigned j = 0; j < nb; ++j )
+                t.merge( Neumaier{ __shfl_sync( 0xffffffffu, qs[k], int( j ) ),
+                                   __shfl_sync( 0xffffffffu, qc[k], int( j ) ) } );
+            if ( lane == 0 )
+                res[k] = t.value();
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for ( int k = 0; k < K; ++k )
+        out[k] = res[k];
+}
+
+__global__ void __launch_bounds__( kCpThreads ) spcg_step_cluster_kernel( ClusterPcgParams P )
+{
+    __shared__ double part3[1][3][2];
+    __shared__ double part1[2][1][2];
+    cg::cluster_group cl = cg::this_cluster();
+    const SpcgParams& S  = P.S;
+    double*           st = S.state;
+    if ( P.it > 0 && st[kSpDone] != 0.0 ) // uniform: read by every thread before any barrier
+        return;
+    const size_t   ns   = S.ns;
+    const size_t   t0   = size_t( cl.block_rank() ) * blockDim.x + threadIdx.x;
+    const size_t   nt   = size_t( cl.num_blocks() ) * blockDim.x;
+    const unsigned n1   = unsigned( S.n1 );
+    const bool     lead = cl.block_rank() == 0 && threadIdx.x == 0;
+    const double   g[3] = { S.fsfs ? S.scratch[3] : 0.0, S.fsfs ? S.scratch[4] : 0.0, S.fsfs ? S.scratch[5] : 0.0 };
+    double         an = st[kSpAn], r0 = st[kSpR0];
+
+    // a = halo sum over the node's copies of (ap + g x x); it 0: r = b - a,
+    // p = r and <r, r>; else aq = a and <p, aq>
+    double red;
+    {
+        Neumaier acc;
+        for ( size_t i = t0; i < ns; i += nt )
+        {
+            double pen[3] = { 0.0, 0.0, 0.0 };
+            if ( S.fsfs )
+            {
+                double xp[3];
+                spcg_position( S, unsigned( i ), xp );
+                pen[0] = g[1] * xp[2] - g[2] * xp[1];
+                pen[1] = g[2] * xp[0] - g[0] * xp[2];
+                pen[2] = g[0] * xp[1] - g[1] * xp[0];
+            }
+            const unsigned lat = unsigned( i ) / n1, rr = unsigned( i ) - lat * n1;
+            const int      grp = S.lat_group[lat];
+            // every load of the node before any store (the fields may alias as far as the compiler knows)
+            double a[3], q[3];
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+                q[c] = __ldcg( ( P.it == 0 ? P.b.p[c] : P.p.p[c] ) + i );
+            if ( grp < 0 )
+            {
+#pragma unroll
+                for ( int c = 0; c < 3; ++c )
+                    a[c] = __ldcg( P.ap.p[c] + i ) + pen[c];
+            }
+            else
+            {
+                a[0] = a[1] = a[2] = 0.0;
+                for ( int k = S.offsets[grp]; k < S.offsets[grp + 1]; ++k )
+                {
+                    const size_t j = size_t( S.members[k] ) * n1 + rr;
+#pragma unroll
+                    for ( int c = 0; c < 3; ++c )
+                        a[c] += __ldcg( P.ap.p[c] + j ) + pen[c];
+                }
+            }
+            double dot = 0.0;
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+            {
+                if ( P.it == 0 )
+                {
+                    const double ri = q[c] - a[c];
+                    __stcg( P.r.p[c] + i, ri );
+                    __stcg( P.p.p[c] + i, ri );
+                    dot += ri * ri;
+                }
+                else
+                {
+                    __stcg( P.aq.p[c] + i, a[c] );
+                    dot += q[c] * a[c];
+                }
+            }
+            acc.add( S.owned[i] ? dot : 0.0 );
+        }
+        cluster_sum< 1 >( cl, &acc, part1, 0, &red );
+    }
+    bool   done;
+    double beta = 0.0;
+    if ( P.it == 0 )
+    {
+        an   = red;
+        r0   = sqrt( an );
+        done = r0 < P.atol;
+        if ( lead )
+        {
+            st[kSpAn] = an, st[kSpR0] = r0, st[kSpBeta] = 0.0, st[kSpDone] = done ? 1.0 : 0.0;
+            st[kSpIts] = 0.0, st[kSpRelres] = 1.0, st[kSpHist] = 1.0;
+        }
+    }
+    else
+    {
+        // x += alpha p, r -= alpha aq, <r, r>, stopping test  (pcg.hpp:88-110)
+        const double pap = red, alpha = an / pap;
+        double       rr;
+        {
+            Neumaier acc;
+            for ( size_t i = t0; i < ns; i += nt )
+            {
+                double xv[3], pv[3], rv[3], qv[3], dot = 0.0;
+#pragma unroll
+                for ( int c = 0; c < 3; ++c )
+                {
+                    xv[c] = __ldcg( P.x.p[c] + i ), pv[c] = __ldcg( P.p.p[c] + i );
+                    rv[c] = __ldcg( P.r.p[c] + i ), qv[c] = __ldcg( P.aq.p[c] + i );
+                }
+#pragma unroll
+                for ( int c = 0; c < 3; ++c )
+                {
+                    __stcg( P.x.p[c] + i, xv[c] + alpha * pv[c] );
+                    const double ri = rv[c] + ( -alpha ) * qv[c];
+                    __stcg( P.r.p[c] + i, ri );
+                    dot += ri * ri;
+                }
+                acc.add( S.owned[i] ? dot : 0.0 );
+            }
+            cluster_sum< 1 >( cl, &acc, part1, 1, &rr );
+        }
+        const double ar = sqrt( rr ), rel = ar / r0;
+        done            = rel <= P.rtol || ar < P.atol;
+        if ( !done )
+            beta = rr / an;
+        if ( lead )
+        {
+            st[kSpPap] = pap, st[kSpHist + P.it] = rel, st[kSpRelres] = rel, st[kSpIts] = double( P.it );
+            if ( done )
+                st[kSpDone] = 1.0;
+            else
+                st[kSpBeta] = beta, st[kSpAn] = rr;
+        }
+    }
+    if ( !done )
+    {
+        // next direction p = r + beta p (p = r after the initial residual),
+        // ap = 0, penalty dots of p and g = eps G^-1 d for the next apply
+        double sum[3] = { 0.0, 0.0, 0.0 };
+        for ( size_t i = t0; i < ns; i += nt )
+        {
+            double w[3], rv[3];
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+            {
+                w[c]  = __ldcg( P.p.p[c] + i );
+                rv[c] = P.it > 0 ? __ldcg( P.r.p[c] + i ) : 0.0;
+            }
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+            {
+                if ( P.it > 0 )
+                {
+                    w[c] = rv[c] + beta * w[c];
+                    __stcg( P.p.p[c] + i, w[c] );
+                }
+                __stcg( P.ap.p[c] + i, 0.0 );
+            }
+            if ( S.fsfs && S.owned[i] )
+            {
+                double xp[3];
+                spcg_position( S, unsigned( i ), xp );
+                sum[0] += xp[1] * w[2] - xp[2] * w[1];
+                sum[1] += xp[2] * w[0] - xp[0] * w[2];
+                sum[2] += xp[0] * w[1] - xp[1] * w[0];
+            }
+        }
+        if ( S.fsfs )
+        {
+            Neumaier acc[3];
+            for ( int k = 0; k < 3; ++k )
+                acc[k].add( sum[k] );
+            double d[3];
+            cluster_sum< 3 >( cl, acc, part3, 0, d );
+            if ( lead )
+                for ( int k = 0; k < 3; ++k )
+                    S.scratch[3 + k] =
+                        S.eps * ( S.ginv[3 * k] * d[0] + S.ginv[3 * k + 1] * d[1] + S.ginv[3 * k + 2] * d[2] );
+        }
+    }
+    cl.sync(); // no CTA leaves while another may still read its shared memory
+}
+
+// Cluster size for the coarse-grid PCG step on this device: 16 where the GPU
+// can schedule a 16-CTA cluster of the kernel, else 8, else 0 (the
+// multi-launch form is used).
+int spcg_cluster_size()
+{
+    static int size = -1;
+    if ( size >= 0 )
+        return size;
+    size = 0;
+    if ( cudaFuncSetAttribute( spcg_step_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1 ) !=
+         cudaSuccess )
+    {
+        cudaGetLastError();
+        return size;
+    }
+    for ( int c : { kClusterMax, 8 } )
+    {
+        cudaLaunchConfig_t  cfg{};
+        cudaLaunchAttribute attr{};
+        attr.id               = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = unsigned( c ), attr.val.clusterDim.y = 1, attr.val.clusterDim.z = 1;
+        cfg.gridDim = dim3( unsigned( c ) ), cfg.blockDim = dim3( kCpThreads ), cfg.attrs = &attr, cfg.numAttrs = 1;
+        int n = 0;
+        if ( cudaOccupancyMaxActiveClusters( &n, spcg_step_cluster_kernel, &cfg ) == cudaSuccess && n >= 1 )
+        {
+            size = c;
+            break;
+        }
+        cudaGetLastError();
+    }
+    return size;
+}
+
 }  // namespace
 
 template < typename T >
@@ -936,13 +1247,35 @@ static int stored_pcg( const tn_mesh* m, const double* mats, const tn_epsdivdiv_
     const double*   aqs[3]   = { work[9], work[10], work[11] };
     Ptr3< const double > cap{ { pap.p[0], pap.p[1], pap.p[2] } }, cr{ { pr.p[0], pr.p[1], pr.p[2] } };
 
+    // coarse meshes: the vector steps of an iteration as one cluster launch
+    const int           csize = m->N <= kClusterPcgMaxN ? spcg_cluster_size() : 0;
+    ClusterPcgParams    CP{};
+    cudaLaunchConfig_t  cfg{};
+    cudaLaunchAttribute attr{};
+    if ( csize > 0 )
+    {
+        CP.S = S, CP.b = pb, CP.x = px, CP.r = pr, CP.p = pp, CP.ap = pap, CP.aq = paq;
+        CP.rtol = rtol, CP.atol = atol;
+        attr.id               = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = unsigned( csize ), attr.val.clusterDim.y = 1, attr.val.clusterDim.z = 1;
+        cfg.gridDim = dim3( unsigned( csize ) ), cfg.blockDim = dim3( kCpThreads ), cfg.dynamicSmemBytes = 0;
+        cfg.stream = st, cfg.attrs = &attr, cfg.numAttrs = 1;
+    }
+
     // r = b - A x, p = r
     spcg_prepare_kernel<<< nblocks, 256, 0, st >>>( S, pp, cr, cx, pap, 0, 0 );
     TN_LAUNCH_CHECK();
     A.src = cx, A.gate = nullptr;
     stored_apply_kernel< double ><<< ablocks, 128, 0, st >>>( A );
     TN_LAUNCH_CHECK();
-    spcg_gather_kernel<<< nblocks, 256, 0, st >>>( S, cap, 0, pb, pr, pp, paq, atol );
+    if ( csize > 0 )
+    {
+        // also clears ap and forms the penalty vector of p for the first iteration
+        CP.it = 0;
+        TN_CUDA_TRY( cudaLaunchKernelEx( &cfg, spcg_step_cluster_kernel, CP ) );
+    }
+    else
+        spcg_gather_kernel<<< nblocks, 256, 0, st >>>( S, cap, 0, pb, pr, pp, paq, atol );
     TN_LAUNCH_CHECK();
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     TN_CUDA_TRY( cudaStreamIsCapturing( st, &cs ) );
@@ -958,6 +1291,16 @@ static int stored_pcg( const tn_mesh* m, const double* mats, const tn_epsdivdiv_
             TN_CUDA_TRY( cudaStreamSynchronize( st ) );
             if ( done != 0.0 )
                 break;
+        }
+        if ( csize > 0 )
+        {
+            // wedge products over the whole GPU, then gather + update + next direction in one cluster
+            stored_apply_kernel< double ><<< ablocks, 128, 0, st >>>( A );
+            TN_LAUNCH_CHECK();
+            CP.it = it;
+            TN_CUDA_TRY( cudaLaunchKernelEx( &cfg, spcg_step_cluster_kernel, CP ) );
+            TN_LAUNCH_CHECK();
+            continue;
         }
         spcg_prepare_kernel<<< nblocks, 256, 0, st >>>( S, pp, cr, A.src, pap, it > 1, 1 );
         TN_LAUNCH_CHECK();

@@ -105,18 +105,48 @@ __global__ void dot_kernel( size_t ns, int ncomp, Ptr3< const T > a, Ptr3< const
 }
 
 // One Chebyshev step (linalg/solvers/chebyshev.hpp:127-160) fused into a
-// single pass: z = D^{-1} (b - Ax), d = alpha z + beta d, x = x + d.
+// single pass: z = D^{-1} (b - Ax), d = alpha z + beta d, x = x + d.  Each
+// thread loads kU entries (a grid stride apart, so every warp load stays
+// coalesced) before it stores any: the input streams of kU entries are in
+// flight together instead of one entry's at a time.
 template < typename T >
 __global__ void chebyshev_kernel( size_t ns, Ptr3< T > x, Ptr3< T > d, Ptr3< const T > b, Ptr3< const T > ax,
                                   Ptr3< const T > inv_diag, T alpha, T beta )
 {
-    const int c = blockIdx.y;
-    for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
+    constexpr int kU = 4;
+    const int     c  = blockIdx.y;
+    T* __restrict__ px       = x.p[c];
+    T* __restrict__ pd       = d.p[c];
+    const T* __restrict__ pb = b.p[c];
+    const T* __restrict__ pa = ax.p[c];
+    const T* __restrict__ pi = inv_diag.p[c];
+    const size_t stride      = size_t( gridDim.x ) * blockDim.x;
+    const bool   use_d       = beta != T( 0 );
+    for ( size_t i0 = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i0 < ns; i0 += kU * stride )
     {
-        const T z  = inv_diag.p[c][i] * ( b.p[c][i] - ax.p[c][i] );
-        const T dn = beta == T( 0 ) ? alpha * z : alpha * z + beta * d.p[c][i];
-        d.p[c][i]  = dn;
-        x.p[c][i]  = x.p[c][i] + dn;
+        T z[kU], dv[kU], xv[kU];
+#pragma unroll
+        for ( int u = 0; u < kU; ++u )
+        {
+            const size_t i = i0 + u * stride;
+            if ( i < ns )
+            {
+                z[u]  = pi[i] * ( pb[i] - pa[i] );
+                dv[u] = use_d ? pd[i] : T( 0 );
+                xv[u] = px[i];
+            }
+        }
+#pragma unroll
+        for ( int u = 0; u < kU; ++u )
+        {
+            const size_t i = i0 + u * stride;
+            if ( i < ns )
+            {
+                const T dn = use_d ? alpha * z[u] + beta * dv[u] : alpha * z[u];
+                pd[i]      = dn;
+                px[i]      = xv[u] + dn;
+            }
+        }
     }
 }
 

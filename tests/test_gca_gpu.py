@@ -132,15 +132,8 @@ def _oracle_pcg(apply, dot, b, maxit, rtol):
     return x, hist
 
 
-@pytest.mark.parametrize("bc", [(1, 1), (2, 2), (2, 1)])
-@pytest.mark.parametrize("contrast", [1.0, 1e3])
-@pytest.mark.parametrize("check_every", [8, 0])
-def test_fused_stored_pcg_matches_oracle_cg(level3, bc, contrast, check_every):
-    """The fused stored-matrix PCG (operator steps folded into the PCG steps) follows the oracle CG on the
-    oracle operator step by step.  Unpreconditioned CG amplifies rounding (the atomics order on the GPU),
-    so with the 1e3 viscosity contrast only the first iterations are compared tightly."""
+def _check_stored_pcg(of, pf, bc, contrast, check_every, n):
     from terraneo_b200 import shell
-    of, oc, pf, pc, _, _ = level3
     k = viscosity_field(of, seed=9, contrast=contrast) if contrast > 1 else np.ones(of.shape)
     kv = shell.VectorQ1Scalar(pf)
     kv.set_numpy(k)
@@ -156,7 +149,6 @@ def test_fused_stored_pcg_matches_oracle_cg(level3, bc, contrast, check_every):
         shell.freeslip_project(fb, bc[0] == 2, bc[1] == 2)
     b = fb.numpy()
     op = shell.StoredEpsilonDivDiv(pf, m, bc[0], bc[1])
-    n = 60 if contrast == 1.0 else 15
     x = shell.VectorQ1Vec(pf)
     its, hist = shell.stored_pcg(op, fb, x, max_iterations=n, relative_tolerance=1e-30, check_every=check_every)
     assert its == n
@@ -171,3 +163,22 @@ def test_fused_stored_pcg_matches_oracle_cg(level3, bc, contrast, check_every):
     its3, hist3 = shell.stored_pcg(op, fb, x2, max_iterations=n - its2, relative_tolerance=1e-30,
                                    check_every=check_every)
     assert its3 == n - its2 and hist3[0] == 1.0
+
+
+@pytest.mark.parametrize("bc", [(1, 1), (2, 2), (2, 1)])
+@pytest.mark.parametrize("contrast", [1.0, 1e3])
+@pytest.mark.parametrize("check_every", [8, 0])
+def test_fused_stored_pcg_matches_oracle_cg(level3, bc, contrast, check_every):
+    """The stored-matrix PCG follows the oracle CG on the oracle operator step by step.  At level 3 the vector
+    steps of each iteration run as one thread-block-cluster launch.  Unpreconditioned CG amplifies rounding (the
+    atomics order on the GPU), so with the 1e3 viscosity contrast only the first iterations are compared tightly."""
+    of, oc, pf, pc, _, _ = level3
+    _check_stored_pcg(of, pf, bc, contrast, check_every, 60 if contrast == 1.0 else 15)
+
+
+@pytest.mark.parametrize("bc", [(1, 1), (2, 2)])
+@pytest.mark.parametrize("check_every", [8, 0])
+def test_fused_stored_pcg_multi_launch_matches_oracle_cg(bc, check_every):
+    """Level 4: the multi-launch form (4 gated launches per iteration, device-side stopping flag)."""
+    from terraneo_b200 import shell
+    _check_stored_pcg(Mesh(4), shell.ShellMesh(4), bc, 1.0, check_every, 30)
