@@ -106,6 +106,11 @@ struct tn_mesh
     double*       d_red_result   = nullptr; // 16 doubles
     unsigned int* d_red_counter  = nullptr;
     double*       h_red_result   = nullptr; // pinned, 16 doubles
+
+    // side stream for work that overlaps a kernel of the caller's stream
+    // (forked from and joined back into that stream with the two events)
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t  ev_fork = nullptr, ev_join = nullptr;
 };
 
 namespace tn {

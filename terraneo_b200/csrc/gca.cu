@@ -39,7 +39,9 @@ namespace tn {
 template < typename T >
 int halo_sum( const tn_mesh* m, T* const* fields, int nfields, cudaStream_t st );
 template < typename T >
-int fsfs_penalty_add( const tn_mesh* m, double eps, const T* const* src, T* const* dst, cudaStream_t st );
+int fsfs_penalty_fork( const tn_mesh* m, double eps, const T* const* src, cudaStream_t st );
+template < typename T >
+int fsfs_penalty_join( const tn_mesh* m, T* const* dst, cudaStream_t st );
 
 namespace {
 
@@ -1182,6 +1184,14 @@ int stored_apply( const tn_mesh* m, const T* mats, const tn_epsdivdiv_params* p,
     P.N = m->N, P.n1 = m->n1, P.coords = m->d_coords, P.mats = mats;
     P.bc_cmb = p->bc_cmb, P.bc_surf = p->bc_surface, P.diag = p->diagonal != 0;
     const long long wedges = 2LL * kDiamonds * m->N * m->N * m->N;
+    const bool      fsfs   = !p->diagonal && p->bc_cmb == TN_BC_FREESLIP && p->bc_surface == TN_BC_FREESLIP;
+    if ( fsfs )
+    {
+        // the penalty dots of src overlap the wedge kernel on the mesh's side stream
+        int rc = fsfs_penalty_fork< T >( m, p->penalty_eps, src, st );
+        if ( rc )
+            return rc;
+    }
     if ( p->diagonal )
         stored_diag_kernel< T ><<< unsigned( ( wedges + 127 ) / 128 ), 128, 0, st >>>( P );
     else
@@ -1189,9 +1199,9 @@ int stored_apply( const tn_mesh* m, const T* mats, const tn_epsdivdiv_params* p,
         stored_apply_kernel< T ><<< unsigned( ( wedges + 127 ) / 128 ), 128, 0, st >>>( P );
     }
     TN_LAUNCH_CHECK();
-    if ( !p->diagonal && p->bc_cmb == TN_BC_FREESLIP && p->bc_surface == TN_BC_FREESLIP )
+    if ( fsfs )
     {
-        int rc = fsfs_penalty_add< T >( m, p->penalty_eps, src, dst, st );
+        int rc = fsfs_penalty_join< T >( m, dst, st );
         if ( rc )
             return rc;
     }

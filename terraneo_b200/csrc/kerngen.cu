@@ -853,27 +853,41 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
 }
 
 // dst += eps sum_i (m_i^T src) m_i, the fs/fs rigid-rotation penalty on every
-// stored node (no halo); shared with the stored-matrix apply.
+// stored node (no halo), in two parts for the stored-matrix apply: the dots
+// of src run on the mesh's side stream, forked from st, so they overlap the
+// wedge kernel the caller launches on st in between; the join makes st wait
+// for them before the update.  The dots use the mesh's reduction scratch:
+// the caller launches no other reduction over the mesh in between.
 template < typename T >
-int fsfs_penalty_add( const tn_mesh* m, double eps, const T* const* src, T* const* dst, cudaStream_t st )
+int fsfs_penalty_fork( const tn_mesh* m, double eps, const T* const* src, cudaStream_t st )
 {
     Ptr3< const T > s{ { src[0], src[1], src[2] } };
-    Ptr3< T >       o{ { dst[0], dst[1], dst[2] } };
     Mat3            gi;
     for ( int i = 0; i < 9; ++i )
         gi.a[i] = m->penalty_gram_inv[i];
-    penalty_dots_kernel< T ><<< penalty_blocks( m->nlat ), 256, 0, st >>>( m->nlat, m->n1, m->d_coords,
-                                                                         mesh_radii< T >( m ), s, m->d_lat_owned,
-                                                                         m->d_red_partials, m->d_red_counter,
-                                                                         m->d_red_result, eps, gi );
+    TN_CUDA_TRY( cudaEventRecord( m->ev_fork, st ) );
+    TN_CUDA_TRY( cudaStreamWaitEvent( m->side_stream, m->ev_fork, 0 ) );
+    penalty_dots_kernel< T ><<< penalty_blocks( m->nlat ), 256, 0, m->side_stream >>>(
+        m->nlat, m->n1, m->d_coords, mesh_radii< T >( m ), s, m->d_lat_owned, m->d_red_partials, m->d_red_counter,
+        m->d_red_result, eps, gi );
     TN_LAUNCH_CHECK();
+    TN_CUDA_TRY( cudaEventRecord( m->ev_join, m->side_stream ) );
+    return TN_OK;
+}
+template < typename T >
+int fsfs_penalty_join( const tn_mesh* m, T* const* dst, cudaStream_t st )
+{
+    Ptr3< T > o{ { dst[0], dst[1], dst[2] } };
+    TN_CUDA_TRY( cudaStreamWaitEvent( st, m->ev_join, 0 ) );
     penalty_axpy_kernel< T ><<< 148 * 8, 256, 0, st >>>( m->ns, m->n1, m->d_coords, mesh_radii< T >( m ),
                                                         m->d_red_result + 3, o );
     TN_LAUNCH_CHECK();
     return TN_OK;
 }
-template int fsfs_penalty_add< double >( const tn_mesh*, double, const double* const*, double* const*, cudaStream_t );
-template int fsfs_penalty_add< float >( const tn_mesh*, double, const float* const*, float* const*, cudaStream_t );
+template int fsfs_penalty_fork< double >( const tn_mesh*, double, const double* const*, cudaStream_t );
+template int fsfs_penalty_fork< float >( const tn_mesh*, double, const float* const*, cudaStream_t );
+template int fsfs_penalty_join< double >( const tn_mesh*, double* const*, cudaStream_t );
+template int fsfs_penalty_join< float >( const tn_mesh*, float* const*, cudaStream_t );
 
 }  // namespace tn
 

@@ -321,9 +321,12 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
          cudaMalloc( &m->d_red_result, sizeof( double ) * 16 ) != cudaSuccess ||
          cudaMalloc( &m->d_red_counter, sizeof( unsigned int ) ) != cudaSuccess ||
          cudaMallocHost( &m->h_red_result, sizeof( double ) * 16 ) != cudaSuccess ||
-         cudaMemset( m->d_red_counter, 0, sizeof( unsigned int ) ) != cudaSuccess )
+         cudaMemset( m->d_red_counter, 0, sizeof( unsigned int ) ) != cudaSuccess ||
+         cudaStreamCreateWithFlags( &m->side_stream, cudaStreamNonBlocking ) != cudaSuccess ||
+         cudaEventCreateWithFlags( &m->ev_fork, cudaEventDisableTiming ) != cudaSuccess ||
+         cudaEventCreateWithFlags( &m->ev_join, cudaEventDisableTiming ) != cudaSuccess )
     {
-        set_error( "tn_mesh_create: device scratch allocation failed" );
+        set_error( "tn_mesh_create: device scratch, stream or event creation failed" );
         tn_mesh_destroy( m );
         return TN_ERR_NOMEM;
     }
@@ -352,6 +355,12 @@ extern "C" int tn_mesh_destroy( tn_mesh* m )
     cudaFree( m->d_red_counter );
     if ( m->h_red_result )
         cudaFreeHost( m->h_red_result );
+    if ( m->side_stream )
+        cudaStreamDestroy( m->side_stream );
+    if ( m->ev_fork )
+        cudaEventDestroy( m->ev_fork );
+    if ( m->ev_join )
+        cudaEventDestroy( m->ev_join );
     delete m;
     return TN_OK;
 }
