@@ -131,10 +131,31 @@ def _case_stokes6(shell, C, torch):
     return {"Stokes solve, level 6 free-slip, FP32 multigrid, 30 FGMRES(100) iterations": run}
 
 
+def _case_coarse_pcg3(shell, C, torch):
+    """The coarsest-level solve of the C3 V-cycle: 50 iterations of the stored-matrix PCG at level 3,
+    free-slip both radii, matrices coarsened (GCA, constant interpolation) from the level-4 kerngen matrices"""
+    mf, m = shell.ShellMesh(4, RMIN, RMAX), shell.ShellMesh(3, RMIN, RMAX)
+    coords, radii = mf.geometry()
+    k_np, _ = synthetic_inputs(coords, radii, None)
+    k = shell.VectorQ1Scalar(mf)
+    k.set_numpy(k_np)
+    mats = shell.gca_coarsen(mf, m, k_fine=k)
+    op = shell.StoredEpsilonDivDiv(m, mats, C.BC_FREESLIP, C.BC_FREESLIP)
+    b, x = shell.VectorQ1Vec(m), shell.VectorQ1Vec(m)
+    b.data.normal_(generator=torch.Generator(device="cuda").manual_seed(3))
+    b.halo_sum()
+    shell.freeslip_project(b, True, True)
+
+    def run():
+        x.data.zero_()
+        shell.stored_pcg(op, b, x, max_iterations=50, relative_tolerance=1e-30, check_every=0)
+    return {"stored-matrix PCG, level 3, free-slip both radii, 50 iterations": run}
+
+
 # name -> builder returning {description: one launch sequence}
 CASES = {"laplace6": _case_laplace6, "vlaplace6": _case_vlaplace6, "divkgrad6": _case_divkgrad6,
          "stokes_b6": _case_stokes_b6, "stored5": _case_stored5, "kerngen6_fs": _case_kerngen6_fs,
-         "stokes6": _case_stokes6}
+         "stokes6": _case_stokes6, "coarse_pcg3": _case_coarse_pcg3}
 
 
 def run_case(args):

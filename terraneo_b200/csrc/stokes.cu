@@ -31,7 +31,9 @@
 // fe/wedge/integrands.hpp at a fraction of the arithmetic.
 //
 // One thread per fine wedge (the wedge uniform within a warp), contributions
-// added with atomics.
+// added with atomics.  In B the lanes of a warp are consecutive radial cells:
+// a lane takes its bottom nodes from the lane below by shuffle, and the two
+// fine cells of one coarse cell add their coarse contributions together.
 #include <cmath>
 
 #include "common.cuh"
@@ -147,13 +149,35 @@ __device__ __forceinline__ void divergence_wedge( const StokesParams< T >& P, co
     T         Ra[2][2], Rb[2];
     radial_sums( P.radii[dm * n1 + r], P.radii[dm * n1 + r + 1], r & 1, Ra, Rb );
     const double* G = P.geom + stokes_tri( N, dm, x, y, W ) * kStokesStride;
-    T             uu[6][3];
+    // lanes are consecutive radial cells of one column: the bottom nodes of a
+    // lane are the top nodes of the lane below (raw values, shuffled before
+    // any boundary treatment); the first lane of a column loads its own
+    const int  lane = threadIdx.x & 31;
+    const bool own_bottom = lane == 0 || r == 0;
+    T          uu[6][3];
+#pragma unroll
+    for ( int n = 3; n < 6; ++n )
+    {
+        const size_t i = lat_index( n1, dm, x + kWedgeNode[W][n][0], y + kWedgeNode[W][n][1] ) * n1 + r + 1;
+        uu[n][0] = u.p[0][i], uu[n][1] = u.p[1][i], uu[n][2] = u.p[2][i];
+    }
+#pragma unroll
+    for ( int n = 0; n < 3; ++n )
+    {
+        // node n lies below node n + 3 (kWedgeNode rows 0-2 and 3-5 share their lateral positions)
+#pragma unroll
+        for ( int a = 0; a < 3; ++a )
+            uu[n][a] = __shfl_up_sync( 0xffffffffu, uu[n + 3][a], 1 );
+        if ( own_bottom )
+        {
+            const size_t i = lat_index( n1, dm, x + kWedgeNode[W][n][0], y + kWedgeNode[W][n][1] ) * n1 + r;
+            uu[n][0] = u.p[0][i], uu[n][1] = u.p[1][i], uu[n][2] = u.p[2][i];
+        }
+    }
 #pragma unroll
     for ( int n = 0; n < 6; ++n )
     {
-        const int    X = x + kWedgeNode[W][n][0], Y = y + kWedgeNode[W][n][1];
-        const size_t i = lat_index( n1, dm, X, Y ) * n1 + r + kWedgeNode[W][n][2];
-        uu[n][0] = u.p[0][i], uu[n][1] = u.p[1][i], uu[n][2] = u.p[2][i];
+        const int X = x + kWedgeNode[W][n][0], Y = y + kWedgeNode[W][n][1];
         const int bc = velocity_bc( N, r, n, P.bc_cmb, P.bc_surf );
         if ( bc == TN_BC_DIRICHLET )
             uu[n][0] = uu[n][1] = uu[n][2] = T( 0 );
@@ -189,7 +213,14 @@ __device__ __forceinline__ void divergence_wedge( const StokesParams< T >& P, co
                     acc[ib * 3 + ic] += Ra[ib][nb] * cu + Rb[ib] * lv;
             }
         }
+    // the two fine cells r = 2 rc, 2 rc + 1 (lanes 2k, 2k + 1) add to the same
+    // six coarse nodes: the even lane adds both
     const int xc = x >> 1, yc = y >> 1, rc = r >> 1;
+#pragma unroll
+    for ( int i = 0; i < 6; ++i )
+        acc[i] += __shfl_down_sync( 0xffffffffu, acc[i], 1 );
+    if ( lane & 1 )
+        return;
 #pragma unroll
     for ( int i = 0; i < 6; ++i )
         atomicAdd( p + lat_index( nc1, dm, xc + kWedgeNode[W][i][0], yc + kWedgeNode[W][i][1] ) * nc1 + rc +
