@@ -510,7 +510,10 @@ typedef struct
     int    gca; /* coarse viscous operators: 0 re-discretised with injected viscosity, 1 GCA with
                    constant interpolation (TwoGridGCA default), 2 GCA with linear interpolation */
     int    outer; /* 0 FGMRES(restart) + block-triangular preconditioner, 1 PMINRES + block-diagonal
-                     preconditioner (pminres.hpp, block_preconditioner_2x2.hpp:38-100) */
+                     preconditioner (pminres.hpp, block_preconditioner_2x2.hpp:38-100), 2 mixed-precision
+                     iterative refinement (needs mg_fp32 = 1): FP64 residual and update around an FGMRES(restart)
+                     + block-triangular solve done entirely in FP32 (coarsest PCG in FP64); no counterpart in
+                     the reference.  `iterations` counts the inner FGMRES iterations of all cycles. */
     int    eager; /* 0: after its first application the preconditioner is captured once per vector pair as a
                      CUDA graph and replayed; 1: always launched kernel by kernel */
 } tn_stokes_params;

@@ -425,5 +425,23 @@ inline void cast( VectorQ1Vec< double >& y, const VectorQ1Vec< float >& x )
     y.ptrs( yp );
     check( tn_vec_cast_f32_to_f64( y.mesh().get(), 3, yp, xp, stream() ), "cast" );
 }
+inline void cast( VectorQ1Scalar< float >& y, const VectorQ1Scalar< double >& x )
+{
+    float*        yp[1] = { y.data() };
+    const double* xp[1] = { x.data() };
+    check( tn_vec_cast_f64_to_f32( y.mesh().get(), 1, yp, xp, stream() ), "cast" );
+}
+inline void cast( VectorQ1Scalar< double >& y, const VectorQ1Scalar< float >& x )
+{
+    double*      yp[1] = { y.data() };
+    const float* xp[1] = { x.data() };
+    check( tn_vec_cast_f32_to_f64( y.mesh().get(), 1, yp, xp, stream() ), "cast" );
+}
+template < typename TO, typename TI >
+void cast( VectorQ1IsoQ2Q1< TO >& y, const VectorQ1IsoQ2Q1< TI >& x )
+{
+    cast( y.block_1(), x.block_1() );
+    cast( y.block_2(), x.block_2() );
+}
 
 }  // namespace tn

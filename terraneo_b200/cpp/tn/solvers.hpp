@@ -741,6 +741,7 @@ class FGMRES
     }
     SolverStatistics stats;
     int              preconditioner_skips = 0;
+    void             set_parameters( const IterativeSolverParameters& prm ) { prm_ = prm; }
 
     void solve_impl( Op& A, V& x, const V& b )
     {

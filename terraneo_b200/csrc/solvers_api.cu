@@ -61,6 +61,15 @@ struct Fp32Preconditioner
     }
 };
 
+// FP32 multigrid on FP32 vectors (the inner system of the refinement form)
+template < typename Inner >
+struct Fp32Direct
+{
+    std::shared_ptr< Inner > mg;
+    std::shared_ptr< V32 >   A;
+    void solve_impl( A32&, VectorQ1Vec< float >& x, const VectorQ1Vec< float >& b ) { solve( *mg, *A, x, b ); }
+};
+
 template < typename Inner >
 struct Fp64Preconditioner
 {
@@ -237,6 +246,98 @@ void finish( tn_stokes_solver& s, std::shared_ptr< Prec11 > p11 )
     };
 }
 
+// Mixed-precision iterative refinement (outer = 2): the FP64 residual
+// r = b - K x of the full Stokes system, one FGMRES cycle (at most `restart`
+// iterations) on K32 d = r / |r| entirely in FP32 (Krylov vectors,
+// Gram-Schmidt, operator, B, B^T, the block-triangular preconditioner with the
+// FP32 V-cycle; the coarsest-level PCG stays FP64), and the FP64 update
+// x += |r| d, until the FP64 residual meets the tolerance.  A cycle is the
+// counterpart of one restart of the FP64 FGMRES(restart): the Krylov space is
+// built in FP32 and the residual it restarts from is the true FP64 one.  A
+// cycle stops early when its residual estimate reaches rtol / (the current
+// relative residual); more inner cycles on the same FP32 system would only
+// chase the FP32 rounding level.
+
+template < typename MGT >
+void finish_refine( tn_stokes_solver& s, std::shared_ptr< MGT > mg, std::shared_ptr< V32 > a32ml )
+{
+    const auto&        prm = s.prm;
+    const int          L   = prm.level;
+    const Mesh &       mu = s.mesh[L], &mp = s.mesh[L - 1];
+    BoundaryConditions bcs{ prm.bc_cmb, prm.bc_surface };
+    s.K  = std::make_unique< EpsDivDivStokes< double > >( mu, mp, s.k64[L], bcs );
+    s.BT = std::make_unique< Gradient< double > >( mu, mp, bcs );
+    auto K32  = std::make_shared< EpsDivDivStokes< float > >( mu, mp, s.k32[L], bcs );
+    auto a11  = std::make_shared< A32 >( mu, s.k32[L], bcs, false );
+    auto bt32 = std::make_shared< Gradient< float > >( mu, mp, bcs );
+    // Schur: lumped KMass with k = 1 / eta on the pressure level (mantlecirculation.cpp:684-699), in FP32
+    VectorQ1Scalar< double > kp( mp ), ones( mp ), dp( mp );
+    VectorQ1Scalar< float >  dp32( mp );
+    assign( kp, s.k64[L - 1] );
+    invert_entries( kp );
+    assign( ones, 1.0 );
+    KMass< double > pm( mp, kp, 2 );
+    apply( pm, ones, dp );
+    cast( dp32, dp );
+    using P22  = DiagonalSolver< KMass< float >, VectorQ1Scalar< float > >;
+    using P11  = Fp32Direct< MGT >;
+    using BTP  = BlockTriangularPreconditioner2x2< A32, Gradient< float >, P11, P22, VectorQ1IsoQ2Q1< float > >;
+    auto p22   = std::make_shared< P22 >( dp32 );
+    auto p11   = std::make_shared< P11 >( P11{ mg, a32ml } );
+    auto prec  = std::make_shared< BTP >( *a11, *bt32, VectorQ1IsoQ2Q1< float >( mu, mp ), *p11, *p22 );
+    auto graph = std::make_shared< GraphReplay< BTP > >( *prec, prm.eager == 0 );
+    std::vector< VectorQ1IsoQ2Q1< float > > tmps;
+    for ( int i = 0; i < 2 * prm.restart + 4; ++i )
+        tmps.emplace_back( mu, mp );
+    auto fg = std::make_shared< FGMRES< EpsDivDivStokes< float >, GraphReplay< BTP > > >(
+        tmps, prm.restart, IterativeSolverParameters{ prm.restart, prm.relative_tolerance, 0.0 }, *graph );
+    auto r64 = std::make_shared< VectorQ1IsoQ2Q1< double > >( mu, mp );
+    auto d64 = std::make_shared< VectorQ1IsoQ2Q1< double > >( mu, mp );
+    auto r32 = std::make_shared< VectorQ1IsoQ2Q1< float > >( mu, mp );
+    auto d32 = std::make_shared< VectorQ1IsoQ2Q1< float > >( mu, mp );
+    tn_stokes_solver* sp = &s;
+    s.run = [sp, fg, prec, graph, p11, p22, a11, bt32, K32, r64, d64, r32, d32](
+                VectorQ1IsoQ2Q1< double >& x, const VectorQ1IsoQ2Q1< double >& b ) {
+        const auto& prm = sp->prm;
+        auto        residual = [&]() {
+            apply( *sp->K, x, *r64 );
+            lincomb( *r64, { 1.0, -1.0 }, { b, *r64 } );
+            return std::sqrt( dot( *r64, *r64 ) );
+        };
+        double       rn = residual();
+        const double r0 = rn;
+        sp->history     = { 1.0 };
+        sp->skips       = 0;
+        int total       = 0;
+        while ( rn > prm.absolute_tolerance && rn / r0 > prm.relative_tolerance && total < prm.max_iterations )
+        {
+            const double rel = rn / r0;
+            lincomb( *r64, { 1.0 / rn }, { *r64 } );
+            cast( *r32, *r64 );
+            assign( *d32, 0.0f );
+            fg->set_parameters( IterativeSolverParameters{ std::min( prm.restart, prm.max_iterations - total ),
+                                                           prm.relative_tolerance / rel, 0.0 } );
+            solve( *fg, *K32, *d32, *r32 );
+            const int its = fg->stats.iterations;
+            total += its;
+            sp->skips += fg->preconditioner_skips;
+            fg->preconditioner_skips = 0;
+            // inner estimates relative to the outer start: (inner relative residual) x (outer relative residual)
+            for ( size_t i = 1; i < fg->stats.relative_residuals.size(); ++i )
+                sp->history.push_back( fg->stats.relative_residuals[i] * rel );
+            cast( *d64, *d32 );
+            lincomb( x, { 1.0, rn }, { x, *d64 } );
+            rn = residual();
+            if ( !sp->history.empty() && its > 0 )
+                sp->history.back() = rn / r0; // the cycle ends at the true FP64 residual
+            if ( its == 0 )
+                break;
+        }
+        sp->iterations = total;
+        sp->relres     = rn / r0;
+    };
+}
+
 }  // namespace
 
 extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min, double r_max, const double* k,
@@ -248,7 +349,8 @@ extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min,
                   "tn_stokes_solver_create: need mg_levels >= 2, level - mg_levels + 1 >= 2 and level <= 8" );
     TN_CHECK_ARG( p->restart >= 1 && p->max_iterations >= 1, "tn_stokes_solver_create: bad Krylov parameters" );
     TN_CHECK_ARG( p->gca >= 0 && p->gca <= 2, "tn_stokes_solver_create: gca must be 0, 1 or 2" );
-    TN_CHECK_ARG( p->outer == 0 || p->outer == 1, "tn_stokes_solver_create: outer must be 0 or 1" );
+    TN_CHECK_ARG( p->outer >= 0 && p->outer <= 2, "tn_stokes_solver_create: outer must be 0, 1 or 2" );
+    TN_CHECK_ARG( p->outer != 2 || p->mg_fp32, "tn_stokes_solver_create: outer = 2 (refinement) needs mg_fp32 = 1" );
     try
     {
         auto s = std::make_unique< tn_stokes_solver >();
@@ -299,6 +401,12 @@ extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min,
             std::vector< std::shared_ptr< V32 > > ops32;
             CoarseFp64 cs{ pcg, Ac64, VectorQ1Vec< double >( s->mesh[Lmin] ), VectorQ1Vec< double >( s->mesh[Lmin] ) };
             auto       mg  = build_mg< float, CoarseFp64 >( *s, ops32, cs );
+            if ( p->outer == 2 )
+            {
+                finish_refine( *s, mg, ops32.back() );
+                *out = s.release();
+                return TN_OK;
+            }
             auto       p11 = std::make_shared< Fp32Preconditioner< MG< float, CoarseFp64 > > >(
                 Fp32Preconditioner< MG< float, CoarseFp64 > >{ mg, ops32.back(), VectorQ1Vec< float >( s->mesh[L] ),
                                                                 VectorQ1Vec< float >( s->mesh[L] ) } );

@@ -222,3 +222,38 @@ def test_stokes_pminres_block_diagonal(stokes_case, bc):
     rp = of.divergence(oc, u, *bc)
     res = np.sqrt(of.dot(ru, ru) + oc.dot(rp, rp)) / np.sqrt(of.dot(b, b))
     assert res <= 1e-6, res
+
+
+@pytest.mark.parametrize("bc,tol", [((1, 1), 1e-9), ((2, 1), 1e-8), ((2, 2), 1e-6)])
+@pytest.mark.parametrize("gca", [0, 1])
+def test_stokes_refinement_true_residual(stokes_case, bc, tol, gca):
+    """outer = 2: FP64 residual / update cycles around an all-FP32 FGMRES solve reach the FP64 tolerance; the
+    true residual is checked with the oracle operators, and the reported history ends at it."""
+    from terraneo_b200 import shell
+    L, of, oc, k, f = stokes_case
+    pf, pc = shell.ShellMesh(L), shell.ShellMesh(L - 1)
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(k)
+    fu, fp = prepared_rhs(shell, pf, f, bc), shell.VectorQ1Scalar(pc)
+    xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+    solver = shell.StokesSolver(L, kv, mg_levels=3, bc_cmb=bc[0], bc_surface=bc[1], mg_fp32=True, gca=gca,
+                                relative_tolerance=tol, max_iterations=600, restart=50, outer=2)
+    it, rr = solver.solve(fu, fp, xu, xp)
+    torch.cuda.synchronize()
+    assert rr <= tol and it < 600, (it, rr)
+    u, p, b = xu.numpy(), xp.numpy()[0], fu.numpy()
+    ru = of.kerngen(k, u, *bc) + of.gradient(oc, p, *bc) - b
+    rp = of.divergence(oc, u, *bc)
+    res = np.sqrt(of.dot(ru, ru) + oc.dot(rp, rp)) / np.sqrt(of.dot(b, b))
+    assert res <= 2 * tol, res
+    hist, skips = solver.history()
+    assert hist[0] == 1.0 and abs(hist[-1] - rr) <= 1e-12 + 1e-6 * rr and skips == 0
+
+
+def test_stokes_refinement_rejects_fp64_multigrid(stokes_case):
+    from terraneo_b200 import shell
+    L, of, oc, k, f = stokes_case
+    kv = shell.VectorQ1Scalar(shell.ShellMesh(L))
+    kv.set_numpy(k)
+    with pytest.raises(RuntimeError, match="refinement"):
+        shell.StokesSolver(L, kv, mg_levels=2, mg_fp32=False, outer=2)
