@@ -5,6 +5,8 @@
 // dot product accumulates in FP64 with Neumaier compensation, reduces with
 // warp shuffles inside a block and finishes deterministically in the last
 // block (fixed order over block partials), so results do not depend on timing.
+#include <algorithm>
+
 #include "common.cuh"
 #include "reduce.cuh"
 
@@ -27,21 +29,31 @@ unsigned grid_for( size_t n, int per_thread = 4 )
     return unsigned( b );
 }
 
+// component c of a pointer triple with compile-time indices only (indexing
+// the kernel-parameter array with a run-time c copies it to the stack)
+template < typename T >
+__device__ __forceinline__ T* comp_ptr( const Ptr3< T >& p, int c )
+{
+    return c == 0 ? p.p[0] : ( c == 1 ? p.p[1] : p.p[2] );
+}
+
 template < typename T >
 __global__ void lincomb_kernel( size_t ns, int ncomp, Ptr3< T > y, T c0, int nx, T c1, Ptr3< const T > x1, T c2,
                                 Ptr3< const T > x2, T c3, Ptr3< const T > x3 )
 {
-    const int c = blockIdx.y;
+    const int c  = blockIdx.y;
+    T*        py = comp_ptr( y, c );
+    const T * p1 = comp_ptr( x1, c ), *p2 = comp_ptr( x2, c ), *p3 = comp_ptr( x3, c );
     for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
     {
         T v = c0;
         if ( nx >= 1 )
-            v = v + c1 * x1.p[c][i];
+            v = v + c1 * p1[i];
         if ( nx >= 2 )
-            v = v + c2 * x2.p[c][i];
+            v = v + c2 * p2[i];
         if ( nx >= 3 )
-            v = v + c3 * x3.p[c][i];
-        y.p[c][i] = v;
+            v = v + c3 * p3[i];
+        py[i] = v;
     }
 }
 
@@ -105,24 +117,125 @@ __global__ void dot_kernel( size_t ns, int ncomp, Ptr3< const T > a, Ptr3< const
 }
 
 // One Chebyshev step (linalg/solvers/chebyshev.hpp:127-160) fused into a
-// single pass: z = D^{-1} (b - Ax), d = alpha z + beta d, x = x + d.  Each
-// thread loads kU entries (a grid stride apart, so every warp load stays
-// coalesced) before it stores any: the input streams of kU entries are in
-// flight together instead of one entry's at a time.
+// single pass: z = D^{-1} (b - Ax), d = alpha z + beta d, x = x + d.
+template < typename T >
+__device__ __forceinline__ void chebyshev_entry( size_t i, T* __restrict__ px, T* __restrict__ pd,
+                                                 const T* __restrict__ pb, const T* __restrict__ pa,
+                                                 const T* __restrict__ pi, T alpha, T beta, bool use_d )
+{
+    const T z  = pi[i] * ( pb[i] - pa[i] );
+    const T dn = use_d ? alpha * z + beta * pd[i] : alpha * z;
+    pd[i]      = dn;
+    px[i]      = px[i] + dn;
+}
+
+template < typename T >
+__device__ __forceinline__ void chebyshev_lane( T b, T a, T inv, T d, T& x, T& dn, T alpha, T beta, bool use_d )
+{
+    const T z = inv * ( b - a );
+    dn        = use_d ? alpha * z + beta * d : alpha * z;
+    x         = x + dn;
+}
+
+template < typename T >
+struct Vec16;
+template <>
+struct Vec16< float >
+{
+    using type = float4;
+    static __device__ __forceinline__ void step( const float4& b, const float4& a, const float4& i, const float4& d,
+                                                 float4& x, float4& dn, float al, float be, bool u )
+    {
+        chebyshev_lane( b.x, a.x, i.x, d.x, x.x, dn.x, al, be, u );
+        chebyshev_lane( b.y, a.y, i.y, d.y, x.y, dn.y, al, be, u );
+        chebyshev_lane( b.z, a.z, i.z, d.z, x.z, dn.z, al, be, u );
+        chebyshev_lane( b.w, a.w, i.w, d.w, x.w, dn.w, al, be, u );
+    }
+};
+template <>
+struct Vec16< double >
+{
+    using type = double2;
+    static __device__ __forceinline__ void step( const double2& b, const double2& a, const double2& i,
+                                                 const double2& d, double2& x, double2& dn, double al, double be,
+                                                 bool u )
+    {
+        chebyshev_lane( b.x, a.x, i.x, d.x, x.x, dn.x, al, be, u );
+        chebyshev_lane( b.y, a.y, i.y, d.y, x.y, dn.y, al, be, u );
+    }
+};
+
+// When the five fields share their offset modulo 16 bytes (always for the
+// library's own vectors), the entries up to the first 16-byte boundary are
+// done one by one and the rest with 16-byte vector loads and stores, two
+// vectors per thread in flight: one load instruction moves 4 FP32 / 2 FP64
+// entries, so the load queue stops throttling the stream.  Otherwise each
+// thread loads kU entries a grid stride apart before it stores any.
 template < typename T >
 __global__ void chebyshev_kernel( size_t ns, Ptr3< T > x, Ptr3< T > d, Ptr3< const T > b, Ptr3< const T > ax,
                                   Ptr3< const T > inv_diag, T alpha, T beta )
 {
-    constexpr int kU = 4;
-    const int     c  = blockIdx.y;
-    T* __restrict__ px       = x.p[c];
-    T* __restrict__ pd       = d.p[c];
-    const T* __restrict__ pb = b.p[c];
-    const T* __restrict__ pa = ax.p[c];
-    const T* __restrict__ pi = inv_diag.p[c];
+    const int c = blockIdx.y;
+    T* __restrict__ px       = comp_ptr( x, c );
+    T* __restrict__ pd       = comp_ptr( d, c );
+    const T* __restrict__ pb = comp_ptr( b, c );
+    const T* __restrict__ pa = comp_ptr( ax, c );
+    const T* __restrict__ pi = comp_ptr( inv_diag, c );
     const size_t stride      = size_t( gridDim.x ) * blockDim.x;
+    const size_t tid         = blockIdx.x * size_t( blockDim.x ) + threadIdx.x;
     const bool   use_d       = beta != T( 0 );
-    for ( size_t i0 = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i0 < ns; i0 += kU * stride )
+    const size_t mis         = reinterpret_cast< size_t >( px ) & 15;
+    const bool   vec = mis % sizeof( T ) == 0 && ( reinterpret_cast< size_t >( pd ) & 15 ) == mis &&
+                     ( reinterpret_cast< size_t >( pb ) & 15 ) == mis &&
+                     ( reinterpret_cast< size_t >( pa ) & 15 ) == mis &&
+                     ( reinterpret_cast< size_t >( pi ) & 15 ) == mis;
+    if ( vec )
+    {
+        using V                 = typename Vec16< T >::type;
+        constexpr int kV        = 16 / sizeof( T );
+        constexpr int kU        = 2;
+        const size_t  head      = std::min( ns, ( ( 16 - mis ) & 15 ) / sizeof( T ) );
+        const size_t  nv        = ( ns - head ) / kV;
+        const size_t  tail      = head + nv * kV;
+        V* __restrict__ vx       = reinterpret_cast< V* >( px + head );
+        V* __restrict__ vd       = reinterpret_cast< V* >( pd + head );
+        const V* __restrict__ vb = reinterpret_cast< const V* >( pb + head );
+        const V* __restrict__ va = reinterpret_cast< const V* >( pa + head );
+        const V* __restrict__ vi = reinterpret_cast< const V* >( pi + head );
+        if ( tid < head )
+            chebyshev_entry( tid, px, pd, pb, pa, pi, alpha, beta, use_d );
+        if ( tid < ns - tail )
+            chebyshev_entry( tail + tid, px, pd, pb, pa, pi, alpha, beta, use_d );
+        for ( size_t j0 = tid; j0 < nv; j0 += kU * stride )
+        {
+            V bv[kU], av[kU], iv[kU], dv[kU], xv[kU];
+#pragma unroll
+            for ( int u = 0; u < kU; ++u )
+            {
+                const size_t j = j0 + u * stride;
+                if ( j < nv )
+                {
+                    bv[u] = vb[j], av[u] = va[j], iv[u] = vi[j], xv[u] = vx[j];
+                    dv[u] = use_d ? vd[j] : V{};
+                }
+            }
+#pragma unroll
+            for ( int u = 0; u < kU; ++u )
+            {
+                const size_t j = j0 + u * stride;
+                if ( j < nv )
+                {
+                    V dn;
+                    Vec16< T >::step( bv[u], av[u], iv[u], dv[u], xv[u], dn, alpha, beta, use_d );
+                    vd[j] = dn;
+                    vx[j] = xv[u];
+                }
+            }
+        }
+        return;
+    }
+    constexpr int kU = 4;
+    for ( size_t i0 = tid; i0 < ns; i0 += kU * stride )
     {
         T z[kU], dv[kU], xv[kU];
 #pragma unroll
@@ -432,7 +545,7 @@ static int chebyshev_step( const tn_mesh* m, int ncomp, T* const* x, T* const* d
          ( rc = ptr3c( ncomp, b, pb, "chebyshev_step" ) ) || ( rc = ptr3c( ncomp, ax, pa, "chebyshev_step" ) ) ||
          ( rc = ptr3c( ncomp, inv_diag, pi, "chebyshev_step" ) ) )
         return rc;
-    chebyshev_kernel< T ><<< dim3( grid_for( m->ns ), ncomp ), kThreads, 0, as_stream( s ) >>>(
+    chebyshev_kernel< T ><<< dim3( grid_for( m->ns, 8 ), ncomp ), kThreads, 0, as_stream( s ) >>>(
         m->ns, px, pd, pb, pa, pi, T( alpha ), T( beta ) );
     TN_LAUNCH_CHECK();
     return TN_OK;

@@ -85,3 +85,35 @@ def test_halo_sum_matches_oracle(meshes):
     v.set_numpy(f)
     v.halo_sum()
     assert rel(v.numpy(), om.halo_sum(f)) <= 1e-15
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+@pytest.mark.parametrize("beta", [0.0, -0.37])
+@pytest.mark.parametrize("layout", ["blocked", "shifted"])
+def test_chebyshev_step(meshes, dtype, beta, layout):
+    """tn_vec_chebyshev_step: d = alpha D^-1 (b - Ax) + beta d, x += d (chebyshev.hpp:127-160).  'blocked': the
+    three components of each field are rows of one tensor (component 1 starts 8 bytes past a 16-byte boundary in
+    FP32, so the vector path starts with a scalar head); 'shifted': x starts one entry later in its buffer than
+    the other fields, so the offsets modulo 16 bytes differ and the scalar path runs."""
+    import ctypes
+    from terraneo_b200 import shell, _capi as C
+    om, pm = meshes
+    ns = pm.stored_nodes
+    rng = np.random.default_rng(11)
+    ref = {k: rng.normal(size=(3, ns)) for k in ("x", "d", "b", "ax", "inv")}
+    dev = {k: torch.as_tensor(v, dtype=dtype, device="cuda").contiguous() for k, v in ref.items()}
+    if layout == "shifted":
+        buf = torch.zeros(3 * ns + 1, dtype=dtype, device="cuda")
+        xs = buf[1:].view(3, ns)
+        xs.copy_(dev["x"])
+        dev["x"] = xs
+    alpha = 0.81
+    P = lambda t: C.ptrs(*[t[c].data_ptr() for c in range(3)])
+    f = C.lib().tn_vec_chebyshev_step_f64 if dtype == torch.float64 else C.lib().tn_vec_chebyshev_step_f32
+    C.check(f(pm.handle, 3, P(dev["x"]), P(dev["d"]), P(dev["b"]), P(dev["ax"]), P(dev["inv"]), alpha, beta,
+              ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), "chebyshev_step")
+    torch.cuda.synchronize()
+    dn = alpha * ref["inv"] * (ref["b"] - ref["ax"]) + beta * ref["d"]
+    tol = 1e-14 if dtype == torch.float64 else 2e-6
+    assert rel(dev["d"].cpu().numpy(), dn) <= tol
+    assert rel(dev["x"].cpu().numpy(), ref["x"] + dn) <= tol
