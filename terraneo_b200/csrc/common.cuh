@@ -47,6 +47,9 @@ template < typename T >
 struct Ptr3
 {
     T* p[3];
+    // component c with compile-time indices only: a kernel that indexes its
+    // parameter array with a run-time c gets the array copied to its stack
+    __host__ __device__ __forceinline__ T* at( int c ) const { return c == 0 ? p[0] : ( c == 1 ? p[1] : p[2] ); }
 };
 
 // Device-side view of the mesh handed to kernels by value.

@@ -118,7 +118,9 @@ __global__ void axpy_dot_kernel( Segs s, SegPtr< T > w, SegPtr< const T > x, con
     constexpr int kU     = 4;
     double        sum[2] = { 0.0, 0.0 };
     const size_t  stride = size_t( gridDim.x ) * blockDim.x;
-    for ( int k = 0; k < s.n; ++k )
+#pragma unroll
+    for ( int k = 0; k < kMaxSegs; ++k ) // compile-time segment indices (no stack copy)
+        if ( k < s.n )
     {
         T* __restrict__ pw             = w.p[k];
         const T* __restrict__ px       = x.p[k];
@@ -179,7 +181,9 @@ __global__ void pcg_begin_kernel( Segs s, SegPtr< const T > r, SegPtr< T > p, do
                                   double* partials, unsigned int* counter )
 {
     Neumaier acc;
-    for ( int k = 0; k < s.n; ++k )
+#pragma unroll
+    for ( int k = 0; k < kMaxSegs; ++k ) // compile-time segment indices (no stack copy)
+        if ( k < s.n )
         for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < s.len[k];
               i += size_t( gridDim.x ) * blockDim.x )
         {
@@ -211,7 +215,9 @@ __global__ void pcg_update_kernel( Segs s, SegPtr< T > x, SegPtr< T > r, SegPtr<
     const double alpha = state[kAn] / state[kPap];
     const T      ta = T( alpha ), tm = T( -alpha );
     Neumaier     acc;
-    for ( int k = 0; k < s.n; ++k )
+#pragma unroll
+    for ( int k = 0; k < kMaxSegs; ++k ) // compile-time segment indices (no stack copy)
+        if ( k < s.n )
         for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < s.len[k];
               i += size_t( gridDim.x ) * blockDim.x )
         {
@@ -243,7 +249,9 @@ __global__ void pcg_direction_kernel( Segs s, SegPtr< T > p, SegPtr< const T > r
     if ( state[kDone] != 0.0 )
         return;
     const T beta = T( state[kBeta] );
-    for ( int k = 0; k < s.n; ++k )
+#pragma unroll
+    for ( int k = 0; k < kMaxSegs; ++k ) // compile-time segment indices (no stack copy)
+        if ( k < s.n )
         for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < s.len[k];
               i += size_t( gridDim.x ) * blockDim.x )
             p.p[k][i] = r.p[k][i] + beta * p.p[k][i];

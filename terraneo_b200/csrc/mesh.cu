@@ -123,7 +123,7 @@ __global__ void halo_sum_kernel( int n_groups, int n1, const int* __restrict__ o
     const int r = int( tid % n1 );
     const int g = int( ( tid / n1 ) % n_groups );
     const int f = int( tid / ( (long long) n1 * n_groups ) );
-    T*        v = fields.p[f];
+    T*        v = fields.at( f );
     const int b = offsets[g], e = offsets[g + 1];
     T         s = 0;
     for ( int m = b; m < e; ++m )

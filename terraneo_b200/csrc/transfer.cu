@@ -46,10 +46,10 @@ __global__ void prolong_constant_kernel( int nf1, int nc1, Ptr3< const T > src, 
         T v = 0;
         for ( int a = 0; a < nl; ++a )
         {
-            const T* col = src.p[c] + ( ( size_t( d ) * nc1 + lx[a] ) * nc1 + ly[a] ) * nc1;
+            const T* col = src.at( c ) + ( ( size_t( d ) * nc1 + lx[a] ) * nc1 + ly[a] ) * nc1;
             v += wl * ( r0 == r1 ? wr * col[r0] : wr * col[r0] + wr * col[r1] );
         }
-        T* o = dst.p[c] + t;
+        T* o = dst.at( c ) + t;
         *o   = add ? *o + v : v;
     }
 }
@@ -66,6 +66,8 @@ __global__ void restrict_constant_kernel( int nf1, int nc1, const uint8_t* __res
     const int d  = int( t / ( (long long) nc1 * nc1 * nc1 ) );
     constexpr int off[7][2] = { { -1, 0 }, { -1, 1 }, { 0, 1 }, { 1, 0 }, { 1, -1 }, { 0, -1 }, { 0, 0 } };
     T             v[3]      = { 0, 0, 0 };
+    // unrolled with guards: compile-time table and component indices (no stack), same summation order
+#pragma unroll
     for ( int s = 0; s < 7; ++s )
     {
         const int xf = 2 * xc + off[s][0], yf = 2 * yc + off[s][1];
@@ -75,21 +77,26 @@ __global__ void restrict_constant_kernel( int nf1, int nc1, const uint8_t* __res
         if ( !owned_f[lat] )
             continue;
         const T wl = s == 6 ? T( 1 ) : T( 0.5 );
+#pragma unroll
         for ( int dr = -1; dr <= 1; ++dr )
         {
             const int rf = 2 * rc + dr;
             if ( rf < 0 || rf >= nf1 )
                 continue;
             const T w = dr == 0 ? wl : T( 0.5 ) * wl;
-            for ( int c = 0; c < ncomp; ++c )
-                v[c] += w * src.p[c][lat * nf1 + rf];
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+                if ( c < ncomp )
+                    v[c] += w * src.at( c )[lat * nf1 + rf];
         }
     }
-    for ( int c = 0; c < ncomp; ++c )
-    {
-        T* o = dst.p[c] + t;
-        *o   = add ? *o + v[c] : v[c];
-    }
+#pragma unroll
+    for ( int c = 0; c < 3; ++c )
+        if ( c < ncomp )
+        {
+            T* o = dst.at( c ) + t;
+            *o   = add ? *o + v[c] : v[c];
+        }
 }
 
 // coarse(X, Y, R) = fine(2X, 2Y, 2R): coefficient fields on coarser levels
@@ -103,7 +110,7 @@ __global__ void inject_kernel( int nf1, int nc1, Ptr3< const T > src, Ptr3< T > 
     const int rc = int( t % nc1 ), yc = int( ( t / nc1 ) % nc1 ), xc = int( ( t / ( (long long) nc1 * nc1 ) ) % nc1 );
     const int d  = int( t / ( (long long) nc1 * nc1 * nc1 ) );
     for ( int c = 0; c < ncomp; ++c )
-        dst.p[c][t] = src.p[c][( ( size_t( d ) * nf1 + 2 * xc ) * nf1 + 2 * yc ) * nf1 + 2 * rc];
+        dst.at( c )[t] = src.at( c )[( ( size_t( d ) * nf1 + 2 * xc ) * nf1 + 2 * yc ) * nf1 + 2 * rc];
 }
 
 // tangential projection of 3-vectors at CMB / SURFACE nodes
@@ -143,11 +150,11 @@ __global__ void prolong_linear_kernel( int Nf, int nc1, const double* __restrict
     int       cx[4], cy[4], cr[4];
     double    w[4];
     const int k = linear_stencil( Nf, coords, radii, d, x, y, r, cx, cy, cr, w );
-    const T*  s = src.p[blockIdx.y];
+    const T*  s = src.at( blockIdx.y );
     T         v = T( 0 );
     for ( int i = 0; i < k; ++i )
         v += T( w[i] ) * s[( ( size_t( d ) * nc1 + cx[i] ) * nc1 + cy[i] ) * nc1 + cr[i]];
-    T* o = dst.p[blockIdx.y] + t;
+    T* o = dst.at( blockIdx.y ) + t;
     *o   = add ? *o + v : v;
 }
 
@@ -169,9 +176,9 @@ __global__ void restrict_linear_kernel( int Nf, int nc1, const double* __restric
     int       cx[4], cy[4], cr[4];
     double    w[4];
     const int k = linear_stencil( Nf, coords, radii, d, x, y, r, cx, cy, cr, w );
-    const T   v = src.p[blockIdx.y][t];
+    const T   v = src.at( blockIdx.y )[t];
     for ( int i = 0; i < k; ++i )
-        atomicAdd( dst.p[blockIdx.y] + ( ( size_t( d ) * nc1 + cx[i] ) * nc1 + cy[i] ) * nc1 + cr[i], T( w[i] ) * v );
+        atomicAdd( dst.at( blockIdx.y ) + ( ( size_t( d ) * nc1 + cx[i] ) * nc1 + cy[i] ) * nc1 + cr[i], T( w[i] ) * v );
 }
 
 int check_levels( const tn_mesh* f, const tn_mesh* c, int ncomp )

@@ -34,7 +34,7 @@ unsigned grid_for( size_t n, int per_thread = 4 )
 template < typename T >
 __device__ __forceinline__ T* comp_ptr( const Ptr3< T >& p, int c )
 {
-    return c == 0 ? p.p[0] : ( c == 1 ? p.p[1] : p.p[2] );
+    return p.at( c );
 }
 
 template < typename T >
@@ -64,9 +64,9 @@ __global__ void elementwise_kernel( size_t ns, int ncomp, Ptr3< T > y, Ptr3< con
     for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
     {
         if ( OP == 0 )
-            y.p[c][i] = T( 1 ) / y.p[c][i]; // invert_inplace (grid_operations.hpp:253)
+            y.at( c )[i] = T( 1 ) / y.at( c )[i]; // invert_inplace (grid_operations.hpp:253)
         else
-            y.p[c][i] = y.p[c][i] * x.p[c][i]; // mult_elementwise_inplace (:273)
+            y.at( c )[i] = y.at( c )[i] * x.at( c )[i]; // mult_elementwise_inplace (:273)
     }
 }
 
@@ -83,7 +83,7 @@ __global__ void randomize_kernel( size_t ns, Ptr3< T > y, unsigned long long see
         z                    = ( z ^ ( z >> 30 ) ) * 0xBF58476D1CE4E5B9ull;
         z                    = ( z ^ ( z >> 27 ) ) * 0x94D049BB133111EBull;
         z                    = z ^ ( z >> 31 );
-        y.p[c][i]            = T( double( z >> 11 ) * ( 2.0 / 9007199254740992.0 ) - 1.0 );
+        y.at( c )[i]         = T( double( z >> 11 ) * ( 2.0 / 9007199254740992.0 ) - 1.0 );
     }
 }
 
@@ -92,7 +92,7 @@ __global__ void cast_kernel( size_t ns, int ncomp, Ptr3< TO > y, Ptr3< const TI 
 {
     const int c = blockIdx.y;
     for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
-        y.p[c][i] = TO( x.p[c][i] );
+        y.at( c )[i] = TO( x.at( c )[i] );
 }
 
 // Owned-node dot product over a flat per-stored-node ownership mask; each
@@ -105,8 +105,8 @@ __global__ void dot_kernel( size_t ns, int ncomp, Ptr3< const T > a, Ptr3< const
     Neumaier acc;
     for ( int c = 0; c < ncomp; ++c )
     {
-        const T* __restrict__ pa = a.p[c];
-        const T* __restrict__ pb = b.p[c];
+        const T* __restrict__ pa = a.at( c );
+        const T* __restrict__ pb = b.at( c );
         for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
         {
             const double v = double( pa[i] ) * double( pb[i] );
@@ -271,7 +271,7 @@ __global__ void max_abs_kernel( size_t ns, int ncomp, Ptr3< const T > x, double*
     for ( int c = 0; c < ncomp; ++c )
     for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
     {
-        const double v = fabs( double( x.p[c][i] ) );
+        const double v = fabs( double( x.at( c )[i] ) );
         // NaN propagates as in Kokkos::max reductions only through comparisons;
         // keep the reference's max-of-abs semantics for finite input.
         m = v > m ? v : m;
@@ -287,7 +287,7 @@ __global__ void nan_kernel( size_t ns, int ncomp, Ptr3< const T > x, double* par
     for ( int c = 0; c < ncomp; ++c )
     for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
     {
-        if ( !isfinite( double( x.p[c][i] ) ) )
+        if ( !isfinite( double( x.at( c )[i] ) ) )
             flag = 1.0;
     }
     block_max_finish( flag, partials, counter, result );
