@@ -421,7 +421,10 @@ def divkgrad_mg_pcg(level, b, x, k=None, mg_levels=3, smoother=1, smoothing_step
 
 class StokesSolver:
     """FGMRES + block-triangular preconditioner + multigrid on the viscous block
-    (apps/mantlecirculation/mantlecirculation.cpp:486-735); mg_fp32 selects the FP32 V-cycle."""
+    (apps/mantlecirculation/mantlecirculation.cpp:486-735); mg_fp32 selects the FP32 V-cycle.
+    outer: 0 FGMRES(restart) in FP64; 1 PMINRES + block-diagonal preconditioner; 2 mixed-precision
+    iterative refinement (needs mg_fp32): FP64 residual and update around FGMRES cycles done entirely in
+    FP32, the coarsest-level PCG in FP64 (no counterpart in the reference)."""
 
     def __init__(self, level, viscosity, mg_levels=4, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=True,
                  chebyshev_order=3, smoothing_steps=2, power_iterations=10, vcycles=1, coarse_max_iterations=50,
