@@ -579,6 +579,23 @@ def cpu_baseline(steps):
             "sample": f"1 oracle apply (Dirichlet/Dirichlet, level {LEVEL}), single thread", "seconds_per_apply": sec}
 
 
+def max_over_ranks(value, world, device):
+    """The largest of the ranks' values (every rank calls this, in the same order); the value itself at N = 1."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gdofs(world, dofs, ms):
+    """Whole-job throughput: each of `world` ranks applies the operator to its own replica of `dofs` DoFs per
+    step, and a step takes `ms` milliseconds on the slowest rank."""
+    return world * dofs / (ms * 1e-3) / 1e9
+
+
 def run_reference(args, rank):
     if rank != 0:
         return 0
@@ -650,13 +667,9 @@ def main():
             step(i)
         ev1.record(stream)
         torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world, "cuda")
     dofs = 3 * mesh.unique_nodes
-    value = world * dofs / (ms * 1e-3) / 1e9
+    value = whole_job_gdofs(world, dofs, ms)
 
     # dominant kernel alone: Neumann/Neumann without communication is exactly one
     # launch of the tiled apply kernel (same per-cell work as the headline step)
@@ -695,7 +708,7 @@ def main():
         shell.apply(op32, s32[i % nsets], d32[i % nsets])
     ev1.record(stream)
     torch.cuda.synchronize()
-    ms32 = ev0.elapsed_time(ev1) / args.steps
+    ms32 = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world, "cuda")
 
     # end to end through the public API with host buffers: pinned H2D of src,
     # apply, D2H of dst, every step
@@ -716,11 +729,7 @@ def main():
         h_dst.copy_(e_dst.data, non_blocking=True)
     ev1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1) / e2e_steps, world, "cuda")
     vec_bytes = 3 * mesh.stored_nodes * 8
 
     if rank == 0:
@@ -740,9 +749,9 @@ def main():
                          "kernel": "kerngen_tile_kernel<double>", "kernel_ms": round(kms, 5),
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
-            "fp32_apply": {"value": round(world * dofs / (ms32 * 1e-3) / 1e9, 3), "unit": "GDoF/s",
+            "fp32_apply": {"value": round(whole_job_gdofs(world, dofs, ms32), 3), "unit": "GDoF/s",
                            "ms_per_step": round(ms32, 5)},
-            "e2e": {"value": round(world * dofs / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GDoF/s",
+            "e2e": {"value": round(whole_job_gdofs(world, dofs, e2e_ms), 3), "unit": "GDoF/s",
                     "h2d_bytes_per_step": vec_bytes, "d2h_bytes_per_step": vec_bytes},
             "gpu_launches": 3 * args.steps,
             "clocks": clk.summary(),
