@@ -17,6 +17,7 @@
 //   laplace L rmin rmax treat diag DIR    Laplace<double> apply
 //   divergence L rmin rmax bcc bcs DIR    Divergence<double>: fine velocity -> coarse pressure
 //   gradient   L rmin rmax bcc bcs DIR    Gradient<double>: coarse pressure -> fine velocity
+//   stokes     L rmin rmax bcc bcs DIR    EpsDivDivStokes<double>: (src_u, src_p) -> (dst_u, dst_p), k.bin
 //   prolong / restrict Lf rmin rmax DIR    constant vector transfer between Lf-1 and Lf
 //   kmass   L rmin rmax mode DIR          KMass<double> (0 full, 1 diagonal, 2 lumped)
 //   divkgrad L rmin rmax treat diag single DIR   DivKGrad<double> (k.bin, src.bin)
@@ -40,6 +41,7 @@
 #include "communication/shell/communication.hpp"
 #include "fe/wedge/operators/shell/epsilon_divdiv.hpp"
 #include "fe/wedge/operators/shell/epsilon_divdiv_kerngen.hpp"
+#include "fe/wedge/operators/shell/epsilon_divdiv_stokes.hpp"
 #include "fe/wedge/operators/shell/div_k_grad.hpp"
 #include "fe/wedge/operators/shell/divergence.hpp"
 #include "fe/wedge/operators/shell/gradient.hpp"
@@ -282,6 +284,27 @@ int cmd_stokes_block( bool div, int L, double rmin, double rmax, int bcc, int bc
     return 0;
 }
 
+// EpsDivDivStokes<double> (epsilon_divdiv_stokes.hpp:55-90): [A B^T; B 0] applied to (u, p), A the
+// kerngen operator with k.bin on level L, p on level L-1
+int cmd_stokes_op( int L, double rmin, double rmax, int bcc, int bcs, const std::string& dir )
+{
+    Setup                            f( L, rmin, rmax ), c( L - 1, rmin, rmax );
+    BoundaryConditions b = { { ShellBoundaryFlag::CMB, bc_of( bcc ) }, { ShellBoundaryFlag::SURFACE, bc_of( bcs ) } };
+    linalg::VectorQ1Scalar< double > k( "k", f.domain, f.omask );
+    view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", f.nodes ).data() );
+    linalg::VectorQ1IsoQ2Q1< double > src( "src", f.domain, c.domain, f.omask, c.omask ),
+        dst( "dst", f.domain, c.domain, f.omask, c.omask );
+    load_vec( src.block_1(), dir + "/src_u.bin", f.nodes );
+    view_from_host( src.block_2().grid_data(), read_file< double >( dir + "/src_p.bin", c.nodes ).data() );
+    fe::wedge::operators::shell::EpsDivDivStokes< double > op( f.domain, c.domain, f.coords, f.radii, f.bmask,
+                                                               k.grid_data(), b, false );
+    linalg::apply( op, src, dst );
+    save_vec( dst.block_1(), dir + "/dst_u.bin", f.nodes );
+    auto out = view_to_host( dst.block_2().grid_data() );
+    write_file( dir + "/dst_p.bin", out.data(), out.size() );
+    return 0;
+}
+
 int cmd_transfer( bool prolong, int Lf, double rmin, double rmax, const std::string& dir )
 {
     Setup                         f( Lf, rmin, rmax ), c( Lf - 1, rmin, rmax );
@@ -497,6 +520,8 @@ int main( int argc, char** argv )
         return cmd_stokes_block( cmd == "divergence", I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     if ( ( cmd == "prolong" || cmd == "restrict" ) && argc == 6 )
         return cmd_transfer( cmd == "prolong", I( 2 ), D( 3 ), D( 4 ), argv[5] );
+    if ( cmd == "stokes" && argc == 8 )
+        return cmd_stokes_op( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     if ( cmd == "kmass" && argc == 7 )
         return cmd_kmass( I( 2 ), D( 3 ), D( 4 ), I( 5 ), argv[6] );
     if ( ( cmd == "prolong_linear" || cmd == "restrict_linear" ) && argc == 6 )

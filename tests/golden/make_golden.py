@@ -26,6 +26,7 @@ R_MIN, R_MAX = 0.55, 1.0
 KERNGEN_CASES = [(1, 1, 0), (2, 2, 0), (2, 1, 0), (1, 2, 0), (0, 0, 0), (0, 1, 0), (1, 1, 1), (2, 2, 1)]
 LAPLACE_CASES = [(1, 0), (0, 0), (1, 1)]
 STOKES_BCS = [(1, 1), (2, 2), (0, 0)]
+STOKES_OP_BCS = [(1, 1), (2, 2), (2, 1)]
 KMASS_MODES = [0, 1, 2]
 MASS_MODES = [0, 1, 2]
 VMASS_MODES = [0, 1]
@@ -115,6 +116,14 @@ def main():
             x["p"].tofile(f"{d}/src.bin")
             run_ref(["gradient", L, R_MIN, R_MAX, bcc, bcs, d], d)
             out[f"gradient_{bcc}{bcs}"] = np.fromfile(f"{d}/dst.bin").reshape((3,) + fine.shape)
+
+        x["k"].tofile(f"{d}/k.bin")
+        x["u"].tofile(f"{d}/src_u.bin")
+        x["p"].tofile(f"{d}/src_p.bin")
+        for bcc, bcs in STOKES_OP_BCS:
+            run_ref(["stokes", L, R_MIN, R_MAX, bcc, bcs, d], d)
+            out[f"stokes_u_{bcc}{bcs}"] = np.fromfile(f"{d}/dst_u.bin").reshape((3,) + fine.shape)
+            out[f"stokes_p_{bcc}{bcs}"] = np.fromfile(f"{d}/dst_p.bin").reshape(coarse.shape)
 
         x["uc"].tofile(f"{d}/src.bin")
         run_ref(["prolong", L, R_MIN, R_MAX, d], d)

@@ -65,6 +65,17 @@ def test_stokes_blocks_match_reference(case, bcc, bcs):
     assert rel(fine.gradient(coarse, x["p"], bcc, bcs), g[f"gradient_{bcc}{bcs}"]) <= TOL
 
 
+@pytest.mark.parametrize("bcc,bcs", G.STOKES_OP_BCS)
+def test_stokes_operator_matches_reference(case, bcc, bcs):
+    """EpsDivDivStokes (epsilon_divdiv_stokes.hpp:55-90): A (no halo) + B^T (Add, halo) on the velocity block,
+    B on the pressure block, equals the composition of the pinned oracle blocks."""
+    g, fine, coarse, x = case
+    u = fine.kerngen(x["k"], x["u"], bcc, bcs) + fine.gradient(coarse, x["p"], bcc, bcs)
+    p = fine.divergence(coarse, x["u"], bcc, bcs)
+    assert rel(u, g[f"stokes_u_{bcc}{bcs}"]) <= TOL
+    assert rel(p, g[f"stokes_p_{bcc}{bcs}"]) <= TOL
+
+
 def test_transfers_match_reference(case):
     g, fine, coarse, x = case
     assert rel(fine.prolong(coarse, x["uc"]), g["prolong"]) <= TOL
