@@ -18,6 +18,8 @@
 //   divergence L rmin rmax bcc bcs DIR    Divergence<double>: fine velocity -> coarse pressure
 //   gradient   L rmin rmax bcc bcs DIR    Gradient<double>: coarse pressure -> fine velocity
 //   stokes     L rmin rmax bcc bcs DIR    EpsDivDivStokes<double>: (src_u, src_p) -> (dst_u, dst_p), k.bin
+//   vcycle Lmin Lmax rmin rmax omega smooth cycles cmaxit DIR  Laplace multigrid (Jacobi, constant
+//                                          transfers, coarse PCG) from x = 0 on b.bin, writes x.bin
 //   prolong / restrict Lf rmin rmax DIR    constant vector transfer between Lf-1 and Lf
 //   kmass   L rmin rmax mode DIR          KMass<double> (0 full, 1 diagonal, 2 lumped)
 //   divkgrad L rmin rmax treat diag single DIR   DivKGrad<double> (k.bin, src.bin)
@@ -58,6 +60,8 @@
 #include "fv/hex/operators/fct_advection_diffusion.hpp"
 #include "grid/bit_masks.hpp"
 #include "linalg/solvers/gca/gca.hpp"
+#include "linalg/solvers/jacobi.hpp"
+#include "linalg/solvers/multigrid.hpp"
 #include "linalg/solvers/pcg.hpp"
 #include "util/table.hpp"
 #include "grid/shell/bit_masks.hpp"
@@ -281,6 +285,63 @@ int cmd_stokes_block( bool div, int L, double rmin, double rmax, int bcc, int bc
         linalg::apply( op, p, u );
         save_vec( u, dir + "/dst.bin", f.nodes );
     }
+    return 0;
+}
+
+// `cycles` multigrid V-cycles (multigrid.hpp:108-211) on Laplace<double> (Dirichlet rows) over levels
+// Lmin..Lmax from x = 0: Jacobi pre / post smoothing (jacobi.hpp:51-62, inverse diagonal of the
+// Dirichlet operator, `smooth` sweeps, damping omega), constant scalar transfers, coarsest-level PCG
+// (pcg.hpp, max `cmaxit` iterations, relative 1e-8, absolute 1e-30); b.bin on Lmax, writes x.bin
+int cmd_vcycle( int Lmin, int Lmax, double rmin, double rmax, double omega, int smooth, int cycles, int cmaxit,
+                const std::string& dir )
+{
+    using V   = linalg::VectorQ1Scalar< double >;
+    using Lap = fe::wedge::operators::shell::Laplace< double >;
+    using P   = fe::wedge::operators::shell::ProlongationConstant< double >;
+    using R   = fe::wedge::operators::shell::RestrictionConstant< double >;
+    std::vector< Setup > lv;
+    for ( int l = Lmin; l <= Lmax; ++l )
+        lv.emplace_back( l, rmin, rmax );
+    std::vector< P >                            Ps;
+    std::vector< R >                            Rs;
+    std::vector< Lap >                          Ac;
+    std::vector< V >                            tr, te, tmp, ctmps;
+    std::vector< linalg::solvers::Jacobi< Lap > > sm;
+    for ( size_t i = 0; i < lv.size(); ++i )
+    {
+        Setup& s = lv[i];
+        tmp.emplace_back( "tmp" + std::to_string( i ), s.domain, s.omask );
+        V ts( "ts" + std::to_string( i ), s.domain, s.omask ), inv( "inv" + std::to_string( i ), s.domain, s.omask );
+        Lap Ad( s.domain, s.coords, s.radii, s.bmask, true, true );
+        linalg::assign( ts, 1.0 );
+        linalg::apply( Ad, ts, inv );
+        linalg::invert_entries( inv );
+        sm.emplace_back( inv, smooth, ts, omega );
+        if ( i == 0 )
+            for ( int k = 0; k < 4; ++k )
+                ctmps.emplace_back( "ct" + std::to_string( k ), s.domain, s.omask );
+        if ( i + 1 < lv.size() )
+        {
+            tr.emplace_back( "tr" + std::to_string( i ), s.domain, s.omask );
+            te.emplace_back( "te" + std::to_string( i ), s.domain, s.omask );
+            Ac.emplace_back( s.domain, s.coords, s.radii, s.bmask, true, false );
+            Ps.emplace_back( linalg::OperatorApplyMode::Add );
+            Rs.emplace_back( s.domain );
+        }
+    }
+    Setup& f = lv.back();
+    V      b( "b", f.domain, f.omask ), x( "x", f.domain, f.omask );
+    view_from_host( b.grid_data(), read_file< double >( dir + "/b.bin", f.nodes ).data() );
+    linalg::assign( x, 0.0 );
+    Lap  A( f.domain, f.coords, f.radii, f.bmask, true, false );
+    auto table = std::make_shared< util::Table >();
+    linalg::solvers::PCG< Lap > coarse( linalg::solvers::IterativeSolverParameters{ cmaxit, 1e-8, 1e-30 }, table,
+                                        ctmps );
+    linalg::solvers::Multigrid< Lap, P, R, linalg::solvers::Jacobi< Lap >, linalg::solvers::PCG< Lap > > mg(
+        Ps, Rs, Ac, tr, te, tmp, sm, sm, coarse, cycles, 0.0 );
+    linalg::solvers::solve( mg, A, x, b );
+    auto out = view_to_host( x.grid_data() );
+    write_file( dir + "/x.bin", out.data(), out.size() );
     return 0;
 }
 
@@ -520,6 +581,8 @@ int main( int argc, char** argv )
         return cmd_stokes_block( cmd == "divergence", I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     if ( ( cmd == "prolong" || cmd == "restrict" ) && argc == 6 )
         return cmd_transfer( cmd == "prolong", I( 2 ), D( 3 ), D( 4 ), argv[5] );
+    if ( cmd == "vcycle" && argc == 11 )
+        return cmd_vcycle( I( 2 ), I( 3 ), D( 4 ), D( 5 ), D( 6 ), I( 7 ), I( 8 ), I( 9 ), argv[10] );
     if ( cmd == "stokes" && argc == 8 )
         return cmd_stokes_op( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     if ( cmd == "kmass" && argc == 7 )

@@ -80,6 +80,16 @@ def cg_rhs(s):
     return b
 
 
+# Laplace V-cycles over levels 1-3 (Jacobi omega 0.6, 2 sweeps, 2 cycles, coarse PCG <= 50 iterations)
+VCYCLE = dict(lmin=1, lmax=3, omega=0.6, smooth=2, cycles=2, cmaxit=50)
+
+
+def vcycle_rhs():
+    """seeded right-hand side on the finest V-cycle level"""
+    m = Mesh(VCYCLE["lmax"])
+    return m.make_consistent(np.random.RandomState(31).normal(size=m.shape)).reshape(m.shape)
+
+
 def checksum(a):
     a = np.asarray(a, dtype=np.float64)
     return np.array([a.sum(), (a * a).sum(), np.abs(a).max()])
@@ -124,6 +134,13 @@ def main():
             run_ref(["stokes", L, R_MIN, R_MAX, bcc, bcs, d], d)
             out[f"stokes_u_{bcc}{bcs}"] = np.fromfile(f"{d}/dst_u.bin").reshape((3,) + fine.shape)
             out[f"stokes_p_{bcc}{bcs}"] = np.fromfile(f"{d}/dst_p.bin").reshape(coarse.shape)
+
+        vb = vcycle_rhs()
+        out["checksum_vcycle_b"] = checksum(vb)
+        vb.tofile(f"{d}/b.bin")
+        V = VCYCLE
+        run_ref(["vcycle", V["lmin"], V["lmax"], R_MIN, R_MAX, V["omega"], V["smooth"], V["cycles"], V["cmaxit"], d], d)
+        out["vcycle_x"] = np.fromfile(f"{d}/x.bin").reshape(vb.shape)
 
         x["uc"].tofile(f"{d}/src.bin")
         run_ref(["prolong", L, R_MIN, R_MAX, d], d)

@@ -274,6 +274,35 @@ class Mesh:
                    for i in range(a.shape[0]))
 
 
+def laplace_vcycles(meshes, b, omega, smooth, cycles, coarse_max_iterations):
+    """Multigrid V-cycles from x = 0 (linalg/solvers/multigrid.hpp:108-211) on Laplace with Dirichlet rows over
+    `meshes` (coarsest first): Jacobi pre / post smoothing (jacobi.hpp:51-62: x += omega D^-1 (b - A x), D the
+    diagonal of the Dirichlet operator, `smooth` sweeps), constant scalar restriction and additive prolongation,
+    and on the coarsest mesh the unpreconditioned PCG from zero (pcg.hpp; relative 1e-8, absolute 1e-30)."""
+    inv = [1.0 / m.laplace(np.ones(m.shape), True, True) for m in meshes]
+
+    def jacobi(l, x, rhs):
+        for _ in range(smooth):
+            x += omega * (inv[l] * (rhs - meshes[l].laplace(x, True, False)))
+
+    def cycle(l, x, rhs):
+        if l == 0:
+            x[...] = meshes[0].laplace_pcg(rhs, coarse_max_iterations, 1e-8, 1e-30)[0]
+            return
+        fine, coarse = meshes[l], meshes[l - 1]
+        jacobi(l, x, rhs)
+        rc = fine.restrict(coarse, rhs - fine.laplace(x, True, False), ncomp=1)[0]
+        ec = np.zeros(coarse.shape)
+        cycle(l - 1, ec, rc)
+        x += fine.prolong(coarse, ec, ncomp=1)[0]
+        jacobi(l, x, rhs)
+
+    x = np.zeros(meshes[-1].shape)
+    for _ in range(cycles):
+        cycle(len(meshes) - 1, x, np.asarray(b, dtype=np.float64))
+    return x
+
+
 def ref_available():
     return os.path.exists(REF_DUMP)
 

@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from helpers import rel
-from oracle_lib import Mesh, ref_available, run_ref
+from oracle_lib import Mesh, laplace_vcycles, ref_available, run_ref
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 import make_golden as G  # noqa: E402
@@ -74,6 +74,18 @@ def test_stokes_operator_matches_reference(case, bcc, bcs):
     p = fine.divergence(coarse, x["u"], bcc, bcs)
     assert rel(u, g[f"stokes_u_{bcc}{bcs}"]) <= TOL
     assert rel(p, g[f"stokes_p_{bcc}{bcs}"]) <= TOL
+
+
+def test_laplace_vcycles_match_reference(case):
+    """Multigrid (multigrid.hpp:108-211) with Jacobi smoothing, constant transfers and the coarse PCG: two
+    V-cycles over levels 1-3 from x = 0 against the reference's own Multigrid<Laplace, ...>."""
+    g = case[0]
+    V = G.VCYCLE
+    b = G.vcycle_rhs()
+    assert np.allclose(G.checksum(b), g["checksum_vcycle_b"], rtol=1e-13, atol=0)
+    meshes = [Mesh(level) for level in range(V["lmin"], V["lmax"] + 1)]
+    x = laplace_vcycles(meshes, b, V["omega"], V["smooth"], V["cycles"], V["cmaxit"])
+    assert rel(x, g["vcycle_x"]) <= TOL
 
 
 def test_transfers_match_reference(case):
