@@ -18,6 +18,7 @@
 //   divergence L rmin rmax bcc bcs DIR    Divergence<double>: fine velocity -> coarse pressure
 //   gradient   L rmin rmax bcc bcs DIR    Gradient<double>: coarse pressure -> fine velocity
 //   stokes     L rmin rmax bcc bcs DIR    EpsDivDivStokes<double>: (src_u, src_p) -> (dst_u, dst_p), k.bin
+//   laplace_fgmres L rmin rmax restart maxit reltol DIR  FGMRES on Laplace from x = 0 on b.bin: x.bin, hist.bin
 //   vcycle Lmin Lmax rmin rmax omega smooth cycles cmaxit DIR  Laplace multigrid (Jacobi, constant
 //                                          transfers, coarse PCG) from x = 0 on b.bin, writes x.bin
 //   prolong / restrict Lf rmin rmax DIR    constant vector transfer between Lf-1 and Lf
@@ -60,6 +61,7 @@
 #include "fv/hex/operators/fct_advection_diffusion.hpp"
 #include "grid/bit_masks.hpp"
 #include "linalg/solvers/gca/gca.hpp"
+#include "linalg/solvers/fgmres.hpp"
 #include "linalg/solvers/jacobi.hpp"
 #include "linalg/solvers/multigrid.hpp"
 #include "linalg/solvers/pcg.hpp"
@@ -345,6 +347,35 @@ int cmd_vcycle( int Lmin, int Lmax, double rmin, double rmax, double omega, int 
     return 0;
 }
 
+// FGMRES<Laplace<double>> (fgmres.hpp:100-330, identity preconditioner, Dirichlet rows) from x = 0 on b.bin;
+// writes x.bin and hist.bin (the relative residual of every row of the solver's statistics table)
+int cmd_laplace_fgmres( int L, double rmin, double rmax, int restart, int maxit, double reltol, const std::string& dir )
+{
+    using V   = linalg::VectorQ1Scalar< double >;
+    using Lap = fe::wedge::operators::shell::Laplace< double >;
+    Setup s( L, rmin, rmax );
+    V     b( "b", s.domain, s.omask ), x( "x", s.domain, s.omask );
+    std::vector< V > tmps;
+    for ( int i = 0; i < 2 * restart + 4; ++i )
+        tmps.emplace_back( "tmp" + std::to_string( i ), s.domain, s.omask );
+    view_from_host( b.grid_data(), read_file< double >( dir + "/b.bin", s.nodes ).data() );
+    linalg::assign( x, 0.0 );
+    Lap  A( s.domain, s.coords, s.radii, s.bmask, true, false );
+    auto table = std::make_shared< util::Table >();
+    linalg::solvers::FGMRESOptions< double > opt;
+    opt.restart = restart, opt.relative_residual_tolerance = reltol, opt.absolute_residual_tolerance = 1e-30;
+    opt.max_iterations = maxit;
+    linalg::solvers::FGMRES< Lap > fg( tmps, opt, table );
+    linalg::solvers::solve( fg, A, x, b );
+    std::vector< double > hist;
+    for ( const auto& row : table->rows() )
+        hist.push_back( std::get< double >( row.at( "relative_residual" ) ) );
+    write_file( dir + "/hist.bin", hist.data(), hist.size() );
+    auto out = view_to_host( x.grid_data() );
+    write_file( dir + "/x.bin", out.data(), out.size() );
+    return 0;
+}
+
 // EpsDivDivStokes<double> (epsilon_divdiv_stokes.hpp:55-90): [A B^T; B 0] applied to (u, p), A the
 // kerngen operator with k.bin on level L, p on level L-1
 int cmd_stokes_op( int L, double rmin, double rmax, int bcc, int bcs, const std::string& dir )
@@ -581,6 +612,8 @@ int main( int argc, char** argv )
         return cmd_stokes_block( cmd == "divergence", I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     if ( ( cmd == "prolong" || cmd == "restrict" ) && argc == 6 )
         return cmd_transfer( cmd == "prolong", I( 2 ), D( 3 ), D( 4 ), argv[5] );
+    if ( cmd == "laplace_fgmres" && argc == 9 )
+        return cmd_laplace_fgmres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), D( 7 ), argv[8] );
     if ( cmd == "vcycle" && argc == 11 )
         return cmd_vcycle( I( 2 ), I( 3 ), D( 4 ), D( 5 ), D( 6 ), I( 7 ), I( 8 ), I( 9 ), argv[10] );
     if ( cmd == "stokes" && argc == 8 )

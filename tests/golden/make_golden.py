@@ -80,6 +80,9 @@ def cg_rhs(s):
     return b
 
 
+# FGMRES(10) on the Laplace (the CG right-hand side), at most 60 iterations, 1e-10
+FGMRES_CASE = dict(restart=10, maxit=60, tol=1e-10)
+
 # Laplace V-cycles over levels 1-3 (Jacobi omega 0.6, 2 sweeps, 2 cycles, coarse PCG <= 50 iterations)
 VCYCLE = dict(lmin=1, lmax=3, omega=0.6, smooth=2, cycles=2, cmaxit=50)
 
@@ -134,6 +137,12 @@ def main():
             run_ref(["stokes", L, R_MIN, R_MAX, bcc, bcs, d], d)
             out[f"stokes_u_{bcc}{bcs}"] = np.fromfile(f"{d}/dst_u.bin").reshape((3,) + fine.shape)
             out[f"stokes_p_{bcc}{bcs}"] = np.fromfile(f"{d}/dst_p.bin").reshape(coarse.shape)
+
+        cg_rhs(x["s"]).tofile(f"{d}/b.bin")
+        F = FGMRES_CASE
+        run_ref(["laplace_fgmres", L, R_MIN, R_MAX, F["restart"], F["maxit"], F["tol"], d], d)
+        out["fgmres_x"] = np.fromfile(f"{d}/x.bin").reshape(fine.shape)
+        out["fgmres_hist"] = np.fromfile(f"{d}/hist.bin")
 
         vb = vcycle_rhs()
         out["checksum_vcycle_b"] = checksum(vb)

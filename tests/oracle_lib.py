@@ -274,6 +274,74 @@ class Mesh:
                    for i in range(a.shape[0]))
 
 
+def fgmres(apply, dot, b, restart, max_iterations, relative_tolerance, absolute_tolerance=1e-30):
+    """FGMRES with the identity preconditioner from x = 0 (linalg/solvers/fgmres.hpp:100-330): modified
+    Gram-Schmidt Arnoldi, Givens rotations, the breakdown and stagnation exits, restarts from the true
+    residual.  Returns (x, relative residual history: 1 at the start, then one entry per iteration)."""
+    eps = np.finfo(np.float64).eps
+    b = np.asarray(b, dtype=np.float64)
+    x = np.zeros_like(b)
+    r = b - apply(x)
+    beta0 = np.sqrt(dot(r, r))
+    r0 = beta0
+    hist = [1.0]
+    if beta0 <= absolute_tolerance:
+        return x, hist
+    m, total = restart, 0
+    while total < max_iterations:
+        V, Z = [r * (1.0 / beta0)], []
+        H = np.zeros((m + 1, m))
+        g = np.zeros(m + 1)
+        cs, sn = np.zeros(m + 1), np.zeros(m + 1)
+        g[0] = beta0
+        inner, j = 0, 0
+        while j < m and total < max_iterations:
+            Z.append(V[j].copy())
+            w = apply(Z[j])
+            for i in range(j + 1):
+                H[i, j] = dot(w, V[i])
+                w = w + (-H[i, j]) * V[i]
+            h = np.sqrt(dot(w, w))
+            if h < eps * r0:
+                H[j + 1, j] = 0.0
+                inner = j + 1
+                break
+            H[j + 1, j] = h
+            if h > 0:
+                V.append(w * (1.0 / h))
+            for i in range(j):
+                t = cs[i] * H[i, j] + sn[i] * H[i + 1, j]
+                H[i + 1, j] = -sn[i] * H[i, j] + cs[i] * H[i + 1, j]
+                H[i, j] = t
+            a, bb = H[j, j], H[j + 1, j]
+            rab = np.hypot(a, bb)
+            cs[j] = 1.0 if rab == 0 else a / rab
+            sn[j] = 0.0 if rab == 0 else bb / rab
+            H[j, j], H[j + 1, j] = rab, 0.0
+            if abs(H[j, j]) < eps:
+                inner = j
+                break
+            g[j], g[j + 1] = cs[j] * g[j] + sn[j] * g[j + 1], -sn[j] * g[j] + cs[j] * g[j + 1]
+            hist.append(abs(g[j + 1]) / r0)
+            inner = j + 1
+            if hist[-1] <= relative_tolerance or abs(g[j + 1]) < absolute_tolerance:
+                break
+            j += 1
+            total += 1
+        y = np.zeros(inner)
+        for row in range(inner - 1, -1, -1):
+            y[row] = (g[row] - sum(H[row, col] * y[col] for col in range(row + 1, inner))) / H[row, row]
+        acc = np.zeros_like(b)
+        for i in range(inner):
+            acc = acc + y[i] * Z[i]
+        x = x + acc
+        r = b - apply(x)
+        beta0 = np.sqrt(dot(r, r))
+        if beta0 <= absolute_tolerance or beta0 / r0 <= relative_tolerance:
+            break
+    return x, hist
+
+
 def laplace_vcycles(meshes, b, omega, smooth, cycles, coarse_max_iterations):
     """Multigrid V-cycles from x = 0 (linalg/solvers/multigrid.hpp:108-211) on Laplace with Dirichlet rows over
     `meshes` (coarsest first): Jacobi pre / post smoothing (jacobi.hpp:51-62: x += omega D^-1 (b - A x), D the
