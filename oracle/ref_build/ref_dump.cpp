@@ -19,6 +19,9 @@
 //   gradient   L rmin rmax bcc bcs DIR    Gradient<double>: coarse pressure -> fine velocity
 //   stokes     L rmin rmax bcc bcs DIR    EpsDivDivStokes<double>: (src_u, src_p) -> (dst_u, dst_p), k.bin
 //   laplace_fgmres L rmin rmax restart maxit reltol DIR  FGMRES on Laplace from x = 0 on b.bin: x.bin, hist.bin
+//   stokes_fgmres L rmin rmax bcc bcs restart maxit tol sweeps omega DIR  FGMRES on EpsDivDivStokes with the
+//                                          block-triangular preconditioner (Jacobi velocity block, lumped
+//                                          KMass(1/kp) Schur block): x_u.bin, x_p.bin, hist.bin
 //   vcycle Lmin Lmax rmin rmax omega smooth cycles cmaxit DIR  Laplace multigrid (Jacobi, constant
 //                                          transfers, coarse PCG) from x = 0 on b.bin, writes x.bin
 //   prolong / restrict Lf rmin rmax DIR    constant vector transfer between Lf-1 and Lf
@@ -61,6 +64,8 @@
 #include "fv/hex/operators/fct_advection_diffusion.hpp"
 #include "grid/bit_masks.hpp"
 #include "linalg/solvers/gca/gca.hpp"
+#include "linalg/solvers/block_preconditioner_2x2.hpp"
+#include "linalg/solvers/diagonal_solver.hpp"
 #include "linalg/solvers/fgmres.hpp"
 #include "linalg/solvers/jacobi.hpp"
 #include "linalg/solvers/multigrid.hpp"
@@ -376,6 +381,67 @@ int cmd_laplace_fgmres( int L, double rmin, double rmax, int restart, int maxit,
     return 0;
 }
 
+// FGMRES on EpsDivDivStokes with the app's block-triangular preconditioner (mantlecirculation.cpp:684-717):
+// Schur block the inverse lumped KMass(1 / eta_p) (kp.bin = eta on the pressure level), velocity block
+// `sweeps` damped Jacobi sweeps with the kerngen diagonal (deterministic, unlike the Chebyshev smoother's
+// randomised power iteration); b = (src_u, src_p), x = 0; writes x_u.bin, x_p.bin, hist.bin
+int cmd_stokes_fgmres( int L, double rmin, double rmax, int bcc, int bcs, int restart, int maxit, double tol,
+                       int sweeps, double omega, const std::string& dir )
+{
+    using Stokes  = fe::wedge::operators::shell::EpsDivDivStokes< double >;
+    using Viscous = Stokes::Block11Type;
+    using Grad    = Stokes::Block12Type;
+    using PMass   = fe::wedge::operators::shell::KMass< double >;
+    using BV      = linalg::VectorQ1IsoQ2Q1< double >;
+    using PrecV   = linalg::solvers::Jacobi< Viscous >;
+    using PrecS   = linalg::solvers::DiagonalSolver< PMass >;
+    using Prec    = linalg::solvers::BlockTriangularPreconditioner2x2< Stokes, Viscous, PMass, Grad, PrecV, PrecS >;
+    Setup f( L, rmin, rmax ), c( L - 1, rmin, rmax );
+    BoundaryConditions b = { { ShellBoundaryFlag::CMB, bc_of( bcc ) }, { ShellBoundaryFlag::SURFACE, bc_of( bcs ) } };
+    linalg::VectorQ1Scalar< double > k( "k", f.domain, f.omask ), kp( "kp", c.domain, c.omask );
+    view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", f.nodes ).data() );
+    view_from_host( kp.grid_data(), read_file< double >( dir + "/kp.bin", c.nodes ).data() );
+    linalg::invert_entries( kp );
+    Stokes K( f.domain, c.domain, f.coords, f.radii, f.bmask, k.grid_data(), b, false );
+    // velocity block: inverse of the kerngen diagonal (diagonal mode of the same operator)
+    linalg::VectorQ1Vec< double > ones( "ones", f.domain, f.omask ), inv( "inv", f.domain, f.omask ),
+        jt( "jt", f.domain, f.omask );
+    Viscous Kd( f.domain, f.coords, f.radii, f.bmask, k.grid_data(), b, true );
+    linalg::assign( ones, 1.0 );
+    linalg::apply( Kd, ones, inv );
+    linalg::invert_entries( inv );
+    PrecV pv( inv, sweeps, jt, omega );
+    PMass pmass( c.domain, c.coords, c.radii, kp.grid_data(), false );
+    pmass.set_lumped_diagonal( true );
+    linalg::VectorQ1Scalar< double > lumped( "lumped", c.domain, c.omask ), t1( "t1", c.domain, c.omask );
+    linalg::assign( t1, 1.0 );
+    linalg::apply( pmass, t1, lumped );
+    PrecS ps( lumped );
+    BV    ptmp( "ptmp", f.domain, c.domain, f.omask, c.omask );
+    Prec  prec( K.block_11(), pmass, K.block_12(), ptmp, pv, ps );
+    std::vector< BV > tmps;
+    for ( int i = 0; i < 2 * restart + 4; ++i )
+        tmps.emplace_back( "tmp" + std::to_string( i ), f.domain, c.domain, f.omask, c.omask );
+    BV rhs( "rhs", f.domain, c.domain, f.omask, c.omask ), x( "x", f.domain, c.domain, f.omask, c.omask );
+    load_vec( rhs.block_1(), dir + "/src_u.bin", f.nodes );
+    view_from_host( rhs.block_2().grid_data(), read_file< double >( dir + "/src_p.bin", c.nodes ).data() );
+    linalg::assign( x, 0.0 );
+    auto table = std::make_shared< util::Table >();
+    linalg::solvers::FGMRESOptions< double > opt;
+    opt.restart = restart, opt.relative_residual_tolerance = tol, opt.absolute_residual_tolerance = 1e-30;
+    opt.max_iterations = maxit;
+    linalg::solvers::FGMRES< Stokes, Prec > fg( tmps, opt, table, prec );
+    linalg::solvers::solve( fg, K, x, rhs );
+    std::vector< double > hist;
+    for ( const auto& row : table->rows() )
+        hist.push_back( std::get< double >( row.at( "relative_residual" ) ) );
+    write_file( dir + "/hist.bin", hist.data(), hist.size() );
+    save_vec( x.block_1(), dir + "/x_u.bin", f.nodes );
+    auto xp = view_to_host( x.block_2().grid_data() );
+    write_file( dir + "/x_p.bin", xp.data(), xp.size() );
+    return 0;
+}
+
 // EpsDivDivStokes<double> (epsilon_divdiv_stokes.hpp:55-90): [A B^T; B 0] applied to (u, p), A the
 // kerngen operator with k.bin on level L, p on level L-1
 int cmd_stokes_op( int L, double rmin, double rmax, int bcc, int bcs, const std::string& dir )
@@ -612,6 +678,9 @@ int main( int argc, char** argv )
         return cmd_stokes_block( cmd == "divergence", I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     if ( ( cmd == "prolong" || cmd == "restrict" ) && argc == 6 )
         return cmd_transfer( cmd == "prolong", I( 2 ), D( 3 ), D( 4 ), argv[5] );
+    if ( cmd == "stokes_fgmres" && argc == 13 )
+        return cmd_stokes_fgmres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), I( 8 ), D( 9 ), I( 10 ), D( 11 ),
+                                  argv[12] );
     if ( cmd == "laplace_fgmres" && argc == 9 )
         return cmd_laplace_fgmres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), D( 7 ), argv[8] );
     if ( cmd == "vcycle" && argc == 11 )

@@ -83,6 +83,15 @@ def cg_rhs(s):
 # FGMRES(10) on the Laplace (the CG right-hand side), at most 60 iterations, 1e-10
 FGMRES_CASE = dict(restart=10, maxit=60, tol=1e-10)
 
+# FGMRES(10) on the Stokes block operator with the block-triangular preconditioner (2 Jacobi sweeps,
+# damping 0.5; Schur block from the pressure-level viscosity exp(0.3 pc)), 30 iterations
+STOKES_FGMRES = dict(restart=10, maxit=30, tol=1e-8, sweeps=2, omega=0.5, bcs=[(2, 2), (1, 1)])
+
+
+def pressure_viscosity(x):
+    return np.exp(0.3 * x["pc"])
+
+
 # Laplace V-cycles over levels 1-3 (Jacobi omega 0.6, 2 sweeps, 2 cycles, coarse PCG <= 50 iterations)
 VCYCLE = dict(lmin=1, lmax=3, omega=0.6, smooth=2, cycles=2, cmaxit=50)
 
@@ -143,6 +152,18 @@ def main():
         run_ref(["laplace_fgmres", L, R_MIN, R_MAX, F["restart"], F["maxit"], F["tol"], d], d)
         out["fgmres_x"] = np.fromfile(f"{d}/x.bin").reshape(fine.shape)
         out["fgmres_hist"] = np.fromfile(f"{d}/hist.bin")
+
+        S = STOKES_FGMRES
+        x["k"].tofile(f"{d}/k.bin")
+        pressure_viscosity(x).tofile(f"{d}/kp.bin")
+        x["u"].tofile(f"{d}/src_u.bin")
+        x["p"].tofile(f"{d}/src_p.bin")
+        for bcc, bcs in S["bcs"]:
+            run_ref(["stokes_fgmres", L, R_MIN, R_MAX, bcc, bcs, S["restart"], S["maxit"], S["tol"], S["sweeps"],
+                     S["omega"], d], d)
+            out[f"stokes_fgmres_u_{bcc}{bcs}"] = np.fromfile(f"{d}/x_u.bin").reshape((3,) + fine.shape)
+            out[f"stokes_fgmres_p_{bcc}{bcs}"] = np.fromfile(f"{d}/x_p.bin").reshape(coarse.shape)
+            out[f"stokes_fgmres_hist_{bcc}{bcs}"] = np.fromfile(f"{d}/hist.bin")
 
         vb = vcycle_rhs()
         out["checksum_vcycle_b"] = checksum(vb)

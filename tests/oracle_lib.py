@@ -274,8 +274,8 @@ class Mesh:
                    for i in range(a.shape[0]))
 
 
-def fgmres(apply, dot, b, restart, max_iterations, relative_tolerance, absolute_tolerance=1e-30):
-    """FGMRES with the identity preconditioner from x = 0 (linalg/solvers/fgmres.hpp:100-330): modified
+def fgmres(apply, dot, b, restart, max_iterations, relative_tolerance, absolute_tolerance=1e-30, prec=None):
+    """FGMRES from x = 0 (linalg/solvers/fgmres.hpp:100-330): z_j = prec(v_j) (identity when None), modified
     Gram-Schmidt Arnoldi, Givens rotations, the breakdown and stagnation exits, restarts from the true
     residual.  Returns (x, relative residual history: 1 at the start, then one entry per iteration)."""
     eps = np.finfo(np.float64).eps
@@ -296,7 +296,7 @@ def fgmres(apply, dot, b, restart, max_iterations, relative_tolerance, absolute_
         g[0] = beta0
         inner, j = 0, 0
         while j < m and total < max_iterations:
-            Z.append(V[j].copy())
+            Z.append(V[j].copy() if prec is None else prec(V[j]))
             w = apply(Z[j])
             for i in range(j + 1):
                 H[i, j] = dot(w, V[i])
@@ -340,6 +340,47 @@ def fgmres(apply, dot, b, restart, max_iterations, relative_tolerance, absolute_
         if beta0 <= absolute_tolerance or beta0 / r0 <= relative_tolerance:
             break
     return x, hist
+
+
+def stokes_block_fgmres(fine, coarse, k, kp, b_u, b_p, bc_cmb, bc_surf, restart, max_iterations, tolerance,
+                        sweeps, omega):
+    """FGMRES on the Stokes block operator [A B^T; B 0] (epsilon_divdiv_stokes.hpp:55-90) with the
+    block-triangular preconditioner of the mantle-circulation app (block_preconditioner_2x2.hpp:205-217,
+    mantlecirculation.cpp:684-717): Schur block the inverse lumped KMass(1 / kp) on the pressure mesh, velocity
+    block `sweeps` damped Jacobi sweeps from zero with the kerngen diagonal.  From x = 0; returns
+    (u, p, relative residual history)."""
+    nu = 3 * fine.ns
+
+    def split(v):
+        return v[:nu].reshape((3,) + fine.shape), v[nu:].reshape(coarse.shape)
+
+    def join(u, p):
+        return np.concatenate([np.ravel(u), np.ravel(p)])
+
+    def apply(v):
+        u, p = split(v)
+        return join(fine.kerngen(k, u, bc_cmb, bc_surf) + fine.gradient(coarse, p, bc_cmb, bc_surf),
+                    fine.divergence(coarse, u, bc_cmb, bc_surf))
+
+    def dot(a, b):
+        (ua, pa), (ub, pb) = split(a), split(b)
+        return fine.dot(ua, ub) + coarse.dot(pa, pb)
+
+    inv_d = 1.0 / fine.kerngen(k, np.ones((3,) + fine.shape), bc_cmb, bc_surf, diag=True)
+    inv_m = 1.0 / coarse.kmass(1.0 / np.asarray(kp, dtype=np.float64), np.ones(coarse.shape), mode=2)
+
+    def prec(v):
+        b1, b2 = split(v)
+        x2 = b2 * inv_m
+        t1 = fine.gradient(coarse, x2, bc_cmb, bc_surf) + b1
+        x1 = np.zeros_like(b1)
+        for _ in range(sweeps):
+            x1 = x1 + omega * (inv_d * (t1 - fine.kerngen(k, x1, bc_cmb, bc_surf)))
+        return join(x1, -x2)
+
+    x, hist = fgmres(apply, dot, join(b_u, b_p), restart, max_iterations, tolerance, prec=prec)
+    u, p = split(x)
+    return u, p, hist
 
 
 def laplace_vcycles(meshes, b, omega, smooth, cycles, coarse_max_iterations):

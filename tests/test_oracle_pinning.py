@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from helpers import rel
-from oracle_lib import Mesh, fgmres, laplace_vcycles, ref_available, run_ref
+from oracle_lib import Mesh, fgmres, laplace_vcycles, ref_available, run_ref, stokes_block_fgmres
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 import make_golden as G  # noqa: E402
@@ -87,6 +87,20 @@ def test_fgmres_matches_reference(case):
     assert len(ho) == len(g["fgmres_hist"])
     np.testing.assert_allclose(ho, g["fgmres_hist"], rtol=1e-6, atol=1e-14)
     assert rel(xo, g["fgmres_x"]) <= TOL
+
+
+@pytest.mark.parametrize("bcc,bcs", G.STOKES_FGMRES["bcs"])
+def test_stokes_block_fgmres_matches_reference(case, bcc, bcs):
+    """The Stokes solve's composition (FGMRES, EpsDivDivStokes, the app's block-triangular preconditioner with
+    the lumped inverse KMass(1/eta) Schur block), with a deterministic Jacobi velocity block in place of the
+    multigrid: the same residual history and solution as the reference's own composition."""
+    g, fine, coarse, x = case
+    S = G.STOKES_FGMRES
+    u, p, hist = stokes_block_fgmres(fine, coarse, x["k"], G.pressure_viscosity(x), x["u"], x["p"], bcc, bcs,
+                                     S["restart"], S["maxit"], S["tol"], S["sweeps"], S["omega"])
+    np.testing.assert_allclose(hist, g[f"stokes_fgmres_hist_{bcc}{bcs}"], rtol=1e-10, atol=1e-16)
+    assert rel(u, g[f"stokes_fgmres_u_{bcc}{bcs}"]) <= TOL
+    assert rel(p, g[f"stokes_fgmres_p_{bcc}{bcs}"]) <= TOL
 
 
 def test_laplace_vcycles_match_reference(case):
