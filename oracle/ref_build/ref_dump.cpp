@@ -18,6 +18,7 @@
 //   divergence L rmin rmax bcc bcs DIR    Divergence<double>: fine velocity -> coarse pressure
 //   gradient   L rmin rmax bcc bcs DIR    Gradient<double>: coarse pressure -> fine velocity
 //   stokes     L rmin rmax bcc bcs DIR    EpsDivDivStokes<double>: (src_u, src_p) -> (dst_u, dst_p), k.bin
+//   laplace_minres L rmin rmax maxit reltol DIR  PMINRES on Laplace from x = 0 on b.bin: x.bin, hist.bin
 //   laplace_fgmres L rmin rmax restart maxit reltol DIR  FGMRES on Laplace from x = 0 on b.bin: x.bin, hist.bin
 //   stokes_fgmres L rmin rmax bcc bcs restart maxit tol sweeps omega DIR  FGMRES on EpsDivDivStokes with the
 //                                          block-triangular preconditioner (Jacobi velocity block, lumped
@@ -70,6 +71,7 @@
 #include "linalg/solvers/jacobi.hpp"
 #include "linalg/solvers/multigrid.hpp"
 #include "linalg/solvers/pcg.hpp"
+#include "linalg/solvers/pminres.hpp"
 #include "util/table.hpp"
 #include "grid/shell/bit_masks.hpp"
 #include "grid/shell/spherical_shell.hpp"
@@ -347,6 +349,33 @@ int cmd_vcycle( int Lmin, int Lmax, double rmin, double rmax, double omega, int 
     linalg::solvers::Multigrid< Lap, P, R, linalg::solvers::Jacobi< Lap >, linalg::solvers::PCG< Lap > > mg(
         Ps, Rs, Ac, tr, te, tmp, sm, sm, coarse, cycles, 0.0 );
     linalg::solvers::solve( mg, A, x, b );
+    auto out = view_to_host( x.grid_data() );
+    write_file( dir + "/x.bin", out.data(), out.size() );
+    return 0;
+}
+
+// PMINRES<Laplace<double>> (pminres.hpp:30-175, identity preconditioner, Dirichlet rows) from x = 0 on b.bin;
+// writes x.bin and hist.bin (the relative residual of every statistics row)
+int cmd_laplace_minres( int L, double rmin, double rmax, int maxit, double reltol, const std::string& dir )
+{
+    using V   = linalg::VectorQ1Scalar< double >;
+    using Lap = fe::wedge::operators::shell::Laplace< double >;
+    Setup s( L, rmin, rmax );
+    V     b( "b", s.domain, s.omask ), x( "x", s.domain, s.omask );
+    std::vector< V > tmps;
+    for ( int i = 0; i < 7; ++i )
+        tmps.emplace_back( "tmp" + std::to_string( i ), s.domain, s.omask );
+    view_from_host( b.grid_data(), read_file< double >( dir + "/b.bin", s.nodes ).data() );
+    linalg::assign( x, 0.0 );
+    Lap  A( s.domain, s.coords, s.radii, s.bmask, true, false );
+    auto table = std::make_shared< util::Table >();
+    linalg::solvers::PMINRES< Lap > mr( linalg::solvers::IterativeSolverParameters{ maxit, reltol, 1e-30 }, table,
+                                        tmps );
+    linalg::solvers::solve( mr, A, x, b );
+    std::vector< double > hist;
+    for ( const auto& row : table->rows() )
+        hist.push_back( std::get< double >( row.at( "relative_residual" ) ) );
+    write_file( dir + "/hist.bin", hist.data(), hist.size() );
     auto out = view_to_host( x.grid_data() );
     write_file( dir + "/x.bin", out.data(), out.size() );
     return 0;
@@ -681,6 +710,8 @@ int main( int argc, char** argv )
     if ( cmd == "stokes_fgmres" && argc == 13 )
         return cmd_stokes_fgmres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), I( 8 ), D( 9 ), I( 10 ), D( 11 ),
                                   argv[12] );
+    if ( cmd == "laplace_minres" && argc == 8 )
+        return cmd_laplace_minres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), D( 6 ), argv[7] );
     if ( cmd == "laplace_fgmres" && argc == 9 )
         return cmd_laplace_fgmres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), D( 7 ), argv[8] );
     if ( cmd == "vcycle" && argc == 11 )

@@ -80,6 +80,9 @@ def cg_rhs(s):
     return b
 
 
+# PMINRES on the Laplace (the CG right-hand side), at most 60 iterations, 1e-10
+MINRES_CASE = dict(maxit=60, tol=1e-10)
+
 # FGMRES(10) on the Laplace (the CG right-hand side), at most 60 iterations, 1e-10
 FGMRES_CASE = dict(restart=10, maxit=60, tol=1e-10)
 
@@ -148,6 +151,9 @@ def main():
             out[f"stokes_p_{bcc}{bcs}"] = np.fromfile(f"{d}/dst_p.bin").reshape(coarse.shape)
 
         cg_rhs(x["s"]).tofile(f"{d}/b.bin")
+        run_ref(["laplace_minres", L, R_MIN, R_MAX, MINRES_CASE["maxit"], MINRES_CASE["tol"], d], d)
+        out["minres_x"] = np.fromfile(f"{d}/x.bin").reshape(fine.shape)
+        out["minres_hist"] = np.fromfile(f"{d}/hist.bin")
         F = FGMRES_CASE
         run_ref(["laplace_fgmres", L, R_MIN, R_MAX, F["restart"], F["maxit"], F["tol"], d], d)
         out["fgmres_x"] = np.fromfile(f"{d}/x.bin").reshape(fine.shape)

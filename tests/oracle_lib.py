@@ -342,6 +342,49 @@ def fgmres(apply, dot, b, restart, max_iterations, relative_tolerance, absolute_
     return x, hist
 
 
+def pminres(apply, dot, b, max_iterations, relative_tolerance, absolute_tolerance=1e-30, prec=None):
+    """Preconditioned MINRES from x = 0 (linalg/solvers/pminres.hpp:30-175; prec None = identity), with the
+    reference's three-term updates of v and w and its stopping on |eta|.  Returns (x, relative residual
+    history: 1 at the start, then one entry per iteration)."""
+    P = (lambda v: v.copy()) if prec is None else prec
+    b = np.asarray(b, dtype=np.float64)
+    x = np.zeros_like(b)
+    v_prev, w, w_prev = np.zeros_like(b), np.zeros_like(b), np.zeros_like(b)
+    v = b - apply(x)
+    z = P(v)
+    g_prev, g = 1.0, np.sqrt(dot(z, v))
+    eta = g
+    s_prev = s = 0.0
+    c_prev = c = 1.0
+    r0 = g
+    hist = [1.0]
+    if r0 < absolute_tolerance:
+        return x, hist
+    for _ in range(max_iterations):
+        z = z * (1.0 / g)
+        az = apply(z)
+        delta = dot(az, z)
+        v_prev, v = v, 1.0 * az + (-delta / g) * v + (-g / g_prev) * v_prev
+        z_next = P(v)
+        g_next = np.sqrt(dot(z_next, v))
+        a0 = c * delta - c_prev * s * g
+        a1 = np.sqrt(a0 * a0 + g_next * g_next)
+        a2 = s * delta + c_prev * c * g
+        a3 = s_prev * g
+        c_next, s_next = a0 / a1, g_next / a1
+        w_prev, w = w, (1.0 / a1) * z + (-a3 / a1) * w_prev + (-a2 / a1) * w
+        x = x + (c_next * eta) * w
+        eta = -s_next * eta
+        hist.append(abs(eta) / r0)
+        if hist[-1] <= relative_tolerance or abs(eta) < absolute_tolerance:
+            break
+        z = z_next
+        g_prev, g = g, g_next
+        c_prev, c = c, c_next
+        s_prev, s = s, s_next
+    return x, hist
+
+
 def stokes_block_fgmres(fine, coarse, k, kp, b_u, b_p, bc_cmb, bc_surf, restart, max_iterations, tolerance,
                         sweeps, omega):
     """FGMRES on the Stokes block operator [A B^T; B 0] (epsilon_divdiv_stokes.hpp:55-90) with the

@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from helpers import rel
-from oracle_lib import Mesh, fgmres, laplace_vcycles, ref_available, run_ref, stokes_block_fgmres
+from oracle_lib import Mesh, fgmres, laplace_vcycles, pminres, ref_available, run_ref, stokes_block_fgmres
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 import make_golden as G  # noqa: E402
@@ -74,6 +74,17 @@ def test_stokes_operator_matches_reference(case, bcc, bcs):
     p = fine.divergence(coarse, x["u"], bcc, bcs)
     assert rel(u, g[f"stokes_u_{bcc}{bcs}"]) <= TOL
     assert rel(p, g[f"stokes_p_{bcc}{bcs}"]) <= TOL
+
+
+def test_pminres_matches_reference(case):
+    """PMINRES (pminres.hpp:30-175) on the Dirichlet Laplace from x = 0: the same iterations and solution as the
+    reference's; residual estimates to 1e-6 relative above 1e-14 (amplified rounding)."""
+    g, fine, _, x = case
+    M = G.MINRES_CASE
+    xo, ho = pminres(lambda v: fine.laplace(v, True, False), fine.dot, G.cg_rhs(x["s"]), M["maxit"], M["tol"])
+    assert len(ho) == len(g["minres_hist"])
+    np.testing.assert_allclose(ho, g["minres_hist"], rtol=1e-6, atol=1e-14)
+    assert rel(xo, g["minres_x"]) <= TOL
 
 
 def test_fgmres_matches_reference(case):
