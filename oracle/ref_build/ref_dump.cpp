@@ -23,6 +23,8 @@
 //   stokes_fgmres L rmin rmax bcc bcs restart maxit tol sweeps omega DIR  FGMRES on EpsDivDivStokes with the
 //                                          block-triangular preconditioner (Jacobi velocity block, lumped
 //                                          KMass(1/kp) Schur block): x_u.bin, x_p.bin, hist.bin
+//   stokes_minres L rmin rmax bcc bcs maxit tol sweeps omega DIR  PMINRES on EpsDivDivStokes with the
+//                                          block-diagonal preconditioner (same blocks): x_u, x_p, hist
 //   vcycle Lmin Lmax rmin rmax omega smooth cycles cmaxit DIR  Laplace multigrid (Jacobi, constant
 //                                          transfers, coarse PCG) from x = 0 on b.bin, writes x.bin
 //   prolong / restrict Lf rmin rmax DIR    constant vector transfer between Lf-1 and Lf
@@ -471,6 +473,61 @@ int cmd_stokes_fgmres( int L, double rmin, double rmax, int bcc, int bcs, int re
     return 0;
 }
 
+// PMINRES on EpsDivDivStokes with the block-diagonal preconditioner (block_preconditioner_2x2.hpp:38-100):
+// velocity block `sweeps` damped Jacobi sweeps with the kerngen diagonal, pressure block the inverse lumped
+// KMass(1 / kp); b = (src_u, src_p), x = 0; writes x_u.bin, x_p.bin, hist.bin
+int cmd_stokes_minres( int L, double rmin, double rmax, int bcc, int bcs, int maxit, double tol, int sweeps,
+                       double omega, const std::string& dir )
+{
+    using Stokes  = fe::wedge::operators::shell::EpsDivDivStokes< double >;
+    using Viscous = Stokes::Block11Type;
+    using PMass   = fe::wedge::operators::shell::KMass< double >;
+    using BV      = linalg::VectorQ1IsoQ2Q1< double >;
+    using PrecV   = linalg::solvers::Jacobi< Viscous >;
+    using PrecS   = linalg::solvers::DiagonalSolver< PMass >;
+    using Prec    = linalg::solvers::BlockDiagonalPreconditioner2x2< Stokes, Viscous, PMass, PrecV, PrecS >;
+    Setup f( L, rmin, rmax ), c( L - 1, rmin, rmax );
+    BoundaryConditions b = { { ShellBoundaryFlag::CMB, bc_of( bcc ) }, { ShellBoundaryFlag::SURFACE, bc_of( bcs ) } };
+    linalg::VectorQ1Scalar< double > k( "k", f.domain, f.omask ), kp( "kp", c.domain, c.omask );
+    view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", f.nodes ).data() );
+    view_from_host( kp.grid_data(), read_file< double >( dir + "/kp.bin", c.nodes ).data() );
+    linalg::invert_entries( kp );
+    Stokes K( f.domain, c.domain, f.coords, f.radii, f.bmask, k.grid_data(), b, false );
+    linalg::VectorQ1Vec< double > ones( "ones", f.domain, f.omask ), inv( "inv", f.domain, f.omask ),
+        jt( "jt", f.domain, f.omask );
+    Viscous Kd( f.domain, f.coords, f.radii, f.bmask, k.grid_data(), b, true );
+    linalg::assign( ones, 1.0 );
+    linalg::apply( Kd, ones, inv );
+    linalg::invert_entries( inv );
+    PrecV pv( inv, sweeps, jt, omega );
+    PMass pmass( c.domain, c.coords, c.radii, kp.grid_data(), false );
+    pmass.set_lumped_diagonal( true );
+    linalg::VectorQ1Scalar< double > lumped( "lumped", c.domain, c.omask ), t1( "t1", c.domain, c.omask );
+    linalg::assign( t1, 1.0 );
+    linalg::apply( pmass, t1, lumped );
+    PrecS ps( lumped );
+    Prec  prec( K.block_11(), pmass, pv, ps );
+    std::vector< BV > tmps;
+    for ( int i = 0; i < 7; ++i )
+        tmps.emplace_back( "tmp" + std::to_string( i ), f.domain, c.domain, f.omask, c.omask );
+    BV rhs( "rhs", f.domain, c.domain, f.omask, c.omask ), x( "x", f.domain, c.domain, f.omask, c.omask );
+    load_vec( rhs.block_1(), dir + "/src_u.bin", f.nodes );
+    view_from_host( rhs.block_2().grid_data(), read_file< double >( dir + "/src_p.bin", c.nodes ).data() );
+    linalg::assign( x, 0.0 );
+    auto table = std::make_shared< util::Table >();
+    linalg::solvers::PMINRES< Stokes, Prec > mr( linalg::solvers::IterativeSolverParameters{ maxit, tol, 1e-30 },
+                                                 table, tmps, prec );
+    linalg::solvers::solve( mr, K, x, rhs );
+    std::vector< double > hist;
+    for ( const auto& row : table->rows() )
+        hist.push_back( std::get< double >( row.at( "relative_residual" ) ) );
+    write_file( dir + "/hist.bin", hist.data(), hist.size() );
+    save_vec( x.block_1(), dir + "/x_u.bin", f.nodes );
+    auto xp = view_to_host( x.block_2().grid_data() );
+    write_file( dir + "/x_p.bin", xp.data(), xp.size() );
+    return 0;
+}
+
 // EpsDivDivStokes<double> (epsilon_divdiv_stokes.hpp:55-90): [A B^T; B 0] applied to (u, p), A the
 // kerngen operator with k.bin on level L, p on level L-1
 int cmd_stokes_op( int L, double rmin, double rmax, int bcc, int bcs, const std::string& dir )
@@ -707,6 +764,8 @@ int main( int argc, char** argv )
         return cmd_stokes_block( cmd == "divergence", I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     if ( ( cmd == "prolong" || cmd == "restrict" ) && argc == 6 )
         return cmd_transfer( cmd == "prolong", I( 2 ), D( 3 ), D( 4 ), argv[5] );
+    if ( cmd == "stokes_minres" && argc == 12 )
+        return cmd_stokes_minres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), D( 8 ), I( 9 ), D( 10 ), argv[11] );
     if ( cmd == "stokes_fgmres" && argc == 13 )
         return cmd_stokes_fgmres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), I( 8 ), D( 9 ), I( 10 ), D( 11 ),
                                   argv[12] );

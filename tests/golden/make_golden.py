@@ -91,6 +91,11 @@ FGMRES_CASE = dict(restart=10, maxit=60, tol=1e-10)
 STOKES_FGMRES = dict(restart=10, maxit=30, tol=1e-8, sweeps=2, omega=0.5, bcs=[(2, 2), (1, 1)])
 
 
+# PMINRES on the Stokes block operator with the block-diagonal preconditioner (1 Jacobi sweep, damping 0.5:
+# a symmetric positive diagonal velocity block), 40 iterations
+STOKES_MINRES = dict(maxit=40, tol=1e-8, sweeps=1, omega=0.5, bcs=[(1, 1), (2, 2)])
+
+
 def pressure_viscosity(x):
     return np.exp(0.3 * x["pc"])
 
@@ -170,6 +175,13 @@ def main():
             out[f"stokes_fgmres_u_{bcc}{bcs}"] = np.fromfile(f"{d}/x_u.bin").reshape((3,) + fine.shape)
             out[f"stokes_fgmres_p_{bcc}{bcs}"] = np.fromfile(f"{d}/x_p.bin").reshape(coarse.shape)
             out[f"stokes_fgmres_hist_{bcc}{bcs}"] = np.fromfile(f"{d}/hist.bin")
+
+        S = STOKES_MINRES
+        for bcc, bcs in S["bcs"]:
+            run_ref(["stokes_minres", L, R_MIN, R_MAX, bcc, bcs, S["maxit"], S["tol"], S["sweeps"], S["omega"], d], d)
+            out[f"stokes_minres_u_{bcc}{bcs}"] = np.fromfile(f"{d}/x_u.bin").reshape((3,) + fine.shape)
+            out[f"stokes_minres_p_{bcc}{bcs}"] = np.fromfile(f"{d}/x_p.bin").reshape(coarse.shape)
+            out[f"stokes_minres_hist_{bcc}{bcs}"] = np.fromfile(f"{d}/hist.bin")
 
         vb = vcycle_rhs()
         out["checksum_vcycle_b"] = checksum(vb)

@@ -385,44 +385,68 @@ def pminres(apply, dot, b, max_iterations, relative_tolerance, absolute_toleranc
     return x, hist
 
 
-def stokes_block_fgmres(fine, coarse, k, kp, b_u, b_p, bc_cmb, bc_surf, restart, max_iterations, tolerance,
-                        sweeps, omega):
-    """FGMRES on the Stokes block operator [A B^T; B 0] (epsilon_divdiv_stokes.hpp:55-90) with the
-    block-triangular preconditioner of the mantle-circulation app (block_preconditioner_2x2.hpp:205-217,
-    mantlecirculation.cpp:684-717): Schur block the inverse lumped KMass(1 / kp) on the pressure mesh, velocity
-    block `sweeps` damped Jacobi sweeps from zero with the kerngen diagonal.  From x = 0; returns
-    (u, p, relative residual history)."""
-    nu = 3 * fine.ns
+class _StokesParts:
+    """The Stokes block operator [A B^T; B 0] (epsilon_divdiv_stokes.hpp:55-90) on flattened (u, p) vectors, its
+    owned-masked dot, and the app's preconditioner blocks (mantlecirculation.cpp:684-717): the inverse lumped
+    KMass(1 / kp) on the pressure mesh and `sweeps` damped Jacobi sweeps from zero with the kerngen diagonal."""
 
-    def split(v):
-        return v[:nu].reshape((3,) + fine.shape), v[nu:].reshape(coarse.shape)
+    def __init__(self, fine, coarse, k, kp, bc_cmb, bc_surf, sweeps, omega):
+        self.fine, self.coarse, self.k, self.bc = fine, coarse, k, (bc_cmb, bc_surf)
+        self.nu, self.sweeps, self.omega = 3 * fine.ns, sweeps, omega
+        self.inv_d = 1.0 / fine.kerngen(k, np.ones((3,) + fine.shape), bc_cmb, bc_surf, diag=True)
+        self.inv_m = 1.0 / coarse.kmass(1.0 / np.asarray(kp, dtype=np.float64), np.ones(coarse.shape), mode=2)
 
+    def split(self, v):
+        return v[:self.nu].reshape((3,) + self.fine.shape), v[self.nu:].reshape(self.coarse.shape)
+
+    @staticmethod
     def join(u, p):
         return np.concatenate([np.ravel(u), np.ravel(p)])
 
-    def apply(v):
-        u, p = split(v)
-        return join(fine.kerngen(k, u, bc_cmb, bc_surf) + fine.gradient(coarse, p, bc_cmb, bc_surf),
-                    fine.divergence(coarse, u, bc_cmb, bc_surf))
+    def apply(self, v):
+        u, p = self.split(v)
+        f, c = self.fine, self.coarse
+        return self.join(f.kerngen(self.k, u, *self.bc) + f.gradient(c, p, *self.bc), f.divergence(c, u, *self.bc))
 
-    def dot(a, b):
-        (ua, pa), (ub, pb) = split(a), split(b)
-        return fine.dot(ua, ub) + coarse.dot(pa, pb)
+    def dot(self, a, b):
+        (ua, pa), (ub, pb) = self.split(a), self.split(b)
+        return self.fine.dot(ua, ub) + self.coarse.dot(pa, pb)
 
-    inv_d = 1.0 / fine.kerngen(k, np.ones((3,) + fine.shape), bc_cmb, bc_surf, diag=True)
-    inv_m = 1.0 / coarse.kmass(1.0 / np.asarray(kp, dtype=np.float64), np.ones(coarse.shape), mode=2)
+    def jacobi(self, rhs):
+        x1 = np.zeros_like(rhs)
+        for _ in range(self.sweeps):
+            x1 = x1 + self.omega * (self.inv_d * (rhs - self.fine.kerngen(self.k, x1, *self.bc)))
+        return x1
 
-    def prec(v):
-        b1, b2 = split(v)
-        x2 = b2 * inv_m
-        t1 = fine.gradient(coarse, x2, bc_cmb, bc_surf) + b1
-        x1 = np.zeros_like(b1)
-        for _ in range(sweeps):
-            x1 = x1 + omega * (inv_d * (t1 - fine.kerngen(k, x1, bc_cmb, bc_surf)))
-        return join(x1, -x2)
+    def triangular(self, v):
+        """block_preconditioner_2x2.hpp:205-217: x_2 = P22 b_2, x_1 = P11 (b_1 + B^T x_2), x_2 = -x_2"""
+        b1, b2 = self.split(v)
+        x2 = b2 * self.inv_m
+        t1 = self.fine.gradient(self.coarse, x2, *self.bc) + b1
+        return self.join(self.jacobi(t1), -x2)
 
-    x, hist = fgmres(apply, dot, join(b_u, b_p), restart, max_iterations, tolerance, prec=prec)
-    u, p = split(x)
+    def diagonal(self, v):
+        """block_preconditioner_2x2.hpp:38-100: x_1 = P11 b_1, x_2 = P22 b_2"""
+        b1, b2 = self.split(v)
+        return self.join(self.jacobi(b1), b2 * self.inv_m)
+
+
+def stokes_block_fgmres(fine, coarse, k, kp, b_u, b_p, bc_cmb, bc_surf, restart, max_iterations, tolerance,
+                        sweeps, omega):
+    """FGMRES on the Stokes block operator with the app's block-triangular preconditioner (Jacobi velocity
+    block, see _StokesParts), from x = 0; returns (u, p, relative residual history)."""
+    S = _StokesParts(fine, coarse, k, kp, bc_cmb, bc_surf, sweeps, omega)
+    x, hist = fgmres(S.apply, S.dot, S.join(b_u, b_p), restart, max_iterations, tolerance, prec=S.triangular)
+    u, p = S.split(x)
+    return u, p, hist
+
+
+def stokes_block_minres(fine, coarse, k, kp, b_u, b_p, bc_cmb, bc_surf, max_iterations, tolerance, sweeps, omega):
+    """PMINRES on the Stokes block operator with the block-diagonal preconditioner (same blocks), from x = 0;
+    returns (u, p, relative residual history)."""
+    S = _StokesParts(fine, coarse, k, kp, bc_cmb, bc_surf, sweeps, omega)
+    x, hist = pminres(S.apply, S.dot, S.join(b_u, b_p), max_iterations, tolerance, prec=S.diagonal)
+    u, p = S.split(x)
     return u, p, hist
 
 

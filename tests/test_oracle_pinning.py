@@ -15,7 +15,8 @@ import numpy as np
 import pytest
 
 from helpers import rel
-from oracle_lib import Mesh, fgmres, laplace_vcycles, pminres, ref_available, run_ref, stokes_block_fgmres
+from oracle_lib import (Mesh, fgmres, laplace_vcycles, pminres, ref_available, run_ref, stokes_block_fgmres,
+                        stokes_block_minres)
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 import make_golden as G  # noqa: E402
@@ -112,6 +113,19 @@ def test_stokes_block_fgmres_matches_reference(case, bcc, bcs):
     np.testing.assert_allclose(hist, g[f"stokes_fgmres_hist_{bcc}{bcs}"], rtol=1e-10, atol=1e-16)
     assert rel(u, g[f"stokes_fgmres_u_{bcc}{bcs}"]) <= TOL
     assert rel(p, g[f"stokes_fgmres_p_{bcc}{bcs}"]) <= TOL
+
+
+@pytest.mark.parametrize("bcc,bcs", G.STOKES_MINRES["bcs"])
+def test_stokes_block_minres_matches_reference(case, bcc, bcs):
+    """PMINRES on the Stokes block operator with the block-diagonal preconditioner (block_preconditioner_2x2.hpp:
+    38-100; the Stokes solver's outer = 1): the same history and solution as the reference's composition."""
+    g, fine, coarse, x = case
+    S = G.STOKES_MINRES
+    u, p, hist = stokes_block_minres(fine, coarse, x["k"], G.pressure_viscosity(x), x["u"], x["p"], bcc, bcs,
+                                     S["maxit"], S["tol"], S["sweeps"], S["omega"])
+    np.testing.assert_allclose(hist, g[f"stokes_minres_hist_{bcc}{bcs}"], rtol=1e-10, atol=1e-16)
+    assert rel(u, g[f"stokes_minres_u_{bcc}{bcs}"]) <= TOL
+    assert rel(p, g[f"stokes_minres_p_{bcc}{bcs}"]) <= TOL
 
 
 def test_laplace_vcycles_match_reference(case):
