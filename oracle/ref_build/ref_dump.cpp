@@ -19,6 +19,8 @@
 //   gradient   L rmin rmax bcc bcs DIR    Gradient<double>: coarse pressure -> fine velocity
 //   stokes     L rmin rmax bcc bcs DIR    EpsDivDivStokes<double>: (src_u, src_p) -> (dst_u, dst_p), k.bin
 //   laplace_minres L rmin rmax maxit reltol DIR  PMINRES on Laplace from x = 0 on b.bin: x.bin, hist.bin
+//   laplace_chebyshev L rmin rmax order iters pits DIR  Chebyshev smoother from x = 0 on b.bin (run on one
+//                                          thread): x.bin, prints the eigenvalue estimate it used
 //   laplace_fgmres L rmin rmax restart maxit reltol DIR  FGMRES on Laplace from x = 0 on b.bin: x.bin, hist.bin
 //   stokes_fgmres L rmin rmax bcc bcs restart maxit tol sweeps omega DIR  FGMRES on EpsDivDivStokes with the
 //                                          block-triangular preconditioner (Jacobi velocity block, lumped
@@ -68,6 +70,8 @@
 #include "grid/bit_masks.hpp"
 #include "linalg/solvers/gca/gca.hpp"
 #include "linalg/solvers/block_preconditioner_2x2.hpp"
+#include "linalg/solvers/chebyshev.hpp"
+#include "linalg/solvers/power_iteration.hpp"
 #include "linalg/solvers/diagonal_solver.hpp"
 #include "linalg/solvers/fgmres.hpp"
 #include "linalg/solvers/jacobi.hpp"
@@ -353,6 +357,38 @@ int cmd_vcycle( int Lmin, int Lmax, double rmin, double rmax, double omega, int 
     linalg::solvers::solve( mg, A, x, b );
     auto out = view_to_host( x.grid_data() );
     write_file( dir + "/x.bin", out.data(), out.size() );
+    return 0;
+}
+
+// Chebyshev<Laplace<double>> smoother (chebyshev.hpp:100-175, Dirichlet rows, inverse diagonal) applied
+// from x = 0 to b.bin: `iters` sweeps of order `order`, the eigenvalue estimate from `pits` power
+// iterations.  The estimate starts from randomize(), a generator pool with a fixed seed created per call:
+// deterministic on one thread (run with OMP_NUM_THREADS=1).  The same estimate is computed here once more
+// (same operator, same start) and printed, so the smoother after it can be checked.  Writes x.bin; prints
+// {"lambda": ...}
+int cmd_laplace_chebyshev( int L, double rmin, double rmax, int order, int iters, int pits, const std::string& dir )
+{
+    using V   = linalg::VectorQ1Scalar< double >;
+    using Lap = fe::wedge::operators::shell::Laplace< double >;
+    Setup s( L, rmin, rmax );
+    V     b( "b", s.domain, s.omask ), x( "x", s.domain, s.omask ), inv( "inv", s.domain, s.omask ),
+        ones( "ones", s.domain, s.omask ), t0( "t0", s.domain, s.omask ), t1( "t1", s.domain, s.omask );
+    view_from_host( b.grid_data(), read_file< double >( dir + "/b.bin", s.nodes ).data() );
+    Lap A( s.domain, s.coords, s.radii, s.bmask, true, false ), Ad( s.domain, s.coords, s.radii, s.bmask, true, true );
+    linalg::assign( ones, 1.0 );
+    linalg::apply( Ad, ones, inv );
+    linalg::invert_entries( inv );
+    linalg::DiagonallyScaledOperator< Lap > scaled( A, inv );
+    const double lambda = linalg::solvers::power_iteration( scaled, t0, t1, pits );
+    std::vector< V > tmps;
+    for ( int i = 0; i < 2; ++i )
+        tmps.emplace_back( "tmp" + std::to_string( i ), s.domain, s.omask );
+    linalg::solvers::Chebyshev< Lap > cheb( order, inv, tmps, iters, pits );
+    linalg::assign( x, 0.0 );
+    linalg::solvers::solve( cheb, A, x, b );
+    auto out = view_to_host( x.grid_data() );
+    write_file( dir + "/x.bin", out.data(), out.size() );
+    std::printf( "{\"lambda\": %.17g}\n", lambda );
     return 0;
 }
 
@@ -769,6 +805,8 @@ int main( int argc, char** argv )
     if ( cmd == "stokes_fgmres" && argc == 13 )
         return cmd_stokes_fgmres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), I( 8 ), D( 9 ), I( 10 ), D( 11 ),
                                   argv[12] );
+    if ( cmd == "laplace_chebyshev" && argc == 9 )
+        return cmd_laplace_chebyshev( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( cmd == "laplace_minres" && argc == 8 )
         return cmd_laplace_minres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), D( 6 ), argv[7] );
     if ( cmd == "laplace_fgmres" && argc == 9 )

@@ -385,6 +385,29 @@ def pminres(apply, dot, b, max_iterations, relative_tolerance, absolute_toleranc
     return x, hist
 
 
+def chebyshev_smoother(apply, inv_diag, b, x, order, iterations, lambda_estimate):
+    """Chebyshev smoothing (linalg/solvers/chebyshev.hpp:100-160) of A x = b with the inverse diagonal, given the
+    power-iteration estimate of the largest eigenvalue of D^-1 A: bounds [0.1, 1.5] x estimate; rho is set once
+    and carried across the sweeps, as in the reference.  Returns the updated x."""
+    lmax, lmin = 1.5 * lambda_estimate, 0.1 * lambda_estimate
+    theta, delta = 0.5 * (lmax + lmin), 0.5 * (lmax - lmin)
+    sigma = theta / delta
+    rho = 1.0 / sigma
+    x = np.array(x, dtype=np.float64)
+    for _ in range(iterations):
+        z = (b - apply(x)) * inv_diag
+        d = (1.0 / theta) * z
+        x = x + d
+        for _ in range(2, order + 1):
+            rho_new = 1.0 / (2.0 * sigma - rho)
+            beta, alpha = rho_new * rho, 2.0 * rho_new / delta
+            z = (b - apply(x)) * inv_diag
+            d = alpha * z + beta * d
+            x = x + d
+            rho = rho_new
+    return x
+
+
 class _StokesParts:
     """The Stokes block operator [A B^T; B 0] (epsilon_divdiv_stokes.hpp:55-90) on flattened (u, p) vectors, its
     owned-masked dot, and the app's preconditioner blocks (mantlecirculation.cpp:684-717): the inverse lumped

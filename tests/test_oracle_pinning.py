@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from helpers import rel
-from oracle_lib import (Mesh, fgmres, laplace_vcycles, pminres, ref_available, run_ref, stokes_block_fgmres,
+from oracle_lib import (Mesh, chebyshev_smoother, fgmres, laplace_vcycles, pminres, ref_available, run_ref, stokes_block_fgmres,
                         stokes_block_minres)
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
@@ -75,6 +75,18 @@ def test_stokes_operator_matches_reference(case, bcc, bcs):
     p = fine.divergence(coarse, x["u"], bcc, bcs)
     assert rel(u, g[f"stokes_u_{bcc}{bcs}"]) <= TOL
     assert rel(p, g[f"stokes_p_{bcc}{bcs}"]) <= TOL
+
+
+def test_chebyshev_smoother_matches_reference(case):
+    """Chebyshev smoothing (chebyshev.hpp:100-160; order 3, 2 sweeps, rho carried across sweeps) from x = 0 with
+    the eigenvalue estimate the reference's smoother computed (its power iteration starts from a seeded
+    random vector, reproducible on one thread): the same iterate."""
+    g, fine, _, x = case
+    C = G.CHEBYSHEV_CASE
+    inv = 1.0 / fine.laplace(np.ones(fine.shape), True, True)
+    xo = chebyshev_smoother(lambda v: fine.laplace(v, True, False), inv, G.cg_rhs(x["s"]), np.zeros(fine.shape),
+                            C["order"], C["iters"], float(g["chebyshev_lambda"]))
+    assert rel(xo, g["chebyshev_x"]) <= TOL
 
 
 def test_pminres_matches_reference(case):
