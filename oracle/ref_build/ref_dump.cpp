@@ -19,6 +19,8 @@
 //   gradient   L rmin rmax bcc bcs DIR    Gradient<double>: coarse pressure -> fine velocity
 //   stokes     L rmin rmax bcc bcs DIR    EpsDivDivStokes<double>: (src_u, src_p) -> (dst_u, dst_p), k.bin
 //   laplace_minres L rmin rmax maxit reltol DIR  PMINRES on Laplace from x = 0 on b.bin: x.bin, hist.bin
+//   laplace_bicgstab L rmin rmax l maxit reltol DIR  PBiCGStab(l) on Laplace from x = 0 on b.bin: x.bin,
+//                                          hist.bin, rshadow.bin (its random shadow residual)
 //   laplace_chebyshev L rmin rmax order iters pits DIR  Chebyshev smoother from x = 0 on b.bin (run on one
 //                                          thread): x.bin, prints the eigenvalue estimate it used
 //   laplace_fgmres L rmin rmax restart maxit reltol DIR  FGMRES on Laplace from x = 0 on b.bin: x.bin, hist.bin
@@ -76,6 +78,7 @@
 #include "linalg/solvers/fgmres.hpp"
 #include "linalg/solvers/jacobi.hpp"
 #include "linalg/solvers/multigrid.hpp"
+#include "linalg/solvers/pbicgstab.hpp"
 #include "linalg/solvers/pcg.hpp"
 #include "linalg/solvers/pminres.hpp"
 #include "util/table.hpp"
@@ -389,6 +392,36 @@ int cmd_laplace_chebyshev( int L, double rmin, double rmax, int order, int iters
     auto out = view_to_host( x.grid_data() );
     write_file( dir + "/x.bin", out.data(), out.size() );
     std::printf( "{\"lambda\": %.17g}\n", lambda );
+    return 0;
+}
+
+// PBiCGStab(l)<Laplace<double>> (pbicgstab.hpp:29-290, identity preconditioner, Dirichlet rows) from x = 0 on
+// b.bin; writes x.bin, hist.bin (the relative residual of every statistics row) and rshadow.bin, the shadow
+// residual the solver drew with randomize() (it keeps it in its first workspace vector, unchanged)
+int cmd_laplace_bicgstab( int L, double rmin, double rmax, int l, int maxit, double reltol, const std::string& dir )
+{
+    using V   = linalg::VectorQ1Scalar< double >;
+    using Lap = fe::wedge::operators::shell::Laplace< double >;
+    Setup s( L, rmin, rmax );
+    V     b( "b", s.domain, s.omask ), x( "x", s.domain, s.omask );
+    std::vector< V > tmps;
+    for ( int i = 0; i < 2 * ( l + 1 ) + 2; ++i )
+        tmps.emplace_back( "tmp" + std::to_string( i ), s.domain, s.omask );
+    view_from_host( b.grid_data(), read_file< double >( dir + "/b.bin", s.nodes ).data() );
+    linalg::assign( x, 0.0 );
+    Lap  A( s.domain, s.coords, s.radii, s.bmask, true, false );
+    auto table = std::make_shared< util::Table >();
+    linalg::solvers::PBiCGStab< Lap > bi( l, linalg::solvers::IterativeSolverParameters{ maxit, reltol, 1e-30 },
+                                          table, tmps );
+    linalg::solvers::solve( bi, A, x, b );
+    std::vector< double > hist;
+    for ( const auto& row : table->rows() )
+        hist.push_back( std::get< double >( row.at( "relative_residual" ) ) );
+    write_file( dir + "/hist.bin", hist.data(), hist.size() );
+    auto out = view_to_host( x.grid_data() );
+    write_file( dir + "/x.bin", out.data(), out.size() );
+    auto rsh = view_to_host( tmps[0].grid_data() );
+    write_file( dir + "/rshadow.bin", rsh.data(), rsh.size() );
     return 0;
 }
 
@@ -807,6 +840,8 @@ int main( int argc, char** argv )
                                   argv[12] );
     if ( cmd == "laplace_chebyshev" && argc == 9 )
         return cmd_laplace_chebyshev( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
+    if ( cmd == "laplace_bicgstab" && argc == 9 )
+        return cmd_laplace_bicgstab( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), D( 7 ), argv[8] );
     if ( cmd == "laplace_minres" && argc == 8 )
         return cmd_laplace_minres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), D( 6 ), argv[7] );
     if ( cmd == "laplace_fgmres" && argc == 9 )

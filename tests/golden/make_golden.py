@@ -84,6 +84,10 @@ def cg_rhs(s):
 # one thread, where the reference's randomised eigenvalue start is reproducible
 CHEBYSHEV_CASE = dict(order=3, iters=2, pits=50)
 
+# PBiCGStab(2) on the Laplace (the CG right-hand side), at most 40 iterations, 1e-10; the fixture keeps the
+# shadow residual the reference drew
+BICGSTAB_CASE = dict(l=2, maxit=40, tol=1e-10)
+
 # PMINRES on the Laplace (the CG right-hand side), at most 60 iterations, 1e-10
 MINRES_CASE = dict(maxit=60, tol=1e-10)
 
@@ -165,6 +169,11 @@ def main():
                        json_out=True)
         out["chebyshev_x"] = np.fromfile(f"{d}/x.bin").reshape(fine.shape)
         out["chebyshev_lambda"] = np.array(info["lambda"])
+        B = BICGSTAB_CASE
+        run_ref(["laplace_bicgstab", L, R_MIN, R_MAX, B["l"], B["maxit"], B["tol"], d], d)
+        out["bicgstab_x"] = np.fromfile(f"{d}/x.bin").reshape(fine.shape)
+        out["bicgstab_hist"] = np.fromfile(f"{d}/hist.bin")
+        out["bicgstab_rshadow"] = np.fromfile(f"{d}/rshadow.bin").reshape(fine.shape)
         run_ref(["laplace_minres", L, R_MIN, R_MAX, MINRES_CASE["maxit"], MINRES_CASE["tol"], d], d)
         out["minres_x"] = np.fromfile(f"{d}/x.bin").reshape(fine.shape)
         out["minres_hist"] = np.fromfile(f"{d}/hist.bin")

@@ -385,6 +385,55 @@ def pminres(apply, dot, b, max_iterations, relative_tolerance, absolute_toleranc
     return x, hist
 
 
+def pbicgstab(apply, dot, b, l, max_iterations, relative_tolerance, r_shadow, absolute_tolerance=1e-30):
+    """PBiCGStab(l) with the identity preconditioner from x = 0 (linalg/solvers/pbicgstab.hpp:98-260): l BiCG
+    steps, then the minimal-residual correction with gamma = M^-1 M0 (M_ij = <r_i+1, r_j+1>, M0_j = <r_0, r_j+1>),
+    the reference's updates u_0 -= sum gamma_j-1 u_j, x += sum gamma_j r_j, r_0 -= sum gamma_j-1 r_j and
+    omega = gamma_l-1; the shadow residual is given (the reference draws it with randomize).  Returns
+    (x, history: the relative residual of every statistics row, the final row repeated)."""
+    b = np.asarray(b, dtype=np.float64)
+    x = np.zeros_like(b)
+    us = [np.zeros_like(b) for _ in range(l + 1)]
+    rs = [b - apply(x)] + [np.zeros_like(b) for _ in range(l)]
+    r0 = np.sqrt(dot(rs[0], rs[0]))
+    absolute, relative = r0, 1.0
+    hist = [1.0]
+    if r0 < absolute_tolerance:
+        return x, hist + [1.0]
+    omega = sigma = 1.0
+    for _ in range(1, max_iterations):
+        sigma = -omega * sigma
+        for j in range(l):
+            rho = dot(r_shadow, rs[j])
+            beta = rho / sigma
+            for i in range(j + 1):
+                us[i] = 1.0 * rs[i] + (-beta) * us[i]
+            us[j + 1] = apply(us[j])
+            sigma = dot(r_shadow, us[j + 1])
+            alpha = rho / sigma
+            for i in range(j + 1):
+                rs[i] = rs[i] + (-alpha) * us[i + 1]
+            rs[j + 1] = apply(rs[j])
+            x = x + alpha * us[0]
+        M0 = np.array([dot(rs[0], rs[j]) for j in range(1, l + 1)])
+        M = np.array([[dot(rs[i + 1], rs[j + 1]) for j in range(l)] for i in range(l)])
+        gamma = np.linalg.solve(M, M0)
+        for j in range(1, l + 1):
+            us[0] = us[0] + (-gamma[j - 1]) * us[j]
+        for j in range(l):
+            x = x + gamma[j] * rs[j]
+        for j in range(1, l + 1):
+            rs[0] = rs[0] + (-gamma[j - 1]) * rs[j]
+        omega = gamma[l - 1]
+        absolute = np.sqrt(dot(rs[0], rs[0]))
+        relative = absolute / r0
+        hist.append(relative)
+        if relative <= relative_tolerance or absolute < absolute_tolerance:
+            break
+    hist.append(relative)
+    return x, hist
+
+
 def chebyshev_smoother(apply, inv_diag, b, x, order, iterations, lambda_estimate):
     """Chebyshev smoothing (linalg/solvers/chebyshev.hpp:100-160) of A x = b with the inverse diagonal, given the
     power-iteration estimate of the largest eigenvalue of D^-1 A: bounds [0.1, 1.5] x estimate; rho is set once

@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from helpers import rel
-from oracle_lib import (Mesh, chebyshev_smoother, fgmres, laplace_vcycles, pminres, ref_available, run_ref, stokes_block_fgmres,
+from oracle_lib import (Mesh, chebyshev_smoother, fgmres, laplace_vcycles, pbicgstab, pminres, ref_available, run_ref, stokes_block_fgmres,
                         stokes_block_minres)
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
@@ -87,6 +87,18 @@ def test_chebyshev_smoother_matches_reference(case):
     xo = chebyshev_smoother(lambda v: fine.laplace(v, True, False), inv, G.cg_rhs(x["s"]), np.zeros(fine.shape),
                             C["order"], C["iters"], float(g["chebyshev_lambda"]))
     assert rel(xo, g["chebyshev_x"]) <= TOL
+
+
+def test_pbicgstab_matches_reference(case):
+    """PBiCGStab(2) (pbicgstab.hpp:98-260) on the Dirichlet Laplace from x = 0, with the shadow residual the
+    reference drew: the same number of steps and the same solution; residuals to 1e-5 relative above 1e-14."""
+    g, fine, _, x = case
+    B = G.BICGSTAB_CASE
+    xo, ho = pbicgstab(lambda v: fine.laplace(v, True, False), fine.dot, G.cg_rhs(x["s"]), B["l"], B["maxit"],
+                       B["tol"], g["bicgstab_rshadow"])
+    assert len(ho) == len(g["bicgstab_hist"])
+    np.testing.assert_allclose(ho, g["bicgstab_hist"], rtol=1e-5, atol=1e-14)
+    assert rel(xo, g["bicgstab_x"]) <= TOL
 
 
 def test_pminres_matches_reference(case):
