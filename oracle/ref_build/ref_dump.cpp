@@ -367,8 +367,8 @@ int cmd_vcycle( int Lmin, int Lmax, double rmin, double rmax, double omega, int 
 // from x = 0 to b.bin: `iters` sweeps of order `order`, the eigenvalue estimate from `pits` power
 // iterations.  The estimate starts from randomize(), a generator pool with a fixed seed created per call:
 // deterministic on one thread (run with OMP_NUM_THREADS=1).  The same estimate is computed here once more
-// (same operator, same start) and printed, so the smoother after it can be checked.  Writes x.bin; prints
-// {"lambda": ...}
+// (same operator, same start) and printed, so the smoother after it can be checked, and the start vector is
+// written out (start.bin) so the power iteration itself can be checked.  Writes x.bin; prints {"lambda": ...}
 int cmd_laplace_chebyshev( int L, double rmin, double rmax, int order, int iters, int pits, const std::string& dir )
 {
     using V   = linalg::VectorQ1Scalar< double >;
@@ -382,6 +382,10 @@ int cmd_laplace_chebyshev( int L, double rmin, double rmax, int order, int iters
     linalg::apply( Ad, ones, inv );
     linalg::invert_entries( inv );
     linalg::DiagonallyScaledOperator< Lap > scaled( A, inv );
+    // the start vector power_iteration draws (randomize re-seeds its pool on every call)
+    linalg::randomize( t0 );
+    auto start = view_to_host( t0.grid_data() );
+    write_file( dir + "/start.bin", start.data(), start.size() );
     const double lambda = linalg::solvers::power_iteration( scaled, t0, t1, pits );
     std::vector< V > tmps;
     for ( int i = 0; i < 2; ++i )

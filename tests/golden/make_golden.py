@@ -169,6 +169,7 @@ def main():
                        json_out=True)
         out["chebyshev_x"] = np.fromfile(f"{d}/x.bin").reshape(fine.shape)
         out["chebyshev_lambda"] = np.array(info["lambda"])
+        out["power_start"] = np.fromfile(f"{d}/start.bin").reshape(fine.shape)
         B = BICGSTAB_CASE
         run_ref(["laplace_bicgstab", L, R_MIN, R_MAX, B["l"], B["maxit"], B["tol"], d], d)
         out["bicgstab_x"] = np.fromfile(f"{d}/x.bin").reshape(fine.shape)

@@ -434,6 +434,21 @@ def pbicgstab(apply, dot, b, l, max_iterations, relative_tolerance, r_shadow, ab
     return x, hist
 
 
+def power_iteration(apply, dot, start, iterations):
+    """Largest-eigenvalue estimate (linalg/solvers/power_iteration.hpp:13-48) from the given start vector (the
+    reference draws it with randomize): normalise, apply, then `iterations` times normalise the image, apply
+    and take the Rayleigh quotient <v, A v>.  Norms are the owned-masked 2-norms."""
+    v = np.asarray(start, dtype=np.float64)
+    v = (1.0 / np.sqrt(dot(v, v))) * v
+    av = apply(v)
+    radius = 0.0
+    for _ in range(iterations):
+        v = (1.0 / np.sqrt(dot(av, av))) * av
+        av = apply(v)
+        radius = dot(v, av)
+    return radius
+
+
 def chebyshev_smoother(apply, inv_diag, b, x, order, iterations, lambda_estimate):
     """Chebyshev smoothing (linalg/solvers/chebyshev.hpp:100-160) of A x = b with the inverse diagonal, given the
     power-iteration estimate of the largest eigenvalue of D^-1 A: bounds [0.1, 1.5] x estimate; rho is set once

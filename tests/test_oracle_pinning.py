@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from helpers import rel
-from oracle_lib import (Mesh, chebyshev_smoother, fgmres, laplace_vcycles, pbicgstab, pminres, ref_available, run_ref, stokes_block_fgmres,
+from oracle_lib import (Mesh, chebyshev_smoother, fgmres, laplace_vcycles, pbicgstab, pminres, power_iteration, ref_available, run_ref, stokes_block_fgmres,
                         stokes_block_minres)
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
@@ -75,6 +75,16 @@ def test_stokes_operator_matches_reference(case, bcc, bcs):
     p = fine.divergence(coarse, x["u"], bcc, bcs)
     assert rel(u, g[f"stokes_u_{bcc}{bcs}"]) <= TOL
     assert rel(p, g[f"stokes_p_{bcc}{bcs}"]) <= TOL
+
+
+def test_power_iteration_matches_reference(case):
+    """power_iteration.hpp:13-48 on D^-1 A (the Chebyshev smoother's estimate, 50 iterations) from the start
+    vector the reference drew: the same eigenvalue estimate."""
+    g, fine, _, _ = case
+    inv = 1.0 / fine.laplace(np.ones(fine.shape), True, True)
+    lam = power_iteration(lambda v: inv * fine.laplace(v, True, False), fine.dot, g["power_start"],
+                          G.CHEBYSHEV_CASE["pits"])
+    assert abs(lam - float(g["chebyshev_lambda"])) <= 1e-12 * abs(lam)
 
 
 def test_chebyshev_smoother_matches_reference(case):
