@@ -318,7 +318,8 @@ def stokes_leg(shell, C, torch, k_np):
     (fp32_mg) or the FP64 V-cycle (fp64_mg) inside the block-triangular preconditioner, and the
     mixed-precision refinement (fp32_refine: FP64 residual and update around FGMRES(100) cycles done
     entirely in FP32); 4-level V-cycle with Chebyshev order 3, coarse PCG in FP64 in every form.
-    Each form: one warm-up solve, then two timed solves from x = 0; `seconds` is the faster one."""
+    Each form: one warm-up solve, then two timed solves from x = 0; `seconds` is the faster one, and each
+    sample carries the SM clocks and throttle reasons sampled during it."""
     pf, pc = shell.ShellMesh(LEVEL, RMIN, RMAX), shell.ShellMesh(LEVEL - 1, RMIN, RMAX)
     coords, radii = pf.geometry()
     kv = shell.VectorQ1Scalar(pf)
@@ -338,23 +339,25 @@ def stokes_leg(shell, C, torch, k_np):
                                restart=100, r_min=RMIN, r_max=RMAX, gca=1, outer=outer)
         xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
         s.solve(fu, fp, xu, xp)  # warm-up: eigenvalue estimates, graph capture, first-touch
-        samples = []
+        samples, clocks = [], []
         for _ in range(2):
             xu.data.zero_()
             xp.data.zero_()
-            torch.cuda.synchronize()
-            ev0.record()
-            it, rr = s.solve(fu, fp, xu, xp)
-            ev1.record()
-            torch.cuda.synchronize()
+            with ClockSampler(0) as clk:
+                torch.cuda.synchronize()
+                ev0.record()
+                it, rr = s.solve(fu, fp, xu, xp)
+                ev1.record()
+                torch.cuda.synchronize()
             samples.append(ev0.elapsed_time(ev1) / 1e3)
+            clocks.append(clk.summary())
         ku, kp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
         s.apply(xu, xp, ku, kp)
         shell.lincomb(ku, [1.0, -1.0], [fu, ku])
         shell.lincomb(kp, [1.0, -1.0], [fp, kp])
         true_rr = np.sqrt(shell.dot(ku, ku) + shell.dot(kp, kp)) / fnorm
         out[tag] = {"seconds": round(min(samples), 4), "samples": [round(t, 4) for t in samples], "iterations": it,
-                    "true_relres": float(f"{true_rr:.3e}")}
+                    "true_relres": float(f"{true_rr:.3e}"), "clocks": clocks}
         del s
     out["speedup_fp32_mg"] = round(out["fp64_mg"]["seconds"] / out["fp32_mg"]["seconds"], 3)
     out["speedup_fp32_refine"] = round(out["fp64_mg"]["seconds"] / out["fp32_refine"]["seconds"], 3)
@@ -545,8 +548,8 @@ class ClockSampler:
                 for n, v in zip(names, r[5:9]):
                     if v.lower() == "active":
                         reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_min_mhz": min(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons), "samples": len(sm)}
 
 
 def cpu_baseline(steps):
