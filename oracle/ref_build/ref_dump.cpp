@@ -29,6 +29,8 @@
 //                                          KMass(1/kp) Schur block): x_u.bin, x_p.bin, hist.bin
 //   stokes_minres L rmin rmax bcc bcs maxit tol sweeps omega DIR  PMINRES on EpsDivDivStokes with the
 //                                          block-diagonal preconditioner (same blocks): x_u, x_p, hist
+//   kerngen_vcycle Lmin Lmax rmin rmax bcc bcs omega smooth cycles cmaxit DIR  epsilon-div-div multigrid
+//                                          (k<l>.bin per level, Jacobi, constant vector transfers, coarse PCG)
 //   vcycle Lmin Lmax rmin rmax omega smooth cycles cmaxit DIR  Laplace multigrid (Jacobi, constant
 //                                          transfers, coarse PCG) from x = 0 on b.bin, writes x.bin
 //   prolong / restrict Lf rmin rmax DIR    constant vector transfer between Lf-1 and Lf
@@ -601,6 +603,68 @@ int cmd_stokes_minres( int L, double rmin, double rmax, int bcc, int bcs, int ma
     return 0;
 }
 
+// `cycles` V-cycles on EpsilonDivDivKerngen<double> (bcc, bcs) over levels Lmin..Lmax from x = 0: the
+// viscosity of level l from k<l>.bin, Jacobi pre / post smoothing with the kerngen diagonal (`smooth` sweeps,
+// damping omega), constant vector transfers, coarsest-level PCG (max `cmaxit`, relative 1e-8, absolute
+// 1e-30); b.bin (vector) on Lmax, writes x.bin
+int cmd_kerngen_vcycle( int Lmin, int Lmax, double rmin, double rmax, int bcc, int bcs, double omega, int smooth,
+                        int cycles, int cmaxit, const std::string& dir )
+{
+    using V  = linalg::VectorQ1Vec< double >;
+    using Op = Kerngen;
+    using P  = fe::wedge::operators::shell::ProlongationVecConstant< double >;
+    using R  = fe::wedge::operators::shell::RestrictionVecConstant< double >;
+    std::vector< Setup >                           lv;
+    std::vector< linalg::VectorQ1Scalar< double > > ks;
+    for ( int l = Lmin; l <= Lmax; ++l )
+    {
+        lv.emplace_back( l, rmin, rmax );
+        ks.emplace_back( "k" + std::to_string( l ), lv.back().domain, lv.back().omask );
+        view_from_host( ks.back().grid_data(),
+                        read_file< double >( dir + "/k" + std::to_string( l ) + ".bin", lv.back().nodes ).data() );
+    }
+    std::vector< P >                            Ps;
+    std::vector< R >                            Rs;
+    std::vector< Op >                           Ac;
+    std::vector< V >                            tr, te, tmp, ctmps;
+    std::vector< linalg::solvers::Jacobi< Op > > sm;
+    for ( size_t i = 0; i < lv.size(); ++i )
+    {
+        Setup& s = lv[i];
+        tmp.emplace_back( "tmp" + std::to_string( i ), s.domain, s.omask );
+        V  ts( "ts" + std::to_string( i ), s.domain, s.omask ), inv( "inv" + std::to_string( i ), s.domain, s.omask );
+        Op Ad = make_kerngen( s, ks[i], bcc, bcs, true );
+        linalg::assign( ts, 1.0 );
+        linalg::apply( Ad, ts, inv );
+        linalg::invert_entries( inv );
+        sm.emplace_back( inv, smooth, ts, omega );
+        if ( i == 0 )
+            for ( int k = 0; k < 4; ++k )
+                ctmps.emplace_back( "ct" + std::to_string( k ), s.domain, s.omask );
+        if ( i + 1 < lv.size() )
+        {
+            tr.emplace_back( "tr" + std::to_string( i ), s.domain, s.omask );
+            te.emplace_back( "te" + std::to_string( i ), s.domain, s.omask );
+            Ac.push_back( make_kerngen( s, ks[i], bcc, bcs, false ) );
+            Ps.emplace_back( linalg::OperatorApplyMode::Add );
+            Rs.emplace_back( s.domain );
+        }
+    }
+    Setup& f = lv.back();
+    V      b( "b", f.domain, f.omask ), x( "x", f.domain, f.omask );
+    load_vec( b, dir + "/b.bin", f.nodes );
+    linalg::assign( x, 0.0 );
+    Op   A     = make_kerngen( f, ks.back(), bcc, bcs, false );
+    auto table = std::make_shared< util::Table >();
+    linalg::solvers::PCG< Op > coarse( linalg::solvers::IterativeSolverParameters{ cmaxit, 1e-8, 1e-30 }, table,
+                                       ctmps );
+    linalg::solvers::Multigrid< Op, P, R, linalg::solvers::Jacobi< Op >, linalg::solvers::PCG< Op > > mg(
+        Ps, Rs, Ac, tr, te, tmp, sm, sm, coarse, cycles, 0.0 );
+    linalg::solvers::solve( mg, A, x, b );
+    save_vec( x, dir + "/x.bin", f.nodes );
+    return 0;
+}
+
 // EpsDivDivStokes<double> (epsilon_divdiv_stokes.hpp:55-90): [A B^T; B 0] applied to (u, p), A the
 // kerngen operator with k.bin on level L, p on level L-1
 int cmd_stokes_op( int L, double rmin, double rmax, int bcc, int bcs, const std::string& dir )
@@ -850,6 +914,9 @@ int main( int argc, char** argv )
         return cmd_laplace_minres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), D( 6 ), argv[7] );
     if ( cmd == "laplace_fgmres" && argc == 9 )
         return cmd_laplace_fgmres( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), D( 7 ), argv[8] );
+    if ( cmd == "kerngen_vcycle" && argc == 13 )
+        return cmd_kerngen_vcycle( I( 2 ), I( 3 ), D( 4 ), D( 5 ), I( 6 ), I( 7 ), D( 8 ), I( 9 ), I( 10 ), I( 11 ),
+                                   argv[12] );
     if ( cmd == "vcycle" && argc == 11 )
         return cmd_vcycle( I( 2 ), I( 3 ), D( 4 ), D( 5 ), D( 6 ), I( 7 ), I( 8 ), I( 9 ), argv[10] );
     if ( cmd == "stokes" && argc == 8 )

@@ -112,6 +112,21 @@ def pressure_viscosity(x):
 VCYCLE = dict(lmin=1, lmax=3, omega=0.6, smooth=2, cycles=2, cmaxit=50)
 
 
+# epsilon-div-div V-cycles over levels 1-3, free-slip both radii (the Stokes velocity block's boundaries):
+# Jacobi omega 0.5, 2 sweeps, 2 cycles, coarse PCG <= 50 iterations; viscosity injected from level 3
+KVCYCLE = dict(lmin=1, lmax=3, bcs=(2, 2), omega=0.5, smooth=2, cycles=2, cmaxit=50)
+
+
+def kvcycle_inputs():
+    """seeded viscosity per level (the finest field injected to the coarser levels) and right-hand side"""
+    m = Mesh(KVCYCLE["lmax"])
+    rs = np.random.RandomState(47)
+    kf = m.make_consistent(np.exp(rs.normal(size=m.shape))).reshape(m.shape)
+    b = m.make_consistent(rs.normal(size=(3,) + m.shape)).reshape((3,) + m.shape)
+    ks = [np.ascontiguousarray(kf[:, ::s, ::s, ::s]) for s in (4, 2, 1)]
+    return ks, b
+
+
 def vcycle_rhs():
     """seeded right-hand side on the finest V-cycle level"""
     m = Mesh(VCYCLE["lmax"])
@@ -201,6 +216,16 @@ def main():
             out[f"stokes_minres_u_{bcc}{bcs}"] = np.fromfile(f"{d}/x_u.bin").reshape((3,) + fine.shape)
             out[f"stokes_minres_p_{bcc}{bcs}"] = np.fromfile(f"{d}/x_p.bin").reshape(coarse.shape)
             out[f"stokes_minres_hist_{bcc}{bcs}"] = np.fromfile(f"{d}/hist.bin")
+
+        ks, kb = kvcycle_inputs()
+        out["checksum_kvcycle_b"] = checksum(kb)
+        K = KVCYCLE
+        for level, k in zip(range(K["lmin"], K["lmax"] + 1), ks):
+            k.tofile(f"{d}/k{level}.bin")
+        kb.tofile(f"{d}/b.bin")
+        run_ref(["kerngen_vcycle", K["lmin"], K["lmax"], R_MIN, R_MAX, *K["bcs"], K["omega"], K["smooth"],
+                 K["cycles"], K["cmaxit"], d], d)
+        out["kvcycle_x"] = np.fromfile(f"{d}/x.bin").reshape(kb.shape)
 
         vb = vcycle_rhs()
         out["checksum_vcycle_b"] = checksum(vb)

@@ -537,34 +537,80 @@ def stokes_block_minres(fine, coarse, k, kp, b_u, b_p, bc_cmb, bc_surf, max_iter
     return u, p, hist
 
 
-def laplace_vcycles(meshes, b, omega, smooth, cycles, coarse_max_iterations):
-    """Multigrid V-cycles from x = 0 (linalg/solvers/multigrid.hpp:108-211) on Laplace with Dirichlet rows over
-    `meshes` (coarsest first): Jacobi pre / post smoothing (jacobi.hpp:51-62: x += omega D^-1 (b - A x), D the
-    diagonal of the Dirichlet operator, `smooth` sweeps), constant scalar restriction and additive prolongation,
-    and on the coarsest mesh the unpreconditioned PCG from zero (pcg.hpp; relative 1e-8, absolute 1e-30)."""
-    inv = [1.0 / m.laplace(np.ones(m.shape), True, True) for m in meshes]
+def pcg(apply, dot, b, max_iterations, relative_tolerance, absolute_tolerance=1e-30):
+    """Unpreconditioned PCG from x = 0 (linalg/solvers/pcg.hpp:78-160 with z = r), the arithmetic of
+    Mesh.laplace_pcg for any operator.  Returns (x, iterations)."""
+    b = np.asarray(b, dtype=np.float64)
+    x = np.zeros_like(b)
+    r = b.copy()
+    p = r.copy()
+    r0 = np.sqrt(dot(r, r))
+    if r0 < absolute_tolerance:
+        return x, 0
+    for it in range(1, max_iterations + 1):
+        rz = dot(r, r)
+        ap = apply(p)
+        alpha = rz / dot(ap, p)
+        x += alpha * p
+        r -= alpha * ap
+        res = np.sqrt(dot(r, r))
+        if res / r0 <= relative_tolerance or res < absolute_tolerance:
+            return x, it
+        p = r + (dot(r, r) / rz) * p
+    return x, max_iterations
 
+
+def _vcycles(applies, inv_diags, restricts, prolongs, coarse_solve, b, omega, smooth, cycles):
+    """V-cycles from x = 0 (linalg/solvers/multigrid.hpp:108-211) over levels 0 (coarsest) .. n-1: Jacobi pre /
+    post smoothing (jacobi.hpp:51-62: x += omega D^-1 (b - A x), `smooth` sweeps), restriction of the residual,
+    recursion from a zero correction, additive prolongation; coarse_solve(rhs) on level 0."""
     def jacobi(l, x, rhs):
         for _ in range(smooth):
-            x += omega * (inv[l] * (rhs - meshes[l].laplace(x, True, False)))
+            x += omega * (inv_diags[l] * (rhs - applies[l](x)))
 
     def cycle(l, x, rhs):
         if l == 0:
-            x[...] = meshes[0].laplace_pcg(rhs, coarse_max_iterations, 1e-8, 1e-30)[0]
+            x[...] = coarse_solve(rhs)
             return
-        fine, coarse = meshes[l], meshes[l - 1]
         jacobi(l, x, rhs)
-        rc = fine.restrict(coarse, rhs - fine.laplace(x, True, False), ncomp=1)[0]
-        ec = np.zeros(coarse.shape)
+        rc = restricts[l](rhs - applies[l](x))
+        ec = np.zeros_like(rc)
         cycle(l - 1, ec, rc)
-        x += fine.prolong(coarse, ec, ncomp=1)[0]
+        x += prolongs[l](ec)
         jacobi(l, x, rhs)
 
-    x = np.zeros(meshes[-1].shape)
+    b = np.asarray(b, dtype=np.float64)
+    x = np.zeros_like(b)
     for _ in range(cycles):
-        cycle(len(meshes) - 1, x, np.asarray(b, dtype=np.float64))
+        cycle(len(applies) - 1, x, b)
     return x
 
+
+def laplace_vcycles(meshes, b, omega, smooth, cycles, coarse_max_iterations):
+    """Multigrid V-cycles from x = 0 (multigrid.hpp:108-211) on Laplace with Dirichlet rows over `meshes`
+    (coarsest first): Jacobi smoothing with the diagonal of the Dirichlet operator, constant scalar restriction
+    and additive prolongation, and on the coarsest mesh the unpreconditioned PCG from zero (pcg.hpp; relative
+    1e-8, absolute 1e-30)."""
+    n = len(meshes)
+    applies = [lambda v, m=m: m.laplace(v, True, False) for m in meshes]
+    inv = [1.0 / m.laplace(np.ones(m.shape), True, True) for m in meshes]
+    restricts = [None] + [lambda r, f=meshes[l], c=meshes[l - 1]: f.restrict(c, r, ncomp=1)[0] for l in range(1, n)]
+    prolongs = [None] + [lambda e, f=meshes[l], c=meshes[l - 1]: f.prolong(c, e, ncomp=1)[0] for l in range(1, n)]
+    coarse = lambda rhs: meshes[0].laplace_pcg(rhs, coarse_max_iterations, 1e-8, 1e-30)[0]
+    return _vcycles(applies, inv, restricts, prolongs, coarse, b, omega, smooth, cycles)
+
+
+def kerngen_vcycles(meshes, ks, b, bc_cmb, bc_surf, omega, smooth, cycles, coarse_max_iterations):
+    """The same V-cycles on the epsilon-div-div (kerngen) operator with boundary conditions (bc_cmb, bc_surf),
+    the viscosity ks[l] on meshes[l], Jacobi with the kerngen diagonal, constant vector transfers, and the PCG
+    on the coarsest kerngen operator."""
+    n = len(meshes)
+    applies = [lambda v, m=m, k=k: m.kerngen(k, v, bc_cmb, bc_surf) for m, k in zip(meshes, ks)]
+    inv = [1.0 / m.kerngen(k, np.ones((3,) + m.shape), bc_cmb, bc_surf, diag=True) for m, k in zip(meshes, ks)]
+    restricts = [None] + [lambda r, f=meshes[l], c=meshes[l - 1]: f.restrict(c, r) for l in range(1, n)]
+    prolongs = [None] + [lambda e, f=meshes[l], c=meshes[l - 1]: f.prolong(c, e) for l in range(1, n)]
+    coarse = lambda rhs: pcg(applies[0], meshes[0].dot, rhs, coarse_max_iterations, 1e-8)[0]
+    return _vcycles(applies, inv, restricts, prolongs, coarse, b, omega, smooth, cycles)
 
 def ref_available():
     return os.path.exists(REF_DUMP)

@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from helpers import rel
-from oracle_lib import (Mesh, chebyshev_smoother, fgmres, laplace_vcycles, pbicgstab, pminres, power_iteration, ref_available, run_ref, stokes_block_fgmres,
+from oracle_lib import (Mesh, chebyshev_smoother, fgmres, kerngen_vcycles, laplace_vcycles, pbicgstab, pminres, power_iteration, ref_available, run_ref, stokes_block_fgmres,
                         stokes_block_minres)
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
@@ -172,6 +172,20 @@ def test_laplace_vcycles_match_reference(case):
     meshes = [Mesh(level) for level in range(V["lmin"], V["lmax"] + 1)]
     x = laplace_vcycles(meshes, b, V["omega"], V["smooth"], V["cycles"], V["cmaxit"])
     assert rel(x, g["vcycle_x"]) <= TOL
+
+
+def test_kerngen_vcycles_match_reference(case):
+    """The velocity block's V-cycle structure: two V-cycles over levels 1-3 on the free-slip epsilon-div-div
+    operator (rotation penalty included) with Jacobi smoothing, constant vector transfers and the coarse PCG,
+    against the reference's own Multigrid<EpsilonDivDivKerngen, ...>.  The 50-iteration coarse CG amplifies
+    rounding, hence 1e-10."""
+    g = case[0]
+    K = G.KVCYCLE
+    ks, b = G.kvcycle_inputs()
+    assert np.allclose(G.checksum(b), g["checksum_kvcycle_b"], rtol=1e-13, atol=0)
+    meshes = [Mesh(level) for level in range(K["lmin"], K["lmax"] + 1)]
+    x = kerngen_vcycles(meshes, ks, b, *K["bcs"], K["omega"], K["smooth"], K["cycles"], K["cmaxit"])
+    assert rel(x, g["kvcycle_x"]) <= 1e-10
 
 
 def test_transfers_match_reference(case):
