@@ -15,8 +15,9 @@ step reads data cached by the previous one.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 For N > 1 (torchrun) every rank runs the same apply on its own GPU (replicas:
-the ten diamonds of one shell fit one GPU), timed with CUDA
-events, max over ranks; value is the aggregate over ranks.
+the ten diamonds of one level-6 shell fit one GPU, so the apply is not
+sharded), timed with CUDA events, max over ranks; value is the aggregate over
+ranks.
 """
 import argparse
 import json

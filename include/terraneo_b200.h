@@ -307,11 +307,14 @@ TN_API int tn_vec_dot_f32( const tn_mesh* mesh, int ncomp, const float* const* a
  * i < n of a[c][i] b[c][i] where owned[i] != 0 (owned NULL: every entry),
  * compensated FP64; returns after the value is on the host.  Limits:
  * n <= 33,554,432 entries per component (a larger n is rejected with
- * TN_ERR_ARG), ncomp 1..3.  The first call on each device does a one-time
- * set-up (the scratch's address is looked up and cached), so make it outside
- * any stream capture.  All calls on one device share the scratch: calls that
- * can overlap (several streams or host threads) race and must be serialised
- * by the caller. */
+ * TN_ERR_ARG), ncomp 1..3.  No call may be made while the stream is being
+ * captured into a CUDA graph: every call copies its result to host memory
+ * and synchronises the stream (a capturing stream is rejected with
+ * TN_ERR_ARG).  The stream must belong to the calling thread's current
+ * device, whose scratch address the first call on that device looks up and
+ * caches (a stream of another device is rejected).  All calls on one device
+ * share the scratch: calls that can overlap (several streams or host
+ * threads) race and must be serialised by the caller. */
 TN_API int tn_vec_dot_noalloc_f64( size_t n, int ncomp, const double* const* a, const double* const* b,
                                    const uint8_t* owned, double* result, void* stream );
 TN_API int tn_vec_invert_f64( const tn_mesh* mesh, int ncomp, double* const* y, void* stream );

@@ -44,6 +44,8 @@
 //   gca L rmin rmax bcc bcs diag mode DIR  TwoGridGCA (mode 0 constant, 1 linear) of the Neumann kerngen
 //                                          operator at level L (k.bin) into level L-1 with bcs, then the
 //                                          stored-matrix apply of the coarse operator to src.bin
+//   kerngen_slow L rmin rmax bcc bcs diag DIR  the kerngen slow path on the reference's own assembled
+//                                          wedge matrices (written to mats.bin) stored in Full mode
 //   vlaplace L rmin rmax bcc bcs diag DIR  VectorLaplace<double>
 //   time_kerngen L rmin rmax bcc bcs reps prints seconds per apply (CPU baseline)
 #include <chrono>
@@ -836,6 +838,50 @@ int cmd_gca( int L, double rmin, double rmax, int bcc, int bcs, int diag, int mo
     return 0;
 }
 
+// The kerngen slow path on the reference's own assembled wedge matrices: the
+// matrices come from get_local_matrix with storage off (assemble_local_matrix,
+// epsilon_divdiv_kerngen.hpp:482-498,2051-2110), are written to mats.bin
+// ([sd][x][y][r][wedge][18][18], row-major), then stored with
+// set_local_matrix under OperatorStoredMatrixMode::Full, which selects the
+// slow path (:151-172, :823-1052) for the apply of src.bin -> dst.bin.
+int cmd_kerngen_slow( int L, double rmin, double rmax, int bcc, int bcs, int diag, const std::string& dir )
+{
+    Setup                            s( L, rmin, rmax );
+    linalg::VectorQ1Scalar< double > k( "k", s.domain, s.omask ), gcae( "gcae", s.domain, s.omask );
+    view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", s.nodes ).data() );
+    linalg::assign( gcae, 1.0 );
+    linalg::VectorQ1Vec< double > src( "src", s.domain, s.omask ), dst( "dst", s.domain, s.omask );
+    load_vec( src, dir + "/src.bin", s.nodes );
+    auto      op = make_kerngen( s, k, bcc, bcs, false );
+    const int N  = 1 << L;
+    using Mat    = dense::Mat< double, 18, 18 >;
+    std::vector< Mat > mats( size_t( 10 ) * N * N * N * 2 );
+    auto cell = [N]( int sd, int x, int y, int r ) { return ( ( size_t( sd ) * N + x ) * N + y ) * N + r; };
+    for ( int sd = 0; sd < 10; ++sd )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                    for ( int w = 0; w < 2; ++w )
+                        mats[cell( sd, x, y, r ) * 2 + w] = op.get_local_matrix( sd, x, y, r, w );
+    std::vector< double > flat( mats.size() * 18 * 18 );
+    for ( size_t i = 0; i < mats.size(); ++i )
+        for ( int a = 0; a < 18; ++a )
+            for ( int b = 0; b < 18; ++b )
+                flat[( i * 18 + a ) * 18 + b] = mats[i]( a, b );
+    write_file( dir + "/mats.bin", flat.data(), flat.size() );
+    op.set_stored_matrix_mode( linalg::OperatorStoredMatrixMode::Full, 0, gcae.grid_data() );
+    for ( int sd = 0; sd < 10; ++sd )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                    for ( int w = 0; w < 2; ++w )
+                        op.set_local_matrix( sd, x, y, r, w, mats[cell( sd, x, y, r ) * 2 + w] );
+    op.set_diagonal( diag != 0 );
+    linalg::apply( op, src, dst );
+    save_vec( dst, dir + "/dst.bin", s.nodes );
+    return 0;
+}
+
 int cmd_epsdivdiv( int L, double rmin, double rmax, int treat, int diag, const std::string& dir )
 {
     Setup                            s( L, rmin, rmax );
@@ -929,6 +975,8 @@ int main( int argc, char** argv )
         return cmd_fct( I( 2 ), D( 3 ), D( 4 ), D( 5 ), D( 6 ), I( 7 ), argv[8] );
     if ( cmd == "gca" && argc == 10 )
         return cmd_gca( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), I( 8 ), argv[9] );
+    if ( cmd == "kerngen_slow" && argc == 9 )
+        return cmd_kerngen_slow( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( cmd == "epsdivdiv" && argc == 8 )
         return cmd_epsdivdiv( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     if ( cmd == "divkgrad" && argc == 9 )

@@ -236,8 +236,22 @@ class Chebyshev
     Chebyshev( int order, const V& inverse_diagonal, std::vector< V > tmps, int iterations, int power_iterations )
     : order_( order ), inv_diag_( inverse_diagonal ), tmps_( std::move( tmps ) ), iterations_( iterations ),
       power_iterations_( power_iterations )
-    {}
+    {
+        // the reference aborts on both (chebyshev.hpp:83-91)
+        if ( order_ < 1 )
+            throw std::runtime_error( "Chebyshev: order must be at least 1" );
+        if ( tmps_.size() < 2 )
+            throw std::runtime_error( "Chebyshev: needs 2 temporary vectors" );
+    }
     void refresh_max_eigenvalue_estimate_in_next_solve() { need_ev_ = true; }
+    // use a given estimate of the largest eigenvalue of D^{-1} A instead of the
+    // power iteration (the reference's smoother draws its start vector at
+    // random; a caller that reproduces a reference run passes its estimate)
+    void set_max_eigenvalue_estimate( double ev )
+    {
+        ev_      = ev;
+        need_ev_ = false;
+    }
     double max_eigenvalue_estimate() const { return ev_; }
     void   solve_impl( Op& A, V& x, const V& b )
     {

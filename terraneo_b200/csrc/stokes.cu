@@ -409,6 +409,12 @@ int check_pair( const tn_mesh* f, const tn_mesh* c )
     TN_CHECK_ARG( f && c, "stokes block: null mesh" );
     TN_CHECK_ARG( c->level == f->level - 1 && c->r_min == f->r_min && c->r_max == f->r_max,
                   "stokes block: the pressure mesh must be the velocity mesh coarsened once" );
+    // the B / B^T kernels run one fine wedge per thread with full-mask warp
+    // shuffles between even and odd lanes: every warp must hold one wedge type
+    // and whole radial columns, i.e. 10 N^3 a multiple of 32 and N even (N >= 4)
+    const long long N = f->N;
+    TN_CHECK_ARG( N >= 4 && N % 2 == 0 && ( 10LL * N * N * N ) % 32 == 0,
+                  "stokes block: the velocity mesh needs level >= 2 (whole radial columns per warp)" );
     return TN_OK;
 }
 

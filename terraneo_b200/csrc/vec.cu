@@ -604,7 +604,11 @@ extern "C" int tn_vec_cast_f32_to_f64( const tn_mesh* m, int ncomp, double* cons
 // per component; longer fields are rejected.  All calls on a device share the
 // array: calls that can overlap (several streams or host threads) race on it
 // and must be serialised by the caller.  The first call on each device looks
-// the array's address up (cudaGetSymbolAddress) and caches it.
+// the array's address up (cudaGetSymbolAddress) and caches it; the array
+// itself is made resident on a device when the library's module is loaded
+// there (with lazy loading, by the first launch or symbol lookup), never by
+// an allocation.  No call may be made while its stream is being captured:
+// every call copies its result to the host and synchronises the stream.
 namespace tn {
 namespace {
 
@@ -685,6 +689,18 @@ extern "C" int tn_vec_dot_noalloc_f64( size_t n, int ncomp, const double* const*
         *result = 0.0;
         return TN_OK;
     }
+    cudaStream_t st = as_stream( s );
+    // the set-up, the counter clear, the result copy to pageable host memory
+    // and the synchronisation are all illegal while the stream is captured
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    TN_CUDA_TRY( cudaStreamIsCapturing( st, &cap ) );
+    TN_CHECK_ARG( cap == cudaStreamCaptureStatusNone,
+                  "tn_vec_dot_noalloc_f64: the stream is being captured (the call reads its result back and synchronises)" );
+    // the cached scratch address is the current device's: the stream must belong to it
+    int cur = 0, sdev = 0;
+    TN_CUDA_TRY( cudaGetDevice( &cur ) );
+    TN_CUDA_TRY( cudaStreamGetDevice( st, &sdev ) );
+    TN_CHECK_ARG( sdev == cur, "tn_vec_dot_noalloc_f64: the stream belongs to another device than the current one" );
     unsigned char* base = nullptr;
     int            rc   = dot_scratch_address( &base );
     if ( rc )
@@ -694,7 +710,6 @@ extern "C" int tn_vec_dot_noalloc_f64( size_t n, int ncomp, const double* const*
     unsigned int* counter  = reinterpret_cast< unsigned int* >( base + kNoAllocCounterOffset );
     const size_t  per_block = size_t( kThreads ) * kNoAllocPerThread;
     const unsigned blocks   = unsigned( ( n + per_block - 1 ) / per_block );
-    cudaStream_t   st       = as_stream( s );
     TN_CUDA_TRY( cudaMemsetAsync( counter, 0, sizeof( unsigned int ), st ) );
     dot_noalloc_kernel<<< blocks, kThreads, 0, st >>>( n, ncomp, pa, pb, owned, partials, counter, dres );
     TN_LAUNCH_CHECK();

@@ -33,6 +33,14 @@ VMASS_MODES = [0, 1]
 DIVKGRAD_CASES = [(1, 0, 0), (0, 0, 0), (1, 1, 0), (1, 0, 1)]
 EPSDIVDIV_CASES = [(1, 0), (0, 0), (1, 1)]
 VLAPLACE_CASES = [(1, 1, 0), (0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 1)]
+# kerngen slow path (the reference's own assembled wedge matrices stored in Full mode): (bcc, bcs, diag)
+KSLOW_CASES = [(1, 1, 0), (2, 2, 0), (2, 1, 0), (0, 0, 0), (2, 2, 1)]
+# wedge matrices kept in the fixture: these cells (flat index (d, x, y, r)), both wedges
+KSLOW_CELLS = [0, 37, 311, 639]
+# TwoGridGCA of the Neumann kerngen operator (level L -> L-1), then the stored-matrix apply of the coarse
+# operator to the coarse vector uc: (interpolation mode 0 constant / 1 linear, bcc, bcs, diag)
+GCA_CASES = [(0, 1, 1, 0), (0, 2, 2, 0), (0, 2, 1, 0), (0, 0, 0, 0), (0, 2, 2, 1),
+             (1, 1, 1, 0), (1, 2, 2, 0), (1, 1, 2, 0), (1, 1, 1, 1)]
 
 
 def inputs(fine, coarse):
@@ -156,6 +164,16 @@ def main():
         for bcc, bcs, diag in KERNGEN_CASES:
             run_ref(["kerngen", L, R_MIN, R_MAX, bcc, bcs, diag, d], d)
             out[f"kerngen_{bcc}{bcs}{diag}"] = np.fromfile(f"{d}/dst.bin").reshape((3,) + fine.shape)
+
+        for bcc, bcs, diag in KSLOW_CASES:
+            run_ref(["kerngen_slow", L, R_MIN, R_MAX, bcc, bcs, diag, d], d)
+            out[f"kslow_{bcc}{bcs}{diag}"] = np.fromfile(f"{d}/dst.bin").reshape((3,) + fine.shape)
+        out["kslow_mats"] = np.fromfile(f"{d}/mats.bin").reshape(-1, 2, 18, 18)[KSLOW_CELLS]
+
+        x["uc"].tofile(f"{d}/src.bin")
+        for mode, bcc, bcs, diag in GCA_CASES:
+            run_ref(["gca", L, R_MIN, R_MAX, bcc, bcs, diag, mode, d], d)
+            out[f"gca_{mode}_{bcc}{bcs}{diag}"] = np.fromfile(f"{d}/dst.bin").reshape((3,) + coarse.shape)
 
         x["s"].tofile(f"{d}/src.bin")
         for treat, diag in LAPLACE_CASES:

@@ -257,6 +257,55 @@ def test_fct_matches_reference(case, kappa, bc):
     assert rel(Tn, g[tag + "_T"]) <= TOL  # ghost layers included
 
 
+@pytest.mark.parametrize("bcc,bcs,diag", G.KSLOW_CASES)
+def test_stored_matrices_and_slow_path_match_reference(case, bcc, bcs, diag):
+    """The kerngen wedge matrices (assemble_local_matrix, epsilon_divdiv_kerngen.hpp:2051-2110) and the slow
+    path that applies them with the boundary treatment at apply time (:823-1052): the oracle's
+    or_kerngen_local_matrices + or_stored_apply against the reference's own matrices stored in Full mode."""
+    g, fine, _, x = case
+    mats = fine.local_matrices(x["k"])
+    assert rel(mats[G.KSLOW_CELLS], g["kslow_mats"]) <= TOL
+    assert rel(fine.stored_apply(mats, x["u"], bcc, bcs, diag), g[f"kslow_{bcc}{bcs}{diag}"]) <= TOL
+
+
+@pytest.mark.parametrize("mode,bcc,bcs,diag", G.GCA_CASES)
+def test_gca_coarse_operator_matches_reference(case, mode, bcc, bcs, diag):
+    """TwoGridGCA (gca/gca.hpp:154-528; constant and linear interpolation) of the Neumann kerngen operator into
+    the coarser level, applied through the slow path with the coarse boundary conditions: the oracle's
+    or_gca_coarsen + or_stored_apply against the reference's coarse operator."""
+    g, fine, coarse, x = case
+    mc = fine.gca_coarsen(coarse, k=x["k"], mode=mode)
+    assert rel(coarse.stored_apply(mc, x["uc"], bcc, bcs, diag), g[f"gca_{mode}_{bcc}{bcs}{diag}"]) <= TOL
+
+
+@pytest.mark.skipif(not ref_available(), reason="compiled reference (oracle/_ref/ref_dump) not built here")
+def test_slow_path_and_gca_match_live_reference_L3():
+    """Level 3 (its coarse level 2), live against the compiled reference: every wedge matrix, the slow-path
+    apply and the GCA coarse operators of both interpolation modes."""
+    L = 3
+    f, c = Mesh(L), Mesh(L - 1)
+    rs = np.random.RandomState(11)
+    k = f.make_consistent(np.exp(2.0 * rs.normal(size=f.shape)))
+    u = f.make_consistent(rs.normal(size=(3,) + f.shape))
+    uc = c.make_consistent(rs.normal(size=(3,) + c.shape))
+    mats = f.local_matrices(k)
+    with tempfile.TemporaryDirectory() as d:
+        k.tofile(f"{d}/k.bin")
+        u.tofile(f"{d}/src.bin")
+        for bcc, bcs, diag in [(2, 2, 0), (1, 2, 0), (2, 1, 1)]:
+            run_ref(["kerngen_slow", L, 0.55, 1.0, bcc, bcs, diag, d], d)
+            assert rel(mats, np.fromfile(f"{d}/mats.bin").reshape(mats.shape)) <= TOL
+            ref = np.fromfile(f"{d}/dst.bin").reshape((3,) + f.shape)
+            assert rel(f.stored_apply(mats, u, bcc, bcs, diag), ref) <= TOL
+        uc.tofile(f"{d}/src.bin")
+        for mode in (0, 1):
+            mc = f.gca_coarsen(c, k=k, mode=mode)
+            for bcc, bcs, diag in [(2, 2, 0), (1, 1, 0), (2, 1, 1)]:
+                run_ref(["gca", L, 0.55, 1.0, bcc, bcs, diag, mode, d], d)
+                ref = np.fromfile(f"{d}/dst.bin").reshape((3,) + c.shape)
+                assert rel(c.stored_apply(mc, uc, bcc, bcs, diag), ref) <= TOL
+
+
 def test_golden_fixture_is_not_trivial(case):
     """A planted error in the oracle's input must break the comparison."""
     g, fine, _, x = case

@@ -58,3 +58,46 @@ def test_noalloc_dot_rejects_sizes_beyond_the_static_scratch():
     assert L.tn_vec_dot_noalloc_f64(pm.stored_nodes, 4, a.comp_ptrs(), a.comp_ptrs(), None, ctypes.byref(r), None) != 0
     assert L.tn_vec_dot_noalloc_f64(pm.stored_nodes, 3, a.comp_ptrs(), a.comp_ptrs(), None, None, None) != 0
     assert r.value == -1.0
+
+
+_FIRST_CALL = r"""
+import ctypes, sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+sys.path.insert(0, sys.argv[1] + "/tests")
+from oracle_lib import Mesh
+from terraneo_b200 import _capi as C
+torch.cuda.set_device(0)
+out = []
+for level in (3, 6):
+    m = Mesh(level)
+    rng = np.random.default_rng(level)
+    a = rng.normal(size=(3, m.ns))
+    b = rng.normal(size=(3, m.ns))
+    own = np.ascontiguousarray(m.omask.reshape(-1)).astype(np.uint8)
+    ta, tb = torch.as_tensor(a, device="cuda"), torch.as_tensor(b, device="cuda")
+    to = torch.as_tensor(own, device="cuda")
+    pa = (ctypes.c_void_p * 3)(*[ta[c].data_ptr() for c in range(3)])
+    pb = (ctypes.c_void_p * 3)(*[tb[c].data_ptr() for c in range(3)])
+    r = ctypes.c_double()
+    rc = C.lib().tn_vec_dot_noalloc_f64(m.ns, 3, pa, pb, to.data_ptr(), ctypes.byref(r), None)
+    assert rc == 0, C.lib().tn_last_error()
+    ref = float(np.sum(a * b * own[None, :]))
+    assert abs(r.value - ref) <= 1e-12 * max(1.0, np.sum(np.abs(a * b))), (level, r.value, ref)
+    out.append(r.value)
+print("first-call ok", out)
+"""
+
+
+def test_noalloc_dot_as_first_library_call_of_a_fresh_process():
+    """The case the entry point exists for: a process whose first library call is tn_vec_dot_noalloc_f64 (its
+    set-up looks the static array up and, under lazy module loading, loads the module), at levels 3 and 6,
+    against the numpy dot of the same fields."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", _FIRST_CALL, root], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "first-call ok" in out.stdout
