@@ -519,6 +519,10 @@ typedef struct
                      the reference.  `iterations` counts the inner FGMRES iterations of all cycles. */
     int    eager; /* 0: after its first application the preconditioner is captured once per vector pair as a
                      CUDA graph and replayed; 1: always launched kernel by kernel */
+    const double* chebyshev_estimates; /* NULL: each level's Chebyshev smoother estimates the largest eigenvalue of
+                     D^-1 A by power iteration on its first use (chebyshev.hpp:159-163); otherwise mg_levels
+                     estimates, coarsest level first, used as given (the reference draws the power iteration's
+                     start vector at random, so reproducing one of its runs needs the estimates it drew) */
 } tn_stokes_params;
 
 typedef struct tn_stokes_solver tn_stokes_solver;

@@ -44,6 +44,11 @@
 //   gca L rmin rmax bcc bcs diag mode DIR  TwoGridGCA (mode 0 constant, 1 linear) of the Neumann kerngen
 //                                          operator at level L (k.bin) into level L-1 with bcs, then the
 //                                          stored-matrix apply of the coarse operator to src.bin
+//   stokes_mg L mglevels rmin rmax bcc bcs restart maxit tol order steps pits vcycles gca cmaxit DIR
+//                                          the app's Stokes solver stack (FGMRES, block-triangular preconditioner,
+//                                          Chebyshev multigrid with GCA coarse operators, coarse PCG) on
+//                                          k.bin / kp.bin / f_u.bin / f_p.bin: x_u, x_p, hist, JSON (iterations,
+//                                          seconds, per-level Chebyshev eigenvalue estimates)
 //   kerngen_slow L rmin rmax bcc bcs diag DIR  the kerngen slow path on the reference's own assembled
 //                                          wedge matrices (written to mats.bin) stored in Full mode
 //   vlaplace L rmin rmax bcc bcs diag DIR  VectorLaplace<double>
@@ -667,6 +672,149 @@ int cmd_kerngen_vcycle( int Lmin, int Lmax, double rmin, double rmax, int bcc, i
     return 0;
 }
 
+// The mantle-circulation app's Stokes solver stack (apps/mantlecirculation/mantlecirculation.cpp:486-735):
+// FGMRES(restart) on EpsDivDivStokes with the block-triangular preconditioner, velocity block one
+// Multigrid V-cycle per application (`vcycles`) over levels L-mglevels+1..L with Chebyshev(order, `steps`
+// sweeps, `pits` power iterations) smoothing, constant vector transfers, GCA coarse operators (gca 1:
+// constant interpolation, Full storage; 2: linear) built from the Neumann block of the finest operator, and
+// the coarse PCG(cmaxit, 1e-6, 1e-16); Schur block the inverse lumped KMass(1 / kp).  Inputs k.bin (level L),
+// kp.bin (level L-1), f_u.bin, f_p.bin; x = 0.  Writes x_u.bin, x_p.bin, hist.bin and prints a JSON line with
+// the iteration count, the solve's seconds and, per level (coarsest first), the largest-eigenvalue estimate
+// each Chebyshev smoother draws (the same power iteration from the same random start, which is reproducible
+// only on one thread).
+int cmd_stokes_mg( int L, int mglevels, double rmin, double rmax, int bcc, int bcs, int restart, int maxit, double tol,
+                   int order, int steps, int pits, int vcycles, int gca, int cmaxit, const std::string& dir )
+{
+    using Stokes   = fe::wedge::operators::shell::EpsDivDivStokes< double >;
+    using Viscous  = Stokes::Block11Type;
+    using Grad     = Stokes::Block12Type;
+    using PMass    = fe::wedge::operators::shell::KMass< double >;
+    using BV       = linalg::VectorQ1IsoQ2Q1< double >;
+    using V        = linalg::VectorQ1Vec< double >;
+    using P        = fe::wedge::operators::shell::ProlongationVecConstant< double >;
+    using R        = fe::wedge::operators::shell::RestrictionVecConstant< double >;
+    using Smoother = linalg::solvers::Chebyshev< Viscous >;
+    using Coarse   = linalg::solvers::PCG< Viscous >;
+    using PrecV    = linalg::solvers::Multigrid< Viscous, P, R, Smoother, Coarse >;
+    using PrecS    = linalg::solvers::DiagonalSolver< PMass >;
+    using Prec     = linalg::solvers::BlockTriangularPreconditioner2x2< Stokes, Viscous, PMass, Grad, PrecV, PrecS >;
+    const int          Lmin = L - mglevels + 1;
+    std::vector< Setup > lv;
+    for ( int l = Lmin; l <= L; ++l )
+        lv.emplace_back( l, rmin, rmax );
+    Setup&             f = lv.back();
+    Setup              c( L - 1, rmin, rmax );
+    BoundaryConditions b  = { { ShellBoundaryFlag::CMB, bc_of( bcc ) }, { ShellBoundaryFlag::SURFACE, bc_of( bcs ) } };
+    BoundaryConditions bn = { { ShellBoundaryFlag::CMB, BoundaryConditionFlag::NEUMANN },
+                              { ShellBoundaryFlag::SURFACE, BoundaryConditionFlag::NEUMANN } };
+    linalg::VectorQ1Scalar< double > k( "k", f.domain, f.omask ), kp( "kp", c.domain, c.omask );
+    view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", f.nodes ).data() );
+    view_from_host( kp.grid_data(), read_file< double >( dir + "/kp.bin", c.nodes ).data() );
+    linalg::invert_entries( kp );
+    Stokes K( f.domain, c.domain, f.coords, f.radii, f.bmask, k.grid_data(), b, false );
+    Stokes Kn( f.domain, c.domain, f.coords, f.radii, f.bmask, k.grid_data(), bn, false );
+
+    std::vector< linalg::VectorQ1Scalar< double > > kc, gcae;
+    std::vector< Viscous >                          Ac;
+    std::vector< P >                                Ps;
+    std::vector< R >                                Rs;
+    std::vector< V >                                tr, te, tmp, tmp2;
+    for ( int i = 0; i < mglevels; ++i )
+    {
+        Setup& s = lv[i];
+        tmp.emplace_back( "tmp" + std::to_string( i ), s.domain, s.omask );
+        tmp2.emplace_back( "tmp2" + std::to_string( i ), s.domain, s.omask );
+        if ( i + 1 < mglevels )
+        {
+            kc.emplace_back( "kc" + std::to_string( i ), s.domain, s.omask );
+            gcae.emplace_back( "gcae" + std::to_string( i ), s.domain, s.omask );
+            linalg::assign( kc.back(), 1.0 ); // replaced by the stored GCA matrices
+            linalg::assign( gcae.back(), 1.0 );
+            Ac.emplace_back( s.domain, s.coords, s.radii, s.bmask, kc.back().grid_data(), b, false );
+            if ( gca )
+                Ac.back().set_stored_matrix_mode( linalg::OperatorStoredMatrixMode::Full, i, gcae.back().grid_data() );
+            tr.emplace_back( "tr" + std::to_string( i ), s.domain, s.omask );
+            te.emplace_back( "te" + std::to_string( i ), s.domain, s.omask );
+            Ps.emplace_back( linalg::OperatorApplyMode::Add );
+            Rs.emplace_back( s.domain );
+        }
+    }
+    if ( gca )
+        for ( int i = mglevels - 2; i >= 0; --i )
+            linalg::solvers::TwoGridGCA< double, Viscous >(
+                i == mglevels - 2 ? Kn.block_11() : Ac[i + 1], Ac[i], i, gcae[i].grid_data(), true,
+                gca == 2 ? linalg::solvers::InterpolationMode::Linear : linalg::solvers::InterpolationMode::Constant );
+
+    std::vector< V >        invd;
+    std::vector< Smoother > sm;
+    std::vector< double >   ev;
+    for ( int i = 0; i < mglevels; ++i )
+    {
+        Setup&   s = lv[i];
+        Viscous& A = i + 1 == mglevels ? K.block_11() : Ac[i];
+        invd.emplace_back( "invd" + std::to_string( i ), s.domain, s.omask );
+        V ones( "ones", s.domain, s.omask );
+        linalg::assign( ones, 1.0 );
+        A.set_diagonal( true );
+        linalg::apply( A, ones, invd.back() );
+        A.set_diagonal( false );
+        linalg::invert_entries( invd.back() );
+        {
+            V                                         t0( "t0", s.domain, s.omask ), t1( "t1", s.domain, s.omask );
+            linalg::DiagonallyScaledOperator< Viscous > dA( A, invd.back() );
+            ev.push_back( linalg::solvers::power_iteration( dA, t0, t1, pits ) );
+        }
+        sm.emplace_back( order, invd.back(), std::vector< V >{ tmp[i], tmp2[i] }, steps, pits );
+    }
+    std::vector< V > ct;
+    for ( int i = 0; i < 4; ++i )
+        ct.emplace_back( "ct" + std::to_string( i ), lv[0].domain, lv[0].omask );
+    auto   table = std::make_shared< util::Table >();
+    Coarse coarse( linalg::solvers::IterativeSolverParameters{ cmaxit, 1e-6, 1e-16 }, table, ct );
+    PrecV  pv( Ps, Rs, Ac, tr, te, tmp, sm, sm, coarse, vcycles, 1e-6 );
+
+    PMass pmass( c.domain, c.coords, c.radii, kp.grid_data(), false );
+    pmass.set_lumped_diagonal( true );
+    linalg::VectorQ1Scalar< double > lumped( "lumped", c.domain, c.omask ), t1( "t1", c.domain, c.omask );
+    linalg::assign( t1, 1.0 );
+    linalg::apply( pmass, t1, lumped );
+    PrecS ps( lumped );
+    BV    ptmp( "ptmp", f.domain, c.domain, f.omask, c.omask );
+    Prec  prec( K.block_11(), pmass, K.block_12(), ptmp, pv, ps );
+    std::vector< BV > tmps;
+    for ( int i = 0; i < 2 * restart + 4; ++i )
+        tmps.emplace_back( "tmp" + std::to_string( i ), f.domain, c.domain, f.omask, c.omask );
+    BV rhs( "rhs", f.domain, c.domain, f.omask, c.omask ), x( "x", f.domain, c.domain, f.omask, c.omask );
+    load_vec( rhs.block_1(), dir + "/f_u.bin", f.nodes );
+    view_from_host( rhs.block_2().grid_data(), read_file< double >( dir + "/f_p.bin", c.nodes ).data() );
+    linalg::assign( x, 0.0 );
+    auto ftable = std::make_shared< util::Table >();
+    linalg::solvers::FGMRESOptions< double > opt;
+    opt.restart = restart, opt.relative_residual_tolerance = tol, opt.absolute_residual_tolerance = 1e-30;
+    opt.max_iterations = maxit;
+    linalg::solvers::FGMRES< Stokes, Prec > fg( tmps, opt, ftable, prec );
+    Kokkos::fence();
+    auto t0 = std::chrono::steady_clock::now();
+    linalg::solvers::solve( fg, K, x, rhs );
+    Kokkos::fence();
+    const double sec = std::chrono::duration< double >( std::chrono::steady_clock::now() - t0 ).count();
+    std::vector< double > hist;
+    for ( const auto& row : ftable->rows() )
+        hist.push_back( std::get< double >( row.at( "relative_residual" ) ) );
+    write_file( dir + "/hist.bin", hist.data(), hist.size() );
+    save_vec( x.block_1(), dir + "/x_u.bin", f.nodes );
+    auto xp = view_to_host( x.block_2().grid_data() );
+    write_file( dir + "/x_p.bin", xp.data(), xp.size() );
+    std::printf( "{\"iterations\": %d, \"seconds\": %.9g, \"threads\": %d, \"eigenvalues\": [",
+                 int( hist.size() ) - 1,
+                 sec,
+                 Kokkos::DefaultExecutionSpace().concurrency() );
+    for ( size_t i = 0; i < ev.size(); ++i )
+        std::printf( "%s%.17g", i ? ", " : "", ev[i] );
+    std::printf( "]}\n" );
+    return 0;
+}
+
 // EpsDivDivStokes<double> (epsilon_divdiv_stokes.hpp:55-90): [A B^T; B 0] applied to (u, p), A the
 // kerngen operator with k.bin on level L, p on level L-1
 int cmd_stokes_op( int L, double rmin, double rmax, int bcc, int bcs, const std::string& dir )
@@ -975,6 +1123,9 @@ int main( int argc, char** argv )
         return cmd_fct( I( 2 ), D( 3 ), D( 4 ), D( 5 ), D( 6 ), I( 7 ), argv[8] );
     if ( cmd == "gca" && argc == 10 )
         return cmd_gca( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), I( 8 ), argv[9] );
+    if ( cmd == "stokes_mg" && argc == 18 )
+        return cmd_stokes_mg( I( 2 ), I( 3 ), D( 4 ), D( 5 ), I( 6 ), I( 7 ), I( 8 ), I( 9 ), D( 10 ), I( 11 ), I( 12 ),
+                              I( 13 ), I( 14 ), I( 15 ), I( 16 ), argv[17] );
     if ( cmd == "kerngen_slow" && argc == 9 )
         return cmd_kerngen_slow( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( cmd == "epsdivdiv" && argc == 8 )

@@ -30,7 +30,8 @@ class StokesParams(ctypes.Structure):
                 ("chebyshev_order", c_int), ("smoothing_steps", c_int), ("power_iterations", c_int),
                 ("vcycles", c_int), ("coarse_max_iterations", c_int), ("coarse_relative_tolerance", c_double),
                 ("restart", c_int), ("max_iterations", c_int), ("relative_tolerance", c_double),
-                ("absolute_tolerance", c_double), ("gca", c_int), ("outer", c_int), ("eager", c_int)]
+                ("absolute_tolerance", c_double), ("gca", c_int), ("outer", c_int), ("eager", c_int),
+                ("chebyshev_estimates", P(c_double))]
 
 
 class ScalarMGParams(ctypes.Structure):

@@ -378,9 +378,14 @@ __global__ void __launch_bounds__( kThreads, TN_TILE_MINBLOCKS ) kerngen_tile_ke
                         F[0] += T( beta[1] * x2 - beta[2] * x1 );
                         F[1] += T( beta[2] * x0 - beta[0] * x2 );
                         F[2] += T( beta[0] * x1 - beta[1] * x0 );
-                        F32[0] += T( beta[1] * y2 - beta[2] * y1 );
-                        F32[1] += T( beta[2] * y0 - beta[0] * y2 );
-                        F32[2] += T( beta[0] * y1 - beta[1] * y0 );
+                        // the top level is level N only in the last radial chunk; otherwise it is the
+                        // next chunk's level r0 + RC, whose lane 0 adds that level's penalty itself
+                        if ( last_chunk )
+                        {
+                            F32[0] += T( beta[1] * y2 - beta[2] * y1 );
+                            F32[1] += T( beta[2] * y0 - beta[0] * y2 );
+                            F32[2] += T( beta[0] * y1 - beta[1] * y0 );
+                        }
                     }
                     (void) lev;
                     if ( lane < RC )

@@ -93,6 +93,7 @@ struct tn_stokes_solver
     std::unique_ptr< Gradient< double > >                    BT;
     std::function< void( VectorQ1IsoQ2Q1< double >&, const VectorQ1IsoQ2Q1< double >& ) > run;
     std::vector< double >                                    history;
+    std::vector< double >                                    chebyshev_estimates;
     int                                                      iterations = 0;
     double                                                   relres     = 1.0;
     int                                                      skips      = 0;
@@ -175,6 +176,8 @@ std::shared_ptr< MG< T, Coarse > > build_mg( tn_stokes_solver& s, std::vector< s
         auto inv = inverse_diagonal_vec( *ops.back(), m );
         sm.emplace_back( prm.chebyshev_order, inv, std::vector< VectorQ1Vec< T > >{ VectorQ1Vec< T >( m ), VectorQ1Vec< T >( m ) },
                          prm.smoothing_steps, prm.power_iterations );
+        if ( prm.chebyshev_estimates )
+            sm.back().set_max_eigenvalue_estimate( prm.chebyshev_estimates[l - Lmin] );
         tmp.emplace_back( m );
         if ( l < L )
         {
@@ -355,6 +358,12 @@ extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min,
     {
         auto s = std::make_unique< tn_stokes_solver >();
         s->prm = *p;
+        if ( p->chebyshev_estimates )
+        {
+            // kept with the solver: the caller's array need not outlive this call
+            s->chebyshev_estimates.assign( p->chebyshev_estimates, p->chebyshev_estimates + p->mg_levels );
+            s->prm.chebyshev_estimates = s->chebyshev_estimates.data();
+        }
         const int L = p->level, Lmin = L - p->mg_levels + 1;
         const int Llo = std::min( Lmin, L - 1 );
         s->mesh.resize( L + 1 );

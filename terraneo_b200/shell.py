@@ -429,11 +429,19 @@ class StokesSolver:
     def __init__(self, level, viscosity, mg_levels=4, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=True,
                  chebyshev_order=3, smoothing_steps=2, power_iterations=10, vcycles=1, coarse_max_iterations=50,
                  coarse_relative_tolerance=1e-6, restart=30, max_iterations=200, relative_tolerance=1e-8,
-                 absolute_tolerance=1e-30, r_min=0.55, r_max=1.0, gca=0, outer=0, eager=False):
+                 absolute_tolerance=1e-30, r_min=0.55, r_max=1.0, gca=0, outer=0, eager=False,
+                 chebyshev_estimates=None):
+        """chebyshev_estimates: None (power iterations, as the reference) or one largest-eigenvalue estimate of
+        D^-1 A per multigrid level, coarsest first, used as given."""
+        est = None
+        if chebyshev_estimates is not None:
+            assert len(chebyshev_estimates) == mg_levels
+            self._est = (ctypes.c_double * mg_levels)(*[float(e) for e in chebyshev_estimates])
+            est = ctypes.cast(self._est, ctypes.POINTER(ctypes.c_double))
         self.prm = C.StokesParams(level, mg_levels, bc_cmb, bc_surface, int(mg_fp32), chebyshev_order, smoothing_steps,
                                   power_iterations, vcycles, coarse_max_iterations, coarse_relative_tolerance, restart,
                                   max_iterations, relative_tolerance, absolute_tolerance, int(gca), int(outer),
-                                  int(eager))
+                                  int(eager), est)
         h = ctypes.c_void_p()
         C.check(C.lib().tn_stokes_solver_create(ctypes.byref(self.prm), r_min, r_max,
                                                 ctypes.c_void_p(viscosity.data.data_ptr()), ctypes.byref(h)),

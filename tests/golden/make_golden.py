@@ -8,7 +8,8 @@ seeds below, and the fixture keeps their checksums so a drift in generation
 shows up as a failing check instead of a silent mismatch.
 
 Usage (in a container that has the reference sources and a built ref_dump):
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py               # ref_L2.npz
+    python tests/golden/make_golden.py --stokes-mg   # ref_stokes_mg_L4.npz (a few minutes on one thread)
 """
 import os
 import sys
@@ -139,6 +140,71 @@ def vcycle_rhs():
     """seeded right-hand side on the finest V-cycle level"""
     m = Mesh(VCYCLE["lmax"])
     return m.make_consistent(np.random.RandomState(31).normal(size=m.shape)).reshape(m.shape)
+
+
+# The app's Stokes solver stack (ref_dump stokes_mg): velocity level 4 / pressure level 3, 3 multigrid levels
+# (GCA coarse operators with constant interpolation at levels 3 and 2), Chebyshev order 3 with 2 sweeps and 10
+# power iterations, 1 V-cycle, coarse PCG(50, 1e-6), FGMRES(30) to 1e-8 (Dirichlet) / 1e-7 (free-slip: the
+# pressure's constant mode makes the system singular and the residual stalls near 9e-8); run on one thread,
+# where the smoothers' randomised eigenvalue estimates are reproducible (the fixture keeps them)
+STOKES_MG = dict(level=4, mg_levels=3, restart=30, maxit=300, order=3, steps=2, pits=10, vcycles=1, gca=1,
+                 cmaxit=50, bcs=[(1, 1), (2, 2)], tol={(1, 1): 1e-8, (2, 2): 1e-7})
+
+
+def stokes_mg_inputs(bcc, bcs):
+    """seeded 1e3-contrast viscosity (level 4), its injection to level 3, and a velocity right-hand side with
+    the boundary rows enforced (zero on Dirichlet layers, tangential on free-slip layers); zero pressure RHS"""
+    f = Mesh(STOKES_MG["level"])
+    rs = np.random.RandomState(4242)
+    x = f.coords[:, :, :, None, :] * f.radii[:, None, None, :, None]
+    ramp = np.broadcast_to(((f.radii - R_MIN) / (R_MAX - R_MIN))[:, None, None, :], f.shape)
+    blobs = np.zeros(f.shape)
+    for _ in range(6):
+        c = rs.normal(size=3)
+        c *= rs.uniform(R_MIN, R_MAX) / np.linalg.norm(c)
+        blobs += np.exp(-np.sum((x - c) ** 2, axis=-1) / (2 * 0.2 ** 2))
+    blobs /= blobs.max()
+    k = np.exp(np.log(1e3) * (0.5 * ramp + 0.5 * blobs))
+    kp = np.ascontiguousarray(k[:, ::2, ::2, ::2])
+    fu = f.make_consistent(rs.normal(size=(3,) + f.shape)).reshape((3,) + f.shape)
+    n = f.coords / np.linalg.norm(f.coords, axis=-1, keepdims=True)
+    for bc, r in ((bcc, 0), (bcs, -1)):
+        if bc == 1:
+            fu[..., r] = 0.0
+        elif bc == 2:
+            nn = np.moveaxis(n, -1, 0)
+            fu[..., r] -= np.sum(fu[..., r] * nn, axis=0) * nn
+    fp = np.zeros((10,) + (f.N // 2 + 1,) * 3)
+    return k, kp, fu, fp
+
+
+def make_stokes_mg():
+    """ref_stokes_mg_L4.npz: the reference's solution, residual history, iteration count and the eigenvalue
+    estimates its smoothers drew, for both boundary cases of STOKES_MG."""
+    S = STOKES_MG
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        for bcc, bcs in S["bcs"]:
+            k, kp, fu, fp = stokes_mg_inputs(bcc, bcs)
+            out[f"checksum_fu_{bcc}{bcs}"] = checksum(fu)
+            out["checksum_k"] = checksum(k)
+            k.tofile(f"{d}/k.bin")
+            kp.tofile(f"{d}/kp.bin")
+            fu.tofile(f"{d}/f_u.bin")
+            fp.tofile(f"{d}/f_p.bin")
+            info = run_ref(["stokes_mg", S["level"], S["mg_levels"], R_MIN, R_MAX, bcc, bcs, S["restart"], S["maxit"],
+                            S["tol"][(bcc, bcs)], S["order"], S["steps"], S["pits"], S["vcycles"], S["gca"], S["cmaxit"], d], d,
+                           threads=1, json_out=True)
+            # solutions kept in FP32 (the fixture's size; 6e-8 rounding, far below the comparison's tolerance)
+            out[f"x_u_{bcc}{bcs}"] = np.fromfile(f"{d}/x_u.bin").reshape(fu.shape).astype(np.float32)
+            out[f"x_p_{bcc}{bcs}"] = np.fromfile(f"{d}/x_p.bin").reshape(fp.shape).astype(np.float32)
+            out[f"hist_{bcc}{bcs}"] = np.fromfile(f"{d}/hist.bin")
+            out[f"iterations_{bcc}{bcs}"] = np.array(info["iterations"])
+            out[f"eigenvalues_{bcc}{bcs}"] = np.array(info["eigenvalues"])
+            print("stokes_mg", bcc, bcs, info)
+    path = os.path.join(HERE, "ref_stokes_mg_L4.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
 
 
 def checksum(a):
@@ -313,4 +379,7 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if "--stokes-mg" in sys.argv:
+        make_stokes_mg()
+    else:
+        main()

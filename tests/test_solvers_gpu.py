@@ -257,3 +257,77 @@ def test_stokes_refinement_rejects_fp64_multigrid(stokes_case):
     kv.set_numpy(k)
     with pytest.raises(RuntimeError, match="refinement"):
         shell.StokesSolver(L, kv, mg_levels=2, mg_fp32=False, outer=2)
+
+
+def _stokes_mg_fixture():
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden as G
+    return G, np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_stokes_mg_L4.npz"))
+
+
+@pytest.mark.parametrize("bc", [(1, 1), (2, 2)])
+@pytest.mark.parametrize("eager", [False, True])
+def test_stokes_production_stack_matches_reference(bc, eager):
+    """The app's Stokes solver stack (mantlecirculation.cpp:486-735) on the GPU in FP64, against the reference's
+    own (ref_dump stokes_mg, tests/golden/ref_stokes_mg_L4.npz): FGMRES(30), block-triangular preconditioner,
+    one V-cycle over levels 2-4 with Chebyshev order 3 (2 sweeps), GCA coarse operators (constant
+    interpolation), coarse PCG(50, 1e-6), lumped inverse KMass(1/eta) Schur block.  The smoothers use the
+    eigenvalue estimates the reference drew.  The same iteration count (+-2), the residual history to rounding
+    amplified by the Krylov process, and solutions within the tolerance's reach."""
+    from terraneo_b200 import shell
+    G, g = _stokes_mg_fixture()
+    S = G.STOKES_MG
+    k, kp, fu_np, fp_np = G.stokes_mg_inputs(*bc)
+    assert np.allclose(G.checksum(k), g["checksum_k"], rtol=1e-13, atol=0)
+    assert np.allclose(G.checksum(fu_np), g[f"checksum_fu_{bc[0]}{bc[1]}"], rtol=1e-13, atol=0)
+    L = S["level"]
+    pf, pc = shell.ShellMesh(L), shell.ShellMesh(L - 1)
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(k)
+    fu, fp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+    fu.set_numpy(fu_np)
+    fp.set_numpy(fp_np)
+    xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+    tol = S["tol"][bc]
+    s = shell.StokesSolver(L, kv, mg_levels=S["mg_levels"], bc_cmb=bc[0], bc_surface=bc[1], mg_fp32=False,
+                           chebyshev_order=S["order"], smoothing_steps=S["steps"], power_iterations=S["pits"],
+                           vcycles=S["vcycles"], coarse_max_iterations=S["cmaxit"], coarse_relative_tolerance=1e-6,
+                           restart=S["restart"], max_iterations=S["maxit"], relative_tolerance=tol, gca=S["gca"],
+                           eager=eager, chebyshev_estimates=g[f"eigenvalues_{bc[0]}{bc[1]}"])
+    it, rr = s.solve(fu, fp, xu, xp)
+    hist, _ = s.history()
+    ref_it = int(g[f"iterations_{bc[0]}{bc[1]}"])
+    ref_hist = g[f"hist_{bc[0]}{bc[1]}"]
+    assert abs(it - ref_it) <= 2, (it, ref_it)
+    assert rr <= tol
+    n = min(len(hist), len(ref_hist), 30)
+    np.testing.assert_allclose(hist[:n], ref_hist[:n], rtol=1e-6, atol=0)
+    xr = g[f"x_u_{bc[0]}{bc[1]}"].astype(np.float64)
+    assert rel(xu.numpy(), xr) <= 100 * tol, rel(xu.numpy(), xr)
+    if bc == (1, 1):  # free-slip both radii leaves the pressure's constant mode free
+        assert rel(xp.numpy()[0], g[f"x_p_{bc[0]}{bc[1]}"].astype(np.float64)) <= 100 * tol
+
+
+def test_stokes_production_stack_own_estimates_close_to_reference():
+    """The same Dirichlet solve with the smoothers' own power iterations (a deterministic start instead of the
+    reference's random one): the iteration count stays within 3 of the reference's."""
+    from terraneo_b200 import shell
+    G, g = _stokes_mg_fixture()
+    S = G.STOKES_MG
+    k, kp, fu_np, fp_np = G.stokes_mg_inputs(1, 1)
+    L = S["level"]
+    pf, pc = shell.ShellMesh(L), shell.ShellMesh(L - 1)
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(k)
+    fu, fp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+    fu.set_numpy(fu_np)
+    xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+    s = shell.StokesSolver(L, kv, mg_levels=S["mg_levels"], bc_cmb=1, bc_surface=1, mg_fp32=False,
+                           chebyshev_order=S["order"], smoothing_steps=S["steps"], power_iterations=S["pits"],
+                           vcycles=S["vcycles"], coarse_max_iterations=S["cmaxit"], coarse_relative_tolerance=1e-6,
+                           restart=S["restart"], max_iterations=S["maxit"], relative_tolerance=S["tol"][(1, 1)],
+                           gca=S["gca"])
+    it, rr = s.solve(fu, fp, xu, xp)
+    assert abs(it - int(g["iterations_11"])) <= 3, (it, int(g["iterations_11"]))
