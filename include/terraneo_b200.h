@@ -322,6 +322,7 @@ TN_API int tn_vec_invert_f32( const tn_mesh* mesh, int ncomp, float* const* y, v
 TN_API int tn_vec_mult_f64( const tn_mesh* mesh, int ncomp, double* const* y, const double* const* x, void* stream );
 TN_API int tn_vec_mult_f32( const tn_mesh* mesh, int ncomp, float* const* y, const float* const* x, void* stream );
 TN_API int tn_vec_max_abs_f64( const tn_mesh* mesh, int ncomp, const double* const* x, double* result, void* stream );
+TN_API int tn_vec_max_abs_f32( const tn_mesh* mesh, int ncomp, const float* const* x, double* result, void* stream );
 TN_API int tn_vec_has_nan_or_inf_f64( const tn_mesh* mesh, int ncomp, const double* const* x, int* result, void* stream );
 TN_API int tn_vec_has_nan_or_inf_f32( const tn_mesh* mesh, int ncomp, const float* const* x, int* result, void* stream );
 /* assign_masked_else_keep_old (kernels/common/grid_operations.hpp) with the

@@ -141,6 +141,7 @@ _SIGS = {
     "tn_vec_mult_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
     "tn_vec_mult_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
     "tn_vec_max_abs_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_double), c_void_p]),
+    "tn_vec_max_abs_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_double), c_void_p]),
     "tn_vec_has_nan_or_inf_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), c_void_p]),
     "tn_vec_has_nan_or_inf_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), c_void_p]),
     "tn_vec_dot_noalloc_f64": (c_int, [c_size_t, c_int, P(c_void_p), P(c_void_p), c_void_p, P(c_double), c_void_p]),

@@ -14,6 +14,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <memory>
 #include <stdexcept>
@@ -98,6 +99,7 @@ struct abi< double >
     static constexpr auto invert   = tn_vec_invert_f64;
     static constexpr auto mult     = tn_vec_mult_f64;
     static constexpr auto has_nan  = tn_vec_has_nan_or_inf_f64;
+    static constexpr auto max_abs  = tn_vec_max_abs_f64;
     static constexpr auto rand     = tn_vec_randomize_f64;
     static constexpr auto cheb     = tn_vec_chebyshev_step_f64;
     static constexpr auto halo     = tn_halo_sum_f64;
@@ -110,6 +112,7 @@ struct abi< float >
     static constexpr auto invert   = tn_vec_invert_f32;
     static constexpr auto mult     = tn_vec_mult_f32;
     static constexpr auto has_nan  = tn_vec_has_nan_or_inf_f32;
+    static constexpr auto max_abs  = tn_vec_max_abs_f32;
     static constexpr auto rand     = tn_vec_randomize_f32;
     static constexpr auto cheb     = tn_vec_chebyshev_step_f32;
     static constexpr auto halo     = tn_halo_sum_f32;
@@ -206,6 +209,13 @@ class VectorQ1Base
         check( detail::abi< T >::has_nan( mesh_.get(), NC, a, &r, stream() ), "has_nan_or_inf" );
         return r != 0;
     }
+    T max_abs_entry_impl() const
+    {
+        const T* a[3] = { comp( 0 ), NC > 1 ? comp( 1 ) : nullptr, NC > 2 ? comp( 2 ) : nullptr };
+        double   r    = 0;
+        check( detail::abi< T >::max_abs( mesh_.get(), NC, a, &r, stream() ), "max_abs_entry" );
+        return T( r );
+    }
     void swap_impl( VectorQ1Base& o ) { std::swap( buf_, o.buf_ ); }
     void halo_sum()
     {
@@ -274,6 +284,7 @@ class VectorQ1IsoQ2Q1
     }
     void randomize_impl() { u_.randomize_impl(), p_.randomize_impl(); }
     bool has_nan_or_inf_impl() const { return u_.has_nan_or_inf_impl() || p_.has_nan_or_inf_impl(); }
+    T    max_abs_entry_impl() const { return std::max( u_.max_abs_entry_impl(), p_.max_abs_entry_impl() ); }
     void swap_impl( VectorQ1IsoQ2Q1& o ) { u_.swap_impl( o.u_ ), p_.swap_impl( o.p_ ); }
 
   private:
@@ -331,7 +342,13 @@ void axpy_dot( const Segments< T >& w, const Segments< T >* x, const double* coe
         check( tn_krylov_axpy_dot_f32( w.n, w.mesh, w.f, px, coeff, pv, gate, result, stream() ), "axpy_dot" );
 }
 
-// free functions (linalg/vector.hpp:72-250)
+// free functions (linalg/vector.hpp:72-250, linalg/operator.hpp:156).  They live in
+// tn::fn, made visible inside tn by a using-directive: argument-dependent
+// lookup ignores using-directives, so the reference's own solver templates,
+// which call these names unqualified on tn vectors, find only the reference's
+// linalg:: overloads and run over this library's vectors and operators
+// unchanged.
+namespace fn {
 template < typename V >
 void lincomb( V& y, const std::vector< typename V::ScalarType >& c, const std::vector< V >& x,
               typename V::ScalarType c0 = 0 )
@@ -390,6 +407,8 @@ void solve( Solver& s, Op& A, X& x, const B& b )
 {
     s.solve_impl( A, x, b );
 }
+}  // namespace fn
+using namespace fn;
 
 // One fused Chebyshev step: d = alpha D^{-1} (b - ax) + beta d, x += d
 template < typename T, int NC >

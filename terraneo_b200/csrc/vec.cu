@@ -447,18 +447,27 @@ extern "C" int tn_vec_mult_f32( const tn_mesh* m, int ncomp, float* const* y, co
 {
     return vec_elementwise< float, 1 >( m, ncomp, y, x, as_stream( s ) );
 }
-extern "C" int tn_vec_max_abs_f64( const tn_mesh* m, int ncomp, const double* const* x, double* result, void* s )
+template < typename T >
+static int max_abs( const tn_mesh* m, int ncomp, const T* const* x, double* result, void* s )
 {
     TN_CHECK_ARG( m && result, "max_abs: bad arguments" );
-    Ptr3< const double > px;
-    int                  rc;
+    Ptr3< const T > px;
+    int             rc;
     if ( ( rc = ptr3c( ncomp, x, px, "max_abs" ) ) )
         return rc;
     const unsigned blocks = std::min< unsigned >( grid_for( m->ns * ncomp, 8 ), kRedMaxBlocks );
-    max_abs_kernel< double ><<< blocks, kThreads, 0, as_stream( s ) >>>( m->ns, ncomp, px, m->d_red_partials,
-                                                                        m->d_red_counter, m->d_red_result );
+    max_abs_kernel< T ><<< blocks, kThreads, 0, as_stream( s ) >>>( m->ns, ncomp, px, m->d_red_partials,
+                                                                   m->d_red_counter, m->d_red_result );
     TN_LAUNCH_CHECK();
     return fetch_result( m, 1, as_stream( s ), result );
+}
+extern "C" int tn_vec_max_abs_f64( const tn_mesh* m, int ncomp, const double* const* x, double* result, void* s )
+{
+    return max_abs< double >( m, ncomp, x, result, s );
+}
+extern "C" int tn_vec_max_abs_f32( const tn_mesh* m, int ncomp, const float* const* x, double* result, void* s )
+{
+    return max_abs< float >( m, ncomp, x, result, s );
 }
 template < typename T >
 static int has_nan( const tn_mesh* m, int ncomp, const T* const* x, int* result, void* s )

@@ -193,3 +193,21 @@ def test_stokes_solve_true_residual_at_level6(meshes):
     shell.lincomb(kp, [1.0, -1.0], [fp, kp])
     true_rr = np.sqrt(shell.dot(ku, ku) + shell.dot(kp, kp)) / np.sqrt(shell.dot(fu, fu))
     assert rr <= 1e-8 and true_rr <= 2e-8, (it, rr, true_rr)
+
+
+def test_freeslip_apply_matches_oracle_at_level7():
+    """Level 7 (N = 128: four 32-cell radial chunks per column, the time-step configuration), free-slip on both
+    radii with the rigid-rotation penalty: the FP64 apply against the oracle.  Every radial chunk seam (levels
+    32, 64, 96) carries partial sums and the penalty from one chunk to the next."""
+    from terraneo_b200 import shell
+    L7 = 7
+    om = Mesh(L7)
+    rng = np.random.default_rng(77)
+    k_np = np.exp(rng.uniform(0.0, 2.0, size=om.shape))
+    u_np = om.make_consistent(rng.normal(size=(3,) + om.shape)).reshape((3,) + om.shape)
+    pf = shell.ShellMesh(L7)
+    k, u, y = shell.VectorQ1Scalar(pf), shell.VectorQ1Vec(pf), shell.VectorQ1Vec(pf)
+    k.set_numpy(k_np)
+    u.set_numpy(u_np)
+    shell.apply(shell.EpsilonDivDivKerngen(pf, k, 2, 2), u, y)
+    assert rel(y.numpy(), om.kerngen(k_np, u_np, 2, 2, False)) <= TOL

