@@ -9,9 +9,10 @@
 //
 // Every kernel runs one thread per interior cell, r fastest.  The cell
 // geometry (face fluxes beta, face vectors S, volume M) is recomputed from the
-// wedge map and the Q1 velocity in FP64 in the dt and predictor kernels, as
-// the reference does: 6 faces x (3 or 4) quadrature points per wedge face
-// plus the 3x2 volume rule, instead of storing ~150 values per cell.
+// wedge map and the Q1 velocity in FP64 in the dt and predictor kernels, with
+// the reference's face and volume quadrature sums evaluated in closed form
+// (fv_geometry).  The antidiffusive fluxes are stored as six planes (SoA),
+// F[n * nf + i] for neighbour n of cell i.
 #include "common.cuh"
 #include "wedge.cuh"
 
@@ -43,104 +44,104 @@ __device__ __forceinline__ void cross3( const double a[3], const double b[3], do
     c[0] = a[1] * b[2] - a[2] * b[1], c[1] = a[2] * b[0] - a[0] * b[2], c[2] = a[0] * b[1] - a[1] * b[0];
 }
 
-// GeometryHelper::compute_geometry (geometry_helper.hpp:180-363)
+// GeometryHelper::compute_geometry (geometry_helper.hpp:180-363) in closed form.
+//
+// The reference integrates each face of the two wedges of the cell with a
+// quadrature rule over the wedge map x = r(zeta) (p0 + xi a + eta b),
+// a = p1 - p0, b = p2 - p0, r(zeta) = r1 + h (1 + zeta), h = (r2 - r1) / 2, and
+// the Q1 velocity u(q) = sum_i N_i(q) u_i: beta = sum_q w_q u(q) . n(q),
+// S = sum_q w_q n(q), and M = sum over the 3x2 volume rule of |det J| / 6.  On
+// this map every such sum has a closed form:
+//   * the radial triangles zeta = -+1 (neighbours 4, 5; 3-point rule, 1/6
+//     weights): n = r^2 (a x b) is constant, each lateral shape function sums
+//     to 1 over the points, so beta = r^2 / 6 (a x b) . (u_0 + u_1 + u_2) of
+//     the face's nodes and S = r^2 / 2 (a x b);
+//   * the quad xi = 0 (2x2 Gauss, weights 1/2 on [0,1] x [-1,1]): n = r(zeta)
+//     h (b x p0), so beta = h (b x p0) . (R_b (u_0 + u_2) + R_t (u_3 + u_5)),
+//     S = (r(-g) + r(g)) h (b x p0), with g = 1/sqrt(3),
+//     R_b = (r(-g) (1 + g) + r(g) (1 - g)) / 4 and R_t = (r(-g) (1 - g) +
+//     r(g) (1 + g)) / 4 the Gauss sums of r(zeta) times the bottom / top
+//     radial shape functions; the quad eta = 0 alike with a in place of b and
+//     nodes 1, 4 in place of 2, 5;
+//   * det J = r(zeta)^2 h (a x b) . p0, so M = sum_w h |(a x b) . p0|
+//     (r(-g)^2 + r(g)^2) / 2.
+// These are the same sums (exact algebra, different rounding: ~1e-16
+// relative), about 150 FP64 operations per cell instead of ~3,000.  Every face
+// is then oriented from this cell towards the neighbour's centre.
 __device__ void fv_geometry( const FvGeom& G, int d, int x, int y, int r, double beta[6], double& Mii, double S[6][3] )
 {
     const int    N = G.N, n1 = N + 1, n2 = N + 2;
     const double r1 = G.radii[d * n1 + r - 1], r2 = G.radii[d * n1 + r];
-    const double g1 = -0.5773502691896258, g2 = 0.5773502691896258; // -+ 1 / sqrt(3)
+    const double g  = 0.5773502691896258; // 1 / sqrt(3)
+    const double h  = 0.5 * ( r2 - r1 );
+    const double rm = r1 + h * ( 1.0 - g ), rp = r1 + h * ( 1.0 + g ); // r(-g), r(+g)
+    const double Rb = 0.25 * ( rm * ( 1.0 + g ) + rp * ( 1.0 - g ) ), Rt = 0.25 * ( rm * ( 1.0 - g ) + rp * ( 1.0 + g ) );
+    const double rs = rm + rp, r1s = r1 * r1, r2s = r2 * r2;
+#pragma unroll
     for ( int n = 0; n < 6; ++n )
     {
         beta[n] = 0.0;
         S[n][0] = S[n][1] = S[n][2] = 0.0;
     }
     Mii = 0.0;
+#pragma unroll
     for ( int w = 0; w < 2; ++w )
     {
         double p[3][3], u[6][3];
+#pragma unroll
         for ( int i = 0; i < 6; ++i )
         {
             const size_t lat = lat_index( n1, d, x - 1 + kWedgeNode[w][i][0], y - 1 + kWedgeNode[w][i][1] );
             if ( i < 3 )
-                for ( int a = 0; a < 3; ++a )
-                    p[i][a] = G.coords[lat * 3 + a];
+#pragma unroll
+                for ( int c = 0; c < 3; ++c )
+                    p[i][c] = G.coords[lat * 3 + c];
             const size_t id = lat * n1 + r - 1 + kWedgeNode[w][i][2];
-            for ( int a = 0; a < 3; ++a )
-                u[i][a] = G.vel.p[a][id];
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+                u[i][c] = G.vel.p[c][id];
         }
-        // faces of this wedge: quads 0, 2 (wedge 0) or 1, 3 (wedge 1); radial triangles 4, 5
-        for ( int f = 0; f < 4; ++f )
+        double va[3], vb[3], ab[3], bp[3], ap[3];
+#pragma unroll
+        for ( int c = 0; c < 3; ++c )
+            va[c] = p[1][c] - p[0][c], vb[c] = p[2][c] - p[0][c];
+        cross3( va, vb, ab );
+        cross3( vb, p[0], bp );
+        cross3( va, p[0], ap );
+        const int nx = w == 0 ? 0 : 1, ny = w == 0 ? 2 : 3; // the wedge's xi = 0 and eta = 0 faces
+        double    bx = 0.0, by = 0.0, bl = 0.0, bt = 0.0;
+#pragma unroll
+        for ( int c = 0; c < 3; ++c )
         {
-            const int  nb   = f < 2 ? ( w == 0 ? 2 * f : 2 * f + 1 ) : f + 2;
-            const bool quad = f < 2;
-            const int  nq   = quad ? 4 : 3;
-            for ( int q = 0; q < nq; ++q )
-            {
-                double s, t, wq;
-                if ( quad )
-                    s = 0.5 * ( ( q >> 1 ? g2 : g1 ) + 1.0 ), t = ( q & 1 ) ? g2 : g1, wq = 0.5;
-                else
-                {
-                    s  = q == 0 ? 0.6666666666666666 : 0.1666666666666667;
-                    t  = q == 1 ? 0.6666666666666666 : 0.1666666666666667;
-                    wq = 0.1666666666666667;
-                }
-                double xi, eta, zeta;
-                if ( nb < 2 )
-                    xi = 0.0, eta = s, zeta = t;
-                else if ( nb < 4 )
-                    xi = s, eta = 0.0, zeta = t;
-                else
-                    xi = s, eta = t, zeta = nb == 4 ? -1.0 : 1.0;
-                double dxi[3] = { 0, 0, 0 }, deta[3] = { 0, 0, 0 }, dzeta[3] = { 0, 0, 0 }, uq[3] = { 0, 0, 0 };
-                const double lat[3] = { 1.0 - xi - eta, xi, eta };
-                for ( int i = 0; i < 6; ++i )
-                {
-                    double gr[3];
-                    grad_shape_ref( i, xi, eta, zeta, gr );
-                    const double sh = lat[i % 3] * ( i < 3 ? 0.5 * ( 1.0 - zeta ) : 0.5 * ( 1.0 + zeta ) );
-                    const double rr = i < 3 ? r1 : r2;
-                    for ( int a = 0; a < 3; ++a )
-                    {
-                        const double xa = p[i % 3][a] * rr;
-                        dxi[a] += gr[0] * xa;
-                        deta[a] += gr[1] * xa;
-                        dzeta[a] += gr[2] * xa;
-                        uq[a] += sh * u[i][a];
-                    }
-                }
-                double nv[3];
-                if ( nb >= 4 )
-                    cross3( dxi, deta, nv );
-                else if ( nb >= 2 )
-                    cross3( dxi, dzeta, nv );
-                else
-                    cross3( deta, dzeta, nv );
-                beta[nb] += wq * ( uq[0] * nv[0] + uq[1] * nv[1] + uq[2] * nv[2] );
-                for ( int a = 0; a < 3; ++a )
-                    S[nb][a] += wq * nv[a];
-            }
+            bx += bp[c] * ( Rb * ( u[0][c] + u[2][c] ) + Rt * ( u[3][c] + u[5][c] ) );
+            by += ap[c] * ( Rb * ( u[0][c] + u[1][c] ) + Rt * ( u[3][c] + u[4][c] ) );
+            bl += ab[c] * ( u[0][c] + u[1][c] + u[2][c] );
+            bt += ab[c] * ( u[3][c] + u[4][c] + u[5][c] );
+            S[nx][c] += rs * h * bp[c];
+            S[ny][c] += rs * h * ap[c];
+            S[4][c] += 0.5 * r1s * ab[c];
+            S[5][c] += 0.5 * r2s * ab[c];
         }
-        for ( int q = 0; q < 6; ++q )
-        {
-            const double xi = q % 3 == 0 ? 0.6666666666666666 : 0.1666666666666667;
-            const double et = q % 3 == 1 ? 0.6666666666666666 : 0.1666666666666667;
-            const double ze = q < 3 ? -0.5773502691896257 : 0.5773502691896257;
-            double       IT[3][3];
-            const double det = wedge_jacobian_it( p[0], p[1], p[2], r1, r2, xi, et, ze, IT );
-            Mii += fabs( det ) * 0.1666666666666667;
-        }
+        beta[nx] += h * bx;
+        beta[ny] += h * by;
+        beta[4] += r1s / 6.0 * bl;
+        beta[5] += r2s / 6.0 * bt;
+        const double D = ab[0] * p[0][0] + ab[1] * p[0][1] + ab[2] * p[0][2];
+        Mii += 0.5 * h * fabs( D ) * ( rm * rm + rp * rp );
     }
     // orient every face from this cell towards the neighbour's centre
     const size_t ci = fv_index( n2, d, x, y, r );
+#pragma unroll
     for ( int nb = 0; nb < 6; ++nb )
     {
         const size_t cj = fv_index( n2, d, x + kFvOff[nb][0], y + kFvOff[nb][1], r + kFvOff[nb][2] );
         double       dc = 0.0;
+#pragma unroll
         for ( int a = 0; a < 3; ++a )
             dc += S[nb][a] * ( G.cen.p[a][cj] - G.cen.p[a][ci] );
         if ( dc < 0 )
         {
+#pragma unroll
             for ( int a = 0; a < 3; ++a )
                 S[nb][a] = -S[nb][a];
             beta[nb] = -beta[nb];
@@ -265,6 +266,7 @@ __global__ void __launch_bounds__( kFvThreads )
     double    beta[6], Mii, S[6][3];
     fv_geometry( G, d, x, y, r, beta, Mii, S );
     const size_t i  = fv_index( n2, d, x, y, r );
+    const size_t nf = size_t( kDiamonds ) * n2 * n2 * n2; // F holds 6 planes of nf (SoA)
     const double Ti = T[i];
     double       lo_diag = 0.0, lo_update = 0.0, bsum = 0.0;
     for ( int n = 0; n < 6; ++n )
@@ -285,7 +287,7 @@ __global__ void __launch_bounds__( kFvThreads )
         const double dc = kappa * ( ss / den );
         lo_diag += dc;
         lo_update -= dc * Tj;
-        F[i * 6 + n] = ( dt / Mii ) * ( fabs( beta[n] ) / 2.0 ) * ( Ti - Tj );
+        F[n * nf + i] = ( dt / Mii ) * ( fabs( beta[n] ) / 2.0 ) * ( Ti - Tj );
     }
     if ( subtract_divergence )
         lo_diag -= bsum;
@@ -319,11 +321,12 @@ __global__ void __launch_bounds__( kFvThreads ) limiter_kernel( int N, const dou
         return;
     const int    n2 = N + 2;
     const size_t i  = fv_index( n2, d, x, y, r );
+    const size_t nf = size_t( kDiamonds ) * n2 * n2 * n2;
     const double ti = TL[i];
     double       Pp = 0.0, Pm = 0.0, tmax = ti, tmin = ti;
     for ( int n = 0; n < 6; ++n )
     {
-        const double f = F[i * 6 + n];
+        const double f = F[n * nf + i];
         if ( f > 0 )
             Pp += f;
         else
@@ -346,11 +349,12 @@ __global__ void __launch_bounds__( kFvThreads )
         return;
     const int    n2 = N + 2;
     const size_t i  = fv_index( n2, d, x, y, r );
+    const size_t nf = size_t( kDiamonds ) * n2 * n2 * n2;
     double       corr = 0.0;
     for ( int n = 0; n < 6; ++n )
     {
         const size_t j  = fv_index( n2, d, x + kFvOff[n][0], y + kFvOff[n][1], r + kFvOff[n][2] );
-        const double f  = F[i * 6 + n];
+        const double f  = F[n * nf + i];
         const double al = f > 0 ? fmin( Rp[i], Rm[j] ) : fmin( Rm[i], Rp[j] );
         corr += al * f;
     }

@@ -101,8 +101,8 @@ __device__ __forceinline__ void wedge_flux( const T* __restrict__ g, const T v1[
 // X gets its two halves from strips X (left side) and X-1 (right side); right
 // halves are exchanged through shared memory, one barrier per step.  Node rows
 // (the CTA's kW+1 columns x 3 src components + k x 33 levels) are streamed
-// into a 4-slot shared-memory ring with cp.async three rows ahead, so global
-// latency overlaps the arithmetic of the previous steps.  The radial chunk
+// into a 4-slot shared-memory ring with cp.async three rows ahead (fill_row),
+// so global latency overlaps the arithmetic of the previous steps.  The radial chunk
 // boundary level r0 + 32 is carried to the next chunk in shared memory.
 constexpr int kLev   = kRC + 1; // node levels per chunk
 constexpr int kSlots = 4;       // row ring depth (prefetch distance 3)
@@ -116,32 +116,60 @@ size_t tile_smem_bytes( int n1, int SY )
     const size_t xbuf  = size_t( 2 ) * kW * 3 * kLev;
     const size_t carry = size_t( kW + 1 ) * ( SY + 2 ) * 3;
     const size_t top   = size_t( kW ) * 2 * 4 * 3;
-    return sizeof( T ) * ( radii + geo + rows + xbuf + carry + top );
+    return sizeof( T ) * ( radii + geo + rows + xbuf + carry + top ) + 16 + 32 * kThreads; // + fill descriptors
 }
 
-// Stream node row Y (the CTA's kW+1 columns, 3 src components + k, levels
-// r0..r0+RC) into a ring slot: warp w copies the (column, field) pairs
-// w, w+kW, ...; lane l copies level l, lane 0 also level 32.
-template < typename T >
-__device__ __forceinline__ void issue_row( const T* f0, const T* f1, const T* f2, const T* f3, int N, int n1, T* slot,
-                                           int d, int sx0, int Y, int r0, int RC, int lane, int warp )
+// Row fill.  A ring slot holds one node row of the CTA's kW+1 columns, stored
+// [field][column][level] (fields: 3 src components, k).  The threads form 4
+// groups of kThreads / 4, one per field; a thread copies elements t, t + 72,
+// ... of its field's (kW+1) x kLev block, each a fixed (column, level) whose
+// 32-bit element offset advances by one node row (n1) per step, so a fill costs
+// one offset add and one 8-byte cp.async per element.  The offsets of the
+// chunk's first row live in shared memory (2 x 16 bytes per thread) and hold
+// no registers across the wedge arithmetic.  Columns outside the diamond and
+// levels past the chunk are not copied; rows outside the diamond not at all
+// (no contributing cell reads them).
+constexpr int kGroup   = kThreads / 4;
+constexpr int kFieldEl = ( kW + 1 ) * kLev;
+constexpr int kFillPer = ( kFieldEl + kGroup - 1 ) / kGroup;
+
+__device__ __forceinline__ void fill_setup( uint4* desc, int N, int n1, int d, int X0, int Y0, int r0, int RC )
 {
+    static_assert( kFillPer == 5, "descriptor layout" );
+    const int t = threadIdx.x % kGroup;
+    unsigned  off[kFillPer], valid = 0;
+#pragma unroll
+    for ( int i = 0; i < kFillPer; ++i )
+    {
+        const int  j   = t + i * kGroup;
+        const int  col = j / kLev, lev = j - col * kLev;
+        const int  X   = X0 + col;
+        const bool ok  = j < kFieldEl && X >= 0 && X <= N && lev <= RC;
+        off[i]         = ok ? unsigned( ( ( d * n1 + X ) * n1 + Y0 ) * n1 + r0 + lev ) : 0u;
+        valid |= ok ? ( 1u << i ) : 0u;
+    }
+    desc[2 * threadIdx.x]     = make_uint4( off[0], off[1], off[2], off[3] );
+    desc[2 * threadIdx.x + 1] = make_uint4( off[4], valid, 0u, 0u );
+}
+
+// node row Y = Y0 + step into `slot`
+template < typename T >
+__device__ __forceinline__ void fill_row( const uint4* desc, const T* f0, const T* f1, const T* f2, const T* f3, T* slot,
+                                          int step, int Y, int N, int n1 )
+{
+    const int      f = threadIdx.x / kGroup, t = threadIdx.x - f * kGroup;
+    const T*       fb = f == 0 ? f0 : ( f == 1 ? f1 : ( f == 2 ? f2 : f3 ) );
+    const uint4    a = desc[2 * threadIdx.x], b = desc[2 * threadIdx.x + 1];
+    const unsigned off[kFillPer] = { a.x, a.y, a.z, a.w, b.x };
+    const unsigned valid         = b.y;
     if ( Y < 0 || Y > N )
         return;
-    for ( int p = warp; p < ( kW + 1 ) * 4; p += kW )
-    {
-        const int col = p >> 2, f = p & 3;
-        const int X   = sx0 + col;
-        if ( X < 0 || X > N )
-            continue;
-        const T* src = ( f == 0 ? f0 : ( f == 1 ? f1 : ( f == 2 ? f2 : f3 ) ) ) +
-                       ( lat_index( n1, d, X, Y ) * n1 + r0 );
-        T* dst = slot + p * kLev;
-        if ( lane <= RC )
-            __pipeline_memcpy_async( dst + lane, src + lane, sizeof( T ) );
-        if ( lane == 0 && RC == kRC )
-            __pipeline_memcpy_async( dst + kRC, src + kRC, sizeof( T ) );
-    }
+    const unsigned adv = unsigned( step * n1 );
+    T*             dst = slot + f * kFieldEl + t;
+#pragma unroll
+    for ( int i = 0; i < kFillPer; ++i )
+        if ( t + i * kGroup < kFieldEl && ( valid >> i & 1u ) )
+            __pipeline_memcpy_async( dst + i * kGroup, fb + ( off[i] + adv ), sizeof( T ) );
 }
 
 template < typename T >
@@ -161,6 +189,8 @@ __global__ void __launch_bounds__( kThreads, TN_TILE_MINBLOCKS ) kerngen_tile_ke
     T* s_xbuf  = s_rows + kSlots * ( kW + 1 ) * 4 * kLev;
     T* s_carry = s_xbuf + 2 * kW * 3 * kLev;
     T* s_top   = s_carry + ( kW + 1 ) * ( SM + 2 ) * 3; // [w][parity][corner][c]: top contributions of lane RC-1
+    uint4* s_fill = reinterpret_cast< uint4* >( ( reinterpret_cast< uintptr_t >( s_top + kW * 24 ) + 15 ) &
+                                                ~uintptr_t( 15 ) ); // fill descriptors, 16-byte aligned
     auto slot  = [s_rows]( int y ) { return s_rows + ( ( y + kSlots ) % kSlots ) * ( ( kW + 1 ) * 4 * kLev ); };
 
     for ( int i = threadIdx.x; i < 10 * n1; i += blockDim.x )
@@ -227,9 +257,10 @@ __global__ void __launch_bounds__( kThreads, TN_TILE_MINBLOCKS ) kerngen_tile_ke
                 lane_ok = false;
 
             const int cyb = row_lo - 1 + s0;
+            fill_setup( s_fill, N, n1, d, sx0, cyb, r0, RC );
             for ( int j = 0; j < kSlots - 1; ++j )
             {
-                issue_row( f0, f1, f2, f3, N, n1, slot( cyb + j ), d, sx0, cyb + j, r0, RC, lane, w );
+                fill_row( s_fill, f0, f1, f2, f3, slot( cyb + j ), j, cyb + j, N, n1 );
                 __pipeline_commit();
             }
             __pipeline_wait_prior( kSlots - 3 );
@@ -250,23 +281,26 @@ __global__ void __launch_bounds__( kThreads, TN_TILE_MINBLOCKS ) kerngen_tile_ke
             {
                 const int  cy      = row_lo - 1 + s;
                 const bool cell_ok = strip_ok && cy <= N - 1;
+                // row cy + 3 into the slot of row cy - 1, which every warp finished reading before the last
+                // barrier; issued here, where few registers are live
+                fill_row( s_fill, f0, f1, f2, f3, slot( cy + kSlots - 1 ), cy + kSlots - 1 - cyb, cy + kSlots - 1, N, n1 );
                 T          L[3], R[3];
                 {
                     // corners: 0 = (X, cy), 1 = (X+1, cy), 2 = (X, cy+1), 3 = (X+1, cy+1)
-                    const T* rp = slot( cy ) + w * 4 * kLev;
-                    const T* rn = slot( cy + 1 ) + w * 4 * kLev;
+                    const T* rp = slot( cy ) + w * kLev;
+                    const T* rn = slot( cy + 1 ) + w * kLev;
                     T        S[4][3], D[4][3], K[4];
 #pragma unroll
                     for ( int q = 0; q < 4; ++q )
                     {
-                        const T* base = ( q < 2 ? rp : rn ) + ( q & 1 ) * 4 * kLev;
+                        const T* base = ( q < 2 ? rp : rn ) + ( q & 1 ) * kLev;
 #pragma unroll
                         for ( int c = 0; c < 3; ++c )
                         {
-                            const T bv = base[c * kLev + lb], tv = base[c * kLev + lb + 1];
+                            const T bv = base[c * kFieldEl + lb], tv = base[c * kFieldEl + lb + 1];
                             S[q][c] = bv + tv, D[q][c] = tv - bv;
                         }
-                        K[q] = base[3 * kLev + lb] + base[3 * kLev + lb + 1];
+                        K[q] = base[3 * kFieldEl + lb] + base[3 * kFieldEl + lb + 1];
                     }
                     const T* g0 = s_geo + ( ( w * ( SM + 2 ) + s ) * 2 ) * 10;
                     const T* g1 = g0 + 10;
@@ -327,7 +361,6 @@ __global__ void __launch_bounds__( kThreads, TN_TILE_MINBLOCKS ) kerngen_tile_ke
                     for ( int c = 0; c < 3; ++c )
                         xb[c * kLev + RC] = tcur[3 + c] + tprv[9 + c];
                 }
-                issue_row( f0, f1, f2, f3, N, n1, slot( cy + kSlots - 1 ), d, sx0, cy + kSlots - 1, r0, RC, lane, w );
                 __pipeline_commit();
                 __pipeline_wait_prior( kSlots - 3 );
                 __syncthreads();
