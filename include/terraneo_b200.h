@@ -557,6 +557,30 @@ TN_API int tn_stokes_viscosity_backward( tn_stokes_solver* solver, const double*
                                          int* iterations );
 TN_API int tn_stokes_solver_destroy( tn_stokes_solver* solver );
 
+/* Pieces of the mantle-circulation time step (apps/mantlecirculation/mantlecirculation.cpp:870-1045).
+ * tn_fv_to_fe_rhs_f64: b_i = sum_K fv_K int_K phi_i (fv: FV field [10][N+2]^3 with ghosts) and / or the lumped
+ * diagonal D_i = sum_K int_K phi_i over the FV cells K (3x2 rule), both summed over node copies
+ * (fv/hex/conversion.hpp:146-190); either output may be NULL (b needs fv). */
+TN_API int tn_fv_to_fe_rhs_f64( const tn_mesh* mesh, const double* fv, double* b, double* lumped_diagonal, void* stream );
+/* FV -> FE transfer (l2_project_fv_to_fe, conversion.hpp:131-205, and l2_project_fv_to_fe_lumped, :243-300):
+ * lumped = 0 solves M dst = b with the unpreconditioned PCG on the Q1 mass matrix starting from dst's values
+ * (the reference uses max_iterations 1000, tolerances 1e-12 / 1e-12); lumped != 0 sets dst = b / D.  work: 5
+ * stored-node fields (2 for the lumped form).  iterations (optional): PCG iterations. */
+TN_API int tn_l2_project_fv_to_fe_f64( const tn_mesh* mesh, const double* fv, double* dst, int lumped, int max_iterations,
+                                       double relative_tolerance, double absolute_tolerance, double* work,
+                                       int* iterations, void* stream );
+/* Stokes buoyancy right-hand side (RHSVelocityInterpolator, mantlecirculation.cpp:117-150, and :883-899):
+ * f_u = VectorMass (rayleigh T n), n the unit radial direction, then zero velocity rows on Dirichlet boundaries
+ * (strong_algebraic_homogeneous_velocity_dirichlet_enforcement_stokes_like) and the normal component removed on
+ * free-slip ones (strong_algebraic_freeslip_enforcement_in_place), each on the boundary the app passes: the first
+ * with that condition (CMB before SURFACE), so the same condition on both radii treats only the CMB rows.
+ * T: FE scalar; work: 3 stored-node fields. */
+TN_API int tn_stokes_buoyancy_rhs_f64( const tn_mesh* mesh, const double* T, double rayleigh, int bc_cmb,
+                                       int bc_surface, double* const* f_u, double* work, void* stream );
+/* Pressure normalisation (mantlecirculation.cpp:930-936): p -= sum over owned nodes of p / unique nodes.
+ * work: one stored-node field; mean (optional) receives the subtracted value.  Synchronises. */
+TN_API int tn_pressure_remove_mean_f64( const tn_mesh* mesh, double* p, double* work, double* mean, void* stream );
+
 #ifdef __cplusplus
 }
 #endif

@@ -2030,3 +2030,50 @@ void or_epsdivdiv3x2_apply( int L, const double* coords, const double* radii, co
     or_halo_sum( L, coords, dst, 3 );
 }
 
+
+/* l2_project_fv_to_fe right-hand side (fv/hex/conversion.hpp:146-190): for every FV cell K (ghosts excluded),
+   b_i += fv_K sum_q shape_i(q) |det J(q)| w_q over the 3x2 Felippa rule on each of the cell's two wedges, and
+   the lumped diagonal D_i += sum_q shape_i(q) |det J(q)| w_q (l2_project_fv_to_fe_lumped, :243-300); then the
+   node copies summed (communication::shell::send_recv).  fv [10][N+2]^3; b, D stored-node fields (either NULL). */
+void or_fv_to_fe_rhs( int L, const double* coords, const double* radii, const double* fv, double* b, double* D )
+{
+    const int    N = 1 << L, n1 = N + 1, n2 = N + 2;
+    const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1;
+    if ( b )
+        memset( b, 0, ns * sizeof( double ) );
+    if ( D )
+        memset( D, 0, ns * sizeof( double ) );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 1; x <= N; ++x )
+            for ( int y = 1; y <= N; ++y )
+                for ( int r = 1; r <= N; ++r )
+                {
+                    const double v  = fv ? fv[fv_idx( n2, d, x, y, r )] : 0.0;
+                    const double r1 = radii[d * n1 + r - 1], r2 = radii[d * n1 + r];
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const double* p[3];
+                        wedge_lateral_points( n1, coords, d, x - 1, y - 1, w, p );
+                        for ( int i = 0; i < 6; ++i )
+                        {
+                            double acc = 0.0;
+                            for ( int q = 0; q < 6; ++q )
+                            {
+                                double J[3][3];
+                                wedge_jac( p, r1, r2, QP32[q][0], QP32[q][1], QP32[q][2], J );
+                                acc += shape_val( i, QP32[q][0], QP32[q][1], QP32[q][2] ) * fabs( det3( J ) ) * QW32;
+                            }
+                            const size_t id = node_idx( n1, d, x - 1 + WNODE[w][i][0], y - 1 + WNODE[w][i][1],
+                                                        r - 1 + WNODE[w][i][2] );
+                            if ( b )
+                                b[id] += acc * v;
+                            if ( D )
+                                D[id] += acc;
+                        }
+                    }
+                }
+    if ( b )
+        or_halo_sum( L, coords, b, 1 );
+    if ( D )
+        or_halo_sum( L, coords, D, 1 );
+}

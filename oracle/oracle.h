@@ -33,6 +33,7 @@ void or_boundary_mask( int L, uint8_t* bmask );
 void or_ownership_mask( int L, const double* coords, uint8_t* omask );
 /* duplicated-node additive reduction (halo SUM) of ncomp scalar fields */
 void or_halo_sum( int L, const double* coords, double* field, int ncomp );
+void or_fv_to_fe_rhs( int L, const double* coords, const double* radii, const double* fv, double* b, double* D );
 
 /* operators (Replace mode, additive communication) */
 void or_kerngen_apply( int L, const double* coords, const double* radii, const double* k, const double* src,

@@ -49,10 +49,13 @@
 //                                          Chebyshev multigrid with GCA coarse operators, coarse PCG) on
 //                                          k.bin / kp.bin / f_u.bin / f_p.bin: x_u, x_p, hist, JSON (iterations,
 //                                          seconds, per-level Chebyshev eigenvalue estimates)
+//   l2proj L rmin rmax lumped DIR  FV -> FE transfer of fv.bin (consistent mass + PCG, or lumped): x.bin
+//   stokes_rhs L rmin rmax Ra bcc bcs DIR  buoyancy right-hand side of T.bin (FE): f_u.bin
 //   kerngen_slow L rmin rmax bcc bcs diag DIR  the kerngen slow path on the reference's own assembled
 //                                          wedge matrices (written to mats.bin) stored in Full mode
 //   vlaplace L rmin rmax bcc bcs diag DIR  VectorLaplace<double>
-//   time_kerngen L rmin rmax bcc bcs reps prints seconds per apply (CPU baseline)
+//   time_kerngen L rmin rmax bcc bcs reps [DIR]  prints seconds per apply (CPU baseline); with DIR the
+//                                          inputs are k.bin / src.bin there, else k = 1, src = 1
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -76,6 +79,9 @@
 #include "fe/wedge/operators/shell/restriction_constant.hpp"
 #include "fe/wedge/operators/shell/restriction_linear.hpp"
 #include "fe/wedge/operators/shell/vector_laplace.hpp"
+#include "fe/strong_algebraic_dirichlet_enforcement.hpp"
+#include "fe/strong_algebraic_freeslip_enforcement.hpp"
+#include "fv/hex/conversion.hpp"
 #include "fv/hex/helpers.hpp"
 #include "fv/hex/operators/fct_advection_diffusion.hpp"
 #include "grid/bit_masks.hpp"
@@ -220,13 +226,21 @@ int cmd_kerngen( int L, double rmin, double rmax, int bcc, int bcs, int diag, co
     return 0;
 }
 
-int cmd_time_kerngen( int L, double rmin, double rmax, int bcc, int bcs, int reps )
+int cmd_time_kerngen( int L, double rmin, double rmax, int bcc, int bcs, int reps, const std::string& dir = "" )
 {
     Setup                            s( L, rmin, rmax );
     linalg::VectorQ1Scalar< double > k( "k", s.domain, s.omask );
     linalg::VectorQ1Vec< double >    src( "src", s.domain, s.omask ), dst( "dst", s.domain, s.omask );
-    linalg::assign( k, 1.0 );
-    linalg::assign( src, 1.0 );
+    if ( dir.empty() )
+    {
+        linalg::assign( k, 1.0 );
+        linalg::assign( src, 1.0 );
+    }
+    else
+    {
+        view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", s.nodes ).data() );
+        load_vec( src, dir + "/src.bin", s.nodes );
+    }
     auto op = make_kerngen( s, k, bcc, bcs, false );
     linalg::apply( op, src, dst ); // warm-up, as measure_run_time does
     Kokkos::fence();
@@ -919,6 +933,68 @@ int cmd_transfer_linear( bool prolong, int Lf, double rmin, double rmax, const s
     return 0;
 }
 
+// FV -> FE transfer on the FV field fv.bin ([10][N+2]^3 with ghosts): l2_project_fv_to_fe (consistent mass,
+// PCG 1000 / 1e-12 / 1e-12 from x = 0; conversion.hpp:131-205) or l2_project_fv_to_fe_lumped (:243-300);
+// writes x.bin
+int cmd_l2proj( int L, double rmin, double rmax, int lumped, const std::string& dir )
+{
+    Setup                                             s( L, rmin, rmax );
+    linalg::VectorFVScalar< double >                  fv( "fv", s.domain );
+    linalg::VectorQ1Scalar< double >                  x( "x", s.domain, s.omask );
+    std::vector< linalg::VectorQ1Scalar< double > >   tmps;
+    for ( int i = 0; i < 5; ++i )
+        tmps.emplace_back( "t" + std::to_string( i ), s.domain, s.omask );
+    view_from_host( fv.grid_data(), read_file< double >( dir + "/fv.bin", fv.grid_data().size() ).data() );
+    linalg::assign( x, 0.0 );
+    if ( lumped )
+        fv::hex::l2_project_fv_to_fe_lumped( x, fv, s.domain, s.coords, s.radii, tmps );
+    else
+        fv::hex::l2_project_fv_to_fe( x, fv, s.domain, s.coords, s.radii, tmps );
+    auto h = view_to_host( x.grid_data() );
+    write_file( dir + "/x.bin", h.data(), h.size() );
+    return 0;
+}
+
+// The app's Stokes buoyancy right-hand side (mantlecirculation.cpp:876-899): g = Ra T n at every node with n the
+// unit radial direction (RHSVelocityInterpolator, :117-150, restated: it is app code), f = VectorMass g, then the
+// library's strong Dirichlet and free-slip enforcement for the boundary conditions (bcc, bcs); T.bin (FE scalar)
+// -> f_u.bin
+int cmd_stokes_rhs( int L, double rmin, double rmax, double ra, int bcc, int bcs, const std::string& dir )
+{
+    Setup                            f( L, rmin, rmax ), c( L - 1, rmin, rmax );
+    BoundaryConditions b = { { ShellBoundaryFlag::CMB, bc_of( bcc ) }, { ShellBoundaryFlag::SURFACE, bc_of( bcs ) } };
+    auto                             T = read_file< double >( dir + "/T.bin", f.nodes );
+    linalg::VectorQ1Vec< double >    g( "g", f.domain, f.omask );
+    linalg::VectorQ1IsoQ2Q1< double > rhs( "rhs", f.domain, c.domain, f.omask, c.omask );
+    {
+        auto coords = view_to_host( f.coords );
+        auto radii  = view_to_host( f.radii );
+        (void) radii;
+        const int n1 = ( 1 << L ) + 1;
+        std::vector< double > h( 3 * f.nodes );
+        for ( size_t i = 0; i < f.nodes; ++i )
+        {
+            const size_t lat = i / n1;
+            const double u0 = coords[lat * 3], u1 = coords[lat * 3 + 1], u2 = coords[lat * 3 + 2];
+            const double nn = std::sqrt( u0 * u0 + u1 * u1 + u2 * u2 );
+            h[i]                = ra * ( u0 / nn ) * T[i];
+            h[f.nodes + i]      = ra * ( u1 / nn ) * T[i];
+            h[2 * f.nodes + i]  = ra * ( u2 / nn ) * T[i];
+        }
+        for ( int dd = 0; dd < 3; ++dd )
+            view_from_host( g.grid_data().comp_[dd], h.data() + dd * f.nodes );
+    }
+    fe::wedge::operators::shell::VectorMass< double > M( f.domain, f.coords, f.radii, false );
+    linalg::apply( M, g, rhs.block_1() );
+    linalg::assign( rhs.block_2(), 0.0 );
+    fe::strong_algebraic_homogeneous_velocity_dirichlet_enforcement_stokes_like(
+        rhs, f.bmask, grid::shell::get_shell_boundary_flag( b, BoundaryConditionFlag::DIRICHLET ) );
+    fe::strong_algebraic_freeslip_enforcement_in_place(
+        rhs, f.coords, f.bmask, grid::shell::get_shell_boundary_flag( b, BoundaryConditionFlag::FREESLIP ) );
+    save_vec( rhs.block_1(), dir + "/f_u.bin", f.nodes );
+    return 0;
+}
+
 int cmd_fct( int L, double rmin, double rmax, double dt, double kappa, int bc, const std::string& dir )
 {
     Setup                               s( L, rmin, rmax );
@@ -1091,6 +1167,8 @@ int main( int argc, char** argv )
         return cmd_kerngen( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( cmd == "time_kerngen" && argc == 8 )
         return cmd_time_kerngen( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ) );
+    if ( cmd == "time_kerngen" && argc == 9 )
+        return cmd_time_kerngen( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( ( cmd == "divergence" || cmd == "gradient" ) && argc == 8 )
         return cmd_stokes_block( cmd == "divergence", I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
     if ( ( cmd == "prolong" || cmd == "restrict" ) && argc == 6 )
@@ -1123,6 +1201,10 @@ int main( int argc, char** argv )
         return cmd_fct( I( 2 ), D( 3 ), D( 4 ), D( 5 ), D( 6 ), I( 7 ), argv[8] );
     if ( cmd == "gca" && argc == 10 )
         return cmd_gca( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), I( 8 ), argv[9] );
+    if ( cmd == "l2proj" && argc == 7 )
+        return cmd_l2proj( I( 2 ), D( 3 ), D( 4 ), I( 5 ), argv[6] );
+    if ( cmd == "stokes_rhs" && argc == 9 )
+        return cmd_stokes_rhs( I( 2 ), D( 3 ), D( 4 ), D( 5 ), I( 6 ), I( 7 ), argv[8] );
     if ( cmd == "stokes_mg" && argc == 18 )
         return cmd_stokes_mg( I( 2 ), I( 3 ), D( 4 ), D( 5 ), I( 6 ), I( 7 ), I( 8 ), I( 9 ), D( 10 ), I( 11 ), I( 12 ),
                               I( 13 ), I( 14 ), I( 15 ), I( 16 ), argv[17] );

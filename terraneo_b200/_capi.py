@@ -132,6 +132,12 @@ _SIGS = {
     "tn_stokes_history": (c_int, [c_void_p, P(c_double), c_int, P(c_int), P(c_int)]),
     "tn_stokes_apply": (c_int, [c_void_p, P(c_void_p), c_void_p, P(c_void_p), c_void_p]),
     "tn_stokes_solver_destroy": (c_int, [c_void_p]),
+    "tn_fv_to_fe_rhs_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "tn_l2_project_fv_to_fe_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_double, c_double, c_void_p,
+                                           P(c_int), c_void_p]),
+    "tn_stokes_buoyancy_rhs_f64": (c_int, [c_void_p, c_void_p, c_double, c_int, c_int, P(c_void_p), c_void_p,
+                                           c_void_p]),
+    "tn_pressure_remove_mean_f64": (c_int, [c_void_p, c_void_p, c_void_p, P(c_double), c_void_p]),
     "tn_vec_lincomb_f64": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p), c_void_p]),
     "tn_vec_lincomb_f32": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p), c_void_p]),
     "tn_vec_dot_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_double), c_void_p]),

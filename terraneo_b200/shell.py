@@ -577,3 +577,106 @@ def assign(y, c0):
 
 def dot(a, b):
     return a.dot_impl(b)
+
+
+# --- the mantle-circulation time step (apps/mantlecirculation/mantlecirculation.cpp:870-1045) ---------------
+
+def fv_to_fe_rhs(mesh, fv, lumped_diagonal=False):
+    """b = sum_K fv_K int_K phi_i (fv/hex/conversion.hpp:146-190), and the lumped diagonal if asked; FE scalars."""
+    b = VectorQ1Scalar(mesh)
+    D = VectorQ1Scalar(mesh) if lumped_diagonal else None
+    C.check(C.lib().tn_fv_to_fe_rhs_f64(mesh.handle, ctypes.c_void_p(fv.data_ptr()),
+                                        ctypes.c_void_p(b.data.data_ptr()),
+                                        ctypes.c_void_p(D.data.data_ptr()) if D is not None else None, _stream()),
+            "fv_to_fe_rhs")
+    return b, D
+
+
+def l2_project_fv_to_fe(mesh, fv, dst, lumped=False, max_iterations=1000, relative_tolerance=1e-12,
+                        absolute_tolerance=1e-12, work=None):
+    """l2_project_fv_to_fe / l2_project_fv_to_fe_lumped (fv/hex/conversion.hpp:131-300): dst (VectorQ1Scalar,
+    its values the PCG's start) from the FV tensor fv [10, N+2, N+2, N+2]; returns the PCG iterations."""
+    if work is None:
+        work = torch.empty(5 * mesh.stored_nodes, dtype=torch.float64, device="cuda")
+    its = ctypes.c_int()
+    C.check(C.lib().tn_l2_project_fv_to_fe_f64(mesh.handle, ctypes.c_void_p(fv.data_ptr()),
+                                               ctypes.c_void_p(dst.data.data_ptr()), int(lumped), max_iterations,
+                                               relative_tolerance, absolute_tolerance,
+                                               ctypes.c_void_p(work.data_ptr()), ctypes.byref(its), _stream()),
+            "l2_project_fv_to_fe")
+    return its.value
+
+
+def stokes_buoyancy_rhs(mesh, T, rayleigh, bc_cmb, bc_surface, f_u, work=None):
+    """f_u = VectorMass (Ra T n) with the app's strong Dirichlet / free-slip enforcement
+    (mantlecirculation.cpp:117-150, 876-899); T a VectorQ1Scalar on the velocity mesh."""
+    if work is None:
+        work = torch.empty(3 * mesh.stored_nodes, dtype=torch.float64, device="cuda")
+    C.check(C.lib().tn_stokes_buoyancy_rhs_f64(mesh.handle, ctypes.c_void_p(T.data.data_ptr()), float(rayleigh),
+                                               bc_cmb, bc_surface, f_u.comp_ptrs(), ctypes.c_void_p(work.data_ptr()),
+                                               _stream()), "stokes_buoyancy_rhs")
+
+
+def pressure_remove_mean(p, work=None):
+    """p -= sum_owned p / unique nodes (mantlecirculation.cpp:930-936); returns the subtracted mean."""
+    if work is None:
+        work = torch.empty(p.mesh.stored_nodes, dtype=torch.float64, device="cuda")
+    mean = ctypes.c_double()
+    C.check(C.lib().tn_pressure_remove_mean_f64(p.mesh.handle, ctypes.c_void_p(p.data.data_ptr()),
+                                                ctypes.c_void_p(work.data_ptr()), ctypes.byref(mean), _stream()),
+            "pressure_remove_mean")
+    return mean.value
+
+
+class MantleTimestep:
+    """One time step of the mantle-circulation app on the GPU (mantlecirculation.cpp:870-1045), in its order:
+    the Stokes right-hand side from the FE temperature (buoyancy Ra T n, VectorMass, strong enforcement), the
+    Stokes solve warm-started from the previous velocity and pressure, the pressure normalisation, dt =
+    dt_scaling x compute_dt_stable, `energy_substeps` FCT explicit steps with the Dirichlet temperatures
+    applied after each, the FV -> FE L2 projection of the temperature (warm-started from the previous FE
+    temperature), and the NaN / Inf guard on it (the app stops its run there; step() returns False).
+
+    T_fv: FV temperature [10, N+2, N+2, N+2] (with ghosts); the FE temperature is projected from it at set-up.
+    solver_kwargs: shell.StokesSolver arguments (the app's: FGMRES(restart), block-triangular preconditioner,
+    V-cycle).  Every array stays on the device."""
+
+    def __init__(self, level, viscosity, T_fv, rayleigh=1e5, dt_scaling=0.5, diffusivity=0.0, energy_substeps=1,
+                 T_cmb=1.0, T_surface=0.0, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, lumped_projection=False,
+                 r_min=0.55, r_max=1.0, **solver_kwargs):
+        self.mesh_u = ShellMesh(level, r_min, r_max)
+        self.mesh_p = ShellMesh(level - 1, r_min, r_max)
+        self.rayleigh, self.dt_scaling, self.kappa = rayleigh, dt_scaling, diffusivity
+        self.substeps, self.bcs = energy_substeps, (bc_cmb, bc_surface)
+        self.lumped = lumped_projection
+        self.solver = StokesSolver(level, viscosity, bc_cmb=bc_cmb, bc_surface=bc_surface, r_min=r_min, r_max=r_max,
+                                   **solver_kwargs)
+        self.fct = FCTAdvectionDiffusion(self.mesh_u)
+        self.fct_bcs = self.fct.dirichlet(T_cmb, T_surface)
+        self.T_fv = T_fv
+        self.T = VectorQ1Scalar(self.mesh_u)
+        self.u, self.p = VectorQ1Vec(self.mesh_u), VectorQ1Scalar(self.mesh_p)
+        self.f_u, self.f_p = VectorQ1Vec(self.mesh_u), VectorQ1Scalar(self.mesh_p)
+        ns = self.mesh_u.stored_nodes
+        self._work = torch.empty(5 * ns, dtype=torch.float64, device="cuda")
+        self._pwork = torch.empty(self.mesh_p.stored_nodes, dtype=torch.float64, device="cuda")
+        self.fct.apply_dirichlet(self.T_fv, self.fct_bcs)
+        self.project_temperature()
+        self.last = {}
+
+    def project_temperature(self):
+        return l2_project_fv_to_fe(self.mesh_u, self.T_fv, self.T, self.lumped, work=self._work)
+
+    def step(self):
+        """One time step; False when the temperature holds NaN or Inf afterwards (the app's guard, :1041)."""
+        stokes_buoyancy_rhs(self.mesh_u, self.T, self.rayleigh, *self.bcs, self.f_u, work=self._work)
+        its, rr = self.solver.solve(self.f_u, self.f_p, self.u, self.p)
+        mean = pressure_remove_mean(self.p, work=self._pwork)
+        dt = self.dt_scaling * self.fct.dt_stable(self.u, self.kappa)
+        for _ in range(self.substeps):
+            self.fct.step(self.T_fv, self.u, dt, self.kappa, None, True, self.fct_bcs)
+            self.fct.apply_dirichlet(self.T_fv, self.fct_bcs)
+        pits = self.project_temperature()
+        ok = not self.T.has_nan_or_inf_impl()
+        self.last = {"stokes_iterations": its, "stokes_relres": rr, "pressure_mean_removed": mean, "dt": dt,
+                     "projection_iterations": pits, "finite": ok}
+        return ok

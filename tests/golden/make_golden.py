@@ -34,6 +34,21 @@ VMASS_MODES = [0, 1]
 DIVKGRAD_CASES = [(1, 0, 0), (0, 0, 0), (1, 1, 0), (1, 0, 1)]
 EPSDIVDIV_CASES = [(1, 0), (0, 0), (1, 1)]
 VLAPLACE_CASES = [(1, 1, 0), (0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 1)]
+# FV -> FE transfer (consistent mass + PCG, lumped) of a seeded FV field, and the app's Stokes buoyancy
+# right-hand side (Ra = 1e5) of a seeded FE temperature for these boundary conditions
+L2PROJ_MODES = [0, 1]
+STOKES_RHS_BCS = [(2, 2), (1, 1), (2, 1), (1, 2), (0, 0)]
+STOKES_RHS_RA = 1e5
+
+
+def timestep_inputs(fine):
+    """seeded FV field (with ghosts) and FE temperature in [0, 1] consistent on duplicated nodes"""
+    rs = np.random.RandomState(55)
+    fv = rs.normal(size=fine.fv_shape)
+    T = fine.make_consistent(rs.uniform(size=fine.shape)).reshape(fine.shape)
+    return fv, T
+
+
 # kerngen slow path (the reference's own assembled wedge matrices stored in Full mode): (bcc, bcs, diag)
 KSLOW_CASES = [(1, 1, 0), (2, 2, 0), (2, 1, 0), (0, 0, 0), (2, 2, 1)]
 # wedge matrices kept in the fixture: these cells (flat index (d, x, y, r)), both wedges
@@ -240,6 +255,17 @@ def main():
         for mode, bcc, bcs, diag in GCA_CASES:
             run_ref(["gca", L, R_MIN, R_MAX, bcc, bcs, diag, mode, d], d)
             out[f"gca_{mode}_{bcc}{bcs}{diag}"] = np.fromfile(f"{d}/dst.bin").reshape((3,) + coarse.shape)
+
+        fv, Tfe = timestep_inputs(fine)
+        out["checksum_ts_fv"], out["checksum_ts_T"] = checksum(fv), checksum(Tfe)
+        fv.tofile(f"{d}/fv.bin")
+        for lumped in L2PROJ_MODES:
+            run_ref(["l2proj", L, R_MIN, R_MAX, lumped, d], d)
+            out[f"l2proj_{lumped}"] = np.fromfile(f"{d}/x.bin").reshape(fine.shape)
+        Tfe.tofile(f"{d}/T.bin")
+        for bcc, bcs in STOKES_RHS_BCS:
+            run_ref(["stokes_rhs", L, R_MIN, R_MAX, STOKES_RHS_RA, bcc, bcs, d], d)
+            out[f"stokes_rhs_{bcc}{bcs}"] = np.fromfile(f"{d}/f_u.bin").reshape((3,) + fine.shape)
 
         x["s"].tofile(f"{d}/src.bin")
         for treat, diag in LAPLACE_CASES:

@@ -55,6 +55,7 @@ def lib():
         L.or_prolongation_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D]
         L.or_restriction_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _U8, _D, _D]
         L.or_kmass_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int]
+        L.or_fv_to_fe_rhs.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D]
         L.or_masked_dot.restype = ctypes.c_double
         L.or_masked_dot.argtypes = [ctypes.c_size_t, _D, _D, _U8]
         _lib = L
@@ -237,6 +238,42 @@ class Mesh:
                           _p(np.ascontiguousarray(vel, dtype=np.float64)), _p(T), dt, diffusivity, sp,
                           int(subtract_divergence), b, _p(TL))
         return T, TL
+
+    def fv_to_fe_rhs(self, fv=None, lumped_diagonal=False):
+        """b = sum_K fv_K int_K phi_i (and / or the lumped diagonal), node copies summed (conversion.hpp:146-190)"""
+        b = np.zeros(self.shape) if fv is not None else None
+        D = np.zeros(self.shape) if lumped_diagonal else None
+        f = None if fv is None else _p(np.ascontiguousarray(fv, dtype=np.float64))
+        lib().or_fv_to_fe_rhs(self.L, _p(self.coords), _p(self.radii), f, None if b is None else _p(b),
+                              None if D is None else _p(D))
+        return b, D
+
+    def l2_project_fv_to_fe(self, fv, lumped=False, max_iterations=1000, rtol=1e-12, atol=1e-12):
+        """l2_project_fv_to_fe (PCG on the Q1 mass matrix from x = 0) or its lumped form (conversion.hpp:131-300)"""
+        b, D = self.fv_to_fe_rhs(fv, lumped_diagonal=lumped)
+        if lumped:
+            return b / D
+        ones = np.ones(self.shape)
+        return pcg(lambda v: self.kmass(ones, v, 0), self.dot, b, max_iterations, rtol, atol)[0]
+
+    def stokes_buoyancy_rhs(self, T, rayleigh, bc_cmb, bc_surf):
+        """f = VectorMass (Ra T n), n the unit radial direction, Dirichlet rows zeroed, the normal component of
+        free-slip rows removed (mantlecirculation.cpp:117-150, 883-899).  As the app calls the enforcement, each
+        condition acts on the boundary get_shell_boundary_flag names, the first with that condition (CMB before
+        SURFACE; grid/shell/bit_masks.hpp:68-76): with the same condition on both radii only the CMB rows."""
+        n = self.coords / np.linalg.norm(self.coords, axis=-1, keepdims=True)
+        ones = np.ones(self.shape)
+        f = np.stack([self.kmass(ones, rayleigh * T * n[:, :, :, None, c], 0) for c in range(3)])
+        nn = np.moveaxis(n, -1, 0)
+        for cond in (1, 2):
+            r = 0 if bc_cmb == cond else (-1 if bc_surf == cond else None)
+            if r is None:
+                continue
+            if cond == 1:
+                f[..., r] = 0.0
+            else:
+                f[..., r] -= np.sum(f[..., r] * nn, axis=0) * nn
+        return f
 
     def kmass(self, k, src, mode=0):
         dst = np.zeros(self.shape)

@@ -306,6 +306,27 @@ def test_slow_path_and_gca_match_live_reference_L3():
                 assert rel(c.stored_apply(mc, uc, bcc, bcs, diag), ref) <= TOL
 
 
+@pytest.mark.parametrize("lumped", G.L2PROJ_MODES)
+def test_l2_projection_matches_reference(case, lumped):
+    """l2_project_fv_to_fe (Q1 mass + PCG to 1e-12, conversion.hpp:131-205) and its lumped form (:243-300) of a
+    seeded FV field: the oracle against the reference (the consistent form to the solver's tolerance)."""
+    g, fine, _, _ = case
+    fv, T = G.timestep_inputs(fine)
+    assert np.allclose(G.checksum(fv), g["checksum_ts_fv"], rtol=1e-13, atol=0)
+    tol = TOL if lumped else 1e-10
+    assert rel(fine.l2_project_fv_to_fe(fv, lumped=bool(lumped)), g[f"l2proj_{lumped}"]) <= tol
+
+
+@pytest.mark.parametrize("bcc,bcs", G.STOKES_RHS_BCS)
+def test_stokes_buoyancy_rhs_matches_reference(case, bcc, bcs):
+    """The app's Stokes right-hand side (mantlecirculation.cpp:876-899): VectorMass of Ra T n with the strong
+    Dirichlet / free-slip enforcement on the boundary get_shell_boundary_flag names."""
+    g, fine, _, _ = case
+    fv, T = G.timestep_inputs(fine)
+    assert np.allclose(G.checksum(T), g["checksum_ts_T"], rtol=1e-13, atol=0)
+    assert rel(fine.stokes_buoyancy_rhs(T, G.STOKES_RHS_RA, bcc, bcs), g[f"stokes_rhs_{bcc}{bcs}"]) <= TOL
+
+
 def test_golden_fixture_is_not_trivial(case):
     """A planted error in the oracle's input must break the comparison."""
     g, fine, _, x = case
