@@ -6,7 +6,7 @@
  * MPI_IN_PLACE), rank = 0, size = 1, and point-to-point calls are never
  * reached because same-rank subdomain pairs use local device copies
  * (src/terra/communication/shell/communication.hpp:256).  MPI-IO is only used
- * by the XDMF writer, which the oracle never calls; those entry points fail.
+ * by the XDMF writer and checkpoint reader: single-rank stdio files below.
  *
  * A datatype handle encodes its element size in bytes in the low byte. */
 #ifndef TN_ORACLE_MPI_STUB_H
@@ -172,53 +172,155 @@ static inline int MPI_Waitall( int n, MPI_Request* q, MPI_Status* st )
     (void) n, (void) q, (void) st;
     return MPI_SUCCESS;
 }
+/* Single-rank MPI-IO over stdio (the XDMF writer and checkpoint reader,
+ * io/xdmf.hpp).  A file handle indexes a small table of open files, each
+ * with its view displacement and file type; a derived (hindexed) type is an
+ * index into a table of block lists and reads its blocks in order.  Opening
+ * with MPI_MODE_CREATE does not truncate an existing file (MPI semantics). */
+#include <stdio.h>
+#include <stdlib.h>
+
+#define TN_STUB_MAX_FILES 16
+#define TN_STUB_MAX_TYPES 16
+#define TN_STUB_TYPE_BASE 0x100000
+
+typedef struct { FILE* f; long long disp; MPI_Datatype ftype; } tn_stub_file;
+typedef struct { int n; int* len; MPI_Aint* off; } tn_stub_type;
+static tn_stub_file tn_stub_files[TN_STUB_MAX_FILES];
+static tn_stub_type tn_stub_types[TN_STUB_MAX_TYPES];
+
 static inline int MPI_Type_create_hindexed( int n, const int* l, const MPI_Aint* d, MPI_Datatype o, MPI_Datatype* t )
 {
-    (void) n, (void) l, (void) d, (void) o;
-    *t = MPI_DATATYPE_NULL;
+    if ( o != MPI_CHAR && o != MPI_BYTE )
+        return MPI_ERR_OTHER;
+    for ( int i = 0; i < TN_STUB_MAX_TYPES; ++i )
+        if ( !tn_stub_types[i].len )
+        {
+            tn_stub_types[i].n   = n;
+            tn_stub_types[i].len = (int*) malloc( sizeof( int ) * ( n > 0 ? n : 1 ) );
+            tn_stub_types[i].off = (MPI_Aint*) malloc( sizeof( MPI_Aint ) * ( n > 0 ? n : 1 ) );
+            for ( int k = 0; k < n; ++k )
+            {
+                tn_stub_types[i].len[k] = l[k];
+                tn_stub_types[i].off[k] = d[k];
+            }
+            *t = ( ( TN_STUB_TYPE_BASE + i ) << 8 ) | 1;
+            return MPI_SUCCESS;
+        }
     return MPI_ERR_OTHER;
 }
-static inline int MPI_Type_commit( MPI_Datatype* t )
+static inline tn_stub_type* tn_stub_derived( MPI_Datatype t )
 {
-    (void) t;
-    return MPI_ERR_OTHER;
+    const int i = ( t >> 8 ) - TN_STUB_TYPE_BASE;
+    return ( i >= 0 && i < TN_STUB_MAX_TYPES && tn_stub_types[i].len ) ? &tn_stub_types[i] : (tn_stub_type*) 0;
 }
+static inline int MPI_Type_commit( MPI_Datatype* t ) { return tn_stub_derived( *t ) ? MPI_SUCCESS : MPI_ERR_OTHER; }
 static inline int MPI_Type_free( MPI_Datatype* t )
 {
-    (void) t;
+    tn_stub_type* d = tn_stub_derived( *t );
+    if ( d )
+    {
+        free( d->len );
+        free( d->off );
+        d->len = 0;
+        d->off = 0;
+    }
+    *t = MPI_DATATYPE_NULL;
     return MPI_SUCCESS;
+}
+static inline tn_stub_file* tn_stub_fh( MPI_File fh )
+{
+    return ( fh >= 1 && fh <= TN_STUB_MAX_FILES && tn_stub_files[fh - 1].f ) ? &tn_stub_files[fh - 1] : (tn_stub_file*) 0;
 }
 static inline int MPI_File_open( MPI_Comm c, const char* f, int m, MPI_Info i, MPI_File* fh )
 {
-    (void) c, (void) f, (void) m, (void) i;
+    (void) c, (void) i;
     *fh = 0;
+    FILE* fp = 0;
+    if ( m & MPI_MODE_RDONLY )
+        fp = fopen( f, "rb" );
+    else
+    {
+        fp = fopen( f, "r+b" );
+        if ( !fp && ( m & MPI_MODE_CREATE ) )
+            fp = fopen( f, "w+b" );
+    }
+    if ( !fp )
+        return MPI_ERR_OTHER;
+    for ( int k = 0; k < TN_STUB_MAX_FILES; ++k )
+        if ( !tn_stub_files[k].f )
+        {
+            tn_stub_files[k].f     = fp;
+            tn_stub_files[k].disp  = 0;
+            tn_stub_files[k].ftype = MPI_CHAR;
+            *fh                    = k + 1;
+            return MPI_SUCCESS;
+        }
+    fclose( fp );
     return MPI_ERR_OTHER;
 }
 static inline int MPI_File_close( MPI_File* fh )
 {
-    (void) fh;
-    return MPI_ERR_OTHER;
+    tn_stub_file* f = tn_stub_fh( *fh );
+    if ( !f )
+        return MPI_ERR_OTHER;
+    fclose( f->f );
+    f->f = 0;
+    *fh  = 0;
+    return MPI_SUCCESS;
 }
-static inline int MPI_File_set_view( MPI_File fh, MPI_Offset o, MPI_Datatype e, MPI_Datatype f, const char* rep, MPI_Info i )
+static inline int MPI_File_set_view( MPI_File fh, MPI_Offset o, MPI_Datatype e, MPI_Datatype t, const char* rep, MPI_Info i )
 {
-    (void) fh, (void) o, (void) e, (void) f, (void) rep, (void) i;
-    return MPI_ERR_OTHER;
+    (void) e, (void) rep, (void) i;
+    tn_stub_file* f = tn_stub_fh( fh );
+    if ( !f )
+        return MPI_ERR_OTHER;
+    f->disp  = o;
+    f->ftype = t;
+    return MPI_SUCCESS;
 }
 static inline int MPI_File_write_all( MPI_File fh, const void* b, int n, MPI_Datatype t, MPI_Status* st )
 {
-    (void) fh, (void) b, (void) n, (void) t, (void) st;
-    return MPI_ERR_OTHER;
+    (void) st;
+    tn_stub_file* f = tn_stub_fh( fh );
+    if ( !f || tn_stub_derived( f->ftype ) || fseeko( f->f, (off_t) f->disp, SEEK_SET ) )
+        return MPI_ERR_OTHER;
+    const size_t bytes = (size_t) n * tn_mpi_stub_size( t );
+    return fwrite( b, 1, bytes, f->f ) == bytes ? MPI_SUCCESS : MPI_ERR_OTHER;
 }
 static inline int MPI_File_read_all( MPI_File fh, void* b, int n, MPI_Datatype t, MPI_Status* st )
 {
-    (void) fh, (void) b, (void) n, (void) t, (void) st;
-    return MPI_ERR_OTHER;
+    (void) st;
+    tn_stub_file* f = tn_stub_fh( fh );
+    if ( !f )
+        return MPI_ERR_OTHER;
+    size_t        left = (size_t) n * tn_mpi_stub_size( t );
+    char*         p    = (char*) b;
+    tn_stub_type* d    = tn_stub_derived( f->ftype );
+    if ( !d )
+    {
+        if ( fseeko( f->f, (off_t) f->disp, SEEK_SET ) )
+            return MPI_ERR_OTHER;
+        return fread( p, 1, left, f->f ) == left ? MPI_SUCCESS : MPI_ERR_OTHER;
+    }
+    for ( int k = 0; k < d->n && left > 0; ++k )
+    {
+        size_t len = (size_t) d->len[k] < left ? (size_t) d->len[k] : left;
+        if ( fseeko( f->f, (off_t) ( f->disp + d->off[k] ), SEEK_SET ) || fread( p, 1, len, f->f ) != len )
+            return MPI_ERR_OTHER;
+        p += len;
+        left -= len;
+    }
+    return left == 0 ? MPI_SUCCESS : MPI_ERR_OTHER;
 }
 static inline int MPI_File_get_size( MPI_File fh, MPI_Offset* s )
 {
-    (void) fh;
-    *s = 0;
-    return MPI_ERR_OTHER;
+    tn_stub_file* f = tn_stub_fh( fh );
+    *s              = 0;
+    if ( !f || fseeko( f->f, 0, SEEK_END ) )
+        return MPI_ERR_OTHER;
+    *s = (MPI_Offset) ftello( f->f );
+    return MPI_SUCCESS;
 }
 
 #endif

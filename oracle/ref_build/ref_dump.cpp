@@ -54,6 +54,14 @@
 //   kerngen_slow L rmin rmax bcc bcs diag DIR  the kerngen slow path on the reference's own assembled
 //                                          wedge matrices (written to mats.bin) stored in Full mode
 //   vlaplace L rmin rmax bcc bcs diag DIR  VectorLaplace<double>
+//   xdmf_write L rmin rmax pts conn DIR    io::XDMFOutput of T.bin / u.bin (FE, FP64) under DIR/xdmf: the six
+//                                          grids T (FP32 out), T64 (FP64), u (FP32), u64 (FP64), s32 (FP32 input,
+//                                          FP32 out), v32 (FP32 input, FP64 out); two write() steps, the second
+//                                          with T + 1 and 2 u; pts / conn = 4|8 bytes of points / connectivity
+//   xdmf_read L rmin rmax label step vec CKDIR DIR  read_xdmf_checkpoint_grid of `label` at `step` from CKDIR
+//                                          into a FP64 grid (vec 0: scalar, 1: 3-vector): out.bin; the metadata
+//                                          as text in meta.txt; on a read error its message in error.txt, exit 3
+//   fe2fv L rmin rmax DIR                  l2_project_fe_to_fv of T.bin (FE): fv.bin ([10][N+2]^3, ghosts set)
 //   time_kerngen L rmin rmax bcc bcs reps [DIR]  prints seconds per apply (CPU baseline); with DIR the
 //                                          inputs are k.bin / src.bin there, else k = 1, src = 1
 #include <chrono>
@@ -82,6 +90,7 @@
 #include "fe/strong_algebraic_dirichlet_enforcement.hpp"
 #include "fe/strong_algebraic_freeslip_enforcement.hpp"
 #include "fv/hex/conversion.hpp"
+#include "io/xdmf.hpp"
 #include "fv/hex/helpers.hpp"
 #include "fv/hex/operators/fct_advection_diffusion.hpp"
 #include "grid/bit_masks.hpp"
@@ -1148,6 +1157,123 @@ int cmd_vlaplace( int L, double rmin, double rmax, int bcc, int bcs, int diag, c
     return 0;
 }
 
+// io::XDMFOutput (io/xdmf.hpp:147-1115) of the FE fields T.bin (scalar) and u.bin (3 x nodes, SoA) under DIR/xdmf
+int cmd_xdmf_write( int L, double rmin, double rmax, int pts, int conn, const std::string& dir )
+{
+    Setup     s( L, rmin, rmax );
+    const int n1 = ( 1 << L ) + 1;
+    auto      T  = read_file< double >( dir + "/T.bin", s.nodes );
+    auto      u  = read_file< double >( dir + "/u.bin", 3 * s.nodes );
+    grid::Grid4DDataScalar< double > gT( "T", 10, n1, n1, n1 ), gT64( "T64", 10, n1, n1, n1 );
+    grid::Grid4DDataScalar< float >  gs( "s32", 10, n1, n1, n1 );
+    grid::Grid4DDataVec< double, 3 > gu( "u", 10, n1, n1, n1 ), gu64( "u64", 10, n1, n1, n1 );
+    grid::Grid4DDataVec< float, 3 >  gv( "v32", 10, n1, n1, n1 );
+    using X = io::XDMFOutput< double >;
+    X out( dir + "/xdmf", s.domain, s.coords, s.radii,
+           pts == 8 ? X::OutputTypeFloat::Float64 : X::OutputTypeFloat::Float32,
+           conn == 4 ? X::OutputTypeInt::Int32 : X::OutputTypeInt::Int64 );
+    out.add( gT );
+    out.add( gT64, X::OutputTypeFloat::Float64 );
+    out.add( gs );
+    out.add( gu );
+    out.add( gu64, X::OutputTypeFloat::Float64 );
+    out.add( gv, X::OutputTypeFloat::Float64 );
+    for ( int step = 0; step < 2; ++step )
+    {
+        std::vector< double > t( T ), w( u );
+        std::vector< float >  t32( s.nodes ), w32( 3 * s.nodes );
+        for ( size_t i = 0; i < s.nodes; ++i )
+            t[i] += step;
+        for ( auto& x : w )
+            x *= ( 1 + step );
+        for ( size_t i = 0; i < s.nodes; ++i )
+            t32[i] = float( t[i] );
+        for ( size_t i = 0; i < 3 * s.nodes; ++i )
+            w32[i] = float( w[i] );
+        view_from_host( gT, t.data() );
+        view_from_host( gT64, t.data() );
+        view_from_host( gs, t32.data() );
+        for ( int d = 0; d < 3; ++d )
+        {
+            view_from_host( gu.comp_[d], w.data() + d * s.nodes );
+            view_from_host( gu64.comp_[d], w.data() + d * s.nodes );
+            view_from_host( gv.comp_[d], w32.data() + d * s.nodes );
+        }
+        Kokkos::fence();
+        out.write();
+    }
+    return 0;
+}
+
+// io::read_xdmf_checkpoint_metadata / read_xdmf_checkpoint_grid (io/xdmf.hpp:1162-1500) into a FP64 grid
+int cmd_xdmf_read( int L, double rmin, double rmax, const std::string& label, int step, int vec,
+                   const std::string& ck, const std::string& dir )
+{
+    Setup     s( L, rmin, rmax );
+    const int n1 = ( 1 << L ) + 1;
+    {
+        auto          m = io::read_xdmf_checkpoint_metadata( ck );
+        std::ofstream f( dir + "/meta.txt" );
+        if ( m.is_err() )
+            f << "error " << m.error() << "\n";
+        else
+        {
+            const auto& md = m.unwrap();
+            f << "version " << md.version << "\nsubdomains " << md.num_subdomains_per_diamond_lateral_direction << " "
+              << md.num_subdomains_per_diamond_radial_direction << "\nsize " << md.size_x << " " << md.size_y << " "
+              << md.size_r << "\ngrid_scalar_bytes " << md.grid_scalar_bytes << "\nordering "
+              << md.checkpoint_subdomain_ordering << "\nradii " << md.radii.size() << "\n";
+            for ( const auto& g : md.grid_data_files )
+                f << "file " << g.grid_name_string << " " << g.scalar_data_type << " " << g.scalar_bytes << " "
+                  << g.vec_dim << "\n";
+            for ( auto id : md.checkpoint_ordering_0_global_subdomain_ids )
+                f << "id " << id << "\n";
+        }
+    }
+    auto fail = [&]( const std::string& msg ) {
+        std::ofstream( dir + "/error.txt" ) << msg;
+        return 3;
+    };
+    if ( vec )
+    {
+        grid::Grid4DDataVec< double, 3 > g( label, 10, n1, n1, n1 );
+        auto                             r = io::read_xdmf_checkpoint_grid( ck, label, step, s.domain, g );
+        if ( r.is_err() )
+            return fail( r.error() );
+        std::vector< double > out( 3 * s.nodes );
+        for ( int d = 0; d < 3; ++d )
+        {
+            auto c = view_to_host( g.comp_[d] );
+            std::copy( c.begin(), c.end(), out.begin() + d * s.nodes );
+        }
+        write_file( dir + "/out.bin", out.data(), out.size() );
+    }
+    else
+    {
+        grid::Grid4DDataScalar< double > g( label, 10, n1, n1, n1 );
+        auto                             r = io::read_xdmf_checkpoint_grid( ck, label, step, s.domain, g );
+        if ( r.is_err() )
+            return fail( r.error() );
+        auto h = view_to_host( g );
+        write_file( dir + "/out.bin", h.data(), h.size() );
+    }
+    return 0;
+}
+
+// FE -> FV cell averages (fv/hex/conversion.hpp:349-416) of T.bin, ghost layers updated: fv.bin
+int cmd_fe2fv( int L, double rmin, double rmax, const std::string& dir )
+{
+    Setup                            s( L, rmin, rmax );
+    linalg::VectorQ1Scalar< double > T( "T", s.domain, s.omask );
+    linalg::VectorFVScalar< double > fv( "fv", s.domain );
+    view_from_host( T.grid_data(), read_file< double >( dir + "/T.bin", s.nodes ).data() );
+    linalg::assign( fv, 0.0 );
+    fv::hex::l2_project_fe_to_fv( fv, T, s.domain, s.coords, s.radii );
+    auto h = view_to_host( fv.grid_data() );
+    write_file( dir + "/fv.bin", h.data(), h.size() );
+    return 0;
+}
+
 } // namespace
 
 int main( int argc, char** argv )
@@ -1222,6 +1348,12 @@ int main( int argc, char** argv )
         return cmd_laplace_cg( I( 2 ), D( 3 ), D( 4 ), I( 5 ), D( 6 ), argv[7] );
     if ( cmd == "laplace" && argc == 8 )
         return cmd_laplace( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
+    if ( cmd == "xdmf_write" && argc == 8 )
+        return cmd_xdmf_write( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), argv[7] );
+    if ( cmd == "xdmf_read" && argc == 10 )
+        return cmd_xdmf_read( I( 2 ), D( 3 ), D( 4 ), argv[5], I( 6 ), I( 7 ), argv[8], argv[9] );
+    if ( cmd == "fe2fv" && argc == 6 )
+        return cmd_fe2fv( I( 2 ), D( 3 ), D( 4 ), argv[5] );
     std::fprintf( stderr, "ref_dump: bad command line\n" );
     return 2;
 }
