@@ -507,6 +507,50 @@ def level8_leg(shell, C, torch, steps=5, warmup=3):
     return out
 
 
+def checkpoint_leg(shell, torch, ts):
+    """The app's XDMF checkpoint of the level-7 step (T, u_u, eta as FP32, mantlecirculation.cpp:789-799) into a
+    temporary directory: the first write (with geometry.bin and topology.bin), then one steady-state write
+    timed three ways (the device time of its conversion kernels on the caller's stream, the host time until
+    write() returns, the time until the files are complete), then the recovery of step 1 (velocity, FE
+    temperature, FV temperature by l2_project_fe_to_fv).  The directory is removed afterwards."""
+    import shutil
+    import tempfile
+    d = tempfile.mkdtemp(prefix="tn_checkpoint_")
+    try:
+        ns = ts.mesh_u.stored_nodes
+        out = ts.checkpoint_output(d)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out.write()
+        out.wait()
+        first = time.perf_counter() - t0
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev[0].record()
+        out.write()
+        ev[1].record()
+        t_ret = time.perf_counter() - t0
+        out.wait()
+        t_all = time.perf_counter() - t0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ts.restore_checkpoint(d, 1)
+        torch.cuda.synchronize()
+        t_restore = time.perf_counter() - t0
+        per_write = ns * 5 * 4
+        files = sum(os.path.getsize(os.path.join(d, f)) for f in os.listdir(d))
+        return {"grids": "T, u_u, eta as FP32 (the app's XDMFOutput defaults)", "bytes_per_write": per_write,
+                "first_write_seconds": round(first, 3), "write_stream_ms": round(ev[0].elapsed_time(ev[1]), 3),
+                "write_returns_ms": round(t_ret * 1e3, 3), "write_complete_seconds": round(t_all, 3),
+                "write_complete_gbs": round(per_write / t_all / 1e9, 2), "restore_seconds": round(t_restore, 3),
+                "directory_bytes": files}
+    except Exception as e:  # a full or read-only scratch disk: report it, keep the bench line
+        return {"error": str(e)[:300]}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def timestep_leg(shell, C, torch, level=7, warm_steps=2, spinup_solves=20):
     """One mantle-circulation time step at level 7 (velocity 63,406,854 DoFs, pressure level 6, 20,971,520 FV
     cells) as the app takes it, with the app's solver settings (shell.MantleTimestep; mantlecirculation.cpp:
@@ -583,6 +627,8 @@ def timestep_leg(shell, C, torch, level=7, warm_steps=2, spinup_solves=20):
            "warm_up_steps": warm, "setup_seconds": round(setup, 2),
            "device_memory_gb": round((total - free1) / 1e9, 2),
            "T_range": [float(Ti.min()), float(Ti.max())], "clocks": clk.summary()}
+    # last: the recovery overwrites the step's state (the pressure restarts from zero, as in the app)
+    out["checkpoint"] = checkpoint_leg(shell, torch, ts)
     del ts, T, kv, ku, kp
     torch.cuda.empty_cache()
     return out

@@ -37,6 +37,7 @@ extern "C" {
 #define TN_ERR_CUDA -2     /* a CUDA runtime call failed */
 #define TN_ERR_NOMEM -3    /* device or host allocation failed */
 #define TN_ERR_STATE -4    /* object not set up for this call */
+#define TN_ERR_IO -5       /* a file could not be read or written, or its content is not as expected */
 
 #define TN_BC_NEUMANN 0
 #define TN_BC_DIRICHLET 1
@@ -580,6 +581,61 @@ TN_API int tn_stokes_buoyancy_rhs_f64( const tn_mesh* mesh, const double* T, dou
 /* Pressure normalisation (mantlecirculation.cpp:930-936): p -= sum over owned nodes of p / unique nodes.
  * work: one stored-node field; mean (optional) receives the subtracted value.  Synchronises. */
 TN_API int tn_pressure_remove_mean_f64( const tn_mesh* mesh, double* p, double* work, double* mean, void* stream );
+
+/* ---- FE -> FV transfer -------------------------------------------------- */
+/* Cell averages of the FE scalar fe on the FV cells of the mesh (fv/hex/conversion.hpp:349-416,
+ * l2_project_fe_to_fv): fv[d][x][y][r] = int_K fe / |K| for the cells x, y, r in 1..N (the two wedges of the
+ * hex cell, integrals in closed form, exact as the reference's 3x2 rule), then the lateral FV ghost layers
+ * (tn_fv_ghost_update_f64).  Radial ghost cells are left as they are.  fv: [10][N+2]^3. */
+TN_API int tn_l2_project_fe_to_fv_f64( const tn_mesh* mesh, const double* fe, double* fv, void* stream );
+
+/* ---- XDMF output and checkpoints (io/xdmf.hpp) -------------------------- */
+/* io::XDMFOutput (io/xdmf.hpp:147-1115): a time series of node fields in the reference's directory format,
+ * which is both the visualisation output and the checkpoint: geometry.bin, topology.bin and
+ * checkpoint_metadata.bin at the first write, <label>_<step>.bin per grid and step_<step>.xmf (written last)
+ * per write.  One subdomain per diamond (global ids diamond << 57), one process.
+ * points_bytes: 4 or 8 (OutputTypeFloat of the coordinates); connectivity_bytes: 4 or 8 (OutputTypeInt). */
+typedef struct tn_xdmf_output tn_xdmf_output;
+TN_API int tn_xdmf_output_create( const tn_mesh* mesh, const char* directory, int points_bytes, int connectivity_bytes,
+                                  tn_xdmf_output** out );
+/* XDMFOutput::set_write_counter (:204): the step number of the next write */
+TN_API int tn_xdmf_output_set_write_counter( tn_xdmf_output* w, int counter );
+/* XDMFOutput::add (:210-280): a device grid of vec_dim 1 or 3 components (SoA pointers, input_bytes 4 = FP32
+ * or 8 = FP64 entries) written as output_bytes 4 or 8 floats under `label`.  The pointers must stay valid for
+ * the writer's lifetime.  Errors (TN_ERR_ARG) after the first write and for a label already added. */
+TN_API int tn_xdmf_output_add( tn_xdmf_output* w, const char* label, int input_bytes, int vec_dim,
+                               const void* const* components, int output_bytes );
+/* XDMFOutput::write (:283-520): converts every grid to the file order and type on `stream` (the grids may
+ * change as soon as the stream has passed this point), copies them to pinned host memory on the writer's own
+ * stream and writes the files from a host thread; returns before the files are complete.  The first call also
+ * writes the mesh and metadata files (synchronously).  A file error of the previous write is returned by the
+ * next write or wait (TN_ERR_IO). */
+TN_API int tn_xdmf_output_write( tn_xdmf_output* w, void* stream );
+/* blocks until the files of the last write are complete; TN_ERR_IO if one could not be written */
+TN_API int tn_xdmf_output_wait( tn_xdmf_output* w );
+TN_API int tn_xdmf_output_destroy( tn_xdmf_output* w );
+
+/* CheckpointMetadata (io/xdmf.hpp:1117-1153) without its lists */
+typedef struct
+{
+    int version, subdomains_lateral, subdomains_radial, size_x, size_y, size_r;
+    int grid_scalar_bytes, num_grid_data_files, ordering, num_radii, num_subdomain_ids;
+} tn_checkpoint_info;
+/* read_xdmf_checkpoint_metadata (:1162-1268), host only: the fixed fields, the radii (up to radii_capacity)
+ * and the global subdomain ids in file order (up to ids_capacity; either array may be null).
+ * TN_ERR_IO with the reference's error text in tn_last_error(). */
+TN_API int tn_read_xdmf_checkpoint_metadata( const char* directory, tn_checkpoint_info* info, double* radii,
+                                             int radii_capacity, long long* subdomain_ids, int ids_capacity );
+/* the index-th grid record of the metadata: label (NUL-terminated), scalar_data_type (2 = float),
+ * scalar_bytes, vec_dim; host only */
+TN_API int tn_xdmf_checkpoint_grid_data_file( const char* directory, int index, char* label, int label_capacity,
+                                              int* scalar_data_type, int* scalar_bytes, int* vec_dim );
+/* read_xdmf_checkpoint_grid (:1270-1500): grid `label` of write `step` into the device field dst (vec_dim 1
+ * or 3 SoA pointers of dst_bytes 4 or 8 entries), converted from the file's type; the diamonds' chunks are
+ * found through the metadata's subdomain ids.  Synchronises the stream.  TN_ERR_IO with the reference's error
+ * text (missing metadata, label or step file, extents, ordering, data type, scalar / vector mismatch). */
+TN_API int tn_read_xdmf_checkpoint_grid( const tn_mesh* mesh, const char* directory, const char* label, int step,
+                                         int dst_bytes, int vec_dim, void* const* dst, void* stream );
 
 #ifdef __cplusplus
 }

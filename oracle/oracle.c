@@ -2077,3 +2077,41 @@ void or_fv_to_fe_rhs( int L, const double* coords, const double* radii, const do
     if ( D )
         or_halo_sum( L, coords, D, 1 );
 }
+
+/* FE -> FV cell averages (fv/hex/conversion.hpp:349-416): the integral of the FE field over the hex cell's two
+ * wedges with the 3x2 rule divided by the cell volume from the same rule, for the cells x, y, r in 1..N of
+ * fv ([10][N+2]^3); then the lateral FV ghost layers. */
+void or_fe_to_fv( int L, const double* coords, const double* radii, const double* fe, double* fv )
+{
+    const int N = 1 << L, n1 = N + 1, n2 = N + 2;
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 1; x <= N; ++x )
+            for ( int y = 1; y <= N; ++y )
+                for ( int r = 1; r <= N; ++r )
+                {
+                    const double r1 = radii[d * n1 + r - 1], r2 = radii[d * n1 + r];
+                    double       volume = 0.0, integral = 0.0;
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const double* p[3];
+                        wedge_lateral_points( n1, coords, d, x - 1, y - 1, w, p );
+                        double u[6];
+                        for ( int i = 0; i < 6; ++i )
+                            u[i] = fe[node_idx( n1, d, x - 1 + WNODE[w][i][0], y - 1 + WNODE[w][i][1],
+                                                r - 1 + WNODE[w][i][2] )];
+                        for ( int q = 0; q < 6; ++q )
+                        {
+                            double J[3][3];
+                            wedge_jac( p, r1, r2, QP32[q][0], QP32[q][1], QP32[q][2], J );
+                            const double jw = fabs( det3( J ) ) * QW32;
+                            double       uq = 0.0;
+                            for ( int i = 0; i < 6; ++i )
+                                uq += u[i] * shape_val( i, QP32[q][0], QP32[q][1], QP32[q][2] );
+                            volume += jw;
+                            integral += uq * jw;
+                        }
+                    }
+                    fv[fv_idx( n2, d, x, y, r )] = integral / volume;
+                }
+    or_fv_ghost_update( L, coords, fv );
+}

@@ -34,6 +34,7 @@ void or_ownership_mask( int L, const double* coords, uint8_t* omask );
 /* duplicated-node additive reduction (halo SUM) of ncomp scalar fields */
 void or_halo_sum( int L, const double* coords, double* field, int ncomp );
 void or_fv_to_fe_rhs( int L, const double* coords, const double* radii, const double* fv, double* b, double* D );
+void or_fe_to_fv( int L, const double* coords, const double* radii, const double* fe, double* fv );
 
 /* operators (Replace mode, additive communication) */
 void or_kerngen_apply( int L, const double* coords, const double* radii, const double* k, const double* src,

@@ -46,6 +46,12 @@ class FCTDirichlet(ctypes.Structure):
     _fields_ = [("T_cmb", c_double), ("T_surface", c_double), ("apply_cmb", c_int), ("apply_surface", c_int)]
 
 
+class CheckpointInfo(ctypes.Structure):
+    _fields_ = [(n, c_int) for n in ("version", "subdomains_lateral", "subdomains_radial", "size_x", "size_y", "size_r",
+                                     "grid_scalar_bytes", "num_grid_data_files", "ordering", "num_radii",
+                                     "num_subdomain_ids")]
+
+
 class TNError(RuntimeError):
     pass
 
@@ -138,6 +144,19 @@ _SIGS = {
     "tn_stokes_buoyancy_rhs_f64": (c_int, [c_void_p, c_void_p, c_double, c_int, c_int, P(c_void_p), c_void_p,
                                            c_void_p]),
     "tn_pressure_remove_mean_f64": (c_int, [c_void_p, c_void_p, c_void_p, P(c_double), c_void_p]),
+    "tn_l2_project_fe_to_fv_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "tn_xdmf_output_create": (c_int, [c_void_p, ctypes.c_char_p, c_int, c_int, P(c_void_p)]),
+    "tn_xdmf_output_set_write_counter": (c_int, [c_void_p, c_int]),
+    "tn_xdmf_output_add": (c_int, [c_void_p, ctypes.c_char_p, c_int, c_int, P(c_void_p), c_int]),
+    "tn_xdmf_output_write": (c_int, [c_void_p, c_void_p]),
+    "tn_xdmf_output_wait": (c_int, [c_void_p]),
+    "tn_xdmf_output_destroy": (c_int, [c_void_p]),
+    "tn_read_xdmf_checkpoint_metadata": (c_int, [ctypes.c_char_p, P(CheckpointInfo), P(c_double), c_int,
+                                                 P(ctypes.c_longlong), c_int]),
+    "tn_xdmf_checkpoint_grid_data_file": (c_int, [ctypes.c_char_p, c_int, ctypes.c_char_p, c_int, P(c_int), P(c_int),
+                                                  P(c_int)]),
+    "tn_read_xdmf_checkpoint_grid": (c_int, [c_void_p, ctypes.c_char_p, ctypes.c_char_p, c_int, c_int, c_int,
+                                             P(c_void_p), c_void_p]),
     "tn_vec_lincomb_f64": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p), c_void_p]),
     "tn_vec_lincomb_f32": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p), c_void_p]),
     "tn_vec_dot_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_double), c_void_p]),

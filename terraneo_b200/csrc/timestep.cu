@@ -105,6 +105,52 @@ __global__ void buoyancy_kernel( size_t ns, int n1, const double* __restrict__ c
     }
 }
 
+// One thread per FV cell: the cell average of the FE field over the hex cell's two wedges,
+// sum_w sum_i u_i int phi_i |det J| / sum_w int |det J| with the closed-form node integrals of
+// fv_to_fe_rhs_kernel (the reference evaluates the same integrals with the 3x2 rule, conversion.hpp:371-411)
+__global__ void __launch_bounds__( kTsThreads ) fe_to_fv_kernel( int N, const double* __restrict__ coords,
+                                                                 const double* __restrict__ radii,
+                                                                 const double* __restrict__ fe, double* fv )
+{
+    const long long t = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if ( t >= (long long) kDiamonds * N * N * N )
+        return;
+    const int    r = int( t % N ) + 1, y = int( ( t / N ) % N ) + 1, x = int( ( t / ( (long long) N * N ) ) % N ) + 1;
+    const int    d  = int( t / ( (long long) N * N * N ) );
+    const int    n1 = N + 1, n2 = N + 2;
+    const double g  = 0.5773502691896257;
+    const double r1 = radii[d * n1 + r - 1], r2 = radii[d * n1 + r];
+    const double h  = 0.5 * ( r2 - r1 );
+    const double rm = r1 + h * ( 1.0 - g ), rp = r1 + h * ( 1.0 + g );
+    const double Ib = ( rm * rm * 0.5 * ( 1.0 + g ) + rp * rp * 0.5 * ( 1.0 - g ) ) * 0.1666666666666667;
+    const double It = ( rm * rm * 0.5 * ( 1.0 - g ) + rp * rp * 0.5 * ( 1.0 + g ) ) * 0.1666666666666667;
+    double       integral = 0.0, volume = 0.0;
+    for ( int w = 0; w < 2; ++w )
+    {
+        double p[3][3];
+        size_t lat[3];
+        for ( int i = 0; i < 3; ++i )
+        {
+            lat[i] = lat_index( n1, d, x - 1 + kWedgeNode[w][i][0], y - 1 + kWedgeNode[w][i][1] );
+            for ( int a = 0; a < 3; ++a )
+                p[i][a] = coords[lat[i] * 3 + a];
+        }
+        const double a0 = p[1][0] - p[0][0], a1 = p[1][1] - p[0][1], a2 = p[1][2] - p[0][2];
+        const double b0 = p[2][0] - p[0][0], b1 = p[2][1] - p[0][1], b2 = p[2][2] - p[0][2];
+        const double Dw = ( a1 * b2 - a2 * b1 ) * p[0][0] + ( a2 * b0 - a0 * b2 ) * p[0][1] + ( a0 * b1 - a1 * b0 ) * p[0][2];
+        const double hd = h * fabs( Dw );
+        double       sb = 0.0, st = 0.0;
+        for ( int i = 0; i < 3; ++i )
+        {
+            sb += fe[lat[i] * n1 + r - 1];
+            st += fe[lat[i] * n1 + r];
+        }
+        integral += hd * ( Ib * sb + It * st );
+        volume += hd * 3.0 * ( Ib + It );
+    }
+    fv[fv_idx( n2, d, x, y, r )] = integral / volume;
+}
+
 unsigned blocks_for( size_t n ) { return unsigned( std::min< size_t >( ( n + 255 ) / 256, 148 * 8 ) ); }
 
 }  // namespace
@@ -251,4 +297,17 @@ extern "C" int tn_pressure_remove_mean_f64( const tn_mesh* m, double* p, double*
     if ( mean )
         *mean = avg;
     return TN_OK;
+}
+
+// FV cell averages of an FE scalar (l2_project_fe_to_fv, fv/hex/conversion.hpp:349-416), then the lateral
+// FV ghost layers
+extern "C" int tn_l2_project_fe_to_fv_f64( const tn_mesh* m, const double* fe, double* fv, void* s )
+{
+    TN_CHECK_ARG( m && fe && fv, "tn_l2_project_fe_to_fv_f64: null argument" );
+    cudaStream_t    st    = as_stream( s );
+    const long long cells = (long long) kDiamonds * m->N * m->N * m->N;
+    fe_to_fv_kernel<<< unsigned( ( cells + kTsThreads - 1 ) / kTsThreads ), kTsThreads, 0, st >>>(
+        m->N, m->d_coords, m->d_radii, fe, fv );
+    TN_LAUNCH_CHECK();
+    return tn_fv_ghost_update_f64( m, fv, s );
 }

@@ -628,6 +628,83 @@ def pressure_remove_mean(p, work=None):
     return mean.value
 
 
+def l2_project_fe_to_fv(mesh, fe, fv):
+    """FV cell averages of the FE scalar fe (VectorQ1Scalar) into fv [10, N+2, N+2, N+2], lateral ghost layers
+    updated (l2_project_fe_to_fv, fv/hex/conversion.hpp:349-416)."""
+    C.check(C.lib().tn_l2_project_fe_to_fv_f64(mesh.handle, ctypes.c_void_p(fe.data.data_ptr()),
+                                               ctypes.c_void_p(fv.data_ptr()), _stream()), "l2_project_fe_to_fv")
+
+
+class XDMFOutput:
+    """io::XDMFOutput (io/xdmf.hpp:147-1115): visualisation output and checkpoint in the reference's directory
+    format.  add() device grids (VectorQ1Scalar / VectorQ1Vec, FP32 or FP64) before the first write(); write()
+    converts them on the current stream and returns while the files are written in the background; wait()
+    blocks until they are complete.  points / connectivity: 4 or 8 bytes."""
+
+    FLOAT32, FLOAT64 = 4, 8
+    INT32, INT64 = 4, 8
+
+    def __init__(self, directory, mesh, points=4, connectivity=8):
+        h = ctypes.c_void_p()
+        C.check(C.lib().tn_xdmf_output_create(mesh.handle, str(directory).encode(), points, connectivity,
+                                              ctypes.byref(h)), "xdmf_output_create")
+        self._h, self.mesh, self.directory, self._keep = h, mesh, str(directory), []
+
+    def set_write_counter(self, counter):
+        C.check(C.lib().tn_xdmf_output_set_write_counter(self._h, counter), "set_write_counter")
+
+    def add(self, vec, label, output=4):
+        """vec: VectorQ1Scalar or VectorQ1Vec (kept alive by the writer); label: the grid's name in the files"""
+        self._keep.append(vec)
+        C.check(C.lib().tn_xdmf_output_add(self._h, label.encode(), vec.data.element_size(), vec.ncomp,
+                                           vec.comp_ptrs(), output), "xdmf_output_add")
+
+    def write(self):
+        C.check(C.lib().tn_xdmf_output_write(self._h, _stream()), "xdmf_output_write")
+
+    def wait(self):
+        C.check(C.lib().tn_xdmf_output_wait(self._h), "xdmf_output_wait")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and C is not None and C._lib is not None:
+            C.lib().tn_xdmf_output_destroy(h)
+            self._h = None
+
+
+def read_xdmf_checkpoint_metadata(directory):
+    """read_xdmf_checkpoint_metadata (io/xdmf.hpp:1162-1268) as a dict; raises C.TNError with the reference's
+    error text.  Host only."""
+    info = C.CheckpointInfo()
+    d = str(directory).encode()
+    C.check(C.lib().tn_read_xdmf_checkpoint_metadata(d, ctypes.byref(info), None, 0, None, 0), "checkpoint metadata")
+    radii = (ctypes.c_double * max(1, info.num_radii))()
+    ids = (ctypes.c_longlong * max(1, info.num_subdomain_ids))()
+    C.check(C.lib().tn_read_xdmf_checkpoint_metadata(d, ctypes.byref(info), radii, info.num_radii, ids,
+                                                     info.num_subdomain_ids), "checkpoint metadata")
+    out = {k: getattr(info, k) for k, _ in C.CheckpointInfo._fields_}
+    out["radii"] = list(radii[:info.num_radii])
+    out["subdomain_ids"] = list(ids[:info.num_subdomain_ids])
+    files = []
+    for i in range(info.num_grid_data_files):
+        label = ctypes.create_string_buffer(4096)
+        t, b, v = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        C.check(C.lib().tn_xdmf_checkpoint_grid_data_file(d, i, label, 4096, ctypes.byref(t), ctypes.byref(b),
+                                                          ctypes.byref(v)), "checkpoint grid record")
+        files.append({"label": label.value.decode(), "scalar_data_type": t.value, "scalar_bytes": b.value,
+                      "vec_dim": v.value})
+    out["grid_data_files"] = files
+    return out
+
+
+def read_xdmf_checkpoint_grid(directory, label, step, vec):
+    """read_xdmf_checkpoint_grid (io/xdmf.hpp:1270-1500) into vec (VectorQ1Scalar / VectorQ1Vec on the mesh the
+    checkpoint was written on); raises C.TNError with the reference's error text."""
+    C.check(C.lib().tn_read_xdmf_checkpoint_grid(vec.mesh.handle, str(directory).encode(), label.encode(), step,
+                                                 vec.data.element_size(), vec.ncomp, vec.comp_ptrs(), _stream()),
+            "read_xdmf_checkpoint_grid")
+
+
 class MantleTimestep:
     """One time step of the mantle-circulation app on the GPU (mantlecirculation.cpp:870-1045), in its order:
     the Stokes right-hand side from the FE temperature (buoyancy Ra T n, VectorMass, strong enforcement), the
@@ -648,6 +725,7 @@ class MantleTimestep:
         self.rayleigh, self.dt_scaling, self.kappa = rayleigh, dt_scaling, diffusivity
         self.substeps, self.bcs = energy_substeps, (bc_cmb, bc_surface)
         self.lumped = lumped_projection
+        self.viscosity = viscosity
         self.solver = StokesSolver(level, viscosity, bc_cmb=bc_cmb, bc_surface=bc_surface, r_min=r_min, r_max=r_max,
                                    **solver_kwargs)
         self.fct = FCTAdvectionDiffusion(self.mesh_u)
@@ -680,3 +758,21 @@ class MantleTimestep:
         self.last = {"stokes_iterations": its, "stokes_relres": rr, "pressure_mean_removed": mean, "dt": dt,
                      "projection_iterations": pits, "finite": ok}
         return ok
+
+    def checkpoint_output(self, directory, points=4, connectivity=8, output=4):
+        """The app's XDMF output (mantlecirculation.cpp:789-799): T, the velocity as "u_u" and the viscosity
+        "eta", written as `output`-byte floats; call write() on it after set-up and after each output step."""
+        x = XDMFOutput(directory, self.mesh_u, points, connectivity)
+        x.add(self.T, "T", output)
+        x.add(self.u, "u_u", output)
+        x.add(self.viscosity, "eta", output)
+        return x
+
+    def restore_checkpoint(self, directory, step):
+        """The app's checkpoint recovery (mantlecirculation.cpp:803-846): the velocity and the FE temperature
+        of `step`, the FV temperature recovered from the FE one (l2_project_fe_to_fv); the pressure restarts
+        from zero, as in the app."""
+        read_xdmf_checkpoint_grid(directory, "u_u", step, self.u)
+        read_xdmf_checkpoint_grid(directory, "T", step, self.T)
+        l2_project_fe_to_fv(self.mesh_u, self.T, self.T_fv)
+        self.p.data.zero_()

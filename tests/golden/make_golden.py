@@ -10,6 +10,7 @@ shows up as a failing check instead of a silent mismatch.
 Usage (in a container that has the reference sources and a built ref_dump):
     python tests/golden/make_golden.py               # ref_L2.npz
     python tests/golden/make_golden.py --stokes-mg   # ref_stokes_mg_L4.npz (a few minutes on one thread)
+    python tests/golden/make_golden.py --xdmf        # xdmf_L2/: a checkpoint written by io::XDMFOutput
 """
 import os
 import sys
@@ -266,6 +267,8 @@ def main():
         for bcc, bcs in STOKES_RHS_BCS:
             run_ref(["stokes_rhs", L, R_MIN, R_MAX, STOKES_RHS_RA, bcc, bcs, d], d)
             out[f"stokes_rhs_{bcc}{bcs}"] = np.fromfile(f"{d}/f_u.bin").reshape((3,) + fine.shape)
+        run_ref(["fe2fv", L, R_MIN, R_MAX, d], d)
+        out["fe2fv"] = np.fromfile(f"{d}/fv.bin").reshape(fine.fv_shape)
 
         x["s"].tofile(f"{d}/src.bin")
         for treat, diag in LAPLACE_CASES:
@@ -404,8 +407,41 @@ def main():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+# The checkpoint fixture: io::XDMFOutput<double> on the L2 mesh with FP32 points and int64 connectivity, the
+# grids of XDMF_GRIDS (label, input bytes, output bytes, vec_dim) filled from the FE temperature of
+# timestep_inputs and the velocity u of inputs(); two writes, the second with T + 1 and 2 u.
+XDMF_DIR = os.path.join(HERE, "xdmf_L2")
+XDMF_GRIDS = [("T", 8, 4, 1), ("T64", 8, 8, 1), ("s32", 4, 4, 1), ("u", 8, 4, 3), ("u64", 8, 8, 3), ("v32", 4, 8, 3)]
+XDMF_PTS, XDMF_CONN = 4, 8
+
+
+def xdmf_fields(fine, coarse, step):
+    """the grids written at `step`: [(label, in_bytes, out_bytes, vec, data)] with data as the writer holds it"""
+    _, T = timestep_inputs(fine)
+    u = inputs(fine, coarse)["u"]
+    t, w = T + step, u * (1 + step)
+    data = {"T": t, "T64": t, "s32": t.astype(np.float32), "u": w, "u64": w, "v32": w.astype(np.float32)}
+    return [(lab, ib, ob, v, data[lab]) for lab, ib, ob, v in XDMF_GRIDS]
+
+
+def make_xdmf():
+    import shutil
+    fine, coarse = Mesh(L), Mesh(L - 1)
+    _, T = timestep_inputs(fine)
+    u = inputs(fine, coarse)["u"]
+    with tempfile.TemporaryDirectory() as d:
+        T.tofile(f"{d}/T.bin")
+        u.tofile(f"{d}/u.bin")
+        run_ref(["xdmf_write", L, R_MIN, R_MAX, XDMF_PTS, XDMF_CONN, d], d)
+        os.makedirs(XDMF_DIR, exist_ok=True)
+        for f in sorted(os.listdir(f"{d}/xdmf")):
+            shutil.copyfile(f"{d}/xdmf/{f}", os.path.join(XDMF_DIR, f))
+
+
 if __name__ == "__main__":
     if "--stokes-mg" in sys.argv:
         make_stokes_mg()
+    elif "--xdmf" in sys.argv:
+        make_xdmf()
     else:
         main()

@@ -56,6 +56,7 @@ def lib():
         L.or_restriction_constant.argtypes = [ctypes.c_int, ctypes.c_int, _D, _U8, _D, _D]
         L.or_kmass_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int]
         L.or_fv_to_fe_rhs.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D]
+        L.or_fe_to_fv.argtypes = [ctypes.c_int, _D, _D, _D, _D]
         L.or_masked_dot.restype = ctypes.c_double
         L.or_masked_dot.argtypes = [ctypes.c_size_t, _D, _D, _U8]
         _lib = L
@@ -255,6 +256,14 @@ class Mesh:
             return b / D
         ones = np.ones(self.shape)
         return pcg(lambda v: self.kmass(ones, v, 0), self.dot, b, max_iterations, rtol, atol)[0]
+
+    def l2_project_fe_to_fv(self, fe, fv=None):
+        """FV cell averages of the FE scalar fe with the 3x2 rule, lateral ghosts updated (conversion.hpp:349-416);
+        the radial ghost cells keep the values of fv (zeros when fv is None)"""
+        out = np.zeros(self.fv_shape) if fv is None else np.array(fv, dtype=np.float64)
+        lib().or_fe_to_fv(self.L, _p(self.coords), _p(self.radii), _p(np.ascontiguousarray(fe, dtype=np.float64)),
+                          _p(out))
+        return out
 
     def stokes_buoyancy_rhs(self, T, rayleigh, bc_cmb, bc_surf):
         """f = VectorMass (Ra T n), n the unit radial direction, Dirichlet rows zeroed, the normal component of
@@ -661,3 +670,135 @@ def run_ref(args, workdir, threads=4, json_out=False):
                          text=True)
     if json_out:
         return json.loads([ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1])
+
+
+# ---------------------------------------------------------------------------
+# XDMF output / checkpoint format (io/xdmf.hpp:80-145, 283-1115), restated with numpy for one subdomain per
+# diamond.  grids: list of dicts {label, in_bytes, out_bytes, vec, data} with data [10, n1, n1, n1] (scalar) or
+# [3, 10, n1, n1, n1] (vector) in the node layout (r fastest).
+
+def xdmf_order(grids):
+    """the reference's write order: FP32 scalars, FP64 scalars, FP32 vectors, FP64 vectors (io/xdmf.hpp:490-512)"""
+    return [g for vec in (1, 3) for ib in (4, 8) for g in grids if g["vec"] == vec and g["in_bytes"] == ib]
+
+
+def xdmf_geometry(om, pts):
+    """node coordinates, subdomain by subdomain in (r, y, x) order, x fastest (io/xdmf.hpp:615-645)"""
+    X = om.coords.transpose(0, 2, 1, 3)[:, None] * om.radii[:, :, None, None, None]
+    return np.ascontiguousarray(X.astype(np.float32 if pts == 4 else np.float64)).tobytes()
+
+
+def xdmf_topology(om, conn):
+    """six node ids per wedge, two wedges per hex cell in (diamond, r, y, x) order (io/xdmf.hpp:647-690)"""
+    n1, N = om.N + 1, om.N
+    d, r, y, x = np.meshgrid(np.arange(10), np.arange(N), np.arange(N), np.arange(N), indexing="ij")
+    v0 = d * n1 ** 3 + r * n1 ** 2 + y * n1 + x
+    v4 = v0 + n1 ** 2
+    w = np.stack([v0, v0 + 1, v0 + n1, v4, v4 + 1, v4 + n1,
+                  v0 + n1 + 1, v0 + n1, v0 + 1, v4 + n1 + 1, v4 + n1, v4 + 1], axis=-1)
+    return np.ascontiguousarray(w.astype(np.int32 if conn == 4 else np.int64)).tobytes()
+
+
+def xdmf_grid_bytes(data, vec, out_bytes):
+    """one grid's file: [10][r][y][x] (x fastest), vector components interleaved (io/xdmf.hpp:692-880)"""
+    a = np.transpose(data, (0, 3, 2, 1)) if vec == 1 else np.transpose(data, (1, 4, 3, 2, 0))
+    return np.ascontiguousarray(a.astype(np.float32 if out_bytes == 4 else np.float64)).tobytes()
+
+
+def xdmf_metadata(om, grids, pts):
+    """checkpoint_metadata.bin (io/xdmf.hpp:882-1063): version 1, one subdomain per diamond"""
+    import struct
+    n1 = om.N + 1
+    b = struct.pack("<6i", 1, 1, 1, n1, n1, n1) + struct.pack(f"<{n1}d", *om.radii[0])
+    order = xdmf_order(grids)
+    b += struct.pack("<2i", pts, len(order))
+    for g in order:
+        lab = g["label"].encode()
+        b += struct.pack("<i", len(lab)) + lab + struct.pack("<3i", 2, g["out_bytes"], g["vec"])
+    return b + struct.pack("<i", 0) + struct.pack("<10q", *[d << 57 for d in range(10)])
+
+
+def _xml_escape(s):
+    return (s.replace("&", "&amp;").replace('"', "&quot;").replace("'", "&apos;").replace("<", "&lt;")
+            .replace(">", "&gt;"))
+
+
+def xdmf_step_xml(om, grids, step, pts, conn):
+    """step_<step>.xmf (io/xdmf.hpp:455-520 with util/xml.hpp: attributes sorted by name, two-space indent)"""
+    n1 = om.N + 1
+    nodes, elems = 10 * n1 ** 3, 10 * om.N ** 3 * 2
+
+    def item(dtype, dims, prec, content):
+        return (f'<DataItem DataType="{dtype}" Dimensions="{dims}" Endian="Little" Format="Binary" '
+                f'Precision="{prec}">{_xml_escape(content)}</DataItem>\n')
+    s = '<?xml version="1.0" ?>\n<!DOCTYPE Xdmf SYSTEM "Xdmf.dtd" []>\n<Xdmf Version="2.0">\n  <Domain>\n'
+    s += '    <Grid GridType="Uniform" Name="Grid">\n      <Geometry Type="XYZ">\n'
+    s += "        " + item("Float", f"{nodes} 3", pts, "geometry.bin") + "      </Geometry>\n"
+    s += f'      <Topology NumberOfElements="{elems}" Type="Wedge">\n'
+    s += "        " + item("Int", f"{6 * elems}", conn, "topology.bin") + "      </Topology>\n"
+    for g in xdmf_order(grids):
+        kind = "Scalar" if g["vec"] == 1 else "Vector"
+        dims = f"{nodes}" if g["vec"] == 1 else f"{nodes} 3"
+        s += f'      <Attribute AttributeType="{kind}" Center="Node" Name="{_xml_escape(g["label"])}">\n'
+        s += "        " + item("Float", dims, g["out_bytes"], f'{g["label"]}_{step}.bin') + "      </Attribute>\n"
+    return s + "    </Grid>\n  </Domain>\n</Xdmf>\n"
+
+
+def xdmf_read_grid(directory, label, step, om, vec):
+    """read_xdmf_checkpoint_grid (io/xdmf.hpp:1270-1500) for one subdomain per diamond: the grid as FP64 in the
+    node layout ([10, n1, n1, n1] or [3, 10, n1, n1, n1])"""
+    import struct
+    with open(os.path.join(directory, "checkpoint_metadata.bin"), "rb") as f:
+        md = f.read()
+    n1 = om.N + 1
+    _, sl, sr, sx, sy, sz = struct.unpack_from("<6i", md, 0)
+    pos = 24 + 8 * (sr * (sz - 1) + 1) + 4
+    nf, = struct.unpack_from("<i", md, pos)
+    pos += 4
+    rec = None
+    for _ in range(nf):
+        ln, = struct.unpack_from("<i", md, pos)
+        lab = md[pos + 4:pos + 4 + ln].decode()
+        t, nb, vd = struct.unpack_from("<3i", md, pos + 4 + ln)
+        pos += 16 + ln
+        if lab == label and rec is None:
+            rec = (nb, vd)
+    pos += 4
+    ids = struct.unpack_from(f"<{10 * sl * sl * sr}q", md, pos)
+    nb, vd = rec
+    assert vd == (1 if not vec else 3) and (sx, sy, sz) == (n1, n1, n1)
+    raw = np.fromfile(os.path.join(directory, f"{label}_{step}.bin"), dtype=np.float32 if nb == 4 else np.float64)
+    chunk = n1 ** 3 * vd
+    parts = [raw[ids.index(d << 57) * chunk:(ids.index(d << 57) + 1) * chunk] for d in range(10)]
+    a = np.stack(parts).astype(np.float64)
+    if vd == 1:
+        return np.transpose(a.reshape(10, n1, n1, n1), (0, 3, 2, 1)).copy()
+    return np.transpose(a.reshape(10, n1, n1, n1, 3), (4, 0, 3, 2, 1)).copy()
+
+
+def xdmf_write_dir(directory, om, steps, pts=4, conn=8, order=None):
+    """A whole checkpoint directory from the restatement: steps = [grids of write 0, grids of write 1, ...];
+    order: the diamonds' order in the data files (a permutation of 0..9; io/xdmf.hpp allows any, the metadata's
+    id list says where each subdomain is)."""
+    import struct
+    order = list(range(10)) if order is None else list(order)
+    os.makedirs(directory, exist_ok=True)
+    with open(os.path.join(directory, "geometry.bin"), "wb") as f:
+        f.write(_permute_chunks(xdmf_geometry(om, pts), order))
+    with open(os.path.join(directory, "topology.bin"), "wb") as f:
+        f.write(xdmf_topology(om, conn))
+    md = xdmf_metadata(om, steps[0], pts)
+    md = md[:-80] + struct.pack("<10q", *[d << 57 for d in order])
+    with open(os.path.join(directory, "checkpoint_metadata.bin"), "wb") as f:
+        f.write(md)
+    for step, grids in enumerate(steps):
+        for g in grids:
+            with open(os.path.join(directory, f'{g["label"]}_{step}.bin'), "wb") as f:
+                f.write(_permute_chunks(xdmf_grid_bytes(g["data"], g["vec"], g["out_bytes"]), order))
+        with open(os.path.join(directory, f"step_{step}.xmf"), "w") as f:
+            f.write(xdmf_step_xml(om, grids, step, pts, conn))
+
+
+def _permute_chunks(b, order):
+    n = len(b) // 10
+    return b"".join(b[d * n:(d + 1) * n] for d in order)

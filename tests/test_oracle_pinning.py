@@ -15,7 +15,8 @@ import numpy as np
 import pytest
 
 from helpers import rel
-from oracle_lib import (Mesh, chebyshev_smoother, fgmres, kerngen_vcycles, laplace_vcycles, pbicgstab, pminres, power_iteration, ref_available, run_ref, stokes_block_fgmres,
+from oracle_lib import (Mesh, xdmf_geometry, xdmf_grid_bytes, xdmf_metadata, xdmf_read_grid, xdmf_step_xml,
+                        xdmf_topology, xdmf_write_dir, chebyshev_smoother, fgmres, kerngen_vcycles, laplace_vcycles, pbicgstab, pminres, power_iteration, ref_available, run_ref, stokes_block_fgmres,
                         stokes_block_minres)
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
@@ -325,6 +326,98 @@ def test_stokes_buoyancy_rhs_matches_reference(case, bcc, bcs):
     fv, T = G.timestep_inputs(fine)
     assert np.allclose(G.checksum(T), g["checksum_ts_T"], rtol=1e-13, atol=0)
     assert rel(fine.stokes_buoyancy_rhs(T, G.STOKES_RHS_RA, bcc, bcs), g[f"stokes_rhs_{bcc}{bcs}"]) <= TOL
+
+
+def test_fe_to_fv_matches_reference(case):
+    """l2_project_fe_to_fv (conversion.hpp:349-416): cell averages of the seeded FE temperature, lateral ghosts
+    updated, against the reference"""
+    g, fine, _, _ = case
+    _, T = G.timestep_inputs(fine)
+    ref = g["fe2fv"]
+    assert np.abs(fine.l2_project_fe_to_fv(T) - ref).max() <= 1e-15 * np.abs(ref).max()
+
+
+def _xdmf_grids(fine, coarse, step):
+    return [dict(label=lab, in_bytes=ib, out_bytes=ob, vec=v, data=a)
+            for lab, ib, ob, v, a in G.xdmf_fields(fine, coarse, step)]
+
+
+def test_xdmf_restatement_matches_reference_files(case):
+    """Every file io::XDMFOutput wrote for the fixture (tests/golden/xdmf_L2: geometry, topology, metadata, the
+    six grids of both writes, both .xmf steps) is byte for byte the restatement's"""
+    _, fine, coarse, _ = case
+    d = G.XDMF_DIR
+
+    def raw(name):
+        with open(os.path.join(d, name), "rb") as f:
+            return f.read()
+    assert raw("geometry.bin") == xdmf_geometry(fine, G.XDMF_PTS)
+    assert raw("topology.bin") == xdmf_topology(fine, G.XDMF_CONN)
+    assert raw("checkpoint_metadata.bin") == xdmf_metadata(fine, _xdmf_grids(fine, coarse, 0), G.XDMF_PTS)
+    for step in (0, 1):
+        grids = _xdmf_grids(fine, coarse, step)
+        for gr in grids:
+            assert raw(f'{gr["label"]}_{step}.bin') == xdmf_grid_bytes(gr["data"], gr["vec"], gr["out_bytes"]), gr["label"]
+        assert raw(f"step_{step}.xmf").decode() == xdmf_step_xml(fine, grids, step, G.XDMF_PTS, G.XDMF_CONN)
+    assert sorted(os.listdir(d)) == sorted(
+        ["README.md", "geometry.bin", "topology.bin", "checkpoint_metadata.bin"]
+        + [f"{lab}_{s}.bin" for lab, *_ in G.XDMF_GRIDS for s in (0, 1)] + ["step_0.xmf", "step_1.xmf"])
+
+
+def test_xdmf_reader_restatement(case):
+    """read_xdmf_checkpoint_grid restated: every grid of the reference's checkpoint reads back as written
+    (FP32 outputs as the cast of the input)"""
+    _, fine, coarse, _ = case
+    for step in (0, 1):
+        for gr in _xdmf_grids(fine, coarse, step):
+            want = gr["data"].astype(np.float32 if gr["out_bytes"] == 4 else np.float64).astype(np.float64)
+            got = xdmf_read_grid(G.XDMF_DIR, gr["label"], step, fine, gr["vec"] == 3)
+            assert np.array_equal(got, want), gr["label"]
+
+
+@pytest.mark.skipif(not ref_available(), reason="compiled reference not built")
+def test_xdmf_live_against_reference():
+    """Live, at level 3: FP64 points and int32 connectivity written by the reference equal the restatement;
+    the reference's reader recovers the grids of a checkpoint the restatement wrote with the diamonds' chunks
+    in a shuffled order (the metadata's subdomain ids say where each is)."""
+    fine, coarse = Mesh(3), Mesh(2)
+    rs = np.random.RandomState(77)
+    T = fine.make_consistent(rs.normal(size=fine.shape)).reshape(fine.shape)
+    u = rs.normal(size=(3,) + fine.shape)
+    with tempfile.TemporaryDirectory() as d:
+        T.tofile(f"{d}/T.bin")
+        u.tofile(f"{d}/u.bin")
+        run_ref(["xdmf_write", 3, 0.55, 1.0, 8, 4, d], d)
+        # FP64 coordinates to one unit in the last place: this build of the reference contracts the sum of
+        # squares of its normalisation (dense/vec.hpp:76-97) into FMAs (-march=x86-64-v3); the oracle does not
+        ref_geo = np.fromfile(f"{d}/xdmf/geometry.bin")
+        geo = np.frombuffer(xdmf_geometry(fine, 8), dtype=np.float64)
+        assert np.abs(ref_geo - geo).max() <= 2.3e-16
+        with open(f"{d}/xdmf/topology.bin", "rb") as f:
+            assert f.read() == xdmf_topology(fine, 4)
+        with open(f"{d}/xdmf/u64_1.bin", "rb") as f:
+            assert f.read() == xdmf_grid_bytes(2 * u, 3, 8)
+        order = [3, 7, 0, 9, 1, 5, 2, 8, 6, 4]
+        grids = [dict(label="T", in_bytes=8, out_bytes=8, vec=1, data=T),
+                 dict(label="u_u", in_bytes=8, out_bytes=4, vec=3, data=u)]
+        xdmf_write_dir(f"{d}/ck", fine, [grids], pts=4, conn=8, order=order)
+        run_ref(["xdmf_read", 3, 0.55, 1.0, "T", 0, 0, f"{d}/ck", d], d)
+        assert np.array_equal(np.fromfile(f"{d}/out.bin").reshape(fine.shape), T)
+        run_ref(["xdmf_read", 3, 0.55, 1.0, "u_u", 0, 1, f"{d}/ck", d], d)
+        got = np.fromfile(f"{d}/out.bin").reshape((3,) + fine.shape)
+        assert np.array_equal(got, u.astype(np.float32).astype(np.float64))
+        assert np.array_equal(xdmf_read_grid(f"{d}/ck", "u_u", 0, fine, True), got)
+
+
+@pytest.mark.skipif(not ref_available(), reason="compiled reference not built")
+def test_fe_to_fv_live_against_reference():
+    fine = Mesh(3)
+    T = fine.make_consistent(np.random.RandomState(78).uniform(size=fine.shape)).reshape(fine.shape)
+    with tempfile.TemporaryDirectory() as d:
+        T.tofile(f"{d}/T.bin")
+        run_ref(["fe2fv", 3, 0.55, 1.0, d], d)
+        ref = np.fromfile(f"{d}/fv.bin").reshape(fine.fv_shape)
+    assert np.abs(fine.l2_project_fe_to_fv(T) - ref).max() <= 1e-15 * np.abs(ref).max()
 
 
 def test_golden_fixture_is_not_trivial(case):

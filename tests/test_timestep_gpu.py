@@ -124,5 +124,8 @@ def test_mantle_timestep_pieces_match_oracle():
     N = om.N
     inner = (slice(None), slice(1, N + 1), slice(1, N + 1), slice(1, N + 1))
     assert rel(ts.T_fv.cpu().numpy()[inner], T1[inner]) <= 1e-12
-    assert rel(ts.T.numpy()[0], om.l2_project_fv_to_fe(ts.T_fv.cpu().numpy())) <= 1e-10
+    # the step's projection is warm-started from the previous FE temperature, the oracle's from zero: both
+    # PCG runs stop at 1e-12 of their own initial residual, so the iterates agree to the mass matrix's
+    # condition number times that
+    assert rel(ts.T.numpy()[0], om.l2_project_fv_to_fe(ts.T_fv.cpu().numpy())) <= 1e-9
     assert ts.step() and ts.last["finite"]
