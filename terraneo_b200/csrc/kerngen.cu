@@ -476,145 +476,186 @@ __device__ __forceinline__ void project_out( const T n[3], T v[3] )
     v[0] -= dt * n[0], v[1] -= dt * n[1], v[2] -= dt * n[2];
 }
 
-// Full contribution of cell (d, x, y, r) to its 8 nodes, acc[dx][dy][dr][c].
-template < typename T >
-__device__ void cell_full( const CellParams< T >& P, int d, int x, int y, int r, T acc[2][2][2][3] )
+// Free-slip rows of the cell's nodes on layer r + DR: the tangential projection of the accumulated rows plus
+// the normal-normal term ann (n . src) n.  DR is a template argument so every acc / ann index is compile-time
+// (a run-time choice of the layer puts both arrays in local memory).
+template < int DR, typename T >
+__device__ __forceinline__ void freeslip_rows( const CellParams< T >& P, int d, int x, int y, int r, T acc[2][2][2][3],
+                                               const T ann[2][2][2] )
+{
+    const int n1 = P.n1;
+#pragma unroll
+    for ( int dx = 0; dx < 2; ++dx )
+#pragma unroll
+        for ( int dy = 0; dy < 2; ++dy )
+        {
+            const size_t  lat = lat_index( n1, d, x + dx, y + dy );
+            const double* u   = P.coords + lat * 3;
+            T             n[3] = { T( u[0] ), T( u[1] ), T( u[2] ) };
+            const T       im   = rsqrt( n[0] * n[0] + n[1] * n[1] + n[2] * n[2] );
+            n[0] *= im, n[1] *= im, n[2] *= im;
+            T* o = acc[dx][dy][DR];
+            project_out( n, o );
+            const size_t i  = lat * n1 + r + DR;
+            const T      un = n[0] * P.src.p[0][i] + n[1] * P.src.p[1][i] + n[2] * P.src.p[2][i];
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+                o[c] += ann[dx][dy][DR] * un * n[c];
+        }
+}
+
+// Full contribution of cell (d, x, y, r) to its 8 nodes, acc[dx][dy][dr][c].  DIAG: the diagonal-mode apply
+// (kerngen :540-575).  Every per-node array is indexed with compile-time indices (loops fully unrolled,
+// wedge_node), so none of them goes to local memory; the unit normals are kept per lateral vertex (the top
+// and bottom nodes of a wedge share them), and one source array holds the source (DIAG) or the source with
+// the normal part of free-slip nodes removed (the only form the full apply reads).
+template < bool DIAG, typename T >
+__device__ __forceinline__ void cell_full( const CellParams< T >& P, int d, int x, int y, int r, T acc[2][2][2][3] )
 {
     const int  N = P.N, n1 = P.n1;
     const bool at_cmb = r == 0, at_surf = r == N - 1;
     const bool cmb_dir = at_cmb && P.bc_cmb == TN_BC_DIRICHLET, surf_dir = at_surf && P.bc_surf == TN_BC_DIRICHLET;
     const bool cmb_fs = at_cmb && P.bc_cmb == TN_BC_FREESLIP, surf_fs = at_surf && P.bc_surf == TN_BC_FREESLIP;
-    const bool diag = P.diag != 0;
 
     T ann[2][2][2];
 #pragma unroll
     for ( int i = 0; i < 8; ++i )
     {
         ann[i >> 2][( i >> 1 ) & 1][i & 1] = T( 0 );
+#pragma unroll
         for ( int c = 0; c < 3; ++c )
             acc[i >> 2][( i >> 1 ) & 1][i & 1][c] = T( 0 );
     }
     const T r0 = P.radii[d * n1 + r], r1 = P.radii[d * n1 + r + 1];
 
+#pragma unroll
     for ( int w = 0; w < 2; ++w )
     {
-        T      p[3][3];
-        T      kn[6], s[6][3], sp[6][3], nrm[6][3];
-        size_t idx[6];
+        T p[3][3], nrm[3][3], kn[6], v[6][3];
+#pragma unroll
         for ( int n = 0; n < 6; ++n )
         {
-            const int X = x + kWedgeNode[w][n][0], Y = y + kWedgeNode[w][n][1], R = r + kWedgeNode[w][n][2];
+            const int X = x + wedge_node( w, n, 0 ), Y = y + wedge_node( w, n, 1 ), R = r + wedge_node( w, n, 2 );
             const size_t  lat = lat_index( n1, d, X, Y );
             const double* u   = P.coords + lat * 3;
             if ( n < 3 )
+            {
+#pragma unroll
                 for ( int a = 0; a < 3; ++a )
                     p[n][a] = T( u[a] );
-            idx[n] = lat * n1 + R;
-            kn[n]  = P.k[idx[n]];
-            // outward unit normals, needed by free-slip layers only (one reciprocal square root)
-            T nn[3] = { T( u[0] ), T( u[1] ), T( u[2] ) };
-            const T im = ( cmb_fs || surf_fs ) ? rsqrt( nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2] ) : T( 0 );
-            for ( int c = 0; c < 3; ++c )
-            {
-                nrm[n][c] = nn[c] * im;
-                s[n][c] = sp[n][c] = P.src.p[c][idx[n]];
+                // outward unit normals, needed by free-slip layers only (one reciprocal square root)
+                T       nn[3] = { T( u[0] ), T( u[1] ), T( u[2] ) };
+                const T im    = ( cmb_fs || surf_fs ) ? rsqrt( nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2] ) : T( 0 );
+#pragma unroll
+                for ( int c = 0; c < 3; ++c )
+                    nrm[n][c] = nn[c] * im;
             }
-            if ( ( cmb_fs && n < 3 ) || ( surf_fs && n >= 3 ) )
-                project_out( nrm[n], sp[n] );
+            const size_t id = lat * n1 + R;
+            kn[n]           = P.k[id];
+#pragma unroll
+            for ( int c = 0; c < 3; ++c )
+                v[n][c] = P.src.at( c )[id];
+            if constexpr ( !DIAG )
+                if ( ( cmb_fs && n < 3 ) || ( surf_fs && n >= 3 ) )
+                    project_out( nrm[n % 3], v[n] );
         }
         T       IT[3][3];
         const T third = T( 1.0 / 3.0 );
         const T det   = wedge_jacobian_it( p[0], p[1], p[2], r0, r1, third, third, T( 0 ), IT );
         T       ksum  = 0;
+#pragma unroll
         for ( int n = 0; n < 6; ++n )
             ksum += kn[n];
         const T kwJ = ( ksum / T( 6 ) ) * fabs( det );
         T       g[6][3];
+#pragma unroll
         for ( int n = 0; n < 6; ++n )
         {
             T gr[3];
             grad_shape_ref( n, third, third, T( 0 ), gr );
+#pragma unroll
             for ( int a = 0; a < 3; ++a )
                 g[n][a] = IT[a][0] * gr[0] + IT[a][1] * gr[1] + IT[a][2] * gr[2];
         }
-        if ( !diag )
+        if constexpr ( !DIAG )
         {
             T G[3][3] = { { 0 } };
+#pragma unroll
             for ( int n = 0; n < 6; ++n )
             {
                 if ( ( cmb_dir && n < 3 ) || ( surf_dir && n >= 3 ) )
                     continue;
+#pragma unroll
                 for ( int a = 0; a < 3; ++a )
+#pragma unroll
                     for ( int bb = 0; bb < 3; ++bb )
-                        G[a][bb] += g[n][a] * sp[n][bb];
+                        G[a][bb] += g[n][a] * v[n][bb];
             }
             const T div = G[0][0] + G[1][1] + G[2][2];
             T       E[3][3];
+#pragma unroll
             for ( int a = 0; a < 3; ++a )
+#pragma unroll
                 for ( int bb = 0; bb < 3; ++bb )
                     E[a][bb] = T( 0.5 ) * ( G[a][bb] + G[bb][a] );
+#pragma unroll
             for ( int n = 0; n < 6; ++n )
             {
                 if ( ( cmb_dir && n < 3 ) || ( surf_dir && n >= 3 ) )
                     continue;
-                T* o = acc[kWedgeNode[w][n][0]][kWedgeNode[w][n][1]][kWedgeNode[w][n][2]];
+                T* o = acc[wedge_node( w, n, 0 )][wedge_node( w, n, 1 )][wedge_node( w, n, 2 )];
+#pragma unroll
                 for ( int c = 0; c < 3; ++c )
                     o[c] += kwJ * ( T( 2 ) * ( g[n][0] * E[0][c] + g[n][1] * E[1][c] + g[n][2] * E[2][c] ) -
                                     T( 2.0 / 3.0 ) * g[n][c] * div );
                 if ( ( cmb_fs && n < 3 ) || ( surf_fs && n >= 3 ) )
                 {
-                    const T gg = g[n][0] * g[n][0] + g[n][1] * g[n][1] + g[n][2] * g[n][2];
-                    const T ng = nrm[n][0] * g[n][0] + nrm[n][1] * g[n][1] + nrm[n][2] * g[n][2];
-                    ann[kWedgeNode[w][n][0]][kWedgeNode[w][n][1]][kWedgeNode[w][n][2]] += kwJ * ( gg + ng * ng * third );
+                    const T* nv = nrm[n % 3];
+                    const T  gg = g[n][0] * g[n][0] + g[n][1] * g[n][1] + g[n][2] * g[n][2];
+                    const T  ng = nv[0] * g[n][0] + nv[1] * g[n][1] + nv[2] * g[n][2];
+                    ann[wedge_node( w, n, 0 )][wedge_node( w, n, 1 )][wedge_node( w, n, 2 )] += kwJ * ( gg + ng * ng * third );
                 }
             }
         }
+        // kept diagonal of Dirichlet nodes (there v is the unprojected source), or the diagonal mode
+#pragma unroll
         for ( int n = 0; n < 6; ++n )
         {
             const bool is_dir = ( cmb_dir && n < 3 ) || ( surf_dir && n >= 3 );
             const bool is_fs  = ( cmb_fs && n < 3 ) || ( surf_fs && n >= 3 );
-            if ( !( diag || is_dir ) )
+            if ( !( DIAG || is_dir ) )
                 continue;
-            T*      o  = acc[kWedgeNode[w][n][0]][kWedgeNode[w][n][1]][kWedgeNode[w][n][2]];
+            T*      o  = acc[wedge_node( w, n, 0 )][wedge_node( w, n, 1 )][wedge_node( w, n, 2 )];
             const T gg = g[n][0] * g[n][0] + g[n][1] * g[n][1] + g[n][2] * g[n][2];
-            if ( diag && is_fs )
+            if ( DIAG && is_fs )
             {
-                T R[3][3], v[3];
-                trafo_normal_tangential( nrm[n], R );
+                T R[3][3], q[3];
+                trafo_normal_tangential( nrm[n % 3], R );
+#pragma unroll
                 for ( int a = 0; a < 3; ++a )
                 {
                     const T Rg = R[a][0] * g[n][0] + R[a][1] * g[n][1] + R[a][2] * g[n][2];
-                    const T Rs = R[a][0] * s[n][0] + R[a][1] * s[n][1] + R[a][2] * s[n][2];
-                    v[a]       = kwJ * ( gg + Rg * Rg * third ) * Rs;
+                    const T Rs = R[a][0] * v[n][0] + R[a][1] * v[n][1] + R[a][2] * v[n][2];
+                    q[a]       = kwJ * ( gg + Rg * Rg * third ) * Rs;
                 }
+#pragma unroll
                 for ( int c = 0; c < 3; ++c )
-                    o[c] += R[0][c] * v[0] + R[1][c] * v[1] + R[2][c] * v[2];
+                    o[c] += R[0][c] * q[0] + R[1][c] * q[1] + R[2][c] * q[2];
             }
             else
             {
+#pragma unroll
                 for ( int c = 0; c < 3; ++c )
-                    o[c] += kwJ * s[n][c] * ( gg + g[n][c] * g[n][c] * third );
+                    o[c] += kwJ * v[n][c] * ( gg + g[n][c] * g[n][c] * third );
             }
         }
     }
-    if ( !diag && ( cmb_fs || surf_fs ) )
+    if constexpr ( !DIAG )
     {
-        const int dr = cmb_fs ? 0 : 1;
-        for ( int dx = 0; dx < 2; ++dx )
-            for ( int dy = 0; dy < 2; ++dy )
-            {
-                const size_t  lat = lat_index( n1, d, x + dx, y + dy );
-                const double* u   = P.coords + lat * 3;
-                T             n[3] = { T( u[0] ), T( u[1] ), T( u[2] ) };
-                const T       im   = rsqrt( n[0] * n[0] + n[1] * n[1] + n[2] * n[2] );
-                n[0] *= im, n[1] *= im, n[2] *= im;
-                T* o = acc[dx][dy][dr];
-                project_out( n, o );
-                const size_t i  = lat * n1 + r + dr;
-                const T      un = n[0] * P.src.p[0][i] + n[1] * P.src.p[1][i] + n[2] * P.src.p[2][i];
-                for ( int c = 0; c < 3; ++c )
-                    o[c] += ann[dx][dy][dr] * un * n[c];
-            }
+        if ( cmb_fs )
+            freeslip_rows< 0 >( P, d, x, y, r, acc, ann );
+        else if ( surf_fs )
+            freeslip_rows< 1 >( P, d, x, y, r, acc, ann );
     }
 }
 
@@ -631,14 +672,21 @@ __global__ void __launch_bounds__( 128 ) kerngen_cell_kernel( CellParams< T > P 
     const int x = int( ( t / ( (long long) N * N ) ) % N );
     const int d = int( t / ( (long long) N * N * N ) );
     T         acc[2][2][2][3];
-    cell_full( P, d, x, y, r, acc );
+    if ( P.diag )
+        cell_full< true >( P, d, x, y, r, acc );
+    else
+        cell_full< false >( P, d, x, y, r, acc );
+#pragma unroll
     for ( int dx = 0; dx < 2; ++dx )
+#pragma unroll
         for ( int dy = 0; dy < 2; ++dy )
+#pragma unroll
             for ( int dr = 0; dr < 2; ++dr )
             {
                 const size_t i = lat_index( n1, d, x + dx, y + dy ) * n1 + r + dr;
+#pragma unroll
                 for ( int c = 0; c < 3; ++c )
-                    atomicAdd( P.dst.p[c] + i, acc[dx][dy][dr][c] );
+                    atomicAdd( P.dst.at( c ) + i, acc[dx][dy][dr][c] );
             }
 }
 
@@ -647,8 +695,11 @@ __global__ void __launch_bounds__( 128 ) kerngen_cell_kernel( CellParams< T > P 
 // boundary treatment of cell_full, atomics onto the values the tile kernel
 // wrote (it leaves these cells out).  Neighbouring threads are neighbouring
 // cells in y of one layer.
+#ifndef TN_BCELL_MINBLOCKS
+#define TN_BCELL_MINBLOCKS 1 // resident 128-thread blocks per SM the boundary-cell kernel is compiled for
+#endif
 template < typename T >
-__global__ void __launch_bounds__( 128 ) kerngen_bcell_kernel( CellParams< T > P, int sides )
+__global__ void __launch_bounds__( 128, TN_BCELL_MINBLOCKS ) kerngen_bcell_kernel( CellParams< T > P, int sides )
 {
     const int       N = P.N, n1 = P.n1;
     const long long per = (long long) kDiamonds * N * N;
@@ -661,14 +712,18 @@ __global__ void __launch_bounds__( 128 ) kerngen_bcell_kernel( CellParams< T > P
     const int x    = int( ( t / N ) % N );
     const int d    = int( ( t % per ) / ( (long long) N * N ) );
     T         acc[2][2][2][3];
-    cell_full( P, d, x, y, r, acc );
+    cell_full< false >( P, d, x, y, r, acc );
+#pragma unroll
     for ( int dx = 0; dx < 2; ++dx )
+#pragma unroll
         for ( int dy = 0; dy < 2; ++dy )
+#pragma unroll
             for ( int dr = 0; dr < 2; ++dr )
             {
                 const size_t i = lat_index( n1, d, x + dx, y + dy ) * n1 + r + dr;
+#pragma unroll
                 for ( int c = 0; c < 3; ++c )
-                    atomicAdd( P.dst.p[c] + i, acc[dx][dy][dr][c] );
+                    atomicAdd( P.dst.at( c ) + i, acc[dx][dy][dr][c] );
             }
 }
 

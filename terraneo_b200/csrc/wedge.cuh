@@ -14,6 +14,14 @@ static __device__ __constant__ const int kWedgeNode[2][6][3] = {
     { { 1, 1, 0 }, { 0, 1, 0 }, { 1, 0, 0 }, { 1, 1, 1 }, { 0, 1, 1 }, { 1, 0, 1 } } };
 
 __host__ __device__ inline size_t lat_index( int n1, int d, int x, int y ) { return ( size_t( d ) * n1 + x ) * n1 + y; }
+// kWedgeNode as a constant expression: offset k (0: x, 1: y, 2: r) of node n of wedge w.  In fully
+// unrolled loops the indices it yields are compile-time, so per-node arrays indexed with them stay in
+// registers (indexing through the __constant__ table puts them in local memory).
+__host__ __device__ constexpr int wedge_node( int w, int n, int k )
+{
+    return k == 2 ? int( n >= 3 ) : ( w == 0 ? int( n % 3 == ( k == 0 ? 1 : 2 ) ) : int( n % 3 != ( k == 0 ? 1 : 2 ) ) );
+}
+
 
 // Lateral triangle matrix M = [p1-p0, p2-p0, (p0+p1+p2)/3] of a wedge.  For
 // the one-point rule J = M diag(r_mid, r_mid, dr/2); Q = M^{-T}.  Writes Q's
