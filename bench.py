@@ -37,7 +37,7 @@ BYTES_PER_NODE_F64 = 56  # 3 src + 1 k + 3 dst doubles per stored node
 BYTES_PER_NODE_F32 = 28
 # DRAM bytes (read + write) of one level-6 kerngen_tile_kernel<double> launch,
 # from an ncu capture (profiles/kerngen_tile_kernel_f64_L6_dirichlet.md)
-TILE_TRAFFIC_BYTES = 126152192 + 39593216
+TILE_TRAFFIC_BYTES = 135726080 + 49133312
 
 
 def _case_laplace6(shell, C, torch):
@@ -875,8 +875,53 @@ def main():
         h_dst.copy_(e_dst.data, non_blocking=True)
     ev1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1) / e2e_steps, world, "cuda")
+    e2e_serial_ms = max_over_ranks(ev0.elapsed_time(ev1) / e2e_steps, world, "cuda")
     vec_bytes = 3 * mesh.stored_nodes * 8
+
+    # the same end-to-end steps pipelined as a serving loop runs them: step i's host->device copy on an input
+    # stream and its device->host copy on an output stream overlap the neighbouring steps' applies (two
+    # device buffer pairs, two pinned result buffers; events order each buffer's reuse)
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    p_src = [shell.VectorQ1Vec(mesh) for _ in range(2)]
+    p_dst = [shell.VectorQ1Vec(mesh) for _ in range(2)]
+    h_out = [torch.empty_like(h_src).pin_memory() for _ in range(2)]
+
+    def pipelined(nsteps, start):
+        ev_in = [torch.cuda.Event() for _ in range(2)]
+        ev_comp = [torch.cuda.Event() for _ in range(2)]
+        ev_out = [torch.cuda.Event() for _ in range(2)]
+        s_in.wait_event(start)
+        s_out.wait_event(start)
+        for i in range(nsteps):
+            b = i % 2
+            with torch.cuda.stream(s_in):
+                if i >= 2:
+                    s_in.wait_event(ev_comp[b])          # the apply of step i-2 has read p_src[b]
+                p_src[b].data.copy_(h_src, non_blocking=True)
+                ev_in[b].record(s_in)
+            stream.wait_event(ev_in[b])
+            if i >= 2:
+                stream.wait_event(ev_out[b])             # step i-2's result has left p_dst[b]
+            shell.apply(op, p_src[b], p_dst[b])
+            ev_comp[b].record(stream)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_comp[b])
+                h_out[b].copy_(p_dst[b].data, non_blocking=True)
+                ev_out[b].record(s_out)
+        for b in range(min(2, nsteps)):
+            stream.wait_event(ev_out[b])
+
+    st0 = torch.cuda.Event()
+    st0.record(stream)
+    pipelined(3, st0)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    pipelined(e2e_steps, ev0)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1) / e2e_steps, world, "cuda")
+    # the last results arrived: compare with the serial loop's
+    e2e_check = float((h_out[(e2e_steps - 1) % 2] - h_dst).abs().max())
 
     if rank == 0:
         line = {
@@ -898,7 +943,12 @@ def main():
             "fp32_apply": {"value": round(whole_job_gdofs(world, dofs, ms32), 3), "unit": "GDoF/s",
                            "ms_per_step": round(ms32, 5)},
             "e2e": {"value": round(whole_job_gdofs(world, dofs, e2e_ms), 3), "unit": "GDoF/s",
-                    "h2d_bytes_per_step": vec_bytes, "d2h_bytes_per_step": vec_bytes},
+                    "h2d_bytes_per_step": vec_bytes, "d2h_bytes_per_step": vec_bytes,
+                    "form": "pinned host src -> device, apply, device -> pinned host dst every step; copies on "
+                            "their own streams overlap the neighbouring steps' applies",
+                    "serial": {"value": round(whole_job_gdofs(world, dofs, e2e_serial_ms), 3),
+                               "form": "copy in, apply, copy out one after another on one stream"},
+                    "max_abs_diff_vs_serial": e2e_check},
             "gpu_launches": 3 * args.steps,
             "clocks": clk.summary(),
         }
