@@ -119,7 +119,7 @@ def level5_adjoint():
     grad = torch.empty(pf.shape, dtype=torch.float64, device="cuda")
     solver.viscosity_backward(xu, gu, grad, C.COMM_SKIP, lam_u, lam_p)
     return dict(om=om, pf=pf, pc=pc, k0=k0, fu=fu, fp=fp, kw=kw, owned=owned, u_obs=u_obs, u=xu.numpy(),
-                lam=lam_u.numpy(), grad=grad.cpu().numpy(), L=L)
+                p=xp.numpy(), lam=lam_u.numpy(), grad=grad.cpu().numpy(), L=L)
 
 
 def test_gradient_matches_reference_directional_derivative_level5(level5_adjoint):
@@ -150,24 +150,33 @@ def test_gradient_matches_reference_directional_derivative_level5(level5_adjoint
 
 
 def test_gradient_matches_central_differences_level5(level5_adjoint):
-    """Central differences with step 1e-6 in 4 seeded smooth directions at the level-5 configuration, every
-    solve to 1e-14: agreement to 1e-6 relative."""
-    from terraneo_b200.adjoint import stokes_velocity
+    """Central differences with step 1e-6 in 4 seeded smooth directions at the level-5 configuration: the
+    perturbed solves start from the unperturbed solution (FGMRES to 1e-10 of their O(h) initial residual, at
+    most 150 iterations), so the difference of the two solutions is not swamped by the solver tolerance;
+    agreement to 1e-7 relative (cold starts to 1e-14 agree to about 1e-5)."""
+    from terraneo_b200 import shell
     a = level5_adjoint
-    om, pf, fu, fp, kw, owned, u_obs = a["om"], a["pf"], a["fu"], a["fp"], a["kw"], a["owned"], a["u_obs"]
+    om, pf, pc, fu, fp, kw, owned, u_obs = (a["om"], a["pf"], a["pc"], a["fu"], a["fp"], a["kw"], a["owned"],
+                                            a["u_obs"])
     m0 = torch.as_tensor(np.log(a["k0"]), device="cuda")
     grad = torch.as_tensor(a["grad"], device="cuda")
+    u0, p0 = torch.as_tensor(a["u"], device="cuda"), torch.as_tensor(a["p"], device="cuda")
+    kw_warm = dict(kw, relative_tolerance=1e-10, max_iterations=150)
+    kv = shell.VectorQ1Scalar(pf)
 
     def J(m):
-        uu = stokes_velocity(m, a["L"], fu, fp, **kw)
-        return 0.5 * (owned * (uu - u_obs) ** 2).sum()
+        kv.data[0].copy_(torch.exp(m))
+        s = shell.StokesSolver(a["L"], kv, **kw_warm)
+        yu = shell.VectorQ1Vec(pf, data=u0.clone())
+        yp = shell.VectorQ1Scalar(pc, data=p0.clone())
+        s.solve(fu, fp, yu, yp)
+        return float(0.5 * (owned * (yu.data - u_obs) ** 2).sum())
 
     h = 1e-6
     errs = []
     for s in range(4):
         d = torch.as_tensor(_smooth_direction(om, 400 + s), device="cuda")
-        with torch.no_grad():
-            fd = (J(m0 + h * d) - J(m0 - h * d)).item() / (2 * h)
+        fd = (J(m0 + h * d) - J(m0 - h * d)) / (2 * h)
         ad = float((grad * d).sum())
         errs.append(abs(fd - ad) / abs(ad))
-    assert max(errs) <= 1e-6, errs
+    assert max(errs) <= 1e-7, errs
