@@ -589,6 +589,29 @@ TN_API int tn_pressure_remove_mean_f64( const tn_mesh* mesh, double* p, double* 
  * (tn_fv_ghost_update_f64).  Radial ghost cells are left as they are.  fv: [10][N+2]^3. */
 TN_API int tn_l2_project_fe_to_fv_f64( const tn_mesh* mesh, const double* fe, double* fv, void* stream );
 
+/* ---- SUPG energy operator ----------------------------------------------- */
+/* UnsteadyAdvectionDiffusionSUPG::apply_impl (fe/wedge/operators/shell/unsteady_advection_diffusion_supg.hpp:
+ * 199-420): dst = (mass_scaling M + dt (K + C + G)) src, the BDF left-hand side of the temperature equation with
+ * SUPG stabilisation for the velocity vel (three SoA components), constant diffusivity kappa, mass lumping,
+ * the reference's boundary mask (treat_boundary: off-diagonal entries of CMB / surface rows and columns
+ * dropped) and diagonal mode; apply / communication modes as the other operators. */
+TN_API int tn_supg_apply_f64( const tn_mesh* mesh, const double* const* vel, double kappa, double dt, double mass_scaling,
+                              int lumped_mass, int treat_boundary, int diagonal, int apply_mode, int comm_mode,
+                              const double* src, double* dst, void* stream );
+TN_API int tn_supg_apply_f32( const tn_mesh* mesh, const float* const* vel, double kappa, double dt, double mass_scaling,
+                              int lumped_mass, int treat_boundary, int diagonal, int apply_mode, int comm_mode,
+                              const float* src, float* dst, void* stream );
+/* One implicit BDF step of the SUPG temperature equation as the reference's tests solve it
+ * (tests/test_unsteady_advection_diffusion_supg.cpp:124-172): x <- solution of
+ * (mass_scaling M + dt (K + C + G)) x = rhs with PBiCGStab(l) (pbicgstab.hpp:29-290, no preconditioner) from the
+ * given x, at most max_iterations iterations, stopping at relative_tolerance (of the initial residual) or
+ * absolute_tolerance.  vel: one contiguous [3][nodes] array (vel[1] = vel[0] + nodes, vel[2] = vel[0] + 2 nodes).
+ * work: (2 (l + 1) + 2) stored-node FP64 fields.  iterations / relative_residual: optional outputs.  Synchronises. */
+TN_API int tn_supg_solve_f64( const tn_mesh* mesh, const double* const* vel, double kappa, double dt, double mass_scaling,
+                              int lumped_mass, int treat_boundary, const double* rhs, double* x, int l, int max_iterations,
+                              double relative_tolerance, double absolute_tolerance, double* work, int* iterations,
+                              double* relative_residual, void* stream );
+
 /* ---- XDMF output and checkpoints (io/xdmf.hpp) -------------------------- */
 /* io::XDMFOutput (io/xdmf.hpp:147-1115): a time series of node fields in the reference's directory format,
  * which is both the visualisation output and the checkpoint: geometry.bin, topology.bin and

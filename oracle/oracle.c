@@ -2115,3 +2115,125 @@ void or_fe_to_fv( int L, const double* coords, const double* radii, const double
                 }
     or_fv_ghost_update( L, coords, fv );
 }
+
+/* ------------------------------------------------------------------------ */
+/* UnsteadyAdvectionDiffusionSUPG (fe/wedge/operators/shell/                 */
+/* unsteady_advection_diffusion_supg.hpp:16-50, 243-420)                     */
+/* ------------------------------------------------------------------------ */
+
+/* supg_tau (:16-50): h / (2 |u|) (coth(Pe) - 1 / Pe), Pe = |u| h / (2 max(kappa, 1e-8)), zero for |u| <= 1e-12
+ * or Pe <= Pe_tol, clamped to 10 h / |u| */
+static double supg_tau( double vel_norm, double kappa, double h, double pe_tol )
+{
+    const double kv = kappa > 1e-8 ? kappa : 1e-8;
+    if ( vel_norm <= 1e-12 )
+        return 0.0;
+    const double pe = vel_norm * h / ( 2.0 * kv );
+    if ( pe <= pe_tol )
+        return 0.0;
+    const double tau_max = 10.0 * h / ( vel_norm > 1e-12 ? vel_norm : 1e-12 );
+    const double coth    = 1.0 / tanh( pe ) - 1.0 / pe;
+    const double tau     = ( h / ( 2.0 * vel_norm ) ) * coth;
+    return tau > tau_max ? tau_max : tau;
+}
+
+/* dst = (mass_scaling M + dt (K + C + G)) src per hex cell, the 6 x 6 wedge matrices built on the 3x2 rule with
+ * the velocity interpolated at the quadrature points and one tau per wedge (the weight-averaged pointwise tau,
+ * h = r2 - r1), then lumping (row sums of M), the boundary mask (off-diagonal entries of rows and columns of
+ * CMB / surface nodes zeroed), the diagonal mode, and the additive halo sum (:243-420). vel: [3][nodes]. */
+void or_supg_apply( int L, const double* coords, const double* radii, const double* vel, const double* src, double* dst,
+                    double kappa, double dt, double mass_scaling, int lumped, int treat_boundary, int diag )
+{
+    const int    N = 1 << L, n1 = N + 1;
+    const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1;
+    memset( dst, 0, ns * sizeof( double ) );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                {
+                    const double r1 = radii[d * n1 + r], r2 = radii[d * n1 + r + 1];
+                    const double h  = r2 - r1;
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        const double* p[3];
+                        wedge_lateral_points( n1, coords, d, x, y, w, p );
+                        size_t id[6];
+                        for ( int i = 0; i < 6; ++i )
+                            id[i] = node_idx( n1, d, x + WNODE[w][i][0], y + WNODE[w][i][1], r + WNODE[w][i][2] );
+                        double uq[6][3];
+                        for ( int q = 0; q < 6; ++q )
+                            for ( int c = 0; c < 3; ++c )
+                            {
+                                uq[q][c] = 0.0;
+                                for ( int i = 0; i < 6; ++i )
+                                    uq[q][c] += vel[(size_t) c * ns + id[i]] * shape_val( i, QP32[q][0], QP32[q][1], QP32[q][2] );
+                            }
+                        double tau_acc = 0.0, w_acc = 0.0;
+                        for ( int q = 0; q < 6; ++q )
+                        {
+                            const double vn = sqrt( uq[q][0] * uq[q][0] + uq[q][1] * uq[q][1] + uq[q][2] * uq[q][2] );
+                            tau_acc += supg_tau( vn, kappa, h, 1e-8 ) * QW32;
+                            w_acc += QW32;
+                        }
+                        const double tau = w_acc > 0.0 ? tau_acc / w_acc : 0.0;
+                        double       M[6][6] = { { 0 } }, A[6][6] = { { 0 } };
+                        for ( int q = 0; q < 6; ++q )
+                        {
+                            double J[3][3], IT[3][3], g[6][3], sh[6];
+                            wedge_jac( p, r1, r2, QP32[q][0], QP32[q][1], QP32[q][2], J );
+                            const double det = det3( J );
+                            inv_transposed3( J, det, IT );
+                            for ( int i = 0; i < 6; ++i )
+                            {
+                                double gr[3];
+                                grad_shape_ref( i, QP32[q][0], QP32[q][1], QP32[q][2], gr );
+                                for ( int a = 0; a < 3; ++a )
+                                    g[i][a] = IT[a][0] * gr[0] + IT[a][1] * gr[1] + IT[a][2] * gr[2];
+                                sh[i] = shape_val( i, QP32[q][0], QP32[q][1], QP32[q][2] );
+                            }
+                            const double ad = fabs( det );
+                            for ( int i = 0; i < 6; ++i )
+                                for ( int j = 0; j < 6; ++j )
+                                {
+                                    const double mass = sh[i] * sh[j];
+                                    const double diff = kappa * ( g[i][0] * g[j][0] + g[i][1] * g[j][1] + g[i][2] * g[j][2] );
+                                    const double ugj  = uq[q][0] * g[j][0] + uq[q][1] * g[j][1] + uq[q][2] * g[j][2];
+                                    const double ugi  = uq[q][0] * g[i][0] + uq[q][1] * g[i][1] + uq[q][2] * g[i][2];
+                                    M[i][j] += QW32 * mass_scaling * mass * ad;
+                                    A[i][j] += QW32 * dt * ( diff + ugj * sh[i] + tau * ugj * ugi ) * ad;
+                                }
+                        }
+                        if ( lumped )
+                            for ( int i = 0; i < 6; ++i )
+                            {
+                                double s = 0.0;
+                                for ( int j = 0; j < 6; ++j )
+                                    s += M[i][j];
+                                for ( int j = 0; j < 6; ++j )
+                                    M[i][j] = i == j ? s : 0.0;
+                            }
+                        if ( treat_boundary )
+                        {
+                            const int cmb = r == 0, surf = r + 1 == N;
+                            for ( int i = 0; i < 6; ++i )
+                                for ( int j = 0; j < 6; ++j )
+                                    if ( i != j && ( ( cmb && ( i < 3 || j < 3 ) ) || ( surf && ( i >= 3 || j >= 3 ) ) ) )
+                                        M[i][j] = A[i][j] = 0.0;
+                        }
+                        if ( diag )
+                            for ( int i = 0; i < 6; ++i )
+                                for ( int j = 0; j < 6; ++j )
+                                    if ( i != j )
+                                        M[i][j] = A[i][j] = 0.0;
+                        for ( int i = 0; i < 6; ++i )
+                        {
+                            double s = 0.0;
+                            for ( int j = 0; j < 6; ++j )
+                                s += ( M[i][j] + A[i][j] ) * src[id[j]];
+                            dst[id[i]] += s;
+                        }
+                    }
+                }
+    or_halo_sum( L, coords, dst, 1 );
+}

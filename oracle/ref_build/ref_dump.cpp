@@ -62,6 +62,8 @@
 //                                          into a FP64 grid (vec 0: scalar, 1: 3-vector): out.bin; the metadata
 //                                          as text in meta.txt; on a read error its message in error.txt, exit 3
 //   fe2fv L rmin rmax DIR                  l2_project_fe_to_fv of T.bin (FE): fv.bin ([10][N+2]^3, ghosts set)
+//   supg L rmin rmax kappa dt ms lumped treat diag DIR  UnsteadyAdvectionDiffusionSUPG<double> with the velocity
+//                                          vel.bin (3 x nodes) applied to src.bin: dst.bin
 //   time_kerngen L rmin rmax bcc bcs reps [DIR]  prints seconds per apply (CPU baseline); with DIR the
 //                                          inputs are k.bin / src.bin there, else k = 1, src = 1
 #include <chrono>
@@ -87,6 +89,7 @@
 #include "fe/wedge/operators/shell/restriction_constant.hpp"
 #include "fe/wedge/operators/shell/restriction_linear.hpp"
 #include "fe/wedge/operators/shell/vector_laplace.hpp"
+#include "fe/wedge/operators/shell/unsteady_advection_diffusion_supg.hpp"
 #include "fe/strong_algebraic_dirichlet_enforcement.hpp"
 #include "fe/strong_algebraic_freeslip_enforcement.hpp"
 #include "fv/hex/conversion.hpp"
@@ -1274,6 +1277,24 @@ int cmd_fe2fv( int L, double rmin, double rmax, const std::string& dir )
     return 0;
 }
 
+// UnsteadyAdvectionDiffusionSUPG (fe/wedge/operators/shell/unsteady_advection_diffusion_supg.hpp:134-420):
+// diffusivity kappa, time step dt, mass scaling ms, lumped mass, boundary treatment, diagonal mode; velocity vel.bin
+int cmd_supg( int L, double rmin, double rmax, double kappa, double dt, double ms, int lumped, int treat, int diag,
+              const std::string& dir )
+{
+    Setup                            s( L, rmin, rmax );
+    linalg::VectorQ1Vec< double >    u( "u", s.domain, s.omask );
+    linalg::VectorQ1Scalar< double > src( "src", s.domain, s.omask ), dst( "dst", s.domain, s.omask );
+    load_vec( u, dir + "/vel.bin", s.nodes );
+    view_from_host( src.grid_data(), read_file< double >( dir + "/src.bin", s.nodes ).data() );
+    fe::wedge::operators::shell::UnsteadyAdvectionDiffusionSUPG< double > A(
+        s.domain, s.coords, s.radii, s.bmask, u, kappa, dt, treat != 0, diag != 0, ms, lumped != 0 );
+    linalg::apply( A, src, dst );
+    auto h = view_to_host( dst.grid_data() );
+    write_file( dir + "/dst.bin", h.data(), h.size() );
+    return 0;
+}
+
 } // namespace
 
 int main( int argc, char** argv )
@@ -1354,6 +1375,8 @@ int main( int argc, char** argv )
         return cmd_xdmf_read( I( 2 ), D( 3 ), D( 4 ), argv[5], I( 6 ), I( 7 ), argv[8], argv[9] );
     if ( cmd == "fe2fv" && argc == 6 )
         return cmd_fe2fv( I( 2 ), D( 3 ), D( 4 ), argv[5] );
+    if ( cmd == "supg" && argc == 12 )
+        return cmd_supg( I( 2 ), D( 3 ), D( 4 ), D( 5 ), D( 6 ), D( 7 ), I( 8 ), I( 9 ), I( 10 ), argv[11] );
     std::fprintf( stderr, "ref_dump: bad command line\n" );
     return 2;
 }

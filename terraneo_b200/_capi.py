@@ -145,6 +145,12 @@ _SIGS = {
                                            c_void_p]),
     "tn_pressure_remove_mean_f64": (c_int, [c_void_p, c_void_p, c_void_p, P(c_double), c_void_p]),
     "tn_l2_project_fe_to_fv_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "tn_supg_apply_f64": (c_int, [c_void_p, P(c_void_p), c_double, c_double, c_double, c_int, c_int, c_int, c_int,
+                                  c_int, c_void_p, c_void_p, c_void_p]),
+    "tn_supg_apply_f32": (c_int, [c_void_p, P(c_void_p), c_double, c_double, c_double, c_int, c_int, c_int, c_int,
+                                  c_int, c_void_p, c_void_p, c_void_p]),
+    "tn_supg_solve_f64": (c_int, [c_void_p, P(c_void_p), c_double, c_double, c_double, c_int, c_int, c_void_p, c_void_p,
+                                  c_int, c_int, c_double, c_double, c_void_p, P(c_int), P(c_double), c_void_p]),
     "tn_xdmf_output_create": (c_int, [c_void_p, ctypes.c_char_p, c_int, c_int, P(c_void_p)]),
     "tn_xdmf_output_set_write_counter": (c_int, [c_void_p, c_int]),
     "tn_xdmf_output_add": (c_int, [c_void_p, ctypes.c_char_p, c_int, c_int, P(c_void_p), c_int]),

@@ -486,6 +486,51 @@ class VectorMass
 };
 
 // DiagonallyScaledOperator (linalg/diagonally_scaled_operator.hpp:15): D^{-1} A
+// UnsteadyAdvectionDiffusionSUPG (unsteady_advection_diffusion_supg.hpp:134-420): the BDF left-hand side
+// mass_scaling M + dt (K + C + G) with SUPG stabilisation for the velocity u
+template < typename T >
+class UnsteadyAdvectionDiffusionSUPG
+{
+  public:
+    using SrcVectorType = VectorQ1Scalar< T >;
+    using DstVectorType = VectorQ1Scalar< T >;
+    using ScalarType    = T;
+    UnsteadyAdvectionDiffusionSUPG( const Mesh& mesh, const VectorQ1Vec< T >& velocity, T diffusivity, T dt,
+                                    bool treat_boundary, bool diagonal = false, T mass_scaling = T( 1 ),
+                                    bool lumped_mass = false )
+    : mesh_( mesh ), u_( velocity ), kappa_( diffusivity ), dt_( dt ), treat_( treat_boundary ), diag_( diagonal ),
+      ms_( mass_scaling ), lumped_( lumped_mass )
+    {}
+    T&       dt() { return dt_; }
+    const T& dt() const { return dt_; }
+    void     set_operator_apply_and_communication_modes( OperatorApplyMode am, OperatorCommunicationMode cm )
+    {
+        am_ = am, cm_ = cm;
+    }
+    void apply_impl( const SrcVectorType& src, DstVectorType& dst )
+    {
+        const T* v[3] = { u_.comp( 0 ), u_.comp( 1 ), u_.comp( 2 ) };
+        if constexpr ( std::is_same_v< T, double > )
+            check( tn_supg_apply_f64( mesh_.get(), v, kappa_, dt_, ms_, lumped_, treat_, diag_, int( am_ ), int( cm_ ),
+                                      src.comp( 0 ), dst.comp( 0 ), stream() ),
+                   "supg apply" );
+        else
+            check( tn_supg_apply_f32( mesh_.get(), v, kappa_, dt_, ms_, lumped_, treat_, diag_, int( am_ ), int( cm_ ),
+                                      src.comp( 0 ), dst.comp( 0 ), stream() ),
+                   "supg apply" );
+    }
+
+  private:
+    Mesh                      mesh_;
+    VectorQ1Vec< T >          u_;
+    T                         kappa_, dt_;
+    bool                      treat_, diag_;
+    T                         ms_;
+    bool                      lumped_;
+    OperatorApplyMode         am_ = OperatorApplyMode::Replace;
+    OperatorCommunicationMode cm_ = OperatorCommunicationMode::CommunicateAdditively;
+};
+
 template < typename Op >
 class DiagonallyScaledOperator
 {

@@ -628,6 +628,42 @@ def pressure_remove_mean(p, work=None):
     return mean.value
 
 
+class UnsteadyAdvectionDiffusionSUPG:
+    """UnsteadyAdvectionDiffusionSUPG (fe/wedge/operators/shell/unsteady_advection_diffusion_supg.hpp:134): the
+    BDF left-hand side mass_scaling M + dt (K + C + G) for the velocity (a VectorQ1Vec of the same precision)."""
+
+    def __init__(self, mesh, velocity, diffusivity, dt, treat_boundary, diagonal=False, mass_scaling=1.0,
+                 lumped_mass=False, apply_mode=C.APPLY_REPLACE, comm_mode=C.COMM_ADDITIVE):
+        self.mesh, self.velocity = mesh, velocity
+        self.diffusivity, self.dt, self.treat, self.diagonal = float(diffusivity), float(dt), treat_boundary, diagonal
+        self.mass_scaling, self.lumped = float(mass_scaling), lumped_mass
+        self.apply_mode, self.comm_mode = apply_mode, comm_mode
+
+    def set_operator_apply_and_communication_modes(self, apply_mode, comm_mode):
+        self.apply_mode, self.comm_mode = apply_mode, comm_mode
+
+    def apply_impl(self, src, dst):
+        f = getattr(C.lib(), f"tn_supg_apply_{src.tag}")
+        C.check(f(self.mesh.handle, self.velocity.comp_ptrs(), self.diffusivity, self.dt, self.mass_scaling,
+                  int(self.lumped), int(self.treat), int(self.diagonal), self.apply_mode, self.comm_mode,
+                  ctypes.c_void_p(src.data.data_ptr()), ctypes.c_void_p(dst.data.data_ptr()), _stream()), "supg apply")
+
+    def solve(self, rhs, x, l=2, max_iterations=10, relative_tolerance=1e-12, absolute_tolerance=1e-12, work=None):
+        """x <- the solution of this operator x = rhs by PBiCGStab(l) from x (the reference tests' time step,
+        tests/test_unsteady_advection_diffusion_supg.cpp:158-172); FP64; returns (iterations, relative residual)"""
+        assert self.velocity.data.is_contiguous() and x.dtype == torch.float64
+        if work is None:
+            work = torch.empty((2 * (l + 1) + 2) * self.mesh.stored_nodes, dtype=torch.float64, device="cuda")
+        its, rr = ctypes.c_int(), ctypes.c_double()
+        C.check(C.lib().tn_supg_solve_f64(self.mesh.handle, self.velocity.comp_ptrs(), self.diffusivity, self.dt,
+                                          self.mass_scaling, int(self.lumped), int(self.treat),
+                                          ctypes.c_void_p(rhs.data.data_ptr()), ctypes.c_void_p(x.data.data_ptr()),
+                                          l, max_iterations, relative_tolerance, absolute_tolerance,
+                                          ctypes.c_void_p(work.data_ptr()), ctypes.byref(its), ctypes.byref(rr),
+                                          _stream()), "supg solve")
+        return its.value, rr.value
+
+
 def l2_project_fe_to_fv(mesh, fe, fv):
     """FV cell averages of the FE scalar fe (VectorQ1Scalar) into fv [10, N+2, N+2, N+2], lateral ghost layers
     updated (l2_project_fe_to_fv, fv/hex/conversion.hpp:349-416)."""

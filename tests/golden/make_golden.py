@@ -11,6 +11,7 @@ Usage (in a container that has the reference sources and a built ref_dump):
     python tests/golden/make_golden.py               # ref_L2.npz
     python tests/golden/make_golden.py --stokes-mg   # ref_stokes_mg_L4.npz (a few minutes on one thread)
     python tests/golden/make_golden.py --xdmf        # xdmf_L2/: a checkpoint written by io::XDMFOutput
+    python tests/golden/make_golden.py --supg        # adds the SUPG operator cases to ref_L2.npz
 """
 import os
 import sys
@@ -407,6 +408,36 @@ def main():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+# UnsteadyAdvectionDiffusionSUPG: (kappa, dt, mass_scaling, lumped, treat_boundary, diagonal)
+SUPG_CASES = [(1e-3, 1e-2, 1.0, 0, 0, 0), (1e-2, 5e-2, 1.5, 1, 1, 0), (0.0, 1e-2, 1.0, 0, 1, 1), (1e-3, 1e-2, 1.0, 0, 1, 0),
+              (1e-4, 2e-2, 1.0, 1, 0, 1)]
+
+
+def supg_inputs(fine):
+    """seeded velocity [3][nodes] (magnitude about 0.5) and source, both consistent on duplicated nodes"""
+    rs = np.random.RandomState(66)
+    vel = np.stack([fine.make_consistent(rs.normal(size=fine.shape)).reshape(fine.shape) for _ in range(3)]) * 0.5
+    src = fine.make_consistent(rs.normal(size=fine.shape)).reshape(fine.shape)
+    return vel, src
+
+
+def make_supg():
+    """adds supg_* (and the inputs' checksums) to ref_L2.npz, keeping the other entries as they are"""
+    fine = Mesh(L)
+    path = os.path.join(HERE, "ref_L2.npz")
+    out = dict(np.load(path))
+    vel, src = supg_inputs(fine)
+    out["checksum_supg_vel"], out["checksum_supg_src"] = checksum(vel), checksum(src)
+    with tempfile.TemporaryDirectory() as d:
+        vel.tofile(f"{d}/vel.bin")
+        src.tofile(f"{d}/src.bin")
+        for case in SUPG_CASES:
+            run_ref(["supg", L, R_MIN, R_MAX, *case, d], d)
+            out["supg_" + "_".join(str(c) for c in case)] = np.fromfile(f"{d}/dst.bin").reshape(fine.shape)
+    np.savez_compressed(path, **out)
+    print("wrote", path)
+
+
 # The checkpoint fixture: io::XDMFOutput<double> on the L2 mesh with FP32 points and int64 connectivity, the
 # grids of XDMF_GRIDS (label, input bytes, output bytes, vec_dim) filled from the FE temperature of
 # timestep_inputs and the velocity u of inputs(); two writes, the second with T + 1 and 2 u.
@@ -443,5 +474,7 @@ if __name__ == "__main__":
         make_stokes_mg()
     elif "--xdmf" in sys.argv:
         make_xdmf()
+    elif "--supg" in sys.argv:
+        make_supg()
     else:
         main()

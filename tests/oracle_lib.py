@@ -57,6 +57,8 @@ def lib():
         L.or_kmass_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int]
         L.or_fv_to_fe_rhs.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D]
         L.or_fe_to_fv.argtypes = [ctypes.c_int, _D, _D, _D, _D]
+        L.or_supg_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.or_masked_dot.restype = ctypes.c_double
         L.or_masked_dot.argtypes = [ctypes.c_size_t, _D, _D, _U8]
         _lib = L
@@ -256,6 +258,14 @@ class Mesh:
             return b / D
         ones = np.ones(self.shape)
         return pcg(lambda v: self.kmass(ones, v, 0), self.dot, b, max_iterations, rtol, atol)[0]
+
+    def supg(self, vel, src, kappa, dt, mass_scaling=1.0, lumped=False, treat_boundary=False, diag=False):
+        """UnsteadyAdvectionDiffusionSUPG apply, halo summed (unsteady_advection_diffusion_supg.hpp:199-420)"""
+        dst = np.zeros(self.shape)
+        lib().or_supg_apply(self.L, _p(self.coords), _p(self.radii), _p(np.ascontiguousarray(vel, dtype=np.float64)),
+                            _p(np.ascontiguousarray(src, dtype=np.float64)), _p(dst), kappa, dt, mass_scaling,
+                            int(lumped), int(treat_boundary), int(diag))
+        return dst
 
     def l2_project_fe_to_fv(self, fe, fv=None):
         """FV cell averages of the FE scalar fe with the 3x2 rule, lateral ghosts updated (conversion.hpp:349-416);

@@ -420,6 +420,38 @@ def test_fe_to_fv_live_against_reference():
     assert np.abs(fine.l2_project_fe_to_fv(T) - ref).max() <= 1e-15 * np.abs(ref).max()
 
 
+def _supg_key(c):
+    return "supg_" + "_".join(str(v) for v in c)
+
+
+@pytest.mark.parametrize("c", G.SUPG_CASES)
+def test_supg_matches_reference(case, c):
+    """UnsteadyAdvectionDiffusionSUPG (unsteady_advection_diffusion_supg.hpp:199-420) with its mass lumping,
+    boundary mask and diagonal mode, against the reference on the seeded level-2 inputs"""
+    g, fine, _, _ = case
+    vel, src = G.supg_inputs(fine)
+    assert np.allclose(G.checksum(vel), g["checksum_supg_vel"], rtol=1e-13, atol=0)
+    kappa, dt, ms, lumped, treat, diag = c
+    out = fine.supg(vel, src, kappa, dt, ms, bool(lumped), bool(treat), bool(diag))
+    assert rel(out, g[_supg_key(c)]) <= TOL
+
+
+@pytest.mark.skipif(not ref_available(), reason="compiled reference not built")
+def test_supg_live_against_reference():
+    fine = Mesh(3)
+    rs = np.random.RandomState(81)
+    vel = rs.normal(size=(3,) + fine.shape)
+    src = rs.normal(size=fine.shape)
+    with tempfile.TemporaryDirectory() as d:
+        vel.tofile(f"{d}/vel.bin")
+        src.tofile(f"{d}/src.bin")
+        for c in [(1e-3, 1e-2, 1.0, 0, 1, 0), (0.05, 0.1, 2.0, 1, 0, 0)]:
+            run_ref(["supg", 3, 0.55, 1.0, *c, d], d)
+            ref = np.fromfile(f"{d}/dst.bin").reshape(fine.shape)
+            kappa, dt, ms, lumped, treat, diag = c
+            assert rel(fine.supg(vel, src, kappa, dt, ms, bool(lumped), bool(treat), bool(diag)), ref) <= TOL
+
+
 def test_golden_fixture_is_not_trivial(case):
     """A planted error in the oracle's input must break the comparison."""
     g, fine, _, x = case
