@@ -57,17 +57,19 @@ def test_supg_apply_matches_oracle_level3(c):
     s.set_numpy(src)
     shell.apply(op, s, d)
     assert rel(d.numpy()[0], want) <= 1e-12
-    # Add mode on top of a prefilled destination, and the copy-wise (no halo) form summing to the additive one
-    d2 = shell.VectorQ1Scalar(pm)
-    d2.data.fill_(1.0)
-    op.set_operator_apply_and_communication_modes(C.APPLY_ADD, C.COMM_ADDITIVE)
-    shell.apply(op, s, d2)
-    assert rel(d2.numpy()[0] - 1.0, want) <= 1e-12
+    # the copy-wise form (no halo sum) sums to the additive one; Add mode adds the copy-wise contributions to a
+    # prefilled destination (with the additive communication the halo sum would also sum the prefilled copies)
     d3 = shell.VectorQ1Scalar(pm)
     op.set_operator_apply_and_communication_modes(C.APPLY_REPLACE, C.COMM_SKIP)
     shell.apply(op, s, d3)
+    copywise = d3.numpy()[0].copy()
     d3.halo_sum()
     assert rel(d3.numpy()[0], want) <= 1e-12
+    d2 = shell.VectorQ1Scalar(pm)
+    d2.data.fill_(1.0)
+    op.set_operator_apply_and_communication_modes(C.APPLY_ADD, C.COMM_SKIP)
+    shell.apply(op, s, d2)
+    assert rel(d2.numpy()[0] - 1.0, copywise) <= 1e-12
 
 
 def test_supg_bdf_steps():
