@@ -146,6 +146,19 @@ TN_API int tn_kerngen_local_matrices_f64( const tn_mesh* mesh, const double* k, 
  * 1 linear interpolation weights. */
 TN_API int tn_gca_coarsen_f64( const tn_mesh* fine, const tn_mesh* coarse, const double* k_fine,
                                const double* mats_fine, int mode, double* mats_coarse, void* stream );
+/* GCAElementsCollector (linalg/solvers/gca/gca_elements_collector.hpp:19-96): marks (one byte per cell of the
+ * coarsest grid, [10][N0][N0][N0], N0 = N >> level_range, zeroed here) the coarsest cell (x, y, r) >> level_range
+ * of every cell of `fine` with a wedge whose nodal k has a reference-coordinate gradient of norm > 10 at the
+ * centroid.  The adaptive GCA (mantlecirculation.cpp:379-387 with gca == 2) builds Galerkin coarse matrices
+ * only below marked cells. */
+TN_API int tn_gca_elements_f64( const tn_mesh* fine, const double* k_fine, int level_range, uint8_t* marks,
+                                void* stream );
+/* The elements the adaptive GCA leaves unmarked (LocalMatrixStorage::Selective, local_matrix_storage.hpp:185-216:
+ * assembled on the fly from the level's own coefficient): overwrites, in the stored-matrix table `mats` of
+ * `mesh`, the matrices of the cells whose coarsest ancestor (>> level_range) is not marked with the kerngen
+ * matrices of k (NULL: k = 1); marked cells keep their (GCA) matrices. */
+TN_API int tn_agca_unmarked_local_matrices_f64( const tn_mesh* mesh, const double* k, const uint8_t* marks,
+                                                int level_range, double* mats, void* stream );
 /* Apply with stored matrices: the slow path's boundary treatment (Dirichlet
  * masks, free-slip rotation with the normal component decoupled), diagonal
  * mode, the fs/fs rotation penalty (p->penalty_eps) and apply / communication
@@ -513,7 +526,10 @@ typedef struct
     double relative_tolerance;
     double absolute_tolerance;
     int    gca; /* coarse viscous operators: 0 re-discretised with injected viscosity, 1 GCA with
-                   constant interpolation (TwoGridGCA default), 2 GCA with linear interpolation */
+                   constant interpolation (TwoGridGCA default), 2 GCA with linear interpolation, 3 adaptive GCA
+                   (the app's gca == 2, mantlecirculation.cpp:379-387, 565-592): Galerkin matrices with constant
+                   interpolation below the coarsest cells GCAElementsCollector marks on the finest viscosity,
+                   the re-discretised matrices of the injected viscosity elsewhere */
     int    outer; /* 0 FGMRES(restart) + block-triangular preconditioner, 1 PMINRES + block-diagonal
                      preconditioner (pminres.hpp, block_preconditioner_2x2.hpp:38-100), 2 mixed-precision
                      iterative refinement (needs mg_fp32 = 1): FP64 residual and update around an FGMRES(restart)

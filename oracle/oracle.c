@@ -2237,3 +2237,36 @@ void or_supg_apply( int L, const double* coords, const double* radii, const doub
                 }
     or_halo_sum( L, coords, dst, 1 );
 }
+
+/* ------------------------------------------------------------------------ */
+/* Adaptive GCA: GCAElementsCollector (linalg/solvers/gca/                   */
+/* gca_elements_collector.hpp:19-96)                                          */
+/* ------------------------------------------------------------------------ */
+
+/* Marks the coarsest-grid cell (x >> level_range, y >> level_range, r >> level_range) of every fine cell one of
+ * whose wedges has |sum_j grad_ref phi_j(1/3, 1/3, 0) k_j| > 10 (the gradient in reference coordinates at the
+ * one-point rule's centroid).  marks: [10][N0][N0][N0] with N0 = N >> level_range, zeroed here. */
+void or_gca_elements( int L, const double* k, int level_range, uint8_t* marks )
+{
+    const int N = 1 << L, n1 = N + 1, N0 = N >> level_range;
+    memset( marks, 0, (size_t) NDIAMOND * N0 * N0 * N0 );
+    for ( int d = 0; d < NDIAMOND; ++d )
+        for ( int x = 0; x < N; ++x )
+            for ( int y = 0; y < N; ++y )
+                for ( int r = 0; r < N; ++r )
+                    for ( int w = 0; w < 2; ++w )
+                    {
+                        double kg[3] = { 0, 0, 0 };
+                        for ( int j = 0; j < 6; ++j )
+                        {
+                            double g[3];
+                            grad_shape_ref( j, 1.0 / 3.0, 1.0 / 3.0, 0.0, g );
+                            const double kj = k[node_idx( n1, d, x + WNODE[w][j][0], y + WNODE[w][j][1], r + WNODE[w][j][2] )];
+                            for ( int a = 0; a < 3; ++a )
+                                kg[a] = kg[a] + g[a] * kj;
+                        }
+                        if ( sqrt( kg[0] * kg[0] + kg[1] * kg[1] + kg[2] * kg[2] ) > 10.0 )
+                            marks[( ( (size_t) d * N0 + ( x >> level_range ) ) * N0 + ( y >> level_range ) ) * N0 +
+                                  ( r >> level_range )] = 1;
+                    }
+}

@@ -35,6 +35,7 @@ void or_ownership_mask( int L, const double* coords, uint8_t* omask );
 void or_halo_sum( int L, const double* coords, double* field, int ncomp );
 void or_fv_to_fe_rhs( int L, const double* coords, const double* radii, const double* fv, double* b, double* D );
 void or_fe_to_fv( int L, const double* coords, const double* radii, const double* fe, double* fv );
+void or_gca_elements( int L, const double* k, int level_range, uint8_t* marks );
 void or_supg_apply( int L, const double* coords, const double* radii, const double* vel, const double* src, double* dst,
                     double kappa, double dt, double mass_scaling, int lumped, int treat_boundary, int diag );
 

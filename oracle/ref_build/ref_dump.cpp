@@ -62,6 +62,11 @@
 //                                          into a FP64 grid (vec 0: scalar, 1: 3-vector): out.bin; the metadata
 //                                          as text in meta.txt; on a read error its message in error.txt, exit 3
 //   fe2fv L rmin rmax DIR                  l2_project_fe_to_fv of T.bin (FE): fv.bin ([10][N+2]^3, ghosts set)
+//   agca L rmin rmax bcc bcs diag DIR      adaptive GCA over three levels: GCAElementsCollector of k.bin (level L,
+//                                          level range 2) on level L-2 (gcae.bin: the marks as a node field), the
+//                                          level-(L-1) kerngen operator with kc.bin in Selective storage, TwoGridGCA
+//                                          from the level-L Neumann kerngen operator, then its apply to src.bin
+//                                          (level L-1): dst.bin
 //   supg L rmin rmax kappa dt ms lumped treat diag DIR  UnsteadyAdvectionDiffusionSUPG<double> with the velocity
 //                                          vel.bin (3 x nodes) applied to src.bin: dst.bin
 //   time_kerngen L rmin rmax bcc bcs reps [DIR]  prints seconds per apply (CPU baseline); with DIR the
@@ -98,6 +103,7 @@
 #include "fv/hex/operators/fct_advection_diffusion.hpp"
 #include "grid/bit_masks.hpp"
 #include "linalg/solvers/gca/gca.hpp"
+#include "linalg/solvers/gca/gca_elements_collector.hpp"
 #include "linalg/solvers/block_preconditioner_2x2.hpp"
 #include "linalg/solvers/chebyshev.hpp"
 #include "linalg/solvers/power_iteration.hpp"
@@ -1295,6 +1301,40 @@ int cmd_supg( int L, double rmin, double rmax, double kappa, double dt, double m
     return 0;
 }
 
+// Adaptive GCA (mantlecirculation.cpp:379-387, 565-592 with gca == 2): GCAElementsCollector
+// (gca_elements_collector.hpp:19-96) on the fine viscosity, Selective local-matrix storage on the coarse operator
+// (local_matrix_storage.hpp:60-216), TwoGridGCA on the marked elements (gca.hpp:155-163) and the coarse apply,
+// which assembles the unmarked elements' matrices from kc on the fly (epsilon_divdiv_kerngen.hpp:856-869)
+int cmd_agca( int L, double rmin, double rmax, int bcc, int bcs, int diag, const std::string& dir )
+{
+    using Op = fe::wedge::operators::shell::EpsilonDivDivKerngen< double >;
+    Setup                            f( L, rmin, rmax ), c( L - 1, rmin, rmax ), z( L - 2, rmin, rmax );
+    linalg::VectorQ1Scalar< double > k( "k", f.domain, f.omask ), kc( "kc", c.domain, c.omask ),
+        gcae( "gcae", z.domain, z.omask );
+    view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", f.nodes ).data() );
+    view_from_host( kc.grid_data(), read_file< double >( dir + "/kc.bin", c.nodes ).data() );
+    linalg::assign( gcae, 0.0 );
+    linalg::solvers::GCAElementsCollector< double >( f.domain, k.grid_data(), 2, gcae.grid_data() );
+    Kokkos::fence();
+    {
+        auto h = view_to_host( gcae.grid_data() );
+        write_file( dir + "/gcae.bin", h.data(), h.size() );
+    }
+    BoundaryConditions bn = { { ShellBoundaryFlag::CMB, BoundaryConditionFlag::NEUMANN },
+                              { ShellBoundaryFlag::SURFACE, BoundaryConditionFlag::NEUMANN } };
+    BoundaryConditions b  = { { ShellBoundaryFlag::CMB, bc_of( bcc ) }, { ShellBoundaryFlag::SURFACE, bc_of( bcs ) } };
+    Op Af( f.domain, f.coords, f.radii, f.bmask, k.grid_data(), bn, false );
+    Op Ac( c.domain, c.coords, c.radii, c.bmask, kc.grid_data(), b, false );
+    Ac.set_stored_matrix_mode( linalg::OperatorStoredMatrixMode::Selective, 1, gcae.grid_data() );
+    linalg::solvers::TwoGridGCA< double, Op >( Af, Ac, 1, gcae.grid_data() );
+    Ac.set_diagonal( diag != 0 );
+    linalg::VectorQ1Vec< double > src( "src", c.domain, c.omask ), dst( "dst", c.domain, c.omask );
+    load_vec( src, dir + "/src.bin", c.nodes );
+    linalg::apply( Ac, src, dst );
+    save_vec( dst, dir + "/dst.bin", c.nodes );
+    return 0;
+}
+
 } // namespace
 
 int main( int argc, char** argv )
@@ -1377,6 +1417,8 @@ int main( int argc, char** argv )
         return cmd_fe2fv( I( 2 ), D( 3 ), D( 4 ), argv[5] );
     if ( cmd == "supg" && argc == 12 )
         return cmd_supg( I( 2 ), D( 3 ), D( 4 ), D( 5 ), D( 6 ), D( 7 ), I( 8 ), I( 9 ), I( 10 ), argv[11] );
+    if ( cmd == "agca" && argc == 9 )
+        return cmd_agca( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     std::fprintf( stderr, "ref_dump: bad command line\n" );
     return 2;
 }

@@ -114,6 +114,8 @@ _SIGS = {
     "tn_local_matrix_count": (c_int, [c_void_p, P(c_size_t)]),
     "tn_kerngen_local_matrices_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "tn_gca_coarsen_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "tn_gca_elements_f64": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "tn_agca_unmarked_local_matrices_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "tn_stored_epsdivdiv_apply_f64": (c_int, [c_void_p, c_void_p, P(EpsDivDivParams), P(c_void_p), P(c_void_p),
                                               c_void_p]),
     "tn_stored_epsdivdiv_apply_f32": (c_int, [c_void_p, c_void_p, P(EpsDivDivParams), P(c_void_p), P(c_void_p),

@@ -180,15 +180,27 @@ __device__ __forceinline__ int gca_coarse_wedge( int h, int w )
     return ( h == 0 || h == 4 ) ? 0 : 1;
 }
 
+// the coarsest-grid ancestor (x, y, r) >> lr of a cell is marked (GCAElements, gca.hpp:155-163)
+__device__ __forceinline__ bool agca_marked( const uint8_t* marks, int N, int lr, int d, int x, int y, int r )
+{
+    const int N0 = N >> lr;
+    return marks[( ( size_t( d ) * N0 + ( x >> lr ) ) * N0 + ( y >> lr ) ) * N0 + ( r >> lr )] != 0;
+}
+
+// marks: nullptr for every cell, else only the cells whose coarsest ancestor is not marked (the elements the
+// adaptive GCA leaves to the re-discretised operator)
 __global__ void __launch_bounds__( 64 ) local_matrices_kernel( int N, const double* __restrict__ coords,
                                                                const double* __restrict__ radii,
-                                                               const double* __restrict__ k, double* __restrict__ mats )
+                                                               const double* __restrict__ k, double* __restrict__ mats,
+                                                               const uint8_t* __restrict__ marks, int lr )
 {
     __shared__ double sg[2][6][3], skw[2];
     const long long   cell = blockIdx.x;
     const int         n1   = N + 1;
     const int         r = int( cell % N ), y = int( ( cell / N ) % N ), x = int( ( cell / ( (long long) N * N ) ) % N );
     const int         d = int( cell / ( (long long) N * N * N ) );
+    if ( marks && agca_marked( marks, N, lr, d, x, y, r ) )
+        return; // uniform over the block: one cell per block
     if ( threadIdx.x < 2 )
         kerngen_geometry( coords, radii, k, n1, d, x, y, r, threadIdx.x, sg[threadIdx.x], skw[threadIdx.x] );
     __syncthreads();
@@ -199,6 +211,40 @@ __global__ void __launch_bounds__( 64 ) local_matrices_kernel( int N, const doub
             mats[stored_pos( cell * 2 + w, packed( I, J ) )] = kerngen_entry( sg[w], skw[w], I, J );
         if ( I == 17 && J == 17 )
             mats[stored_pos( cell * 2 + w, kP )] = 0.0; // padding entry
+    }
+}
+
+// GCAElementsCollector (gca_elements_collector.hpp:59-94): one thread per fine cell; a wedge whose nodal
+// viscosity has a reference-coordinate gradient of norm > 10 at the centroid (1/3, 1/3, 0) marks the coarsest
+// cell (x, y, r) >> lr.  Concurrent writers store the same value.
+__global__ void gca_elements_kernel( int N, int lr, const double* __restrict__ k, uint8_t* marks )
+{
+    const long long t = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if ( t >= (long long) kDiamonds * N * N * N )
+        return;
+    const int n1 = N + 1;
+    const int r = int( t % N ), y = int( ( t / N ) % N ), x = int( ( t / ( (long long) N * N ) ) % N );
+    const int d = int( t / ( (long long) N * N * N ) );
+#pragma unroll
+    for ( int w = 0; w < 2; ++w )
+    {
+        double kg[3] = { 0, 0, 0 };
+#pragma unroll
+        for ( int j = 0; j < 6; ++j )
+        {
+            double g[3];
+            grad_shape_ref( j, 1.0 / 3.0, 1.0 / 3.0, 0.0, g );
+            const double kj = k[lat_index( n1, d, x + wedge_node( w, j, 0 ), y + wedge_node( w, j, 1 ) ) * n1 + r +
+                                wedge_node( w, j, 2 )];
+#pragma unroll
+            for ( int a = 0; a < 3; ++a )
+                kg[a] = kg[a] + g[a] * kj;
+        }
+        if ( sqrt( kg[0] * kg[0] + kg[1] * kg[1] + kg[2] * kg[2] ) > 10.0 )
+        {
+            const int N0 = N >> lr;
+            marks[( ( size_t( d ) * N0 + ( x >> lr ) ) * N0 + ( y >> lr ) ) * N0 + ( r >> lr )] = 1;
+        }
     }
 }
 
@@ -1341,7 +1387,33 @@ extern "C" int tn_kerngen_local_matrices_f64( const tn_mesh* m, const double* k,
 {
     TN_CHECK_ARG( m && mats, "tn_kerngen_local_matrices_f64: null argument" );
     const long long cells = (long long) kDiamonds * m->N * m->N * m->N;
-    local_matrices_kernel<<< unsigned( cells ), 64, 0, as_stream( s ) >>>( m->N, m->d_coords, m->d_radii, k, mats );
+    local_matrices_kernel<<< unsigned( cells ), 64, 0, as_stream( s ) >>>( m->N, m->d_coords, m->d_radii, k, mats,
+                                                                          nullptr, 0 );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+extern "C" int tn_gca_elements_f64( const tn_mesh* fine, const double* k_fine, int level_range, uint8_t* marks, void* s )
+{
+    TN_CHECK_ARG( fine && k_fine && marks, "tn_gca_elements_f64: null argument" );
+    TN_CHECK_ARG( level_range >= 0 && level_range <= fine->level, "tn_gca_elements_f64: bad level range" );
+    const int       N0    = fine->N >> level_range;
+    const long long cells = (long long) kDiamonds * fine->N * fine->N * fine->N;
+    TN_CUDA_TRY( cudaMemsetAsync( marks, 0, size_t( kDiamonds ) * N0 * N0 * N0, as_stream( s ) ) );
+    gca_elements_kernel<<< unsigned( ( cells + 127 ) / 128 ), 128, 0, as_stream( s ) >>>( fine->N, level_range, k_fine,
+                                                                                         marks );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+extern "C" int tn_agca_unmarked_local_matrices_f64( const tn_mesh* m, const double* k, const uint8_t* marks,
+                                                    int level_range, double* mats, void* s )
+{
+    TN_CHECK_ARG( m && mats && marks, "tn_agca_unmarked_local_matrices_f64: null argument" );
+    TN_CHECK_ARG( level_range >= 0 && level_range <= m->level, "tn_agca_unmarked_local_matrices_f64: bad level range" );
+    const long long cells = (long long) kDiamonds * m->N * m->N * m->N;
+    local_matrices_kernel<<< unsigned( cells ), 64, 0, as_stream( s ) >>>( m->N, m->d_coords, m->d_radii, k, mats,
+                                                                          marks, level_range );
     TN_LAUNCH_CHECK();
     return TN_OK;
 }

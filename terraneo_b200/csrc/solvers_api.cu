@@ -88,6 +88,7 @@ struct tn_stokes_solver
     std::vector< VectorQ1Scalar< float > >                   k32;
     std::vector< std::shared_ptr< double > >                 mats64; // GCA matrices per coarse level
     std::vector< std::shared_ptr< float > >                  mats32;
+    std::shared_ptr< uint8_t >                               gca_marks; // adaptive GCA: marked coarsest cells
     std::shared_ptr< A64 >                                   A64fine;
     std::unique_ptr< EpsDivDivStokes< double > >             K;
     std::unique_ptr< Gradient< double > >                    BT;
@@ -136,11 +137,23 @@ ViscousOp< T > level_op( tn_stokes_solver& s, int l )
 // GCA matrices of levels [Lmin, L-1] (mantlecirculation.cpp:580-592): the
 // finest from the Neumann kerngen matrices of the finest viscosity, each
 // coarser one from the stored matrices above it
+// With gca == 3 (adaptive) the coarsest cells are marked once from the finest viscosity
+// (GCAElementsCollector with level range L - Lmin) and each level keeps the GCA matrices of the cells below a
+// marked cell, the kerngen matrices of its injected viscosity elsewhere (the reference's Selective storage
+// assembles those on the fly; here every cell's matrix is stored, the apply is the same stored-matrix kernel).
 void build_gca( tn_stokes_solver& s )
 {
     const int L = s.prm.level, Lmin = L - s.prm.mg_levels + 1, mode = s.prm.gca == 2 ? 1 : 0;
+    const bool adaptive = s.prm.gca == 3;
     s.mats64.assign( L + 1, nullptr );
     s.mats32.assign( L + 1, nullptr );
+    if ( adaptive )
+    {
+        const size_t N0 = size_t( 1 ) << Lmin;
+        s.gca_marks     = device_alloc< uint8_t >( 10 * N0 * N0 * N0 );
+        check( tn_gca_elements_f64( s.mesh[L].get(), s.k64[L].data(), L - Lmin, s.gca_marks.get(), stream() ),
+               "gca_elements" );
+    }
     for ( int l = L - 1; l >= Lmin; --l )
     {
         size_t n = 0;
@@ -149,6 +162,10 @@ void build_gca( tn_stokes_solver& s )
         check( tn_gca_coarsen_f64( s.mesh[l + 1].get(), s.mesh[l].get(), l == L - 1 ? s.k64[L].data() : nullptr,
                                    l == L - 1 ? nullptr : s.mats64[l + 1].get(), mode, s.mats64[l].get(), stream() ),
                "gca_coarsen" );
+        if ( adaptive )
+            check( tn_agca_unmarked_local_matrices_f64( s.mesh[l].get(), s.k64[l].data(), s.gca_marks.get(), l - Lmin,
+                                                        s.mats64[l].get(), stream() ),
+                   "agca unmarked matrices" );
         if ( s.prm.mg_fp32 )
         {
             s.mats32[l] = device_alloc< float >( n );
@@ -351,7 +368,7 @@ extern "C" int tn_stokes_solver_create( const tn_stokes_params* p, double r_min,
     TN_CHECK_ARG( p->mg_levels >= 2 && p->level - p->mg_levels + 1 >= 2 && p->level <= 8,
                   "tn_stokes_solver_create: need mg_levels >= 2, level - mg_levels + 1 >= 2 and level <= 8" );
     TN_CHECK_ARG( p->restart >= 1 && p->max_iterations >= 1, "tn_stokes_solver_create: bad Krylov parameters" );
-    TN_CHECK_ARG( p->gca >= 0 && p->gca <= 2, "tn_stokes_solver_create: gca must be 0, 1 or 2" );
+    TN_CHECK_ARG( p->gca >= 0 && p->gca <= 3, "tn_stokes_solver_create: gca must be 0, 1, 2 or 3" );
     TN_CHECK_ARG( p->outer >= 0 && p->outer <= 2, "tn_stokes_solver_create: outer must be 0, 1 or 2" );
     TN_CHECK_ARG( p->outer != 2 || p->mg_fp32, "tn_stokes_solver_create: outer = 2 (refinement) needs mg_fp32 = 1" );
     try

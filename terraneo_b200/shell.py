@@ -185,6 +185,28 @@ def gca_coarsen(fine, coarse, k_fine=None, mats_fine=None, mode=0):
     return out
 
 
+def gca_elements(fine, k_fine, level_range):
+    """GCAElementsCollector (linalg/solvers/gca/gca_elements_collector.hpp:19-96): uint8 marks [10, N0, N0, N0]
+    of the coarsest cells (N0 = N >> level_range) below which the adaptive GCA builds Galerkin matrices."""
+    N0 = fine.N >> level_range
+    marks = torch.empty((10, N0, N0, N0), dtype=torch.uint8, device="cuda")
+    C.check(C.lib().tn_gca_elements_f64(fine.handle, ctypes.c_void_p(k_fine.data.data_ptr()), level_range,
+                                        ctypes.c_void_p(marks.data_ptr()), _stream()), "gca_elements")
+    return marks
+
+
+def agca_coarsen(fine, coarse, marks, level_range_coarse, k_coarse=None, k_fine=None, mats_fine=None):
+    """Adaptive GCA matrices of `coarse` (TwoGridGCA with Selective storage, gca.hpp:155-163): the GCA matrices of
+    the cells below a marked coarsest cell (cell >> level_range_coarse), the kerngen matrices of k_coarse (None:
+    k = 1) elsewhere, in the stored layout."""
+    out = gca_coarsen(fine, coarse, k_fine=k_fine, mats_fine=mats_fine)
+    kp = ctypes.c_void_p(k_coarse.data.data_ptr()) if k_coarse is not None else None
+    C.check(C.lib().tn_agca_unmarked_local_matrices_f64(coarse.handle, kp, ctypes.c_void_p(marks.data_ptr()),
+                                                        level_range_coarse, ctypes.c_void_p(out.data_ptr()),
+                                                        _stream()), "agca_unmarked_local_matrices")
+    return out
+
+
 def stored_pcg(op, b, x, max_iterations=50, relative_tolerance=1e-6, absolute_tolerance=1e-30, check_every=8):
     """Unpreconditioned PCG (linalg/solvers/pcg.hpp:78) on a StoredEpsilonDivDiv (FP64) with the operator's steps
     fused into the PCG steps (tn_stored_pcg_f64); x is updated in place.

@@ -12,6 +12,7 @@ Usage (in a container that has the reference sources and a built ref_dump):
     python tests/golden/make_golden.py --stokes-mg   # ref_stokes_mg_L4.npz (a few minutes on one thread)
     python tests/golden/make_golden.py --xdmf        # xdmf_L2/: a checkpoint written by io::XDMFOutput
     python tests/golden/make_golden.py --supg        # adds the SUPG operator cases to ref_L2.npz
+    python tests/golden/make_golden.py --agca        # adds the adaptive-GCA cases (level 3) to ref_L2.npz
 """
 import os
 import sys
@@ -438,6 +439,44 @@ def make_supg():
     print("wrote", path)
 
 
+# Adaptive GCA over levels 3 (fine), 2 (coarse) and 1 (coarsest, the marks): (bcc, bcs, diag) of the coarse apply
+AGCA_L = 3
+AGCA_CASES = [(1, 1, 0), (2, 2, 0), (0, 0, 0), (2, 1, 1)]
+
+
+def blob_viscosity(mesh, centre=(0.6, 0.3, 0.4), amp=400.0, width=0.01):
+    """1 + amp exp(-|x - centre|^2 / width) at the nodes: a sharp blob the GCA element collector marks only
+    around"""
+    x = mesh.coords[:, :, :, None, :] * mesh.radii[:, None, None, :, None]
+    return 1.0 + amp * np.exp(-np.sum((x - np.array(centre)) ** 2, axis=-1) / width)
+
+
+def agca_inputs():
+    fine, coarse = Mesh(AGCA_L), Mesh(AGCA_L - 1)
+    src = np.random.RandomState(91).normal(size=(3,) + coarse.shape)
+    return fine, coarse, blob_viscosity(fine), blob_viscosity(coarse), src
+
+
+def make_agca():
+    """adds agca_marks and agca_<bcc><bcs><diag> (and the source's checksum) to ref_L2.npz"""
+    path = os.path.join(HERE, "ref_L2.npz")
+    out = dict(np.load(path))
+    fine, coarse, k, kc, src = agca_inputs()
+    out["checksum_agca_src"] = checksum(src)
+    z = Mesh(AGCA_L - 2)
+    with tempfile.TemporaryDirectory() as d:
+        k.tofile(f"{d}/k.bin")
+        kc.tofile(f"{d}/kc.bin")
+        src.tofile(f"{d}/src.bin")
+        for bcc, bcs, diag in AGCA_CASES:
+            run_ref(["agca", AGCA_L, R_MIN, R_MAX, bcc, bcs, diag, d], d)
+            out[f"agca_{bcc}{bcs}{diag}"] = np.fromfile(f"{d}/dst.bin").reshape((3,) + coarse.shape)
+        g = np.fromfile(f"{d}/gcae.bin").reshape(z.shape)
+        out["agca_marks"] = (g[:, :-1, :-1, :-1] != 0).astype(np.uint8)
+    np.savez_compressed(path, **out)
+    print("wrote", path)
+
+
 # The checkpoint fixture: io::XDMFOutput<double> on the L2 mesh with FP32 points and int64 connectivity, the
 # grids of XDMF_GRIDS (label, input bytes, output bytes, vec_dim) filled from the FE temperature of
 # timestep_inputs and the velocity u of inputs(); two writes, the second with T + 1 and 2 u.
@@ -476,5 +515,7 @@ if __name__ == "__main__":
         make_xdmf()
     elif "--supg" in sys.argv:
         make_supg()
+    elif "--agca" in sys.argv:
+        make_agca()
     else:
         main()

@@ -57,6 +57,7 @@ def lib():
         L.or_kmass_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int]
         L.or_fv_to_fe_rhs.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D]
         L.or_fe_to_fv.argtypes = [ctypes.c_int, _D, _D, _D, _D]
+        L.or_gca_elements.argtypes = [ctypes.c_int, _D, ctypes.c_int, _U8]
         L.or_supg_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.or_masked_dot.restype = ctypes.c_double
@@ -201,6 +202,26 @@ class Mesh:
         kf = None if k is None else _p(np.ascontiguousarray(k, dtype=np.float64))
         lib().or_gca_coarsen(self.L, _p(self.coords), _p(self.radii), kf, mf, mode, _p(out))
         return out
+
+    def gca_elements(self, k, level_range):
+        """GCAElementsCollector: marks [10, N0, N0, N0] (uint8) of the coarsest cells, N0 = N >> level_range"""
+        N0 = self.N >> level_range
+        marks = np.zeros((10, N0, N0, N0), np.uint8)
+        lib().or_gca_elements(self.L, _p(np.ascontiguousarray(k, dtype=np.float64)), level_range, _p(marks))
+        return marks
+
+    def agca_coarsen(self, coarse, marks, level_range_coarse, k_coarse, mats_fine=None, k=None):
+        """Adaptive GCA matrices of `coarse` (TwoGridGCA with LocalMatrixStorage::Selective, gca.hpp:155-163,
+        local_matrix_storage.hpp:185-216): the GCA matrix of every coarse cell whose coarsest ancestor (cell >>
+        level_range_coarse) is marked, the kerngen matrix of k_coarse (assembled on the fly by the reference)
+        elsewhere"""
+        mats = self.gca_coarsen(coarse, mats_fine=mats_fine, k=k)
+        asm = coarse.local_matrices(k_coarse)
+        N, lr = coarse.N, level_range_coarse
+        d, x, y, r = np.meshgrid(np.arange(10), np.arange(N), np.arange(N), np.arange(N), indexing="ij")
+        keep = marks[d, x >> lr, y >> lr, r >> lr].reshape(-1) != 0
+        mats[~keep] = asm[~keep]
+        return mats
 
     def stored_apply(self, mats, src, bc_cmb, bc_surf, diag=False):
         dst = np.zeros((3,) + self.shape)

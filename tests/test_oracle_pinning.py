@@ -452,6 +452,21 @@ def test_supg_live_against_reference():
             assert rel(fine.supg(vel, src, kappa, dt, ms, bool(lumped), bool(treat), bool(diag)), ref) <= TOL
 
 
+@pytest.mark.parametrize("bc", G.AGCA_CASES)
+def test_agca_matches_reference(case, bc):
+    """Adaptive GCA (GCAElementsCollector marks on level 1 from the level-3 viscosity, Selective storage on
+    level 2, TwoGridGCA on the marked elements, the level-2 kerngen matrices elsewhere) and the coarse apply,
+    against the reference"""
+    g = case[0]
+    fine, coarse, k, kc, src = G.agca_inputs()
+    assert np.allclose(G.checksum(src), g["checksum_agca_src"], rtol=1e-13, atol=0)
+    marks = fine.gca_elements(k, 2)
+    assert np.array_equal(marks, g["agca_marks"]) and 0 < marks.sum() < marks.size
+    mats = fine.agca_coarsen(coarse, marks, 1, kc, k=k)
+    bcc, bcs, diag = bc
+    assert rel(coarse.stored_apply(mats, src, bcc, bcs, bool(diag)), g[f"agca_{bcc}{bcs}{diag}"]) <= TOL
+
+
 def test_golden_fixture_is_not_trivial(case):
     """A planted error in the oracle's input must break the comparison."""
     g, fine, _, x = case
