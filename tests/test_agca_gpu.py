@@ -67,11 +67,12 @@ def test_agca_two_coarsenings_match_oracle():
     assert rel(v.numpy(), want) <= 1e-12
 
 
-@pytest.mark.parametrize("bc", [(1, 1), (2, 2)])
+@pytest.mark.parametrize("bc", [(1, 1), (2, 1)])
 def test_stokes_solve_with_adaptive_gca(bc):
     """the Stokes solver with gca = 3 at level 4 (blob viscosity, a part of the coarsest cells marked): the FP64
     true residual under the oracle operators reaches the tolerance, in a few more or fewer iterations than the
-    full GCA"""
+    full GCA (free-slip on both radii is left out: with a random right-hand side the rigid rotations make it
+    nearly singular)"""
     from terraneo_b200 import shell
     L = 4
     om, oc = Mesh(L), Mesh(L - 1)
