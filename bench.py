@@ -175,10 +175,33 @@ def _case_coarse_pcg3(shell, C, torch):
     return {"stored-matrix PCG, level 3, free-slip both radii, 50 iterations": run}
 
 
+def _fct_case(shell, torch, level):
+    m = shell.ShellMesh(level, RMIN, RMAX)
+    fct = shell.FCTAdvectionDiffusion(m)
+    v = shell.VectorQ1Vec(m)
+    v.data.normal_(generator=torch.Generator(device="cuda").manual_seed(5))
+    T = fct.field()
+    T.uniform_(generator=torch.Generator(device="cuda").manual_seed(6))
+    dt = 0.5 * fct.dt_stable(v)
+    cells = 10 * (1 << level) ** 3
+    return {f"FCT explicit step (predictor, limiter, correction), level {level}, {cells:,} cells":
+            lambda: fct.step(T, v, dt),
+            f"FCT stable time step, level {level}": lambda: fct.dt_stable(v)}
+
+
+def _case_fct6(shell, C, torch):
+    return _fct_case(shell, torch, 6)
+
+
+def _case_fct7(shell, C, torch):
+    return _fct_case(shell, torch, 7)
+
+
 # name -> builder returning {description: one launch sequence}
 CASES = {"laplace6": _case_laplace6, "vlaplace6": _case_vlaplace6, "divkgrad6": _case_divkgrad6,
          "stokes_b6": _case_stokes_b6, "stored5": _case_stored5, "kerngen6_fs": _case_kerngen6_fs,
-         "stokes6": _case_stokes6, "stokes6_refine": _case_stokes6_refine, "coarse_pcg3": _case_coarse_pcg3}
+         "stokes6": _case_stokes6, "stokes6_refine": _case_stokes6_refine, "coarse_pcg3": _case_coarse_pcg3,
+         "fct6": _case_fct6, "fct7": _case_fct7}
 
 
 def run_case(args):
@@ -775,6 +798,101 @@ def cpu_baseline(steps):
             "seconds_per_apply": sec}
 
 
+def stokes_reference_solution(shell, C, torch):
+    """Each solver form against the reference's own FP64 solution of a level-4 free-slip Stokes problem
+    (tests/golden/ref_stokes_mg_L4.npz: ref_dump stokes_mg, FGMRES(30) to 1e-7 with the app's preconditioner
+    stack over 3 levels; inputs in tests/golden/stokes_mg_L4_inputs.npz), the same settings and the smoothers'
+    eigenvalue estimates the reference drew."""
+    gdir = os.path.join(ROOT, "tests", "golden")
+    ref = np.load(os.path.join(gdir, "ref_stokes_mg_L4.npz"))
+    inp = np.load(os.path.join(gdir, "stokes_mg_L4_inputs.npz"))
+    pf, pc = shell.ShellMesh(4, RMIN, RMAX), shell.ShellMesh(3, RMIN, RMAX)
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(inp["k"])
+    fu, fp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+    fu.set_numpy(inp["f_u"])
+    fp.set_numpy(inp["f_p"])
+    u_ref, p_ref = ref["x_u_22"].astype(np.float64), ref["x_p_22"].astype(np.float64)
+    out = {"workload": "level-4 velocity / level-3 pressure, free-slip both radii, 1e3-contrast viscosity, FGMRES(30) "
+                       "to 1e-7 + block-triangular preconditioner + V-cycle over 3 levels (Chebyshev order 3, GCA, "
+                       "coarse PCG 50 / 1e-6)",
+           "reference_iterations": int(ref["iterations_22"])}
+    for tag, mg32, outer in (("fp64_mg", False, 0), ("fp32_mg", True, 0), ("fp32_refine", True, 2)):
+        s = shell.StokesSolver(4, kv, mg_levels=3, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=mg32,
+                               chebyshev_order=3, smoothing_steps=2, power_iterations=10, vcycles=1,
+                               coarse_max_iterations=50, coarse_relative_tolerance=1e-6, restart=30, max_iterations=300,
+                               relative_tolerance=1e-7, r_min=RMIN, r_max=RMAX, gca=1, outer=outer,
+                               chebyshev_estimates=list(ref["eigenvalues_22"]))
+        xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+        it, rr = s.solve(fu, fp, xu, xp)
+        du = np.linalg.norm(xu.numpy() - u_ref) / np.linalg.norm(u_ref)
+        dp = np.linalg.norm(xp.numpy()[0] - p_ref) / np.linalg.norm(p_ref)
+        out[tag] = {"iterations": it, "relres": float(f"{rr:.3e}"), "u_rel_diff": float(f"{du:.3e}"),
+                    "p_rel_diff": float(f"{dp:.3e}")}
+        del s
+    return out
+
+
+def stokes_cpu_baseline(shell, C, torch, level=5, cores=None):
+    """The reference's own FP64 Stokes stack (oracle/_ref/ref_dump stokes_mg: FGMRES(100) + block-triangular
+    preconditioner + V-cycle with Chebyshev order 3, 2 smoothing steps, GCA coarse operators, coarse PCG 50 /
+    1e-6, mantlecirculation.cpp:486-735) on this host's cores, on the C3 problem at level 5 (velocity level 5,
+    pressure level 4, 4 multigrid levels; the level-6 solve takes about 20-40 s per FGMRES iteration on a host,
+    hours to 1e-8): the time per FGMRES iteration from a 1- and a 3-iteration solve (their difference leaves
+    out the smoothers' first-use power iterations), beside the B200's FP64 and refinement forms on the same
+    inputs and settings."""
+    import tempfile
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
+    if not os.path.exists(ref):
+        return {"unavailable": "oracle/_ref/ref_dump is not built"}
+    cores = cores or os.cpu_count() or 1
+    pf, pc = shell.ShellMesh(level, RMIN, RMAX), shell.ShellMesh(level - 1, RMIN, RMAX)
+    coords, radii = pf.geometry()
+    k_np, _ = synthetic_inputs(coords, radii, None)
+    fu, fp = stokes_rhs(shell, pf, coords, radii), shell.VectorQ1Scalar(pc)
+    secs = {}
+    with tempfile.TemporaryDirectory() as d:
+        k_np.tofile(os.path.join(d, "k.bin"))
+        np.ascontiguousarray(k_np[:, ::2, ::2, ::2]).tofile(os.path.join(d, "kp.bin"))
+        fu.numpy().tofile(os.path.join(d, "f_u.bin"))
+        fp.numpy().tofile(os.path.join(d, "f_p.bin"))
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="spread", OMP_PLACES="cores")
+        for its in (1, 3):
+            out = subprocess.run([ref, "stokes_mg", str(level), "4", str(RMIN), str(RMAX), "2", "2", "100", str(its),
+                                  "1e-30", "3", "2", "10", "1", "1", "50", d], env=env, capture_output=True, text=True,
+                                 timeout=1200)
+            line = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+            if out.returncode != 0 or not line:
+                return {"unavailable": f"ref_dump stokes_mg failed (rc {out.returncode})"}
+            secs[its] = json.loads(line[-1])["seconds"]
+    per_it_ref = (secs[3] - secs[1]) / 2
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(k_np)
+    gpu = {}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for tag, mg32, outer in (("fp64_mg", False, 0), ("fp32_refine", True, 2)):
+        s = shell.StokesSolver(level, kv, mg_levels=4, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=mg32,
+                               chebyshev_order=3, relative_tolerance=1e-30, max_iterations=20, restart=100,
+                               r_min=RMIN, r_max=RMAX, gca=1, outer=outer)
+        xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+        s.solve(fu, fp, xu, xp)  # warm-up: eigenvalue estimates, graph capture
+        xu.data.zero_()
+        xp.data.zero_()
+        torch.cuda.synchronize()
+        ev0.record()
+        it, _ = s.solve(fu, fp, xu, xp)
+        ev1.record()
+        torch.cuda.synchronize()
+        gpu[tag] = round(ev0.elapsed_time(ev1) / 1e3 / it, 6)
+        del s
+    return {"kind": "reference", "cores": cores, "level": level,
+            "seconds_per_iteration": round(per_it_ref, 4), "unit": "s per FGMRES iteration",
+            "sample": f"ref_dump stokes_mg at level {level} (free-slip both radii, the bench's 1e4-contrast viscosity "
+                      f"and buoyancy RHS), 1 and 3 FGMRES(100) iterations ({secs[1]:.1f} s, {secs[3]:.1f} s), "
+                      f"Kokkos-OpenMP, {cores} threads",
+            "b200_seconds_per_iteration": gpu}
+
+
 def max_over_ranks(value, world, device):
     """The largest of the ranks' values (every rank calls this, in the same order); the value itself at N = 1."""
     if world <= 1:
@@ -1006,6 +1124,9 @@ def main():
             line["laplace_cg"] = laplace_cg_leg(shell, torch, reference=not args.no_cpu_baseline)
         if world == 1 and not args.no_stokes:
             line["stokes"] = stokes_leg(shell, C, torch, k_np)
+            line["stokes"]["vs_reference_solution"] = stokes_reference_solution(shell, C, torch)
+            if not args.no_cpu_baseline:
+                line["stokes"]["cpu_baseline"] = stokes_cpu_baseline(shell, C, torch)
         if world == 1 and not args.no_adjoint:
             line["adjoint"] = adjoint_leg(shell, C, torch)
         if world == 1 and not args.no_level8:

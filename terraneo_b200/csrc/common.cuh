@@ -94,6 +94,9 @@ struct tn_mesh
     // (diamond, x, y) FV cell across the face of ghost cell i on side
     // (x = 0, x = N+1, y = 0, y = N+1) of diamond d
     int* d_fv_ghost = nullptr;
+    // per FV cell (with ghosts, fv index): bit n set when face n's geometric normal points into the cell and is
+    // flipped (the orientation test against the neighbour's centre), built on first use
+    uint8_t* d_fv_orient = nullptr;
 
     // lateral quadrature tables of the gradient-form operators (Laplace,
     // DivKGrad, VectorLaplace), built on first use: [10][N][N][2 wedges][105]

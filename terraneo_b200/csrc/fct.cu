@@ -37,6 +37,7 @@ struct FvGeom
     const double*        radii;
     Ptr3< const double > cen; // FV cell centres with ghosts
     Ptr3< const double > vel; // Q1 velocity (stored nodes)
+    const uint8_t*       orient; // face orientation bits per cell (nullptr: the centre test)
 };
 
 __device__ __forceinline__ void cross3( const double a[3], const double b[3], double c[3] )
@@ -68,7 +69,11 @@ __device__ __forceinline__ void cross3( const double a[3], const double b[3], do
 // These are the same sums (exact algebra, different rounding: ~1e-16
 // relative), about 150 FP64 operations per cell instead of ~3,000.  Every face
 // is then oriented from this cell towards the neighbour's centre.
-__device__ void fv_geometry( const FvGeom& G, int d, int x, int y, int r, double beta[6], double& Mii, double S[6][3] )
+// WITH_VELOCITY: the face fluxes beta (false: geometry only); WITH_S: the face vectors S, needed by the
+// orientation test and the diffusion term only (with the orientation bits and no diffusivity they are dead).
+template < bool WITH_VELOCITY = true, bool WITH_S = true >
+__device__ void fv_geometry( const FvGeom& G, int d, int x, int y, int r, double beta[6], double& Mii, double S[6][3],
+                             uint8_t* flips = nullptr )
 {
     const int    N = G.N, n1 = N + 1, n2 = N + 2;
     const double r1 = G.radii[d * n1 + r - 1], r2 = G.radii[d * n1 + r];
@@ -99,7 +104,7 @@ __device__ void fv_geometry( const FvGeom& G, int d, int x, int y, int r, double
             const size_t id = lat * n1 + r - 1 + kWedgeNode[w][i][2];
 #pragma unroll
             for ( int c = 0; c < 3; ++c )
-                u[i][c] = G.vel.p[c][id];
+                u[i][c] = WITH_VELOCITY ? G.vel.p[c][id] : 0.0;
         }
         double va[3], vb[3], ab[3], bp[3], ap[3];
 #pragma unroll
@@ -117,10 +122,13 @@ __device__ void fv_geometry( const FvGeom& G, int d, int x, int y, int r, double
             by += ap[c] * ( Rb * ( u[0][c] + u[1][c] ) + Rt * ( u[3][c] + u[4][c] ) );
             bl += ab[c] * ( u[0][c] + u[1][c] + u[2][c] );
             bt += ab[c] * ( u[3][c] + u[4][c] + u[5][c] );
-            S[nx][c] += rs * h * bp[c];
-            S[ny][c] += rs * h * ap[c];
-            S[4][c] += 0.5 * r1s * ab[c];
-            S[5][c] += 0.5 * r2s * ab[c];
+            if ( WITH_S )
+            {
+                S[nx][c] += rs * h * bp[c];
+                S[ny][c] += rs * h * ap[c];
+                S[4][c] += 0.5 * r1s * ab[c];
+                S[5][c] += 0.5 * r2s * ab[c];
+            }
         }
         beta[nx] += h * bx;
         beta[ny] += h * by;
@@ -129,24 +137,38 @@ __device__ void fv_geometry( const FvGeom& G, int d, int x, int y, int r, double
         const double D = ab[0] * p[0][0] + ab[1] * p[0][1] + ab[2] * p[0][2];
         Mii += 0.5 * h * fabs( D ) * ( rm * rm + rp * rp );
     }
-    // orient every face from this cell towards the neighbour's centre
-    const size_t ci = fv_index( n2, d, x, y, r );
-#pragma unroll
-    for ( int nb = 0; nb < 6; ++nb )
+    // orient every face from this cell towards the neighbour's centre: from the mesh's orientation bits (the
+    // same test, made once per mesh), else the test itself
+    const size_t ci   = fv_index( n2, d, x, y, r );
+    unsigned     bits = 0;
+    if ( G.orient )
+        bits = G.orient[ci];
+    else if ( WITH_S )
     {
-        const size_t cj = fv_index( n2, d, x + kFvOff[nb][0], y + kFvOff[nb][1], r + kFvOff[nb][2] );
-        double       dc = 0.0;
 #pragma unroll
-        for ( int a = 0; a < 3; ++a )
-            dc += S[nb][a] * ( G.cen.p[a][cj] - G.cen.p[a][ci] );
-        if ( dc < 0 )
+        for ( int nb = 0; nb < 6; ++nb )
         {
+            const size_t cj = fv_index( n2, d, x + kFvOff[nb][0], y + kFvOff[nb][1], r + kFvOff[nb][2] );
+            double       dc = 0.0;
 #pragma unroll
             for ( int a = 0; a < 3; ++a )
-                S[nb][a] = -S[nb][a];
-            beta[nb] = -beta[nb];
+                dc += S[nb][a] * ( G.cen.p[a][cj] - G.cen.p[a][ci] );
+            if ( dc < 0 )
+                bits |= 1u << nb;
         }
     }
+    if ( flips )
+        *flips = uint8_t( bits );
+#pragma unroll
+    for ( int nb = 0; nb < 6; ++nb )
+        if ( bits >> nb & 1u )
+        {
+            if ( WITH_S )
+#pragma unroll
+                for ( int a = 0; a < 3; ++a )
+                    S[nb][a] = -S[nb][a];
+            beta[nb] = -beta[nb];
+        }
 }
 
 __device__ __forceinline__ bool cell_of_thread( int N, int& d, int& x, int& y, int& r )
@@ -219,6 +241,17 @@ __global__ void fv_ghost_kernel( int N, const int* __restrict__ map, double* __r
 
 // compute_dt_stable (fct_advection_diffusion.hpp:193-254): min over cells of
 // M / (inflow + diffusion); positive doubles order like their bit patterns
+// the face orientation bits of every interior cell (fv_geometry's centre test, no velocity)
+__global__ void __launch_bounds__( kFvThreads ) orient_kernel( FvGeom G, uint8_t* bits )
+{
+    int d, x, y, r;
+    if ( !cell_of_thread( G.N, d, x, y, r ) )
+        return;
+    double beta[6], Mii, S[6][3];
+    fv_geometry< false >( G, d, x, y, r, beta, Mii, S, bits + fv_index( G.N + 2, d, x, y, r ) );
+}
+
+template < bool DIFFUSION >
 __global__ void __launch_bounds__( kFvThreads ) dt_kernel( FvGeom G, double kappa, unsigned long long* out )
 {
     int    d, x, y, r;
@@ -227,13 +260,13 @@ __global__ void __launch_bounds__( kFvThreads ) dt_kernel( FvGeom G, double kapp
     {
         const int n2 = G.N + 2;
         double    beta[6], Mii, S[6][3], lambda = 0.0;
-        fv_geometry( G, d, x, y, r, beta, Mii, S );
+        fv_geometry< true, DIFFUSION >( G, d, x, y, r, beta, Mii, S );
         const size_t ci = fv_index( n2, d, x, y, r );
         for ( int n = 0; n < 6; ++n )
         {
             if ( beta[n] < 0 )
                 lambda -= beta[n];
-            if ( kappa > 0 )
+            if ( DIFFUSION && kappa > 0 )
             {
                 const size_t cj  = fv_index( n2, d, x + kFvOff[n][0], y + kFvOff[n][1], r + kFvOff[n][2] );
                 double       den = 0.0, ss = 0.0;
@@ -254,7 +287,8 @@ __global__ void __launch_bounds__( kFvThreads ) dt_kernel( FvGeom G, double kapp
         atomicMin( out, (unsigned long long) __double_as_longlong( dtc ) );
 }
 
-// FCTPredictorKernel (fct_advection_diffusion.hpp:262-376)
+// FCTPredictorKernel (fct_advection_diffusion.hpp:262-376); DIFFUSION: kappa != 0
+template < bool DIFFUSION >
 __global__ void __launch_bounds__( kFvThreads )
     predictor_kernel( FvGeom G, const double* __restrict__ T, double* __restrict__ TL, double* __restrict__ F, double dt,
                       double kappa, const double* __restrict__ src, int subtract_divergence )
@@ -264,7 +298,7 @@ __global__ void __launch_bounds__( kFvThreads )
         return;
     const int n2 = G.N + 2;
     double    beta[6], Mii, S[6][3];
-    fv_geometry( G, d, x, y, r, beta, Mii, S );
+    fv_geometry< true, DIFFUSION >( G, d, x, y, r, beta, Mii, S );
     const size_t i  = fv_index( n2, d, x, y, r );
     const size_t nf = size_t( kDiamonds ) * n2 * n2 * n2; // F holds 6 planes of nf (SoA)
     const double Ti = T[i];
@@ -278,15 +312,18 @@ __global__ void __launch_bounds__( kFvThreads )
         else
             lo_update += beta[n] * Tj;
         bsum += beta[n];
-        double den = 0.0, ss = 0.0;
-        for ( int a = 0; a < 3; ++a )
+        if ( DIFFUSION ) // the diffusion term; zero without diffusivity (no centre loads)
         {
-            den += ( G.cen.p[a][j] - G.cen.p[a][i] ) * S[n][a];
-            ss += S[n][a] * S[n][a];
+            double den = 0.0, ss = 0.0;
+            for ( int a = 0; a < 3; ++a )
+            {
+                den += ( G.cen.p[a][j] - G.cen.p[a][i] ) * S[n][a];
+                ss += S[n][a] * S[n][a];
+            }
+            const double dc = kappa * ( ss / den );
+            lo_diag += dc;
+            lo_update -= dc * Tj;
         }
-        const double dc = kappa * ( ss / den );
-        lo_diag += dc;
-        lo_update -= dc * Tj;
         F[n * nf + i] = ( dt / Mii ) * ( fabs( beta[n] ) / 2.0 ) * ( Ti - Tj );
     }
     if ( subtract_divergence )
@@ -380,7 +417,56 @@ int ghost_update( const tn_mesh* m, double* f, cudaStream_t st )
     return TN_OK;
 }
 
-int make_geom( const tn_mesh* m, const double* const* vel, const double* const* cen, FvGeom& G )
+// The face orientation bits of the mesh, from its own cell centres (compute_cell_centers, the centres
+// tn_fv_cell_centers_f64 gives), built on the first FCT call of the mesh: the orientation is geometry, so the
+// per-step kernels read one byte per cell instead of the six neighbours' centres.
+const uint8_t* fv_orientation( const tn_mesh* m, cudaStream_t st )
+{
+    tn_mesh*                      mm = const_cast< tn_mesh* >( m );
+    std::lock_guard< std::mutex > lock( mm->geom_mutex );
+    if ( !mm->d_fv_orient )
+    {
+        const size_t nf = fv_size( m );
+        double*      c  = nullptr;
+        uint8_t*     b  = nullptr;
+        if ( cudaMalloc( &c, 3 * nf * sizeof( double ) ) != cudaSuccess )
+            return nullptr;
+        if ( cudaMalloc( &b, nf ) != cudaSuccess )
+        {
+            cudaFree( c );
+            return nullptr;
+        }
+        bool ok = cudaMemsetAsync( c, 0, 3 * nf * sizeof( double ), st ) == cudaSuccess &&
+                  cudaMemsetAsync( b, 0, nf, st ) == cudaSuccess;
+        Ptr3< double > cp{ { c, c + nf, c + 2 * nf } };
+        if ( ok )
+        {
+            cell_centers_kernel<<< cell_blocks( m ), kFvThreads, 0, st >>>( m->N, m->d_coords, m->d_radii, cp );
+            ok = cudaGetLastError() == cudaSuccess;
+        }
+        for ( int a = 0; a < 3 && ok; ++a )
+            ok = ghost_update( m, c + a * nf, st ) == TN_OK;
+        if ( ok )
+        {
+            FvGeom G{};
+            G.N = m->N, G.coords = m->d_coords, G.radii = m->d_radii;
+            G.cen    = Ptr3< const double >{ { c, c + nf, c + 2 * nf } };
+            G.orient = nullptr;
+            orient_kernel<<< cell_blocks( m ), kFvThreads, 0, st >>>( G, b );
+            ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize( st ) == cudaSuccess;
+        }
+        cudaFree( c );
+        if ( !ok )
+        {
+            cudaFree( b );
+            return nullptr;
+        }
+        mm->d_fv_orient = b;
+    }
+    return mm->d_fv_orient;
+}
+
+int make_geom( const tn_mesh* m, const double* const* vel, const double* const* cen, FvGeom& G, cudaStream_t st )
 {
     TN_CHECK_ARG( vel && cen, "fct: null field list" );
     for ( int a = 0; a < 3; ++a )
@@ -390,6 +476,12 @@ int make_geom( const tn_mesh* m, const double* const* vel, const double* const* 
         G.cen.p[a] = cen[a];
     }
     G.N = m->N, G.coords = m->d_coords, G.radii = m->d_radii;
+    G.orient = fv_orientation( m, st );
+    if ( !G.orient )
+    {
+        set_error( "fct: building the face orientation of the mesh failed" );
+        return TN_ERR_CUDA;
+    }
     return TN_OK;
 }
 
@@ -443,13 +535,16 @@ extern "C" int tn_fct_dt_stable_f64( const tn_mesh* m, const double* const* vel,
     TN_CHECK_ARG( m && dt_stable, "tn_fct_dt_stable_f64: null argument" );
     FvGeom G{};
     int    rc;
-    if ( ( rc = make_geom( m, vel, centers, G ) ) )
+    cudaStream_t st = as_stream( s );
+    if ( ( rc = make_geom( m, vel, centers, G, st ) ) )
         return rc;
-    cudaStream_t        st   = as_stream( s );
     unsigned long long* slot = reinterpret_cast< unsigned long long* >( m->d_red_result + 12 );
     const double        init = 1e300;
     TN_CUDA_TRY( cudaMemcpyAsync( slot, &init, sizeof( double ), cudaMemcpyHostToDevice, st ) );
-    dt_kernel<<< cell_blocks( m ), kFvThreads, 0, st >>>( G, diffusivity, slot );
+    if ( diffusivity != 0.0 )
+        dt_kernel< true ><<< cell_blocks( m ), kFvThreads, 0, st >>>( G, diffusivity, slot );
+    else
+        dt_kernel< false ><<< cell_blocks( m ), kFvThreads, 0, st >>>( G, diffusivity, slot );
     TN_LAUNCH_CHECK();
     TN_CUDA_TRY( cudaMemcpyAsync( dt_stable, slot, sizeof( double ), cudaMemcpyDeviceToHost, st ) );
     TN_CUDA_TRY( cudaStreamSynchronize( st ) );
@@ -473,9 +568,9 @@ extern "C" int tn_fct_step_f64( const tn_mesh* m, double* T, const double* const
     TN_CHECK_ARG( m && T && workspace, "tn_fct_step_f64: null argument" );
     FvGeom G{};
     int    rc;
-    if ( ( rc = make_geom( m, vel, centers, G ) ) )
-        return rc;
     cudaStream_t st = as_stream( s );
+    if ( ( rc = make_geom( m, vel, centers, G, st ) ) )
+        return rc;
     const size_t nf = fv_size( m );
     double *     TL = workspace, *F = workspace + nf, *Rp = workspace + 7 * nf, *Rm = workspace + 8 * nf;
     TN_CUDA_TRY( cudaMemsetAsync( TL, 0, sizeof( double ) * nf, st ) );
@@ -483,8 +578,12 @@ extern "C" int tn_fct_step_f64( const tn_mesh* m, double* T, const double* const
     // predictor (fct_advection_diffusion.hpp:384-433) on T with fresh lateral ghosts
     if ( ( rc = ghost_update( m, T, st ) ) )
         return rc;
-    predictor_kernel<<< cell_blocks( m ), kFvThreads, 0, st >>>( G, T, TL, F, dt, diffusivity, source,
-                                                                 subtract_divergence );
+    if ( diffusivity != 0.0 )
+        predictor_kernel< true ><<< cell_blocks( m ), kFvThreads, 0, st >>>( G, T, TL, F, dt, diffusivity, source,
+                                                                             subtract_divergence );
+    else
+        predictor_kernel< false ><<< cell_blocks( m ), kFvThreads, 0, st >>>( G, T, TL, F, dt, diffusivity, source,
+                                                                              subtract_divergence );
     TN_LAUNCH_CHECK();
     if ( bcs && ( rc = tn_fct_apply_dirichlet_f64( m, TL, bcs, s ) ) )
         return rc;

@@ -348,6 +348,7 @@ extern "C" int tn_mesh_destroy( tn_mesh* m )
     cudaFree( m->d_halo_members );
     cudaFree( m->d_lat_group );
     cudaFree( m->d_fv_ghost );
+    cudaFree( m->d_fv_orient );
     cudaFree( m->d_grad_geom );
     cudaFree( m->d_stokes_geom );
     cudaFree( m->d_red_partials );

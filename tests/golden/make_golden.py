@@ -13,6 +13,8 @@ Usage (in a container that has the reference sources and a built ref_dump):
     python tests/golden/make_golden.py --xdmf        # xdmf_L2/: a checkpoint written by io::XDMFOutput
     python tests/golden/make_golden.py --supg        # adds the SUPG operator cases to ref_L2.npz
     python tests/golden/make_golden.py --agca        # adds the adaptive-GCA cases (level 3) to ref_L2.npz
+    python tests/golden/make_golden.py --stokes-mg-inputs  # stokes_mg_L4_inputs.npz: the free-slip inputs of
+                                                           # ref_stokes_mg_L4.npz for a reader without the oracle
 """
 import os
 import sys
@@ -222,6 +224,15 @@ def make_stokes_mg():
             print("stokes_mg", bcc, bcs, info)
     path = os.path.join(HERE, "ref_stokes_mg_L4.npz")
     np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+def make_stokes_mg_inputs():
+    """stokes_mg_L4_inputs.npz: the free-slip (2, 2) inputs of ref_stokes_mg_L4.npz as arrays (the bench compares
+    its solver forms with the reference's solution there and does not load the oracle)"""
+    k, kp, fu, fp = stokes_mg_inputs(2, 2)
+    path = os.path.join(HERE, "stokes_mg_L4_inputs.npz")
+    np.savez_compressed(path, k=k, kp=kp, f_u=fu, f_p=fp)
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
@@ -509,7 +520,7 @@ def make_xdmf():
 
 
 if __name__ == "__main__":
-    if "--stokes-mg" in sys.argv:
+    if "--stokes-mg" in sys.argv and "--stokes-mg-inputs" not in sys.argv:
         make_stokes_mg()
     elif "--xdmf" in sys.argv:
         make_xdmf()
@@ -517,5 +528,7 @@ if __name__ == "__main__":
         make_supg()
     elif "--agca" in sys.argv:
         make_agca()
+    elif "--stokes-mg-inputs" in sys.argv:
+        make_stokes_mg_inputs()
     else:
         main()
