@@ -243,13 +243,18 @@ __global__ void __launch_bounds__( 128 ) divergence_kernel( StokesParams< T > P,
         divergence_wedge< T, 1 >( P, u, p, dm, x, y, r );
 }
 
-// u_fine += B^T p, wedge W of fine cell (dm, x, y, r)
+// u_fine += B^T p, wedge W of fine cell (dm, x, y, r).  Lanes are consecutive radial cells of one column
+// (whole columns per warp): the top-node contributions of a lane go to the lane above by shuffle, where they
+// meet the same nodes as that lane's bottom nodes, so each lane adds its bottom nodes and only the column's
+// last cell in the warp also adds its top nodes (about half the reductions).  Boundary treatment acts on
+// bottom nodes at r = 0 and top nodes at r = N - 1, never on a handed-over value.
 template < typename T, int W >
 __device__ __forceinline__ void gradient_wedge( const StokesParams< T >& P, const T* p, const Ptr3< T >& u, int dm,
                                                 int x, int y, int r )
 {
     const int N = P.N, n1 = P.n1, nc1 = P.nc1;
     const int xc = x >> 1, yc = y >> 1, rc = r >> 1;
+    const int lane = threadIdx.x & 31;
     T         Ra[2][2], Rb[2];
     radial_sums( P.radii[dm * n1 + r], P.radii[dm * n1 + r + 1], r & 1, Ra, Rb );
     const double* G = P.geom + stokes_tri( N, dm, x, y, W ) * kStokesStride;
@@ -269,6 +274,8 @@ __device__ __forceinline__ void gradient_wedge( const StokesParams< T >& P, cons
         for ( int nb = 0; nb < 2; ++nb )
             pr[nb][ic] = Ra[0][nb] * pc[ic] + Ra[1][nb] * pc[3 + ic];
     }
+    const bool from_below = lane > 0 && r > 0;        // the lane below is cell r - 1 of this column
+    const bool adds_top   = lane == 31 || r == N - 1; // no lane above takes this cell's top nodes
 #pragma unroll
     for ( int m = 0; m < 3; ++m )
     {
@@ -276,33 +283,47 @@ __device__ __forceinline__ void gradient_wedge( const StokesParams< T >& P, cons
 #pragma unroll
         for ( int ic = 0; ic < 3; ++ic )
             sv += T( G[30 + ic * 3 + m] ) * pl[ic];
+        T v[2][3];
 #pragma unroll
         for ( int nb = 0; nb < 2; ++nb )
         {
-            const int j = nb * 3 + m;
-            const T   s = ( nb ? T( 0.5 ) : T( -0.5 ) ) * sv;
-            T         v[3] = { s * vt[0], s * vt[1], s * vt[2] };
+            const T s = ( nb ? T( 0.5 ) : T( -0.5 ) ) * sv;
+            v[nb][0] = s * vt[0], v[nb][1] = s * vt[1], v[nb][2] = s * vt[2];
 #pragma unroll
             for ( int ic = 0; ic < 3; ++ic )
             {
                 const double* U = G + ( ic * 3 + m ) * 3;
-                v[0] += pr[nb][ic] * T( U[0] ), v[1] += pr[nb][ic] * T( U[1] ), v[2] += pr[nb][ic] * T( U[2] );
+                v[nb][0] += pr[nb][ic] * T( U[0] ), v[nb][1] += pr[nb][ic] * T( U[1] ),
+                    v[nb][2] += pr[nb][ic] * T( U[2] );
             }
-            const int bc = velocity_bc( N, r, j, P.bc_cmb, P.bc_surf );
+        }
+        const int X = x + kWedgeNode[W][m][0], Y = y + kWedgeNode[W][m][1];
+#pragma unroll
+        for ( int c = 0; c < 3; ++c )
+        {
+            const T below = __shfl_up_sync( 0xffffffffu, v[1][c], 1 );
+            if ( from_below )
+                v[0][c] += below;
+        }
+#pragma unroll
+        for ( int nb = 0; nb < 2; ++nb )
+        {
+            if ( nb == 1 && !adds_top )
+                continue;
+            const int bc = velocity_bc( N, r, nb * 3 + m, P.bc_cmb, P.bc_surf );
             if ( bc == TN_BC_DIRICHLET )
                 continue;
-            const int X = x + kWedgeNode[W][j][0], Y = y + kWedgeNode[W][j][1];
             if ( bc == TN_BC_FREESLIP )
             {
                 T nn[3];
                 unit_normal( P.coords + lat_index( n1, dm, X, Y ) * 3, nn );
-                const T dt = nn[0] * v[0] + nn[1] * v[1] + nn[2] * v[2];
-                v[0] -= dt * nn[0], v[1] -= dt * nn[1], v[2] -= dt * nn[2];
+                const T dt = nn[0] * v[nb][0] + nn[1] * v[nb][1] + nn[2] * v[nb][2];
+                v[nb][0] -= dt * nn[0], v[nb][1] -= dt * nn[1], v[nb][2] -= dt * nn[2];
             }
-            const size_t i = lat_index( n1, dm, X, Y ) * n1 + r + kWedgeNode[W][j][2];
-            atomicAdd( u.p[0] + i, v[0] );
-            atomicAdd( u.p[1] + i, v[1] );
-            atomicAdd( u.p[2] + i, v[2] );
+            const size_t i = lat_index( n1, dm, X, Y ) * n1 + r + nb;
+            atomicAdd( u.p[0] + i, v[nb][0] );
+            atomicAdd( u.p[1] + i, v[nb][1] );
+            atomicAdd( u.p[2] + i, v[nb][2] );
         }
     }
 }
