@@ -765,9 +765,34 @@ def reference_inputs(directory):
     return m
 
 
-def cpu_baseline(steps):
+def apply_errors_vs_reference(ref, env, d, m):
+    """The reference's FP64 apply (ref_dump kerngen, Dirichlet both radii) of the inputs in d against the B200's
+    FP64 and FP32 applies of the same inputs: relative 2-norm differences over all stored nodes"""
+    import torch
+    from terraneo_b200 import shell, _capi as C
+    out = subprocess.run([ref, "kerngen", str(LEVEL), str(RMIN), str(RMAX), "1", "1", "0", d], env=env,
+                         capture_output=True, text=True, timeout=600)
+    if out.returncode != 0:
+        return None
+    want = np.fromfile(os.path.join(d, "dst.bin")).reshape((3,) + m.shape)
+    k = np.fromfile(os.path.join(d, "k.bin")).reshape(m.shape)
+    u = np.fromfile(os.path.join(d, "src.bin")).reshape((3,) + m.shape)
+    pm = shell.ShellMesh(LEVEL, RMIN, RMAX)
+    res = {}
+    for tag, dt in (("fp64", torch.float64), ("fp32", torch.float32)):
+        kv, s, o = shell.VectorQ1Scalar(pm, dt), shell.VectorQ1Vec(pm, dt), shell.VectorQ1Vec(pm, dt)
+        kv.set_numpy(k)
+        s.set_numpy(u)
+        shell.apply(shell.EpsilonDivDivKerngen(pm, kv, C.BC_DIRICHLET, C.BC_DIRICHLET), s, o)
+        torch.cuda.synchronize()
+        res[tag] = float(f"{np.linalg.norm(o.numpy().astype(np.float64) - want) / np.linalg.norm(want):.3e}")
+    return res
+
+
+def cpu_baseline(steps, shell_mods=True):
     """The reference's own Kokkos-OpenMP apply (oracle/_ref) on the bench's seeded inputs, else the C oracle,
-    on this host."""
+    on this host; with shell_mods, also the B200 FP64 / FP32 applies' relative errors against the reference's
+    output on the same inputs."""
     import tempfile
     ref = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
     cores = os.cpu_count() or 1
@@ -782,7 +807,9 @@ def cpu_baseline(steps):
             if out.returncode == 0 and line:
                 info = json.loads(line[-1])
                 sec = info["seconds_per_apply"]
+                errors = apply_errors_vs_reference(ref, env, d, m) if shell_mods else None
                 return {"value": dofs / sec / 1e9, "unit": "GDoF/s", "cores": info["threads"], "kind": "reference",
+                        "rel_error_vs_reference": errors,
                         "sample": f"{steps} EpsilonDivDivKerngen<double> applies (Dirichlet/Dirichlet, level {LEVEL}, "
                                   f"the bench's seeded 1e4-contrast k and N(0,1) src) after 1 warm-up, "
                                   f"Kokkos-OpenMP, {info['threads']} threads",
@@ -914,7 +941,7 @@ def run_reference(args, rank):
     if rank != 0:
         return 0
     steps = max(1, args.steps)  # the same number of timed applies as the library's arm
-    cb = cpu_baseline(steps)
+    cb = cpu_baseline(steps, shell_mods=False)  # the reference alone: none of this library's kernels
     line = {"metric": METRIC, "impl": "reference", "value": cb["value"], "unit": "GDoF/s", "n_gpus": args.gpus,
             "steps": steps, "warmup": 1, "ms_per_step": cb["seconds_per_apply"] * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -1136,6 +1163,8 @@ def main():
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_baseline(steps=3)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            # the C2 comparison: the B200's FP64 and FP32 applies against the reference's own FP64 apply
+            line["apply_rel_error_vs_reference"] = cb.get("rel_error_vs_reference")
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -13,6 +13,7 @@
 #include "linalg/operator.hpp"
 #include "linalg/solvers/chebyshev.hpp"
 #include "linalg/solvers/fgmres.hpp"
+#include "linalg/solvers/pbicgstab.hpp"
 #include "linalg/solvers/pcg.hpp"
 #include "linalg/solvers/power_iteration.hpp"
 #include "linalg/solvers/solver.hpp"
@@ -34,6 +35,7 @@ static_assert( L::OperatorLike< tn::EpsilonDivDivKerngen< double > > );
 static_assert( L::OperatorLike< tn::EpsilonDivDivKerngen< float > > );
 static_assert( L::OperatorLike< tn::Laplace< double > > );
 static_assert( L::OperatorLike< tn::EpsDivDivStokes< double > > );
+static_assert( L::OperatorLike< tn::UnsteadyAdvectionDiffusionSUPG< double > > );
 static_assert( L::OperatorLike< B200Op > );
 
 // the reference's drivers over the library's operators and vectors
@@ -41,9 +43,11 @@ template class S::PCG< tn::EpsilonDivDivKerngen< double > >;
 template class S::PCG< tn::Laplace< double > >;
 template class S::Chebyshev< tn::EpsilonDivDivKerngen< double > >;
 template class S::FGMRES< tn::EpsDivDivStokes< double > >;
+template class S::PBiCGStab< tn::UnsteadyAdvectionDiffusionSUPG< double > >;
 static_assert( S::SolverLike< S::PCG< tn::EpsilonDivDivKerngen< double > > > );
 static_assert( S::SolverLike< S::Chebyshev< tn::EpsilonDivDivKerngen< double > > > );
 static_assert( S::SolverLike< S::FGMRES< tn::EpsDivDivStokes< double > > > );
+static_assert( S::SolverLike< S::PBiCGStab< tn::UnsteadyAdvectionDiffusionSUPG< double > > > );
 template double S::power_iteration< tn::EpsilonDivDivKerngen< double > >( tn::EpsilonDivDivKerngen< double >&,
                                                                            tn::VectorQ1Vec< double >&,
                                                                            tn::VectorQ1Vec< double >&, int );
