@@ -676,6 +676,61 @@ TN_API int tn_xdmf_checkpoint_grid_data_file( const char* directory, int index, 
 TN_API int tn_read_xdmf_checkpoint_grid( const tn_mesh* mesh, const char* directory, const char* label, int step,
                                          int dst_bytes, int vec_dim, void* const* dst, void* stream );
 
+/* ---------------------------------------------------------------------------
+ * Sharded shell: one rank's diamonds, one process per GPU.
+ *
+ * The reference's DistributedDomain::create_uniform (grid/shell/spherical_shell.hpp:2566-2590) with lateral and
+ * radial subdomain refinement level 0 and its default map subdomain_to_rank_iterate_diamond_subdomains (:717-745)
+ * gives rank q of P a contiguous block of diamonds: 10 / P of them, one more on the first 10 % P ranks.  A shard
+ * holds that block compactly (local diamond index = global id - first diamond; the node layout of the mesh for each
+ * diamond).  Finer subdomains are not supported: the operator kernels sweep whole diamonds.
+ *
+ * The additive halo of the reference's apply (send_recv: pack_send_and_recv_local_subdomain_boundaries +
+ * unpack_and_reduce_local_subdomain_boundaries with SUM, communication/shell/communication.hpp:242-747) is split:
+ * an apply with TN_COMM_ADDITIVE sums the copies of the duplicated nodes that all lie on this rank; the nodes with
+ * copies on two or more ranks ("cross groups", in one order on every rank) are summed by
+ *     tn_shard_pack   (buf = per cross group and radius the sum of this rank's copies, layout [field][group][r]),
+ *     an all-reduce (SUM) of buf over the ranks by the caller's communicator (NCCL, MPI),
+ *     tn_shard_unpack (every local copy = buf).
+ * An exchange buffer holds nfields * exchange_values entries (tn_shard_dims); it is the same size on every rank. */
+typedef struct tn_shard tn_shard;
+
+/* Host only: the first diamond and the number of diamonds of `rank` (num_ranks in [1, 10]). */
+TN_API int tn_shell_partition( int num_ranks, int rank, int* first_diamond, int* num_diamonds );
+/* Host only: the rank's duplicate groups at `level`, CSR over local lateral indices
+ * (local diamond * (N+1)^2 + x (N+1) + y), copies ascending: cross = 0 the groups whose copies all lie on this rank,
+ * cross = 1 the cross groups (a group without a copy here is empty).  offsets has n_groups + 1 entries, members
+ * n_members; pass NULL arrays to query the counts. */
+TN_API int tn_shard_halo_plan( int level, int num_ranks, int rank, int cross, int* n_groups, int* n_members,
+                               int* offsets, int* members );
+TN_API int tn_shard_create( int level, double r_min, double r_max, int num_ranks, int rank, tn_shard** out );
+TN_API int tn_shard_destroy( tn_shard* shard );
+/* stored nodes = diamonds (N+1)^3; owned = the nodes this rank owns (ownership as on the whole shell: the copy in
+ * the lowest diamond), summing to (10 N^2 + 2)(N+1) over the ranks; exchange_values = cross groups x (N+1) */
+TN_API int tn_shard_dims( const tn_shard* shard, int* first_diamond, int* num_diamonds, size_t* stored_nodes,
+                          size_t* owned_nodes, size_t* exchange_values );
+/* host copies: coords [diamonds][N+1][N+1][3], radii [diamonds][N+1]; masks [diamonds][N+1][N+1][N+1] */
+TN_API int tn_shard_geometry( const tn_shard* shard, double* coords, double* radii );
+TN_API int tn_shard_masks( const tn_shard* shard, uint8_t* boundary_mask, uint8_t* ownership_mask );
+/* EpsilonDivDivKerngen apply on the shard's cells (tn_epsdivdiv_apply_*); free-slip on both radii (the global
+ * rigid-rotation penalty) only with num_ranks = 1 */
+TN_API int tn_shard_epsdivdiv_apply_f64( const tn_shard* shard, const tn_epsdivdiv_params* p, const double* k,
+                                         const double* const* src, double* const* dst, void* stream );
+TN_API int tn_shard_epsdivdiv_apply_f32( const tn_shard* shard, const tn_epsdivdiv_params* p, const float* k,
+                                         const float* const* src, float* const* dst, void* stream );
+TN_API int tn_shard_pack_f64( const tn_shard* shard, const double* const* fields, int nfields, double* buf,
+                              void* stream );
+TN_API int tn_shard_pack_f32( const tn_shard* shard, const float* const* fields, int nfields, float* buf, void* stream );
+TN_API int tn_shard_unpack_f64( const tn_shard* shard, const double* buf, double* const* fields, int nfields,
+                                void* stream );
+TN_API int tn_shard_unpack_f32( const tn_shard* shard, const float* buf, float* const* fields, int nfields,
+                                void* stream );
+/* this rank's owned-node part of a dot product (tn_vec_dot_f64); the global dot is its sum over the ranks */
+TN_API int tn_shard_vec_dot_f64( const tn_shard* shard, int ncomp, const double* const* a, const double* const* b,
+                                 double* result, void* stream );
+TN_API int tn_shard_vec_lincomb_f64( const tn_shard* shard, int ncomp, double* const* y, double c0, int nx,
+                                     const double* c, const double* const* x, void* stream );
+
 #ifdef __cplusplus
 }
 #endif

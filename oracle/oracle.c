@@ -416,8 +416,22 @@ static void kerngen_null_modes( int L, const double* coords, const double* radii
  * with one-point quadrature, restating the fast Dirichlet/Neumann path
  * (kerngen :1055-1389), the fast free-slip path (:1421-1940) and the fs/fs
  * penalty (:585-606) followed by the additive halo (:611-616).  Replace mode. */
+static void kerngen_apply( int L, const double* coords, const double* radii, const double* k, const double* src,
+                           double* dst, int bc_cmb, int bc_surf, int diag, int halo );
 void or_kerngen_apply( int L, const double* coords, const double* radii, const double* k, const double* src,
                        double* dst, int bc_cmb, int bc_surf, int diag )
+{
+    kerngen_apply( L, coords, radii, k, src, dst, bc_cmb, bc_surf, diag, 1 );
+}
+/* the same without the closing halo sum: every diamond's copy of a node holds that diamond's cells' contributions
+ * (the copy-wise result of the reference's apply with OperatorCommunicationMode::SkipCommunication) */
+void or_kerngen_apply_copywise( int L, const double* coords, const double* radii, const double* k, const double* src,
+                                double* dst, int bc_cmb, int bc_surf, int diag )
+{
+    kerngen_apply( L, coords, radii, k, src, dst, bc_cmb, bc_surf, diag, 0 );
+}
+static void kerngen_apply( int L, const double* coords, const double* radii, const double* k, const double* src,
+                           double* dst, int bc_cmb, int bc_surf, int diag, int halo )
 {
     const int    N = 1 << L, n1 = N + 1;
     const size_t ns = (size_t) NDIAMOND * n1 * n1 * n1;
@@ -566,7 +580,8 @@ void or_kerngen_apply( int L, const double* coords, const double* radii, const d
         free( modes );
         free( om );
     }
-    or_halo_sum( L, coords, dst, 3 );
+    if ( halo )
+        or_halo_sum( L, coords, dst, 3 );
 }
 
 /* ------------------------------------------------------------------------ */

@@ -42,6 +42,8 @@ void or_supg_apply( int L, const double* coords, const double* radii, const doub
 /* operators (Replace mode, additive communication) */
 void or_kerngen_apply( int L, const double* coords, const double* radii, const double* k, const double* src,
                        double* dst, int bc_cmb, int bc_surf, int diag );
+void or_kerngen_apply_copywise( int L, const double* coords, const double* radii, const double* k, const double* src,
+                                double* dst, int bc_cmb, int bc_surf, int diag );
 void or_laplace_apply( int L, const double* coords, const double* radii, const double* src, double* dst,
                        int treat_boundary, int diag );
 

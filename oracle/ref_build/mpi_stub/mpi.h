@@ -91,16 +91,19 @@ static inline int MPI_Finalized( int* flag )
     *flag = tn_mpi_stub_state == 2;
     return MPI_SUCCESS;
 }
+/* the communicator's size and this process's rank: 1 and 0 unless a driver poses as rank q of P to build that
+ * rank's part of a distributed domain (no message is ever delivered) */
+static int tn_mpi_stub_world_size = 1, tn_mpi_stub_rank = 0;
 static inline int MPI_Comm_rank( MPI_Comm c, int* r )
 {
     (void) c;
-    *r = 0;
+    *r = tn_mpi_stub_rank;
     return MPI_SUCCESS;
 }
 static inline int MPI_Comm_size( MPI_Comm c, int* s )
 {
     (void) c;
-    *s = 1;
+    *s = tn_mpi_stub_world_size;
     return MPI_SUCCESS;
 }
 static inline int MPI_Comm_set_errhandler( MPI_Comm c, MPI_Errhandler e )

@@ -69,6 +69,11 @@
 //                                          (level L-1): dst.bin
 //   supg L rmin rmax kappa dt ms lumped treat diag DIR  UnsteadyAdvectionDiffusionSUPG<double> with the velocity
 //                                          vel.bin (3 x nodes) applied to src.bin: dst.bin
+//   kerngen_rank L rmin rmax bcc bcs P q DIR  the distributed domain as rank q of P (subdomain refinement
+//                                          level 0, the default rank map): prints the rank's diamonds in local
+//                                          order as JSON, then the EpsilonDivDivKerngen<double> apply on them with
+//                                          SkipCommunication (the copy-wise result) of k.bin / src.bin (the rank's
+//                                          nodes): dst.bin
 //   time_kerngen L rmin rmax bcc bcs reps [DIR]  prints seconds per apply (CPU baseline); with DIR the
 //                                          inputs are k.bin / src.bin there, else k = 1, src = 1
 #include <chrono>
@@ -241,6 +246,37 @@ int cmd_kerngen( int L, double rmin, double rmax, int bcc, int bcs, int diag, co
     auto op = make_kerngen( s, k, bcc, bcs, diag != 0 );
     linalg::apply( op, src, dst );
     save_vec( dst, dir + "/dst.bin", s.nodes );
+    return 0;
+}
+
+// The apply of one rank of a distributed run: the stub poses as rank q of P while the domain is built
+// (DistributedDomain::create_uniform_single_subdomain_per_diamond -> subdomain_to_rank_iterate_diamond_subdomains,
+// grid/shell/spherical_shell.hpp:717-745,2520-2590); the apply skips the halo exchange, whose messages the stub
+// cannot deliver.  The ownership mask is left unset (only dot products read it).
+int cmd_kerngen_rank( int L, double rmin, double rmax, int bcc, int bcs, int P, int q, const std::string& dir )
+{
+    tn_mpi_stub_world_size = P, tn_mpi_stub_rank = q;
+    DistributedDomain domain = DistributedDomain::create_uniform_single_subdomain_per_diamond( L, L, rmin, rmax );
+    auto              omask  = grid::shell::allocate_scalar_grid< grid::NodeOwnershipFlag >( "omask", domain );
+    auto              bmask  = grid::shell::setup_boundary_mask_data( domain );
+    auto              coords = grid::shell::subdomain_unit_sphere_single_shell_coords< double >( domain );
+    auto              radii  = grid::shell::subdomain_shell_radii< double >( domain );
+    const size_t      nodes  = omask.size();
+    std::printf( "{\"diamonds\": [" );
+    for ( int i = 0; i < int( domain.subdomains().size() ); ++i )
+        std::printf( "%s%d", i ? ", " : "", domain.subdomain_info_from_local_idx( i ).diamond_id() );
+    std::printf( "], \"nodes\": %zu}\n", nodes );
+    linalg::VectorQ1Scalar< double > k( "k", domain, omask );
+    view_from_host( k.grid_data(), read_file< double >( dir + "/k.bin", nodes ).data() );
+    linalg::VectorQ1Vec< double > src( "src", domain, omask ), dst( "dst", domain, omask );
+    load_vec( src, dir + "/src.bin", nodes );
+    BoundaryConditions bcs_ = { { ShellBoundaryFlag::CMB, bc_of( bcc ) }, { ShellBoundaryFlag::SURFACE, bc_of( bcs ) } };
+    Kerngen            op( domain, coords, radii, bmask, k.grid_data(), bcs_, false );
+    op.set_operator_apply_and_communication_modes(
+        linalg::OperatorApplyMode::Replace, linalg::OperatorCommunicationMode::SkipCommunication );
+    linalg::apply( op, src, dst );
+    save_vec( dst, dir + "/dst.bin", nodes );
+    tn_mpi_stub_world_size = 1, tn_mpi_stub_rank = 0;
     return 0;
 }
 
@@ -1417,6 +1453,8 @@ int main( int argc, char** argv )
         return cmd_fe2fv( I( 2 ), D( 3 ), D( 4 ), argv[5] );
     if ( cmd == "supg" && argc == 12 )
         return cmd_supg( I( 2 ), D( 3 ), D( 4 ), D( 5 ), D( 6 ), D( 7 ), I( 8 ), I( 9 ), I( 10 ), argv[11] );
+    if ( cmd == "kerngen_rank" && argc == 10 )
+        return cmd_kerngen_rank( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), I( 8 ), argv[9] );
     if ( cmd == "agca" && argc == 9 )
         return cmd_agca( I( 2 ), D( 3 ), D( 4 ), I( 5 ), I( 6 ), I( 7 ), argv[8] );
     std::fprintf( stderr, "ref_dump: bad command line\n" );

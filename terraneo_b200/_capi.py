@@ -192,6 +192,24 @@ _SIGS = {
     "tn_vec_randomize_f32": (c_int, [c_void_p, c_int, P(c_void_p), ctypes.c_ulonglong, c_void_p]),
     "tn_vec_cast_f64_to_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
     "tn_vec_cast_f32_to_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_shell_partition": (c_int, [c_int, c_int, P(c_int), P(c_int)]),
+    "tn_shard_halo_plan": (c_int, [c_int, c_int, c_int, c_int, P(c_int), P(c_int), c_void_p, c_void_p]),
+    "tn_shard_create": (c_int, [c_int, c_double, c_double, c_int, c_int, P(c_void_p)]),
+    "tn_shard_destroy": (c_int, [c_void_p]),
+    "tn_shard_dims": (c_int, [c_void_p, P(c_int), P(c_int), P(c_size_t), P(c_size_t), P(c_size_t)]),
+    "tn_shard_geometry": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "tn_shard_masks": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "tn_shard_epsdivdiv_apply_f64": (c_int, [c_void_p, P(EpsDivDivParams), c_void_p, P(c_void_p), P(c_void_p),
+                                             c_void_p]),
+    "tn_shard_epsdivdiv_apply_f32": (c_int, [c_void_p, P(EpsDivDivParams), c_void_p, P(c_void_p), P(c_void_p),
+                                             c_void_p]),
+    "tn_shard_pack_f64": (c_int, [c_void_p, P(c_void_p), c_int, c_void_p, c_void_p]),
+    "tn_shard_pack_f32": (c_int, [c_void_p, P(c_void_p), c_int, c_void_p, c_void_p]),
+    "tn_shard_unpack_f64": (c_int, [c_void_p, c_void_p, P(c_void_p), c_int, c_void_p]),
+    "tn_shard_unpack_f32": (c_int, [c_void_p, c_void_p, P(c_void_p), c_int, c_void_p]),
+    "tn_shard_vec_dot_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_double), c_void_p]),
+    "tn_shard_vec_lincomb_f64": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p),
+                                         c_void_p]),
 }
 
 

@@ -24,6 +24,7 @@ void set_error( const std::string& msg );
         if ( err_ != cudaSuccess )                                                                       \
         {                                                                                                \
             ::tn::set_error( std::string( #expr ) + ": " + cudaGetErrorString( err_ ) );                 \
+            (void) cudaGetLastError(); /* the status is returned: clear a non-sticky error */            \
             return TN_ERR_CUDA;                                                                          \
         }                                                                                                \
     } while ( 0 )
@@ -58,10 +59,36 @@ struct MeshView
 {
     int      N;      // cells per side
     int      n1;     // nodes per side (N + 1)
-    size_t   ns;     // stored nodes 10 (N+1)^3
+    size_t   ns;     // stored nodes 10 (N+1)^3 (whole shell)
     const T* coords; // [10][n1][n1][3] lateral unit-sphere points
     const T* radii;  // [10][n1]
 };
+
+}  // namespace tn
+
+namespace tn {
+
+// Host-side topology of the whole 10-diamond shell (no device calls): what a
+// mesh of any subset of the diamonds is cut from.
+struct ShellTopology
+{
+    int                    level = 0, N = 0, n1 = 0;
+    std::vector< double >  coords;    // [10][n1][n1][3]
+    std::vector< double >  radii;     // [10][n1]
+    std::vector< uint8_t > lat_owned; // [10][n1][n1], owner = lowest diamond id of a duplicated point
+    // duplicated lateral points, CSR over global lateral indices (d n1 + x) n1 + y,
+    // members ascending (= ascending diamond id), groups ordered by point
+    std::vector< int > offsets, members;
+    std::vector< int > fv_ghost; // finite-volume lateral ghost map of the whole shell
+    double             gram_inv[9] = { 0 };
+};
+
+int shell_topology( int level, double r_min, double r_max, ShellTopology& t );
+
+// The diamonds [d0, d0 + nd) of the shell as a mesh (stored compactly, local
+// diamond index = global - d0); the halo groups kept are those whose copies all
+// lie in the range.  d0 = 0, nd = 10 is the whole shell.
+int mesh_create_diamonds( const ShellTopology& t, double r_min, double r_max, int d0, int nd, tn_mesh** out );
 
 }  // namespace tn
 
@@ -69,12 +96,13 @@ struct MeshView
 struct tn_mesh
 {
     int    level = 0, N = 0, n1 = 0;
+    int    d0 = 0, nd = tn::kDiamonds; // global id of the first stored diamond, number of stored diamonds
     double r_min = 0, r_max = 0;
     size_t ns = 0, nu = 0, nlat = 0;
 
-    std::vector< double > h_coords;    // [10][n1][n1][3]
-    std::vector< double > h_radii;     // [10][n1]
-    std::vector< uint8_t > h_lat_owned; // [10][n1][n1]
+    std::vector< double > h_coords;    // [nd][n1][n1][3]
+    std::vector< double > h_radii;     // [nd][n1]
+    std::vector< uint8_t > h_lat_owned; // [nd][n1][n1]
 
     double*  d_coords   = nullptr;
     double*  d_radii    = nullptr;
@@ -92,7 +120,7 @@ struct tn_mesh
 
     // finite-volume lateral ghost map: entry (d * 4 + side) * N + i gives the
     // (diamond, x, y) FV cell across the face of ghost cell i on side
-    // (x = 0, x = N+1, y = 0, y = N+1) of diamond d
+    // (x = 0, x = N+1, y = 0, y = N+1) of diamond d (whole shell only)
     int* d_fv_ghost = nullptr;
     // per FV cell (with ghosts, fv index): bit n set when face n's geometric normal points into the cell and is
     // flipped (the orientation test against the neighbour's centre), built on first use

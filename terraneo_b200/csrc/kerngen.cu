@@ -51,6 +51,7 @@ template < typename T >
 struct TileParams
 {
     int           N, n1, xtiles, seg_max; // seg_max: longest run of node rows one segment finalises
+    int           nd;                     // stored diamonds
     const double* coords;
     const T*      radii;
     const T*      k;
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__( kThreads, TN_TILE_MINBLOCKS ) kerngen_tile_ke
                                                 ~uintptr_t( 15 ) ); // fill descriptors, 16-byte aligned
     auto slot  = [s_rows]( int y ) { return s_rows + ( ( y + kSlots ) % kSlots ) * ( ( kW + 1 ) * 4 * kLev ); };
 
-    for ( int i = threadIdx.x; i < 10 * n1; i += blockDim.x )
+    for ( int i = threadIdx.x; i < P.nd * n1; i += blockDim.x )
         s_radii[( i / n1 ) * ( ( n1 + 1 ) & ~1 ) + i % n1] = P.radii[i];
 
     const int  lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__( kThreads, TN_TILE_MINBLOCKS ) kerngen_tile_ke
     // CTA finalises rows [g_begin, g_end) of the flattened list, in runs
     // (segments) of at most seg_max consecutive rows of one x tile.
     const long long rows_per_tile = N + 1;
-    const long long total         = (long long) kDiamonds * P.xtiles * rows_per_tile;
+    const long long total         = (long long) P.nd * P.xtiles * rows_per_tile;
     const long long g_begin       = total * blockIdx.x / gridDim.x;
     const long long g_end         = total * ( blockIdx.x + 1 ) / gridDim.x;
 
@@ -467,6 +468,7 @@ struct CellParams
     Ptr3< const T > src;
     Ptr3< T >     dst;
     int           bc_cmb, bc_surf, diag;
+    int           nd; // stored diamonds
 };
 
 template < typename T >
@@ -665,7 +667,7 @@ __global__ void __launch_bounds__( 128 ) kerngen_cell_kernel( CellParams< T > P 
 {
     const int       N = P.N, n1 = P.n1;
     const long long t = blockIdx.x * (long long) blockDim.x + threadIdx.x;
-    if ( t >= (long long) kDiamonds * N * N * N )
+    if ( t >= (long long) P.nd * N * N * N )
         return;
     const int r = int( t % N );
     const int y = int( ( t / N ) % N );
@@ -702,7 +704,7 @@ template < typename T >
 __global__ void __launch_bounds__( 128, TN_BCELL_MINBLOCKS ) kerngen_bcell_kernel( CellParams< T > P, int sides )
 {
     const int       N = P.N, n1 = P.n1;
-    const long long per = (long long) kDiamonds * N * N;
+    const long long per = (long long) P.nd * N * N;
     const long long t   = blockIdx.x * (long long) blockDim.x + threadIdx.x;
     if ( t >= per * ( sides == 3 ? 2 : 1 ) )
         return;
@@ -846,8 +848,8 @@ template < typename T >
 CellParams< T > cell_params( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k, Ptr3< const T > src,
                              Ptr3< T > dst )
 {
-    return CellParams< T >{ m->N, m->n1, m->d_coords, mesh_radii< T >( m ), k, src, dst, p->bc_cmb, p->bc_surface,
-                            p->diagonal };
+    return CellParams< T >{
+        m->N, m->n1, m->d_coords, mesh_radii< T >( m ), k, src, dst, p->bc_cmb, p->bc_surface, p->diagonal, m->nd };
 }
 
 }  // namespace
@@ -884,7 +886,7 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
         if ( p->apply_mode == TN_APPLY_REPLACE )
             for ( int c = 0; c < 3; ++c )
                 TN_CUDA_TRY( cudaMemsetAsync( dst[c], 0, m->ns * sizeof( T ), st ) );
-        const long long cells = (long long) kDiamonds * N * N * N;
+        const long long cells = (long long) m->nd * N * N * N;
         kerngen_cell_kernel< T ><<< unsigned( ( cells + 127 ) / 128 ), 128, 0, st >>>( cell_params( m, p, k, s, o ) );
         TN_LAUNCH_CHECK();
         if ( fsfs )
@@ -905,13 +907,14 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
             TN_CUDA_TRY( cudaDeviceGetAttribute( &num_sms, cudaDevAttrMultiProcessorCount, dev ) );
         }
         const int       xtiles = N / kTS;
-        const long long items  = (long long) kDiamonds * xtiles * ( N + 1 );
+        const long long items  = (long long) m->nd * xtiles * ( N + 1 );
         const int       grid   = int( std::min< long long >( (long long) num_sms * TN_TILE_MINBLOCKS, items ) );
         const int       seg    = int( std::min< long long >( kSegMax, ( items + grid - 1 ) / grid ) );
         TileParams< T > P{ N,
                            m->n1,
                            xtiles,
                            seg,
+                           m->nd,
                            m->d_coords,
                            mesh_radii< T >( m ),
                            k,
@@ -934,7 +937,7 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
         if ( skip_cmb || skip_surf )
         {
             const int       sides   = skip_cmb && skip_surf ? 3 : ( skip_cmb ? 1 : 2 );
-            const long long cells = (long long) kDiamonds * N * N * ( sides == 3 ? 2 : 1 );
+            const long long cells = (long long) m->nd * N * N * ( sides == 3 ? 2 : 1 );
             kerngen_bcell_kernel< T ><<< unsigned( ( cells + 127 ) / 128 ), 128, 0, st >>>( cell_params( m, p, k, s, o ),
                                                                                             sides );
             TN_LAUNCH_CHECK();
@@ -944,6 +947,11 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
         return halo_sum< T >( m, dst, 3, st );
     return TN_OK;
 }
+
+template int epsdivdiv_apply< double >( const tn_mesh*, const tn_epsdivdiv_params*, const double*, const double* const*,
+                                        double* const*, cudaStream_t );
+template int epsdivdiv_apply< float >( const tn_mesh*, const tn_epsdivdiv_params*, const float*, const float* const*,
+                                       float* const*, cudaStream_t );
 
 // dst += eps sum_i (m_i^T src) m_i, the fs/fs rigid-rotation penalty on every
 // stored node (no halo), in two parts for the stored-matrix apply: the dots

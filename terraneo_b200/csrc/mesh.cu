@@ -98,11 +98,13 @@ void diamond_lateral_points( int diamond, int N, double* out /* [n1][n1][3] */ )
     }
 }
 
+// a device copy of n host values (an empty array still gets a one-element allocation)
 template < typename T >
 int upload( const T* h, size_t n, T** d )
 {
-    TN_CUDA_TRY( cudaMalloc( d, n * sizeof( T ) ) );
-    TN_CUDA_TRY( cudaMemcpy( *d, h, n * sizeof( T ), cudaMemcpyHostToDevice ) );
+    TN_CUDA_TRY( cudaMalloc( d, std::max< size_t >( n, 1 ) * sizeof( T ) ) );
+    if ( n )
+        TN_CUDA_TRY( cudaMemcpy( *d, h, n * sizeof( T ), cudaMemcpyHostToDevice ) );
     return TN_OK;
 }
 
@@ -161,58 +163,54 @@ using namespace tn;
 
 extern "C" const char* tn_last_error( void ) { return tn::g_last_error.c_str(); }
 
-extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** out )
+namespace tn {
+
+int shell_topology( int level, double r_min, double r_max, ShellTopology& t )
 {
-    TN_CHECK_ARG( out, "tn_mesh_create: out is NULL" );
-    *out = nullptr;
     TN_CHECK_ARG( level >= 1 && level <= 9, "tn_mesh_create: level must be in [1, 9]" );
     TN_CHECK_ARG( r_min < r_max, "tn_mesh_create: r_min must be strictly less than r_max" );
-    tn_mesh* m = new tn_mesh();
-    m->level = level, m->N = 1 << level, m->n1 = m->N + 1;
-    m->r_min = r_min, m->r_max = r_max;
-    const int n1 = m->n1, N = m->N;
-    m->nlat = size_t( kDiamonds ) * n1 * n1;
-    m->ns   = m->nlat * n1;
-    m->nu   = ( size_t( 10 ) * N * N + 2 ) * n1;
+    t.level = level, t.N = 1 << level, t.n1 = t.N + 1;
+    const int    n1 = t.n1, N = t.N;
+    const size_t nlat = size_t( kDiamonds ) * n1 * n1;
 
-    m->h_coords.resize( m->nlat * 3 );
+    t.coords.resize( nlat * 3 );
     for ( int d = 0; d < kDiamonds; ++d )
-        diamond_lateral_points( d, N, m->h_coords.data() + size_t( d ) * n1 * n1 * 3 );
-    m->h_radii.resize( size_t( kDiamonds ) * n1 );
+        diamond_lateral_points( d, N, t.coords.data() + size_t( d ) * n1 * n1 * 3 );
+    t.radii.resize( size_t( kDiamonds ) * n1 );
     const double step = ( r_max - r_min ) / N;
     for ( int d = 0; d < kDiamonds; ++d )
     {
         for ( int i = 0; i <= N; ++i )
-            m->h_radii[d * n1 + i] = r_min + i * step;
-        m->h_radii[d * n1 + N] = r_max;
+            t.radii[d * n1 + i] = r_min + i * step;
+        t.radii[d * n1 + N] = r_max;
     }
 
     // Duplicates: identical lateral points in different diamonds (the bisection
     // reproduces shared edges bit for bit).  Owner = lowest diamond id.
     std::map< std::array< uint64_t, 3 >, std::vector< int > > by_point;
-    for ( size_t l = 0; l < m->nlat; ++l )
+    for ( size_t l = 0; l < nlat; ++l )
     {
         std::array< uint64_t, 3 > key;
-        std::memcpy( key.data(), &m->h_coords[l * 3], 24 );
+        std::memcpy( key.data(), &t.coords[l * 3], 24 );
         by_point[key].push_back( int( l ) );
     }
-    m->h_lat_owned.assign( m->nlat, 0 );
-    std::vector< int > offsets{ 0 }, members;
+    t.lat_owned.assign( nlat, 0 );
+    t.offsets.assign( 1, 0 );
+    t.members.clear();
     for ( auto& kv : by_point )
     {
         auto& v = kv.second; // lateral indices, ascending = ascending diamond id
-        m->h_lat_owned[v[0]] = 1;
+        t.lat_owned[v[0]] = 1;
         if ( v.size() > 1 )
         {
-            members.insert( members.end(), v.begin(), v.end() );
-            offsets.push_back( int( members.size() ) );
+            t.members.insert( t.members.end(), v.begin(), v.end() );
+            t.offsets.push_back( int( t.members.size() ) );
         }
     }
-    m->n_halo_groups = int( offsets.size() ) - 1;
 
     // FV ghost map: every lateral boundary face of a diamond is shared with
     // exactly one other diamond; both sides hold its two edge nodes bit for bit
-    std::vector< int > fv_ghost( size_t( kDiamonds ) * 4 * N * 3, -1 );
+    t.fv_ghost.assign( size_t( kDiamonds ) * 4 * N * 3, -1 );
     {
         using Key = std::array< uint64_t, 6 >;
         std::map< Key, std::vector< std::array< int, 3 > > > edges; // (diamond, side, i)
@@ -224,8 +222,8 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
         };
         auto key_of = [&]( int d, int ax, int ay, int bx, int by ) {
             std::array< uint64_t, 3 > ka, kb;
-            std::memcpy( ka.data(), &m->h_coords[( ( size_t( d ) * n1 + ax ) * n1 + ay ) * 3], 24 );
-            std::memcpy( kb.data(), &m->h_coords[( ( size_t( d ) * n1 + bx ) * n1 + by ) * 3], 24 );
+            std::memcpy( ka.data(), &t.coords[( ( size_t( d ) * n1 + ax ) * n1 + ay ) * 3], 24 );
+            std::memcpy( kb.data(), &t.coords[( ( size_t( d ) * n1 + bx ) * n1 + by ) * 3], 24 );
             if ( kb < ka )
                 std::swap( ka, kb );
             return Key{ ka[0], ka[1], ka[2], kb[0], kb[1], kb[2] };
@@ -243,7 +241,6 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
             if ( kv.second.size() != 2 )
             {
                 set_error( "tn_mesh_create: a diamond boundary edge is not shared by exactly two diamonds" );
-                tn_mesh_destroy( m );
                 return TN_ERR_STATE;
             }
             for ( int k = 0; k < 2; ++k )
@@ -260,7 +257,7 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
                     x = ot[2] + 1, y = 1;
                 else
                     x = ot[2] + 1, y = N;
-                int* e = &fv_ghost[( size_t( me[0] * 4 + me[1] ) * N + me[2] ) * 3];
+                int* e = &t.fv_ghost[( size_t( me[0] * 4 + me[1] ) * N + me[2] ) * 3];
                 e[0] = ot[0], e[1] = x, e[2] = y;
             }
         }
@@ -269,15 +266,15 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
     // Gram matrix of the rigid rotations e_j x x over owned nodes, inverted:
     // the orthonormalised penalty modes m = C (e_j x x) satisfy C^T C = Gram^{-1}.
     double Gm[3][3] = { { 0 } };
-    for ( size_t l = 0; l < m->nlat; ++l )
+    for ( size_t l = 0; l < nlat; ++l )
     {
-        if ( !m->h_lat_owned[l] )
+        if ( !t.lat_owned[l] )
             continue;
         const int d = int( l / ( size_t( n1 ) * n1 ) );
         for ( int r = 0; r < n1; ++r )
         {
-            const double rr = m->h_radii[d * n1 + r];
-            const double x[3] = { m->h_coords[l * 3] * rr, m->h_coords[l * 3 + 1] * rr, m->h_coords[l * 3 + 2] * rr };
+            const double rr = t.radii[d * n1 + r];
+            const double x[3] = { t.coords[l * 3] * rr, t.coords[l * 3 + 1] * rr, t.coords[l * 3 + 2] * rr };
             const double x2   = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
             for ( int i = 0; i < 3; ++i )
                 for ( int j = 0; j < 3; ++j )
@@ -290,8 +287,47 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
         const double c11 = a * f - c * c, c12 = b * c - a * e, c22 = a * d - b * b;
         const double det = a * c00 + b * c01 + c * c02;
         const double inv[9] = { c00 / det, c01 / det, c02 / det, c01 / det, c11 / det, c12 / det, c02 / det, c12 / det, c22 / det };
-        std::memcpy( m->penalty_gram_inv, inv, sizeof( inv ) );
+        std::memcpy( t.gram_inv, inv, sizeof( inv ) );
     }
+    return TN_OK;
+}
+
+int mesh_create_diamonds( const ShellTopology& t, double r_min, double r_max, int d0, int nd, tn_mesh** out )
+{
+    TN_CHECK_ARG( d0 >= 0 && nd >= 1 && d0 + nd <= kDiamonds, "mesh_create_diamonds: bad diamond range" );
+    tn_mesh* m = new tn_mesh();
+    m->level = t.level, m->N = t.N, m->n1 = t.n1;
+    m->d0 = d0, m->nd = nd;
+    m->r_min = r_min, m->r_max = r_max;
+    const int    n1 = m->n1;
+    const size_t per = size_t( n1 ) * n1, lat0 = size_t( d0 ) * per;
+    m->nlat = size_t( nd ) * per;
+    m->ns   = m->nlat * n1;
+
+    m->h_coords.assign( t.coords.begin() + lat0 * 3, t.coords.begin() + ( lat0 + m->nlat ) * 3 );
+    m->h_radii.assign( t.radii.begin() + size_t( d0 ) * n1, t.radii.begin() + size_t( d0 + nd ) * n1 );
+    m->h_lat_owned.assign( t.lat_owned.begin() + lat0, t.lat_owned.begin() + lat0 + m->nlat );
+    size_t owned = 0;
+    for ( uint8_t o : m->h_lat_owned )
+        owned += o;
+    m->nu = owned * n1; // (10 N^2 + 2) n1 for the whole shell
+
+    // the duplicate groups whose copies all lie in the range, as local lateral indices
+    std::vector< int > offsets{ 0 }, members;
+    const int          lo = int( lat0 ), hi = int( lat0 + m->nlat );
+    for ( size_t g = 0; g + 1 < t.offsets.size(); ++g )
+    {
+        bool inside = true;
+        for ( int k = t.offsets[g]; k < t.offsets[g + 1]; ++k )
+            inside = inside && t.members[k] >= lo && t.members[k] < hi;
+        if ( !inside )
+            continue;
+        for ( int k = t.offsets[g]; k < t.offsets[g + 1]; ++k )
+            members.push_back( t.members[k] - lo );
+        offsets.push_back( int( members.size() ) );
+    }
+    m->n_halo_groups = int( offsets.size() ) - 1;
+    std::memcpy( m->penalty_gram_inv, t.gram_inv, sizeof( t.gram_inv ) );
 
     std::vector< int > lat_group( m->nlat, -1 );
     for ( int g = 0; g + 1 < int( offsets.size() ); ++g )
@@ -310,8 +346,8 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
          ( rc = upload( m->h_lat_owned.data(), m->h_lat_owned.size(), &m->d_lat_owned ) ) ||
          ( rc = upload( node_owned.data(), node_owned.size(), &m->d_node_owned ) ) ||
          ( rc = upload( offsets.data(), offsets.size(), &m->d_halo_offsets ) ) ||
-         ( rc = upload( fv_ghost.data(), fv_ghost.size(), &m->d_fv_ghost ) ) ||
-         ( rc = upload( members.data(), std::max< size_t >( members.size(), 1 ), &m->d_halo_members ) ) ||
+         ( nd == kDiamonds && ( rc = upload( t.fv_ghost.data(), t.fv_ghost.size(), &m->d_fv_ghost ) ) ) ||
+         ( rc = upload( members.data(), members.size(), &m->d_halo_members ) ) ||
          ( rc = upload( lat_group.data(), lat_group.size(), &m->d_lat_group ) ) )
     {
         tn_mesh_destroy( m );
@@ -332,6 +368,18 @@ extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** 
     }
     *out = m;
     return TN_OK;
+}
+
+}  // namespace tn
+
+extern "C" int tn_mesh_create( int level, double r_min, double r_max, tn_mesh** out )
+{
+    TN_CHECK_ARG( out, "tn_mesh_create: out is NULL" );
+    *out = nullptr;
+    ShellTopology t;
+    if ( const int rc = shell_topology( level, r_min, r_max, t ) )
+        return rc;
+    return mesh_create_diamonds( t, r_min, r_max, 0, kDiamonds, out );
 }
 
 extern "C" int tn_mesh_destroy( tn_mesh* m )

@@ -1,0 +1,216 @@
+"""The shell sharded over the ranks of a torch.distributed process group: one process per GPU, each holding the
+diamonds the reference's rank map gives it (DistributedDomain::create_uniform with subdomain refinement level 0 and
+subdomain_to_rank_iterate_diamond_subdomains, grid/shell/spherical_shell.hpp:717-745,2566-2590).
+
+The operator kernels run on the shard's diamonds unchanged; the additive halo of an apply
+(communication/shell/communication.hpp:242-747) is the shard-local halo kernel plus, for the nodes with copies on
+two or more ranks, tn_shard_pack -> an all-reduce (SUM) of the exchange buffer over the process group (NCCL over
+NVLink / NVSwitch on GPUs) -> tn_shard_unpack.  Dot products are the owned-node parts of every rank, all-reduced.
+
+Vectors are CUDA tensors of shape (ncomp, diamonds, N+1, N+1, N+1), the component-major layout of the library.
+"""
+import ctypes
+
+import numpy as np
+import torch
+import torch.distributed as dist
+
+from . import _capi as C
+
+
+def partition(num_ranks, rank):
+    """(first diamond, number of diamonds) of `rank` among `num_ranks` (host only)."""
+    f, n = ctypes.c_int(), ctypes.c_int()
+    C.check(C.lib().tn_shell_partition(num_ranks, rank, ctypes.byref(f), ctypes.byref(n)), "tn_shell_partition")
+    return f.value, n.value
+
+
+def halo_plan(level, num_ranks, rank, cross):
+    """The rank's local (cross False) or cross-rank (cross True) duplicate groups as CSR arrays over local lateral
+    indices (host only): (offsets int32[groups + 1], members int32[copies])."""
+    L = C.lib()
+    g, m = ctypes.c_int(), ctypes.c_int()
+    C.check(L.tn_shard_halo_plan(level, num_ranks, rank, int(cross), ctypes.byref(g), ctypes.byref(m), None, None),
+            "tn_shard_halo_plan")
+    off = np.zeros(g.value + 1, np.int32)
+    mem = np.zeros(max(m.value, 1), np.int32)
+    C.check(L.tn_shard_halo_plan(level, num_ranks, rank, int(cross), ctypes.byref(g), ctypes.byref(m),
+                                 off.ctypes.data_as(ctypes.c_void_p), mem.ctypes.data_as(ctypes.c_void_p)),
+            "tn_shard_halo_plan")
+    return off, mem[:m.value]
+
+
+def _comp_ptrs(t):
+    return C.ptrs(*[t[c].data_ptr() for c in range(t.shape[0])])
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class ShellShard:
+    """One rank's diamonds of the level-`level` shell on the current CUDA device (tn_shard)."""
+
+    def __init__(self, level, num_ranks, rank, r_min=0.55, r_max=1.0):
+        L = C.lib()
+        self.level, self.num_ranks, self.rank = level, num_ranks, rank
+        self.N, self.n1 = 1 << level, (1 << level) + 1
+        self.r_min, self.r_max = r_min, r_max
+        h = ctypes.c_void_p()
+        C.check(L.tn_shard_create(level, r_min, r_max, num_ranks, rank, ctypes.byref(h)), "tn_shard_create")
+        self.handle = h
+        f, n = ctypes.c_int(), ctypes.c_int()
+        st, ow, ex = c_size(), c_size(), c_size()
+        C.check(L.tn_shard_dims(h, ctypes.byref(f), ctypes.byref(n), ctypes.byref(st), ctypes.byref(ow),
+                                ctypes.byref(ex)), "tn_shard_dims")
+        self.first_diamond, self.num_diamonds = f.value, n.value
+        self.stored_nodes, self.owned_nodes, self.exchange_values = st.value, ow.value, ex.value
+        self.shape = (self.num_diamonds, self.n1, self.n1, self.n1)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            C.lib().tn_shard_destroy(h)
+            self.handle = None
+
+    def geometry(self):
+        coords = np.zeros((self.num_diamonds, self.n1, self.n1, 3))
+        radii = np.zeros((self.num_diamonds, self.n1))
+        C.check(C.lib().tn_shard_geometry(self.handle, coords.ctypes.data_as(ctypes.c_void_p),
+                                          radii.ctypes.data_as(ctypes.c_void_p)), "tn_shard_geometry")
+        return coords, radii
+
+    def masks(self):
+        b = np.zeros(self.shape, np.uint8)
+        o = np.zeros(self.shape, np.uint8)
+        C.check(C.lib().tn_shard_masks(self.handle, b.ctypes.data_as(ctypes.c_void_p),
+                                       o.ctypes.data_as(ctypes.c_void_p)), "tn_shard_masks")
+        return b, o
+
+    def vector(self, ncomp=3, dtype=torch.float64):
+        return torch.zeros((ncomp,) + self.shape, dtype=dtype, device="cuda")
+
+    def exchange_buffer(self, ncomp, dtype=torch.float64):
+        return torch.zeros(ncomp * self.exchange_values, dtype=dtype, device="cuda")
+
+    def epsdivdiv_apply(self, k, src, dst, bc_cmb, bc_surface, diagonal=False, apply_mode=C.APPLY_REPLACE,
+                        comm_mode=C.COMM_ADDITIVE, penalty_eps=1.0):
+        """The kerngen apply on this rank's cells; with COMM_ADDITIVE the copies on this rank are summed (the
+        cross-rank copies by pack / all-reduce / unpack)."""
+        f64 = src.dtype == torch.float64
+        p = C.EpsDivDivParams(bc_cmb, bc_surface, int(diagonal), apply_mode, comm_mode, penalty_eps)
+        fn = C.lib().tn_shard_epsdivdiv_apply_f64 if f64 else C.lib().tn_shard_epsdivdiv_apply_f32
+        C.check(fn(self.handle, ctypes.byref(p), ctypes.c_void_p(k.data_ptr()), _comp_ptrs(src), _comp_ptrs(dst),
+                   _stream()), "tn_shard_epsdivdiv_apply")
+
+    def pack(self, fields, buf):
+        fn = C.lib().tn_shard_pack_f64 if fields.dtype == torch.float64 else C.lib().tn_shard_pack_f32
+        C.check(fn(self.handle, _comp_ptrs(fields), fields.shape[0], ctypes.c_void_p(buf.data_ptr()), _stream()),
+                "tn_shard_pack")
+
+    def unpack(self, buf, fields):
+        fn = C.lib().tn_shard_unpack_f64 if fields.dtype == torch.float64 else C.lib().tn_shard_unpack_f32
+        C.check(fn(self.handle, ctypes.c_void_p(buf.data_ptr()), _comp_ptrs(fields), fields.shape[0], _stream()),
+                "tn_shard_unpack")
+
+    def local_dot(self, a, b):
+        r = ctypes.c_double()
+        C.check(C.lib().tn_shard_vec_dot_f64(self.handle, a.shape[0], _comp_ptrs(a), _comp_ptrs(b), ctypes.byref(r),
+                                             _stream()), "tn_shard_vec_dot_f64")
+        return r.value
+
+    def lincomb(self, y, c0, coeffs, xs):
+        """y = c0 + sum_i coeffs[i] xs[i] (up to three inputs, FP64)."""
+        c = (ctypes.c_double * 3)(*list(coeffs) + [0.0] * (3 - len(coeffs)))
+        x = (ctypes.c_void_p * 9)()  # three pointer slots per input vector
+        for i, v in enumerate(xs):
+            for cpt in range(v.shape[0]):
+                x[3 * i + cpt] = v[cpt].data_ptr()
+        C.check(C.lib().tn_shard_vec_lincomb_f64(self.handle, y.shape[0], _comp_ptrs(y), c0, len(xs), c, x,
+                                                 _stream()), "tn_shard_vec_lincomb_f64")
+
+
+def c_size():
+    return ctypes.c_size_t()
+
+
+class DistributedShell:
+    """The level-`level` shell over the ranks of a process group (the default group when None): this process's
+    shard, the exchange and the global dot.  Without an initialised process group it is the whole shell on one
+    rank.  With the NCCL backend the all-reduces run on the GPUs over NVLink; with gloo they stage through the
+    host."""
+
+    def __init__(self, level, r_min=0.55, r_max=1.0, group=None):
+        self.group = group
+        if dist.is_available() and dist.is_initialized():
+            self.world, self.rank = dist.get_world_size(group), dist.get_rank(group)
+            self.backend = dist.get_backend(group)
+        else:
+            self.world, self.rank, self.backend = 1, 0, None
+        self.shard = ShellShard(level, self.world, self.rank, r_min, r_max)
+        self._bufs = {}
+
+    def _all_reduce(self, t):
+        if self.world == 1:
+            return t
+        if self.backend == "nccl" or t.device.type == "cpu":
+            dist.all_reduce(t, group=self.group)
+            return t
+        h = t.cpu()  # gloo on CUDA tensors: through the host
+        dist.all_reduce(h, group=self.group)
+        t.copy_(h)
+        return t
+
+    def exchange(self, fields):
+        """Sum the copies of the nodes shared with other ranks (the cross-rank part of the additive halo)."""
+        key = (fields.shape[0], fields.dtype)
+        buf = self._bufs.get(key)
+        if buf is None:
+            buf = self._bufs[key] = self.shard.exchange_buffer(fields.shape[0], fields.dtype)
+        if buf.numel() == 0 and self.world == 1:
+            return
+        self.shard.pack(fields, buf)
+        self._all_reduce(buf)
+        self.shard.unpack(buf, fields)
+
+    def epsdivdiv_apply(self, k, src, dst, bc_cmb, bc_surface, diagonal=False, apply_mode=C.APPLY_REPLACE):
+        """EpsilonDivDivKerngen apply with the additive halo over all ranks (every copy of a node holds the sum)."""
+        self.shard.epsdivdiv_apply(k, src, dst, bc_cmb, bc_surface, diagonal, apply_mode, C.COMM_ADDITIVE)
+        self.exchange(dst)
+
+    def dot(self, a, b):
+        """Global owned-node dot product (every rank returns the same value)."""
+        part = self.shard.local_dot(a, b)
+        if self.world == 1:
+            return part
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([part], dtype=torch.float64, device=dev)
+        self._all_reduce(t)
+        return float(t.item())
+
+    def cg(self, k, b, x, bc_cmb=C.BC_DIRICHLET, bc_surface=C.BC_DIRICHLET, max_iterations=500,
+           relative_tolerance=1e-10, absolute_tolerance=0.0):
+        """Unpreconditioned CG on the kerngen operator over all ranks (the reference's PCG, linalg/solvers/pcg.hpp:
+        78-160, with the identity preconditioner): b and x are consistent vectors (every copy of a node equal).
+        Returns (iterations, relative residual)."""
+        sh = self.shard
+        r, p, ap = sh.vector(3), sh.vector(3), sh.vector(3)
+        self.epsdivdiv_apply(k, x, ap, bc_cmb, bc_surface)
+        sh.lincomb(r, 0.0, [1.0, -1.0], [b, ap])
+        rr = self.dot(r, r)
+        r0 = rr ** 0.5
+        if r0 <= absolute_tolerance or r0 == 0.0:
+            return 0, 0.0
+        p.copy_(r)
+        for it in range(1, max_iterations + 1):
+            self.epsdivdiv_apply(k, p, ap, bc_cmb, bc_surface)
+            alpha = rr / self.dot(p, ap)
+            sh.lincomb(x, 0.0, [1.0, alpha], [x, p])
+            sh.lincomb(r, 0.0, [1.0, -alpha], [r, ap])
+            rr_new = self.dot(r, r)
+            res = rr_new ** 0.5
+            if res / r0 <= relative_tolerance or res <= absolute_tolerance:
+                return it, res / r0
+            sh.lincomb(p, 0.0, [1.0, rr_new / rr], [r, p])
+            rr = rr_new
+        return max_iterations, res / r0

@@ -15,6 +15,7 @@ Usage (in a container that has the reference sources and a built ref_dump):
     python tests/golden/make_golden.py --agca        # adds the adaptive-GCA cases (level 3) to ref_L2.npz
     python tests/golden/make_golden.py --stokes-mg-inputs  # stokes_mg_L4_inputs.npz: the free-slip inputs of
                                                            # ref_stokes_mg_L4.npz for a reader without the oracle
+    python tests/golden/make_golden.py --shard       # shard_L2.npz: the reference run as rank q of P
 """
 import os
 import sys
@@ -519,6 +520,55 @@ def make_xdmf():
             shutil.copyfile(f"{d}/xdmf/{f}", os.path.join(XDMF_DIR, f))
 
 
+# The distributed domain as rank q of P (subdomain refinement level 0, the reference's default rank map): the
+# diamonds of every rank for P = 1..10, and the copy-wise (SkipCommunication) kerngen apply of the ranks of
+# SHARD_APPLY_P with the boundary conditions SHARD_BCS on the seeded inputs of shard_inputs.
+SHARD_L = 2
+SHARD_APPLY_P = (3, 8)
+SHARD_BCS = [(1, 2), (2, 0)]
+
+
+def shard_inputs(fine):
+    """seeded positive k and a source, both consistent on duplicated nodes"""
+    rs = np.random.RandomState(123)
+    k = fine.make_consistent(np.exp(rs.normal(size=fine.shape))).reshape(fine.shape)
+    src = np.stack([fine.make_consistent(rs.normal(size=fine.shape)).reshape(fine.shape) for _ in range(3)])
+    return k, src
+
+
+def make_shard():
+    """shard_L2.npz: diamonds_P<P>_q<q> (the reference's local subdomains, in local order) and
+    dst_<bcc><bcs>_P<P>_q<q> (the rank's copy-wise apply), plus the inputs' checksums"""
+    fine = Mesh(SHARD_L)
+    k, src = shard_inputs(fine)
+    out = {"checksum_k": checksum(k), "checksum_src": checksum(src)}
+    with tempfile.TemporaryDirectory() as d:
+        for P in range(1, 11):
+            first = 0
+            for q in range(P):
+                # the rank's diamonds are not known before the run: a first run reads the leading entries of the
+                # whole shell's fields and reports them; the apply runs again on the rank's own slices
+                k.tofile(f"{d}/k.bin")
+                src.tofile(f"{d}/src.bin")
+                info = run_ref(["kerngen_rank", SHARD_L, R_MIN, R_MAX, 1, 2, P, q, d], d, json_out=True)
+                dia = np.array(info["diamonds"], np.int32)
+                out[f"diamonds_P{P}_q{q}"] = dia
+                assert dia[0] == first and np.all(np.diff(dia) == 1), dia
+                first = dia[-1] + 1
+                if P not in SHARD_APPLY_P:
+                    continue
+                sl = slice(int(dia[0]), int(dia[-1]) + 1)
+                k[sl].tofile(f"{d}/k.bin")
+                np.ascontiguousarray(src[:, sl]).tofile(f"{d}/src.bin")
+                for bcc, bcs in SHARD_BCS:
+                    run_ref(["kerngen_rank", SHARD_L, R_MIN, R_MAX, bcc, bcs, P, q, d], d)
+                    out[f"dst_{bcc}{bcs}_P{P}_q{q}"] = np.fromfile(f"{d}/dst.bin").reshape((3, len(dia)) + fine.shape[1:])
+            assert first == 10
+    path = os.path.join(HERE, "shard_L2.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
     if "--stokes-mg" in sys.argv and "--stokes-mg-inputs" not in sys.argv:
         make_stokes_mg()
@@ -530,5 +580,7 @@ if __name__ == "__main__":
         make_agca()
     elif "--stokes-mg-inputs" in sys.argv:
         make_stokes_mg_inputs()
+    elif "--shard" in sys.argv:
+        make_shard()
     else:
         main()

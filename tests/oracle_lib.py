@@ -33,6 +33,7 @@ def lib():
         L.or_ownership_mask.argtypes = [ctypes.c_int, _D, _U8]
         L.or_halo_sum.argtypes = [ctypes.c_int, _D, _D, ctypes.c_int]
         L.or_kerngen_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.or_kerngen_apply_copywise.argtypes = L.or_kerngen_apply.argtypes
         L.or_laplace_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
         L.or_divergence_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
         L.or_gradient_apply.argtypes = [ctypes.c_int, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
@@ -105,12 +106,13 @@ class Mesh:
         om = np.tile(self.omask.reshape(-1), ncomp).reshape(f.shape)
         return self.halo_sum(np.where(om == 1, f, 0.0))
 
-    def kerngen(self, k, src, bc_cmb, bc_surf, diag=False):
+    def kerngen(self, k, src, bc_cmb, bc_surf, diag=False, halo=True):
+        """halo=False: the copy-wise result (no additive halo), every diamond's copy holding its own cells' sum"""
         dst = np.zeros((3,) + self.shape)
         k = np.ascontiguousarray(k, dtype=np.float64)
         src = np.ascontiguousarray(src, dtype=np.float64)
-        lib().or_kerngen_apply(self.L, _p(self.coords), _p(self.radii), _p(k), _p(src), _p(dst),
-                               bc_cmb, bc_surf, int(diag))
+        fn = lib().or_kerngen_apply if halo else lib().or_kerngen_apply_copywise
+        fn(self.L, _p(self.coords), _p(self.radii), _p(k), _p(src), _p(dst), bc_cmb, bc_surf, int(diag))
         return dst
 
     def laplace(self, src, treat_boundary=True, diag=False):

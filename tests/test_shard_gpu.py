@@ -1,0 +1,201 @@
+"""The sharded shell on the GPU: tn_shard_* through terraneo_b200.distributed.
+
+Several ranks are emulated in one process on one GPU, one after another, never waiting on one another: every
+rank's shard applies the operator and packs its exchange buffer, the buffers are summed (what the all-reduce over
+the ranks' GPUs does), every shard unpacks.  The result is compared with the oracle's whole-shell apply (pinned to
+the reference), with the whole-shell GPU apply at the benchmark size, and, copy-wise, with the reference's own
+applies as rank q of P (tests/golden/shard_L2.npz).  The torch.distributed path is run as a one-rank NCCL group.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import rel
+from oracle_lib import Mesh
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+import make_golden as G  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "shard_L2.npz")
+
+
+def _dev(a, dtype):
+    return torch.tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+def _emulated_apply(level, P, k, src, bcc, bcs, diag=False, dtype=torch.float64):
+    from terraneo_b200.distributed import ShellShard
+    shards = [ShellShard(level, P, q) for q in range(P)]
+    outs, bufs = [], []
+    for sh in shards:
+        f, n = sh.first_diamond, sh.num_diamonds
+        d = sh.vector(3, dtype)
+        sh.epsdivdiv_apply(_dev(k[f:f + n], dtype), _dev(src[:, f:f + n], dtype), d, bcc, bcs, diag)
+        b = sh.exchange_buffer(3, dtype)
+        sh.pack(d, b)
+        outs.append(d), bufs.append(b)
+    total = torch.stack(bufs).sum(dim=0)  # the all-reduce over the ranks
+    for sh, d in zip(shards, outs):
+        sh.unpack(total, d)
+    torch.cuda.synchronize()
+    return shards, [d.double().cpu().numpy() for d in outs]
+
+
+def _inputs(om):
+    k, src = G.shard_inputs(om)
+    return k, src
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4, 8, 10])
+def test_shard_geometry_masks_and_ownership(P):
+    from terraneo_b200.distributed import ShellShard
+    om = Mesh(3)
+    owned = 0
+    for q in range(P):
+        sh = ShellShard(3, P, q)
+        f, n = sh.first_diamond, sh.num_diamonds
+        coords, radii = sh.geometry()
+        assert np.array_equal(coords, om.coords[f:f + n]) and np.array_equal(radii, om.radii[f:f + n])
+        b, o = sh.masks()
+        assert np.array_equal(b, om.bmask[f:f + n]) and np.array_equal(o, om.omask[f:f + n])
+        assert sh.owned_nodes == int(o.sum())
+        owned += sh.owned_nodes
+    assert owned == (10 * om.N ** 2 + 2) * om.n1
+
+
+@pytest.mark.parametrize("level", [2, 3, 4])
+@pytest.mark.parametrize("P", [1, 2, 3, 4, 8, 10])
+def test_sharded_apply_matches_oracle(level, P):
+    om = Mesh(level)
+    k, src = _inputs(om)
+    for bcc, bcs, diag in ((1, 1, 0), (1, 2, 0), (2, 0, 0), (0, 0, 0), (2, 1, 0), (1, 1, 1), (2, 2, 1)):
+        want = om.kerngen(k, src, bcc, bcs, bool(diag))
+        _, outs = _emulated_apply(level, P, k, src, bcc, bcs, bool(diag))
+        for q, d in enumerate(outs):
+            from terraneo_b200.distributed import partition
+            f, n = partition(P, q)
+            assert rel(d, want[:, f:f + n]) <= 1e-12, (bcc, bcs, diag, q)
+
+
+@pytest.mark.parametrize("P", [2, 5])
+def test_sharded_apply_fp32(P):
+    from terraneo_b200.distributed import partition
+    om = Mesh(4)
+    k, src = _inputs(om)
+    want = om.kerngen(k, src, 1, 2)
+    _, outs = _emulated_apply(4, P, k, src, 1, 2, dtype=torch.float32)
+    for q, d in enumerate(outs):
+        f, n = partition(P, q)
+        assert rel(d, want[:, f:f + n]) <= 2e-5, q
+
+
+def test_copywise_shard_apply_matches_reference_rank_applies():
+    from terraneo_b200 import _capi as C
+    from terraneo_b200.distributed import ShellShard
+    g = np.load(GOLDEN)
+    om = Mesh(G.SHARD_L)
+    k, src = G.shard_inputs(om)
+    for bcc, bcs in G.SHARD_BCS:
+        for P in G.SHARD_APPLY_P:
+            for q in range(P):
+                sh = ShellShard(G.SHARD_L, P, q)
+                f, n = sh.first_diamond, sh.num_diamonds
+                d = sh.vector(3)
+                sh.epsdivdiv_apply(_dev(k[f:f + n], torch.float64), _dev(src[:, f:f + n], torch.float64), d, bcc,
+                                   bcs, comm_mode=C.COMM_SKIP)
+                assert rel(d.cpu().numpy(), g[f"dst_{bcc}{bcs}_P{P}_q{q}"]) <= 1e-12, (bcc, bcs, P, q)
+
+
+@pytest.mark.parametrize("P", [2, 8])
+def test_sharded_apply_at_level6_matches_whole_shell_gpu_apply(P):
+    """the benchmark size: the emulated ranks against the whole-shell apply of the same kernels (only the order in
+    which the copies of a shared node are summed differs)"""
+    from terraneo_b200 import shell
+    from terraneo_b200.distributed import partition
+    L = 6
+    pm = shell.ShellMesh(L)
+    rs = np.random.RandomState(5)
+    k = np.exp(rs.uniform(0, np.log(1e4), size=pm.shape))  # a 1e4 viscosity contrast
+    src = rs.normal(size=(3,) + pm.shape)
+    kv = shell.VectorQ1Scalar(pm)
+    kv.set_numpy(k)
+    u, v = shell.VectorQ1Vec(pm), shell.VectorQ1Vec(pm)
+    u.set_numpy(src)
+    for bcc, bcs in ((1, 1), (2, 1)):
+        op = shell.EpsilonDivDivKerngen(pm, kv, bcc, bcs)
+        shell.apply(op, u, v)
+        want = v.numpy()
+        _, outs = _emulated_apply(L, P, k, src, bcc, bcs)
+        for q, d in enumerate(outs):
+            f, n = partition(P, q)
+            assert rel(d, want[:, f:f + n]) <= 1e-13, (bcc, bcs, q)
+
+
+def test_freeslip_both_radii_refused_on_two_ranks():
+    from terraneo_b200 import _capi as C
+    from terraneo_b200.distributed import ShellShard
+    sh = ShellShard(3, 2, 0)
+    d = sh.vector(3)
+    with pytest.raises(C.TNError):
+        sh.epsdivdiv_apply(torch.ones(sh.shape, dtype=torch.float64, device="cuda"), sh.vector(3), d, 2, 2)
+
+
+def test_distributed_shell_single_rank_dot_and_cg():
+    """without a process group the shell is one rank: the dot is the owned-node dot and CG on the Dirichlet
+    operator reaches its tolerance with the oracle's true residual"""
+    from terraneo_b200.distributed import DistributedShell
+    L = 3
+    om = Mesh(L)
+    k, src = _inputs(om)
+    ds = DistributedShell(L)
+    assert ds.world == 1 and ds.shard.num_diamonds == 10
+    a, b = _dev(src, torch.float64), _dev(src[::-1].copy(), torch.float64)
+    assert abs(ds.dot(a, b) - om.dot(src, src[::-1])) <= 1e-12 * abs(om.dot(src, src[::-1]))
+    kd = _dev(k, torch.float64)
+    x = ds.shard.vector(3)
+    its, rr = ds.cg(kd, a, x, max_iterations=400, relative_tolerance=1e-10)
+    xs = x.cpu().numpy()
+    res = om.kerngen(k, xs, 1, 1) - src
+    assert np.sqrt(om.dot(res, res)) <= 1e-9 * np.sqrt(om.dot(src, src)), (its, rr)
+
+
+_NCCL_ONE_RANK = r"""
+import os, socket, sys, datetime
+sys.path.insert(0, sys.argv[1]); sys.path.insert(0, os.path.join(sys.argv[1], "tests"))
+sys.path.insert(0, os.path.join(sys.argv[1], "tests", "golden"))
+import numpy as np, torch, torch.distributed as dist
+with socket.socket() as s:
+    s.bind(("127.0.0.1", 0)); port = s.getsockname()[1]
+os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+torch.cuda.set_device(0)
+dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+try:
+    import make_golden as G
+    from oracle_lib import Mesh
+    from terraneo_b200.distributed import DistributedShell
+    om = Mesh(3)
+    k, src = G.shard_inputs(om)
+    ds = DistributedShell(3)
+    assert ds.world == 1 and ds.backend == "nccl"
+    kd = torch.tensor(k, device="cuda"); s = torch.tensor(src, device="cuda"); d = ds.shard.vector(3)
+    ds.epsdivdiv_apply(kd, s, d, 1, 2)
+    want = om.kerngen(k, src, 1, 2)
+    err = np.abs(d.cpu().numpy() - want).max() / np.abs(want).max()
+    dd = ds.dot(s, s)
+    print("RESULT", err, abs(dd - om.dot(src, src)) / om.dot(src, src))
+finally:
+    dist.destroy_process_group()
+"""
+
+
+def test_distributed_shell_in_a_one_rank_nccl_group():
+    out = subprocess.run([sys.executable, "-c", _NCCL_ONE_RANK, ROOT], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = [ln for ln in out.stdout.splitlines() if ln.startswith("RESULT")][-1].split()
+    assert float(line[1]) <= 1e-12 and float(line[2]) <= 1e-12, line
