@@ -197,11 +197,40 @@ def _case_fct7(shell, C, torch):
     return _fct_case(shell, torch, 7)
 
 
+def _case_shard7(shell, C, torch):
+    """The sharded apply on one GPU: rank 0's shard (the largest) of the level-7 shell split over P = 1, 2, 4, 8
+    ranks, FP64 Dirichlet apply with the shard-local halo, then pack and unpack of the cross-rank exchange buffer
+    (the all-reduce between the GPUs is not part of a one-GPU run)"""
+    from terraneo_b200.distributed import ShellShard
+    out = {}
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    for P in (1, 2, 4, 8):
+        sh = ShellShard(7, P, 0, RMIN, RMAX)
+        k = torch.empty(sh.shape, dtype=torch.float64, device="cuda").uniform_(0.0, 9.2, generator=gen).exp_()
+        u, v = sh.vector(3), sh.vector(3)
+        u.uniform_(-1, 1, generator=gen)
+        buf = sh.exchange_buffer(3)
+        tag = (f"P={P}, rank 0: {sh.num_diamonds} diamonds, {3 * sh.stored_nodes:,} DoFs stored, exchange "
+               f"{buf.numel() * 8:,} bytes")
+
+        def apply_exchange(sh=sh, k=k, u=u, v=v, buf=buf):
+            sh.epsdivdiv_apply(k, u, v, C.BC_DIRICHLET, C.BC_DIRICHLET)
+            sh.pack(v, buf)
+            sh.unpack(buf, v)
+
+        def exchange_only(sh=sh, v=v, buf=buf):
+            sh.pack(v, buf)
+            sh.unpack(buf, v)
+        out[f"shard apply + pack + unpack, level 7, {tag}"] = apply_exchange
+        out[f"pack + unpack only, level 7, P={P}"] = exchange_only
+    return out
+
+
 # name -> builder returning {description: one launch sequence}
 CASES = {"laplace6": _case_laplace6, "vlaplace6": _case_vlaplace6, "divkgrad6": _case_divkgrad6,
          "stokes_b6": _case_stokes_b6, "stored5": _case_stored5, "kerngen6_fs": _case_kerngen6_fs,
          "stokes6": _case_stokes6, "stokes6_refine": _case_stokes6_refine, "coarse_pcg3": _case_coarse_pcg3,
-         "fct6": _case_fct6, "fct7": _case_fct7}
+         "fct6": _case_fct6, "fct7": _case_fct7, "shard7": _case_shard7}
 
 
 def run_case(args):

@@ -509,8 +509,9 @@ __global__ void assign_boundary_kernel( size_t nlat, int n1, Ptr3< T > y, Ptr3< 
     if ( ( side == 0 && !cmb ) || ( side == 1 && !surf ) )
         return;
     const size_t i = ( t % nlat ) * n1 + ( side == 0 ? 0 : n1 - 1 );
-    const int    k = blockIdx.y;
-    y.p[k][i]      = x.p[k] ? x.p[k][i] : c;
+    const int    k  = blockIdx.y;
+    const T*     xs = x.at( k );
+    y.at( k )[i]    = xs ? xs[i] : c;
 }
 
 template < typename T >
@@ -660,8 +661,8 @@ __global__ void dot_noalloc_kernel( size_t n, int ncomp, Ptr3< const double > a,
     Neumaier acc;
     for ( int c = 0; c < ncomp; ++c )
     {
-        const double* __restrict__ pa = a.p[c];
-        const double* __restrict__ pb = b.p[c];
+        const double* __restrict__ pa = a.at( c );
+        const double* __restrict__ pb = b.at( c );
         for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < n; i += size_t( gridDim.x ) * blockDim.x )
         {
             const double v = pa[i] * pb[i];
