@@ -154,6 +154,26 @@ def _case_stokes6_refine(shell, C, torch):
     return {"Stokes solve, level 6 free-slip, refinement form, 30 FGMRES(100) iterations": run}
 
 
+def _case_stokes6_fp64(shell, C, torch):
+    """30 FGMRES iterations of the level-6 free-slip Stokes solve in the plain FP64 form (FP64 multigrid)"""
+    pf, pc = shell.ShellMesh(6, RMIN, RMAX), shell.ShellMesh(5, RMIN, RMAX)
+    coords, radii = pf.geometry()
+    k_np, _ = synthetic_inputs(coords, radii, None)
+    kv = shell.VectorQ1Scalar(pf)
+    kv.set_numpy(k_np)
+    fu, fp = stokes_rhs(shell, pf, coords, radii), shell.VectorQ1Scalar(pc)
+    s = shell.StokesSolver(6, kv, mg_levels=4, bc_cmb=C.BC_FREESLIP, bc_surface=C.BC_FREESLIP, mg_fp32=False,
+                           chebyshev_order=3, relative_tolerance=1e-30, max_iterations=30, restart=100,
+                           r_min=RMIN, r_max=RMAX, gca=1)
+    xu, xp = shell.VectorQ1Vec(pf), shell.VectorQ1Scalar(pc)
+
+    def run():
+        xu.data.zero_()
+        xp.data.zero_()
+        s.solve(fu, fp, xu, xp)
+    return {"Stokes solve, level 6 free-slip, FP64 multigrid, 30 FGMRES(100) iterations": run}
+
+
 def _case_coarse_pcg3(shell, C, torch):
     """The coarsest-level solve of the C3 V-cycle: 50 iterations of the stored-matrix PCG at level 3,
     free-slip both radii, matrices coarsened (GCA, constant interpolation) from the level-4 kerngen matrices"""
@@ -229,8 +249,31 @@ def _case_shard7(shell, C, torch):
 # name -> builder returning {description: one launch sequence}
 CASES = {"laplace6": _case_laplace6, "vlaplace6": _case_vlaplace6, "divkgrad6": _case_divkgrad6,
          "stokes_b6": _case_stokes_b6, "stored5": _case_stored5, "kerngen6_fs": _case_kerngen6_fs,
-         "stokes6": _case_stokes6, "stokes6_refine": _case_stokes6_refine, "coarse_pcg3": _case_coarse_pcg3,
+         "stokes6": _case_stokes6, "stokes6_refine": _case_stokes6_refine, "stokes6_fp64": _case_stokes6_fp64,
+         "coarse_pcg3": _case_coarse_pcg3,
          "fct6": _case_fct6, "fct7": _case_fct7, "shard7": _case_shard7}
+
+
+def kernel_breakdown(fn, torch, top=30):
+    """One more call of fn under the CUDA activity trace (torch.profiler): per kernel name the device
+    microseconds and launches of that call, largest first.  Kernels that run concurrently on two streams each
+    count their whole duration, so the sum can exceed the call's elapsed time."""
+    import re
+    from torch.profiler import profile, ProfilerActivity
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    rows = {}
+    for e in prof.key_averages():
+        if e.device_time_total <= 0:
+            continue
+        k = re.sub(r"\(anonymous namespace\)::|tn::|void ", "", e.key)
+        k = re.sub(r"\(.*", "", k)[:80]
+        t, c = rows.get(k, (0.0, 0))
+        rows[k] = (t + e.device_time_total, c + e.count)
+    out = sorted(rows.items(), key=lambda kv: -kv[1][0])[:top]
+    return [{"kernel": k, "us": round(t, 1), "launches": c} for k, (t, c) in out]
 
 
 def run_case(args):
@@ -252,6 +295,8 @@ def run_case(args):
         ev1.record()
         torch.cuda.synchronize()
         res[name] = {"ms_per_call": round(ev0.elapsed_time(ev1) / args.steps, 5)}
+        if args.kernel_breakdown:
+            res[name]["kernels"] = kernel_breakdown(fn, torch)
     print(json.dumps({"case": args.case, "steps": args.steps, "warmup": args.warmup, "results": res}), flush=True)
     return 0
 
@@ -269,6 +314,8 @@ def parse():
     ap.add_argument("--no-timestep", action="store_true", help="skip the level-7 mantle-circulation time-step leg")
     ap.add_argument("--no-level8", action="store_true", help="skip the level-8 apply (the published configuration)")
     ap.add_argument("--case", choices=sorted(CASES), help="time one operator workload (see CASES) instead of the bench")
+    ap.add_argument("--kernel-breakdown", action="store_true",
+                    help="with --case: also report one call's device time per kernel (CUDA activity trace)")
     return ap.parse_args()
 
 
