@@ -744,9 +744,11 @@ struct Mat3
 
 // <m_j, u> over owned nodes for the three rotation modes m_j = e_j x x:
 // sum over owned lateral columns of c_lat x (sum_r rad_r u(lat, r)), c the
-// unit lateral position.  One warp per column (lanes along r, coalesced),
-// FP64 sums per lane, the column's radial sum reduced with shuffles and
-// crossed with c once; compensated sums across warps and blocks.
+// unit lateral position.  One warp per column (lanes along r, coalesced);
+// the cross product is linear, so every lane crosses its own part of the
+// column's radial sum and keeps accumulating across columns in FP64, and the
+// lanes are combined once, in the compensated block / grid reduction.  Indices
+// are 32-bit (nlat < 2^32 at every level).
 template < typename T >
 __global__ void __launch_bounds__( 256 ) penalty_dots_kernel( size_t nlat, int n1, const double* __restrict__ coords,
                                                               const T* __restrict__ radii, Ptr3< const T > src,
@@ -754,39 +756,31 @@ __global__ void __launch_bounds__( 256 ) penalty_dots_kernel( size_t nlat, int n
                                                               unsigned int* counter, double* result, double eps,
                                                               Mat3 ginv )
 {
-    const int    lane  = threadIdx.x & 31;
-    const size_t warp  = ( blockIdx.x * size_t( blockDim.x ) + threadIdx.x ) >> 5;
-    const size_t warps = ( size_t( gridDim.x ) * blockDim.x ) >> 5;
-    double       sum[3] = { 0.0, 0.0, 0.0 };
-    for ( size_t lat = warp; lat < nlat; lat += warps )
+    const int      lane  = threadIdx.x & 31;
+    const unsigned warp  = ( blockIdx.x * blockDim.x + threadIdx.x ) >> 5;
+    const unsigned warps = ( gridDim.x * blockDim.x ) >> 5;
+    const unsigned per   = unsigned( n1 ) * unsigned( n1 ), nl = unsigned( nlat );
+    const T *      s0 = src.at( 0 ), *s1 = src.at( 1 ), *s2 = src.at( 2 );
+    double         sum[3] = { 0.0, 0.0, 0.0 };
+    for ( unsigned lat = warp; lat < nl; lat += warps )
     {
         if ( !lat_owned[lat] )
             continue;
-        const int  d  = int( lat / ( size_t( n1 ) * n1 ) );
-        const T*   rd = radii + size_t( d ) * n1;
-        double     v0 = 0.0, v1 = 0.0, v2 = 0.0;
+        const T*       rd   = radii + ( lat / per ) * unsigned( n1 );
+        const unsigned base = lat * unsigned( n1 );
+        double         v0 = 0.0, v1 = 0.0, v2 = 0.0;
         for ( int r = lane; r < n1; r += 32 )
         {
-            const size_t i   = lat * n1 + r;
             const double rad = double( rd[r] );
-            v0 += rad * double( src.p[0][i] );
-            v1 += rad * double( src.p[1][i] );
-            v2 += rad * double( src.p[2][i] );
+            v0 += rad * double( s0[base + r] );
+            v1 += rad * double( s1[base + r] );
+            v2 += rad * double( s2[base + r] );
         }
-#pragma unroll
-        for ( int off = 16; off > 0; off >>= 1 )
-        {
-            v0 += __shfl_xor_sync( 0xffffffffu, v0, off );
-            v1 += __shfl_xor_sync( 0xffffffffu, v1, off );
-            v2 += __shfl_xor_sync( 0xffffffffu, v2, off );
-        }
-        if ( lane == 0 )
-        {
-            const double* c = coords + lat * 3;
-            sum[0] += c[1] * v2 - c[2] * v1;
-            sum[1] += c[2] * v0 - c[0] * v2;
-            sum[2] += c[0] * v1 - c[1] * v0;
-        }
+        const double* c = coords + size_t( lat ) * 3;
+        const double  c0 = c[0], c1 = c[1], c2 = c[2];
+        sum[0] += c1 * v2 - c2 * v1;
+        sum[1] += c2 * v0 - c0 * v2;
+        sum[2] += c0 * v1 - c1 * v0;
     }
     Neumaier acc[3];
     for ( int k = 0; k < 3; ++k )

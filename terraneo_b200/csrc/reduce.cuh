@@ -76,16 +76,38 @@ __device__ bool block_sum_finish( Neumaier* acc, double* partials, unsigned int*
     if ( !is_last )
         return false;
     __threadfence();
+    // each thread merges the partials of blocks tid, tid + blockDim, ... in that order; the loads of J of them
+    // (all K sums) are issued before their merges, so the L2 round trips overlap (a merge of the zero padding past
+    // the last block leaves a sum unchanged)
+    constexpr int J = K == 1 ? 4 : 2;
+    Neumaier      t[K];
+    for ( unsigned b0 = threadIdx.x; b0 < gridDim.x; b0 += J * blockDim.x )
+    {
+        double vs[J][K], vc[J][K];
+#pragma unroll
+        for ( int j = 0; j < J; ++j )
+        {
+            const unsigned b  = b0 + j * blockDim.x;
+            const bool     in = b < gridDim.x;
+#pragma unroll
+            for ( int k = 0; k < K; ++k )
+            {
+                vs[j][k] = in ? __ldcg( &partials[( size_t( b ) * K + k ) * 2] ) : 0.0;
+                vc[j][k] = in ? __ldcg( &partials[( size_t( b ) * K + k ) * 2 + 1] ) : 0.0;
+            }
+        }
+#pragma unroll
+        for ( int j = 0; j < J; ++j )
+#pragma unroll
+            for ( int k = 0; k < K; ++k )
+                t[k].merge( Neumaier{ vs[j][k], vc[j][k] } );
+    }
 #pragma unroll
     for ( int k = 0; k < K; ++k )
     {
-        Neumaier t;
-        for ( unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x )
-            t.merge( Neumaier{ __ldcg( &partials[( size_t( b ) * K + k ) * 2] ),
-                               __ldcg( &partials[( size_t( b ) * K + k ) * 2 + 1] ) } );
-        t = warp_reduce( t );
+        const Neumaier w = warp_reduce( t[k] );
         if ( lane == 0 )
-            sh_s[warp][k] = t.s, sh_c[warp][k] = t.c;
+            sh_s[warp][k] = w.s, sh_c[warp][k] = w.c;
     }
     __syncthreads();
     if ( threadIdx.x == 0 )
