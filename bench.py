@@ -35,9 +35,9 @@ METRIC = "L6 Stokes time-to-1e-8 (FP32-MG+FP64 refine vs FP64); apply GDoF/s, %H
 LEVEL, RMIN, RMAX = 6, 0.55, 1.0
 BYTES_PER_NODE_F64 = 56  # 3 src + 1 k + 3 dst doubles per stored node
 BYTES_PER_NODE_F32 = 28
-# DRAM bytes (read + write) of one level-6 kerngen_tile_kernel<double> launch,
+# DRAM bytes (read + write) of one level-6 kerngen_tile_kernel<double, 16> launch,
 # from an ncu capture (profiles/kerngen_tile_kernel_f64_L6_dirichlet.md)
-TILE_TRAFFIC_BYTES = 135726080 + 49133312
+TILE_TRAFFIC_BYTES = 141040384 + 48047360
 
 
 def _case_laplace6(shell, C, torch):
@@ -1210,9 +1210,9 @@ def main():
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": TILE_TRAFFIC_BYTES,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                           "kerngen_tile_kernel<double> launch at level 6 (Dirichlet apply; "
+                                           "kerngen_tile_kernel<double, 16> launch at level 6 (Dirichlet apply; "
                                            "profiles/kerngen_tile_kernel_f64_L6_dirichlet.md)",
-                         "kernel": "kerngen_tile_kernel<double>", "kernel_ms": round(kms, 5),
+                         "kernel": "kerngen_tile_kernel<double, 16>", "kernel_ms": round(kms, 5),
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
             "fp32_apply": {"value": round(whole_job_gdofs(world, dofs, ms32), 3), "unit": "GDoF/s",

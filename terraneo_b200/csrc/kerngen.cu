@@ -38,14 +38,25 @@ int halo_sum( const tn_mesh* m, T* const* fields, int nfields, cudaStream_t st )
 
 namespace {
 
-constexpr int kTS      = 8;       // owned node columns per x tile
-constexpr int kW       = kTS + 1; // warps = cell strips per CTA
-constexpr int kThreads = kW * 32;
-constexpr int kRC      = 32;      // radial cells per chunk (one per lane)
-#ifndef TN_TILE_MINBLOCKS
-#define TN_TILE_MINBLOCKS 2 // resident CTAs per SM the tiled kernel is compiled for
-#endif
-constexpr int kSegMax  = 24;      // longest run of node rows a CTA finalises in one y march
+constexpr int kRC     = 32; // radial cells per chunk (one per lane)
+constexpr int kSegMax = 24; // longest run of node rows a CTA finalises in one y march
+constexpr int kLev    = kRC + 1; // node levels per chunk
+constexpr int kSlots  = 4;       // row ring depth (prefetch distance 3)
+
+// The shape of the tiled kernel for x tiles of TS owned node columns: TS + 1
+// warps (cell strips) per CTA, so a tile recomputes one strip of cells its
+// neighbour also computes (1/TS of the work); 16 columns where N allows it
+// (one 544-thread CTA per SM), 8 at N = 8 (two 288-thread CTAs per SM).
+template < int TS >
+struct Tile
+{
+    static constexpr int W         = TS + 1;        // warps = cell strips per CTA
+    static constexpr int Threads   = W * 32;
+    static constexpr int MinBlocks = TS == 8 ? 2 : 1; // resident CTAs per SM the kernel is compiled for
+    static constexpr int Group     = Threads / 4;   // fill threads per field
+    static constexpr int FieldEl   = ( W + 1 ) * kLev;
+    static constexpr int FillPer   = ( FieldEl + Group - 1 ) / Group;
+};
 
 template < typename T >
 struct TileParams
@@ -105,12 +116,10 @@ __device__ __forceinline__ void wedge_flux( const T* __restrict__ g, const T v1[
 // into a 4-slot shared-memory ring with cp.async three rows ahead (fill_row),
 // so global latency overlaps the arithmetic of the previous steps.  The radial chunk
 // boundary level r0 + 32 is carried to the next chunk in shared memory.
-constexpr int kLev   = kRC + 1; // node levels per chunk
-constexpr int kSlots = 4;       // row ring depth (prefetch distance 3)
-
-template < typename T >
+template < typename T, int TS >
 size_t tile_smem_bytes( int n1, int SY )
 {
+    constexpr int kW = Tile< TS >::W, kThreads = Tile< TS >::Threads;
     const size_t radii = size_t( 10 ) * ( ( n1 + 1 ) & ~1 );
     const size_t geo   = size_t( kW ) * ( SY + 2 ) * 20;
     const size_t rows  = size_t( kSlots ) * ( kW + 1 ) * 4 * kLev;
@@ -122,7 +131,7 @@ size_t tile_smem_bytes( int n1, int SY )
 
 // Row fill.  A ring slot holds one node row of the CTA's kW+1 columns, stored
 // [field][column][level] (fields: 3 src components, k).  The threads form 4
-// groups of kThreads / 4, one per field; a thread copies elements t, t + 72,
+// groups of kThreads / 4, one per field; a thread copies elements t, t + group,
 // ... of its field's (kW+1) x kLev block, each a fixed (column, level) whose
 // 32-bit element offset advances by one node row (n1) per step, so a fill costs
 // one offset add and one 8-byte cp.async per element.  The offsets of the
@@ -130,12 +139,10 @@ size_t tile_smem_bytes( int n1, int SY )
 // no registers across the wedge arithmetic.  Columns outside the diamond and
 // levels past the chunk are not copied; rows outside the diamond not at all
 // (no contributing cell reads them).
-constexpr int kGroup   = kThreads / 4;
-constexpr int kFieldEl = ( kW + 1 ) * kLev;
-constexpr int kFillPer = ( kFieldEl + kGroup - 1 ) / kGroup;
-
+template < int TS >
 __device__ __forceinline__ void fill_setup( uint4* desc, int N, int n1, int d, int X0, int Y0, int r0, int RC )
 {
+    constexpr int kGroup = Tile< TS >::Group, kFieldEl = Tile< TS >::FieldEl, kFillPer = Tile< TS >::FillPer;
     static_assert( kFillPer == 5, "descriptor layout" );
     const int t = threadIdx.x % kGroup;
     unsigned  off[kFillPer], valid = 0;
@@ -154,10 +161,11 @@ __device__ __forceinline__ void fill_setup( uint4* desc, int N, int n1, int d, i
 }
 
 // node row Y = Y0 + step into `slot`
-template < typename T >
+template < int TS, typename T >
 __device__ __forceinline__ void fill_row( const uint4* desc, const T* f0, const T* f1, const T* f2, const T* f3, T* slot,
                                           int step, int Y, int N, int n1 )
 {
+    constexpr int kGroup = Tile< TS >::Group, kFieldEl = Tile< TS >::FieldEl, kFillPer = Tile< TS >::FillPer;
     const int      f = threadIdx.x / kGroup, t = threadIdx.x - f * kGroup;
     const T*       fb = f == 0 ? f0 : ( f == 1 ? f1 : ( f == 2 ? f2 : f3 ) );
     const uint4    a = desc[2 * threadIdx.x], b = desc[2 * threadIdx.x + 1];
@@ -173,9 +181,10 @@ __device__ __forceinline__ void fill_row( const uint4* desc, const T* f0, const 
             __pipeline_memcpy_async( dst + i * kGroup, fb + ( off[i] + adv ), sizeof( T ) );
 }
 
-template < typename T >
-__global__ void __launch_bounds__( kThreads, TN_TILE_MINBLOCKS ) kerngen_tile_kernel( TileParams< T > P )
+template < typename T, int TS >
+__global__ void __launch_bounds__( Tile< TS >::Threads, Tile< TS >::MinBlocks ) kerngen_tile_kernel( TileParams< T > P )
 {
+    constexpr int kTS = TS, kW = Tile< TS >::W, kFieldEl = Tile< TS >::FieldEl;
     extern __shared__ __align__( 16 ) unsigned char smem_raw[];
     constexpr unsigned FULL = 0xffffffffu;
     const int          N = P.N, n1 = P.n1, SM = P.seg_max;
@@ -258,10 +267,10 @@ __global__ void __launch_bounds__( kThreads, TN_TILE_MINBLOCKS ) kerngen_tile_ke
                 lane_ok = false;
 
             const int cyb = row_lo - 1 + s0;
-            fill_setup( s_fill, N, n1, d, sx0, cyb, r0, RC );
+            fill_setup< TS >( s_fill, N, n1, d, sx0, cyb, r0, RC );
             for ( int j = 0; j < kSlots - 1; ++j )
             {
-                fill_row( s_fill, f0, f1, f2, f3, slot( cyb + j ), j, cyb + j, N, n1 );
+                fill_row< TS >( s_fill, f0, f1, f2, f3, slot( cyb + j ), j, cyb + j, N, n1 );
                 __pipeline_commit();
             }
             __pipeline_wait_prior( kSlots - 3 );
@@ -284,7 +293,8 @@ __global__ void __launch_bounds__( kThreads, TN_TILE_MINBLOCKS ) kerngen_tile_ke
                 const bool cell_ok = strip_ok && cy <= N - 1;
                 // row cy + 3 into the slot of row cy - 1, which every warp finished reading before the last
                 // barrier; issued here, where few registers are live
-                fill_row( s_fill, f0, f1, f2, f3, slot( cy + kSlots - 1 ), cy + kSlots - 1 - cyb, cy + kSlots - 1, N, n1 );
+                fill_row< TS >( s_fill, f0, f1, f2, f3, slot( cy + kSlots - 1 ), cy + kSlots - 1 - cyb, cy + kSlots - 1, N,
+                                n1 );
                 T          L[3], R[3];
                 {
                     // corners: 0 = (X, cy), 1 = (X+1, cy), 2 = (X, cy+1), 3 = (X+1, cy+1)
@@ -848,6 +858,50 @@ CellParams< T > cell_params( const tn_mesh* m, const tn_epsdivdiv_params* p, con
 
 }  // namespace
 
+// The tiled kernel over the interior layers (all layers the boundary-cell kernel does not take).
+template < typename T, int TS >
+int tile_launch( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k, Ptr3< const T > s, Ptr3< T > o, bool fsfs,
+                 bool skip_cmb, bool skip_surf, cudaStream_t st )
+{
+    const int  N = m->N;
+    static int num_sms = 0;
+    if ( num_sms == 0 )
+    {
+        int dev = 0;
+        TN_CUDA_TRY( cudaGetDevice( &dev ) );
+        TN_CUDA_TRY( cudaDeviceGetAttribute( &num_sms, cudaDevAttrMultiProcessorCount, dev ) );
+    }
+    const int       xtiles = N / TS;
+    const long long items  = (long long) m->nd * xtiles * ( N + 1 );
+    const int       grid   = int( std::min< long long >( (long long) num_sms * Tile< TS >::MinBlocks, items ) );
+    const int       seg    = int( std::min< long long >( kSegMax, ( items + grid - 1 ) / grid ) );
+    TileParams< T > P{ N,
+                       m->n1,
+                       xtiles,
+                       seg,
+                       m->nd,
+                       m->d_coords,
+                       mesh_radii< T >( m ),
+                       k,
+                       s,
+                       o,
+                       p->apply_mode == TN_APPLY_ADD,
+                       skip_cmb,
+                       skip_surf,
+                       fsfs ? m->d_red_result + 3 : nullptr };
+    const size_t smem      = tile_smem_bytes< T, TS >( m->n1, seg );
+    static int   smem_attr = 0; // largest dynamic shared memory requested so far for this instantiation
+    if ( int( smem ) > smem_attr )
+    {
+        TN_CUDA_TRY( cudaFuncSetAttribute( kerngen_tile_kernel< T, TS >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           int( smem ) ) );
+        smem_attr = int( smem );
+    }
+    kerngen_tile_kernel< T, TS ><<< grid, Tile< TS >::Threads, smem, st >>>( P );
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
 template < typename T >
 int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k, const T* const* src, T* const* dst,
                      cudaStream_t st )
@@ -875,7 +929,7 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
         TN_LAUNCH_CHECK();
     }
 
-    if ( p->diagonal || N < kTS )
+    if ( p->diagonal || N < 8 )
     {
         if ( p->apply_mode == TN_APPLY_REPLACE )
             for ( int c = 0; c < 3; ++c )
@@ -892,42 +946,11 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
     }
     else
     {
-        const bool      skip_cmb = p->bc_cmb != TN_BC_NEUMANN, skip_surf = p->bc_surface != TN_BC_NEUMANN;
-        static int num_sms = 0;
-        if ( num_sms == 0 )
-        {
-            int dev = 0;
-            TN_CUDA_TRY( cudaGetDevice( &dev ) );
-            TN_CUDA_TRY( cudaDeviceGetAttribute( &num_sms, cudaDevAttrMultiProcessorCount, dev ) );
-        }
-        const int       xtiles = N / kTS;
-        const long long items  = (long long) m->nd * xtiles * ( N + 1 );
-        const int       grid   = int( std::min< long long >( (long long) num_sms * TN_TILE_MINBLOCKS, items ) );
-        const int       seg    = int( std::min< long long >( kSegMax, ( items + grid - 1 ) / grid ) );
-        TileParams< T > P{ N,
-                           m->n1,
-                           xtiles,
-                           seg,
-                           m->nd,
-                           m->d_coords,
-                           mesh_radii< T >( m ),
-                           k,
-                           s,
-                           o,
-                           p->apply_mode == TN_APPLY_ADD,
-                           skip_cmb,
-                           skip_surf,
-                           fsfs ? m->d_red_result + 3 : nullptr };
-        const size_t smem = tile_smem_bytes< T >( m->n1, seg );
-        static int smem_attr[2] = { 0, 0 }; // largest dynamic shared memory requested so far (per precision)
-        if ( int( smem ) > smem_attr[sizeof( T ) == 8] )
-        {
-            TN_CUDA_TRY( cudaFuncSetAttribute( kerngen_tile_kernel< T >, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               int( smem ) ) );
-            smem_attr[sizeof( T ) == 8] = int( smem );
-        }
-        kerngen_tile_kernel< T ><<< grid, kThreads, smem, st >>>( P );
-        TN_LAUNCH_CHECK();
+        const bool skip_cmb = p->bc_cmb != TN_BC_NEUMANN, skip_surf = p->bc_surface != TN_BC_NEUMANN;
+        const int  rc       = N >= 16 ? tile_launch< T, 16 >( m, p, k, s, o, fsfs, skip_cmb, skip_surf, st )
+                                      : tile_launch< T, 8 >( m, p, k, s, o, fsfs, skip_cmb, skip_surf, st );
+        if ( rc )
+            return rc;
         if ( skip_cmb || skip_surf )
         {
             const int       sides   = skip_cmb && skip_surf ? 3 : ( skip_cmb ? 1 : 2 );
