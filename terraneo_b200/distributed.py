@@ -69,7 +69,7 @@ class ShellShard:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h is not None and h.value:
+        if h is not None and h.value and C is not None and C._lib is not None:
             C.lib().tn_shard_destroy(h)
             self.handle = None
 
