@@ -15,9 +15,11 @@ step reads data cached by the previous one.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 For N > 1 (torchrun) every rank runs the same apply on its own GPU (replicas:
-the ten diamonds of one level-6 shell fit one GPU, so the apply is not
-sharded), timed with CUDA events, max over ranks; value is the aggregate over
-ranks.
+the ten diamonds of one level-6 shell fit one GPU, so the headline apply is
+not sharded), timed with CUDA events, max over ranks; value is the aggregate
+over ranks. The `sharded` object of the line (always with two or more ranks,
+with --sharded on one) times the level-7 apply with the shell split over the
+ranks by diamond and one all-reduce of the shared copies per apply.
 """
 import argparse
 import json
@@ -314,6 +316,8 @@ def parse():
     ap.add_argument("--no-timestep", action="store_true", help="skip the level-7 mantle-circulation time-step leg")
     ap.add_argument("--no-level8", action="store_true", help="skip the level-8 apply (the published configuration)")
     ap.add_argument("--case", choices=sorted(CASES), help="time one operator workload (see CASES) instead of the bench")
+    ap.add_argument("--sharded", action="store_true",
+                    help="also time the level-7 apply sharded over the ranks (always on with two or more ranks)")
     ap.add_argument("--kernel-breakdown", action="store_true",
                     help="with --case: also report one call's device time per kernel (CUDA activity trace)")
     return ap.parse_args()
@@ -1033,6 +1037,45 @@ def run_reference(args, rank):
     return 0
 
 
+def sharded_leg(C, torch, world, rank, steps, warmup, level=7):
+    """The level-7 EpsilonDivDivKerngen FP64 apply with the shell sharded over the ranks (one process per GPU):
+    every rank applies the operator on the diamonds the reference's rank map gives it, then the copies shared
+    between ranks are summed by one all-reduce of the exchange buffer (NCCL).  Timed with CUDA events on the
+    launching stream, max over ranks; the value is the whole shell's DoFs per second (strong scaling)."""
+    import torch.distributed as dist
+    from terraneo_b200.distributed import DistributedShell, partition
+    ds = DistributedShell(level, RMIN, RMAX)
+    sh = ds.shard
+    gen = torch.Generator(device="cuda").manual_seed(17 + rank)
+    k = torch.empty(sh.shape, dtype=torch.float64, device="cuda").uniform_(0.0, 9.2, generator=gen).exp_()
+    u, v = sh.vector(3), sh.vector(3)
+    u.uniform_(-1, 1, generator=gen)
+
+    def step():
+        ds.epsdivdiv_apply(k, u, v, C.BC_DIRICHLET, C.BC_DIRICHLET)
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / steps, world, "cuda")
+    n1 = (1 << level) + 1
+    dofs = 3 * (10 * (n1 - 1) ** 2 + 2) * n1
+    return {"workload": f"EpsilonDivDivKerngen FP64 apply, level-{level} shell ({dofs:,} velocity DoFs), "
+                        f"Dirichlet/Dirichlet, sharded over {world} rank(s) by diamond, one all-reduce of the "
+                        "cross-rank copies per apply",
+            "value": round(dofs / (ms * 1e-3) / 1e9, 3), "unit": "GDoF/s", "ms_per_apply": round(ms, 5),
+            "scaling": "strong", "ranks": world,
+            "diamonds_per_rank": [partition(world, q)[1] for q in range(world)],
+            "exchange_bytes_per_apply": 3 * sh.exchange_values * 8}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -1198,6 +1241,9 @@ def main():
     # the last results arrived: compare with the serial loop's
     e2e_check = float((h_out[(e2e_steps - 1) % 2] - h_dst).abs().max())
 
+    # every rank takes part in the sharded leg (collectives), before the rank-0-only legs
+    sharded = sharded_leg(C, torch, world, rank, args.steps, args.warmup) if (world > 1 or args.sharded) else None
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
@@ -1238,6 +1284,8 @@ def main():
             line["adjoint"] = adjoint_leg(shell, C, torch)
         if world == 1 and not args.no_level8:
             line["level8"] = level8_leg(shell, C, torch)
+        if sharded is not None:
+            line["sharded"] = sharded
         if world == 1 and not args.no_timestep:
             line["timestep"] = timestep_leg(shell, C, torch)
         if world == 1 and not args.no_cpu_baseline:

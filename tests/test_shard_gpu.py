@@ -199,3 +199,16 @@ def test_distributed_shell_in_a_one_rank_nccl_group():
     assert out.returncode == 0, out.stderr[-2000:]
     line = [ln for ln in out.stdout.splitlines() if ln.startswith("RESULT")][-1].split()
     assert float(line[1]) <= 1e-12 and float(line[2]) <= 1e-12, line
+
+
+def test_bench_sharded_leg_on_one_rank():
+    """bench.py --sharded on one GPU: the leg the bench runs on every rank of a multi-GPU job"""
+    import json
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--steps", "3", "--warmup", "3", "--no-stokes",
+           "--no-cpu-baseline", "--no-laplace-cg", "--no-adjoint", "--no-timestep", "--no-level8", "--sharded"]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=900, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads([ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1])
+    sh = line["sharded"]
+    assert sh["ranks"] == 1 and sh["diamonds_per_rank"] == [10] and sh["exchange_bytes_per_apply"] == 0
+    assert sh["value"] > 1.0 and sh["scaling"] == "strong"
