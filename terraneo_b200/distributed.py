@@ -138,7 +138,7 @@ class DistributedShell:
     """The level-`level` shell over the ranks of a process group (the default group when None): this process's
     shard, the exchange and the global dot.  Without an initialised process group it is the whole shell on one
     rank.  With the NCCL backend the all-reduces run on the GPUs over NVLink; with gloo they stage through the
-    host."""
+    host.  Vectors are the shard's tensors; the solvers below (`cg`) take this object as their domain."""
 
     def __init__(self, level, r_min=0.55, r_max=1.0, group=None):
         self.group = group
@@ -160,6 +160,9 @@ class DistributedShell:
         dist.all_reduce(h, group=self.group)
         t.copy_(h)
         return t
+
+    def vector(self, ncomp=3, dtype=torch.float64):
+        return self.shard.vector(ncomp, dtype)
 
     def exchange(self, fields):
         """Sum the copies of the nodes shared with other ranks (the cross-rank part of the additive halo)."""
@@ -188,29 +191,103 @@ class DistributedShell:
         self._all_reduce(t)
         return float(t.item())
 
+    def lincomb(self, y, c0, coeffs, xs):
+        self.shard.lincomb(y, c0, coeffs, xs)
+
+    def copy(self, dst, src):
+        self.shard.lincomb(dst, 0.0, [1.0], [src])
+
     def cg(self, k, b, x, bc_cmb=C.BC_DIRICHLET, bc_surface=C.BC_DIRICHLET, max_iterations=500,
            relative_tolerance=1e-10, absolute_tolerance=0.0):
-        """Unpreconditioned CG on the kerngen operator over all ranks (the reference's PCG, linalg/solvers/pcg.hpp:
-        78-160, with the identity preconditioner): b and x are consistent vectors (every copy of a node equal).
-        Returns (iterations, relative residual)."""
-        sh = self.shard
-        r, p, ap = sh.vector(3), sh.vector(3), sh.vector(3)
-        self.epsdivdiv_apply(k, x, ap, bc_cmb, bc_surface)
-        sh.lincomb(r, 0.0, [1.0, -1.0], [b, ap])
-        rr = self.dot(r, r)
-        r0 = rr ** 0.5
-        if r0 <= absolute_tolerance or r0 == 0.0:
-            return 0, 0.0
-        p.copy_(r)
-        for it in range(1, max_iterations + 1):
-            self.epsdivdiv_apply(k, p, ap, bc_cmb, bc_surface)
-            alpha = rr / self.dot(p, ap)
-            sh.lincomb(x, 0.0, [1.0, alpha], [x, p])
-            sh.lincomb(r, 0.0, [1.0, -alpha], [r, ap])
-            rr_new = self.dot(r, r)
-            res = rr_new ** 0.5
-            if res / r0 <= relative_tolerance or res <= absolute_tolerance:
-                return it, res / r0
-            sh.lincomb(p, 0.0, [1.0, rr_new / rr], [r, p])
-            rr = rr_new
-        return max_iterations, res / r0
+        return cg(self, k, b, x, bc_cmb, bc_surface, max_iterations, relative_tolerance, absolute_tolerance)
+
+
+class EmulatedShell:
+    """All P ranks of a sharded shell in one process, on the current GPU: the same domain interface as
+    `DistributedShell`, with vectors as lists of the ranks' tensors.  Each operation runs rank after rank, the
+    exchange sums the ranks' buffers (what the all-reduce does across GPUs) and the dot sums their owned parts,
+    so no kernel ever waits on another.  For checking a decomposition (and the solvers over it) on one GPU."""
+
+    def __init__(self, level, num_ranks, r_min=0.55, r_max=1.0):
+        self.world = num_ranks
+        self.shards = [ShellShard(level, num_ranks, q, r_min, r_max) for q in range(num_ranks)]
+        self._bufs = {}
+
+    def vector(self, ncomp=3, dtype=torch.float64):
+        return [sh.vector(ncomp, dtype) for sh in self.shards]
+
+    def scatter(self, whole):
+        """the ranks' parts of a whole-shell array [ncomp][10][...] (numpy or tensor) as a vector"""
+        out = []
+        for sh in self.shards:
+            f, n = sh.first_diamond, sh.num_diamonds
+            part = whole[..., f:f + n, :, :, :]
+            out.append(torch.as_tensor(np.ascontiguousarray(part) if isinstance(part, np.ndarray) else part,
+                                       device="cuda").contiguous())
+        return out
+
+    def gather(self, v):
+        """a vector as one whole-shell numpy array"""
+        return np.concatenate([t.detach().cpu().numpy() for t in v], axis=-4)
+
+    def exchange(self, fields):
+        key = (fields[0].shape[0], fields[0].dtype)
+        bufs = self._bufs.get(key)
+        if bufs is None:
+            bufs = self._bufs[key] = [sh.exchange_buffer(*key) for sh in self.shards]
+        if bufs[0].numel() == 0:
+            return
+        for sh, f, b in zip(self.shards, fields, bufs):
+            sh.pack(f, b)
+        total = bufs[0].clone()
+        for b in bufs[1:]:
+            total += b
+        for sh, f in zip(self.shards, fields):
+            sh.unpack(total, f)
+
+    def epsdivdiv_apply(self, k, src, dst, bc_cmb, bc_surface, diagonal=False, apply_mode=C.APPLY_REPLACE):
+        for sh, kk, s, d in zip(self.shards, k, src, dst):
+            sh.epsdivdiv_apply(kk, s, d, bc_cmb, bc_surface, diagonal, apply_mode, C.COMM_ADDITIVE)
+        self.exchange(dst)
+
+    def dot(self, a, b):
+        return sum(sh.local_dot(x, y) for sh, x, y in zip(self.shards, a, b))
+
+    def lincomb(self, y, c0, coeffs, xs):
+        for q, sh in enumerate(self.shards):
+            sh.lincomb(y[q], c0, coeffs, [x[q] for x in xs])
+
+    def copy(self, dst, src):
+        self.lincomb(dst, 0.0, [1.0], [src])
+
+    def cg(self, k, b, x, bc_cmb=C.BC_DIRICHLET, bc_surface=C.BC_DIRICHLET, max_iterations=500,
+           relative_tolerance=1e-10, absolute_tolerance=0.0):
+        return cg(self, k, b, x, bc_cmb, bc_surface, max_iterations, relative_tolerance, absolute_tolerance)
+
+
+def cg(D, k, b, x, bc_cmb=C.BC_DIRICHLET, bc_surface=C.BC_DIRICHLET, max_iterations=500, relative_tolerance=1e-10,
+       absolute_tolerance=0.0):
+    """Unpreconditioned CG on the kerngen operator over a sharded domain D (`DistributedShell` or `EmulatedShell`):
+    the reference's PCG (linalg/solvers/pcg.hpp:78-160) with the identity preconditioner.  b and x are consistent
+    vectors (every copy of a node equal), k the shard-local viscosity.  Returns (iterations, relative residual)."""
+    r, p, ap = D.vector(3), D.vector(3), D.vector(3)
+    D.epsdivdiv_apply(k, x, ap, bc_cmb, bc_surface)
+    D.lincomb(r, 0.0, [1.0, -1.0], [b, ap])
+    rr = D.dot(r, r)
+    r0 = rr ** 0.5
+    if r0 <= absolute_tolerance or r0 == 0.0:
+        return 0, 0.0
+    D.copy(p, r)
+    res = r0
+    for it in range(1, max_iterations + 1):
+        D.epsdivdiv_apply(k, p, ap, bc_cmb, bc_surface)
+        alpha = rr / D.dot(p, ap)
+        D.lincomb(x, 0.0, [1.0, alpha], [x, p])
+        D.lincomb(r, 0.0, [1.0, -alpha], [r, ap])
+        rr_new = D.dot(r, r)
+        res = rr_new ** 0.5
+        if res / r0 <= relative_tolerance or res <= absolute_tolerance:
+            return it, res / r0
+        D.lincomb(p, 0.0, [1.0, rr_new / rr], [r, p])
+        rr = rr_new
+    return max_iterations, res / r0

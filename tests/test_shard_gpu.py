@@ -212,3 +212,28 @@ def test_bench_sharded_leg_on_one_rank():
     sh = line["sharded"]
     assert sh["ranks"] == 1 and sh["diamonds_per_rank"] == [10] and sh["exchange_bytes_per_apply"] == 0
     assert sh["value"] > 1.0 and sh["scaling"] == "strong"
+
+
+@pytest.mark.parametrize("bc", [(1, 1), (1, 2), (2, 1)])
+def test_emulated_ranks_cg_matches_one_rank(bc):
+    """CG over P = 2, 3, 5, 8 emulated ranks (distributed.EmulatedShell: the ranks one after another on one GPU,
+    the exchange a sum of their buffers) against the one-rank solve: the same iteration count within 2, the
+    solutions within the tolerance, and the oracle's true residual"""
+    from terraneo_b200.distributed import EmulatedShell
+    L = 3
+    om = Mesh(L)
+    k, _ = _inputs(om)
+    rs = np.random.RandomState(40)
+    b = np.stack([om.make_consistent(rs.normal(size=om.shape)).reshape(om.shape) for _ in range(3)])
+    sols, its = {}, {}
+    for P in (1, 2, 3, 5, 8):
+        D = EmulatedShell(L, P)
+        kk, bb, x = D.scatter(k), D.scatter(b), D.vector(3)
+        its[P], rr = D.cg(kk, bb, x, *bc, max_iterations=1000, relative_tolerance=1e-10)
+        assert rr <= 1e-10, (P, its[P], rr)
+        sols[P] = D.gather(x)
+        res = om.kerngen(k, sols[P], *bc) - b
+        assert np.sqrt(om.dot(res, res)) <= 2e-10 * np.sqrt(om.dot(b, b)), P
+    for P in (2, 3, 5, 8):
+        assert abs(its[P] - its[1]) <= 2, its
+        assert rel(sols[P], sols[1]) <= 1e-8, P
