@@ -730,6 +730,22 @@ TN_API int tn_shard_vec_dot_f64( const tn_shard* shard, int ncomp, const double*
                                  double* result, void* stream );
 TN_API int tn_shard_vec_lincomb_f64( const tn_shard* shard, int ncomp, double* const* y, double c0, int nx,
                                      const double* c, const double* const* x, void* stream );
+/* Multigrid on shards (a rank's shards at two levels, the same rank of the same partition):
+ * tn_prolongation_constant_f64, tn_restriction_constant_f64 (its coarse halo sums the copies on this rank; the
+ * cross-rank copies follow with pack / all-reduce / unpack on the coarse shard), tn_injection_f64,
+ * tn_vec_invert_f64, tn_vec_mult_f64 and tn_vec_chebyshev_step_f64 on the shard's nodes. */
+TN_API int tn_shard_prolongation_constant_f64( const tn_shard* fine, const tn_shard* coarse, int ncomp, int apply_mode,
+                                               const double* const* src, double* const* dst, void* stream );
+TN_API int tn_shard_restriction_constant_f64( const tn_shard* fine, const tn_shard* coarse, int ncomp,
+                                              const double* const* src, double* const* dst, void* stream );
+TN_API int tn_shard_injection_f64( const tn_shard* fine, const tn_shard* coarse, int ncomp, const double* const* src,
+                                   double* const* dst, void* stream );
+TN_API int tn_shard_vec_invert_f64( const tn_shard* shard, int ncomp, double* const* y, void* stream );
+TN_API int tn_shard_vec_mult_f64( const tn_shard* shard, int ncomp, double* const* y, const double* const* x,
+                                  void* stream );
+TN_API int tn_shard_vec_chebyshev_step_f64( const tn_shard* shard, int ncomp, double* const* x, double* const* d,
+                                            const double* const* b, const double* const* ax,
+                                            const double* const* inv_diag, double alpha, double beta, void* stream );
 
 #ifdef __cplusplus
 }

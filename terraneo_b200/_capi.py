@@ -210,6 +210,14 @@ _SIGS = {
     "tn_shard_vec_dot_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_double), c_void_p]),
     "tn_shard_vec_lincomb_f64": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p),
                                          c_void_p]),
+    "tn_shard_prolongation_constant_f64": (c_int, [c_void_p, c_void_p, c_int, c_int, P(c_void_p), P(c_void_p),
+                                                   c_void_p]),
+    "tn_shard_restriction_constant_f64": (c_int, [c_void_p, c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_shard_injection_f64": (c_int, [c_void_p, c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_shard_vec_invert_f64": (c_int, [c_void_p, c_int, P(c_void_p), c_void_p]),
+    "tn_shard_vec_mult_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), c_void_p]),
+    "tn_shard_vec_chebyshev_step_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_void_p), P(c_void_p),
+                                                P(c_void_p), c_double, c_double, c_void_p]),
 }
 
 

@@ -27,6 +27,10 @@ namespace tn {
 
 template < typename T >
 int epsdivdiv_apply( const tn_mesh*, const tn_epsdivdiv_params*, const T*, const T* const*, T* const*, cudaStream_t );
+template < typename T >
+int prolong_constant( const tn_mesh*, const tn_mesh*, int, int, const T* const*, T* const*, cudaStream_t );
+template < typename T >
+int restrict_constant( const tn_mesh*, const tn_mesh*, int, int, const T* const*, T* const*, cudaStream_t );
 
 namespace {
 
@@ -335,4 +339,64 @@ extern "C" int tn_shard_vec_lincomb_f64( const tn_shard* s, int ncomp, double* c
 {
     TN_CHECK_ARG( s, "tn_shard_vec_lincomb_f64: shard is NULL" );
     return tn_vec_lincomb_f64( s->mesh, ncomp, y, c0, nx, c, x, st );
+}
+
+// ---------------------------------------------------------------------------
+// Multigrid on shards: every level's shard holds the same diamonds (the rank map does not depend on the level), so
+// the transfers stay within the rank; the restriction's coarse halo covers the rank's own copies and the caller
+// completes it with the coarse shard's exchange, as after an apply.
+
+static int same_ranks( const tn_shard* f, const tn_shard* c )
+{
+    TN_CHECK_ARG( f && c, "shard transfer: null shard" );
+    TN_CHECK_ARG( f->num_ranks == c->num_ranks && f->rank == c->rank,
+                  "shard transfer: the shards must belong to the same rank of the same partition" );
+    return TN_OK;
+}
+
+extern "C" int tn_shard_prolongation_constant_f64( const tn_shard* fine, const tn_shard* coarse, int ncomp,
+                                                   int apply_mode, const double* const* src, double* const* dst,
+                                                   void* st )
+{
+    if ( const int rc = same_ranks( fine, coarse ) )
+        return rc;
+    TN_CHECK_ARG( src && dst, "tn_shard_prolongation_constant_f64: null argument" );
+    return prolong_constant< double >( fine->mesh, coarse->mesh, ncomp, apply_mode, src, dst, as_stream( st ) );
+}
+
+extern "C" int tn_shard_restriction_constant_f64( const tn_shard* fine, const tn_shard* coarse, int ncomp,
+                                                  const double* const* src, double* const* dst, void* st )
+{
+    if ( const int rc = same_ranks( fine, coarse ) )
+        return rc;
+    TN_CHECK_ARG( src && dst, "tn_shard_restriction_constant_f64: null argument" );
+    return restrict_constant< double >( fine->mesh, coarse->mesh, ncomp, TN_APPLY_REPLACE, src, dst, as_stream( st ) );
+}
+
+extern "C" int tn_shard_injection_f64( const tn_shard* fine, const tn_shard* coarse, int ncomp, const double* const* src,
+                                       double* const* dst, void* st )
+{
+    if ( const int rc = same_ranks( fine, coarse ) )
+        return rc;
+    return tn_injection_f64( fine->mesh, coarse->mesh, ncomp, src, dst, st );
+}
+
+extern "C" int tn_shard_vec_invert_f64( const tn_shard* s, int ncomp, double* const* y, void* st )
+{
+    TN_CHECK_ARG( s, "tn_shard_vec_invert_f64: shard is NULL" );
+    return tn_vec_invert_f64( s->mesh, ncomp, y, st );
+}
+
+extern "C" int tn_shard_vec_chebyshev_step_f64( const tn_shard* s, int ncomp, double* const* x, double* const* d,
+                                                const double* const* b, const double* const* ax,
+                                                const double* const* inv_diag, double alpha, double beta, void* st )
+{
+    TN_CHECK_ARG( s, "tn_shard_vec_chebyshev_step_f64: shard is NULL" );
+    return tn_vec_chebyshev_step_f64( s->mesh, ncomp, x, d, b, ax, inv_diag, alpha, beta, st );
+}
+
+extern "C" int tn_shard_vec_mult_f64( const tn_shard* s, int ncomp, double* const* y, const double* const* x, void* st )
+{
+    TN_CHECK_ARG( s, "tn_shard_vec_mult_f64: shard is NULL" );
+    return tn_vec_mult_f64( s->mesh, ncomp, y, x, st );
 }

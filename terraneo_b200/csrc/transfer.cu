@@ -20,10 +20,11 @@ int halo_sum( const tn_mesh* m, T* const* fields, int nfields, cudaStream_t st )
 namespace {
 
 template < typename T >
-__global__ void prolong_constant_kernel( int nf1, int nc1, Ptr3< const T > src, Ptr3< T > dst, int ncomp, int add )
+__global__ void prolong_constant_kernel( int nd, int nf1, int nc1, Ptr3< const T > src, Ptr3< T > dst, int ncomp,
+                                         int add )
 {
     const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
-    const long long total = (long long) kDiamonds * nf1 * nf1 * nf1;
+    const long long total = (long long) nd * nf1 * nf1 * nf1;
     if ( t >= total )
         return;
     const int rf = int( t % nf1 ), yf = int( ( t / nf1 ) % nf1 ), xf = int( ( t / ( (long long) nf1 * nf1 ) ) % nf1 );
@@ -55,11 +56,11 @@ __global__ void prolong_constant_kernel( int nf1, int nc1, Ptr3< const T > src, 
 }
 
 template < typename T >
-__global__ void restrict_constant_kernel( int nf1, int nc1, const uint8_t* __restrict__ owned_f, Ptr3< const T > src,
-                                          Ptr3< T > dst, int ncomp, int add )
+__global__ void restrict_constant_kernel( int nd, int nf1, int nc1, const uint8_t* __restrict__ owned_f,
+                                          Ptr3< const T > src, Ptr3< T > dst, int ncomp, int add )
 {
     const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
-    const long long total = (long long) kDiamonds * nc1 * nc1 * nc1;
+    const long long total = (long long) nd * nc1 * nc1 * nc1;
     if ( t >= total )
         return;
     const int rc = int( t % nc1 ), yc = int( ( t / nc1 ) % nc1 ), xc = int( ( t / ( (long long) nc1 * nc1 ) ) % nc1 );
@@ -101,10 +102,10 @@ __global__ void restrict_constant_kernel( int nf1, int nc1, const uint8_t* __res
 
 // coarse(X, Y, R) = fine(2X, 2Y, 2R): coefficient fields on coarser levels
 template < typename T >
-__global__ void inject_kernel( int nf1, int nc1, Ptr3< const T > src, Ptr3< T > dst, int ncomp )
+__global__ void inject_kernel( int nd, int nf1, int nc1, Ptr3< const T > src, Ptr3< T > dst, int ncomp )
 {
     const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
-    const long long total = (long long) kDiamonds * nc1 * nc1 * nc1;
+    const long long total = (long long) nd * nc1 * nc1 * nc1;
     if ( t >= total )
         return;
     const int rc = int( t % nc1 ), yc = int( ( t / nc1 ) % nc1 ), xc = int( ( t / ( (long long) nc1 * nc1 ) ) % nc1 );
@@ -116,10 +117,11 @@ __global__ void inject_kernel( int nf1, int nc1, Ptr3< const T > src, Ptr3< T > 
 // tangential projection of 3-vectors at CMB / SURFACE nodes
 // (strong_algebraic_freeslip_enforcement_in_place, fe/strong_algebraic_freeslip_enforcement.hpp:23)
 template < typename T >
-__global__ void freeslip_project_kernel( int n1, const double* __restrict__ coords, Ptr3< T > y, int cmb, int surf )
+__global__ void freeslip_project_kernel( int nd, int n1, const double* __restrict__ coords, Ptr3< T > y, int cmb,
+                                         int surf )
 {
     const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
-    const long long total = (long long) kDiamonds * n1 * n1 * 2;
+    const long long total = (long long) nd * n1 * n1 * 2;
     if ( t >= total )
         return;
     const int    side = int( t & 1 );
@@ -137,12 +139,12 @@ __global__ void freeslip_project_kernel( int n1, const double* __restrict__ coor
 
 // Prolongation: each fine node gathers its coarse parents (blockIdx.y = component).
 template < typename T >
-__global__ void prolong_linear_kernel( int Nf, int nc1, const double* __restrict__ coords,
+__global__ void prolong_linear_kernel( int nd, int Nf, int nc1, const double* __restrict__ coords,
                                        const double* __restrict__ radii, Ptr3< const T > src, Ptr3< T > dst, int add )
 {
     const int       nf1   = Nf + 1;
     const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
-    const long long total = (long long) kDiamonds * nf1 * nf1 * nf1;
+    const long long total = (long long) nd * nf1 * nf1 * nf1;
     if ( t >= total )
         return;
     const int r = int( t % nf1 ), y = int( ( t / nf1 ) % nf1 ), x = int( ( t / ( (long long) nf1 * nf1 ) ) % nf1 );
@@ -162,13 +164,13 @@ __global__ void prolong_linear_kernel( int Nf, int nc1, const double* __restrict
 // value to its coarse parents (restriction_linear.hpp:106-222); the coarse
 // halo then sums duplicated coarse nodes.
 template < typename T >
-__global__ void restrict_linear_kernel( int Nf, int nc1, const double* __restrict__ coords,
+__global__ void restrict_linear_kernel( int nd, int Nf, int nc1, const double* __restrict__ coords,
                                         const double* __restrict__ radii, const uint8_t* __restrict__ owned,
                                         Ptr3< const T > src, Ptr3< T > dst )
 {
     const int       nf1   = Nf + 1;
     const long long t     = blockIdx.x * (long long) blockDim.x + threadIdx.x;
-    const long long total = (long long) kDiamonds * nf1 * nf1 * nf1;
+    const long long total = (long long) nd * nf1 * nf1 * nf1;
     if ( t >= total || !owned[t] )
         return;
     const int r = int( t % nf1 ), y = int( ( t / nf1 ) % nf1 ), x = int( ( t / ( (long long) nf1 * nf1 ) ) % nf1 );
@@ -185,6 +187,7 @@ int check_levels( const tn_mesh* f, const tn_mesh* c, int ncomp )
 {
     TN_CHECK_ARG( f && c, "transfer: null mesh" );
     TN_CHECK_ARG( c->level == f->level - 1, "transfer: coarse mesh must be one level below the fine mesh" );
+    TN_CHECK_ARG( c->d0 == f->d0 && c->nd == f->nd, "transfer: the meshes must hold the same diamonds" );
     TN_CHECK_ARG( ncomp >= 1 && ncomp <= 3, "transfer: ncomp must be 1..3" );
     return TN_OK;
 }
@@ -206,7 +209,7 @@ int prolong_constant( const tn_mesh* f, const tn_mesh* c, int ncomp, int apply_m
         s.p[i] = src[i], o.p[i] = dst[i];
     }
     const long long n = (long long) f->ns;
-    prolong_constant_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( f->n1, c->n1, s, o, ncomp,
+    prolong_constant_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( f->nd, f->n1, c->n1, s, o, ncomp,
                                                                                  apply_mode == TN_APPLY_ADD );
     TN_LAUNCH_CHECK();
     return TN_OK;
@@ -228,7 +231,7 @@ int restrict_constant( const tn_mesh* f, const tn_mesh* c, int ncomp, int apply_
         s.p[i] = src[i], o.p[i] = dst[i];
     }
     const long long n = (long long) c->ns;
-    restrict_constant_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( f->n1, c->n1, f->d_lat_owned, s, o,
+    restrict_constant_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( f->nd, f->n1, c->n1, f->d_lat_owned, s, o,
                                                                                   ncomp, 0 );
     TN_LAUNCH_CHECK();
     return halo_sum< T >( c, dst, ncomp, st );
@@ -251,7 +254,7 @@ int prolong_linear( const tn_mesh* f, const tn_mesh* c, int ncomp, int apply_mod
     }
     const long long n = (long long) f->ns;
     prolong_linear_kernel< T ><<< dim3( unsigned( ( n + 255 ) / 256 ), ncomp ), 256, 0, st >>>(
-        f->N, c->n1, f->d_coords, f->d_radii, s, o, apply_mode == TN_APPLY_ADD );
+        f->nd, f->N, c->n1, f->d_coords, f->d_radii, s, o, apply_mode == TN_APPLY_ADD );
     TN_LAUNCH_CHECK();
     return TN_OK;
 }
@@ -274,7 +277,7 @@ int restrict_linear( const tn_mesh* f, const tn_mesh* c, int ncomp, const T* con
     }
     const long long n = (long long) f->ns;
     restrict_linear_kernel< T ><<< dim3( unsigned( ( n + 255 ) / 256 ), ncomp ), 256, 0, st >>>(
-        f->N, c->n1, f->d_coords, f->d_radii, f->d_node_owned, s, o );
+        f->nd, f->N, c->n1, f->d_coords, f->d_radii, f->d_node_owned, s, o );
     TN_LAUNCH_CHECK();
     return halo_sum< T >( c, dst, ncomp, st );
 }
@@ -293,7 +296,7 @@ int inject( const tn_mesh* f, const tn_mesh* c, int ncomp, const T* const* src, 
         s.p[i] = src[i], o.p[i] = dst[i];
     }
     const long long n = (long long) c->ns;
-    inject_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( f->n1, c->n1, s, o, ncomp );
+    inject_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( f->nd, f->n1, c->n1, s, o, ncomp );
     TN_LAUNCH_CHECK();
     return TN_OK;
 }
@@ -303,9 +306,8 @@ int freeslip_project( const tn_mesh* m, T* const* y, int cmb, int surf, cudaStre
 {
     TN_CHECK_ARG( m && y && y[0] && y[1] && y[2], "freeslip_project: null argument" );
     const long long n = (long long) m->nlat * 2;
-    freeslip_project_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>( m->n1, m->d_coords,
-                                                                                  Ptr3< T >{ { y[0], y[1], y[2] } },
-                                                                                  cmb, surf );
+    freeslip_project_kernel< T ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, st >>>(
+        m->nd, m->n1, m->d_coords, Ptr3< T >{ { y[0], y[1], y[2] } }, cmb, surf );
     TN_LAUNCH_CHECK();
     return TN_OK;
 }

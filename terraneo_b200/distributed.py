@@ -129,6 +129,52 @@ class ShellShard:
         C.check(C.lib().tn_shard_vec_lincomb_f64(self.handle, y.shape[0], _comp_ptrs(y), c0, len(xs), c, x,
                                                  _stream()), "tn_shard_vec_lincomb_f64")
 
+    # multigrid pieces: this shard and the same rank's shard one level coarser
+    def prolong_add(self, coarse, src_c, dst_f):
+        """dst_f += P src_c (constant prolongation)"""
+        C.check(C.lib().tn_shard_prolongation_constant_f64(self.handle, coarse.handle, src_c.shape[0], C.APPLY_ADD,
+                                                           _comp_ptrs(src_c), _comp_ptrs(dst_f), _stream()),
+                "tn_shard_prolongation_constant_f64")
+
+    def restrict(self, coarse, src_f, dst_c):
+        """dst_c = R src_f (constant restriction, coarse copies on this rank summed)"""
+        C.check(C.lib().tn_shard_restriction_constant_f64(self.handle, coarse.handle, src_f.shape[0], _comp_ptrs(src_f),
+                                                          _comp_ptrs(dst_c), _stream()),
+                "tn_shard_restriction_constant_f64")
+
+    def inject(self, coarse, src_f, dst_c):
+        """dst_c = src_f at the coarse nodes; a scalar field may come without its component axis"""
+        src_f = src_f.unsqueeze(0) if src_f.dim() == 4 else src_f
+        dst_c = dst_c.unsqueeze(0) if dst_c.dim() == 4 else dst_c
+        C.check(C.lib().tn_shard_injection_f64(self.handle, coarse.handle, src_f.shape[0], _comp_ptrs(src_f),
+                                               _comp_ptrs(dst_c), _stream()), "tn_shard_injection_f64")
+
+    def invert(self, y):
+        C.check(C.lib().tn_shard_vec_invert_f64(self.handle, y.shape[0], _comp_ptrs(y), _stream()),
+                "tn_shard_vec_invert_f64")
+
+    def mult(self, y, x):
+        """y *= x elementwise"""
+        C.check(C.lib().tn_shard_vec_mult_f64(self.handle, y.shape[0], _comp_ptrs(y), _comp_ptrs(x), _stream()),
+                "tn_shard_vec_mult_f64")
+
+    def chebyshev_step(self, x, d, b, ax, inv_diag, alpha, beta):
+        """d = alpha D^-1 (b - ax) + beta d;  x += d"""
+        C.check(C.lib().tn_shard_vec_chebyshev_step_f64(self.handle, x.shape[0], _comp_ptrs(x), _comp_ptrs(d),
+                                                        _comp_ptrs(b), _comp_ptrs(ax), _comp_ptrs(inv_diag), alpha,
+                                                        beta, _stream()), "tn_shard_vec_chebyshev_step_f64")
+
+    def random(self, ncomp, seed):
+        """a start vector in [-0.5, 0.5) that depends on the node's global index only (every partition draws the
+        same values): frac(sin(12.9898 g + 78.233 (seed + c)) 43758.5453) - 0.5"""
+        ns = self.stored_nodes
+        g = torch.arange(ns, dtype=torch.float64, device="cuda") + float(self.first_diamond * self.n1 ** 3)
+        out = torch.empty((ncomp,) + self.shape, dtype=torch.float64, device="cuda")
+        for c in range(ncomp):
+            v = torch.sin(g * 12.9898 + 78.233 * (seed + c)) * 43758.5453
+            out[c] = (v - torch.floor(v) - 0.5).reshape(self.shape)
+        return out
+
 
 def c_size():
     return ctypes.c_size_t()
@@ -197,6 +243,28 @@ class DistributedShell:
     def copy(self, dst, src):
         self.shard.lincomb(dst, 0.0, [1.0], [src])
 
+    def restrict_to(self, coarse, src_f, dst_c):
+        self.shard.restrict(coarse.shard, src_f, dst_c)
+        coarse.exchange(dst_c)
+
+    def prolong_add_from(self, coarse, src_c, dst_f):
+        self.shard.prolong_add(coarse.shard, src_c, dst_f)
+
+    def inject_to(self, coarse, src_f, dst_c):
+        self.shard.inject(coarse.shard, src_f, dst_c)
+
+    def invert(self, y):
+        self.shard.invert(y)
+
+    def mult(self, y, x):
+        self.shard.mult(y, x)
+
+    def chebyshev_step(self, x, d, b, ax, inv_diag, alpha, beta):
+        self.shard.chebyshev_step(x, d, b, ax, inv_diag, alpha, beta)
+
+    def random(self, ncomp, seed):
+        return self.shard.random(ncomp, seed)
+
     def cg(self, k, b, x, bc_cmb=C.BC_DIRICHLET, bc_surface=C.BC_DIRICHLET, max_iterations=500,
            relative_tolerance=1e-10, absolute_tolerance=0.0):
         return cg(self, k, b, x, bc_cmb, bc_surface, max_iterations, relative_tolerance, absolute_tolerance)
@@ -260,6 +328,34 @@ class EmulatedShell:
     def copy(self, dst, src):
         self.lincomb(dst, 0.0, [1.0], [src])
 
+    def restrict_to(self, coarse, src_f, dst_c):
+        for f, c, x, y in zip(self.shards, coarse.shards, src_f, dst_c):
+            f.restrict(c, x, y)
+        coarse.exchange(dst_c)
+
+    def prolong_add_from(self, coarse, src_c, dst_f):
+        for f, c, x, y in zip(self.shards, coarse.shards, src_c, dst_f):
+            f.prolong_add(c, x, y)
+
+    def inject_to(self, coarse, src_f, dst_c):
+        for f, c, x, y in zip(self.shards, coarse.shards, src_f, dst_c):
+            f.inject(c, x, y)
+
+    def invert(self, y):
+        for sh, v in zip(self.shards, y):
+            sh.invert(v)
+
+    def mult(self, y, x):
+        for sh, a, b in zip(self.shards, y, x):
+            sh.mult(a, b)
+
+    def chebyshev_step(self, x, d, b, ax, inv_diag, alpha, beta):
+        for q, sh in enumerate(self.shards):
+            sh.chebyshev_step(x[q], d[q], b[q], ax[q], inv_diag[q], alpha, beta)
+
+    def random(self, ncomp, seed):
+        return [sh.random(ncomp, seed) for sh in self.shards]
+
     def cg(self, k, b, x, bc_cmb=C.BC_DIRICHLET, bc_surface=C.BC_DIRICHLET, max_iterations=500,
            relative_tolerance=1e-10, absolute_tolerance=0.0):
         return cg(self, k, b, x, bc_cmb, bc_surface, max_iterations, relative_tolerance, absolute_tolerance)
@@ -290,4 +386,121 @@ def cg(D, k, b, x, bc_cmb=C.BC_DIRICHLET, bc_surface=C.BC_DIRICHLET, max_iterati
             return it, res / r0
         D.lincomb(p, 0.0, [1.0, rr_new / rr], [r, p])
         rr = rr_new
+    return max_iterations, res / r0
+
+
+class ShardedMultigrid:
+    """Geometric multigrid V-cycle for the kerngen (epsilon-div-div) operator over a hierarchy of sharded domains
+    `levels` (finest first, one level apart, the same partition): the operator re-discretised on every level with
+    the viscosity injected from the finest, the Chebyshev smoother (linalg/solvers/chebyshev.hpp:50-175: order,
+    `smoothing_steps` sweeps before and after, lambda_max = 1.5 x the power-iteration estimate of D^-1 A,
+    lambda_min = 0.1 x it), constant vector transfers and CG on the coarsest level, as the reference's Multigrid
+    (linalg/solvers/multigrid.hpp:184-211) composes them.  Every operation is sharded: applies and restrictions
+    finish with the exchange, dots are global."""
+
+    def __init__(self, levels, k_fine, bc_cmb, bc_surface, order=3, smoothing_steps=2, power_iterations=10,
+                 coarse_max_iterations=50, coarse_relative_tolerance=1e-6, seed=7):
+        self.D, self.bc = levels, (bc_cmb, bc_surface)
+        self.order, self.steps = order, smoothing_steps
+        self.coarse_maxit, self.coarse_rtol = coarse_max_iterations, coarse_relative_tolerance
+        self.k = [k_fine]
+        for lf, lc in zip(levels[:-1], levels[1:]):
+            kc = lc.vector(1)
+            lf.inject_to(lc, self.k[-1], kc)
+            self.k.append(kc)
+        # per level: residual, correction, smoother direction, operator result
+        self.tmp = [tuple(D.vector(3) for _ in range(4)) for D in levels]
+        self.inv_diag, self.ev = [], []
+        for lev, (D, k) in enumerate(zip(levels[:-1], self.k[:-1])):
+            dg = D.vector(3)
+            D.lincomb(self.tmp[lev][0], 1.0, [], [])
+            D.epsdivdiv_apply(k, self.tmp[lev][0], dg, bc_cmb, bc_surface, diagonal=True)
+            D.invert(dg)
+            self.inv_diag.append(dg)
+            self.ev.append(self._power_iteration(lev, power_iterations, seed + lev))
+
+    def _power_iteration(self, lev, iterations, seed):
+        """power_iteration (linalg/solvers/power_iteration.hpp:13-48) on D^-1 A, from a start vector that depends
+        on the global node index only"""
+        D, k, dinv = self.D[lev], self.k[lev], self.inv_diag[lev]
+        it, aux = D.random(3, seed), self.tmp[lev][3]
+
+        def op(src, dst):
+            D.epsdivdiv_apply(k, src, dst, *self.bc)
+            D.mult(dst, dinv)
+        n = D.dot(it, it) ** 0.5
+        D.lincomb(it, 0.0, [1.0 / n], [it])
+        op(it, aux)
+        radius = 0.0
+        for _ in range(iterations):
+            n = D.dot(aux, aux) ** 0.5
+            D.lincomb(it, 0.0, [1.0 / n], [aux])
+            op(it, aux)
+            radius = D.dot(it, aux)
+        return radius
+
+    def _smooth(self, lev, x, b):
+        D, k, dinv, ev = self.D[lev], self.k[lev], self.inv_diag[lev], self.ev[lev]
+        d, z = self.tmp[lev][2], self.tmp[lev][3]
+        lmax, lmin = 1.5 * ev, 0.1 * ev
+        theta, delta = 0.5 * (lmax + lmin), 0.5 * (lmax - lmin)
+        sigma = theta / delta
+        rho = 1.0 / sigma  # carried across sweeps as in the reference (chebyshev.hpp:119)
+        for _ in range(self.steps):
+            D.epsdivdiv_apply(k, x, z, *self.bc)
+            D.chebyshev_step(x, d, b, z, dinv, 1.0 / theta, 0.0)
+            for _ in range(2, self.order + 1):
+                rho_new = 1.0 / (2.0 * sigma - rho)
+                D.epsdivdiv_apply(k, x, z, *self.bc)
+                D.chebyshev_step(x, d, b, z, dinv, 2.0 * rho_new / delta, rho_new * rho)
+                rho = rho_new
+
+    def _recurse(self, lev, x, b):
+        D, k = self.D[lev], self.k[lev]
+        if lev == len(self.D) - 1:
+            cg(D, k, b, x, *self.bc, max_iterations=self.coarse_maxit, relative_tolerance=self.coarse_rtol)
+            return
+        self._smooth(lev, x, b)
+        r = self.tmp[lev][0]
+        D.epsdivdiv_apply(k, x, r, *self.bc)
+        D.lincomb(r, 0.0, [1.0, -1.0], [b, r])
+        rc, ec = self.tmp[lev + 1][0], self.tmp[lev + 1][1]
+        D.restrict_to(self.D[lev + 1], r, rc)
+        self.D[lev + 1].lincomb(ec, 0.0, [], [])
+        self._recurse(lev + 1, ec, rc)
+        D.prolong_add_from(self.D[lev + 1], ec, x)
+        self._smooth(lev, x, b)
+
+    def solve(self, x, b):
+        """one V-cycle on A x = b from the given x"""
+        self._recurse(0, x, b)
+
+
+def mg_pcg(D, mg, k, b, x, bc_cmb, bc_surface, max_iterations=200, relative_tolerance=1e-8,
+           absolute_tolerance=0.0):
+    """The reference's PCG (linalg/solvers/pcg.hpp:78-160) over a sharded domain with the V-cycle `mg`
+    (ShardedMultigrid, z = V(r) from z = 0) as the preconditioner.  Returns (iterations, relative residual)."""
+    r, z, p, ap = D.vector(3), D.vector(3), D.vector(3), D.vector(3)
+    D.epsdivdiv_apply(k, x, r, bc_cmb, bc_surface)
+    D.lincomb(r, 0.0, [1.0, -1.0], [b, r])
+    D.lincomb(z, 0.0, [], [])
+    mg.solve(z, r)
+    D.copy(p, z)
+    r0 = D.dot(r, r) ** 0.5
+    if r0 <= absolute_tolerance or r0 == 0.0:
+        return 0, 0.0
+    res = r0
+    for it in range(1, max_iterations + 1):
+        an = D.dot(z, r)
+        D.epsdivdiv_apply(k, p, ap, bc_cmb, bc_surface)
+        alpha = an / D.dot(ap, p)
+        D.lincomb(x, 0.0, [1.0, alpha], [x, p])
+        D.lincomb(r, 0.0, [1.0, -alpha], [r, ap])
+        res = D.dot(r, r) ** 0.5
+        if res / r0 <= relative_tolerance or res < absolute_tolerance:
+            return it, res / r0
+        D.lincomb(z, 0.0, [], [])
+        mg.solve(z, r)
+        beta = D.dot(z, r) / an
+        D.lincomb(p, 0.0, [1.0, beta], [z, p])
     return max_iterations, res / r0

@@ -237,3 +237,36 @@ def test_emulated_ranks_cg_matches_one_rank(bc):
     for P in (2, 3, 5, 8):
         assert abs(its[P] - its[1]) <= 2, its
         assert rel(sols[P], sols[1]) <= 1e-8, P
+
+
+@pytest.mark.parametrize("bc", [(1, 1), (1, 2)])
+def test_emulated_ranks_multigrid_pcg(bc):
+    """the sharded multigrid (distributed.ShardedMultigrid: Chebyshev order 3, 2 sweeps, constant transfers, CG on
+    the coarsest level; levels 4, 3, 2) as the preconditioner of CG, over P = 1, 2, 3, 5 emulated ranks: the oracle's
+    true residual, the one-rank iteration count within 1, the solutions within the tolerance, and far fewer
+    iterations than plain CG"""
+    from terraneo_b200.distributed import EmulatedShell, ShardedMultigrid, mg_pcg
+    L = 4
+    om = Mesh(L)
+    k, _ = _inputs(om)
+    rs = np.random.RandomState(41)
+    b = np.stack([om.make_consistent(rs.normal(size=om.shape)).reshape(om.shape) for _ in range(3)])
+    its, sols, evs = {}, {}, {}
+    for P in (1, 2, 3, 5):
+        levels = [EmulatedShell(lv, P) for lv in (L, L - 1, L - 2)]
+        kk = levels[0].scatter(k)
+        mg = ShardedMultigrid(levels, kk, *bc, order=3, smoothing_steps=2, power_iterations=10,
+                              coarse_max_iterations=50, coarse_relative_tolerance=1e-6)
+        evs[P] = mg.ev
+        x = levels[0].vector(3)
+        its[P], rr = mg_pcg(levels[0], mg, kk, levels[0].scatter(b), x, *bc, max_iterations=100,
+                            relative_tolerance=1e-8)
+        assert rr <= 1e-8, (P, its[P], rr)
+        sols[P] = levels[0].gather(x)
+        res = om.kerngen(k, sols[P], *bc) - b
+        assert np.sqrt(om.dot(res, res)) <= 2e-8 * np.sqrt(om.dot(b, b)), P
+    assert its[1] <= 40, its
+    for P in (2, 3, 5):
+        assert np.allclose(evs[P], evs[1], rtol=1e-10), (evs[P], evs[1])
+        assert abs(its[P] - its[1]) <= 1, its
+        assert rel(sols[P], sols[1]) <= 1e-6, P
