@@ -713,11 +713,23 @@ TN_API int tn_shard_dims( const tn_shard* shard, int* first_diamond, int* num_di
 TN_API int tn_shard_geometry( const tn_shard* shard, double* coords, double* radii );
 TN_API int tn_shard_masks( const tn_shard* shard, uint8_t* boundary_mask, uint8_t* ownership_mask );
 /* EpsilonDivDivKerngen apply on the shard's cells (tn_epsdivdiv_apply_*); free-slip on both radii (the global
- * rigid-rotation penalty) only with num_ranks = 1 */
+ * rigid-rotation penalty) only with num_ranks = 1 here, with more ranks through the two calls below */
 TN_API int tn_shard_epsdivdiv_apply_f64( const tn_shard* shard, const tn_epsdivdiv_params* p, const double* k,
                                          const double* const* src, double* const* dst, void* stream );
 TN_API int tn_shard_epsdivdiv_apply_f32( const tn_shard* shard, const tn_epsdivdiv_params* p, const float* k,
                                          const float* const* src, float* const* dst, void* stream );
+/* Free-slip on both radii with two or more ranks: the rigid-rotation penalty needs the whole shell's three rotation
+ * dots b_j = sum over owned nodes of (e_j x x) . src.  tn_shard_penalty_dots_* writes this rank's part to `dots`
+ * (3 doubles, device); the caller sums them over the ranks (an all-reduce) and passes the sums to
+ * tn_shard_epsdivdiv_apply_fsfs_*, which forms the penalty vector eps G^-1 b from them (kerngen :287-408, :585-606). */
+TN_API int tn_shard_penalty_dots_f64( const tn_shard* shard, const double* const* src, double* dots, void* stream );
+TN_API int tn_shard_penalty_dots_f32( const tn_shard* shard, const float* const* src, double* dots, void* stream );
+TN_API int tn_shard_epsdivdiv_apply_fsfs_f64( const tn_shard* shard, const tn_epsdivdiv_params* p, const double* k,
+                                              const double* const* src, double* const* dst, const double* dots,
+                                              void* stream );
+TN_API int tn_shard_epsdivdiv_apply_fsfs_f32( const tn_shard* shard, const tn_epsdivdiv_params* p, const float* k,
+                                              const float* const* src, float* const* dst, const double* dots,
+                                              void* stream );
 TN_API int tn_shard_pack_f64( const tn_shard* shard, const double* const* fields, int nfields, double* buf,
                               void* stream );
 TN_API int tn_shard_pack_f32( const tn_shard* shard, const float* const* fields, int nfields, float* buf, void* stream );

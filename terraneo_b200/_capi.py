@@ -203,6 +203,12 @@ _SIGS = {
                                              c_void_p]),
     "tn_shard_epsdivdiv_apply_f32": (c_int, [c_void_p, P(EpsDivDivParams), c_void_p, P(c_void_p), P(c_void_p),
                                              c_void_p]),
+    "tn_shard_penalty_dots_f64": (c_int, [c_void_p, P(c_void_p), c_void_p, c_void_p]),
+    "tn_shard_penalty_dots_f32": (c_int, [c_void_p, P(c_void_p), c_void_p, c_void_p]),
+    "tn_shard_epsdivdiv_apply_fsfs_f64": (c_int, [c_void_p, P(EpsDivDivParams), c_void_p, P(c_void_p), P(c_void_p),
+                                                  c_void_p, c_void_p]),
+    "tn_shard_epsdivdiv_apply_fsfs_f32": (c_int, [c_void_p, P(EpsDivDivParams), c_void_p, P(c_void_p), P(c_void_p),
+                                                  c_void_p, c_void_p]),
     "tn_shard_pack_f64": (c_int, [c_void_p, P(c_void_p), c_int, c_void_p, c_void_p]),
     "tn_shard_pack_f32": (c_int, [c_void_p, P(c_void_p), c_int, c_void_p, c_void_p]),
     "tn_shard_unpack_f64": (c_int, [c_void_p, c_void_p, P(c_void_p), c_int, c_void_p]),

@@ -902,9 +902,44 @@ int tile_launch( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k, Ptr
     return TN_OK;
 }
 
+// beta = eps G^-1 b from the three rotation dots b of the whole shell (a sharded apply: the ranks' parts summed)
+__global__ void penalty_beta_kernel( const double* __restrict__ dots, double eps, Mat3 ginv, double* beta )
+{
+    if ( threadIdx.x == 0 && blockIdx.x == 0 )
+    {
+        const double b0 = dots[0], b1 = dots[1], b2 = dots[2];
+        beta[0]         = eps * ( ginv.a[0] * b0 + ginv.a[1] * b1 + ginv.a[2] * b2 );
+        beta[1]         = eps * ( ginv.a[3] * b0 + ginv.a[4] * b1 + ginv.a[5] * b2 );
+        beta[2]         = eps * ( ginv.a[6] * b0 + ginv.a[7] * b1 + ginv.a[8] * b2 );
+    }
+}
+
+// The rotation dots of src over this mesh's owned nodes into dots[0..2] (device); a whole shell's penalty needs
+// the sum of these over the meshes that partition it.
+template < typename T >
+int penalty_dots( const tn_mesh* m, const T* const* src, double* dots, cudaStream_t st )
+{
+    TN_CHECK_ARG( m && src && src[0] && src[1] && src[2] && dots, "penalty_dots: null argument" );
+    Ptr3< const T > s{ { src[0], src[1], src[2] } };
+    Mat3            gi;
+    for ( int i = 0; i < 9; ++i )
+        gi.a[i] = m->penalty_gram_inv[i];
+    penalty_dots_kernel< T ><<< penalty_blocks( m->nlat ), 256, 0, st >>>( m->nlat, m->n1, m->d_coords,
+                                                                            mesh_radii< T >( m ), s, m->d_lat_owned,
+                                                                            m->d_red_partials, m->d_red_counter,
+                                                                            m->d_red_result, 1.0, gi );
+    TN_LAUNCH_CHECK();
+    TN_CUDA_TRY( cudaMemcpyAsync( dots, m->d_red_result, 3 * sizeof( double ), cudaMemcpyDeviceToDevice, st ) );
+    return TN_OK;
+}
+template int penalty_dots< double >( const tn_mesh*, const double* const*, double*, cudaStream_t );
+template int penalty_dots< float >( const tn_mesh*, const float* const*, double*, cudaStream_t );
+
+// global_dots != nullptr (free-slip on both radii only): the rotation dots of the whole shell are given, so the
+// penalty vector is formed from them instead of from this mesh's own dots
 template < typename T >
 int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k, const T* const* src, T* const* dst,
-                     cudaStream_t st )
+                     cudaStream_t st, const double* global_dots )
 {
     TN_CHECK_ARG( m && p && k && src && dst, "epsdivdiv_apply: null argument" );
     for ( int c = 0; c < 3; ++c )
@@ -923,9 +958,12 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
         Mat3 gi;
         for ( int i = 0; i < 9; ++i )
             gi.a[i] = m->penalty_gram_inv[i];
-        penalty_dots_kernel< T ><<< penalty_blocks( m->nlat ), 256, 0, st >>>(
-            m->nlat, m->n1, m->d_coords, mesh_radii< T >( m ), s, m->d_lat_owned, m->d_red_partials, m->d_red_counter,
-            m->d_red_result, p->penalty_eps, gi );
+        if ( global_dots )
+            penalty_beta_kernel<<< 1, 32, 0, st >>>( global_dots, p->penalty_eps, gi, m->d_red_result + 3 );
+        else
+            penalty_dots_kernel< T ><<< penalty_blocks( m->nlat ), 256, 0, st >>>(
+                m->nlat, m->n1, m->d_coords, mesh_radii< T >( m ), s, m->d_lat_owned, m->d_red_partials,
+                m->d_red_counter, m->d_red_result, p->penalty_eps, gi );
         TN_LAUNCH_CHECK();
     }
 
@@ -966,9 +1004,9 @@ int epsdivdiv_apply( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k,
 }
 
 template int epsdivdiv_apply< double >( const tn_mesh*, const tn_epsdivdiv_params*, const double*, const double* const*,
-                                        double* const*, cudaStream_t );
+                                        double* const*, cudaStream_t, const double* );
 template int epsdivdiv_apply< float >( const tn_mesh*, const tn_epsdivdiv_params*, const float*, const float* const*,
-                                       float* const*, cudaStream_t );
+                                       float* const*, cudaStream_t, const double* );
 
 // dst += eps sum_i (m_i^T src) m_i, the fs/fs rigid-rotation penalty on every
 // stored node (no halo), in two parts for the stored-matrix apply: the dots
@@ -1014,10 +1052,10 @@ using namespace tn;
 extern "C" int tn_epsdivdiv_apply_f64( const tn_mesh* m, const tn_epsdivdiv_params* p, const double* k,
                                        const double* const* src, double* const* dst, void* s )
 {
-    return epsdivdiv_apply< double >( m, p, k, src, dst, as_stream( s ) );
+    return epsdivdiv_apply< double >( m, p, k, src, dst, as_stream( s ), nullptr );
 }
 extern "C" int tn_epsdivdiv_apply_f32( const tn_mesh* m, const tn_epsdivdiv_params* p, const float* k,
                                        const float* const* src, float* const* dst, void* s )
 {
-    return epsdivdiv_apply< float >( m, p, k, src, dst, as_stream( s ) );
+    return epsdivdiv_apply< float >( m, p, k, src, dst, as_stream( s ), nullptr );
 }

@@ -26,7 +26,10 @@
 namespace tn {
 
 template < typename T >
-int epsdivdiv_apply( const tn_mesh*, const tn_epsdivdiv_params*, const T*, const T* const*, T* const*, cudaStream_t );
+int epsdivdiv_apply( const tn_mesh*, const tn_epsdivdiv_params*, const T*, const T* const*, T* const*, cudaStream_t,
+                     const double* );
+template < typename T >
+int penalty_dots( const tn_mesh*, const T* const*, double*, cudaStream_t );
 template < typename T >
 int prolong_constant( const tn_mesh*, const tn_mesh*, int, int, const T* const*, T* const*, cudaStream_t );
 template < typename T >
@@ -192,9 +195,19 @@ int shard_apply( const tn_shard* s, const tn_epsdivdiv_params* p, const T* k, co
     TN_CHECK_ARG( s && p, "tn_shard_epsdivdiv_apply: null argument" );
     TN_CHECK_ARG( p->diagonal || !( p->bc_cmb == TN_BC_FREESLIP && p->bc_surface == TN_BC_FREESLIP ) ||
                       s->num_ranks == 1,
-                  "tn_shard_epsdivdiv_apply: free-slip on both radii needs the global rigid-rotation dots inside the "
-                  "apply and is not supported on a shard of two or more ranks" );
-    return epsdivdiv_apply< T >( s->mesh, p, k, src, dst, st );
+                  "tn_shard_epsdivdiv_apply: free-slip on both radii needs the whole shell's rotation dots; with two "
+                  "or more ranks use tn_shard_penalty_dots and tn_shard_epsdivdiv_apply_fsfs" );
+    return epsdivdiv_apply< T >( s->mesh, p, k, src, dst, st, nullptr );
+}
+
+template < typename T >
+int shard_apply_fsfs( const tn_shard* s, const tn_epsdivdiv_params* p, const T* k, const T* const* src, T* const* dst,
+                      const double* dots, cudaStream_t st )
+{
+    TN_CHECK_ARG( s && p && dots, "tn_shard_epsdivdiv_apply_fsfs: null argument" );
+    TN_CHECK_ARG( !p->diagonal && p->bc_cmb == TN_BC_FREESLIP && p->bc_surface == TN_BC_FREESLIP,
+                  "tn_shard_epsdivdiv_apply_fsfs: free-slip on both radii, non-diagonal only" );
+    return epsdivdiv_apply< T >( s->mesh, p, k, src, dst, st, dots );
 }
 
 }  // namespace
@@ -399,4 +412,32 @@ extern "C" int tn_shard_vec_mult_f64( const tn_shard* s, int ncomp, double* cons
 {
     TN_CHECK_ARG( s, "tn_shard_vec_mult_f64: shard is NULL" );
     return tn_vec_mult_f64( s->mesh, ncomp, y, x, st );
+}
+
+// ---------------------------------------------------------------------------
+// Free-slip on both radii over shards: the rigid-rotation penalty (kerngen :287-408, :585-606) needs three dot
+// products over the whole shell's owned nodes; each rank forms its part, the caller sums them over the ranks, and
+// the apply forms the penalty vector from the sums (the shell's Gram matrix is the same on every rank).
+
+extern "C" int tn_shard_penalty_dots_f64( const tn_shard* s, const double* const* src, double* dots, void* st )
+{
+    TN_CHECK_ARG( s, "tn_shard_penalty_dots_f64: shard is NULL" );
+    return penalty_dots< double >( s->mesh, src, dots, as_stream( st ) );
+}
+extern "C" int tn_shard_penalty_dots_f32( const tn_shard* s, const float* const* src, double* dots, void* st )
+{
+    TN_CHECK_ARG( s, "tn_shard_penalty_dots_f32: shard is NULL" );
+    return penalty_dots< float >( s->mesh, src, dots, as_stream( st ) );
+}
+extern "C" int tn_shard_epsdivdiv_apply_fsfs_f64( const tn_shard* s, const tn_epsdivdiv_params* p, const double* k,
+                                                  const double* const* src, double* const* dst, const double* dots,
+                                                  void* st )
+{
+    return shard_apply_fsfs< double >( s, p, k, src, dst, dots, as_stream( st ) );
+}
+extern "C" int tn_shard_epsdivdiv_apply_fsfs_f32( const tn_shard* s, const tn_epsdivdiv_params* p, const float* k,
+                                                  const float* const* src, float* const* dst, const double* dots,
+                                                  void* st )
+{
+    return shard_apply_fsfs< float >( s, p, k, src, dst, dots, as_stream( st ) );
 }

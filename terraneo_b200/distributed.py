@@ -103,6 +103,20 @@ class ShellShard:
         C.check(fn(self.handle, ctypes.byref(p), ctypes.c_void_p(k.data_ptr()), _comp_ptrs(src), _comp_ptrs(dst),
                    _stream()), "tn_shard_epsdivdiv_apply")
 
+    def penalty_dots(self, src, dots):
+        """this rank's part of the three rigid-rotation dots of src into the device tensor dots (3 doubles)"""
+        fn = C.lib().tn_shard_penalty_dots_f64 if src.dtype == torch.float64 else C.lib().tn_shard_penalty_dots_f32
+        C.check(fn(self.handle, _comp_ptrs(src), ctypes.c_void_p(dots.data_ptr()), _stream()), "tn_shard_penalty_dots")
+
+    def epsdivdiv_apply_fsfs(self, k, src, dst, dots, apply_mode=C.APPLY_REPLACE, comm_mode=C.COMM_ADDITIVE,
+                             penalty_eps=1.0):
+        """the free-slip (both radii) apply with the whole shell's rotation dots given (device tensor, 3 doubles)"""
+        p = C.EpsDivDivParams(C.BC_FREESLIP, C.BC_FREESLIP, 0, apply_mode, comm_mode, penalty_eps)
+        fn = C.lib().tn_shard_epsdivdiv_apply_fsfs_f64 if src.dtype == torch.float64 else \
+            C.lib().tn_shard_epsdivdiv_apply_fsfs_f32
+        C.check(fn(self.handle, ctypes.byref(p), ctypes.c_void_p(k.data_ptr()), _comp_ptrs(src), _comp_ptrs(dst),
+                   ctypes.c_void_p(dots.data_ptr()), _stream()), "tn_shard_epsdivdiv_apply_fsfs")
+
     def pack(self, fields, buf):
         fn = C.lib().tn_shard_pack_f64 if fields.dtype == torch.float64 else C.lib().tn_shard_pack_f32
         C.check(fn(self.handle, _comp_ptrs(fields), fields.shape[0], ctypes.c_void_p(buf.data_ptr()), _stream()),
@@ -223,8 +237,15 @@ class DistributedShell:
         self.shard.unpack(buf, fields)
 
     def epsdivdiv_apply(self, k, src, dst, bc_cmb, bc_surface, diagonal=False, apply_mode=C.APPLY_REPLACE):
-        """EpsilonDivDivKerngen apply with the additive halo over all ranks (every copy of a node holds the sum)."""
-        self.shard.epsdivdiv_apply(k, src, dst, bc_cmb, bc_surface, diagonal, apply_mode, C.COMM_ADDITIVE)
+        """EpsilonDivDivKerngen apply with the additive halo over all ranks (every copy of a node holds the sum);
+        with free-slip on both radii the rotation dots are all-reduced first."""
+        if self.world > 1 and not diagonal and bc_cmb == C.BC_FREESLIP and bc_surface == C.BC_FREESLIP:
+            dots = torch.zeros(3, dtype=torch.float64, device="cuda")
+            self.shard.penalty_dots(src, dots)
+            self._all_reduce(dots)
+            self.shard.epsdivdiv_apply_fsfs(k, src, dst, dots, apply_mode)
+        else:
+            self.shard.epsdivdiv_apply(k, src, dst, bc_cmb, bc_surface, diagonal, apply_mode, C.COMM_ADDITIVE)
         self.exchange(dst)
 
     def dot(self, a, b):
@@ -314,8 +335,17 @@ class EmulatedShell:
             sh.unpack(total, f)
 
     def epsdivdiv_apply(self, k, src, dst, bc_cmb, bc_surface, diagonal=False, apply_mode=C.APPLY_REPLACE):
-        for sh, kk, s, d in zip(self.shards, k, src, dst):
-            sh.epsdivdiv_apply(kk, s, d, bc_cmb, bc_surface, diagonal, apply_mode, C.COMM_ADDITIVE)
+        if self.world > 1 and not diagonal and bc_cmb == C.BC_FREESLIP and bc_surface == C.BC_FREESLIP:
+            parts = []
+            for sh, s in zip(self.shards, src):
+                parts.append(torch.zeros(3, dtype=torch.float64, device="cuda"))
+                sh.penalty_dots(s, parts[-1])
+            dots = torch.stack(parts).sum(dim=0)  # the all-reduce over the ranks
+            for sh, kk, s, d in zip(self.shards, k, src, dst):
+                sh.epsdivdiv_apply_fsfs(kk, s, d, dots, apply_mode)
+        else:
+            for sh, kk, s, d in zip(self.shards, k, src, dst):
+                sh.epsdivdiv_apply(kk, s, d, bc_cmb, bc_surface, diagonal, apply_mode, C.COMM_ADDITIVE)
         self.exchange(dst)
 
     def dot(self, a, b):

@@ -214,7 +214,7 @@ def test_bench_sharded_leg_on_one_rank():
     assert sh["value"] > 1.0 and sh["scaling"] == "strong"
 
 
-@pytest.mark.parametrize("bc", [(1, 1), (1, 2), (2, 1)])
+@pytest.mark.parametrize("bc", [(1, 1), (1, 2), (2, 1), (2, 2)])
 def test_emulated_ranks_cg_matches_one_rank(bc):
     """CG over P = 2, 3, 5, 8 emulated ranks (distributed.EmulatedShell: the ranks one after another on one GPU,
     the exchange a sum of their buffers) against the one-rank solve: the same iteration count within 2, the
@@ -239,7 +239,7 @@ def test_emulated_ranks_cg_matches_one_rank(bc):
         assert rel(sols[P], sols[1]) <= 1e-8, P
 
 
-@pytest.mark.parametrize("bc", [(1, 1), (1, 2)])
+@pytest.mark.parametrize("bc", [(1, 1), (1, 2), (2, 2)])
 def test_emulated_ranks_multigrid_pcg(bc):
     """the sharded multigrid (distributed.ShardedMultigrid: Chebyshev order 3, 2 sweeps, constant transfers, CG on
     the coarsest level; levels 4, 3, 2) as the preconditioner of CG, over P = 1, 2, 3, 5 emulated ranks: the oracle's
@@ -265,8 +265,28 @@ def test_emulated_ranks_multigrid_pcg(bc):
         sols[P] = levels[0].gather(x)
         res = om.kerngen(k, sols[P], *bc) - b
         assert np.sqrt(om.dot(res, res)) <= 2e-8 * np.sqrt(om.dot(b, b)), P
-    assert its[1] <= 40, its
+    # free-slip on both radii converges more slowly (the smoother's diagonal leaves out the rotation penalty)
+    assert its[1] <= (40 if bc != (2, 2) else 90), its
     for P in (2, 3, 5):
         assert np.allclose(evs[P], evs[1], rtol=1e-10), (evs[P], evs[1])
         assert abs(its[P] - its[1]) <= 1, its
         assert rel(sols[P], sols[1]) <= 1e-6, P
+
+
+@pytest.mark.parametrize("level", [3, 4])
+def test_emulated_ranks_freeslip_both_radii(level):
+    """free-slip on both radii over 2-10 emulated ranks: every rank's part of the rotation dots
+    (tn_shard_penalty_dots), their sum, the apply with the sums (tn_shard_epsdivdiv_apply_fsfs) and the exchange
+    give the oracle's whole-shell apply with the rigid-rotation penalty"""
+    from terraneo_b200.distributed import EmulatedShell
+    om = Mesh(level)
+    k, src = _inputs(om)
+    want = om.kerngen(k, src, 2, 2)
+    for P in (2, 3, 5, 8, 10):
+        D = EmulatedShell(level, P)
+        for dtype, tol in ((torch.float64, 1e-12), (torch.float32, 2e-5)):
+            kk = [t.to(dtype) for t in D.scatter(k)]
+            ss = [t.to(dtype) for t in D.scatter(src)]
+            dd = D.vector(3, dtype)
+            D.epsdivdiv_apply(kk, ss, dd, 2, 2)
+            assert rel(D.gather(dd), want) <= tol, (P, dtype)
