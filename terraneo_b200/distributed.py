@@ -44,6 +44,31 @@ def _comp_ptrs(t):
     return C.ptrs(*[t[c].data_ptr() for c in range(t.shape[0])])
 
 
+def _f64(what, *ts):
+    """the FP64-only shard calls: refuse other dtypes and non-contiguous or host tensors before any kernel sees
+    their pointers"""
+    for t in ts:
+        if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous():
+            raise TypeError(f"{what}: needs contiguous float64 CUDA tensors, got {t.dtype} on {t.device}")
+
+
+def _fields(what, shard, dtype, *ts):
+    """every tensor a field of `shard`, shaped (1 to 3 components, diamonds, N+1, N+1, N+1), contiguous, on the GPU,
+    of dtype: checked before a kernel gets the component pointers, so no launch reads or writes past a tensor"""
+    for t in ts:
+        if (t.dtype != dtype or not t.is_cuda or not t.is_contiguous() or t.dim() != 5
+                or tuple(t.shape[1:]) != shard.shape or not 1 <= t.shape[0] <= 3):
+            raise TypeError(f"{what}: needs contiguous {dtype} CUDA fields of shape (ncomp,) + {shard.shape}, got "
+                            f"{tuple(t.shape)} {t.dtype} on {t.device}")
+
+
+def _scalar(what, shard, dtype, k):
+    """a coefficient field passed by its data pointer: the shard's stored nodes, contiguous, on the GPU"""
+    if k.dtype != dtype or not k.is_cuda or not k.is_contiguous() or k.numel() != shard.stored_nodes:
+        raise TypeError(f"{what}: the coefficient field needs {shard.stored_nodes} contiguous {dtype} CUDA values, "
+                        f"got {tuple(k.shape)} {k.dtype} on {k.device}")
+
+
 def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
@@ -98,6 +123,10 @@ class ShellShard:
         """The kerngen apply on this rank's cells; with COMM_ADDITIVE the copies on this rank are summed (the
         cross-rank copies by pack / all-reduce / unpack)."""
         f64 = src.dtype == torch.float64
+        _fields("epsdivdiv_apply", self, src.dtype, src, dst)
+        _scalar("epsdivdiv_apply", self, src.dtype, k)
+        if src.shape[0] != 3 or dst.shape[0] != 3:
+            raise TypeError("epsdivdiv_apply: src and dst need 3 components")
         p = C.EpsDivDivParams(bc_cmb, bc_surface, int(diagonal), apply_mode, comm_mode, penalty_eps)
         fn = C.lib().tn_shard_epsdivdiv_apply_f64 if f64 else C.lib().tn_shard_epsdivdiv_apply_f32
         C.check(fn(self.handle, ctypes.byref(p), ctypes.c_void_p(k.data_ptr()), _comp_ptrs(src), _comp_ptrs(dst),
@@ -105,12 +134,21 @@ class ShellShard:
 
     def penalty_dots(self, src, dots):
         """this rank's part of the three rigid-rotation dots of src into the device tensor dots (3 doubles)"""
+        _fields("penalty_dots", self, src.dtype, src)
+        _f64("penalty_dots", dots)
+        if src.shape[0] != 3 or dots.numel() < 3:
+            raise TypeError("penalty_dots: src needs 3 components, dots 3 doubles")
         fn = C.lib().tn_shard_penalty_dots_f64 if src.dtype == torch.float64 else C.lib().tn_shard_penalty_dots_f32
         C.check(fn(self.handle, _comp_ptrs(src), ctypes.c_void_p(dots.data_ptr()), _stream()), "tn_shard_penalty_dots")
 
     def epsdivdiv_apply_fsfs(self, k, src, dst, dots, apply_mode=C.APPLY_REPLACE, comm_mode=C.COMM_ADDITIVE,
                              penalty_eps=1.0):
         """the free-slip (both radii) apply with the whole shell's rotation dots given (device tensor, 3 doubles)"""
+        _fields("epsdivdiv_apply_fsfs", self, src.dtype, src, dst)
+        _scalar("epsdivdiv_apply_fsfs", self, src.dtype, k)
+        _f64("epsdivdiv_apply_fsfs", dots)
+        if src.shape[0] != 3 or dst.shape[0] != 3 or dots.numel() < 3:
+            raise TypeError("epsdivdiv_apply_fsfs: src and dst need 3 components, dots 3 doubles")
         p = C.EpsDivDivParams(C.BC_FREESLIP, C.BC_FREESLIP, 0, apply_mode, comm_mode, penalty_eps)
         fn = C.lib().tn_shard_epsdivdiv_apply_fsfs_f64 if src.dtype == torch.float64 else \
             C.lib().tn_shard_epsdivdiv_apply_fsfs_f32
@@ -118,16 +156,25 @@ class ShellShard:
                    ctypes.c_void_p(dots.data_ptr()), _stream()), "tn_shard_epsdivdiv_apply_fsfs")
 
     def pack(self, fields, buf):
+        _fields("pack", self, fields.dtype, fields)
+        if buf.dtype != fields.dtype or not buf.is_cuda or buf.numel() < fields.shape[0] * self.exchange_values:
+            raise TypeError("pack: the exchange buffer needs ncomp x exchange_values entries of the fields' dtype")
         fn = C.lib().tn_shard_pack_f64 if fields.dtype == torch.float64 else C.lib().tn_shard_pack_f32
         C.check(fn(self.handle, _comp_ptrs(fields), fields.shape[0], ctypes.c_void_p(buf.data_ptr()), _stream()),
                 "tn_shard_pack")
 
     def unpack(self, buf, fields):
+        _fields("unpack", self, fields.dtype, fields)
+        if buf.dtype != fields.dtype or not buf.is_cuda or buf.numel() < fields.shape[0] * self.exchange_values:
+            raise TypeError("unpack: the exchange buffer needs ncomp x exchange_values entries of the fields' dtype")
         fn = C.lib().tn_shard_unpack_f64 if fields.dtype == torch.float64 else C.lib().tn_shard_unpack_f32
         C.check(fn(self.handle, ctypes.c_void_p(buf.data_ptr()), _comp_ptrs(fields), fields.shape[0], _stream()),
                 "tn_shard_unpack")
 
     def local_dot(self, a, b):
+        _fields("local_dot", self, torch.float64, a, b)
+        if a.shape[0] != b.shape[0]:
+            raise TypeError("local_dot: the fields need the same number of components")
         r = ctypes.c_double()
         C.check(C.lib().tn_shard_vec_dot_f64(self.handle, a.shape[0], _comp_ptrs(a), _comp_ptrs(b), ctypes.byref(r),
                                              _stream()), "tn_shard_vec_dot_f64")
@@ -135,6 +182,9 @@ class ShellShard:
 
     def lincomb(self, y, c0, coeffs, xs):
         """y = c0 + sum_i coeffs[i] xs[i] (up to three inputs, FP64)."""
+        _fields("lincomb", self, torch.float64, y, *xs)
+        if any(x.shape[0] != y.shape[0] for x in xs) or len(xs) > 3:
+            raise TypeError("lincomb: up to three inputs with the output's number of components")
         c = (ctypes.c_double * 3)(*list(coeffs) + [0.0] * (3 - len(coeffs)))
         x = (ctypes.c_void_p * 9)()  # three pointer slots per input vector
         for i, v in enumerate(xs):
@@ -146,12 +196,20 @@ class ShellShard:
     # multigrid pieces: this shard and the same rank's shard one level coarser
     def prolong_add(self, coarse, src_c, dst_f):
         """dst_f += P src_c (constant prolongation)"""
+        _fields("prolong_add", coarse, torch.float64, src_c)
+        _fields("prolong_add", self, torch.float64, dst_f)
+        if src_c.shape[0] != dst_f.shape[0]:
+            raise TypeError("prolong_add: the fields need the same number of components")
         C.check(C.lib().tn_shard_prolongation_constant_f64(self.handle, coarse.handle, src_c.shape[0], C.APPLY_ADD,
                                                            _comp_ptrs(src_c), _comp_ptrs(dst_f), _stream()),
                 "tn_shard_prolongation_constant_f64")
 
     def restrict(self, coarse, src_f, dst_c):
         """dst_c = R src_f (constant restriction, coarse copies on this rank summed)"""
+        _fields("restrict", self, torch.float64, src_f)
+        _fields("restrict", coarse, torch.float64, dst_c)
+        if src_f.shape[0] != dst_c.shape[0]:
+            raise TypeError("restrict: the fields need the same number of components")
         C.check(C.lib().tn_shard_restriction_constant_f64(self.handle, coarse.handle, src_f.shape[0], _comp_ptrs(src_f),
                                                           _comp_ptrs(dst_c), _stream()),
                 "tn_shard_restriction_constant_f64")
@@ -160,20 +218,31 @@ class ShellShard:
         """dst_c = src_f at the coarse nodes; a scalar field may come without its component axis"""
         src_f = src_f.unsqueeze(0) if src_f.dim() == 4 else src_f
         dst_c = dst_c.unsqueeze(0) if dst_c.dim() == 4 else dst_c
+        _fields("inject", self, torch.float64, src_f)
+        _fields("inject", coarse, torch.float64, dst_c)
+        if src_f.shape[0] != dst_c.shape[0]:
+            raise TypeError("inject: the fields need the same number of components")
         C.check(C.lib().tn_shard_injection_f64(self.handle, coarse.handle, src_f.shape[0], _comp_ptrs(src_f),
                                                _comp_ptrs(dst_c), _stream()), "tn_shard_injection_f64")
 
     def invert(self, y):
+        _fields("invert", self, torch.float64, y)
         C.check(C.lib().tn_shard_vec_invert_f64(self.handle, y.shape[0], _comp_ptrs(y), _stream()),
                 "tn_shard_vec_invert_f64")
 
     def mult(self, y, x):
         """y *= x elementwise"""
+        _fields("mult", self, torch.float64, y, x)
+        if x.shape[0] != y.shape[0]:
+            raise TypeError("mult: the fields need the same number of components")
         C.check(C.lib().tn_shard_vec_mult_f64(self.handle, y.shape[0], _comp_ptrs(y), _comp_ptrs(x), _stream()),
                 "tn_shard_vec_mult_f64")
 
     def chebyshev_step(self, x, d, b, ax, inv_diag, alpha, beta):
         """d = alpha D^-1 (b - ax) + beta d;  x += d"""
+        _fields("chebyshev_step", self, torch.float64, x, d, b, ax, inv_diag)
+        if len({t.shape[0] for t in (x, d, b, ax, inv_diag)}) != 1:
+            raise TypeError("chebyshev_step: the fields need the same number of components")
         C.check(C.lib().tn_shard_vec_chebyshev_step_f64(self.handle, x.shape[0], _comp_ptrs(x), _comp_ptrs(d),
                                                         _comp_ptrs(b), _comp_ptrs(ax), _comp_ptrs(inv_diag), alpha,
                                                         beta, _stream()), "tn_shard_vec_chebyshev_step_f64")

@@ -290,3 +290,27 @@ def test_emulated_ranks_freeslip_both_radii(level):
             dd = D.vector(3, dtype)
             D.epsdivdiv_apply(kk, ss, dd, 2, 2)
             assert rel(D.gather(dd), want) <= tol, (P, dtype)
+
+
+def test_shard_calls_refuse_mismatched_tensors():
+    """wrong dtypes, shapes, component counts and host tensors are refused before a kernel sees their pointers"""
+    from terraneo_b200.distributed import ShellShard
+    sh = ShellShard(3, 2, 0)
+    good = sh.vector(3)
+    k = torch.ones(sh.shape, dtype=torch.float64, device="cuda")
+    bad = [sh.vector(3, torch.float32), torch.zeros((3, 1) + sh.shape[1:], dtype=torch.float64, device="cuda"),
+           good.cpu(), good[:, :1], good.transpose(3, 4)]
+    for b in bad:
+        with pytest.raises(TypeError):
+            sh.local_dot(good, b)
+        with pytest.raises(TypeError):
+            sh.lincomb(good, 0.0, [1.0], [b])
+        with pytest.raises(TypeError):
+            sh.epsdivdiv_apply(k, b, good, 1, 1)
+    with pytest.raises(TypeError):
+        sh.epsdivdiv_apply(k[:1], good, sh.vector(3), 1, 1)
+    with pytest.raises(TypeError):
+        sh.pack(good, torch.zeros(1, dtype=torch.float64, device="cuda"))
+    coarse = ShellShard(2, 2, 0)
+    with pytest.raises(TypeError):
+        sh.restrict(coarse, good, sh.vector(3))  # the destination lives on the coarse shard
