@@ -441,7 +441,9 @@ TN_API int tn_krylov_axpy_dot_f32( int nseg, const tn_mesh* const* mesh, float* 
  * after tn_pcg_begin_f64 on r = b - A x.  Once the stopping rule fires
  * (relres <= rtol or |r| < atol; begin: |r0| < atol) every later step leaves
  * x, r, p and state untouched, so a caller may read the flag only now and
- * then, or issue all iterations. */
+ * then, or issue all iterations.  iteration <= 0 takes the step number from the state (the count of the
+ * steps done so far + 1), so a captured graph of steps can be replayed; the caller issues at most max_iterations
+ * steps in all (the history has room for that many). */
 TN_API int tn_pcg_begin_f64( int nseg, const tn_mesh* const* mesh, const double* const* r, double* const* p,
                              double* state, double atol, void* stream );
 TN_API int tn_pcg_pap_f64( int nseg, const tn_mesh* const* mesh, const double* const* ap, const double* const* p,

@@ -163,18 +163,53 @@ class DevicePCG
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         cudaStreamIsCapturing( stream(), &cs );
         const bool capturing = cs != cudaStreamCaptureStatusNone;
-        for ( int it = 1; it <= prm_.max_iterations; ++it )
-        {
-            if ( !capturing && ( it == 1 || ( it - 1 ) % check_every_ == 0 ) && done() )
-                break;
+        // one step; it <= 0: the step number follows the device's count (replayable in a graph)
+        auto step = [&]( int it ) {
             apply( A, p, ap );
             check( tn_pcg_pap_f64( sp.n, sp.mesh, sap.f, sp.f, st, stream() ), "pcg_pap" );
             check( tn_pcg_update_f64( sx.n, sx.mesh, sx.f, sr.f, sp.f, sap.f, st, it, prm_.relative_residual_tolerance,
                                       prm_.absolute_residual_tolerance, stream() ),
                    "pcg_update" );
             check( tn_pcg_direction_f64( sp.n, sp.mesh, sp.f, sr.f, st, stream() ), "pcg_direction" );
+        };
+        if ( capturing || !graphs || check_every_ < 2 )
+        {
+            for ( int it = 1; it <= prm_.max_iterations; ++it )
+            {
+                if ( !capturing && ( it == 1 || ( it - 1 ) % check_every_ == 0 ) && done() )
+                    break;
+                step( it );
+            }
+            return;
+        }
+        // Outside a capture: the first step runs eagerly (tables an operator builds on first use), then a graph of
+        // check_every steps, captured once per operator and storage, is replayed with the stopping flag read
+        // between replays; the steps after convergence are no-ops on the device.  At most max_iterations steps
+        // are issued.
+        int issued = 0;
+        if ( prm_.max_iterations >= 1 && !done() )
+            step( ++issued );
+        const std::vector< const void* > key{ &A, sx.f[0], sr.f[0], sp.f[0], sap.f[0] };
+        while ( issued < prm_.max_iterations && !done() )
+        {
+            if ( issued + check_every_ > prm_.max_iterations )
+            {
+                while ( issued < prm_.max_iterations )
+                {
+                    step( 0 );
+                    ++issued;
+                }
+                break;
+            }
+            if ( !chunk_ || chunk_key_ != key )
+                capture_chunk( step, key );
+            if ( cudaGraphLaunch( static_cast< cudaGraphExec_t >( chunk_.get() ), stream() ) != cudaSuccess )
+                throw std::runtime_error( "DevicePCG: cudaGraphLaunch failed" );
+            issued += check_every_;
         }
     }
+    // replay the iterations from a captured graph outside stream capture (on by default)
+    bool graphs = true;
     // statistics of the last solve (synchronises)
     SolverStatistics statistics() const
     {
@@ -200,10 +235,68 @@ class DevicePCG
             throw std::runtime_error( "DevicePCG: reading the done flag failed" );
         return f != 0.0;
     }
+    // capture check_every steps (device-counted) on a private stream into chunk_
+    template < typename Step >
+    void capture_chunk( Step& step, const std::vector< const void* >& key )
+    {
+        if ( !cap_ )
+        {
+            cudaStream_t c = nullptr;
+            if ( cudaStreamCreateWithFlags( &c, cudaStreamNonBlocking ) != cudaSuccess )
+                throw std::runtime_error( "DevicePCG: creating the capture stream failed" );
+            cap_ = std::shared_ptr< void >( c, []( void* q ) { cudaStreamDestroy( static_cast< cudaStream_t >( q ) ); } );
+        }
+        cudaStream_t cap   = static_cast< cudaStream_t >( cap_.get() );
+        cudaStream_t saved = stream_ref();
+        // the capture stream starts after the work already queued on the solve's stream
+        cudaEvent_t ev = nullptr;
+        if ( cudaEventCreateWithFlags( &ev, cudaEventDisableTiming ) != cudaSuccess ||
+             cudaEventRecord( ev, saved ) != cudaSuccess || cudaStreamWaitEvent( cap, ev, 0 ) != cudaSuccess )
+        {
+            if ( ev )
+                cudaEventDestroy( ev );
+            throw std::runtime_error( "DevicePCG: ordering the capture stream failed" );
+        }
+        cudaEventDestroy( ev );
+        stream_ref()  = cap;
+        cudaGraph_t g = nullptr;
+        if ( cudaStreamBeginCapture( cap, cudaStreamCaptureModeThreadLocal ) != cudaSuccess )
+        {
+            stream_ref() = saved;
+            throw std::runtime_error( "DevicePCG: cudaStreamBeginCapture failed" );
+        }
+        try
+        {
+            for ( int i = 0; i < check_every_; ++i )
+                step( 0 );
+        }
+        catch ( ... )
+        {
+            cudaStreamEndCapture( cap, &g );
+            if ( g )
+                cudaGraphDestroy( g );
+            stream_ref() = saved;
+            throw;
+        }
+        const cudaError_t ec = cudaStreamEndCapture( cap, &g );
+        stream_ref()         = saved;
+        cudaGraphExec_t e    = nullptr;
+        if ( ec != cudaSuccess || cudaGraphInstantiate( &e, g, 0 ) != cudaSuccess )
+        {
+            if ( g )
+                cudaGraphDestroy( g );
+            throw std::runtime_error( "DevicePCG: capturing the iteration failed" );
+        }
+        cudaGraphDestroy( g );
+        chunk_     = std::shared_ptr< void >( e, []( void* q ) { cudaGraphExecDestroy( static_cast< cudaGraphExec_t >( q ) ); } );
+        chunk_key_ = key;
+    }
     IterativeSolverParameters  prm_;
     std::vector< V >           tmps_;
     int                        check_every_;
     std::shared_ptr< double >  state_;
+    std::shared_ptr< void >    cap_, chunk_;
+    std::vector< const void* > chunk_key_;
 };
 
 // power_iteration (power_iteration.hpp:13-48) from a deterministic random start

@@ -228,10 +228,12 @@ __global__ void pcg_update_kernel( Segs s, SegPtr< T > x, SegPtr< T > r, SegPtr<
         }
     if ( block_sum_finish< 1 >( &acc, partials, counter, scratch ) && threadIdx.x == 0 )
     {
+        // it <= 0: the step number follows the device's count (a replayed graph of steps)
+        const int    k  = it > 0 ? it : int( state[kIts] ) + 1;
         const double rr = scratch[0], ar = sqrt( rr ), rel = ar / state[kR0];
-        state[kHist + it] = rel;
-        state[kRelres]    = rel;
-        state[kIts]       = double( it );
+        state[kHist + k] = rel;
+        state[kRelres]   = rel;
+        state[kIts]      = double( k );
         if ( rel <= rtol || ar < atol )
             state[kDone] = 1.0;
         else
@@ -333,7 +335,7 @@ extern "C" int tn_pcg_update_f64( int nseg, const tn_mesh* const* mesh, double* 
          ( rc = make_ptr( nseg, r, pr, false, "pcg_update" ) ) || ( rc = make_ptr( nseg, p, pp, false, "pcg_update" ) ) ||
          ( rc = make_ptr( nseg, ap, pa, false, "pcg_update" ) ) )
         return rc;
-    TN_CHECK_ARG( state && iteration >= 1, "pcg_update: bad state or iteration" );
+    TN_CHECK_ARG( state, "pcg_update: state is NULL" );
     const tn_mesh* m0 = mesh[0];
     pcg_update_kernel< double ><<< red_blocks( s ), kThreads, 0, as_stream( stream ) >>>(
         s, px, pr, pp, pa, state, iteration, rtol, atol, m0->d_red_partials, m0->d_red_counter, m0->d_red_result + 8 );
