@@ -53,17 +53,6 @@ struct Ptr3
     __host__ __device__ __forceinline__ T* at( int c ) const { return c == 0 ? p[0] : ( c == 1 ? p[1] : p[2] ); }
 };
 
-// Device-side view of the mesh handed to kernels by value.
-template < typename T >
-struct MeshView
-{
-    int      N;      // cells per side
-    int      n1;     // nodes per side (N + 1)
-    size_t   ns;     // stored nodes 10 (N+1)^3 (whole shell)
-    const T* coords; // [10][n1][n1][3] lateral unit-sphere points
-    const T* radii;  // [10][n1]
-};
-
 }  // namespace tn
 
 namespace tn {
