@@ -11,7 +11,10 @@ pytestmark = pytest.mark.gpu
 BCS = [(1, 1), (2, 2), (2, 1), (1, 2), (0, 0), (0, 1), (0, 2)]
 
 
-@pytest.fixture(scope="module", params=[2, 3, 4])
+# level 1 (the smallest shell, the cell kernel), levels 2-3 (the cell kernel and 8-column tiles), 4 (16-column
+# tiles, half the lanes of the radial chunk idle) and 5 (one full radial chunk, the top level written by its last
+# lane)
+@pytest.fixture(scope="module", params=[1, 2, 3, 4, 5])
 def setup(request):
     from terraneo_b200 import shell
     L = request.param

@@ -9,7 +9,7 @@ from oracle_lib import Mesh
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("L", [2, 3])
+@pytest.mark.parametrize("L", [1, 2, 3])
 @pytest.mark.parametrize("mode", [0, 1, 2])
 def test_kmass(L, mode):
     from terraneo_b200 import shell
