@@ -42,6 +42,20 @@ void set_error( const std::string& msg );
 // Launch-error check after a kernel launch.
 #define TN_LAUNCH_CHECK() TN_CUDA_TRY( cudaGetLastError() )
 
+// Launch settings cached per device (the SM count, a kernel's shared-memory limit, a cluster size): indexed by
+// the calling thread's current device, so one process may drive several GPUs.
+constexpr int kMaxDevices = 64;
+inline int current_device()
+{
+    int d = 0;
+    if ( cudaGetDevice( &d ) != cudaSuccess || d < 0 || d >= kMaxDevices )
+    {
+        (void) cudaGetLastError();
+        return 0;
+    }
+    return d;
+}
+
 inline cudaStream_t as_stream( void* s ) { return reinterpret_cast< cudaStream_t >( s ); }
 
 template < typename T >

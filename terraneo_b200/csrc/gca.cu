@@ -1180,10 +1180,14 @@ __global__ void __launch_bounds__( kCpThreads ) spcg_step_cluster_kernel( Cluste
 // multi-launch form is used).
 int spcg_cluster_size()
 {
-    static int size = -1;
-    if ( size >= 0 )
+    static int size_of[kMaxDevices];
+    static bool known[kMaxDevices] = {};
+    const int   dev  = current_device();
+    int&        size = size_of[dev];
+    if ( known[dev] )
         return size;
-    size = 0;
+    known[dev] = true;
+    size       = 0;
     if ( cudaFuncSetAttribute( spcg_step_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1 ) !=
          cudaSuccess )
     {

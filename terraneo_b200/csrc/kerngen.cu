@@ -863,14 +863,12 @@ template < typename T, int TS >
 int tile_launch( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k, Ptr3< const T > s, Ptr3< T > o, bool fsfs,
                  bool skip_cmb, bool skip_surf, cudaStream_t st )
 {
-    const int  N = m->N;
-    static int num_sms = 0;
-    if ( num_sms == 0 )
-    {
-        int dev = 0;
-        TN_CUDA_TRY( cudaGetDevice( &dev ) );
-        TN_CUDA_TRY( cudaDeviceGetAttribute( &num_sms, cudaDevAttrMultiProcessorCount, dev ) );
-    }
+    const int  N   = m->N;
+    const int  dev = current_device();
+    static int sms_of[kMaxDevices] = {};
+    if ( sms_of[dev] == 0 )
+        TN_CUDA_TRY( cudaDeviceGetAttribute( &sms_of[dev], cudaDevAttrMultiProcessorCount, dev ) );
+    const int num_sms = sms_of[dev];
     const int       xtiles = N / TS;
     const long long items  = (long long) m->nd * xtiles * ( N + 1 );
     const int       grid   = int( std::min< long long >( (long long) num_sms * Tile< TS >::MinBlocks, items ) );
@@ -890,12 +888,12 @@ int tile_launch( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k, Ptr
                        skip_surf,
                        fsfs ? m->d_red_result + 3 : nullptr };
     const size_t smem      = tile_smem_bytes< T, TS >( m->n1, seg );
-    static int   smem_attr = 0; // largest dynamic shared memory requested so far for this instantiation
-    if ( int( smem ) > smem_attr )
+    static int   smem_attr[kMaxDevices] = {}; // largest dynamic shared memory set so far for this instantiation
+    if ( int( smem ) > smem_attr[dev] )
     {
         TN_CUDA_TRY( cudaFuncSetAttribute( kerngen_tile_kernel< T, TS >, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            int( smem ) ) );
-        smem_attr = int( smem );
+        smem_attr[dev] = int( smem );
     }
     kerngen_tile_kernel< T, TS ><<< grid, Tile< TS >::Threads, smem, st >>>( P );
     TN_LAUNCH_CHECK();
