@@ -335,6 +335,10 @@ TN_API int tn_vec_invert_f64( const tn_mesh* mesh, int ncomp, double* const* y, 
 TN_API int tn_vec_invert_f32( const tn_mesh* mesh, int ncomp, float* const* y, void* stream );
 TN_API int tn_vec_mult_f64( const tn_mesh* mesh, int ncomp, double* const* y, const double* const* x, void* stream );
 TN_API int tn_vec_mult_f32( const tn_mesh* mesh, int ncomp, float* const* y, const float* const* x, void* stream );
+/* masked_sum (grid_operations.hpp:569-590) with the ownership mask: the sum over owned nodes, components summed,
+ * compensated FP64 accumulation; the number of owned nodes (count_masked, :544) is tn_mesh_dims' unique_nodes */
+TN_API int tn_vec_sum_f64( const tn_mesh* mesh, int ncomp, const double* const* x, double* result, void* stream );
+TN_API int tn_vec_sum_f32( const tn_mesh* mesh, int ncomp, const float* const* x, double* result, void* stream );
 TN_API int tn_vec_max_abs_f64( const tn_mesh* mesh, int ncomp, const double* const* x, double* result, void* stream );
 TN_API int tn_vec_max_abs_f32( const tn_mesh* mesh, int ncomp, const float* const* x, double* result, void* stream );
 TN_API int tn_vec_has_nan_or_inf_f64( const tn_mesh* mesh, int ncomp, const double* const* x, int* result, void* stream );

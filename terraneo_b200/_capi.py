@@ -167,6 +167,8 @@ _SIGS = {
                                              P(c_void_p), c_void_p]),
     "tn_vec_lincomb_f64": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p), c_void_p]),
     "tn_vec_lincomb_f32": (c_int, [c_void_p, c_int, P(c_void_p), c_double, c_int, P(c_double), P(c_void_p), c_void_p]),
+    "tn_vec_sum_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_double), c_void_p]),
+    "tn_vec_sum_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_double), c_void_p]),
     "tn_vec_dot_f64": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_double), c_void_p]),
     "tn_vec_dot_f32": (c_int, [c_void_p, c_int, P(c_void_p), P(c_void_p), P(c_double), c_void_p]),
     "tn_vec_invert_f64": (c_int, [c_void_p, c_int, P(c_void_p), c_void_p]),

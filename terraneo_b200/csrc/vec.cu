@@ -116,6 +116,21 @@ __global__ void dot_kernel( size_t ns, int ncomp, Ptr3< const T > a, Ptr3< const
     block_sum_finish< 1 >( &acc, partials, counter, result );
 }
 
+// Owned-node sum of a field's components (masked_sum, grid_operations.hpp:569-590), compensated FP64.
+template < typename T >
+__global__ void sum_kernel( size_t ns, int ncomp, Ptr3< const T > a, const uint8_t* __restrict__ owned,
+                            double* partials, unsigned int* counter, double* result )
+{
+    Neumaier acc;
+    for ( int c = 0; c < ncomp; ++c )
+    {
+        const T* __restrict__ pa = a.at( c );
+        for ( size_t i = blockIdx.x * size_t( blockDim.x ) + threadIdx.x; i < ns; i += size_t( gridDim.x ) * blockDim.x )
+            acc.add( owned[i] ? double( pa[i] ) : 0.0 );
+    }
+    block_sum_finish< 1 >( &acc, partials, counter, result );
+}
+
 // One Chebyshev step (linalg/solvers/chebyshev.hpp:127-160) fused into a
 // single pass: z = D^{-1} (b - Ax), d = alpha z + beta d, x = x + d.
 template < typename T >
@@ -355,6 +370,20 @@ int vec_lincomb( const tn_mesh* m, int ncomp, T* const* y, double c0, int nx, co
 }
 
 template < typename T >
+int vec_sum( const tn_mesh* m, int ncomp, const T* const* a, double* result, cudaStream_t st )
+{
+    TN_CHECK_ARG( m && result, "sum: bad arguments" );
+    Ptr3< const T > pa;
+    if ( const int rc = ptr3c( ncomp, a, pa, "sum" ) )
+        return rc;
+    const unsigned blocks = std::min< unsigned >( grid_for( m->ns, 8 ), kRedMaxBlocks );
+    sum_kernel< T ><<< blocks, kThreads, 0, st >>>( m->ns, ncomp, pa, m->d_node_owned, m->d_red_partials,
+                                                   m->d_red_counter, m->d_red_result );
+    TN_LAUNCH_CHECK();
+    return fetch_result( m, 1, st, result );
+}
+
+template < typename T >
 int vec_dot( const tn_mesh* m, int ncomp, const T* const* a, const T* const* b, double* result, cudaStream_t st )
 {
     TN_CHECK_ARG( m && result, "dot: bad arguments" );
@@ -420,6 +449,14 @@ extern "C" int tn_vec_lincomb_f32( const tn_mesh* m, int ncomp, float* const* y,
                                    const float* const* x, void* s )
 {
     return vec_lincomb< float >( m, ncomp, y, c0, nx, c, x, as_stream( s ) );
+}
+extern "C" int tn_vec_sum_f64( const tn_mesh* m, int ncomp, const double* const* a, double* r, void* s )
+{
+    return vec_sum< double >( m, ncomp, a, r, as_stream( s ) );
+}
+extern "C" int tn_vec_sum_f32( const tn_mesh* m, int ncomp, const float* const* a, double* r, void* s )
+{
+    return vec_sum< float >( m, ncomp, a, r, as_stream( s ) );
 }
 extern "C" int tn_vec_dot_f64( const tn_mesh* m, int ncomp, const double* const* a, const double* const* b, double* r,
                                void* s )

@@ -95,6 +95,13 @@ class _VectorBase:
         C.check(f(self.mesh.handle, self.ncomp, self.comp_ptrs(), other.comp_ptrs(), ctypes.byref(r), _stream()), "dot")
         return r.value
 
+    def masked_sum_impl(self):
+        """the sum over owned nodes (masked_sum with the ownership mask), components summed"""
+        r = ctypes.c_double()
+        f = getattr(C.lib(), f"tn_vec_sum_{self.tag}")
+        C.check(f(self.mesh.handle, self.ncomp, self.comp_ptrs(), ctypes.byref(r), _stream()), "sum")
+        return r.value
+
     def invert_entries_impl(self):
         C.check(getattr(C.lib(), f"tn_vec_invert_{self.tag}")(self.mesh.handle, self.ncomp, self.comp_ptrs(),
                                                               _stream()), "invert")

@@ -117,3 +117,19 @@ def test_chebyshev_step(meshes, dtype, beta, layout):
     tol = 1e-14 if dtype == torch.float64 else 2e-6
     assert rel(dev["d"].cpu().numpy(), dn) <= tol
     assert rel(dev["x"].cpu().numpy(), ref["x"] + dn) <= tol
+
+
+@pytest.mark.parametrize("L", [1, 3])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_masked_sum_over_owned_nodes(L, dtype):
+    """tn_vec_sum (masked_sum with the ownership mask, grid_operations.hpp:569) against the oracle's owned mask"""
+    from terraneo_b200 import shell
+    om, pm = Mesh(L), shell.ShellMesh(L)
+    rs = np.random.RandomState(3 + L)
+    a = rs.normal(size=(3,) + om.shape)
+    v = shell.VectorQ1Vec(pm, dtype)
+    v.set_numpy(a)
+    want = float((a.astype(np.float32 if dtype == torch.float32 else np.float64).astype(np.float64)
+                  * om.omask[None]).sum())
+    got = v.masked_sum_impl()
+    assert abs(got - want) <= 1e-12 * np.abs(a).sum(), (got, want)
