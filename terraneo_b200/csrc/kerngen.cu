@@ -43,14 +43,15 @@ constexpr int kSegMax = 24; // longest run of node rows a CTA finalises in one y
 constexpr int kLev    = kRC + 1; // node levels per chunk
 constexpr int kSlots  = 4;       // row ring depth (prefetch distance 3)
 
-// The shape of the tiled kernel for x tiles of TS owned node columns: TS + 1
-// warps (cell strips) per CTA, so a tile recomputes one strip of cells its
-// neighbour also computes (1/TS of the work); 16 columns where N allows it
-// (one 544-thread CTA per SM), 8 at N = 8 (two 288-thread CTAs per SM).
+// The shape of the tiled kernel for x tiles of TS cell strips: TS warps per
+// CTA, one strip each; 16 strips where N allows it (one 512-thread CTA per SM),
+// 8 at N = 8 (two 256-thread CTAs per SM).  Sixteen warps per SM leave 128
+// registers per thread (each SM sub-partition holds 16,384 registers for its
+// four warps; a seventeenth warp would cap every thread at 96).
 template < int TS >
 struct Tile
 {
-    static constexpr int W         = TS + 1;        // warps = cell strips per CTA
+    static constexpr int W         = TS;            // warps = cell strips per CTA
     static constexpr int Threads   = W * 32;
     static constexpr int MinBlocks = TS == 8 ? 2 : 1; // resident CTAs per SM the kernel is compiled for
     static constexpr int Group     = Threads / 4;   // fill threads per field
@@ -73,37 +74,42 @@ struct TileParams
     const double* beta;                   // fs/fs penalty vector (3) or nullptr
 };
 
-// Per-wedge flux vectors S1 = sigma q0, S2 = sigma q1, S3 = kappa sigma q2 with
-// sigma = omega (2 sym(G) - 2/3 tr(G) I), G = q0 (x) v1 + q1 (x) v2 + q2 (x) kappa v3.
+// Per-wedge flux vectors S1 = sigma q0, S2 = sigma q1, S3 = sigma kq2 with
+// sigma = omega (2 sym(G) - 2/3 tr(G) I), G = q0 (x) v1 + q1 (x) v2 + kq2 (x) v3
+// and kq2 = kappa q2 (the radial factor folded into the third row once per wedge).
+// A lane whose cell does not contribute (ok false) gets sigma = 0: the six stress
+// components are selected, so its fluxes are exact zeros whatever its (possibly
+// unloaded) corner values hold.
 template < typename T >
 __device__ __forceinline__ void wedge_flux( const T* __restrict__ g, const T v1[3], const T v2[3], const T v3[3],
-                                            T kappa, T omega, T S1[3], T S2[3], T S3[3] )
+                                            T kappa, T omega, bool ok, T S1[3], T S2[3], T S3[3] )
 {
     T q0[3], q1[3], q2[3];
 #pragma unroll
     for ( int a = 0; a < 3; ++a )
-        q0[a] = g[a], q1[a] = g[3 + a], q2[a] = g[6 + a];
-    const T w3[3] = { kappa * v3[0], kappa * v3[1], kappa * v3[2] };
-    const T G00   = q0[0] * v1[0] + q1[0] * v2[0] + q2[0] * w3[0];
-    const T G11   = q0[1] * v1[1] + q1[1] * v2[1] + q2[1] * w3[1];
-    const T G22   = q0[2] * v1[2] + q1[2] * v2[2] + q2[2] * w3[2];
-    const T H01   = q0[0] * v1[1] + q1[0] * v2[1] + q2[0] * w3[1] + q0[1] * v1[0] + q1[1] * v2[0] + q2[1] * w3[0];
-    const T H02   = q0[0] * v1[2] + q1[0] * v2[2] + q2[0] * w3[2] + q0[2] * v1[0] + q1[2] * v2[0] + q2[2] * w3[0];
-    const T H12   = q0[1] * v1[2] + q1[1] * v2[2] + q2[1] * w3[2] + q0[2] * v1[1] + q1[2] * v2[1] + q2[2] * w3[1];
-    const T div   = G00 + G11 + G22;
-    const T tdiv  = T( 2.0 / 3.0 ) * div;
-    const T s00 = omega * ( T( 2 ) * G00 - tdiv ), s11 = omega * ( T( 2 ) * G11 - tdiv ),
-            s22 = omega * ( T( 2 ) * G22 - tdiv );
-    const T s01 = omega * H01, s02 = omega * H02, s12 = omega * H12;
+        q0[a] = g[a], q1[a] = g[3 + a], q2[a] = kappa * g[6 + a];
+    const T G00  = q0[0] * v1[0] + q1[0] * v2[0] + q2[0] * v3[0];
+    const T G11  = q0[1] * v1[1] + q1[1] * v2[1] + q2[1] * v3[1];
+    const T G22  = q0[2] * v1[2] + q1[2] * v2[2] + q2[2] * v3[2];
+    const T H01  = q0[0] * v1[1] + q1[0] * v2[1] + q2[0] * v3[1] + q0[1] * v1[0] + q1[1] * v2[0] + q2[1] * v3[0];
+    const T H02  = q0[0] * v1[2] + q1[0] * v2[2] + q2[0] * v3[2] + q0[2] * v1[0] + q1[2] * v2[0] + q2[2] * v3[0];
+    const T H12  = q0[1] * v1[2] + q1[1] * v2[2] + q2[1] * v3[2] + q0[2] * v1[1] + q1[2] * v2[1] + q2[2] * v3[1];
+    const T div  = G00 + G11 + G22;
+    const T tdiv = T( 2.0 / 3.0 ) * div;
+    T       s00 = omega * ( T( 2 ) * G00 - tdiv ), s11 = omega * ( T( 2 ) * G11 - tdiv ),
+      s22 = omega * ( T( 2 ) * G22 - tdiv );
+    T s01 = omega * H01, s02 = omega * H02, s12 = omega * H12;
+    if ( !ok )
+        s00 = s11 = s22 = s01 = s02 = s12 = T( 0 );
     S1[0] = s00 * q0[0] + s01 * q0[1] + s02 * q0[2];
     S1[1] = s01 * q0[0] + s11 * q0[1] + s12 * q0[2];
     S1[2] = s02 * q0[0] + s12 * q0[1] + s22 * q0[2];
     S2[0] = s00 * q1[0] + s01 * q1[1] + s02 * q1[2];
     S2[1] = s01 * q1[0] + s11 * q1[1] + s12 * q1[2];
     S2[2] = s02 * q1[0] + s12 * q1[1] + s22 * q1[2];
-    S3[0] = kappa * ( s00 * q2[0] + s01 * q2[1] + s02 * q2[2] );
-    S3[1] = kappa * ( s01 * q2[0] + s11 * q2[1] + s12 * q2[2] );
-    S3[2] = kappa * ( s02 * q2[0] + s12 * q2[1] + s22 * q2[2] );
+    S3[0] = s00 * q2[0] + s01 * q2[1] + s02 * q2[2];
+    S3[1] = s01 * q2[0] + s11 * q2[1] + s12 * q2[2];
+    S3[2] = s02 * q2[0] + s12 * q2[1] + s22 * q2[2];
 }
 
 // Tiled owner-computes apply.  CTA = kW warps; warp w handles the cell strip
@@ -111,7 +117,11 @@ __device__ __forceinline__ void wedge_flux( const T* __restrict__ g, const T v1[
 // warp marches along y: at step s it computes cell (X, cy) and finalises node
 // row cy, carrying its contributions to row cy+1 in registers.  A node column
 // X gets its two halves from strips X (left side) and X-1 (right side); right
-// halves are exchanged through shared memory, one barrier per step.  Node rows
+// halves are exchanged through shared memory, one barrier per step.  The tile's
+// first column sx0 (sx0 > 0) has its right half in the previous tile's last
+// strip: both tiles add their halves to it atomically (two addends onto the
+// zeros seam_zero_kernel left, so the sum does not depend on their order), and
+// every other node is written once with plain stores.  Node rows
 // (the CTA's kW+1 columns x 3 src components + k x 33 levels) are streamed
 // into a 4-slot shared-memory ring with cp.async three rows ahead (fill_row),
 // so global latency overlaps the arithmetic of the previous steps.  The radial chunk
@@ -125,7 +135,7 @@ size_t tile_smem_bytes( int n1, int SY )
     const size_t rows  = size_t( kSlots ) * ( kW + 1 ) * 4 * kLev;
     const size_t xbuf  = size_t( 2 ) * kW * 3 * kLev;
     const size_t carry = size_t( kW + 1 ) * ( SY + 2 ) * 3;
-    const size_t top   = size_t( kW ) * 2 * 4 * 3;
+    const size_t top   = size_t( kW ) * 6;
     return sizeof( T ) * ( radii + geo + rows + xbuf + carry + top ) + 16 + 32 * kThreads; // + fill descriptors
 }
 
@@ -198,8 +208,8 @@ __global__ void __launch_bounds__( Tile< TS >::Threads, Tile< TS >::MinBlocks ) 
     T* s_rows  = s_geo + kW * ( SM + 2 ) * 20;
     T* s_xbuf  = s_rows + kSlots * ( kW + 1 ) * 4 * kLev;
     T* s_carry = s_xbuf + 2 * kW * 3 * kLev;
-    T* s_top   = s_carry + ( kW + 1 ) * ( SM + 2 ) * 3; // [w][parity][corner][c]: top contributions of lane RC-1
-    uint4* s_fill = reinterpret_cast< uint4* >( ( reinterpret_cast< uintptr_t >( s_top + kW * 24 ) + 15 ) &
+    T* s_top   = s_carry + ( kW + 1 ) * ( SM + 2 ) * 3; // [w][column][c]: top sums of lane RC-1 (level r0 + RC)
+    uint4* s_fill = reinterpret_cast< uint4* >( ( reinterpret_cast< uintptr_t >( s_top + kW * 6 ) + 15 ) &
                                                 ~uintptr_t( 15 ) ); // fill descriptors, 16-byte aligned
     auto slot  = [s_rows]( int y ) { return s_rows + ( ( y + kSlots ) % kSlots ) * ( ( kW + 1 ) * 4 * kLev ); };
 
@@ -225,12 +235,14 @@ __global__ void __launch_bounds__( Tile< TS >::Threads, Tile< TS >::MinBlocks ) 
         g += row_hi - row_lo + 1;
         const int  tx        = int( tile % P.xtiles );
         const int  d         = int( tile / P.xtiles );
-        const int  sx0       = tx * kTS - 1; // strip of warp 0
+        const int  sx0       = tx * kTS; // strip of warp 0
         const int  nsteps    = row_hi - row_lo + 2; // step s computes cell cy = row_lo - 1 + s
         const int  X         = sx0 + w;
         const bool strip_ok  = X >= 0 && X <= N - 1;
-        const bool col_owned = w >= 1;                              // node column X belongs to this tile
-        const bool owns_last = tx == P.xtiles - 1 && w == kW - 1;   // ... and node column N = X + 1
+        const bool seam_lo   = w == 0 && tx > 0;                   // column X: its right half is the last tile's
+        const bool last_tile = tx == P.xtiles - 1;
+        const bool seam_hi   = w == kW - 1 && !last_tile;           // column X + 1: the next tile's column sx0
+        const bool owns_last = w == kW - 1 && last_tile;            // column N = X + 1, whole
         const int  s0        = row_lo == 0 ? 1 : 0;
         const T*   radii     = s_radii + d * ( ( n1 + 1 ) & ~1 );
 
@@ -240,8 +252,14 @@ __global__ void __launch_bounds__( Tile< TS >::Threads, Tile< TS >::MinBlocks ) 
             const int wdg = i & 1, cs = i >> 1;
             const int ww = cs / nsteps, s = cs % nsteps;
             const int Xg = sx0 + ww, Y = row_lo - 1 + s;
+            T*        gg = s_geo + ( ( ww * ( SM + 2 ) + s ) * 2 + wdg ) * 10;
             if ( Xg < 0 || Xg > N - 1 || Y < 0 || Y > N - 1 )
+            {
+                // no cell: zero geometry, so the masked flux of the step is exactly zero
+                for ( int j = 0; j < 10; ++j )
+                    gg[j] = T( 0 );
                 continue;
+            }
             const double* c00 = P.coords + lat_index( n1, d, Xg, Y ) * 3;
             const double* c10 = P.coords + lat_index( n1, d, Xg + 1, Y ) * 3;
             const double* c01 = P.coords + lat_index( n1, d, Xg, Y + 1 ) * 3;
@@ -251,7 +269,6 @@ __global__ void __launch_bounds__( Tile< TS >::Threads, Tile< TS >::MinBlocks ) 
                 lateral_geometry( c00, c10, c01, q, &adet );
             else
                 lateral_geometry( c11, c01, c10, q, &adet );
-            T* gg = s_geo + ( ( ww * ( SM + 2 ) + s ) * 2 + wdg ) * 10;
             for ( int j = 0; j < 9; ++j )
                 gg[j] = T( q[j] );
             gg[9] = T( adet );
@@ -282,11 +299,11 @@ __global__ void __launch_bounds__( Tile< TS >::Threads, Tile< TS >::MinBlocks ) 
             const T   wbase = h * T( 0.25 / 6.0 ); // omega = (k_sum / 6) |det M| h / 4
             const int lb    = min( lane, kRC - 1 );
 
-            T  cL[3] = { 0, 0, 0 }, cR[3] = { 0, 0, 0 };
-            T* tw    = s_top + w * 24;
-            if ( lane < 24 )
-                tw[lane] = T( 0 );
-            __syncwarp();
+            // y-carry of the cell row below: its contributions to the node row it shares with this one, per
+            // column (L: X, R: X + 1), bottom (level r) and top (level r + 1, still to be handed to the lane
+            // above) parts kept apart so one shuffle per column and component moves both rows' tops
+            T  cLb[3] = { 0, 0, 0 }, cLt[3] = { 0, 0, 0 }, cRb[3] = { 0, 0, 0 }, cRt[3] = { 0, 0, 0 };
+            T* tw = s_top + w * 6; // lane RC - 1: its top sums (level r0 + RC) of columns X and X + 1
             for ( int s = s0; s < nsteps; ++s )
             {
                 const int  cy      = row_lo - 1 + s;
@@ -315,45 +332,35 @@ __global__ void __launch_bounds__( Tile< TS >::Threads, Tile< TS >::MinBlocks ) 
                     }
                     const T* g0 = s_geo + ( ( w * ( SM + 2 ) + s ) * 2 ) * 10;
                     const T* g1 = g0 + 10;
+                    const bool ok = cell_ok && lane_ok;
                     T        v1[3], v2[3], v3[3], A1[3], A2[3], A3[3], B1[3], B2[3], B3[3];
 #pragma unroll
                     for ( int c = 0; c < 3; ++c )
                         v1[c] = S[1][c] - S[0][c], v2[c] = S[2][c] - S[0][c], v3[c] = D[0][c] + D[1][c] + D[2][c];
-                    wedge_flux( g0, v1, v2, v3, kappa, wbase * ( K[0] + K[1] + K[2] ) * g0[9], A1, A2, A3 );
+                    wedge_flux( g0, v1, v2, v3, kappa, wbase * ( K[0] + K[1] + K[2] ) * g0[9], ok, A1, A2, A3 );
 #pragma unroll
                     for ( int c = 0; c < 3; ++c )
                         v1[c] = S[2][c] - S[3][c], v2[c] = S[1][c] - S[3][c], v3[c] = D[3][c] + D[2][c] + D[1][c];
-                    wedge_flux( g1, v1, v2, v3, kappa, wbase * ( K[3] + K[2] + K[1] ) * g1[9], B1, B2, B3 );
-                    const bool ok = cell_ok && lane_ok;
+                    wedge_flux( g1, v1, v2, v3, kappa, wbase * ( K[3] + K[2] + K[1] ) * g1[9], ok, B1, B2, B3 );
 #pragma unroll
                     for ( int c = 0; c < 3; ++c )
                     {
                         const T xa = A1[c] + A2[c], xb = B1[c] + B2[c];
                         const T s33 = A3[c] + B3[c];
                         const T e10 = A1[c] + B2[c], e01 = A2[c] + B1[c];
-                        T       bo[4], tp[4], val[4];
-                        bo[0] = -xa - A3[c], tp[0] = -xa + A3[c];
-                        bo[1] = e10 - s33, tp[1] = e10 + s33;
-                        bo[2] = e01 - s33, tp[2] = e01 + s33;
-                        bo[3] = -xb - B3[c], tp[3] = -xb + B3[c];
-#pragma unroll
-                        for ( int q = 0; q < 4; ++q )
-                        {
-                            if ( !ok )
-                                bo[q] = tp[q] = T( 0 );
-                            const T below = __shfl_up_sync( FULL, tp[q], 1 );
-                            val[q]        = bo[q] + ( lane > 0 ? below : T( 0 ) );
-                        }
-                        L[c] = val[0] + cL[c];
-                        R[c] = val[1] + cR[c];
-                        cL[c] = val[2], cR[c] = val[3];
+                        // the cell's bottom (level r) and top (level r + 1) parts at its four corner columns
+                        const T bo0 = -xa - A3[c], tp0 = -xa + A3[c];
+                        const T bo1 = e10 - s33, tp1 = e10 + s33;
+                        const T bo2 = e01 - s33, tp2 = e01 + s33;
+                        const T bo3 = -xb - B3[c], tp3 = -xb + B3[c];
+                        // node row cy: this cell's near corners plus the carried far corners of the cell below
+                        const T tL = tp0 + cLt[c], tR = tp1 + cRt[c];
+                        const T bL = __shfl_up_sync( FULL, tL, 1 ), bR = __shfl_up_sync( FULL, tR, 1 );
+                        L[c]   = bo0 + cLb[c] + ( lane > 0 ? bL : T( 0 ) );
+                        R[c]   = bo1 + cRb[c] + ( lane > 0 ? bR : T( 0 ) );
+                        cLb[c] = bo2, cLt[c] = tp2, cRb[c] = bo3, cRt[c] = tp3;
                         if ( lane == RC - 1 ) // level r0 + RC: only the top cell of the chunk contributes
-                        {
-                            T* tcur = tw + ( s & 1 ) * 12;
-#pragma unroll
-                            for ( int q = 0; q < 4; ++q )
-                                tcur[q * 3 + c] = tp[q];
-                        }
+                            tw[c] = tL, tw[3 + c] = tR;
                     }
                 }
 
@@ -366,11 +373,9 @@ __global__ void __launch_bounds__( Tile< TS >::Threads, Tile< TS >::MinBlocks ) 
                 }
                 if ( lane == RC - 1 )
                 {
-                    const T* tcur = tw + ( s & 1 ) * 12;
-                    const T* tprv = tw + ( ( s + 1 ) & 1 ) * 12;
 #pragma unroll
                     for ( int c = 0; c < 3; ++c )
-                        xb[c * kLev + RC] = tcur[3 + c] + tprv[9 + c];
+                        xb[c * kLev + RC] = tw[3 + c];
                 }
                 __pipeline_commit();
                 __pipeline_wait_prior( kSlots - 3 );
@@ -381,26 +386,25 @@ __global__ void __launch_bounds__( Tile< TS >::Threads, Tile< TS >::MinBlocks ) 
 #pragma unroll
                 for ( int side = 0; side < 2; ++side )
                 {
-                    if ( side == 0 ? !col_owned : !owns_last )
+                    if ( side == 1 && !owns_last && !seam_hi )
                         continue;
-                    const int Xn  = X + side;
-                    const int slt = side == 0 ? w : kW;
-                    T         F[3], F32[3];
-                    const T*  xl   = s_xbuf + ( ( s & 1 ) * kW + ( w - 1 ) ) * 3 * kLev;
-                    const T*  tcur = tw + ( s & 1 ) * 12;
-                    const T*  tprv = tw + ( ( s + 1 ) & 1 ) * 12;
+                    const bool seam = side == 0 ? seam_lo : seam_hi; // half of the column: atomic add
+                    const int  Xn   = X + side;
+                    const int  slt  = side == 0 ? w : kW;
+                    T          F[3], F32[3];
+                    const T*   xl = s_xbuf + ( ( s & 1 ) * kW + max( w - 1, 0 ) ) * 3 * kLev;
 #pragma unroll
                     for ( int c = 0; c < 3; ++c )
                     {
                         if ( side == 0 )
                         {
-                            F[c]   = L[c] + ( lane < RC ? xl[c * kLev + lane] : T( 0 ) );
-                            F32[c] = tcur[c] + tprv[6 + c] + xl[c * kLev + RC];
+                            F[c]   = L[c] + ( w > 0 && lane < RC ? xl[c * kLev + lane] : T( 0 ) );
+                            F32[c] = tw[c] + ( w > 0 ? xl[c * kLev + RC] : T( 0 ) );
                         }
                         else
                         {
                             F[c]   = R[c];
-                            F32[c] = tcur[3 + c] + tprv[9 + c];
+                            F32[c] = tw[3 + c];
                         }
                     }
                     T* carry = s_carry + ( slt * ( SM + 2 ) + s ) * 3;
@@ -413,7 +417,7 @@ __global__ void __launch_bounds__( Tile< TS >::Threads, Tile< TS >::MinBlocks ) 
                     __syncwarp();
                     const size_t nb  = lat_index( n1, d, Xn, cy ) * n1;
                     const int    lev = lane < RC ? r : N; // lanes < RC: level r; lane RC-1 also level N
-                    if ( beta )
+                    if ( beta && !( side == 1 && seam ) ) // the penalty once per node: with the left half
                     {
                         const double* u   = P.coords + lat_index( n1, d, Xn, cy ) * 3;
                         const double  rr  = double( radii[lane < RC ? r : 0] ), rN = double( radii[N] );
@@ -437,9 +441,14 @@ __global__ void __launch_bounds__( Tile< TS >::Threads, Tile< TS >::MinBlocks ) 
                         T* p0 = o0 + nb + r;
                         T* p1 = o1 + nb + r;
                         T* p2 = o2 + nb + r;
-                        *p0   = add_mode ? *p0 + F[0] : F[0];
-                        *p1   = add_mode ? *p1 + F[1] : F[1];
-                        *p2   = add_mode ? *p2 + F[2] : F[2];
+                        if ( seam )
+                            atomicAdd( p0, F[0] ), atomicAdd( p1, F[1] ), atomicAdd( p2, F[2] );
+                        else
+                        {
+                            *p0 = add_mode ? *p0 + F[0] : F[0];
+                            *p1 = add_mode ? *p1 + F[1] : F[1];
+                            *p2 = add_mode ? *p2 + F[2] : F[2];
+                        }
                     }
                     if ( lane == RC - 1 )
                     {
@@ -448,9 +457,14 @@ __global__ void __launch_bounds__( Tile< TS >::Threads, Tile< TS >::MinBlocks ) 
                             T* p0 = o0 + nb + N;
                             T* p1 = o1 + nb + N;
                             T* p2 = o2 + nb + N;
-                            *p0   = add_mode ? *p0 + F32[0] : F32[0];
-                            *p1   = add_mode ? *p1 + F32[1] : F32[1];
-                            *p2   = add_mode ? *p2 + F32[2] : F32[2];
+                            if ( seam )
+                                atomicAdd( p0, F32[0] ), atomicAdd( p1, F32[1] ), atomicAdd( p2, F32[2] );
+                            else
+                            {
+                                *p0 = add_mode ? *p0 + F32[0] : F32[0];
+                                *p1 = add_mode ? *p1 + F32[1] : F32[1];
+                                *p2 = add_mode ? *p2 + F32[2] : F32[2];
+                            }
                         }
                         else
                         {
@@ -856,6 +870,20 @@ CellParams< T > cell_params( const tn_mesh* m, const tn_epsdivdiv_params* p, con
         m->N, m->n1, m->d_coords, mesh_radii< T >( m ), k, src, dst, p->bc_cmb, p->bc_surface, p->diagonal, m->nd };
 }
 
+// Zeros the tile-seam node columns X = j TS (0 < j < xtiles) of dst, which the
+// tile kernel then fills with two atomic halves: one block per (component,
+// diamond, seam), each column a contiguous run of n1 x n1 values.
+template < typename T >
+__global__ void __launch_bounds__( 256 ) seam_zero_kernel( Ptr3< T > o, int n1, int ts, int seams )
+{
+    const int    b = blockIdx.x, j = b % seams + 1, dc = b / seams;
+    const int    d = dc / 3, c = dc - 3 * d;
+    T*           col = o.at( c ) + lat_index( n1, d, j * ts, 0 ) * n1;
+    const int    n   = n1 * n1;
+    for ( int i = threadIdx.x; i < n; i += blockDim.x )
+        col[i] = T( 0 );
+}
+
 }  // namespace
 
 // The tiled kernel over the interior layers (all layers the boundary-cell kernel does not take).
@@ -887,6 +915,11 @@ int tile_launch( const tn_mesh* m, const tn_epsdivdiv_params* p, const T* k, Ptr
                        skip_cmb,
                        skip_surf,
                        fsfs ? m->d_red_result + 3 : nullptr };
+    if ( xtiles > 1 && p->apply_mode != TN_APPLY_ADD )
+    {
+        seam_zero_kernel< T ><<< unsigned( m->nd * 3 * ( xtiles - 1 ) ), 256, 0, st >>>( o, m->n1, TS, xtiles - 1 );
+        TN_LAUNCH_CHECK();
+    }
     const size_t smem      = tile_smem_bytes< T, TS >( m->n1, seg );
     static int   smem_attr[kMaxDevices] = {}; // largest dynamic shared memory set so far for this instantiation
     if ( int( smem ) > smem_attr[dev] )
