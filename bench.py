@@ -39,7 +39,7 @@ BYTES_PER_NODE_F64 = 56  # 3 src + 1 k + 3 dst doubles per stored node
 BYTES_PER_NODE_F32 = 28
 # DRAM bytes (read + write) of one level-6 kerngen_tile_kernel<double, 16> launch,
 # from an ncu capture (profiles/kerngen_tile_kernel_f64_L6_dirichlet.md)
-TILE_TRAFFIC_BYTES = 141040384 + 48047360
+TILE_TRAFFIC_BYTES = 141426176 + 43898112
 
 
 def _case_laplace6(shell, C, torch):
