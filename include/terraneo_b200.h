@@ -470,6 +470,22 @@ TN_API int tn_laplace_pcg_solve_f64( const tn_mesh* mesh, const double* b, doubl
                                      double relative_tolerance, double absolute_tolerance, int* iterations,
                                      double* relative_residual );
 
+/* The library's Krylov solver templates without a preconditioner on the
+ * scalar Laplace with Dirichlet elimination (fe/wedge/operators/shell/laplace.hpp:106,
+ * treat_boundary = true), from the given x (the compositions of the
+ * reference's tests/test_laplace_fgmres.cpp, test_laplace_minres.cpp and
+ * test_laplace_bicgstab.cpp): solver 0 = FGMRES(param) (linalg/solvers/fgmres.hpp:108-330),
+ * 1 = PMINRES (linalg/solvers/pminres.hpp:30-175, param unused),
+ * 2 = PBiCGStab(param) (linalg/solvers/pbicgstab.hpp:29-290) with the shadow
+ * residual `shadow` (device, stored nodes) or, when NULL, this library's
+ * seeded random field. history (host, optional): the relative residual
+ * estimates the solver records (entry 0 = 1), at most history_capacity of
+ * them; *history_count = how many it recorded. */
+TN_API int tn_laplace_krylov_solve_f64( const tn_mesh* mesh, int solver, int param, const double* b, double* x,
+                                        const double* shadow, int max_iterations, double relative_tolerance,
+                                        double absolute_tolerance, int* iterations, double* history,
+                                        int history_capacity, int* history_count );
+
 /* Multigrid-preconditioned Krylov solve (CG, BiCGStab(2) or MINRES) on
  * DivKGrad (k NULL: k = 1, the Laplace) with
  * homogeneous Dirichlet elimination on both radii: one V-cycle per CG

@@ -133,6 +133,8 @@ _SIGS = {
                                           c_void_p]),
     "tn_epsdivdiv3x2_apply_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, P(c_void_p), P(c_void_p),
                                           c_void_p]),
+    "tn_laplace_krylov_solve_f64": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int, c_double,
+                                             c_double, P(c_int), c_void_p, c_int, P(c_int)]),
     "tn_laplace_pcg_solve_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, P(c_int),
                                          P(c_double)]),
     "tn_stokes_solver_create": (c_int, [P(StokesParams), c_double, c_double, c_void_p, P(c_void_p)]),

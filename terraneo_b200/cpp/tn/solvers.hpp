@@ -739,7 +739,8 @@ inline std::vector< double > dense_solve_full_pivot( std::vector< double > M, st
 
 // Preconditioned BiCGStab(l) (pbicgstab.hpp:29-290): l BiCG steps and an
 // l-dimensional minimal-residual update per iteration, left preconditioning;
-// the shadow residual is the deterministic randomize of this library.
+// the shadow residual is the deterministic randomize of this library, or a
+// given field (set_shadow: the reference draws its own, pbicgstab.hpp:98).
 template < typename Op, typename Prec = IdentitySolver< Op > >
 class PBiCGStab
 {
@@ -752,11 +753,18 @@ class PBiCGStab
             throw std::runtime_error( "PBiCGStab: needs 2 (l + 1) + 2 temporary vectors" );
     }
     SolverStatistics stats;
-    void             solve_impl( Op& A, V& x, const V& b )
+    // use `shadow` as the shadow residual of every later solve instead of a random field
+    void set_shadow( const V& shadow )
+    {
+        assign( rshadow(), shadow );
+        shadow_given_ = true;
+    }
+    void solve_impl( Op& A, V& x, const V& b )
     {
         using S = typename V::ScalarType;
         stats   = {};
-        randomize( rshadow() );
+        if ( !shadow_given_ )
+            randomize( rshadow() );
         for ( int j = 0; j < l_ + 1; ++j )
             assign( us( j ), S( 0 ) );
         apply( A, x, rs( 0 ) );
@@ -828,6 +836,7 @@ class PBiCGStab
     IterativeSolverParameters prm_;
     std::vector< V >          tmp_;
     Prec                      prec_;
+    bool                      shadow_given_ = false;
 };
 
 // FGMRES(m) with modified Gram-Schmidt Arnoldi and Givens rotations

@@ -783,6 +783,71 @@ extern "C" int tn_laplace_pcg_solve_f64( const tn_mesh* mesh, const double* b, d
     }
 }
 
+// The library's Krylov solver templates without a preconditioner on the scalar
+// Laplace with Dirichlet elimination (the compositions of the reference's
+// tests/test_laplace_fgmres.cpp, test_laplace_minres.cpp, test_laplace_bicgstab.cpp).
+extern "C" int tn_laplace_krylov_solve_f64( const tn_mesh* mesh, int solver, int param, const double* b, double* x,
+                                            const double* shadow, int max_iterations, double relative_tolerance,
+                                            double absolute_tolerance, int* iterations, double* history,
+                                            int history_capacity, int* history_count )
+{
+    TN_CHECK_ARG( mesh && b && x, "tn_laplace_krylov_solve_f64: null argument" );
+    TN_CHECK_ARG( solver >= 0 && solver <= 2, "tn_laplace_krylov_solve_f64: solver must be 0, 1 or 2" );
+    TN_CHECK_ARG( solver == 1 || param >= 1, "tn_laplace_krylov_solve_f64: restart / l must be at least 1" );
+    TN_CHECK_ARG( history_capacity >= 0 && ( history_capacity == 0 || history ),
+                  "tn_laplace_krylov_solve_f64: history buffer missing" );
+    try
+    {
+        using Lap = Laplace< double >;
+        Mesh                     m = Mesh::wrap( mesh );
+        Lap                      A( m, true, false );
+        VectorQ1Scalar< double > vb( m, const_cast< double* >( b ) ), vx( m, x );
+        auto                     tmps = [&m]( int n ) {
+            std::vector< VectorQ1Scalar< double > > t;
+            for ( int i = 0; i < n; ++i )
+                t.emplace_back( m );
+            return t;
+        };
+        const IterativeSolverParameters ip{ max_iterations, relative_tolerance, absolute_tolerance };
+        SolverStatistics                st;
+        if ( solver == 0 )
+        {
+            IdentitySolver< Lap >                id;
+            FGMRES< Lap, IdentitySolver< Lap > > s( tmps( 2 * param + 4 ), param, ip, id );
+            solve( s, A, vx, vb );
+            st = s.stats;
+        }
+        else if ( solver == 1 )
+        {
+            PMINRES< Lap > s( ip, tmps( 7 ) );
+            solve( s, A, vx, vb );
+            st = s.stats;
+        }
+        else
+        {
+            PBiCGStab< Lap > s( param, ip, tmps( 2 * ( param + 1 ) + 2 ) );
+            if ( shadow )
+                s.set_shadow( VectorQ1Scalar< double >( m, const_cast< double* >( shadow ) ) );
+            solve( s, A, vx, vb );
+            st = s.stats;
+        }
+        TN_CUDA_TRY( cudaDeviceSynchronize() );
+        if ( iterations )
+            *iterations = st.iterations;
+        const int n = int( st.relative_residuals.size() );
+        for ( int i = 0; i < std::min( n, history_capacity ); ++i )
+            history[i] = st.relative_residuals[size_t( i )];
+        if ( history_count )
+            *history_count = n;
+        return TN_OK;
+    }
+    catch ( const std::exception& e )
+    {
+        set_error( std::string( "tn_laplace_krylov_solve_f64: " ) + e.what() );
+        return TN_ERR_STATE;
+    }
+}
+
 // compile the header-only operators that no driver above instantiates
 template class tn::VectorMass< double, 3 >;
 template class tn::VectorMass< float, 3 >;

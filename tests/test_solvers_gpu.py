@@ -335,3 +335,57 @@ def test_stokes_production_stack_own_estimates_close_to_reference():
                            gca=S["gca"])
     it, rr = s.solve(fu, fp, xu, xp)
     assert abs(it - int(g["iterations_11"])) <= 3, (it, int(g["iterations_11"]))
+
+
+@pytest.mark.parametrize("solver", ["fgmres", "minres", "bicgstab"])
+def test_laplace_krylov_templates_match_reference_golden(solver):
+    """The library's FGMRES(10), PMINRES and PBiCGStab(2) templates on the golden level-2 Dirichlet Laplace from
+    x = 0 (the reference's tests/test_laplace_fgmres.cpp, test_laplace_minres.cpp, test_laplace_bicgstab.cpp
+    compositions), PBiCGStab given the shadow residual the reference drew: the reference's number of
+    iterations, its residual history to rounding amplified by the Krylov process, and its solution."""
+    import ctypes
+    import os
+    import sys
+    from terraneo_b200 import _capi as C, shell
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden as G
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_L2.npz"))
+    fine, coarse = Mesh(G.L), Mesh(G.L - 1)
+    b = G.cg_rhs(G.inputs(fine, coarse)["s"])
+    pm = shell.ShellMesh(G.L)
+    vb, vx, vs = shell.VectorQ1Scalar(pm), shell.VectorQ1Scalar(pm), shell.VectorQ1Scalar(pm)
+    vb.set_numpy(b)
+    if solver == "fgmres":
+        code, param, case, key = 0, G.FGMRES_CASE["restart"], G.FGMRES_CASE, "fgmres"
+    elif solver == "minres":
+        code, param, case, key = 1, 0, G.MINRES_CASE, "minres"
+    else:
+        code, param, case, key = 2, G.BICGSTAB_CASE["l"], G.BICGSTAB_CASE, "bicgstab"
+        vs.set_numpy(g["bicgstab_rshadow"].reshape(pm.shape))
+    hist = np.zeros(case["maxit"] + 2)
+    it, cnt = ctypes.c_int(), ctypes.c_int()
+    rc = C.lib().tn_laplace_krylov_solve_f64(pm.handle, code, param, vb.data.data_ptr(), vx.data.data_ptr(),
+                                             vs.data.data_ptr() if code == 2 else None, case["maxit"], case["tol"],
+                                             1e-30, ctypes.byref(it), hist.ctypes.data, len(hist), ctypes.byref(cnt))
+    C.check(rc, "laplace_krylov_solve")
+    ref_hist = g[f"{key}_hist"]
+    # the same steps (one more or fewer only if a residual lands on the tolerance within rounding)
+    n = min(cnt.value, len(ref_hist))
+    assert abs(cnt.value - len(ref_hist)) <= 1, (cnt.value, len(ref_hist))
+    np.testing.assert_allclose(hist[:n], ref_hist[:n], rtol=1e-5, atol=1e-14)
+    assert rel(vx.numpy()[0], g[f"{key}_x"]) <= (1e-11 if cnt.value == len(ref_hist) else 1e-8)
+
+
+def test_laplace_krylov_rejects_bad_arguments():
+    import ctypes
+    from terraneo_b200 import _capi as C, shell
+    pm = shell.ShellMesh(2)
+    vb, vx = shell.VectorQ1Scalar(pm), shell.VectorQ1Scalar(pm)
+    it = ctypes.c_int()
+    L = C.lib()
+    assert L.tn_laplace_krylov_solve_f64(pm.handle, 3, 2, vb.data.data_ptr(), vx.data.data_ptr(), None, 10, 1e-8,
+                                         1e-30, ctypes.byref(it), None, 0, None) != 0
+    assert L.tn_laplace_krylov_solve_f64(pm.handle, 0, 0, vb.data.data_ptr(), vx.data.data_ptr(), None, 10, 1e-8,
+                                         1e-30, ctypes.byref(it), None, 0, None) != 0
+    assert L.tn_laplace_krylov_solve_f64(pm.handle, 2, 2, vb.data.data_ptr(), vx.data.data_ptr(), None, 10, 1e-8,
+                                         1e-30, ctypes.byref(it), None, 4, None) != 0
