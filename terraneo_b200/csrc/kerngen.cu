@@ -5,16 +5,17 @@
 // (centroid) wedge rule and k averaged over the six wedge nodes (:1189-1196).
 //
 // Kernels
-//  * kerngen_tile_kernel: the hot path.  One CTA owns a tile of 8 x 8 lateral
-//    node columns of one diamond over the full radial extent and computes every
-//    cell touching them (owner computes: no global atomics, no zero-fill pass,
-//    every stored node written exactly once with coalesced stores).  Lanes of
-//    a warp are 32 consecutive radial cells of one cell column, so loads are
-//    coalesced along r and the radial node sharing is a warp shuffle; lateral
-//    node sharing goes through a shared-memory accumulator in four colour
-//    phases (cells of one colour share no node).  Per-wedge geometry is
-//    factorised as J = M diag(r_mid, r_mid, dr/2) with M the lateral triangle
-//    matrix, so M^{-T} is computed once per tile and each cell only rescales.
+//  * kerngen_tile_kernel: the hot path.  One CTA of TS warps owns TS cell
+//    strips (x) of one diamond over a run of y rows and the full radial
+//    extent; each warp marches its strip along y, lanes = 32 consecutive
+//    radial cells, so loads are coalesced along r and the radial node sharing
+//    is a warp shuffle.  Node rows stream through a shared-memory ring; the
+//    node column shared by two strips of the CTA is summed in shared memory,
+//    the one shared with the previous tile (seam column) by two atomic halves
+//    onto the zeros seam_zero_kernel writes first; every other node is written
+//    once with coalesced stores.  Per-wedge geometry is factorised as
+//    J = M diag(r_mid, r_mid, dr/2) with M the lateral triangle matrix, so
+//    M^{-T} is computed once per wedge column and each cell only rescales.
 //    Boundary-layer cells of a non-Neumann boundary are left out and added by
 //  * kerngen_bcell_kernel: one thread per boundary-layer cell with the full
 //    boundary logic of cell_full (Dirichlet elimination with kept diagonal,
